@@ -1,0 +1,134 @@
+/*
+ * ugks_b200.h -- C ABI of the B200 (sm_100a, FP64) UGKS2D kinetic hot path.
+ *
+ * The reference (Sherlmess/UGKS2D_high_order, Fortran 2008 + MPI) drives its hot path through
+ * argument-less subroutines that act on module globals, called from Solve_UGKS
+ * (src/mod_Solve.f90:84-186).  Each entry point below replaces one of them; the citation on each
+ * declaration names the routine it stands in for.  Plain pointers and sizes only: a Fortran
+ * `bind(C)` interface or ctypes can call every function.
+ *
+ * Host arrays use the reference's backing-store layout with the halo stripped:
+ *   h, b : [ny][nx][nvel]  (Fortran cell_h_store(Nvel, 1:nx, 1:ny), velocity fastest)
+ *   W    : [ny][nx][4]     (ctr%conVars packed)
+ * The library owns the device mirrors for the context lifetime; state stays resident in HBM
+ * between calls and crosses PCIe only in upload/download.
+ *
+ * Every function returns UGKS_OK (0) or a positive status.  Numerical failures detected on the
+ * device are reported with the reference's own MPI_Abort codes (ugks_status_reference_code).
+ * Nothing traps on the device; a failing call leaves the context usable.
+ * One context is not thread-safe: all its work is serialised on one CUDA stream.
+ */
+#ifndef UGKS_B200_H
+#define UGKS_B200_H
+
+#include <stddef.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define UGKS_OK 0
+#define UGKS_EINVAL 1        /* bad argument */
+#define UGKS_ECUDA 2         /* CUDA runtime error */
+#define UGKS_ENUMERIC 3      /* device-side numerical gate failed (see ugks_last_status) */
+#define UGKS_ETIMEOUT 4      /* a bounded device-side wait expired */
+#define UGKS_ENOMEM 5
+#define UGKS_EUNSUPPORTED 6
+
+#define UGKS_METHOD_EXPLICIT 0
+#define UGKS_METHOD_IMPLICIT_STEADY 1
+
+/* Subset of the reference's &config_para / &boundary_para that the hot path reads
+ * (src/mod_ImportPara.f90:141-173, set_const_para :911-930). */
+typedef struct ugks_params {
+    int nx, ny;              /* Nx_all, Ny_all (one domain; the reference's NP_X x NP_Y blocking collapses) */
+    int nvel;                /* Nu*Nv */
+    double dx, dy;           /* uniform cell lengths of Mesh2d.dat */
+    int ck;                  /* internal degrees of freedom */
+    double pr;               /* Prandtl number (Shakhov) */
+    double omega;            /* power-law viscosity exponent */
+    double mu_ref;           /* CouetteMuRef */
+    double cfl;              /* CFL */
+    double wall_ux[2];       /* WallUx(3), WallUx(4): bottom and top wall speed */
+    double wall_tnative[2];  /* wall temperature (native scale, Tw) bottom/top */
+    double fixed_dt;         /* > 0: Time_global_fixed with this dt; <= 0: global CFL dt */
+    int method;              /* UGKS_METHOD_* */
+    /* ImplicitSteady controls (mod_SteadyImplicit.f90, mod_ImplicitMacro.f90, mod_ImplicitMicro.f90) */
+    double ncfl;             /* Implicit_nCFL */
+    int nslab;               /* NP_Y of the reference blocking: LU-SGS/PR2 seams are block-Jacobi per slab */
+    int mass_rescale;        /* ClosedCouetteMassRescale */
+    int macro_sweeps;        /* Implicit_MacroSweeps */
+    double residual_tol;     /* Implicit_ResidualTol */
+    double moment_tol;       /* Implicit_MomentTol */
+    double min_alpha;        /* Implicit_MinAlpha */
+} ugks_params;
+
+typedef struct ugks_ctx ugks_ctx;
+
+/* Create a context on CUDA device `device` with the velocity table (u, v, w of nvel entries,
+ * k = i + (j-1)*Nu as in InitVelocityFromStructuredFile, src/mod_InitializeFlow.f90:480-509). */
+int ugks_ctx_create(const ugks_params* params, const double* u, const double* v, const double* w, int device,
+                    ugks_ctx** out);
+int ugks_ctx_destroy(ugks_ctx* ctx);
+
+/* Copy state host <-> device (the only PCIe crossings). */
+int ugks_upload_state(ugks_ctx* ctx, const double* h, const double* b, const double* W);
+int ugks_download_state(ugks_ctx* ctx, double* h, double* b, double* W);
+
+/* InitFlow_Freestream + cold-start EnforceAcceptedMomentCompatibility
+ * (src/mod_InitializeFlow.f90:826-856; src/mod_SteadyImplicit.f90:28-42). */
+int ugks_init_freestream(ugks_ctx* ctx, double rho, double U, double V, double tnative);
+
+/* TimeStep (src/mod_Solve.f90:373-421): computes dt_global on the device; *dt_out optional. */
+int ugks_timestep(ugks_ctx* ctx, double* dt_out);
+
+/* Interpolation() + Evolution() (src/mod_Interpolation.f90:26, src/mod_Evolution.f90:35-177):
+ * Van-Leer slopes fused into the UGKS face fluxes (interior faces and W2B moving walls). */
+int ugks_evolution(ugks_ctx* ctx);
+
+/* ComputeResidual() (src/mod_Residual.f90:17-132) with the unified streaming-moment projection;
+ * with_collision also forms the physical equilibrium/collision used by the implicit paths. */
+int ugks_compute_residual(ugks_ctx* ctx, int with_collision);
+
+/* ApplyExplicitUpdate() (src/mod_TimeIntegrator.f90:16-134): macro update, CN Shakhov
+ * collision with variable tau, residual norms; res_out[4] optional = the reference `res`. */
+int ugks_apply_explicit_update(ugks_ctx* ctx, double* res_out);
+
+/* nsteps full Explicit steps (TimeStep, Interpolation, Evolution, ComputeResidual,
+ * ApplyExplicitUpdate; src/mod_Solve.f90:84-186) fused into two kernels per step and replayed
+ * from a CUDA graph.  dt_out / res_out (optional) report the last step. */
+int ugks_step_explicit(ugks_ctx* ctx, int nsteps, double* dt_out, double* res_out);
+
+/* Wall Aerodynamics of the last Evolution (src/mod_Evolution.f90:2402-2409): out[2][nx][3] =
+ * local-frame (pnn, pnt, qn) per bottom/top wall face. */
+int ugks_wall_aero(ugks_ctx* ctx, double* out);
+
+/* Copy a named device work array to the host (diagnostics / parity tests).  Names:
+ * "res_w" [nc][4], "res_h", "res_b" [nc][nvel], "fxh", "fxb" [ny][nx][nvel], "fyh", "fyb"
+ * [ny+1][nx][nvel], "fxw" [ny][nx][4], "fyw" [ny+1][nx][4], "pcol_h", "pcol_b", "peq_h",
+ * "peq_b" [nc][nvel], "dt" [1]. n = number of doubles the caller's buffer holds. */
+int ugks_copy_array(ugks_ctx* ctx, const char* name, double* host, size_t n);
+
+/* Device status word of the last synchronising call and the reference abort code it maps to
+ * (101-106 GetPrimary/GetTau, 444/446 projections, 13-16 non-finite flux, 4/17 state). */
+unsigned ugks_last_status(const ugks_ctx* ctx);
+int ugks_status_reference_code(unsigned status);
+const char* ugks_error_string(int code);
+
+/* The context's CUDA stream (cudaStream_t) for event timing by the caller, and a blocking sync. */
+void* ugks_stream(ugks_ctx* ctx);
+int ugks_synchronize(ugks_ctx* ctx);
+
+/* Kernel-level timing: when enabled, ugks_step_explicit records CUDA events around each kernel
+ * launch (graph replay off) and accumulates per-kernel milliseconds and launch counts.
+ * names: "faces", "cells". */
+int ugks_profile_enable(ugks_ctx* ctx, int enable);
+int ugks_profile_read(ugks_ctx* ctx, const char* kernel, double* total_ms, long long* launches);
+
+/* Number of kernels this library launched on the context since creation (evidence counter). */
+long long ugks_launch_count(const ugks_ctx* ctx);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,855 @@
+/*
+ * ugks_oracle.c -- TEST INFRASTRUCTURE ONLY (parity checker and CPU baseline; see the header).
+ *
+ * Plain-C restatement of the reference's second-order UGKS hot path for the planar Couette
+ * case (x-periodic, diffuse moving walls at y=0 and y=H, FluxWall_type=1 + CouetteUseW2BWall,
+ * UnifiedPhysicalOperators=.true., power-law viscosity).  Loop and summation order follow the
+ * Fortran so that the restatement reproduces the reference's printed numbers to their digits.
+ * File:line citations are relative to the reference project root.
+ */
+#include "ugks_oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+#include <float.h>
+
+#define PI_D 3.14159265358979323846264338327950288
+static const double SMV = (double)FLT_MIN;   /* mod_Globaldata.f90:26 SMV = tiny(0.0_real32) */
+
+struct uo_ctx {
+    uo_params p;
+    int nc;                       /* nx*ny */
+    double area;
+    double *u, *v, *w;
+    double umax, vmax;
+    double *h, *b, *W;
+    double *sh, *sb;              /* [c][2][nvel] Van-Leer slopes; dir 0 = x, 1 = y */
+    double *fxh, *fxb, *fxw;      /* x faces [j][i][..], face i between cells i-1 and i (periodic) */
+    double *fyLh, *fyLb, *fyLw;   /* y faces [jf][i][..], jf = 0..ny; L flux */
+    double *fyRh, *fyRb, *fyRw;   /* R flux (equal to L for interior faces) */
+    double *res_w, *res_h, *res_b;  /* res_macro_flux_store, res_h/b_flux_store */
+    double *rate_w, *stream_h, *stream_b;
+    double *peq_h, *peq_b, *pcol_h, *pcol_b;
+    double *wall_aero;            /* [2][nx][3] */
+    /* scratch */
+    double *t[24];
+};
+
+/* ------------------------------------------------------------------ kinetic math library */
+
+/* GetPrimary (mod_Tools.f90:209-235) */
+static int get_primary(const uo_params* p, const double w[4], double prim[4]) {
+    for (int m = 0; m < 4; ++m) if (!isfinite(w[m])) return 101;
+    if (w[0] <= 0.0) return 102;
+    double denom = w[3] - 0.5 * (w[1] * w[1] + w[2] * w[2]) / w[0];
+    if (!isfinite(denom) || denom <= 0.0) return 103;
+    prim[0] = w[0];
+    prim[1] = w[1] / w[0];
+    prim[2] = w[2] / w[0];
+    prim[3] = 0.5 * w[0] / ((p->gamma - 1.0) * denom);
+    return 0;
+}
+
+/* GetConserved (mod_Tools.f90:190-200) */
+static void get_conserved(const uo_params* p, const double prim[4], double w[4]) {
+    w[0] = prim[0];
+    w[1] = prim[0] * prim[1];
+    w[2] = prim[0] * prim[2];
+    w[3] = 0.5 * prim[0] / (prim[3] * (p->gamma - 1.0)) + 0.5 * prim[0] * (prim[1] * prim[1] + prim[2] * prim[2]);
+}
+
+/* GetTau, power law (mod_Tools.f90:267-299) */
+static int get_tau(const uo_params* p, const double prim[4], double* tau) {
+    if (prim[0] <= 0.0 || prim[3] <= 0.0 || !isfinite(prim[0]) || !isfinite(prim[1]) ||
+        !isfinite(prim[2]) || !isfinite(prim[3])) return 104;
+    double mu = p->mu_ref * pow(1.0 / prim[3], p->omega);
+    if (!isfinite(mu) || mu <= 0.0) return 105;
+    *tau = mu / (0.5 * prim[0] / prim[3]);
+    if (!isfinite(*tau) || *tau <= 0.0) return 106;
+    return 0;
+}
+
+/* DiscreteMaxwell_LocalVec (mod_Tools.f90:44-64) */
+static void maxwell(const uo_params* p, int n, const double* vn, const double* vt, const double prim[4],
+                    double* H, double* B) {
+    double pref = prim[0] * (prim[3] / PI_D);
+    double bf = (double)p->ck / (2.0 * prim[3]);
+    for (int k = 0; k < n; ++k) {
+        double dvn = vn[k] - prim[1], dvt = vt[k] - prim[2];
+        double v2 = dvn * dvn + dvt * dvt;
+        double hk = pref * exp(-prim[3] * v2);
+        H[k] = hk;
+        B[k] = hk * bf;
+    }
+}
+
+/* ShakhovPart_LocalVec, ck>0 branch (mod_Tools.f90:110-128) */
+static void shakhov(const uo_params* p, int n, const double* H, const double* B, const double* vn,
+                    const double* vt, const double qf[2], const double prim[4], double* Hp, double* Bp) {
+    double coeff = 0.8 * (1.0 - p->pr) * prim[3] * prim[3] / prim[0];
+    for (int k = 0; k < n; ++k) {
+        double dvn = vn[k] - prim[1], dvt = vt[k] - prim[2];
+        double v2 = dvn * dvn + dvt * dvt;
+        double qdot = dvn * qf[0] + dvt * qf[1];
+        double shH = 2.0 * prim[3] * v2 - 4.0;
+        double shB = shH + 2.0 / (double)p->ck;
+        Hp[k] = coeff * qdot * shH * H[k];
+        Bp[k] = coeff * qdot * shB * B[k];
+    }
+}
+
+/* GetHeatFlux_LocalVec (mod_Tools.f90:379-400) */
+static void heat_flux(int n, const double* h, const double* b, const double* vn, const double* vt,
+                      const double* wv, const double prim[4], double q[2]) {
+    q[0] = 0.0; q[1] = 0.0;
+    for (int k = 0; k < n; ++k) {
+        double dvn = vn[k] - prim[1], dvt = vt[k] - prim[2];
+        double v2 = dvn * dvn + dvt * dvt;
+        q[0] = q[0] + 0.5 * wv[k] * dvn * (v2 * h[k] + b[k]);
+        q[1] = q[1] + 0.5 * wv[k] * dvt * (v2 * h[k] + b[k]);
+    }
+}
+
+/* MomentConserved (mod_ImplicitCommon.f90:32-40): Fortran sum() intrinsic, sequential */
+static void moment_conserved(int n, const double* h, const double* b, const double* u, const double* v,
+                             const double* wl, double m[4]) {
+    double s0 = 0, s1 = 0, s2 = 0, s3 = 0;
+    for (int k = 0; k < n; ++k) {
+        s0 += wl[k] * h[k];
+        s1 += wl[k] * u[k] * h[k];
+        s2 += wl[k] * v[k] * h[k];
+        s3 += wl[k] * ((u[k] * u[k] + v[k] * v[k]) * h[k] + b[k]);
+    }
+    m[0] = s0; m[1] = s1; m[2] = s2; m[3] = 0.5 * s3;
+}
+
+/* SolveDense4 (mod_ImplicitCommon.f90:84-113): Gauss-Jordan with partial pivoting.
+ * m is row-major m[r*4+c]. */
+int uo_solve_dense4(const double m[16], const double rhs[4], double sol[4]) {
+    double a[4][5];
+    double pscale = 0.0;
+    for (int r = 0; r < 4; ++r) {
+        for (int c = 0; c < 4; ++c) { a[r][c] = m[r * 4 + c]; if (fabs(m[r * 4 + c]) > pscale) pscale = fabs(m[r * 4 + c]); }
+        a[r][4] = rhs[r];
+    }
+    if (pscale < DBL_MIN) pscale = DBL_MIN;
+    for (int col = 0; col < 4; ++col) {
+        int piv = col;
+        for (int r = col + 1; r < 4; ++r) if (fabs(a[r][col]) > fabs(a[piv][col])) piv = r;
+        if (fabs(a[piv][col]) <= 1000.0 * DBL_EPSILON * pscale) return 0;
+        if (piv != col) for (int c = 0; c < 5; ++c) { double t = a[col][c]; a[col][c] = a[piv][c]; a[piv][c] = t; }
+        double d = a[col][col];
+        for (int c = 0; c < 5; ++c) a[col][c] = a[col][c] / d;
+        for (int r = 0; r < 4; ++r) {
+            if (r == col) continue;
+            double f = a[r][col];
+            for (int c = 0; c < 5; ++c) a[r][c] = a[r][c] - f * a[col][c];
+        }
+    }
+    for (int r = 0; r < 4; ++r) { sol[r] = a[r][4]; if (!isfinite(sol[r])) return 0; }
+    return 1;
+}
+
+/* ProjectToConservedMoments (mod_ImplicitCommon.f90:42-82).  Returns 1 when ok. */
+int uo_project_moments(int n, double* h, double* b, const double target[4], const double* u,
+                       const double* v, const double* wl, const double* ref_h, const double* ref_b) {
+    for (int m = 0; m < 4; ++m) if (!isfinite(target[m])) return 0;
+    for (int k = 0; k < n; ++k) if (!isfinite(h[k]) || !isfinite(b[k])) return 0;
+    double mom[4], rhs[4], gram[16] = {0}, lam[4];
+    moment_conserved(n, h, b, u, v, wl, mom);
+    for (int m = 0; m < 4; ++m) rhs[m] = target[m] - mom[m];
+    double sh = 0.0, sb = 0.0;
+    for (int k = 0; k < n; ++k) { if (fabs(ref_h[k]) > sh) sh = fabs(ref_h[k]); if (fabs(ref_b[k]) > sb) sb = fabs(ref_b[k]); }
+    if (sh < 1.0) sh = 1.0;
+    if (sb < 1.0) sb = 1.0;
+    const double kb[4] = {0.0, 0.0, 0.0, 0.5};
+    for (int k = 0; k < n; ++k) {
+        double kh[4] = {1.0, u[k], v[k], 0.5 * (u[k] * u[k] + v[k] * v[k])};
+        double wh = fmax(fabs(ref_h[k]), DBL_EPSILON * sh);
+        double wb = fmax(fabs(ref_b[k]), DBL_EPSILON * sb);
+        for (int a = 0; a < 4; ++a)
+            for (int c = 0; c < 4; ++c)
+                gram[a * 4 + c] = gram[a * 4 + c] + wl[k] * (wh * kh[a] * kh[c] + wb * kb[a] * kb[c]);
+    }
+    if (!uo_solve_dense4(gram, rhs, lam)) return 0;
+    for (int k = 0; k < n; ++k) {
+        double kh[4] = {1.0, u[k], v[k], 0.5 * (u[k] * u[k] + v[k] * v[k])};
+        double wh = fmax(fabs(ref_h[k]), DBL_EPSILON * sh);
+        double wb = fmax(fabs(ref_b[k]), DBL_EPSILON * sb);
+        h[k] = h[k] + wh * (kh[0] * lam[0] + kh[1] * lam[1] + kh[2] * lam[2] + kh[3] * lam[3]);
+        b[k] = b[k] + 0.5 * wb * lam[3];
+    }
+    moment_conserved(n, h, b, u, v, wl, mom);
+    double rs = 1.0;
+    for (int m = 0; m < 4; ++m) if (fabs(target[m]) > rs) rs = fabs(target[m]);
+    double err = 0.0;
+    for (int m = 0; m < 4; ++m) if (fabs(mom[m] - target[m]) > err) err = fabs(mom[m] - target[m]);
+    for (int k = 0; k < n; ++k) if (!isfinite(h[k]) || !isfinite(b[k])) return 0;
+    return err <= 1.0e-10 * rs;
+}
+
+/* MicroSlope (mod_Evolution.f90:1792-1800) */
+static void micro_slope(int ck, const double prim[4], const double sw[4], double a[4]) {
+    double r = prim[0], U = prim[1], V = prim[2], L = prim[3];
+    a[3] = 4.0 * (L * L) / ((double)(ck + 2) * r) *
+           (2.0 * sw[3] - 2.0 * U * sw[1] - 2.0 * V * sw[2] + sw[0] * (U * U + V * V - 0.5 * (double)(ck + 2) / L));
+    a[2] = 2.0 * L / r * (sw[2] - V * sw[0]) - V * a[3];
+    a[1] = 2.0 * L / r * (sw[1] - U * sw[0]) - U * a[3];
+    a[0] = sw[0] / r - U * a[1] - V * a[2] - 0.5 * (U * U + V * V + 0.5 * (double)(ck + 2) / L) * a[3];
+}
+
+#define MNUM 6
+#define MTUM 5
+/* CalcMoment (mod_Evolution.f90:1810-1842) */
+static void calc_moment(int ck, const double prim[4], double Mu[MNUM + 1], double Mv[MTUM + 1], double Mxi[3],
+                        double MuL[MNUM + 1], double MuR[MNUM + 1]) {
+    double U = prim[1], L = prim[3];
+    MuL[0] = 0.5 * erfc(-sqrt(L) * U);
+    MuL[1] = U * MuL[0] + 0.5 * exp(-L * U * U) / sqrt(PI_D * L);
+    MuR[0] = 0.5 * erfc(sqrt(L) * U);
+    MuR[1] = U * MuR[0] - 0.5 * exp(-L * U * U) / sqrt(PI_D * L);
+    for (int i = 2; i <= MNUM; ++i) {
+        MuL[i] = U * MuL[i - 1] + 0.5 * (double)(i - 1) * MuL[i - 2] / L;
+        MuR[i] = U * MuR[i - 1] + 0.5 * (double)(i - 1) * MuR[i - 2] / L;
+    }
+    for (int i = 0; i <= MNUM; ++i) Mu[i] = MuL[i] + MuR[i];
+    Mv[0] = 1.0;
+    Mv[1] = prim[2];
+    for (int i = 2; i <= MTUM; ++i) Mv[i] = prim[2] * Mv[i - 1] + 0.5 * (double)(i - 1) * Mv[i - 2] / L;
+    Mxi[0] = 1.0;
+    Mxi[1] = 0.5 * (double)ck / L;
+    Mxi[2] = (double)ck * ((double)ck + 2.0) / (4.0 * L * L);
+}
+
+/* Moment_uvxi (mod_Evolution.f90:1853-1862) */
+static void moment_uvxi(const double* Mu, const double* Mv, const double* Mxi, int al, int be, int de, double o[4]) {
+    o[0] = Mu[al] * Mv[be] * Mxi[de / 2];
+    o[1] = Mu[al + 1] * Mv[be] * Mxi[de / 2];
+    o[2] = Mu[al] * Mv[be + 1] * Mxi[de / 2];
+    o[3] = 0.5 * (Mu[al + 2] * Mv[be] * Mxi[de / 2] + Mu[al] * Mv[be + 2] * Mxi[de / 2] + Mu[al] * Mv[be] * Mxi[(de + 2) / 2]);
+}
+
+/* Moment_auvxi (mod_Evolution.f90:1874-1885) */
+static void moment_auvxi(const double a[4], const double* Mu, const double* Mv, const double* Mxi, int al, int be,
+                         double o[4]) {
+    double t0[4], t1[4], t2[4], t3[4], t4[4], t5[4];
+    moment_uvxi(Mu, Mv, Mxi, al + 0, be + 0, 0, t0);
+    moment_uvxi(Mu, Mv, Mxi, al + 1, be + 0, 0, t1);
+    moment_uvxi(Mu, Mv, Mxi, al + 0, be + 1, 0, t2);
+    moment_uvxi(Mu, Mv, Mxi, al + 2, be + 0, 0, t3);
+    moment_uvxi(Mu, Mv, Mxi, al + 0, be + 2, 0, t4);
+    moment_uvxi(Mu, Mv, Mxi, al + 0, be + 0, 2, t5);
+    for (int m = 0; m < 4; ++m)
+        o[m] = a[0] * t0[m] + a[1] * t1[m] + a[2] * t2[m] + 0.5 * a[3] * t3[m] + 0.5 * a[3] * t4[m] + 0.5 * a[3] * t5[m];
+}
+
+/* Mt(1..5) time-integration coefficients (mod_Evolution.f90:346-350) */
+static void time_coeffs(double dt, double tau, double Mt[5]) {
+    Mt[3] = tau * (1.0 - exp(-dt / tau));
+    Mt[4] = -tau * dt * exp(-dt / tau) + tau * Mt[3];
+    Mt[0] = dt - Mt[3];
+    Mt[1] = -tau * Mt[0] + Mt[4];
+    Mt[2] = 0.5 * (dt * dt) - tau * Mt[0];
+}
+
+/* PrepareNativeFaceEquilibrium (mod_Evolution.f90:16-30) */
+static int face_equilibrium(const uo_params* p, int n, const double* vn, const double* vt, const double* wv,
+                            const double prim[4], double* H, double* B, double* rh, double* rb) {
+    maxwell(p, n, vn, vt, prim, H, B);
+    memcpy(rh, H, sizeof(double) * n);
+    memcpy(rb, B, sizeof(double) * n);
+    double target[4];
+    get_conserved(p, prim, target);
+    return uo_project_moments(n, H, B, target, vn, vt, wv, rh, rb) ? 0 : 446;
+}
+
+/* ------------------------------------------------------------------ context */
+
+uo_ctx* uo_create(const uo_params* p, const double* u, const double* v, const double* w) {
+    uo_ctx* c = (uo_ctx*)calloc(1, sizeof(uo_ctx));
+    c->p = *p;
+    int nv = p->nvel, nx = p->nx, ny = p->ny;
+    c->nc = nx * ny;
+    c->area = fabs((-p->dx) * (-p->dy) - (p->dx) * (-p->dy)) * 0.5;  /* rectangle area, mod_InitializeFlow.f90:388-389 */
+    c->u = (double*)malloc(sizeof(double) * nv);
+    c->v = (double*)malloc(sizeof(double) * nv);
+    c->w = (double*)malloc(sizeof(double) * nv);
+    memcpy(c->u, u, sizeof(double) * nv);
+    memcpy(c->v, v, sizeof(double) * nv);
+    memcpy(c->w, w, sizeof(double) * nv);
+    c->umax = -INFINITY; c->vmax = -INFINITY;
+    for (int k = 0; k < nv; ++k) { if (u[k] > c->umax) c->umax = u[k]; if (v[k] > c->vmax) c->vmax = v[k]; }
+    size_t S = (size_t)c->nc * nv;
+    c->h = (double*)calloc(S, sizeof(double));
+    c->b = (double*)calloc(S, sizeof(double));
+    c->W = (double*)calloc((size_t)c->nc * 4, sizeof(double));
+    c->sh = (double*)calloc(2 * S, sizeof(double));
+    c->sb = (double*)calloc(2 * S, sizeof(double));
+    c->fxh = (double*)calloc(S, sizeof(double));
+    c->fxb = (double*)calloc(S, sizeof(double));
+    c->fxw = (double*)calloc((size_t)c->nc * 4, sizeof(double));
+    size_t SY = (size_t)(ny + 1) * nx * nv;
+    c->fyLh = (double*)calloc(SY, sizeof(double));
+    c->fyLb = (double*)calloc(SY, sizeof(double));
+    c->fyRh = (double*)calloc(SY, sizeof(double));
+    c->fyRb = (double*)calloc(SY, sizeof(double));
+    c->fyLw = (double*)calloc((size_t)(ny + 1) * nx * 4, sizeof(double));
+    c->fyRw = (double*)calloc((size_t)(ny + 1) * nx * 4, sizeof(double));
+    c->res_w = (double*)calloc((size_t)c->nc * 4, sizeof(double));
+    c->res_h = (double*)calloc(S, sizeof(double));
+    c->res_b = (double*)calloc(S, sizeof(double));
+    c->rate_w = (double*)calloc((size_t)c->nc * 4, sizeof(double));
+    c->stream_h = (double*)calloc(S, sizeof(double));
+    c->stream_b = (double*)calloc(S, sizeof(double));
+    c->peq_h = (double*)calloc(S, sizeof(double));
+    c->peq_b = (double*)calloc(S, sizeof(double));
+    c->pcol_h = (double*)calloc(S, sizeof(double));
+    c->pcol_b = (double*)calloc(S, sizeof(double));
+    c->wall_aero = (double*)calloc((size_t)2 * nx * 3, sizeof(double));
+    for (int i = 0; i < 24; ++i) c->t[i] = (double*)calloc(nv, sizeof(double));
+    return c;
+}
+
+void uo_destroy(uo_ctx* c) {
+    if (!c) return;
+    double* ptrs[] = {c->u, c->v, c->w, c->h, c->b, c->W, c->sh, c->sb, c->fxh, c->fxb, c->fxw, c->fyLh, c->fyLb,
+                      c->fyRh, c->fyRb, c->fyLw, c->fyRw, c->res_w, c->res_h, c->res_b, c->rate_w, c->stream_h,
+                      c->stream_b, c->peq_h, c->peq_b, c->pcol_h, c->pcol_b, c->wall_aero};
+    for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
+    for (int i = 0; i < 24; ++i) free(c->t[i]);
+    free(c);
+}
+
+void uo_set_state(uo_ctx* c, const double* h, const double* b, const double* W) {
+    size_t S = (size_t)c->nc * c->p.nvel;
+    memcpy(c->h, h, S * sizeof(double));
+    memcpy(c->b, b, S * sizeof(double));
+    memcpy(c->W, W, (size_t)c->nc * 4 * sizeof(double));
+}
+
+void uo_get_state(const uo_ctx* c, double* h, double* b, double* W) {
+    size_t S = (size_t)c->nc * c->p.nvel;
+    if (h) memcpy(h, c->h, S * sizeof(double));
+    if (b) memcpy(b, c->b, S * sizeof(double));
+    if (W) memcpy(W, c->W, (size_t)c->nc * 4 * sizeof(double));
+}
+
+const double* uo_res_macro(const uo_ctx* c) { return c->res_w; }
+const double* uo_res_h(const uo_ctx* c) { return c->res_h; }
+const double* uo_res_b(const uo_ctx* c) { return c->res_b; }
+const double* uo_wall_aero(const uo_ctx* c) { return c->wall_aero; }
+const double* uo_face_x_h(const uo_ctx* c) { return c->fxh; }
+const double* uo_face_y_h(const uo_ctx* c) { return c->fyLh; }
+const double* uo_face_x_w(const uo_ctx* c) { return c->fxw; }
+const double* uo_face_y_w(const uo_ctx* c) { return c->fyLw; }
+const double* uo_phys_eq_h(const uo_ctx* c) { return c->peq_h; }
+const double* uo_phys_col_h(const uo_ctx* c) { return c->pcol_h; }
+const double* uo_phys_col_b(const uo_ctx* c) { return c->pcol_b; }
+
+/* InitFlow_Freestream (mod_InitializeFlow.f90:826-856) followed by the cold-start
+ * EnforceAcceptedMomentCompatibility of InitializeSteadyImplicit (mod_SteadyImplicit.f90:28-42,
+ * mod_ImplicitMicro.f90 EnforceAcceptedMomentCompatibility). */
+int uo_init_freestream(uo_ctx* c, double rho, double U, double V, double tnative) {
+    const uo_params* p = &c->p;
+    int nv = p->nvel;
+    double prim[4] = {rho, U, V, 1.0 / tnative}, W[4];
+    get_conserved(p, prim, W);
+    double *H = c->t[0], *B = c->t[1], *rh = c->t[2], *rb = c->t[3];
+    maxwell(p, nv, c->u, c->v, prim, H, B);
+    for (int cell = 0; cell < c->nc; ++cell) {
+        memcpy(c->h + (size_t)cell * nv, H, sizeof(double) * nv);
+        memcpy(c->b + (size_t)cell * nv, B, sizeof(double) * nv);
+        memcpy(c->W + cell * 4, W, sizeof(double) * 4);
+    }
+    for (int cell = 0; cell < c->nc; ++cell) {
+        double* hc = c->h + (size_t)cell * nv;
+        double* bc = c->b + (size_t)cell * nv;
+        memcpy(rh, hc, sizeof(double) * nv);
+        memcpy(rb, bc, sizeof(double) * nv);
+        if (!uo_project_moments(nv, hc, bc, c->W + cell * 4, c->u, c->v, c->w, rh, rb)) return 447;
+    }
+    return 0;
+}
+
+/* TimeStep (mod_Solve.f90:373-421), Time_global_varying */
+double uo_timestep(uo_ctx* c) {
+    const uo_params* p = &c->p;
+    double tmin = INFINITY;
+    for (int cell = 0; cell < c->nc; ++cell) {
+        double prim[4];
+        if (get_primary(p, c->W + cell * 4, prim)) return NAN;
+        double sos = sqrt(0.5 * p->gamma / prim[3]);
+        double a = fmax(c->umax, fabs(prim[1]) + sos);
+        double bq = fmax(c->vmax, fabs(prim[2]) + sos);
+        double dtl = p->cfl * c->area / (p->dy * a + p->dx * bq);
+        if (dtl < tmin) tmin = dtl;
+    }
+    return tmin;
+}
+
+/* ------------------------------------------------------------------ Interpolation */
+
+/* Interp_VanLeer limiter (mod_Interpolation.f90:142-170) */
+static inline double vanleer(double sL, double sR) {
+    return (copysign(1.0, sR) + copysign(1.0, sL)) * fabs(sR) * fabs(sL) / (fabs(sR) + fabs(sL) + SMV);
+}
+
+/* Interpolation (mod_Interpolation.f90:26-90) on one domain: x-periodic Van Leer for every cell;
+ * y Van Leer for rows 2..ny-1 and the one-sided InterpBoundary slope on the wall rows
+ * (UnifiedPhysicalOperators skips the wall rows in the inner loop, :40-45,78-88). */
+void uo_interpolation(uo_ctx* c) {
+    const uo_params* p = &c->p;
+    int nx = p->nx, ny = p->ny, nv = p->nvel;
+    double dL = 0.5 * (p->dx + p->dx), dR = 0.5 * (p->dx + p->dx);
+    double eL = 0.5 * (p->dy + p->dy);
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            int cc = j * nx + i, cl = j * nx + (i + nx - 1) % nx, cr = j * nx + (i + 1) % nx;
+            double *sh = c->sh + ((size_t)cc * 2 + 0) * nv, *sb = c->sb + ((size_t)cc * 2 + 0) * nv;
+            const double *h0 = c->h + (size_t)cc * nv, *hl = c->h + (size_t)cl * nv, *hr = c->h + (size_t)cr * nv;
+            const double *b0 = c->b + (size_t)cc * nv, *bl = c->b + (size_t)cl * nv, *br = c->b + (size_t)cr * nv;
+            for (int k = 0; k < nv; ++k) {
+                sh[k] = vanleer((h0[k] - hl[k]) / dL, (hr[k] - h0[k]) / dR);
+                sb[k] = vanleer((b0[k] - bl[k]) / dL, (br[k] - b0[k]) / dR);
+            }
+        }
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            int cc = j * nx + i;
+            double *sh = c->sh + ((size_t)cc * 2 + 1) * nv, *sb = c->sb + ((size_t)cc * 2 + 1) * nv;
+            if (j == 0 || j == ny - 1) {
+                int lo = (j == 0) ? cc : (j - 1) * nx + i;
+                int hi = (j == 0) ? (j + 1) * nx + i : cc;
+                const double *hl = c->h + (size_t)lo * nv, *hr = c->h + (size_t)hi * nv;
+                const double *bl = c->b + (size_t)lo * nv, *br = c->b + (size_t)hi * nv;
+                for (int k = 0; k < nv; ++k) {
+                    sh[k] = (hr[k] - hl[k]) / eL;
+                    sb[k] = (br[k] - bl[k]) / eL;
+                }
+            } else {
+                int cl = (j - 1) * nx + i, cr = (j + 1) * nx + i;
+                const double *h0 = c->h + (size_t)cc * nv, *hl = c->h + (size_t)cl * nv, *hr = c->h + (size_t)cr * nv;
+                const double *b0 = c->b + (size_t)cc * nv, *bl = c->b + (size_t)cl * nv, *br = c->b + (size_t)cr * nv;
+                for (int k = 0; k < nv; ++k) {
+                    sh[k] = vanleer((h0[k] - hl[k]) / eL, (hr[k] - h0[k]) / eL);
+                    sb[k] = vanleer((b0[k] - bl[k]) / eL, (br[k] - b0[k]) / eL);
+                }
+            }
+        }
+}
+
+/* ------------------------------------------------------------------ Evolution */
+
+/* LocalFrame / GlobalFrame (mod_Tools.f90:150-183) */
+static void local_frame(const double w[4], double cx, double cy, double o[4]) {
+    o[0] = w[0]; o[1] = w[1] * cx + w[2] * cy; o[2] = -w[1] * cy + w[2] * cx; o[3] = w[3];
+}
+static void global_frame(const double w[4], double cx, double cy, double o[4]) {
+    o[0] = w[0]; o[1] = w[1] * cx - w[2] * cy; o[2] = w[1] * cy + w[2] * cx; o[3] = w[3];
+}
+
+/* CalcFlux_MultiDimension (mod_Evolution.f90:186-492) for an interior face.
+ * dir 0: vertical face (normal x, cosx=1, cosy=-0); dir 1: horizontal face (cosx=-0, cosy=1).
+ * Output: micro flux Fh,Fb (already times face length) and macro flux Fw (MomentConserved of it). */
+static int interior_face(uo_ctx* c, int dir, int cl, int cr, double dt, double* Fh, double* Fb, double Fw[4]) {
+    const uo_params* p = &c->p;
+    int nv = p->nvel;
+    double cx = dir == 0 ? 1.0 : -0.0, cy = dir == 0 ? -0.0 : 1.0;
+    double flen = dir == 0 ? p->dy : p->dx;
+    double len = dir == 0 ? p->dx : p->dy;   /* leftCell%length(idx) == rightCell%length(idx) */
+    double *vn = c->t[0], *vt = c->t[1], *dl = c->t[2], *hv = c->t[3], *bv = c->t[4], *shn = c->t[5], *sbn = c->t[6];
+    double *sht = c->t[7], *sbt = c->t[8], *H0 = c->t[9], *B0 = c->t[10], *Hp = c->t[11], *Bp = c->t[12];
+    double *rh = c->t[13], *rb = c->t[14];
+    const double *hL = c->h + (size_t)cl * nv, *hR = c->h + (size_t)cr * nv;
+    const double *bL = c->b + (size_t)cl * nv, *bR = c->b + (size_t)cr * nv;
+    const double *shL = c->sh + (size_t)cl * 2 * nv, *shR = c->sh + (size_t)cr * 2 * nv;
+    const double *sbL = c->sb + (size_t)cl * 2 * nv, *sbR = c->sb + (size_t)cr * 2 * nv;
+    int nd = dir, td = 1 - dir;
+    for (int k = 0; k < nv; ++k) {
+        vn[k] = c->u[k] * cx + c->v[k] * cy;
+        vt[k] = -c->u[k] * cy + c->v[k] * cx;
+        dl[k] = (copysign(1.0, vn[k]) + 1.0) / 2.0;
+    }
+    for (int k = 0; k < nv; ++k) {
+        double dL = dl[k], dR = 1.0 - dL;
+        hv[k] = (hL[k] + 0.5 * len * shL[nd * nv + k]) * dL + (hR[k] - 0.5 * len * shR[nd * nv + k]) * dR;
+        bv[k] = (bL[k] + 0.5 * len * sbL[nd * nv + k]) * dL + (bR[k] - 0.5 * len * sbR[nd * nv + k]) * dR;
+        shn[k] = shL[nd * nv + k] * dL + shR[nd * nv + k] * dR;
+        sbn[k] = sbL[nd * nv + k] * dL + sbR[nd * nv + k] * dR;
+        if (dir == 0) {
+            sht[k] = shL[td * nv + k] * dL + shR[td * nv + k] * dR;
+            sbt[k] = sbL[td * nv + k] * dL + sbR[td * nv + k] * dR;
+        } else {
+            sht[k] = -(shL[td * nv + k] * dL + shR[td * nv + k] * dR);
+            sbt[k] = -(sbL[td * nv + k] * dL + sbR[td * nv + k] * dR);
+        }
+    }
+    double cv[4] = {0, 0, 0, 0};
+    for (int k = 0; k < nv; ++k) {
+        double wk = c->w[k], a = vn[k], t = vt[k], v2 = a * a + t * t;
+        cv[0] = cv[0] + wk * hv[k];
+        cv[1] = cv[1] + wk * a * hv[k];
+        cv[2] = cv[2] + wk * t * hv[k];
+        cv[3] = cv[3] + 0.5 * wk * (v2 * hv[k] + bv[k]);
+    }
+    double prim[4];
+    int e = get_primary(p, cv, prim);
+    if (e) return e;
+    double wl[4], wr[4], sw[4], aL[4], aR[4], bs[4], aT[4];
+    local_frame(c->W + cl * 4, cx, cy, wl);
+    local_frame(c->W + cr * 4, cx, cy, wr);
+    for (int m = 0; m < 4; ++m) sw[m] = (cv[m] - wl[m]) / (0.5 * len);
+    micro_slope(p->ck, prim, sw, aL);
+    for (int m = 0; m < 4; ++m) sw[m] = (wr[m] - cv[m]) / (0.5 * len);
+    micro_slope(p->ck, prim, sw, aR);
+    double swt[4] = {0, 0, 0, 0};
+    for (int k = 0; k < nv; ++k) {
+        double wk = c->w[k], a = vn[k], t = vt[k], v2 = a * a + t * t;
+        swt[0] = swt[0] + wk * sht[k];
+        swt[1] = swt[1] + wk * a * sht[k];
+        swt[2] = swt[2] + wk * t * sht[k];
+        swt[3] = swt[3] + 0.5 * wk * (v2 * sht[k] + sbt[k]);
+    }
+    micro_slope(p->ck, prim, swt, bs);
+    double Mu[MNUM + 1], MuL[MNUM + 1], MuR[MNUM + 1], Mv[MTUM + 1], Mxi[3];
+    calc_moment(p->ck, prim, Mu, Mv, Mxi, MuL, MuR);
+    double MauL[4], MauR[4], Mbv[4];
+    moment_auvxi(aL, MuL, Mv, Mxi, 1, 0, MauL);
+    moment_auvxi(aR, MuR, Mv, Mxi, 1, 0, MauR);
+    moment_auvxi(bs, Mu, Mv, Mxi, 0, 1, Mbv);
+    for (int m = 0; m < 4; ++m) sw[m] = -prim[0] * (MauL[m] + MauR[m] + Mbv[m]);
+    micro_slope(p->ck, prim, sw, aT);
+    double tau;
+    e = get_tau(p, prim, &tau);
+    if (e) return e;
+    double Mt[5];
+    time_coeffs(dt, tau, Mt);
+    /* the Maxwellian-part macro flux (mod_Evolution.f90:356-404) is overwritten by the
+     * MomentConserved of the micro flux in unified mode (:470-473); only the micro flux matters. */
+    e = face_equilibrium(p, nv, vn, vt, c->w, prim, H0, B0, rh, rb);
+    if (e) return e;
+    double qf[2];
+    heat_flux(nv, hv, bv, vn, vt, c->w, prim, qf);
+    shakhov(p, nv, H0, B0, vn, vt, qf, prim, Hp, Bp);
+    for (int k = 0; k < nv; ++k) {
+        double a = vn[k], t = vt[k], v2 = a * a + t * t;
+        double dL = dl[k], dR = 1.0 - dL;
+        double slh = a * shn[k] + t * sht[k];
+        double slb = a * sbn[k] + t * sbt[k];
+        double H = H0[k], B = B0[k];
+        double h_aL = aL[0] * H + aL[1] * a * H + aL[2] * t * H + 0.5 * aL[3] * (v2 * H + B);
+        double h_aR = aR[0] * H + aR[1] * a * H + aR[2] * t * H + 0.5 * aR[3] * (v2 * H + B);
+        double h_b = bs[0] * H + bs[1] * a * H + bs[2] * t * H + 0.5 * bs[3] * (v2 * H + B);
+        double h_aT = aT[0] * H + aT[1] * a * H + aT[2] * t * H + 0.5 * aT[3] * (v2 * H + B);
+        double b_aL = aL[0] * B + aL[1] * a * B + aL[2] * t * B + 0.5 * aL[3] * (v2 * B + Mxi[2] * H);
+        double b_aR = aR[0] * B + aR[1] * a * B + aR[2] * t * B + 0.5 * aR[3] * (v2 * B + Mxi[2] * H);
+        double b_b = bs[0] * B + bs[1] * a * B + bs[2] * t * B + 0.5 * bs[3] * (v2 * B + Mxi[2] * H);
+        double b_aT = aT[0] * B + aT[1] * a * B + aT[2] * t * B + 0.5 * aT[3] * (v2 * B + Mxi[2] * H);
+        double fh = Mt[0] * a * (H + Hp[k]) + Mt[1] * a * a * (h_aL * dL + h_aR * dR) + Mt[1] * a * t * h_b +
+                    Mt[2] * a * h_aT + Mt[3] * a * hv[k] - Mt[4] * a * slh;
+        double fb = Mt[0] * a * (B + Bp[k]) + Mt[1] * a * a * (b_aL * dL + b_aR * dR) + Mt[1] * a * t * b_b +
+                    Mt[2] * a * b_aT + Mt[3] * a * bv[k] - Mt[4] * a * slb;
+        Fh[k] = flen * fh;
+        Fb[k] = flen * fb;
+    }
+    moment_conserved(nv, Fh, Fb, c->u, c->v, c->w, Fw);
+    return 0;
+}
+
+/* W2BMultiscaleFluxBoundary (mod_Evolution.f90:1888-2449) for the horizontal wall faces.
+ * side = -1 (Lside, bottom wall, face below row 0) or +1 (Rside, top wall). */
+static int wall_face(uo_ctx* c, int side, int cell, int iw, double dt, double* Fh, double* Fb, double Fw[4],
+                     double aero[3]) {
+    const uo_params* p = &c->p;
+    int nv = p->nvel;
+    double cx = -0.0, cy = 1.0, flen = p->dx, len = p->dy;
+    double rot = -(double)side;
+    double *vn = c->t[0], *vt = c->t[1], *dl = c->t[2], *hv = c->t[3], *bv = c->t[4], *shn = c->t[5], *sbn = c->t[6];
+    double *sht = c->t[7], *sbt = c->t[8], *Hg = c->t[9], *Bg = c->t[10], *Hp = c->t[11], *Bp = c->t[12];
+    double *rh = c->t[13], *rb = c->t[14], *Hw = c->t[15], *Bw = c->t[16];
+    const double *h = c->h + (size_t)cell * nv, *b = c->b + (size_t)cell * nv;
+    const double *sh = c->sh + (size_t)cell * 2 * nv, *sb = c->sb + (size_t)cell * 2 * nv;
+    for (int k = 0; k < nv; ++k) {
+        vn[k] = c->u[k] * cx + c->v[k] * cy;
+        vt[k] = -c->u[k] * cy + c->v[k] * cx;
+        dl[k] = (copysign(1.0, vn[k]) * rot + 1.0) / 2.0;
+    }
+    for (int k = 0; k < nv; ++k) {
+        shn[k] = sh[nv + k];
+        sbn[k] = sb[nv + k];
+        sht[k] = -sh[k];
+        sbt[k] = -sb[k];
+    }
+    for (int k = 0; k < nv; ++k) {
+        hv[k] = h[k] - rot * 0.5 * len * shn[k];
+        bv[k] = b[k] - rot * 0.5 * len * sbn[k];
+    }
+    double bc[4] = {1.0, p->wall_ux[iw], 0.0, 1.0 / p->wall_tnative[iw]};
+    double prim_w[4], prim_g[4], prim[4], pc[4];
+    local_frame(bc, cx, cy, prim_w);
+    memcpy(prim_g, prim_w, sizeof prim_g);
+    int e = get_primary(p, c->W + cell * 4, pc);
+    if (e) return e;
+    local_frame(pc, cx, cy, prim);
+    prim_g[0] = prim[0] / prim[3] * prim_w[3];
+    double tau;
+    e = get_tau(p, prim_g, &tau);
+    if (e) return e;
+    double Mt[5];
+    time_coeffs(dt, tau, Mt);
+    e = face_equilibrium(p, nv, vn, vt, c->w, prim_g, Hg, Bg, rh, rb);
+    if (e) return e;
+    double qf[2];
+    heat_flux(nv, hv, bv, vn, vt, c->w, prim_g, qf);
+    shakhov(p, nv, Hg, Bg, vn, vt, qf, prim_g, Hp, Bp);
+    double cg[4], cg1[4], sw[4], a_gn[4], a_gt[4], a_T[4];
+    get_conserved(p, prim_g, cg);
+    local_frame(c->W + cell * 4, cx, cy, cg1);
+    for (int m = 0; m < 4; ++m) sw[m] = (cg[m] - cg1[m]) / ((double)side * 0.5 * len);
+    micro_slope(p->ck, prim_g, sw, a_gn);
+    double swt[4] = {0, 0, 0, 0};
+    for (int k = 0; k < nv; ++k) {
+        double wk = c->w[k], a = vn[k], t = vt[k], v2 = a * a + t * t;
+        swt[0] = swt[0] + wk * sht[k];
+        swt[1] = swt[1] + wk * a * sht[k];
+        swt[2] = swt[2] + wk * t * sht[k];
+        swt[3] = swt[3] + 0.5 * wk * (v2 * sht[k] + sbt[k]);
+    }
+    micro_slope(p->ck, prim_g, swt, a_gt);
+    double Mu[MNUM + 1], MuL[MNUM + 1], MuR[MNUM + 1], Mv[MTUM + 1], Mxi[3], Mau[4], Mbv[4];
+    calc_moment(p->ck, prim_g, Mu, Mv, Mxi, MuL, MuR);
+    moment_auvxi(a_gn, Mu, Mv, Mxi, 1, 0, Mau);
+    moment_auvxi(a_gt, Mu, Mv, Mxi, 0, 1, Mbv);
+    for (int m = 0; m < 4; ++m) sw[m] = -prim_g[0] * (Mau[m] + Mbv[m]);
+    micro_slope(p->ck, prim_g, sw, a_T);
+    double pshape[4] = {1.0, prim_w[1], prim_w[2], prim_w[3]};
+    e = face_equilibrium(p, nv, vn, vt, c->w, pshape, Hw, Bw, rh, rb);
+    if (e) return e;
+    double inc = 0.0, refl = 0.0;
+    for (int k = 0; k < nv; ++k) {
+        double wk = c->w[k], a = vn[k], t = vt[k];
+        double dk = dl[k], ik = 1.0 - dk;
+        double slh = a * shn[k] + t * sht[k];
+        double Ha_gn = (a_gn[0] + a_gn[1] * a + a_gn[2] * t) * Hg[k] + 0.5 * a_gn[3] * ((a * a + t * t) * Hg[k] + Bg[k]);
+        double Ha_gt = (a_gt[0] + a_gt[1] * a + a_gt[2] * t) * Hg[k] + 0.5 * a_gt[3] * ((a * a + t * t) * Hg[k] + Bg[k]);
+        double Ha_T = (a_T[0] + a_T[1] * a + a_T[2] * t) * Hg[k] + 0.5 * a_T[3] * ((a * a + t * t) * Hg[k] + Bg[k]);
+        inc = inc + wk * a * ik * (Mt[0] * (Hg[k] + Hp[k]) + Mt[1] * (a * Ha_gn + t * Ha_gt) + Mt[2] * Ha_T +
+                                   Mt[3] * hv[k] - Mt[4] * slh);
+        refl = refl + wk * a * Hw[k] * dk;
+    }
+    refl = dt * refl;
+    prim_w[0] = -inc / refl;
+    for (int k = 0; k < nv; ++k) { Hw[k] = prim_w[0] * Hw[k]; Bw[k] = prim_w[0] * Bw[k]; }
+    for (int k = 0; k < nv; ++k) {
+        double a = vn[k], t = vt[k], v2 = a * a + t * t;
+        double dk = dl[k], ik = 1.0 - dk;
+        double Hgk = Hg[k], Bgk = Bg[k];
+        double Ha_gn = (a_gn[0] + a_gn[1] * a + a_gn[2] * t) * Hgk + 0.5 * a_gn[3] * (v2 * Hgk + Bgk);
+        double Ha_gt = (a_gt[0] + a_gt[1] * a + a_gt[2] * t) * Hgk + 0.5 * a_gt[3] * (v2 * Hgk + Bgk);
+        double Ha_T = (a_T[0] + a_T[1] * a + a_T[2] * t) * Hgk + 0.5 * a_T[3] * (v2 * Hgk + Bgk);
+        double Ba_gn = (a_gn[0] + a_gn[1] * a + a_gn[2] * t) * Bgk + 0.5 * a_gn[3] * (v2 * Bgk + Mxi[2] * Hgk);
+        double Ba_gt = (a_gt[0] + a_gt[1] * a + a_gt[2] * t) * Bgk + 0.5 * a_gt[3] * (v2 * Bgk + Mxi[2] * Hgk);
+        double Ba_T = (a_T[0] + a_T[1] * a + a_T[2] * t) * Bgk + 0.5 * a_T[3] * (v2 * Bgk + Mxi[2] * Hgk);
+        Fh[k] = flen * (dt * a * Hw[k] * dk + Mt[0] * a * (Hgk + Hp[k]) * ik + Mt[1] * a * a * Ha_gn * ik +
+                        Mt[1] * a * t * Ha_gt * ik + Mt[2] * a * Ha_T * ik + Mt[3] * a * hv[k] * ik -
+                        Mt[4] * a * (a * shn[k] + t * sht[k]) * ik);
+        Fb[k] = flen * (dt * a * Bw[k] * dk + Mt[0] * a * (Bgk + Bp[k]) * ik + Mt[1] * a * a * Ba_gn * ik +
+                        Mt[1] * a * t * Ba_gt * ik + Mt[2] * a * Ba_T * ik + Mt[3] * a * bv[k] * ik -
+                        Mt[4] * a * (a * sbn[k] + t * sbt[k]) * ik);
+    }
+    double fl[4] = {0, 0, 0, 0};
+    for (int k = 0; k < nv; ++k) {
+        double hk = Fh[k] / flen, bk = Fb[k] / flen;
+        fl[0] = fl[0] + c->w[k] * hk;
+        fl[1] = fl[1] + c->w[k] * (vn[k] * hk);
+        fl[2] = fl[2] + c->w[k] * (vt[k] * hk);
+        fl[3] = fl[3] + c->w[k] * (0.5 * ((vn[k] * vn[k] + vt[k] * vt[k]) * hk + bk));
+    }
+    aero[0] = fl[1] / dt;
+    aero[1] = fl[2] / dt;
+    aero[2] = fl[3] / dt - prim_w[2] * fl[2] / dt;
+    double g[4];
+    global_frame(fl, cx, cy, g);
+    for (int m = 0; m < 4; ++m) Fw[m] = flen * g[m];
+    return 0;
+}
+
+/* EvolutionNative (mod_Evolution.f90:46-177) for x-periodic + two walls. */
+int uo_evolution(uo_ctx* c, double dt) {
+    const uo_params* p = &c->p;
+    int nx = p->nx, ny = p->ny, nv = p->nvel;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            int cl = j * nx + (i + nx - 1) % nx, cr = j * nx + i;
+            size_t f = (size_t)j * nx + i;
+            int e = interior_face(c, 0, cl, cr, dt, c->fxh + f * nv, c->fxb + f * nv, c->fxw + f * 4);
+            if (e) return e;
+        }
+    for (int jf = 1; jf < ny; ++jf)
+        for (int i = 0; i < nx; ++i) {
+            int cl = (jf - 1) * nx + i, cr = jf * nx + i;
+            size_t f = (size_t)jf * nx + i;
+            int e = interior_face(c, 1, cl, cr, dt, c->fyLh + f * nv, c->fyLb + f * nv, c->fyLw + f * 4);
+            if (e) return e;
+            memcpy(c->fyRh + f * nv, c->fyLh + f * nv, sizeof(double) * nv);
+            memcpy(c->fyRb + f * nv, c->fyLb + f * nv, sizeof(double) * nv);
+            memcpy(c->fyRw + f * 4, c->fyLw + f * 4, sizeof(double) * 4);
+        }
+    for (int i = 0; i < nx; ++i) {
+        size_t f = (size_t)i;
+        int e = wall_face(c, -1, i, 0, dt, c->fyLh + f * nv, c->fyLb + f * nv, c->fyLw + f * 4, c->wall_aero + i * 3);
+        if (e) return e;
+        f = (size_t)ny * nx + i;
+        e = wall_face(c, +1, (ny - 1) * nx + i, 1, dt, c->fyRh + f * nv, c->fyRb + f * nv, c->fyRw + f * 4,
+                      c->wall_aero + (nx + i) * 3);
+        if (e) return e;
+    }
+    return 0;
+}
+
+/* ------------------------------------------------------------------ residual + update */
+
+/* ComputeResidual (mod_Residual.f90:17-132) for the unified low-order path:
+ * AssembleMacroResidual, AssembleMicroFluxResidual, AssembleSteadyRateResiduals with the
+ * EnforceStreamingMomentCompatibility projection (mod_ImplicitMicro.f90:293-306) and, when
+ * with_collision, the physical equilibrium/collision used by the implicit paths. */
+int uo_compute_residual(uo_ctx* c, double dt, int with_collision) {
+    const uo_params* p = &c->p;
+    int nx = p->nx, ny = p->ny, nv = p->nvel;
+    double area_inv = 1.0 / c->area;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            int cc = j * nx + i;
+            const double *vl = c->fxw + ((size_t)j * nx + i) * 4, *vr = c->fxw + ((size_t)j * nx + (i + 1) % nx) * 4;
+            const double *hl = c->fyLw + ((size_t)j * nx + i) * 4, *hr = c->fyRw + ((size_t)(j + 1) * nx + i) * 4;
+            for (int m = 0; m < 4; ++m) c->res_w[cc * 4 + m] = (vl[m] - vr[m] + hl[m] - hr[m]) / c->area;
+            const double *vlh = c->fxh + ((size_t)j * nx + i) * nv, *vrh = c->fxh + ((size_t)j * nx + (i + 1) % nx) * nv;
+            const double *vlb = c->fxb + ((size_t)j * nx + i) * nv, *vrb = c->fxb + ((size_t)j * nx + (i + 1) % nx) * nv;
+            const double *hlh = c->fyLh + ((size_t)j * nx + i) * nv, *hrh = c->fyRh + ((size_t)(j + 1) * nx + i) * nv;
+            const double *hlb = c->fyLb + ((size_t)j * nx + i) * nv, *hrb = c->fyRb + ((size_t)(j + 1) * nx + i) * nv;
+            for (int k = 0; k < nv; ++k) {
+                c->res_h[(size_t)cc * nv + k] = (vlh[k] - vrh[k] + hlh[k] - hrh[k]) * area_inv;
+                c->res_b[(size_t)cc * nv + k] = (vlb[k] - vrb[k] + hlb[k] - hrb[k]) * area_inv;
+            }
+        }
+    double dti = 1.0 / dt;
+    for (int cc = 0; cc < c->nc; ++cc) {
+        for (int m = 0; m < 4; ++m) c->rate_w[cc * 4 + m] = c->res_w[cc * 4 + m] * dti;
+        for (int k = 0; k < nv; ++k) {
+            c->stream_h[(size_t)cc * nv + k] = c->res_h[(size_t)cc * nv + k] * dti;
+            c->stream_b[(size_t)cc * nv + k] = c->res_b[(size_t)cc * nv + k] * dti;
+        }
+    }
+    int ok = 1;
+    for (int cc = 0; cc < c->nc; ++cc)
+        ok &= uo_project_moments(nv, c->stream_h + (size_t)cc * nv, c->stream_b + (size_t)cc * nv, c->rate_w + cc * 4,
+                                 c->u, c->v, c->w, c->h + (size_t)cc * nv, c->b + (size_t)cc * nv);
+    for (int cc = 0; cc < c->nc; ++cc) {
+        for (int k = 0; k < nv; ++k) {
+            c->res_h[(size_t)cc * nv + k] = c->stream_h[(size_t)cc * nv + k] * dt;
+            c->res_b[(size_t)cc * nv + k] = c->stream_b[(size_t)cc * nv + k] * dt;
+        }
+        if (!with_collision) continue;
+        double prim[4], tau, q[2];
+        int e = get_primary(p, c->W + cc * 4, prim);
+        if (e) return e;
+        e = get_tau(p, prim, &tau);
+        if (e) return e;
+        const double *h = c->h + (size_t)cc * nv, *b = c->b + (size_t)cc * nv;
+        double *eh = c->peq_h + (size_t)cc * nv, *eb = c->peq_b + (size_t)cc * nv;
+        heat_flux(nv, h, b, c->u, c->v, c->w, prim, q);
+        maxwell(p, nv, c->u, c->v, prim, eh, eb);
+        shakhov(p, nv, eh, eb, c->u, c->v, q, prim, c->t[0], c->t[1]);
+        for (int k = 0; k < nv; ++k) { eh[k] = eh[k] + c->t[0][k]; eb[k] = eb[k] + c->t[1][k]; }
+        memcpy(c->t[2], eh, sizeof(double) * nv);
+        memcpy(c->t[3], eb, sizeof(double) * nv);
+        ok &= uo_project_moments(nv, eh, eb, c->W + cc * 4, c->u, c->v, c->w, c->t[2], c->t[3]);
+        for (int k = 0; k < nv; ++k) {
+            c->pcol_h[(size_t)cc * nv + k] = (eh[k] - h[k]) / tau;
+            c->pcol_b[(size_t)cc * nv + k] = (eb[k] - b[k]) / tau;
+        }
+    }
+    return ok ? 0 : 444;
+}
+
+/* ApplyExplicitUpdate + ApplyMicroExplicitUpdate + residual norms
+ * (mod_TimeIntegrator.f90:16-134,163-191,235-293). */
+int uo_apply_explicit_update(uo_ctx* c, double dt, double* res_out) {
+    const uo_params* p = &c->p;
+    int nv = p->nvel;
+    double sumRes[4] = {0, 0, 0, 0}, sumAvg[4] = {0, 0, 0, 0}, areaSq = 0.0, maxCell[4] = {0, 0, 0, 0};
+    double *Ho = c->t[17], *Bo = c->t[18], *Hn = c->t[19], *Bn = c->t[20], *Hp = c->t[21], *Bp = c->t[22];
+    double *rh = c->t[13], *rb = c->t[14];
+    for (int cc = 0; cc < c->nc; ++cc) {
+        double Wold[4], po[4], pn[4], to, tn;
+        memcpy(Wold, c->W + cc * 4, sizeof Wold);
+        int e = get_primary(p, Wold, po);
+        if (e) return e;
+        maxwell(p, nv, c->u, c->v, po, Ho, Bo);
+        if ((e = get_tau(p, po, &to))) return e;
+        for (int m = 0; m < 4; ++m) c->W[cc * 4 + m] = c->W[cc * 4 + m] + c->res_w[cc * 4 + m];
+        for (int m = 0; m < 4; ++m) if (!isfinite(c->W[cc * 4 + m])) return 4;
+        if ((e = get_primary(p, c->W + cc * 4, pn))) return e;
+        maxwell(p, nv, c->u, c->v, pn, Hn, Bn);
+        if ((e = get_tau(p, pn, &tn))) return e;
+        for (int m = 0; m < 4; ++m) {
+            double d = (Wold[m] - c->W[cc * 4 + m]) * c->area / dt;
+            double rc = fabs(d);
+            if (rc > maxCell[m]) maxCell[m] = rc;
+            sumRes[m] = sumRes[m] + d * d;
+        }
+        for (int m = 0; m < 4; ++m) sumAvg[m] = sumAvg[m] + fabs(c->W[cc * 4 + m]) * c->area;
+        areaSq = areaSq + c->area * c->area;
+        double* h = c->h + (size_t)cc * nv;
+        double* b = c->b + (size_t)cc * nv;
+        double qf[2];
+        heat_flux(nv, h, b, c->u, c->v, c->w, po, qf);
+        shakhov(p, nv, Ho, Bo, c->u, c->v, qf, po, Hp, Bp);
+        for (int k = 0; k < nv; ++k) { Ho[k] = Ho[k] + Hp[k]; Bo[k] = Bo[k] + Bp[k]; }
+        shakhov(p, nv, Hn, Bn, c->u, c->v, qf, pn, Hp, Bp);
+        for (int k = 0; k < nv; ++k) { Hn[k] = Hn[k] + Hp[k]; Bn[k] = Bn[k] + Bp[k]; }
+        double tg[4];
+        get_conserved(p, po, tg);
+        memcpy(rh, Ho, sizeof(double) * nv); memcpy(rb, Bo, sizeof(double) * nv);
+        if (!uo_project_moments(nv, Ho, Bo, tg, c->u, c->v, c->w, rh, rb)) return 444;
+        memcpy(rh, Hn, sizeof(double) * nv); memcpy(rb, Bn, sizeof(double) * nv);
+        if (!uo_project_moments(nv, Hn, Bn, c->W + cc * 4, c->u, c->v, c->w, rh, rb)) return 444;
+        double inv = 1.0 / (1.0 + 0.5 * dt / tn);
+        const double *fh = c->res_h + (size_t)cc * nv, *fb = c->res_b + (size_t)cc * nv;
+        for (int k = 0; k < nv; ++k) {
+            double ho = h[k], bo = b[k];
+            h[k] = (ho + fh[k] + 0.5 * dt * (Hn[k] / tn + (Ho[k] - ho) / to)) * inv;
+            b[k] = (bo + fb[k] + 0.5 * dt * (Bn[k] / tn + (Bo[k] - bo) / to)) * inv;
+        }
+    }
+    /* residual norms (mod_TimeIntegrator.f90:102-127) */
+    double ncell = (double)(p->nx * p->ny);
+    double num[4], den[4], rel[4], absr[4], res[4];
+    for (int m = 0; m < 4; ++m) {
+        num[m] = sqrt(ncell * sumRes[m]);
+        den[m] = sumAvg[m] + SMV;
+        rel[m] = num[m] / den[m];
+        absr[m] = sqrt(sumRes[m] / fmax(areaSq, SMV));
+    }
+    double ords = fmax(fmax(sumAvg[0], sumAvg[3]), SMV);
+    for (int m = 0; m < 4; ++m) {
+        int near0 = sumAvg[m] <= sqrt(DBL_EPSILON) * fmax(ords, DBL_MIN);
+        res[m] = near0 ? absr[m] : rel[m];
+        if (!isfinite(res[m])) return 8;
+    }
+    if (res_out) memcpy(res_out, res, sizeof res);
+    return 0;
+}
+
+int uo_explicit_step(uo_ctx* c, double* dt_out, double* res_out) {
+    double dt = uo_timestep(c);
+    if (!isfinite(dt)) return 101;
+    if (dt_out) *dt_out = dt;
+    uo_interpolation(c);
+    int e = uo_evolution(c, dt);
+    if (e) return e;
+    e = uo_compute_residual(c, dt, 0);
+    if (e) return e;
+    return uo_apply_explicit_update(c, dt, res_out);
+}

@@ -1,0 +1,91 @@
+/*
+ * ugks_oracle.h -- TEST INFRASTRUCTURE ONLY.
+ *
+ * A plain-C, single-threaded CPU restatement of the reference UGKS2D Fortran hot path
+ * (Sherlmess/UGKS2D_high_order, Fortran sources under src/), used solely as the parity checker for the CUDA
+ * library and as the timed CPU baseline in bench.py.  Nothing in the product library links,
+ * calls or falls back to this code.  Each function cites the Fortran routine it restates.
+ *
+ * Parity of this restatement is pinned against the reference's own printed outputs
+ * (tests/golden/reference_golden.json, generated by tests/golden/make_fixtures.py):
+ *   - the 2-step low_explicit `dtPhysical` and `res:` line,
+ *   - the 2-step low_implicit sparse_residual.csv rows (8-slab emulation),
+ *   - the static-equilibrium residual/update maxima of checks/VERIFICATION.json.
+ *
+ * Layout: single domain, cells c = j*nx + i (0-based, i fastest), velocity k fastest:
+ *   h[c*nvel + k], b[c*nvel + k], W[c*4 + m].  x is periodic; y has diffuse moving walls.
+ */
+#ifndef UGKS_ORACLE_H
+#define UGKS_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct {
+    int nx, ny, nvel;
+    double dx, dy;            /* cell lengths: Fortran ctr%length(1), ctr%length(2) */
+    int ck;                   /* internal degrees of freedom (integer in the reference) */
+    double pr, omega, mu_ref, gamma, cfl;
+    double wall_ux[2];        /* WallUx(3:4): bottom (y=0), top (y=H) */
+    double wall_tnative[2];   /* wall T_native (Tw); lambda_w = 1/Tw */
+    double ncfl;              /* Implicit_nCFL (pseudo-time CFL) */
+    int nslab;                /* number of 1-D slabs in y the reference's MPI blocking used (NP_Y) */
+    int mass_rescale;         /* ClosedCouetteMassRescale */
+    int macro_sweeps;         /* Implicit_MacroSweeps */
+    double residual_tol, moment_tol, min_alpha;
+} uo_params;
+
+typedef struct uo_ctx uo_ctx;
+
+uo_ctx* uo_create(const uo_params* p, const double* u, const double* v, const double* w);
+void    uo_destroy(uo_ctx* c);
+
+/* state access: copy in/out of h, b (ncell*nvel) and W (ncell*4) */
+void uo_set_state(uo_ctx* c, const double* h, const double* b, const double* W);
+void uo_get_state(const uo_ctx* c, double* h, double* b, double* W);
+
+/* InitFlow_Freestream + EnforceAcceptedMomentCompatibility (mod_InitializeFlow.f90:826-856,
+ * mod_ImplicitMicro.f90 EnforceAcceptedMomentCompatibility, via InitializeSteadyImplicit). */
+int uo_init_freestream(uo_ctx* c, double rho, double U, double V, double tnative);
+
+/* TimeStep, Time_global_varying (mod_Solve.f90:373-421).  Returns dt_global. */
+double uo_timestep(uo_ctx* c);
+
+/* One full Explicit step: TimeStep, Interpolation, EvolutionNative, ComputeResidual,
+ * ApplyExplicitUpdate (mod_Solve.f90:84-186).  res_out[4] = the `res` vector; returns 0 or a
+ * reference abort code. */
+int uo_explicit_step(uo_ctx* c, double* dt_out, double* res_out);
+
+/* Pieces of the step, for piecewise parity checks. */
+void uo_interpolation(uo_ctx* c);                 /* mod_Interpolation.f90:26-90 */
+int  uo_evolution(uo_ctx* c, double dt);          /* mod_Evolution.f90:46-177 (Couette subset) */
+int  uo_compute_residual(uo_ctx* c, double dt, int with_collision); /* mod_Residual.f90:17-132 */
+int  uo_apply_explicit_update(uo_ctx* c, double dt, double* res_out); /* mod_TimeIntegrator.f90:16-134 */
+
+/* Read-only views of the work arrays (valid until the next call). */
+const double* uo_res_macro(const uo_ctx* c);     /* res_macro_flux_store  [ncell][4] */
+const double* uo_res_h(const uo_ctx* c);         /* res_h_flux_store      [ncell][nvel] */
+const double* uo_res_b(const uo_ctx* c);
+const double* uo_wall_aero(const uo_ctx* c);     /* [2][nx][3] local-frame pnn, pnt, qn */
+const double* uo_face_x_h(const uo_ctx* c);      /* x-face micro flux [ny][nx][nvel] (face i between i-1,i) */
+const double* uo_face_y_h(const uo_ctx* c);      /* y-face micro flux [ny+1][nx][nvel] */
+const double* uo_face_x_w(const uo_ctx* c);      /* [ny][nx][4] */
+const double* uo_face_y_w(const uo_ctx* c);      /* [ny+1][nx][4] */
+const double* uo_phys_eq_h(const uo_ctx* c);     /* physical_equilibrium_h [ncell][nvel] */
+const double* uo_phys_col_h(const uo_ctx* c);    /* physical_collision_h */
+const double* uo_phys_col_b(const uo_ctx* c);
+
+/* Standalone kinetic-library entry points (mod_Tools.f90, mod_ImplicitCommon.f90). */
+int uo_project_moments(int n, double* h, double* b, const double target[4], const double* u,
+                       const double* v, const double* wl, const double* ref_h, const double* ref_b);
+int uo_solve_dense4(const double m[16], const double rhs[4], double sol[4]);
+
+/* ImplicitSteady pseudo-step (mod_SteadyImplicit.f90:379-462) with the reference's nslab
+ * block-Jacobi seams.  out[] receives the diagnostics listed in ugks_oracle.c. */
+int uo_implicit_step(uo_ctx* c, double* out, int nout);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,15 @@
+"""B200-native (sm_100a, FP64) implementation of the UGKS2D kinetic hot path.
+
+The compute lives in libugks_b200.so (hand-written CUDA, C ABI in include/ugks_b200.h);
+this package holds the host-side mirror of the reference's operator interface.
+"""
+from .case import CouetteCase, reference_case, baseline_explicit_case, load_velocity_half32  # noqa: F401
+
+__all__ = ["CouetteCase", "reference_case", "baseline_explicit_case", "load_velocity_half32", "Solver"]
+
+
+def __getattr__(name):
+    if name == "Solver":
+        from .solver import Solver
+        return Solver
+    raise AttributeError(name)

@@ -1,0 +1,68 @@
+"""Couette case description: the subset of the reference's `&config_para` / `&boundary_para`
+namelists (Config.ini, parsed by mod_ImportPara.f90:141-173) that the kinetic hot path reads.
+
+Derived constants follow set_const_para (mod_ImportPara.f90:911-930):
+gamma = (ck+4)/(ck+2); with CouetteMuRef > 0, mu_ref = CouetteMuRef and Kn = sqrt(pi)*mu_ref.
+"""
+from dataclasses import dataclass, field, replace
+import math
+import os
+
+import numpy as np
+
+_GOLDEN = os.path.join(os.path.dirname(os.path.dirname(os.path.abspath(__file__))), "tests", "golden")
+
+
+@dataclass
+class CouetteCase:
+    nx: int = 8                      # Nx_all
+    ny: int = 64                     # Ny_all
+    dx: float = 0.125                # uniform mesh of Mesh2d.dat: x in [0,1], y in [0,1]
+    dy: float = 1.0 / 64.0
+    ck: int = 1
+    pr: float = 0.66666666666666666667
+    omega: float = 0.5
+    mu_ref: float = 0.05637282460904075   # CouetteMuRef
+    cfl: float = 0.1
+    tinf: float = 2.0                # initial T_native (theta = T/2 = 1)
+    wall_ux: tuple = (-3.872983346207417, 3.872983346207417)   # WallUx(3:4): bottom, top
+    wall_tnative: tuple = (2.0, 2.0)                           # Tw per wall
+    method: str = "Explicit"        # Explicit | ImplicitSteady | HighOrderImplicit | S2CN2
+    ncfl: float = 1000.0             # Implicit_nCFL
+    nslab: int = 8                   # NP_Y of the reference's 1 x NP_Y MPI blocking (block-Jacobi seams)
+    mass_rescale: bool = False       # ClosedCouetteMassRescale
+    macro_sweeps: int = 2            # Implicit_MacroSweeps
+    residual_tol: float = 1.0e-8     # Implicit_ResidualTol
+    moment_tol: float = 1.0e-12      # Implicit_MomentTol
+    min_alpha: float = 1.0e-6        # Implicit_MinAlpha
+    max_iter: int = 3000
+
+    @property
+    def gamma(self):
+        return float(self.ck + 4) / float(self.ck + 2)
+
+    @property
+    def kn(self):
+        return math.sqrt(math.pi) * self.mu_ref
+
+    def with_(self, **kw):
+        return replace(self, **kw)
+
+
+def reference_case(method="Explicit"):
+    """The reference's delivered Ma3 Couette case (cases/low_explicit|low_implicit|high_implicit)."""
+    c = CouetteCase(method=method)
+    if method in ("ImplicitSteady", "HighOrderImplicit"):
+        c.mass_rescale = True
+    return c
+
+
+def baseline_explicit_case():
+    """Throughput variant of the explicit case: CFL 0.5, omega 0.81 (same mesh, walls, Kn)."""
+    return CouetteCase(cfl=0.5, omega=0.81)
+
+
+def load_velocity_half32():
+    """The reference's velocity_half32_scale2.dat table (u, v, w), k = i + (j-1)*Nu."""
+    t = np.load(os.path.join(_GOLDEN, "velocity_half32_scale2.npy"))
+    return t[:, 0].copy(), t[:, 1].copy(), t[:, 2].copy()

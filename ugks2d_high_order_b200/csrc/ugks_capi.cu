@@ -1,0 +1,401 @@
+// ugks_capi.cu -- C ABI (include/ugks_b200.h): context, device buffers, launch sequencing,
+// CUDA-graph replay of the explicit step, status mapping and kernel timing.
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+
+#include "../../include/ugks_b200.h"
+#include "ugks_lo.cuh"
+
+namespace ugks {
+int lo_threads(int nvel);
+cudaError_t launch_lo_faces(const LoParams& P, const LoBuffers& B, cudaStream_t s);
+cudaError_t launch_lo_cells(const LoParams& P, const LoBuffers& B, int mode, bool collision, cudaStream_t s);
+cudaError_t launch_lo_timestep(const LoParams& P, const LoBuffers& B, cudaStream_t s);
+cudaError_t launch_lo_init(const LoParams& P, const LoBuffers& B, double rho, double U, double V, double tn,
+                           cudaStream_t s);
+}  // namespace ugks
+
+using namespace ugks;
+
+struct KernelTimer {
+    double total_ms = 0.0;
+    long long launches = 0;
+};
+
+struct ugks_ctx {
+    ugks_params prm;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    LoParams P{};
+    LoBuffers B{};
+    double* dmem = nullptr;      // one allocation backing every double buffer
+    unsigned* dflags = nullptr;  // [0] counter, [1] status
+    size_t ndoubles = 0;
+    unsigned last_status = 0;
+    long long launches = 0;
+    // explicit-step graph
+    cudaGraphExec_t graph = nullptr;
+    int graph_steps = 0;
+    // profiling
+    bool profile = false;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    KernelTimer t_faces, t_cells;
+};
+
+static int cuda_fail(cudaError_t e) {
+    if (e == cudaSuccess) return UGKS_OK;
+    std::fprintf(stderr, "ugks_b200: CUDA error %s\n", cudaGetErrorString(e));
+    return e == cudaErrorMemoryAllocation ? UGKS_ENOMEM : UGKS_ECUDA;
+}
+
+#define UGKS_CK(x)                                   \
+    do {                                             \
+        cudaError_t _e = (x);                        \
+        if (_e != cudaSuccess) return cuda_fail(_e); \
+    } while (0)
+
+extern "C" const char* ugks_error_string(int code) {
+    switch (code) {
+        case UGKS_OK: return "ok";
+        case UGKS_EINVAL: return "invalid argument";
+        case UGKS_ECUDA: return "CUDA runtime error";
+        case UGKS_ENUMERIC: return "device-side numerical gate failed";
+        case UGKS_ETIMEOUT: return "bounded device wait expired";
+        case UGKS_ENOMEM: return "out of device memory";
+        case UGKS_EUNSUPPORTED: return "unsupported configuration";
+        default: return "unknown";
+    }
+}
+
+extern "C" int ugks_status_reference_code(unsigned st) {
+    if (st & ST_GETPRIMARY) return 101;
+    if (st & ST_TAU) return 104;
+    if (st & ST_FACE_PROJECTION) return 446;
+    if (st & ST_PROJECTION) return 444;
+    if (st & ST_NONFINITE_FLUX) return 13;
+    if (st & ST_NONFINITE_STATE) return 4;
+    if (st & ST_MOMENT_GATE) return 451;
+    if (st & ST_ALPHA) return 433;
+    if (st & ST_TIMEOUT) return 999;
+    return 0;
+}
+
+// Read (and clear) the device status word; synchronises the stream.
+static int collect_status(ugks_ctx* c) {
+    unsigned st = 0;
+    UGKS_CK(cudaMemcpyAsync(&st, c->dflags + 1, sizeof(unsigned), cudaMemcpyDeviceToHost, c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    if (st) UGKS_CK(cudaMemsetAsync(c->dflags + 1, 0, sizeof(unsigned), c->stream));
+    c->last_status = st;
+    if (st & ST_TIMEOUT) return UGKS_ETIMEOUT;
+    return st ? UGKS_ENUMERIC : UGKS_OK;
+}
+
+extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const double* v, const double* w, int device,
+                               ugks_ctx** out) {
+    if (!p || !u || !v || !w || !out) return UGKS_EINVAL;
+    if (p->nx < 1 || p->ny < 3 || p->nvel < 1 || p->nvel > kMaxVel || !(p->dx > 0) || !(p->dy > 0) ||
+        p->ck < 1)
+        return UGKS_EINVAL;
+    if (p->method != UGKS_METHOD_EXPLICIT && p->method != UGKS_METHOD_IMPLICIT_STEADY) return UGKS_EUNSUPPORTED;
+    UGKS_CK(cudaSetDevice(device));
+    ugks_ctx* c = new (std::nothrow) ugks_ctx();
+    if (!c) return UGKS_ENOMEM;
+    c->prm = *p;
+    c->device = device;
+    const int nx = p->nx, ny = p->ny, nv = p->nvel, nc = nx * ny;
+    LoParams& P = c->P;
+    P.nx = nx; P.ny = ny; P.nvel = nv; P.ck = p->ck;
+    P.dx = p->dx; P.dy = p->dy;
+    P.area = std::fabs((-p->dx) * (-p->dy) - (p->dx) * (-p->dy)) * 0.5;
+    P.gm1 = (double)(p->ck + 4) / (double)(p->ck + 2) - 1.0;
+    P.pr = p->pr; P.omega = p->omega; P.mu_ref = p->mu_ref; P.cfl = p->cfl;
+    P.umax = -INFINITY; P.vmax = -INFINITY;
+    for (int k = 0; k < nv; ++k) { P.umax = std::fmax(P.umax, u[k]); P.vmax = std::fmax(P.vmax, v[k]); }
+    for (int s = 0; s < 2; ++s) { P.wall_ux[s] = p->wall_ux[s]; P.wall_lam[s] = 1.0 / p->wall_tnative[s]; }
+    P.fixed_dt = p->fixed_dt;
+
+    // buffer plan (doubles)
+    const size_t S = (size_t)nc * nv, SY = (size_t)(ny + 1) * nx * nv;
+    size_t off = 0;
+    auto take = [&](size_t n) { size_t o = off; off += (n + 31) / 32 * 32; return o; };
+    const size_t o_u = take(nv), o_v = take(nv), o_w = take(nv);
+    const size_t o_h = take(S), o_b = take(S), o_W = take((size_t)nc * 4);
+    const size_t o_fxh = take(S), o_fxb = take(S), o_fxw = take((size_t)nc * 4);
+    const size_t o_fyh = take(SY), o_fyb = take(SY), o_fyw = take((size_t)(ny + 1) * nx * 4);
+    const size_t o_rw = take((size_t)nc * 4), o_rh = take(S), o_rb = take(S);
+    const size_t o_eh = take(S), o_eb = take(S), o_ch = take(S), o_cb = take(S);
+    const size_t o_dtl = take(nc), o_dt = take(2), o_cd = take((size_t)nc * kNDiag), o_dg = take(kNDiag);
+    const size_t o_wa = take((size_t)2 * nx * 3);
+    c->ndoubles = off;
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaMalloc(&c->dmem, off * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&c->dflags, 4 * sizeof(unsigned));
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->dmem, 0, off * sizeof(double), c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(c->dflags, 0, 4 * sizeof(unsigned), c->stream);
+    if (e != cudaSuccess) { ugks_ctx_destroy(c); return cuda_fail(e); }
+    double* d = c->dmem;
+    LoBuffers& B = c->B;
+    B.u = d + o_u; B.v = d + o_v; B.w = d + o_w;
+    B.h = d + o_h; B.b = d + o_b; B.W = d + o_W;
+    B.fxh = d + o_fxh; B.fxb = d + o_fxb; B.fxw = d + o_fxw;
+    B.fyh = d + o_fyh; B.fyb = d + o_fyb; B.fyw = d + o_fyw;
+    B.res_w = d + o_rw; B.res_h = d + o_rh; B.res_b = d + o_rb;
+    B.peq_h = d + o_eh; B.peq_b = d + o_eb; B.pcol_h = d + o_ch; B.pcol_b = d + o_cb;
+    B.dtl = d + o_dtl; B.dt = d + o_dt; B.cell_diag = d + o_cd; B.diag = d + o_dg; B.wall_aero = d + o_wa;
+    B.counter = c->dflags; B.status = c->dflags + 1;
+    e = cudaMemcpyAsync(d + o_u, u, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d + o_v, v, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(d + o_w, w, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
+    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e != cudaSuccess) { ugks_ctx_destroy(c); return cuda_fail(e); }
+    *out = c;
+    return UGKS_OK;
+}
+
+extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
+    if (!c) return UGKS_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    if (c->graph) cudaGraphExecDestroy(c->graph);
+    for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    if (c->dmem) cudaFree(c->dmem);
+    if (c->dflags) cudaFree(c->dflags);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return UGKS_OK;
+}
+
+static int kernel_timestep(ugks_ctx* c) {
+    UGKS_CK(launch_lo_timestep(c->P, c->B, c->stream));
+    c->launches += 1;
+    return UGKS_OK;
+}
+
+extern "C" int ugks_upload_state(ugks_ctx* c, const double* h, const double* b, const double* W) {
+    if (!c || !h || !b || !W) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
+    UGKS_CK(cudaMemcpyAsync(c->B.h, h, S * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    UGKS_CK(cudaMemcpyAsync(c->B.b, b, S * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    UGKS_CK(cudaMemcpyAsync(c->B.W, W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+    int r = kernel_timestep(c);
+    if (r) return r;
+    return collect_status(c);
+}
+
+extern "C" int ugks_download_state(ugks_ctx* c, double* h, double* b, double* W) {
+    if (!c) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
+    if (h) UGKS_CK(cudaMemcpyAsync(h, c->B.h, S * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (b) UGKS_CK(cudaMemcpyAsync(b, c->B.b, S * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (W)
+        UGKS_CK(cudaMemcpyAsync(W, c->B.W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    return UGKS_OK;
+}
+
+extern "C" int ugks_init_freestream(ugks_ctx* c, double rho, double U, double V, double tnative) {
+    if (!c || !(rho > 0) || !(tnative > 0)) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    UGKS_CK(launch_lo_init(c->P, c->B, rho, U, V, tnative, c->stream));
+    c->launches += 1;
+    int r = kernel_timestep(c);
+    if (r) return r;
+    return collect_status(c);
+}
+
+extern "C" int ugks_timestep(ugks_ctx* c, double* dt_out) {
+    if (!c) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    int r = kernel_timestep(c);
+    if (r) return r;
+    if (dt_out) UGKS_CK(cudaMemcpyAsync(dt_out, c->B.dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return collect_status(c);
+}
+
+extern "C" int ugks_evolution(ugks_ctx* c) {
+    if (!c) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    UGKS_CK(launch_lo_faces(c->P, c->B, c->stream));
+    c->launches += 1;
+    return collect_status(c);
+}
+
+extern "C" int ugks_compute_residual(ugks_ctx* c, int with_collision) {
+    if (!c) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    UGKS_CK(launch_lo_cells(c->P, c->B, 1, with_collision != 0, c->stream));
+    c->launches += 1;
+    return collect_status(c);
+}
+
+// residual vector of ApplyExplicitUpdate (mod_TimeIntegrator.f90:108-127) from the reduced sums
+static void finish_res(const ugks_ctx* c, const double* dg, double* res) {
+    const double SMV = 1.1754943508222875e-38;
+    const double ncell = (double)(c->P.nx * c->P.ny);
+    double sumRes[4], sumAvg[4];
+    for (int m = 0; m < 4; ++m) { sumRes[m] = dg[m]; sumAvg[m] = dg[4 + m]; }
+    const double areaSq = dg[8];
+    const double ords = std::fmax(std::fmax(sumAvg[0], sumAvg[3]), SMV);
+    for (int m = 0; m < 4; ++m) {
+        const double rel = std::sqrt(ncell * sumRes[m]) / (sumAvg[m] + SMV);
+        const double ab = std::sqrt(sumRes[m] / std::fmax(areaSq, SMV));
+        const bool near0 = sumAvg[m] <= std::sqrt(2.220446049250313e-16) * std::fmax(ords, 2.2250738585072014e-308);
+        res[m] = near0 ? ab : rel;
+    }
+}
+
+static int read_step_outputs(ugks_ctx* c, double* dt_out, double* res_out) {
+    double dg[kNDiag];
+    if (res_out) UGKS_CK(cudaMemcpyAsync(dg, c->B.diag, sizeof dg, cudaMemcpyDeviceToHost, c->stream));
+    int r = collect_status(c);
+    if (res_out) finish_res(c, dg, res_out);
+    (void)dt_out;
+    return r;
+}
+
+extern "C" int ugks_apply_explicit_update(ugks_ctx* c, double* res_out) {
+    if (!c) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    UGKS_CK(launch_lo_cells(c->P, c->B, 2, false, c->stream));
+    c->launches += 1;
+    return read_step_outputs(c, nullptr, res_out);
+}
+
+static cudaError_t enqueue_explicit_steps(ugks_ctx* c, int n) {
+    for (int s = 0; s < n; ++s) {
+        cudaError_t e = launch_lo_faces(c->P, c->B, c->stream);
+        if (e != cudaSuccess) return e;
+        e = launch_lo_cells(c->P, c->B, 3, false, c->stream);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
+}
+
+static int build_graph(ugks_ctx* c, int steps) {
+    if (c->graph && c->graph_steps == steps) return UGKS_OK;
+    if (c->graph) { cudaGraphExecDestroy(c->graph); c->graph = nullptr; }
+    cudaGraph_t g;
+    UGKS_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_explicit_steps(c, steps);
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) { if (e2 == cudaSuccess) cudaGraphDestroy(g); return cuda_fail(e); }
+    UGKS_CK(e2);
+    e = cudaGraphInstantiate(&c->graph, g, 0);
+    cudaGraphDestroy(g);
+    UGKS_CK(e);
+    c->graph_steps = steps;
+    return UGKS_OK;
+}
+
+extern "C" int ugks_step_explicit(ugks_ctx* c, int nsteps, double* dt_out, double* res_out) {
+    if (!c || nsteps < 0) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    if (nsteps == 0) return UGKS_OK;
+    if (c->profile) {
+        for (int s = 0; s < nsteps; ++s) {
+            UGKS_CK(cudaEventRecord(c->ev[0], c->stream));
+            UGKS_CK(launch_lo_faces(c->P, c->B, c->stream));
+            UGKS_CK(cudaEventRecord(c->ev[1], c->stream));
+            UGKS_CK(launch_lo_cells(c->P, c->B, 3, false, c->stream));
+            UGKS_CK(cudaEventRecord(c->ev[2], c->stream));
+            UGKS_CK(cudaEventSynchronize(c->ev[2]));
+            float a = 0.f, b = 0.f;
+            UGKS_CK(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
+            UGKS_CK(cudaEventElapsedTime(&b, c->ev[1], c->ev[2]));
+            c->t_faces.total_ms += a; c->t_faces.launches += 1;
+            c->t_cells.total_ms += b; c->t_cells.launches += 1;
+        }
+        c->launches += 2LL * nsteps;
+    } else {
+        const int G = 16;
+        int full = nsteps / G, rem = nsteps % G;
+        if (full > 0) {
+            int r = build_graph(c, G);
+            if (r) return r;
+            for (int i = 0; i < full; ++i) UGKS_CK(cudaGraphLaunch(c->graph, c->stream));
+        }
+        UGKS_CK(enqueue_explicit_steps(c, rem));
+        c->launches += 2LL * nsteps;
+    }
+    if (dt_out) UGKS_CK(cudaMemcpyAsync(dt_out, c->B.dt + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return read_step_outputs(c, dt_out, res_out);
+}
+
+extern "C" int ugks_wall_aero(ugks_ctx* c, double* out) {
+    if (!c || !out) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    UGKS_CK(cudaMemcpyAsync(out, c->B.wall_aero, (size_t)2 * c->P.nx * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                            c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    return UGKS_OK;
+}
+
+extern "C" int ugks_copy_array(ugks_ctx* c, const char* name, double* host, size_t n) {
+    if (!c || !name || !host) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    const size_t nx = c->P.nx, ny = c->P.ny, nv = c->P.nvel, nc = nx * ny;
+    const double* src = nullptr;
+    size_t cnt = 0;
+    const std::string s(name);
+    if (s == "res_w") { src = c->B.res_w; cnt = nc * 4; }
+    else if (s == "res_h") { src = c->B.res_h; cnt = nc * nv; }
+    else if (s == "res_b") { src = c->B.res_b; cnt = nc * nv; }
+    else if (s == "fxh") { src = c->B.fxh; cnt = nc * nv; }
+    else if (s == "fxb") { src = c->B.fxb; cnt = nc * nv; }
+    else if (s == "fxw") { src = c->B.fxw; cnt = nc * 4; }
+    else if (s == "fyh") { src = c->B.fyh; cnt = (ny + 1) * nx * nv; }
+    else if (s == "fyb") { src = c->B.fyb; cnt = (ny + 1) * nx * nv; }
+    else if (s == "fyw") { src = c->B.fyw; cnt = (ny + 1) * nx * 4; }
+    else if (s == "pcol_h") { src = c->B.pcol_h; cnt = nc * nv; }
+    else if (s == "pcol_b") { src = c->B.pcol_b; cnt = nc * nv; }
+    else if (s == "peq_h") { src = c->B.peq_h; cnt = nc * nv; }
+    else if (s == "peq_b") { src = c->B.peq_b; cnt = nc * nv; }
+    else if (s == "dt") { src = c->B.dt; cnt = 2; }
+    else return UGKS_EINVAL;
+    if (n < cnt) return UGKS_EINVAL;
+    UGKS_CK(cudaMemcpyAsync(host, src, cnt * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    return UGKS_OK;
+}
+
+extern "C" unsigned ugks_last_status(const ugks_ctx* c) { return c ? c->last_status : 0u; }
+
+extern "C" void* ugks_stream(ugks_ctx* c) { return c ? (void*)c->stream : nullptr; }
+
+extern "C" int ugks_synchronize(ugks_ctx* c) {
+    if (!c) return UGKS_EINVAL;
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    return UGKS_OK;
+}
+
+extern "C" int ugks_profile_enable(ugks_ctx* c, int enable) {
+    if (!c) return UGKS_EINVAL;
+    c->profile = enable != 0;
+    c->t_faces = KernelTimer();
+    c->t_cells = KernelTimer();
+    return UGKS_OK;
+}
+
+extern "C" int ugks_profile_read(ugks_ctx* c, const char* kernel, double* total_ms, long long* launches) {
+    if (!c || !kernel) return UGKS_EINVAL;
+    const KernelTimer* t = nullptr;
+    if (!std::strcmp(kernel, "faces")) t = &c->t_faces;
+    else if (!std::strcmp(kernel, "cells")) t = &c->t_cells;
+    else return UGKS_EINVAL;
+    if (total_ms) *total_ms = t->total_ms;
+    if (launches) *launches = t->launches;
+    return UGKS_OK;
+}
+
+extern "C" long long ugks_launch_count(const ugks_ctx* c) { return c ? c->launches : 0; }

@@ -1,0 +1,49 @@
+// ugks_lo.cuh -- device-side state of one Couette domain and the second-order (Van-Leer UGKS)
+// kernels' parameter blocks.
+#pragma once
+#include "ugks_device.cuh"
+
+namespace ugks {
+
+constexpr int kMaxVel = 5 * 512;  // largest velocity set one CTA row covers (5 velocities x 512 threads)
+constexpr int kRedSlots = 40;    // max values reduced together in one block_reduce
+constexpr int kNDiag = 13;       // per-cell explicit residual-norm contributions
+
+struct LoParams {
+    int nx, ny, nvel, ck;
+    double dx, dy, area, gm1, pr, omega, mu_ref, cfl, umax, vmax;
+    double wall_ux[2];       // bottom, top wall speed (WallUx(3:4))
+    double wall_lam[2];      // 1/Tw per wall
+    double fixed_dt;         // > 0: Time_global_fixed
+};
+
+struct LoBuffers {
+    const double* u;         // [nvel] velocity table, k = i + j*Nu
+    const double* v;
+    const double* w;
+    double* h;               // [nc][nvel] state, cell c = j*nx + i
+    double* b;
+    double* W;               // [nc][4] conservative variables
+    double* fxh;             // [ny][nx][nvel] x-face micro flux (face i is between cells i-1 and i)
+    double* fxb;
+    double* fxw;             // [ny][nx][4] x-face macro flux
+    double* fyh;             // [ny+1][nx][nvel] y-face micro flux (row 0 / ny are the walls)
+    double* fyb;
+    double* fyw;             // [ny+1][nx][4]
+    double* res_w;           // [nc][4]   res_macro_flux_store
+    double* res_h;           // [nc][nvel] res_h_flux_store (moment-projected stream * dt)
+    double* res_b;
+    double* peq_h;           // [nc][nvel] physical equilibrium (implicit paths)
+    double* peq_b;
+    double* pcol_h;          // [nc][nvel] physical collision
+    double* pcol_b;
+    double* dtl;             // [nc] dt_local of the next TimeStep
+    double* dt;              // [2] dt_global of the next step; [1] dt of the last completed update
+    double* cell_diag;       // [nc][kNDiag]
+    double* diag;            // [kNDiag] reduced over cells by the last CTA
+    double* wall_aero;       // [2][nx][3] local-frame pnn, pnt, qn per wall face
+    unsigned* counter;       // [1] last-CTA counter (self-resetting)
+    unsigned* status;        // [1] error bits
+};
+
+}  // namespace ugks

@@ -1,0 +1,144 @@
+"""Host-side mirror of the reference's hot-path operator interface.
+
+The reference calls argument-less Fortran subroutines from Solve_UGKS (src/mod_Solve.f90:84-186):
+TimeStep, Interpolation, Evolution, ComputeResidual, ApplyExplicitUpdate,
+ApplySteadyImplicitUpdate.  `Solver` exposes the same operators, in the same order and with the
+same failure behaviour (a numerical gate failure raises `UgksError` carrying the reference's
+MPI_Abort code), over one device-resident Couette domain.  All compute runs in libugks_b200.so.
+"""
+import ctypes
+
+import numpy as np
+
+from . import capi
+from .case import CouetteCase
+
+_dp = ctypes.POINTER(ctypes.c_double)
+
+
+def _p(a):
+    return a.ctypes.data_as(_dp)
+
+
+class Solver:
+    """One Couette domain resident on a B200."""
+
+    def __init__(self, case: CouetteCase, u, v, w, device=0):
+        self.L = capi.load()
+        self.case = case
+        self.u = np.ascontiguousarray(u, dtype=np.float64)
+        self.v = np.ascontiguousarray(v, dtype=np.float64)
+        self.w = np.ascontiguousarray(w, dtype=np.float64)
+        self.nx, self.ny, self.nvel = case.nx, case.ny, len(self.u)
+        p = capi.UgksParams()
+        p.nx, p.ny, p.nvel = case.nx, case.ny, self.nvel
+        p.dx, p.dy = case.dx, case.dy
+        p.ck = case.ck
+        p.pr, p.omega, p.mu_ref, p.cfl = case.pr, case.omega, case.mu_ref, case.cfl
+        p.wall_ux[0], p.wall_ux[1] = case.wall_ux
+        p.wall_tnative[0], p.wall_tnative[1] = case.wall_tnative
+        p.fixed_dt = 0.0
+        p.method = capi.UGKS_METHOD_IMPLICIT_STEADY if case.method == "ImplicitSteady" else capi.UGKS_METHOD_EXPLICIT
+        p.ncfl, p.nslab, p.mass_rescale, p.macro_sweeps = case.ncfl, case.nslab, int(case.mass_rescale), case.macro_sweeps
+        p.residual_tol, p.moment_tol, p.min_alpha = case.residual_tol, case.moment_tol, case.min_alpha
+        self._params = p
+        ctx = ctypes.c_void_p()
+        self._check(self.L.ugks_ctx_create(ctypes.byref(p), _p(self.u), _p(self.v), _p(self.w), device,
+                                           ctypes.byref(ctx)), "ugks_ctx_create", None)
+        self.ctx = ctx
+
+    def _check(self, code, what, ctx="self"):
+        capi.check(self.L, self.ctx if ctx == "self" else ctx, code, what)
+
+    def close(self):
+        if getattr(self, "ctx", None):
+            self.L.ugks_ctx_destroy(self.ctx)
+            self.ctx = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def ncell(self):
+        return self.nx * self.ny
+
+    # ---- state
+    def init_freestream(self, rho=1.0, U=0.0, V=0.0, tnative=None):
+        t = self.case.tinf if tnative is None else tnative
+        self._check(self.L.ugks_init_freestream(self.ctx, rho, U, V, t), "ugks_init_freestream")
+
+    def upload(self, h, b, W):
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        assert h.size == self.ncell * self.nvel and W.size == self.ncell * 4
+        self._check(self.L.ugks_upload_state(self.ctx, _p(h), _p(b), _p(W)), "ugks_upload_state")
+
+    def download(self):
+        h = np.empty((self.ny, self.nx, self.nvel))
+        b = np.empty_like(h)
+        W = np.empty((self.ny, self.nx, 4))
+        self._check(self.L.ugks_download_state(self.ctx, _p(h), _p(b), _p(W)), "ugks_download_state")
+        return h, b, W
+
+    # ---- reference operators
+    def time_step(self):
+        """TimeStep (mod_Solve.f90:373-421): global CFL dt, computed on the device."""
+        dt = np.zeros(1)
+        self._check(self.L.ugks_timestep(self.ctx, _p(dt)), "TimeStep")
+        return float(dt[0])
+
+    def evolution(self):
+        """Interpolation + Evolution (mod_Interpolation.f90:26-90, mod_Evolution.f90:35-177)."""
+        self._check(self.L.ugks_evolution(self.ctx), "Evolution")
+
+    def compute_residual(self, with_collision=False):
+        """ComputeResidual (mod_Residual.f90:17-132)."""
+        self._check(self.L.ugks_compute_residual(self.ctx, int(with_collision)), "ComputeResidual")
+
+    def apply_explicit_update(self):
+        """ApplyExplicitUpdate (mod_TimeIntegrator.f90:16-134); returns the `res` vector."""
+        res = np.zeros(4)
+        self._check(self.L.ugks_apply_explicit_update(self.ctx, _p(res)), "ApplyExplicitUpdate")
+        return res
+
+    def step_explicit(self, nsteps=1):
+        """nsteps Explicit steps (mod_Solve.f90:84-186) fused and graph-replayed; returns (dt, res)."""
+        dt = np.zeros(1)
+        res = np.zeros(4)
+        self._check(self.L.ugks_step_explicit(self.ctx, int(nsteps), _p(dt), _p(res)), "Explicit step")
+        return float(dt[0]), res
+
+    def wall_aero(self):
+        out = np.empty((2, self.nx, 3))
+        self._check(self.L.ugks_wall_aero(self.ctx, _p(out)), "wall_aero")
+        return out
+
+    def array(self, name, shape):
+        out = np.empty(int(np.prod(shape)))
+        self._check(self.L.ugks_copy_array(self.ctx, name.encode(), _p(out), out.size), f"copy {name}")
+        return out.reshape(shape)
+
+    @property
+    def stream(self):
+        return self.L.ugks_stream(self.ctx)
+
+    def synchronize(self):
+        self._check(self.L.ugks_synchronize(self.ctx), "synchronize")
+
+    def profile(self, enable=True):
+        self._check(self.L.ugks_profile_enable(self.ctx, int(enable)), "profile")
+
+    def profile_read(self, kernel):
+        ms = ctypes.c_double()
+        n = ctypes.c_longlong()
+        self._check(self.L.ugks_profile_read(self.ctx, kernel.encode(), ctypes.byref(ms), ctypes.byref(n)),
+                    "profile_read")
+        return ms.value, n.value
+
+    @property
+    def launch_count(self):
+        return self.L.ugks_launch_count(self.ctx)
