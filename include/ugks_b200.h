@@ -121,7 +121,7 @@ int ugks_synchronize(ugks_ctx* ctx);
 
 /* Kernel-level timing: when enabled, ugks_step_explicit records CUDA events around each kernel
  * launch (graph replay off) and accumulates per-kernel milliseconds and launch counts.
- * names: "faces", "cells". */
+ * names: "slopes", "faces", "walls", "cells". */
 int ugks_profile_enable(ugks_ctx* ctx, int enable);
 int ugks_profile_read(ugks_ctx* ctx, const char* kernel, double* total_ms, long long* launches);
 

@@ -13,7 +13,9 @@
 
 namespace ugks {
 int lo_threads(int nvel);
+cudaError_t launch_lo_slopes(const LoParams& P, const LoBuffers& B, cudaStream_t s);
 cudaError_t launch_lo_faces(const LoParams& P, const LoBuffers& B, cudaStream_t s);
+cudaError_t launch_lo_walls(const LoParams& P, const LoBuffers& B, cudaStream_t s);
 cudaError_t launch_lo_cells(const LoParams& P, const LoBuffers& B, int mode, bool collision, cudaStream_t s);
 cudaError_t launch_lo_timestep(const LoParams& P, const LoBuffers& B, cudaStream_t s);
 cudaError_t launch_lo_init(const LoParams& P, const LoBuffers& B, double rho, double U, double V, double tn,
@@ -43,8 +45,8 @@ struct ugks_ctx {
     int graph_steps = 0;
     // profiling
     bool profile = false;
-    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
-    KernelTimer t_faces, t_cells;
+    cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
+    KernelTimer t_slopes, t_faces, t_walls, t_cells;
 };
 
 static int cuda_fail(cudaError_t e) {
@@ -119,6 +121,8 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     for (int k = 0; k < nv; ++k) { P.umax = std::fmax(P.umax, u[k]); P.vmax = std::fmax(P.vmax, v[k]); }
     for (int s = 0; s < 2; ++s) { P.wall_ux[s] = p->wall_ux[s]; P.wall_lam[s] = 1.0 / p->wall_tnative[s]; }
     P.fixed_dt = p->fixed_dt;
+    P.inv_dx = 1.0 / p->dx;
+    P.inv_dy = 1.0 / p->dy;
 
     // buffer plan (doubles)
     const size_t S = (size_t)nc * nv, SY = (size_t)(ny + 1) * nx * nv;
@@ -126,6 +130,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     auto take = [&](size_t n) { size_t o = off; off += (n + 31) / 32 * 32; return o; };
     const size_t o_u = take(nv), o_v = take(nv), o_w = take(nv);
     const size_t o_h = take(S), o_b = take(S), o_W = take((size_t)nc * 4);
+    const size_t o_sxh = take(S), o_syh = take(S), o_sxb = take(S), o_syb = take(S);
     const size_t o_fxh = take(S), o_fxb = take(S), o_fxw = take((size_t)nc * 4);
     const size_t o_fyh = take(SY), o_fyb = take(SY), o_fyw = take((size_t)(ny + 1) * nx * 4);
     const size_t o_rw = take((size_t)nc * 4), o_rh = take(S), o_rb = take(S);
@@ -143,6 +148,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     LoBuffers& B = c->B;
     B.u = d + o_u; B.v = d + o_v; B.w = d + o_w;
     B.h = d + o_h; B.b = d + o_b; B.W = d + o_W;
+    B.sxh = d + o_sxh; B.syh = d + o_syh; B.sxb = d + o_sxb; B.syb = d + o_syb;
     B.fxh = d + o_fxh; B.fxb = d + o_fxb; B.fxw = d + o_fxw;
     B.fyh = d + o_fyh; B.fyb = d + o_fyb; B.fyw = d + o_fyw;
     B.res_w = d + o_rw; B.res_h = d + o_rh; B.res_b = d + o_rb;
@@ -152,7 +158,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     e = cudaMemcpyAsync(d + o_u, u, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d + o_v, v, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d + o_w, w, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
-    for (int i = 0; i < 4 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+    for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { ugks_ctx_destroy(c); return cuda_fail(e); }
     *out = c;
@@ -164,7 +170,7 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
-    for (int i = 0; i < 4; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->dmem) cudaFree(c->dmem);
     if (c->dflags) cudaFree(c->dflags);
     if (c->stream) cudaStreamDestroy(c->stream);
@@ -226,8 +232,10 @@ extern "C" int ugks_timestep(ugks_ctx* c, double* dt_out) {
 extern "C" int ugks_evolution(ugks_ctx* c) {
     if (!c) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
+    UGKS_CK(launch_lo_slopes(c->P, c->B, c->stream));
     UGKS_CK(launch_lo_faces(c->P, c->B, c->stream));
-    c->launches += 1;
+    UGKS_CK(launch_lo_walls(c->P, c->B, c->stream));
+    c->launches += 3;
     return collect_status(c);
 }
 
@@ -274,7 +282,11 @@ extern "C" int ugks_apply_explicit_update(ugks_ctx* c, double* res_out) {
 
 static cudaError_t enqueue_explicit_steps(ugks_ctx* c, int n) {
     for (int s = 0; s < n; ++s) {
-        cudaError_t e = launch_lo_faces(c->P, c->B, c->stream);
+        cudaError_t e = launch_lo_slopes(c->P, c->B, c->stream);
+        if (e != cudaSuccess) return e;
+        e = launch_lo_faces(c->P, c->B, c->stream);
+        if (e != cudaSuccess) return e;
+        e = launch_lo_walls(c->P, c->B, c->stream);
         if (e != cudaSuccess) return e;
         e = launch_lo_cells(c->P, c->B, 3, false, c->stream);
         if (e != cudaSuccess) return e;
@@ -304,19 +316,27 @@ extern "C" int ugks_step_explicit(ugks_ctx* c, int nsteps, double* dt_out, doubl
     if (nsteps == 0) return UGKS_OK;
     if (c->profile) {
         for (int s = 0; s < nsteps; ++s) {
+            UGKS_CK(cudaEventRecord(c->ev[4], c->stream));
+            UGKS_CK(launch_lo_slopes(c->P, c->B, c->stream));
             UGKS_CK(cudaEventRecord(c->ev[0], c->stream));
             UGKS_CK(launch_lo_faces(c->P, c->B, c->stream));
             UGKS_CK(cudaEventRecord(c->ev[1], c->stream));
-            UGKS_CK(launch_lo_cells(c->P, c->B, 3, false, c->stream));
+            UGKS_CK(launch_lo_walls(c->P, c->B, c->stream));
             UGKS_CK(cudaEventRecord(c->ev[2], c->stream));
-            UGKS_CK(cudaEventSynchronize(c->ev[2]));
-            float a = 0.f, b = 0.f;
+            UGKS_CK(launch_lo_cells(c->P, c->B, 3, false, c->stream));
+            UGKS_CK(cudaEventRecord(c->ev[3], c->stream));
+            UGKS_CK(cudaEventSynchronize(c->ev[3]));
+            float a = 0.f, w = 0.f, b = 0.f, sl = 0.f;
+            UGKS_CK(cudaEventElapsedTime(&sl, c->ev[4], c->ev[0]));
             UGKS_CK(cudaEventElapsedTime(&a, c->ev[0], c->ev[1]));
-            UGKS_CK(cudaEventElapsedTime(&b, c->ev[1], c->ev[2]));
+            UGKS_CK(cudaEventElapsedTime(&w, c->ev[1], c->ev[2]));
+            UGKS_CK(cudaEventElapsedTime(&b, c->ev[2], c->ev[3]));
+            c->t_slopes.total_ms += sl; c->t_slopes.launches += 1;
             c->t_faces.total_ms += a; c->t_faces.launches += 1;
+            c->t_walls.total_ms += w; c->t_walls.launches += 1;
             c->t_cells.total_ms += b; c->t_cells.launches += 1;
         }
-        c->launches += 2LL * nsteps;
+        c->launches += 4LL * nsteps;
     } else {
         const int G = 16;
         int full = nsteps / G, rem = nsteps % G;
@@ -326,7 +346,7 @@ extern "C" int ugks_step_explicit(ugks_ctx* c, int nsteps, double* dt_out, doubl
             for (int i = 0; i < full; ++i) UGKS_CK(cudaGraphLaunch(c->graph, c->stream));
         }
         UGKS_CK(enqueue_explicit_steps(c, rem));
-        c->launches += 2LL * nsteps;
+        c->launches += 4LL * nsteps;
     }
     if (dt_out) UGKS_CK(cudaMemcpyAsync(dt_out, c->B.dt + 1, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     return read_step_outputs(c, dt_out, res_out);
@@ -382,7 +402,9 @@ extern "C" int ugks_synchronize(ugks_ctx* c) {
 extern "C" int ugks_profile_enable(ugks_ctx* c, int enable) {
     if (!c) return UGKS_EINVAL;
     c->profile = enable != 0;
+    c->t_slopes = KernelTimer();
     c->t_faces = KernelTimer();
+    c->t_walls = KernelTimer();
     c->t_cells = KernelTimer();
     return UGKS_OK;
 }
@@ -390,7 +412,9 @@ extern "C" int ugks_profile_enable(ugks_ctx* c, int enable) {
 extern "C" int ugks_profile_read(ugks_ctx* c, const char* kernel, double* total_ms, long long* launches) {
     if (!c || !kernel) return UGKS_EINVAL;
     const KernelTimer* t = nullptr;
-    if (!std::strcmp(kernel, "faces")) t = &c->t_faces;
+    if (!std::strcmp(kernel, "slopes")) t = &c->t_slopes;
+    else if (!std::strcmp(kernel, "faces")) t = &c->t_faces;
+    else if (!std::strcmp(kernel, "walls")) t = &c->t_walls;
     else if (!std::strcmp(kernel, "cells")) t = &c->t_cells;
     else return UGKS_EINVAL;
     if (total_ms) *total_ms = t->total_ms;

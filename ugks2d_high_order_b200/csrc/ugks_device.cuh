@@ -142,7 +142,9 @@ __device__ __forceinline__ double vanleer(double sL, double sR) {
 }
 
 // SolveDense4 (mod_ImplicitCommon.f90:84-113): Gauss-Jordan with partial pivoting on a
-// row-major 4x4.  Returns false where the reference sets ok=.false.
+// row-major 4x4.  Returns false where the reference sets ok=.false.  The pivot row is found as in
+// the reference (first row with the strictly largest |a(r,col)|) and swapped with predicated moves
+// on compile-time indices, so the augmented matrix stays in registers.
 __device__ __forceinline__ bool solve_dense4(const double m[16], const double rhs[4], double sol[4]) {
     double a[4][5];
     double ps = 0.0;
@@ -153,15 +155,26 @@ __device__ __forceinline__ bool solve_dense4(const double m[16], const double rh
         a[r][4] = rhs[r];
     }
     ps = fmax(ps, DBL_MIN);
+    bool ok = true;
 #pragma unroll
     for (int col = 0; col < 4; ++col) {
         int piv = col;
+        double best = fabs(a[col][col]);
 #pragma unroll
-        for (int r = col + 1; r < 4; ++r) if (fabs(a[r][col]) > fabs(a[piv][col])) piv = r;
-        if (fabs(a[piv][col]) <= 1000.0 * kEps * ps) return false;
-        if (piv != col) {
+        for (int r = col + 1; r < 4; ++r) {
+            const double v = fabs(a[r][col]);
+            if (v > best) { best = v; piv = r; }
+        }
+        ok = ok && !(best <= 1000.0 * kEps * ps);
 #pragma unroll
-            for (int c = 0; c < 5; ++c) { double t = a[col][c]; a[col][c] = a[piv][c]; a[piv][c] = t; }
+        for (int r = col + 1; r < 4; ++r) {
+            const bool sw = (piv == r);
+#pragma unroll
+            for (int c = 0; c < 5; ++c) {
+                const double t = a[col][c];
+                a[col][c] = sw ? a[r][c] : t;
+                a[r][c] = sw ? t : a[r][c];
+            }
         }
         const double d = a[col][col];
 #pragma unroll
@@ -174,7 +187,6 @@ __device__ __forceinline__ bool solve_dense4(const double m[16], const double rh
             for (int c = 0; c < 5; ++c) a[r][c] = a[r][c] - f * a[col][c];
         }
     }
-    bool ok = true;
 #pragma unroll
     for (int r = 0; r < 4; ++r) { sol[r] = a[r][4]; ok = ok && isfinite(sol[r]); }
     return ok;
@@ -214,35 +226,72 @@ __device__ __forceinline__ void moment_add(double wl, double un, double ut, doub
 }
 
 // ---------------------------------------------------------------------------------------------
-// Block-wide reductions (deterministic fixed tree: warp xor-shuffle, then a serial sum over the
-// warps' partials).  NS sums followed by NM maxima are reduced together; every thread returns
-// with the block totals in v[].  red must hold (blockDim/32) * (NS+NM) doubles; out NS+NM.
+// Block-wide reductions.  NS sums followed by NM maxima (NS, NM <= 32) are reduced in a fixed
+// tree, so results are deterministic run to run.  Inside a warp the values are reduced by
+// recursive halving: at each xor-shuffle distance every lane keeps one half of its values and sends
+// the other half, so N values cost about N shuffles instead of 5N.  Then one lane per value and
+// warp writes a partial, and a serial sum over the warps finishes.  Every thread returns with the
+// block totals in v[0..NS+NM).  red needs (blockDim/32)*(pow2(NS)+pow2(NM)) doubles, out NS+NM.
+constexpr int pow2_ceil(int n) { return n <= 1 ? 1 : 2 * pow2_ceil((n + 1) / 2); }
+constexpr int ilog2(int n) { return n <= 1 ? 0 : 1 + ilog2(n / 2); }
+
+template <int N, bool MAX>
+__device__ __forceinline__ double warp_halving(const double* v) {
+    constexpr int NP = pow2_ceil(N);
+    double t[NP];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) t[i] = i < N ? v[i] : (MAX ? -INFINITY : 0.0);
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int s = 0; s < 5; ++s) {
+        const int o = 16 >> s;
+        const int len = NP >> s;          // live values per lane before this step
+        if (len > 1) {
+            const int half = len >> 1;
+            const bool up = (lane & o) != 0;
+#pragma unroll
+            for (int i = 0; i < half; ++i) {
+                const double keep = up ? t[i + half] : t[i];
+                const double send = up ? t[i] : t[i + half];
+                const double recv = __shfl_xor_sync(0xffffffffu, send, o);
+                t[i] = MAX ? fmax(keep, recv) : keep + recv;
+            }
+        } else {
+            const double recv = __shfl_xor_sync(0xffffffffu, t[0], o);
+            t[0] = MAX ? fmax(t[0], recv) : t[0] + recv;
+        }
+    }
+    return t[0];   // the total of logical index (lane >> (5 - log2 NP)) when NP <= 32
+}
+
 template <int NS, int NM>
 __device__ __forceinline__ void block_reduce(double* v, double* red, double* out) {
-    constexpr int N = NS + NM;
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) {
-#pragma unroll
-        for (int i = 0; i < NS; ++i) v[i] += __shfl_xor_sync(0xffffffffu, v[i], o);
-#pragma unroll
-        for (int i = NS; i < N; ++i) v[i] = fmax(v[i], __shfl_xor_sync(0xffffffffu, v[i], o));
-    }
+    constexpr int PS = NS > 0 ? pow2_ceil(NS) : 0;
+    constexpr int PM = NM > 0 ? pow2_ceil(NM) : 0;
+    constexpr int W = PS + PM;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31, nw = blockDim.x >> 5;
-    if (lane == 0) {
-#pragma unroll
-        for (int i = 0; i < N; ++i) red[warp * N + i] = v[i];
+    if (NS > 0) {
+        const double r = warp_halving<NS, false>(v);
+        constexpr int sh = 5 - ilog2(PS);
+        if ((lane & ((1 << sh) - 1)) == 0) red[warp * W + (lane >> sh)] = r;
+    }
+    if (NM > 0) {
+        const double r = warp_halving<NM, true>(v + NS);
+        constexpr int sh = 5 - ilog2(PM);
+        if ((lane & ((1 << sh) - 1)) == 0) red[warp * W + PS + (lane >> sh)] = r;
     }
     __syncthreads();
-    if (threadIdx.x < N) {
+    if (threadIdx.x < NS + NM) {
         const int i = threadIdx.x;
-        double s = red[i];
-        if (i < NS) { for (int w = 1; w < nw; ++w) s += red[w * N + i]; }
-        else { for (int w = 1; w < nw; ++w) s = fmax(s, red[w * N + i]); }
+        const int col = i < NS ? i : PS + (i - NS);
+        double s = red[col];
+        if (i < NS) { for (int w = 1; w < nw; ++w) s += red[w * W + col]; }
+        else { for (int w = 1; w < nw; ++w) s = fmax(s, red[w * W + col]); }
         out[i] = s;
     }
     __syncthreads();
 #pragma unroll
-    for (int i = 0; i < N; ++i) v[i] = out[i];
+    for (int i = 0; i < NS + NM; ++i) v[i] = out[i];
     __syncthreads();
 }
 

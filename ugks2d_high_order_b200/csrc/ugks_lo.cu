@@ -1,114 +1,136 @@
 // ugks_lo.cu -- second-order UGKS hot path for one Couette domain on sm_100a (FP64).
 //
-//   k_lo_faces  : Interpolation (mod_Interpolation.f90:26-170) fused into the face flux of
-//                 EvolutionNative (mod_Evolution.f90:46-177): one CTA per face, the upwind cell's
-//                 Van-Leer slopes recomputed on the fly from the L2-resident state;
-//                 CalcFlux_MultiDimension (:186-492) for interior faces, W2BMultiscaleFluxBoundary
-//                 (:1888-2449) for the 2*nx wall faces.
+//   k_lo_slopes : Interpolation (mod_Interpolation.f90:26-170): Van-Leer slopes of h and b in x
+//                 and y for every (cell, velocity); one-sided slopes on the wall rows.
+//   k_lo_faces  : the interior-face flux of EvolutionNative / CalcFlux_MultiDimension
+//                 (mod_Evolution.f90:46-177,186-492): one CTA per face.
+//   k_lo_walls  : W2BMultiscaleFluxBoundary (mod_Evolution.f90:1888-2449) on the 2*nx wall faces.
 //   k_lo_cells  : ComputeResidual (mod_Residual.f90:17-132) + ApplyExplicitUpdate
 //                 (mod_TimeIntegrator.f90:16-293) fused, one CTA per cell, plus the next TimeStep
-//                 (mod_Solve.f90:373-421) and the residual norms reduced by the last CTA.
+//                 (mod_Solve.f90:373-421) and the residual norms, reduced by the last CTA.
 //
-// Layout: h, b are [cell][velocity] (velocity fastest, coalesced FP64 rows); one CTA covers a
-// whole velocity row with kVPT velocities per thread, so every moment sum is one block reduction.
+// Layout: h, b and the slopes are [cell][velocity] (velocity fastest, coalesced FP64 rows).  A
+// CTA covers a whole velocity row, VPT velocities per thread, so every velocity-space moment sum
+// is one block reduction.  Velocity loops are branch-free: a thread slot beyond nvel reads a valid
+// velocity with weight 0 and skips its stores, so the compiler can interleave the VPT chains.
 #include "ugks_lo.cuh"
 
 namespace ugks {
 
 __device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i >= nx ? i - nx : i); }
 
-// Slope of array A at cell (i,j) in direction d for velocity k (Interp_VanLeer / InterpBoundary).
-// Wall rows use the one-sided (right-left)/dy slope (mod_Interpolation.f90:40-45,78-88).
-__device__ __forceinline__ double lo_slope(const LoParams& P, const double* __restrict__ A, int d, int i, int j,
-                                           int k) {
-    const int nv = P.nvel;
-    const double a0 = A[(size_t)(j * P.nx + i) * nv + k];
-    if (d == 0) {
-        const double am = A[(size_t)(j * P.nx + wrapx(i - 1, P.nx)) * nv + k];
-        const double ap = A[(size_t)(j * P.nx + wrapx(i + 1, P.nx)) * nv + k];
-        return vanleer((a0 - am) / P.dx, (ap - a0) / P.dx);
-    }
+// Velocity slot r of this thread: k, clamped index kk, and whether it is a real velocity.
+struct Slot {
+    int k, kk;
+    bool ok;
+};
+__device__ __forceinline__ Slot slot(int r, int nv) {
+    Slot s;
+    s.k = threadIdx.x + r * blockDim.x;
+    s.ok = s.k < nv;
+    s.kk = s.ok ? s.k : nv - 1;
+    return s;
+}
+
+// -------------------------------------------------------------------------------------------
+// Interpolation (mod_Interpolation.f90:26-90): slopes sx*, sy* of h and b.  x is periodic; on
+// the wall rows the y slope is the one-sided (right-left)/dy of InterpBoundary (:100-117), and
+// UnifiedPhysicalOperators skips the Van-Leer inner loop there (:40-45,78-88).
+__global__ void __launch_bounds__(256) k_lo_slopes(LoParams P, LoBuffers B) {
+    const int nv = P.nvel, nx = P.nx, ny = P.ny;
+    const size_t n = (size_t)nx * ny * nv;
+    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx >= n) return;
+    const int k = (int)(idx % nv);
+    const int c = (int)(idx / nv), i = c % nx, j = c / nx;
+    const size_t cm = (size_t)(j * nx + wrapx(i - 1, nx)) * nv + k, cp = (size_t)(j * nx + wrapx(i + 1, nx)) * nv + k;
+    const double h0 = B.h[idx], b0 = B.b[idx];
+    B.sxh[idx] = vanleer((h0 - B.h[cm]) * P.inv_dx, (B.h[cp] - h0) * P.inv_dx);
+    B.sxb[idx] = vanleer((b0 - B.b[cm]) * P.inv_dx, (B.b[cp] - b0) * P.inv_dx);
+    double syh, syb;
     if (j == 0) {
-        const double ap = A[(size_t)((j + 1) * P.nx + i) * nv + k];
-        return (ap - a0) / P.dy;
+        const size_t u = idx + (size_t)nx * nv;
+        syh = (B.h[u] - h0) * P.inv_dy;
+        syb = (B.b[u] - b0) * P.inv_dy;
+    } else if (j == ny - 1) {
+        const size_t d = idx - (size_t)nx * nv;
+        syh = (h0 - B.h[d]) * P.inv_dy;
+        syb = (b0 - B.b[d]) * P.inv_dy;
+    } else {
+        const size_t u = idx + (size_t)nx * nv, d = idx - (size_t)nx * nv;
+        syh = vanleer((h0 - B.h[d]) * P.inv_dy, (B.h[u] - h0) * P.inv_dy);
+        syb = vanleer((b0 - B.b[d]) * P.inv_dy, (B.b[u] - b0) * P.inv_dy);
     }
-    if (j == P.ny - 1) {
-        const double am = A[(size_t)((j - 1) * P.nx + i) * nv + k];
-        return (a0 - am) / P.dy;
-    }
-    const double am = A[(size_t)((j - 1) * P.nx + i) * nv + k];
-    const double ap = A[(size_t)((j + 1) * P.nx + i) * nv + k];
-    return vanleer((a0 - am) / P.dy, (ap - a0) / P.dy);
+    B.syh[idx] = syh;
+    B.syb[idx] = syb;
 }
 
 // -------------------------------------------------------------------------------------------
 // Interior face: CalcFlux_MultiDimension (mod_Evolution.f90:186-492), UnifiedPhysicalOperators.
-// dir 0: vertical face (vn = u, vt = v); dir 1: horizontal face (vn = v, vt = -u).
+// dir 0: vertical face (vn = u, vt = v); dir 1: horizontal face (vn = v, vt = -u).  The upwind
+// cell per velocity is the reference's delta = (sign(1,vn)+1)/2 selector (:236-266).
 template <int VPT>
-__device__ void lo_face_interior(const LoParams& P, const LoBuffers& B, int dir, int iL, int jL, int iR, int jR,
-                                 double dt, double* __restrict__ Fh, double* __restrict__ Fb, double* Fw,
-                                 double* red, double* rout) {
-    const int nv = P.nvel, tid = threadIdx.x, NT = blockDim.x;
+__device__ __forceinline__ void lo_face_interior(const LoParams& P, const LoBuffers& B, int dir, int cL, int cR,
+                                                 double dt, double* __restrict__ Fh, double* __restrict__ Fb,
+                                                 double* Fw, double* red, double* rout) {
+    const int nv = P.nvel, tid = threadIdx.x;
     const double len = dir == 0 ? P.dx : P.dy;      // cell length normal to the face
     const double flen = dir == 0 ? P.dy : P.dx;     // face length
     const double hl = 0.5 * len;
-    double hv[VPT], bv[VPT], shn[VPT], sbn[VPT], sht[VPT], sbt[VPT], H0[VPT], B0[VPT];
-    double acc[16];
+    const double* sN_h = dir == 0 ? B.sxh : B.syh;
+    const double* sN_b = dir == 0 ? B.sxb : B.syb;
+    const double* sT_h = dir == 0 ? B.syh : B.sxh;
+    const double* sT_b = dir == 0 ? B.syb : B.sxb;
+    const double tsg = dir == 0 ? 1.0 : -1.0;       // tangential sign flip on horizontal faces (:262-265)
+    double hv[VPT], bv[VPT], H0[VPT];
+    double acc[14];
 #pragma unroll
     for (int m = 0; m < 8; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        hv[r] = bv[r] = shn[r] = sbn[r] = sht[r] = sbt[r] = 0.0;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], wk = B.w[k];
+        const Slot s = slot(r, nv);
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
         const double vn = dir == 0 ? uk : vk, vt = dir == 0 ? vk : -uk;
-        const bool left = copysign(1.0, vn) > 0.0;       // delta = (sign(1,vn)+1)/2
-        const int ci = left ? iL : iR, cj = left ? jL : jR;
-        const size_t ck = (size_t)(cj * P.nx + ci) * nv + k;
-        const double sgn = left ? 1.0 : -1.0;
-        const double snh = lo_slope(P, B.h, dir, ci, cj, k), snb = lo_slope(P, B.b, dir, ci, cj, k);
-        const double sth = lo_slope(P, B.h, 1 - dir, ci, cj, k), stb = lo_slope(P, B.b, 1 - dir, ci, cj, k);
-        hv[r] = B.h[ck] + sgn * (hl * snh);
-        bv[r] = B.b[ck] + sgn * (hl * snb);
-        shn[r] = snh; sbn[r] = snb;
-        sht[r] = dir == 0 ? sth : -sth;
-        sbt[r] = dir == 0 ? stb : -stb;
+        const bool left = copysign(1.0, vn) > 0.0;
+        const size_t q = (size_t)(left ? cL : cR) * nv + s.kk;
+        const double sg = left ? hl : -hl;
+        hv[r] = B.h[q] + sg * sN_h[q];
+        bv[r] = B.b[q] + sg * sN_b[q];
+        const double sht = tsg * sT_h[q], sbt = tsg * sT_b[q];
         const double v2 = vn * vn + vt * vt;
         acc[0] += wk * hv[r];
         acc[1] += wk * vn * hv[r];
         acc[2] += wk * vt * hv[r];
         acc[3] += 0.5 * wk * (v2 * hv[r] + bv[r]);
-        acc[4] += wk * sht[r];
-        acc[5] += wk * vn * sht[r];
-        acc[6] += wk * vt * sht[r];
-        acc[7] += 0.5 * wk * (v2 * sht[r] + sbt[r]);
+        acc[4] += wk * sht;
+        acc[5] += wk * vn * sht;
+        acc[6] += wk * vt * sht;
+        acc[7] += 0.5 * wk * (v2 * sht + sbt);
     }
     block_reduce<8, 0>(acc, red, rout);
-    // face state, slopes, collision time (every thread, identical values)
+    // face state, micro slopes aL, aR, b, A and the time coefficients (every thread, same values)
     Prim pf;
     const double cv[4] = {acc[0], acc[1], acc[2], acc[3]};
-    bool ok = get_primary(P.gm1, cv, pf);
-    const double* WL = B.W + (jL * P.nx + iL) * 4;
-    const double* WR = B.W + (jR * P.nx + iR) * 4;
-    double wl[4], wr[4];
-    if (dir == 0) { wl[0] = WL[0]; wl[1] = WL[1]; wl[2] = WL[2]; wl[3] = WL[3];
-                    wr[0] = WR[0]; wr[1] = WR[1]; wr[2] = WR[2]; wr[3] = WR[3]; }
-    else { wl[0] = WL[0]; wl[1] = WL[2]; wl[2] = -WL[1]; wl[3] = WL[3];
-           wr[0] = WR[0]; wr[1] = WR[2]; wr[2] = -WR[1]; wr[3] = WR[3]; }
-    double sw[4], aL[4], aR[4], bs[4], aT[4], Mt[5], tau = 1.0;
+    const bool ok = get_primary(P.gm1, cv, pf);
     if (!ok) { pf.r = 1.0; pf.U = 0.0; pf.V = 0.0; pf.L = 1.0; }
+    const double* WL = B.W + cL * 4;
+    const double* WR = B.W + cR * 4;
+    double wl[4], wr[4];
+    wl[0] = WL[0]; wl[3] = WL[3]; wr[0] = WR[0]; wr[3] = WR[3];
+    if (dir == 0) { wl[1] = WL[1]; wl[2] = WL[2]; wr[1] = WR[1]; wr[2] = WR[2]; }
+    else { wl[1] = WL[2]; wl[2] = -WL[1]; wr[1] = WR[2]; wr[2] = -WR[1]; }
+    double sw[4], aL[4], aR[4], bs[4], aT[4], Mt[5], tau = 1.0, mxi2;
 #pragma unroll
     for (int m = 0; m < 4; ++m) sw[m] = (cv[m] - wl[m]) / hl;
     micro_slope(P.ck, pf, sw, aL);
 #pragma unroll
     for (int m = 0; m < 4; ++m) sw[m] = (wr[m] - cv[m]) / hl;
     micro_slope(P.ck, pf, sw, aR);
-    const double swt[4] = {acc[4], acc[5], acc[6], acc[7]};
-    micro_slope(P.ck, pf, swt, bs);
-    Moments M;
-    calc_moment(P.ck, pf, M);
     {
+        const double swt[4] = {acc[4], acc[5], acc[6], acc[7]};
+        micro_slope(P.ck, pf, swt, bs);
+        Moments M;
+        calc_moment(P.ck, pf, M);
         double MauL[4], MauR[4], Mbv[4];
         moment_auvxi(aL, M.MuL, M.Mv, M.Mxi, 1, 0, MauL);
         moment_auvxi(aR, M.MuR, M.Mv, M.Mxi, 1, 0, MauR);
@@ -116,6 +138,7 @@ __device__ void lo_face_interior(const LoParams& P, const LoBuffers& B, int dir,
 #pragma unroll
         for (int m = 0; m < 4; ++m) sw[m] = -pf.r * (MauL[m] + MauR[m] + Mbv[m]);
         micro_slope(P.ck, pf, sw, aT);
+        mxi2 = M.Mxi[2];
     }
     const bool tok = get_tau(P.mu_ref, P.omega, pf, tau);
     if (!tok) tau = 1.0;
@@ -124,85 +147,88 @@ __device__ void lo_face_interior(const LoParams& P, const LoBuffers& B, int dir,
         if (!ok) set_status(B.status, ST_GETPRIMARY);
         if (ok && !tok) set_status(B.status, ST_TAU);
     }
-    // face equilibrium H0, B0 (PrepareNativeFaceEquilibrium, mod_Evolution.f90:16-30) + heat flux
+    // face equilibrium H0 (PrepareNativeFaceEquilibrium, mod_Evolution.f90:16-30) + heat flux
     const double pref = pf.r * (pf.L / kPi), bfac = (double)P.ck / (2.0 * pf.L);
-    acc[0] = acc[1] = 0.0;
-    acc[2] = acc[3] = 0.0;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        H0[r] = B0[r] = 0.0;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], wk = B.w[k];
+        const Slot s = slot(r, nv);
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
         const double vn = dir == 0 ? uk : vk, vt = dir == 0 ? vk : -uk;
         const double dvn = vn - pf.U, dvt = vt - pf.V, v2 = dvn * dvn + dvt * dvt;
         H0[r] = pref * exp(-pf.L * v2);
-        B0[r] = H0[r] * bfac;
-        acc[0] += 0.5 * wk * dvn * (v2 * hv[r] + bv[r]);
-        acc[1] += 0.5 * wk * dvt * (v2 * hv[r] + bv[r]);
-        acc[2] = fmax(acc[2], fabs(H0[r]));
-        acc[3] = fmax(acc[3], fabs(B0[r]));
+        const double t = 0.5 * wk * (v2 * hv[r] + bv[r]);
+        acc[0] += t * dvn;
+        acc[1] += t * dvt;
+        acc[2] = fmax(acc[2], s.ok ? fabs(H0[r]) : 0.0);
+        acc[3] = fmax(acc[3], s.ok ? fabs(H0[r] * bfac) : 0.0);
     }
     block_reduce<2, 2>(acc, red, rout);
     const double qf0 = acc[0], qf1 = acc[1];
     const double sch = fmax(acc[2], 1.0), scb = fmax(acc[3], 1.0);
-    // ProjectToConservedMoments of H0,B0 onto GetConserved(pf) in the local frame
+    // ProjectToConservedMoments of (H0, B0) onto GetConserved(pf), local frame (mod_ImplicitCommon.f90:42-82)
 #pragma unroll
     for (int m = 0; m < 14; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], wk = B.w[k];
+        const Slot s = slot(r, nv);
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
         const double vn = dir == 0 ? uk : vk, vt = dir == 0 ? vk : -uk;
-        moment_add(wk, vn, vt, H0[r], B0[r], acc);
-        gram_add(wk, fmax(fabs(H0[r]), kEps * sch), fmax(fabs(B0[r]), kEps * scb), vn, vt, acc + 4);
+        const double b0 = H0[r] * bfac;
+        moment_add(wk, vn, vt, H0[r], b0, acc);
+        gram_add(wk, fmax(fabs(H0[r]), kEps * sch), fmax(fabs(b0), kEps * scb), vn, vt, acc + 4);
     }
     block_reduce<14, 0>(acc, red, rout);
-    double tgt[4], rhs[4], gm[16], lam[4];
+    double tgt[4], lam[4];
     get_conserved(P.gm1, pf, tgt);
+    {
+        double rhs[4], gm[16];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) rhs[m] = tgt[m] - acc[m];
-    gram_expand(acc + 4, gm);
-    const bool pok = solve_dense4(gm, rhs, lam);
-    if (!pok) { lam[0] = lam[1] = lam[2] = lam[3] = 0.0; }
-    // Shakhov part and the micro flux (mod_Evolution.f90:396-453), scaled by the face length.
+        for (int m = 0; m < 4; ++m) rhs[m] = tgt[m] - acc[m];
+        gram_expand(acc + 4, gm);
+        if (!solve_dense4(gm, rhs, lam)) {
+            lam[0] = lam[1] = lam[2] = lam[3] = 0.0;
+            if (tid == 0) set_status(B.status, ST_FACE_PROJECTION);
+        }
+    }
+    // Shakhov part and the micro flux (mod_Evolution.f90:396-453), times the face length.
     const double coeff = 0.8 * (1.0 - P.pr) * pf.L * pf.L / pf.r;
     const double c2ck = 2.0 / (double)P.ck;
 #pragma unroll
     for (int m = 0; m < 8; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], wk = B.w[k];
+        const Slot s = slot(r, nv);
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
         const double a = dir == 0 ? uk : vk, t = dir == 0 ? vk : -uk;
-        const double wh = fmax(fabs(H0[r]), kEps * sch), wb = fmax(fabs(B0[r]), kEps * scb);
+        const double b0 = H0[r] * bfac;
         const double e = 0.5 * (a * a + t * t);
-        const double H = H0[r] + wh * (lam[0] + a * lam[1] + t * lam[2] + e * lam[3]);
-        const double Bq = B0[r] + 0.5 * wb * lam[3];
+        const double H = H0[r] + fmax(fabs(H0[r]), kEps * sch) * (lam[0] + a * lam[1] + t * lam[2] + e * lam[3]);
+        const double Bq = b0 + 0.5 * fmax(fabs(b0), kEps * scb) * lam[3];
         moment_add(wk, a, t, H, Bq, acc);   // projection gate
+        const bool left = copysign(1.0, a) > 0.0;
+        const size_t q = (size_t)(left ? cL : cR) * nv + s.kk;
+        const double shn = sN_h[q], sbn = sN_b[q], sht = tsg * sT_h[q], sbt = tsg * sT_b[q];
         const double dvn = a - pf.U, dvt = t - pf.V, dv2 = dvn * dvn + dvt * dvt;
         const double qdot = dvn * qf0 + dvt * qf1;
-        const double shH = 2.0 * pf.L * dv2 - 4.0, shB = shH + c2ck;
-        const double Hp = coeff * qdot * shH * H, Bp = coeff * qdot * shB * Bq;
+        const double shH = 2.0 * pf.L * dv2 - 4.0;
+        const double Hp = coeff * qdot * shH * H, Bp = coeff * qdot * (shH + c2ck) * Bq;
         const double v2 = a * a + t * t;
-        const bool left = copysign(1.0, a) > 0.0;
-        const double slh = a * shn[r] + t * sht[r], slb = a * sbn[r] + t * sbt[r];
+        const double slh = a * shn + t * sht, slb = a * sbn + t * sbt;
         const double* as = left ? aL : aR;
         const double h_a = as[0] * H + as[1] * a * H + as[2] * t * H + 0.5 * as[3] * (v2 * H + Bq);
         const double h_b = bs[0] * H + bs[1] * a * H + bs[2] * t * H + 0.5 * bs[3] * (v2 * H + Bq);
         const double h_T = aT[0] * H + aT[1] * a * H + aT[2] * t * H + 0.5 * aT[3] * (v2 * H + Bq);
-        const double b_a = as[0] * Bq + as[1] * a * Bq + as[2] * t * Bq + 0.5 * as[3] * (v2 * Bq + M.Mxi[2] * H);
-        const double b_b = bs[0] * Bq + bs[1] * a * Bq + bs[2] * t * Bq + 0.5 * bs[3] * (v2 * Bq + M.Mxi[2] * H);
-        const double b_T = aT[0] * Bq + aT[1] * a * Bq + aT[2] * t * Bq + 0.5 * aT[3] * (v2 * Bq + M.Mxi[2] * H);
+        const double b_a = as[0] * Bq + as[1] * a * Bq + as[2] * t * Bq + 0.5 * as[3] * (v2 * Bq + mxi2 * H);
+        const double b_b = bs[0] * Bq + bs[1] * a * Bq + bs[2] * t * Bq + 0.5 * bs[3] * (v2 * Bq + mxi2 * H);
+        const double b_T = aT[0] * Bq + aT[1] * a * Bq + aT[2] * t * Bq + 0.5 * aT[3] * (v2 * Bq + mxi2 * H);
         const double fh = Mt[0] * a * (H + Hp) + Mt[1] * a * a * h_a + Mt[1] * a * t * h_b + Mt[2] * a * h_T +
                           Mt[3] * a * hv[r] - Mt[4] * a * slh;
         const double fb = Mt[0] * a * (Bq + Bp) + Mt[1] * a * a * b_a + Mt[1] * a * t * b_b + Mt[2] * a * b_T +
                           Mt[3] * a * bv[r] - Mt[4] * a * slb;
         const double Fhk = flen * fh, Fbk = flen * fb;
-        Fh[k] = Fhk;
-        Fb[k] = Fbk;
+        if (s.ok) { Fh[s.k] = Fhk; Fb[s.k] = Fbk; }
         moment_add(wk, uk, vk, Fhk, Fbk, acc + 4);   // MomentConserved in the global frame (:470-473)
     }
     block_reduce<8, 0>(acc, red, rout);
@@ -211,7 +237,7 @@ __device__ void lo_face_interior(const LoParams& P, const LoBuffers& B, int dir,
         double err = 0.0;
 #pragma unroll
         for (int m = 0; m < 4; ++m) err = fmax(err, fabs(acc[m] - tgt[m]));
-        if (!pok || !(err <= 1.0e-10 * rs)) set_status(B.status, ST_FACE_PROJECTION);
+        if (!(err <= 1.0e-10 * rs)) set_status(B.status, ST_FACE_PROJECTION);
         bool fin = true;
 #pragma unroll
         for (int m = 0; m < 4; ++m) { Fw[m] = acc[4 + m]; fin = fin && isfinite(acc[4 + m]); }
@@ -223,24 +249,24 @@ __device__ void lo_face_interior(const LoParams& P, const LoBuffers& B, int dir,
 // Wall face: W2BMultiscaleFluxBoundary (mod_Evolution.f90:1888-2449) on the horizontal walls.
 // side -1: bottom wall below row 0 (Lside); +1: top wall above row ny-1 (Rside).
 template <int VPT>
-__device__ void lo_face_wall(const LoParams& P, const LoBuffers& B, int side, int i, double dt,
-                             double* __restrict__ Fh, double* __restrict__ Fb, double* Fw, double* aero,
-                             double* red, double* rout) {
-    const int nv = P.nvel, tid = threadIdx.x, NT = blockDim.x;
+__device__ __forceinline__ void lo_face_wall(const LoParams& P, const LoBuffers& B, int side, int i, double dt,
+                                             double* __restrict__ Fh, double* __restrict__ Fb, double* Fw,
+                                             double* aero, double* red, double* rout) {
+    const int nv = P.nvel, tid = threadIdx.x;
     const int iw = side < 0 ? 0 : 1;
     const int j = side < 0 ? 0 : P.ny - 1;
     const int cell = j * P.nx + i;
     const double len = P.dy, flen = P.dx;
     const double rot = -(double)side;
-    double hv[VPT], bv[VPT], shn[VPT], sbn[VPT], sht[VPT], sbt[VPT], Hg[VPT], Bg[VPT], Hw[VPT], Bw[VPT];
-    // wall and cell states in the local frame (vn = v, vt = -u)
+    double hv[VPT], bv[VPT], Hg[VPT], Hw[VPT];
     const double* Wc = B.W + cell * 4;
     Prim pc;
     const bool ok = get_primary(P.gm1, Wc, pc);
-    Prim prim{pc.r, pc.V, -pc.U, pc.L};
-    Prim pw{1.0, P.wall_ux[iw] * (-0.0) + 0.0 * 1.0, -P.wall_ux[iw] * 1.0 + 0.0 * (-0.0), P.wall_lam[iw]};
+    // LocalFrame with cosx = -0, cosy = 1 (mod_Tools.f90:150-162): (r, U, V) -> (r, V, -U)
+    const Prim prim{pc.r, pc.V, -pc.U, pc.L};
+    const Prim pw{1.0, P.wall_ux[iw] * (-0.0) + 0.0 * 1.0, -P.wall_ux[iw] * 1.0 + 0.0 * (-0.0), P.wall_lam[iw]};
     Prim pg = pw;
-    pg.r = prim.r / prim.L * pw.L;
+    pg.r = prim.r / prim.L * pw.L;   // keep the cell pressure (:2027)
     double tau = 1.0, Mt[5];
     const bool tok = get_tau(P.mu_ref, P.omega, pg, tau);
     if (!tok) tau = 1.0;
@@ -250,109 +276,109 @@ __device__ void lo_face_wall(const LoParams& P, const LoBuffers& B, int side, in
         if (ok && !tok) set_status(B.status, ST_TAU);
     }
     const double prefg = pg.r * (pg.L / kPi), prefw = 1.0 * (pw.L / kPi), bfac = (double)P.ck / (2.0 * pw.L);
-    double acc[40];
+    double acc[28];
 #pragma unroll
     for (int m = 0; m < 10; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        hv[r] = bv[r] = shn[r] = sbn[r] = sht[r] = sbt[r] = Hg[r] = Bg[r] = Hw[r] = Bw[r] = 0.0;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], wk = B.w[k];
+        const Slot s = slot(r, nv);
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
         const double vn = vk, vt = -uk;
-        const size_t ckk = (size_t)cell * nv + k;
-        shn[r] = lo_slope(P, B.h, 1, i, j, k);
-        sbn[r] = lo_slope(P, B.b, 1, i, j, k);
-        sht[r] = -lo_slope(P, B.h, 0, i, j, k);
-        sbt[r] = -lo_slope(P, B.b, 0, i, j, k);
-        hv[r] = B.h[ckk] - rot * 0.5 * len * shn[r];
-        bv[r] = B.b[ckk] - rot * 0.5 * len * sbn[r];
+        const size_t q = (size_t)cell * nv + s.kk;
+        const double sht = -B.sxh[q], sbt = -B.sxb[q];
+        hv[r] = B.h[q] - rot * 0.5 * len * B.syh[q];
+        bv[r] = B.b[q] - rot * 0.5 * len * B.syb[q];
         const double dvn = vn - pg.U, dvt = vt - pg.V, v2 = dvn * dvn + dvt * dvt;
         const double ex = exp(-pg.L * v2);
         Hg[r] = prefg * ex;
-        Bg[r] = Hg[r] * bfac;
         Hw[r] = prefw * ex;
-        Bw[r] = Hw[r] * bfac;
         const double lv2 = vn * vn + vt * vt;
-        acc[0] += wk * sht[r];
-        acc[1] += wk * vn * sht[r];
-        acc[2] += wk * vt * sht[r];
-        acc[3] += 0.5 * wk * (lv2 * sht[r] + sbt[r]);
+        acc[0] += wk * sht;
+        acc[1] += wk * vn * sht;
+        acc[2] += wk * vt * sht;
+        acc[3] += 0.5 * wk * (lv2 * sht + sbt);
         acc[4] += 0.5 * wk * dvn * (v2 * hv[r] + bv[r]);
         acc[5] += 0.5 * wk * dvt * (v2 * hv[r] + bv[r]);
-        acc[6] = fmax(acc[6], fabs(Hg[r]));
-        acc[7] = fmax(acc[7], fabs(Bg[r]));
-        acc[8] = fmax(acc[8], fabs(Hw[r]));
-        acc[9] = fmax(acc[9], fabs(Bw[r]));
+        acc[6] = fmax(acc[6], s.ok ? fabs(Hg[r]) : 0.0);
+        acc[7] = fmax(acc[7], s.ok ? fabs(Hg[r] * bfac) : 0.0);
+        acc[8] = fmax(acc[8], s.ok ? fabs(Hw[r]) : 0.0);
+        acc[9] = fmax(acc[9], s.ok ? fabs(Hw[r] * bfac) : 0.0);
     }
     block_reduce<6, 4>(acc, red, rout);
     const double swt[4] = {acc[0], acc[1], acc[2], acc[3]};
     const double qf0 = acc[4], qf1 = acc[5];
     const double sgh = fmax(acc[6], 1.0), sgb = fmax(acc[7], 1.0), swh = fmax(acc[8], 1.0), swb = fmax(acc[9], 1.0);
     // micro slopes a_gn, a_gt, a_T (mod_Evolution.f90:2044-2087)
-    double cg[4], a_gn[4], a_gt[4], a_T[4], sw[4];
+    double cg[4], a_gn[4], a_gt[4], a_T[4], sw[4], mxi2;
     get_conserved(P.gm1, pg, cg);
     const double cg1[4] = {Wc[0], Wc[2], -Wc[1], Wc[3]};
 #pragma unroll
     for (int m = 0; m < 4; ++m) sw[m] = (cg[m] - cg1[m]) / ((double)side * 0.5 * len);
     micro_slope(P.ck, pg, sw, a_gn);
     micro_slope(P.ck, pg, swt, a_gt);
-    Moments M;
-    calc_moment(P.ck, pg, M);
     {
+        Moments M;
+        calc_moment(P.ck, pg, M);
         double Mau[4], Mbv[4];
         moment_auvxi(a_gn, M.Mu, M.Mv, M.Mxi, 1, 0, Mau);
         moment_auvxi(a_gt, M.Mu, M.Mv, M.Mxi, 0, 1, Mbv);
 #pragma unroll
         for (int m = 0; m < 4; ++m) sw[m] = -pg.r * (Mau[m] + Mbv[m]);
         micro_slope(P.ck, pg, sw, a_T);
+        mxi2 = M.Mxi[2];
     }
-    // two face-equilibrium projections (H_g onto GetConserved(pg), H_w onto GetConserved(pshape))
+    // the two face-equilibrium projections: H_g onto GetConserved(pg), H_w onto GetConserved(pshape)
 #pragma unroll
     for (int m = 0; m < 28; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], wk = B.w[k];
+        const Slot s = slot(r, nv);
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
         const double vn = vk, vt = -uk;
-        moment_add(wk, vn, vt, Hg[r], Bg[r], acc);
-        gram_add(wk, fmax(fabs(Hg[r]), kEps * sgh), fmax(fabs(Bg[r]), kEps * sgb), vn, vt, acc + 4);
-        moment_add(wk, vn, vt, Hw[r], Bw[r], acc + 14);
-        gram_add(wk, fmax(fabs(Hw[r]), kEps * swh), fmax(fabs(Bw[r]), kEps * swb), vn, vt, acc + 18);
+        const double bg = Hg[r] * bfac, bw = Hw[r] * bfac;
+        moment_add(wk, vn, vt, Hg[r], bg, acc);
+        gram_add(wk, fmax(fabs(Hg[r]), kEps * sgh), fmax(fabs(bg), kEps * sgb), vn, vt, acc + 4);
+        moment_add(wk, vn, vt, Hw[r], bw, acc + 14);
+        gram_add(wk, fmax(fabs(Hw[r]), kEps * swh), fmax(fabs(bw), kEps * swb), vn, vt, acc + 18);
     }
     block_reduce<28, 0>(acc, red, rout);
-    double tg[4], tw[4], rhs[4], gm[16], lg[4], lw[4];
+    double tg[4], tw[4], lg[4], lw[4];
     const Prim pshape{1.0, pw.U, pw.V, pw.L};
     get_conserved(P.gm1, pg, tg);
     get_conserved(P.gm1, pshape, tw);
+    bool pok;
+    {
+        double rhs[4], gm[16];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) rhs[m] = tg[m] - acc[m];
-    gram_expand(acc + 4, gm);
-    bool pok = solve_dense4(gm, rhs, lg);
+        for (int m = 0; m < 4; ++m) rhs[m] = tg[m] - acc[m];
+        gram_expand(acc + 4, gm);
+        pok = solve_dense4(gm, rhs, lg);
 #pragma unroll
-    for (int m = 0; m < 4; ++m) rhs[m] = tw[m] - acc[14 + m];
-    gram_expand(acc + 18, gm);
-    pok = solve_dense4(gm, rhs, lw) && pok;
+        for (int m = 0; m < 4; ++m) rhs[m] = tw[m] - acc[14 + m];
+        gram_expand(acc + 18, gm);
+        pok = solve_dense4(gm, rhs, lw) && pok;
+    }
     if (!pok) { lg[0] = lg[1] = lg[2] = lg[3] = lw[0] = lw[1] = lw[2] = lw[3] = 0.0; }
     const double coeff = 0.8 * (1.0 - P.pr) * pg.L * pg.L / pg.r;
     const double c2ck = 2.0 / (double)P.ck;
+    double Bg[VPT], Bw[VPT];
 #pragma unroll
     for (int m = 0; m < 10; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], wk = B.w[k];
+        const Slot s = slot(r, nv);
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
         const double a = vk, t = -uk, e = 0.5 * (a * a + t * t);
+        const double bg = Hg[r] * bfac, bw = Hw[r] * bfac;
         Hg[r] = Hg[r] + fmax(fabs(Hg[r]), kEps * sgh) * (lg[0] + a * lg[1] + t * lg[2] + e * lg[3]);
-        Bg[r] = Bg[r] + 0.5 * fmax(fabs(Bg[r]), kEps * sgb) * lg[3];
+        Bg[r] = bg + 0.5 * fmax(fabs(bg), kEps * sgb) * lg[3];
         Hw[r] = Hw[r] + fmax(fabs(Hw[r]), kEps * swh) * (lw[0] + a * lw[1] + t * lw[2] + e * lw[3]);
-        Bw[r] = Bw[r] + 0.5 * fmax(fabs(Bw[r]), kEps * swb) * lw[3];
+        Bw[r] = bw + 0.5 * fmax(fabs(bw), kEps * swb) * lw[3];
         moment_add(wk, a, t, Hg[r], Bg[r], acc + 2);
         moment_add(wk, a, t, Hw[r], Bw[r], acc + 6);
         const double dk = (copysign(1.0, a) * rot + 1.0) / 2.0, ik = 1.0 - dk;
-        const double slh = a * shn[r] + t * sht[r];
+        const size_t q = (size_t)cell * nv + s.kk;
+        const double slh = a * B.syh[q] + t * (-B.sxh[q]);
         const double v2 = a * a + t * t;
         const double dvn = a - pg.U, dvt = t - pg.V, dv2 = dvn * dvn + dvt * dvt;
         const double Hp = coeff * (dvn * qf0 + dvt * qf1) * (2.0 * pg.L * dv2 - 4.0) * Hg[r];
@@ -362,10 +388,9 @@ __device__ void lo_face_wall(const LoParams& P, const LoBuffers& B, int side, in
         acc[0] += wk * a * ik * (Mt[0] * (Hg[r] + Hp) + Mt[1] * (a * Ha_gn + t * Ha_gt) + Mt[2] * Ha_T +
                                  Mt[3] * hv[r] - Mt[4] * slh);
         acc[1] += wk * a * Hw[r] * dk;
-        (void)c2ck;
     }
     block_reduce<10, 0>(acc, red, rout);
-    const double rhow = -acc[0] / (dt * acc[1]);   // prim_w(1) = -incidence/reflection
+    const double rhow = -acc[0] / (dt * acc[1]);   // prim_w(1) = -incidence/reflection (:2166)
     if (tid == 0) {
         const double rg = fmax(fmax(fmax(fabs(tg[0]), fabs(tg[1])), fmax(fabs(tg[2]), fabs(tg[3]))), 1.0);
         const double rw = fmax(fmax(fmax(fabs(tw[0]), fabs(tw[1])), fmax(fabs(tw[2]), fabs(tw[3]))), 1.0);
@@ -378,11 +403,12 @@ __device__ void lo_face_wall(const LoParams& P, const LoBuffers& B, int side, in
     for (int m = 0; m < 4; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], wk = B.w[k];
+        const Slot s = slot(r, nv);
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
         const double a = vk, t = -uk, v2 = a * a + t * t;
         const double dk = (copysign(1.0, a) * rot + 1.0) / 2.0, ik = 1.0 - dk;
+        const size_t q = (size_t)cell * nv + s.kk;
+        const double shn = B.syh[q], sbn = B.syb[q], sht = -B.sxh[q], sbt = -B.sxb[q];
         const double Hwk = rhow * Hw[r], Bwk = rhow * Bw[r];
         const double Hgk = Hg[r], Bgk = Bg[r];
         const double dvn = a - pg.U, dvt = t - pg.V, dv2 = dvn * dvn + dvt * dvt;
@@ -392,17 +418,16 @@ __device__ void lo_face_wall(const LoParams& P, const LoBuffers& B, int side, in
         const double Ha_gn = (a_gn[0] + a_gn[1] * a + a_gn[2] * t) * Hgk + 0.5 * a_gn[3] * (v2 * Hgk + Bgk);
         const double Ha_gt = (a_gt[0] + a_gt[1] * a + a_gt[2] * t) * Hgk + 0.5 * a_gt[3] * (v2 * Hgk + Bgk);
         const double Ha_T = (a_T[0] + a_T[1] * a + a_T[2] * t) * Hgk + 0.5 * a_T[3] * (v2 * Hgk + Bgk);
-        const double Ba_gn = (a_gn[0] + a_gn[1] * a + a_gn[2] * t) * Bgk + 0.5 * a_gn[3] * (v2 * Bgk + M.Mxi[2] * Hgk);
-        const double Ba_gt = (a_gt[0] + a_gt[1] * a + a_gt[2] * t) * Bgk + 0.5 * a_gt[3] * (v2 * Bgk + M.Mxi[2] * Hgk);
-        const double Ba_T = (a_T[0] + a_T[1] * a + a_T[2] * t) * Bgk + 0.5 * a_T[3] * (v2 * Bgk + M.Mxi[2] * Hgk);
+        const double Ba_gn = (a_gn[0] + a_gn[1] * a + a_gn[2] * t) * Bgk + 0.5 * a_gn[3] * (v2 * Bgk + mxi2 * Hgk);
+        const double Ba_gt = (a_gt[0] + a_gt[1] * a + a_gt[2] * t) * Bgk + 0.5 * a_gt[3] * (v2 * Bgk + mxi2 * Hgk);
+        const double Ba_T = (a_T[0] + a_T[1] * a + a_T[2] * t) * Bgk + 0.5 * a_T[3] * (v2 * Bgk + mxi2 * Hgk);
         const double fh = flen * (dt * a * Hwk * dk + Mt[0] * a * (Hgk + Hp) * ik + Mt[1] * a * a * Ha_gn * ik +
                                   Mt[1] * a * t * Ha_gt * ik + Mt[2] * a * Ha_T * ik + Mt[3] * a * hv[r] * ik -
-                                  Mt[4] * a * (a * shn[r] + t * sht[r]) * ik);
+                                  Mt[4] * a * (a * shn + t * sht) * ik);
         const double fb = flen * (dt * a * Bwk * dk + Mt[0] * a * (Bgk + Bp) * ik + Mt[1] * a * a * Ba_gn * ik +
                                   Mt[1] * a * t * Ba_gt * ik + Mt[2] * a * Ba_T * ik + Mt[3] * a * bv[r] * ik -
-                                  Mt[4] * a * (a * sbn[r] + t * sbt[r]) * ik);
-        Fh[k] = fh;
-        Fb[k] = fb;
+                                  Mt[4] * a * (a * sbn + t * sbt) * ik);
+        if (s.ok) { Fh[s.k] = fh; Fb[s.k] = fb; }
         const double hk = fh / flen, bk = fb / flen;
         acc[0] += wk * hk;
         acc[1] += wk * (a * hk);
@@ -414,7 +439,7 @@ __device__ void lo_face_wall(const LoParams& P, const LoBuffers& B, int side, in
         aero[0] = acc[1] / dt;
         aero[1] = acc[2] / dt;
         aero[2] = acc[3] / dt - pw.V * acc[2] / dt;
-        // GlobalFrame with cosx = -0, cosy = 1: [f1, -f3, f2, f4], then times the face length
+        // GlobalFrame with cosx = -0, cosy = 1: (f1, f2, f3, f4) -> (f1, -f3, f2, f4), times the face length
         Fw[0] = flen * acc[0];
         Fw[1] = flen * (-acc[2]);
         Fw[2] = flen * acc[1];
@@ -425,8 +450,8 @@ __device__ void lo_face_wall(const LoParams& P, const LoBuffers& B, int side, in
 }
 
 template <int VPT, int NTMAX>
-__global__ void __launch_bounds__(NTMAX) k_lo_faces(LoParams P, LoBuffers B) {
-    __shared__ double red[32 * kRedSlots];
+__global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_faces(LoParams P, LoBuffers B) {
+    __shared__ double red[16 * 64];
     __shared__ double rout[kRedSlots];
     const double dt = B.dt[0];
     const int nx = P.nx, ny = P.ny, nv = P.nvel;
@@ -434,19 +459,24 @@ __global__ void __launch_bounds__(NTMAX) k_lo_faces(LoParams P, LoBuffers B) {
     if (f < nx * ny) {
         const int j = f / nx, i = f % nx;
         const size_t o = (size_t)(j * nx + i);
-        lo_face_interior<VPT>(P, B, 0, wrapx(i - 1, nx), j, i, j, dt, B.fxh + o * nv, B.fxb + o * nv, B.fxw + o * 4,
-                              red, rout);
+        lo_face_interior<VPT>(P, B, 0, j * nx + wrapx(i - 1, nx), j * nx + i, dt, B.fxh + o * nv, B.fxb + o * nv,
+                              B.fxw + o * 4, red, rout);
         return;
     }
     f -= nx * ny;
-    if (f < nx * (ny - 1)) {
-        const int jf = 1 + f / nx, i = f % nx;
-        const size_t o = (size_t)(jf * nx + i);
-        lo_face_interior<VPT>(P, B, 1, i, jf - 1, i, jf, dt, B.fyh + o * nv, B.fyb + o * nv, B.fyw + o * 4, red,
-                              rout);
-        return;
-    }
-    f -= nx * (ny - 1);
+    const int jf = 1 + f / nx, i = f % nx;
+    const size_t o = (size_t)(jf * nx + i);
+    lo_face_interior<VPT>(P, B, 1, (jf - 1) * nx + i, jf * nx + i, dt, B.fyh + o * nv, B.fyb + o * nv, B.fyw + o * 4,
+                          red, rout);
+}
+
+template <int VPT, int NTMAX>
+__global__ void __launch_bounds__(NTMAX) k_lo_walls(LoParams P, LoBuffers B) {
+    __shared__ double red[16 * 64];
+    __shared__ double rout[kRedSlots];
+    const double dt = B.dt[0];
+    const int nx = P.nx, ny = P.ny, nv = P.nvel;
+    const int f = blockIdx.x;
     const int side = f < nx ? -1 : 1, i = f % nx;
     const size_t o = (size_t)((side < 0 ? 0 : ny) * nx + i);
     lo_face_wall<VPT>(P, B, side, i, dt, B.fyh + o * nv, B.fyb + o * nv, B.fyw + o * 4,
@@ -476,40 +506,34 @@ __device__ void last_cta_epilogue(const LoParams& P, const LoBuffers& B, bool wr
     if (!s_last) return;
     __threadfence();
     const int nc = P.nx * P.ny;
-    double acc[kNDiag + 1];
+    double acc[14];
 #pragma unroll
-    for (int m = 0; m < kNDiag; ++m) acc[m] = 0.0;
-    acc[kNDiag] = -INFINITY;   // max of -dt_local == -min(dt_local)
+    for (int m = 0; m < 13; ++m) acc[m] = 0.0;
+    acc[13] = -INFINITY;   // max of -dt_local == -min(dt_local)
     for (int c = threadIdx.x; c < nc; c += blockDim.x) {
-        if (write_dt) acc[kNDiag] = fmax(acc[kNDiag], -__ldcg(B.dtl + c));
+        if (write_dt) acc[13] = fmax(acc[13], -__ldcg(B.dtl + c));
         if (write_diag) {
 #pragma unroll
             for (int m = 0; m < 9; ++m) acc[m] += __ldcg(B.cell_diag + (size_t)c * kNDiag + m);
+#pragma unroll
+            for (int m = 0; m < 4; ++m) acc[9 + m] = fmax(acc[9 + m], __ldcg(B.cell_diag + (size_t)c * kNDiag + 9 + m));
         }
     }
-    // maxima (res_max) are reduced as sums of nothing here; do them separately below
-    block_reduce<9, 0>(acc, red, rout);
-    double mx[5];
-    for (int m = 0; m < 4; ++m) mx[m] = 0.0;
-    mx[4] = acc[kNDiag];
-    for (int c = threadIdx.x; c < nc && write_diag; c += blockDim.x)
-        for (int m = 0; m < 4; ++m) mx[m] = fmax(mx[m], __ldcg(B.cell_diag + (size_t)c * kNDiag + 9 + m));
-    block_reduce<0, 5>(mx, red, rout);
+    block_reduce<9, 5>(acc, red, rout);
     if (threadIdx.x == 0) {
         if (write_diag) {
-            for (int m = 0; m < 9; ++m) B.diag[m] = acc[m];
-            for (int m = 0; m < 4; ++m) B.diag[9 + m] = mx[m];
+            for (int m = 0; m < 13; ++m) B.diag[m] = acc[m];
         }
         if (write_dt) {
             B.dt[1] = B.dt[0];   // dt_global of the step that just completed
-            B.dt[0] = P.fixed_dt > 0.0 ? P.fixed_dt : -mx[4];
+            B.dt[0] = P.fixed_dt > 0.0 ? P.fixed_dt : -acc[13];
         }
         *B.counter = 0u;
     }
 }
 
 __global__ void __launch_bounds__(256) k_lo_timestep(LoParams P, LoBuffers B) {
-    __shared__ double red[32 * kRedSlots];
+    __shared__ double red[8 * 64];
     __shared__ double rout[kRedSlots];
     const int nc = P.nx * P.ny;
     for (int c = blockIdx.x * blockDim.x + threadIdx.x; c < nc; c += gridDim.x * blockDim.x) {
@@ -528,10 +552,10 @@ __global__ void __launch_bounds__(256) k_lo_timestep(LoParams P, LoBuffers B) {
 enum { MODE_RESIDUAL = 1, MODE_UPDATE = 2, MODE_FUSED = 3 };
 
 template <int VPT, int NTMAX, int MODE, bool COLLISION>
-__global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
-    __shared__ double red[32 * kRedSlots];
+__global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
+    __shared__ double red[16 * 64];
     __shared__ double rout[kRedSlots];
-    const int nv = P.nvel, tid = threadIdx.x, NT = blockDim.x, nx = P.nx;
+    const int nv = P.nvel, tid = threadIdx.x, nx = P.nx;
     const int c = blockIdx.x, i = c % nx, j = c / nx;
     const double dt = B.dt[0];
     const double* hc = B.h + (size_t)c * nv;
@@ -541,12 +565,12 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
 #pragma unroll
     for (int m = 0; m < 4; ++m) Wold[m] = B.W[c * 4 + m];
     double resw[4];
-    double acc[40];
+    double acc[28];
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        h[r] = b[r] = rh[r] = rb[r] = 0.0;
-        if (k < nv) { h[r] = hc[k]; b[r] = bc[k]; }
+        const Slot s = slot(r, nv);
+        h[r] = hc[s.kk];
+        b[r] = bc[s.kk];
     }
     if (MODE & MODE_RESIDUAL) {
         // AssembleMacroResidual / AssembleMicroFluxResidual (mod_Residual.f90:30-76)
@@ -561,19 +585,20 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
         for (int m = 0; m < 6; ++m) acc[m] = 0.0;
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
-            const int k = tid + r * NT;
-            if (k >= nv) continue;
+            const Slot s = slot(r, nv);
+            const int k = s.kk;
+            const double wk = s.ok ? B.w[k] : 0.0;
             const double sh = (B.fxh[fl * nv + k] - B.fxh[fr * nv + k] + B.fyh[gl * nv + k] - B.fyh[gr * nv + k]) * area_inv;
             const double sb = (B.fxb[fl * nv + k] - B.fxb[fr * nv + k] + B.fyb[gl * nv + k] - B.fyb[gr * nv + k]) * area_inv;
             rh[r] = sh * dti;   // stream_h
             rb[r] = sb * dti;
-            moment_add(B.w[k], B.u[k], B.v[k], rh[r], rb[r], acc);
-            acc[4] = fmax(acc[4], fabs(h[r]));
-            acc[5] = fmax(acc[5], fabs(b[r]));
+            moment_add(wk, B.u[k], B.v[k], rh[r], rb[r], acc);
+            acc[4] = fmax(acc[4], s.ok ? fabs(h[r]) : 0.0);
+            acc[5] = fmax(acc[5], s.ok ? fabs(b[r]) : 0.0);
         }
         block_reduce<4, 2>(acc, red, rout);
         // EnforceStreamingMomentCompatibility (mod_ImplicitMicro.f90:293-306): stream onto rate_w
-        double rate[4], rhs[4], gm[16], lam[4];
+        double rate[4], rhs[4], lam[4];
 #pragma unroll
         for (int m = 0; m < 4; ++m) { rate[m] = resw[m] * dti; rhs[m] = rate[m] - acc[m]; }
         const double sh_ = fmax(acc[4], 1.0), sb_ = fmax(acc[5], 1.0);
@@ -581,25 +606,28 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
         for (int m = 0; m < 10; ++m) acc[m] = 0.0;
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
-            const int k = tid + r * NT;
-            if (k >= nv) continue;
-            gram_add(B.w[k], fmax(fabs(h[r]), kEps * sh_), fmax(fabs(b[r]), kEps * sb_), B.u[k], B.v[k], acc);
+            const Slot s = slot(r, nv);
+            const double wk = s.ok ? B.w[s.kk] : 0.0;
+            gram_add(wk, fmax(fabs(h[r]), kEps * sh_), fmax(fabs(b[r]), kEps * sb_), B.u[s.kk], B.v[s.kk], acc);
         }
         block_reduce<10, 0>(acc, red, rout);
-        gram_expand(acc, gm);
-        bool pok = solve_dense4(gm, rhs, lam);
+        bool pok;
+        {
+            double gm[16];
+            gram_expand(acc, gm);
+            pok = solve_dense4(gm, rhs, lam);
+        }
         if (!pok) lam[0] = lam[1] = lam[2] = lam[3] = 0.0;
 #pragma unroll
         for (int m = 0; m < 4; ++m) acc[m] = 0.0;
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
-            const int k = tid + r * NT;
-            if (k >= nv) continue;
-            const double uk = B.u[k], vk = B.v[k];
+            const Slot s = slot(r, nv);
+            const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
             const double e = 0.5 * (uk * uk + vk * vk);
             rh[r] = rh[r] + fmax(fabs(h[r]), kEps * sh_) * (lam[0] + uk * lam[1] + vk * lam[2] + e * lam[3]);
             rb[r] = rb[r] + 0.5 * fmax(fabs(b[r]), kEps * sb_) * lam[3];
-            moment_add(B.w[k], uk, vk, rh[r], rb[r], acc);
+            moment_add(wk, uk, vk, rh[r], rb[r], acc);
             rh[r] = rh[r] * dt;   // res_h_flux_store = stream_h * dt (mod_Residual.f90:114-115)
             rb[r] = rb[r] * dt;
         }
@@ -614,10 +642,10 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
         if (MODE == MODE_RESIDUAL) {
 #pragma unroll
             for (int r = 0; r < VPT; ++r) {
-                const int k = tid + r * NT;
-                if (k >= nv) continue;
-                B.res_h[(size_t)c * nv + k] = rh[r];
-                B.res_b[(size_t)c * nv + k] = rb[r];
+                const Slot s = slot(r, nv);
+                if (!s.ok) continue;
+                B.res_h[(size_t)c * nv + s.k] = rh[r];
+                B.res_b[(size_t)c * nv + s.k] = rb[r];
             }
             if (tid < 4) B.res_w[c * 4 + tid] = resw[tid];
         }
@@ -626,8 +654,9 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
         for (int m = 0; m < 4; ++m) resw[m] = B.res_w[c * 4 + m];
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
-            const int k = tid + r * NT;
-            if (k < nv) { rh[r] = B.res_h[(size_t)c * nv + k]; rb[r] = B.res_b[(size_t)c * nv + k]; }
+            const Slot s = slot(r, nv);
+            rh[r] = B.res_h[(size_t)c * nv + s.kk];
+            rb[r] = B.res_b[(size_t)c * nv + s.kk];
         }
     }
 
@@ -643,11 +672,11 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
         acc[0] = acc[1] = 0.0;
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
-            const int k = tid + r * NT;
-            if (k >= nv) continue;
-            const double dvn = B.u[k] - p.U, dvt = B.v[k] - p.V, v2 = dvn * dvn + dvt * dvt;
-            acc[0] += 0.5 * B.w[k] * dvn * (v2 * h[r] + b[r]);
-            acc[1] += 0.5 * B.w[k] * dvt * (v2 * h[r] + b[r]);
+            const Slot s = slot(r, nv);
+            const double wk = s.ok ? B.w[s.kk] : 0.0;
+            const double dvn = B.u[s.kk] - p.U, dvt = B.v[s.kk] - p.V, v2 = dvn * dvn + dvt * dvt;
+            acc[0] += 0.5 * wk * dvn * (v2 * h[r] + b[r]);
+            acc[1] += 0.5 * wk * dvt * (v2 * h[r] + b[r]);
         }
         block_reduce<2, 0>(acc, red, rout);
         const double q0 = acc[0], q1 = acc[1];
@@ -657,16 +686,14 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
         acc[0] = acc[1] = 0.0;
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
-            const int k = tid + r * NT;
-            E[r] = F[r] = 0.0;
-            if (k >= nv) continue;
-            const double dvn = B.u[k] - p.U, dvt = B.v[k] - p.V, v2 = dvn * dvn + dvt * dvt;
+            const Slot s = slot(r, nv);
+            const double dvn = B.u[s.kk] - p.U, dvt = B.v[s.kk] - p.V, v2 = dvn * dvn + dvt * dvt;
             const double H = pref * exp(-p.L * v2), Bm = H * bfac;
             const double qd = dvn * q0 + dvt * q1, sH = 2.0 * p.L * v2 - 4.0;
             E[r] = H + coeff * qd * sH * H;
             F[r] = Bm + coeff * qd * (sH + c2ck) * Bm;
-            acc[0] = fmax(acc[0], fabs(E[r]));
-            acc[1] = fmax(acc[1], fabs(F[r]));
+            acc[0] = fmax(acc[0], s.ok ? fabs(E[r]) : 0.0);
+            acc[1] = fmax(acc[1], s.ok ? fabs(F[r]) : 0.0);
         }
         block_reduce<0, 2>(acc, red, rout);
         const double se = fmax(acc[0], 1.0), sf = fmax(acc[1], 1.0);
@@ -674,32 +701,37 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
         for (int m = 0; m < 14; ++m) acc[m] = 0.0;
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
-            const int k = tid + r * NT;
-            if (k >= nv) continue;
-            moment_add(B.w[k], B.u[k], B.v[k], E[r], F[r], acc);
-            gram_add(B.w[k], fmax(fabs(E[r]), kEps * se), fmax(fabs(F[r]), kEps * sf), B.u[k], B.v[k], acc + 4);
+            const Slot s = slot(r, nv);
+            const double wk = s.ok ? B.w[s.kk] : 0.0;
+            moment_add(wk, B.u[s.kk], B.v[s.kk], E[r], F[r], acc);
+            gram_add(wk, fmax(fabs(E[r]), kEps * se), fmax(fabs(F[r]), kEps * sf), B.u[s.kk], B.v[s.kk], acc + 4);
         }
         block_reduce<14, 0>(acc, red, rout);
-        double rhs[4], gm[16], lam[4];
+        double lam[4];
+        bool pok;
+        {
+            double rhs[4], gm[16];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) rhs[m] = Wold[m] - acc[m];
-        gram_expand(acc + 4, gm);
-        const bool pok = solve_dense4(gm, rhs, lam);
+            for (int m = 0; m < 4; ++m) rhs[m] = Wold[m] - acc[m];
+            gram_expand(acc + 4, gm);
+            pok = solve_dense4(gm, rhs, lam);
+        }
         if (!pok) lam[0] = lam[1] = lam[2] = lam[3] = 0.0;
 #pragma unroll
         for (int m = 0; m < 4; ++m) acc[m] = 0.0;
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
-            const int k = tid + r * NT;
-            if (k >= nv) continue;
-            const double uk = B.u[k], vk = B.v[k], e = 0.5 * (uk * uk + vk * vk);
+            const Slot s = slot(r, nv);
+            const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0, e = 0.5 * (uk * uk + vk * vk);
             const double Ep = E[r] + fmax(fabs(E[r]), kEps * se) * (lam[0] + uk * lam[1] + vk * lam[2] + e * lam[3]);
             const double Fp = F[r] + 0.5 * fmax(fabs(F[r]), kEps * sf) * lam[3];
-            moment_add(B.w[k], uk, vk, Ep, Fp, acc);
-            B.peq_h[(size_t)c * nv + k] = Ep;
-            B.peq_b[(size_t)c * nv + k] = Fp;
-            B.pcol_h[(size_t)c * nv + k] = (Ep - h[r]) / tau;
-            B.pcol_b[(size_t)c * nv + k] = (Fp - b[r]) / tau;
+            moment_add(wk, uk, vk, Ep, Fp, acc);
+            if (s.ok) {
+                B.peq_h[(size_t)c * nv + s.k] = Ep;
+                B.peq_b[(size_t)c * nv + s.k] = Fp;
+                B.pcol_h[(size_t)c * nv + s.k] = (Ep - h[r]) / tau;
+                B.pcol_b[(size_t)c * nv + s.k] = (Fp - b[r]) / tau;
+            }
         }
         block_reduce<4, 0>(acc, red, rout);
         if (tid == 0) {
@@ -728,11 +760,12 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
     acc[0] = acc[1] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        if (k >= nv) continue;
-        const double dvn = B.u[k] - po.U, dvt = B.v[k] - po.V, v2 = dvn * dvn + dvt * dvt;
-        acc[0] += 0.5 * B.w[k] * dvn * (v2 * h[r] + b[r]);
-        acc[1] += 0.5 * B.w[k] * dvt * (v2 * h[r] + b[r]);
+        const Slot s = slot(r, nv);
+        const double wk = s.ok ? B.w[s.kk] : 0.0;
+        const double dvn = B.u[s.kk] - po.U, dvt = B.v[s.kk] - po.V, v2 = dvn * dvn + dvt * dvt;
+        const double t = 0.5 * wk * (v2 * h[r] + b[r]);
+        acc[0] += t * dvn;
+        acc[1] += t * dvt;
     }
     block_reduce<2, 0>(acc, red, rout);
     const double q0 = acc[0], q1 = acc[1];
@@ -746,10 +779,8 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
         for (int m = 0; m < 4; ++m) acc[m] = 0.0;
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
-            const int k = tid + r * NT;
-            Ho[r] = Bo[r] = Hn[r] = Bn[r] = 0.0;
-            if (k >= nv) continue;
-            const double uk = B.u[k], vk = B.v[k];
+            const Slot s = slot(r, nv);
+            const double uk = B.u[s.kk], vk = B.v[s.kk];
             double dvn = uk - po.U, dvt = vk - po.V, v2 = dvn * dvn + dvt * dvt;
             double H = pro * exp(-po.L * v2), Bm = H * bfo, qd = dvn * q0 + dvt * q1, sH = 2.0 * po.L * v2 - 4.0;
             Ho[r] = H + co * qd * sH * H;
@@ -758,10 +789,10 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
             H = prn * exp(-pn.L * v2); Bm = H * bfn; qd = dvn * q0 + dvt * q1; sH = 2.0 * pn.L * v2 - 4.0;
             Hn[r] = H + cn * qd * sH * H;
             Bn[r] = Bm + cn * qd * (sH + c2ck) * Bm;
-            acc[0] = fmax(acc[0], fabs(Ho[r]));
-            acc[1] = fmax(acc[1], fabs(Bo[r]));
-            acc[2] = fmax(acc[2], fabs(Hn[r]));
-            acc[3] = fmax(acc[3], fabs(Bn[r]));
+            acc[0] = fmax(acc[0], s.ok ? fabs(Ho[r]) : 0.0);
+            acc[1] = fmax(acc[1], s.ok ? fabs(Bo[r]) : 0.0);
+            acc[2] = fmax(acc[2], s.ok ? fabs(Hn[r]) : 0.0);
+            acc[3] = fmax(acc[3], s.ok ? fabs(Bn[r]) : 0.0);
         }
         block_reduce<0, 4>(acc, red, rout);
     }
@@ -770,34 +801,36 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
     for (int m = 0; m < 28; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], wk = B.w[k];
+        const Slot s = slot(r, nv);
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
         moment_add(wk, uk, vk, Ho[r], Bo[r], acc);
         gram_add(wk, fmax(fabs(Ho[r]), kEps * sHo), fmax(fabs(Bo[r]), kEps * sBo), uk, vk, acc + 4);
         moment_add(wk, uk, vk, Hn[r], Bn[r], acc + 14);
         gram_add(wk, fmax(fabs(Hn[r]), kEps * sHn), fmax(fabs(Bn[r]), kEps * sBn), uk, vk, acc + 18);
     }
     block_reduce<28, 0>(acc, red, rout);
-    double to4[4], rhs[4], gm[16], lo[4], ln[4];
+    double to4[4], lo[4], ln[4];
     get_conserved(P.gm1, po, to4);
+    bool pok;
+    {
+        double rhs[4], gm[16];
 #pragma unroll
-    for (int m = 0; m < 4; ++m) rhs[m] = to4[m] - acc[m];
-    gram_expand(acc + 4, gm);
-    bool pok = solve_dense4(gm, rhs, lo);
+        for (int m = 0; m < 4; ++m) rhs[m] = to4[m] - acc[m];
+        gram_expand(acc + 4, gm);
+        pok = solve_dense4(gm, rhs, lo);
 #pragma unroll
-    for (int m = 0; m < 4; ++m) rhs[m] = Wn[m] - acc[14 + m];
-    gram_expand(acc + 18, gm);
-    pok = solve_dense4(gm, rhs, ln) && pok;
+        for (int m = 0; m < 4; ++m) rhs[m] = Wn[m] - acc[14 + m];
+        gram_expand(acc + 18, gm);
+        pok = solve_dense4(gm, rhs, ln) && pok;
+    }
     if (!pok) lo[0] = lo[1] = lo[2] = lo[3] = ln[0] = ln[1] = ln[2] = ln[3] = 0.0;
     const double inv = 1.0 / (1.0 + 0.5 * dt / tn);
 #pragma unroll
     for (int m = 0; m < 8; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], wk = B.w[k], e = 0.5 * (uk * uk + vk * vk);
+        const Slot s = slot(r, nv);
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0, e = 0.5 * (uk * uk + vk * vk);
         const double Hop = Ho[r] + fmax(fabs(Ho[r]), kEps * sHo) * (lo[0] + uk * lo[1] + vk * lo[2] + e * lo[3]);
         const double Bop = Bo[r] + 0.5 * fmax(fabs(Bo[r]), kEps * sBo) * lo[3];
         const double Hnp = Hn[r] + fmax(fabs(Hn[r]), kEps * sHn) * (ln[0] + uk * ln[1] + vk * ln[2] + e * ln[3]);
@@ -806,8 +839,10 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
         moment_add(wk, uk, vk, Hnp, Bnp, acc + 4);
         const double hnew = (h[r] + rh[r] + 0.5 * dt * (Hnp / tn + (Hop - h[r]) / to)) * inv;
         const double bnew = (b[r] + rb[r] + 0.5 * dt * (Bnp / tn + (Bop - b[r]) / to)) * inv;
-        B.h[(size_t)c * nv + k] = hnew;
-        B.b[(size_t)c * nv + k] = bnew;
+        if (s.ok) {
+            B.h[(size_t)c * nv + s.k] = hnew;
+            B.b[(size_t)c * nv + s.k] = bnew;
+        }
     }
     block_reduce<8, 0>(acc, red, rout);
     if (tid == 0) {
@@ -839,10 +874,10 @@ __global__ void __launch_bounds__(NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
 // EnforceAcceptedMomentCompatibility (mod_ImplicitMicro.f90, via InitializeSteadyImplicit).
 template <int VPT, int NTMAX>
 __global__ void __launch_bounds__(NTMAX) k_lo_init(LoParams P, LoBuffers B, double rho, double U, double V,
-                                                         double tn) {
-    __shared__ double red[32 * kRedSlots];
+                                                   double tn) {
+    __shared__ double red[16 * 64];
     __shared__ double rout[kRedSlots];
-    const int nv = P.nvel, tid = threadIdx.x, NT = blockDim.x, c = blockIdx.x;
+    const int nv = P.nvel, tid = threadIdx.x, c = blockIdx.x;
     const Prim p{rho, U, V, 1.0 / tn};
     double W[4];
     get_conserved(P.gm1, p, W);
@@ -851,14 +886,12 @@ __global__ void __launch_bounds__(NTMAX) k_lo_init(LoParams P, LoBuffers B, doub
     acc[0] = acc[1] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        H[r] = Bm[r] = 0.0;
-        if (k >= nv) continue;
-        const double dvn = B.u[k] - p.U, dvt = B.v[k] - p.V;
+        const Slot s = slot(r, nv);
+        const double dvn = B.u[s.kk] - p.U, dvt = B.v[s.kk] - p.V;
         H[r] = pref * exp(-p.L * (dvn * dvn + dvt * dvt));
         Bm[r] = H[r] * bfac;
-        acc[0] = fmax(acc[0], fabs(H[r]));
-        acc[1] = fmax(acc[1], fabs(Bm[r]));
+        acc[0] = fmax(acc[0], s.ok ? fabs(H[r]) : 0.0);
+        acc[1] = fmax(acc[1], s.ok ? fabs(Bm[r]) : 0.0);
     }
     block_reduce<0, 2>(acc, red, rout);
     const double sh = fmax(acc[0], 1.0), sb = fmax(acc[1], 1.0);
@@ -866,10 +899,10 @@ __global__ void __launch_bounds__(NTMAX) k_lo_init(LoParams P, LoBuffers B, doub
     for (int m = 0; m < 14; ++m) acc[m] = 0.0;
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        if (k >= nv) continue;
-        moment_add(B.w[k], B.u[k], B.v[k], H[r], Bm[r], acc);
-        gram_add(B.w[k], fmax(fabs(H[r]), kEps * sh), fmax(fabs(Bm[r]), kEps * sb), B.u[k], B.v[k], acc + 4);
+        const Slot s = slot(r, nv);
+        const double wk = s.ok ? B.w[s.kk] : 0.0;
+        moment_add(wk, B.u[s.kk], B.v[s.kk], H[r], Bm[r], acc);
+        gram_add(wk, fmax(fabs(H[r]), kEps * sh), fmax(fabs(Bm[r]), kEps * sb), B.u[s.kk], B.v[s.kk], acc + 4);
     }
     block_reduce<14, 0>(acc, red, rout);
     double rhs[4], gm[16], lam[4];
@@ -882,15 +915,16 @@ __global__ void __launch_bounds__(NTMAX) k_lo_init(LoParams P, LoBuffers B, doub
     }
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
-        const int k = tid + r * NT;
-        if (k >= nv) continue;
-        const double uk = B.u[k], vk = B.v[k], e = 0.5 * (uk * uk + vk * vk);
-        B.h[(size_t)c * nv + k] = H[r] + fmax(fabs(H[r]), kEps * sh) * (lam[0] + uk * lam[1] + vk * lam[2] + e * lam[3]);
-        B.b[(size_t)c * nv + k] = Bm[r] + 0.5 * fmax(fabs(Bm[r]), kEps * sb) * lam[3];
+        const Slot s = slot(r, nv);
+        if (!s.ok) continue;
+        const double uk = B.u[s.k], vk = B.v[s.k], e = 0.5 * (uk * uk + vk * vk);
+        B.h[(size_t)c * nv + s.k] = H[r] + fmax(fabs(H[r]), kEps * sh) * (lam[0] + uk * lam[1] + vk * lam[2] + e * lam[3]);
+        B.b[(size_t)c * nv + s.k] = Bm[r] + 0.5 * fmax(fabs(Bm[r]), kEps * sb) * lam[3];
     }
     if (tid < 4) B.W[c * 4 + tid] = W[tid];
 }
 
+// -------------------------------------------------------------------------------------------
 // Host-visible launchers (used by ugks_capi.cu).  Tile = (velocities per thread, threads):
 // nvel <= 1024 -> (4, <=256 threads); nvel <= 2560 -> (5, <=512 threads).
 int lo_vpt(int nvel) { return nvel <= 4 * 256 ? 4 : 5; }
@@ -902,11 +936,24 @@ int lo_threads(int nvel) {
     return t < 32 ? 32 : t;
 }
 
+cudaError_t launch_lo_slopes(const LoParams& P, const LoBuffers& B, cudaStream_t s) {
+    const size_t n = (size_t)P.nx * P.ny * P.nvel;
+    k_lo_slopes<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, B);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_lo_faces(const LoParams& P, const LoBuffers& B, cudaStream_t s) {
-    const int nface = P.nx * P.ny + P.nx * (P.ny - 1) + 2 * P.nx;
+    const int nface = P.nx * P.ny + P.nx * (P.ny - 1);
     const int nt = lo_threads(P.nvel);
     if (lo_vpt(P.nvel) == 4) k_lo_faces<4, 256><<<nface, nt, 0, s>>>(P, B);
     else k_lo_faces<5, 512><<<nface, nt, 0, s>>>(P, B);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_lo_walls(const LoParams& P, const LoBuffers& B, cudaStream_t s) {
+    const int nt = lo_threads(P.nvel);
+    if (lo_vpt(P.nvel) == 4) k_lo_walls<4, 256><<<2 * P.nx, nt, 0, s>>>(P, B);
+    else k_lo_walls<5, 512><<<2 * P.nx, nt, 0, s>>>(P, B);
     return cudaGetLastError();
 }
 

@@ -15,6 +15,7 @@ struct LoParams {
     double wall_ux[2];       // bottom, top wall speed (WallUx(3:4))
     double wall_lam[2];      // 1/Tw per wall
     double fixed_dt;         // > 0: Time_global_fixed
+    double inv_dx, inv_dy;   // 1/dx, 1/dy for the slope stencils
 };
 
 struct LoBuffers {
@@ -24,6 +25,10 @@ struct LoBuffers {
     double* h;               // [nc][nvel] state, cell c = j*nx + i
     double* b;
     double* W;               // [nc][4] conservative variables
+    double* sxh;             // [nc][nvel] Van-Leer slopes of h, b in x and y (Interpolation)
+    double* syh;
+    double* sxb;
+    double* syb;
     double* fxh;             // [ny][nx][nvel] x-face micro flux (face i is between cells i-1 and i)
     double* fxb;
     double* fxw;             // [ny][nx][4] x-face macro flux

@@ -1,0 +1,58 @@
+"""Command-line driver for the Couette case (the role of the reference's run.sh + Solve_UGKS loop).
+
+    python -m ugks2d_high_order_b200.driver --method Explicit --steps 200 [--cfl 0.5 --omega 0.81]
+
+Runs the case on cuda:0 and prints the residual line every --show steps, as Write_residuals does
+(src/mod_Solve.f90:427-461).  Also the small, self-contained command used for ncu captures.
+"""
+import argparse
+import time
+
+from .case import CouetteCase, load_velocity_half32, reference_case
+from .solver import Solver
+
+
+def main(argv=None):
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--method", default="Explicit", choices=["Explicit", "ImplicitSteady"])
+    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--show", type=int, default=100)
+    ap.add_argument("--cfl", type=float, default=None)
+    ap.add_argument("--omega", type=float, default=None)
+    ap.add_argument("--ny", type=int, default=None)
+    ap.add_argument("--nx", type=int, default=None)
+    a = ap.parse_args(argv)
+    case = reference_case(a.method)
+    kw = {}
+    if a.cfl is not None:
+        kw["cfl"] = a.cfl
+    if a.omega is not None:
+        kw["omega"] = a.omega
+    if a.ny is not None:
+        kw["ny"] = a.ny
+        kw["dy"] = 1.0 / a.ny
+    if a.nx is not None:
+        kw["nx"] = a.nx
+        kw["dx"] = 1.0 / a.nx
+    case = case.with_(**kw) if kw else case
+    s = Solver(case, *load_velocity_half32())
+    s.init_freestream()
+    t0 = time.perf_counter()
+    done = 0
+    while done < a.steps:
+        n = min(a.show, a.steps - done)
+        if a.method == "Explicit":
+            dt, res = s.step_explicit(n)
+            done += n
+            print(f"iter={done:8d} dt={dt:.7e} res={' '.join(f'{r:.7e}' for r in res)}", flush=True)
+        else:
+            out = s.step_implicit(n)
+            done += n
+            print(f"iter={done:8d} {out}", flush=True)
+    el = time.perf_counter() - t0
+    print(f"{a.steps} steps in {el:.3f} s ({case.nx * case.ny * s.nvel * a.steps / el:.3e} cell-vel updates/s)")
+    s.close()
+
+
+if __name__ == "__main__":
+    main()
