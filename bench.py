@@ -46,54 +46,93 @@ def peaks():
 
 
 class ClockSampler:
-    """nvidia-smi clocks / throttle reasons sampled during the timed region."""
+    """SM clocks and clock-event (throttle) reasons sampled during the timed region.
 
-    def __init__(self, index):
-        self.index = index
+    NVML (the library nvidia-smi is built on) is polled from a host thread every `period` s;
+    `nvidia-smi -lms` is the alternative (--sampler smi).  Reasons recorded: hw_slowdown,
+    hw_thermal_slowdown, sw_thermal_slowdown, sw_power_cap.
+    """
+
+    REASONS = {"hw_slowdown": 0x8, "sw_thermal_slowdown": 0x20, "hw_thermal_slowdown": 0x40, "sw_power_cap": 0x4}
+
+    def __init__(self, index, kind="nvml", period=0.2):
+        self.index, self.kind, self.period = index, kind, period
+        self.samples, self.reasons, self.smax = [], set(), None
+        self._stop = threading.Event()
         self.proc = None
         self.lines = []
 
     def start(self):
-        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        if self.kind == "none":
+            return
+        if self.kind == "smi":
+            q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+                 "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+                 "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+            try:
+                self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
+                                              "--format=csv,noheader,nounits", "-lms", str(int(self.period * 1000))],
+                                             stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+                self.t = threading.Thread(target=self._read_smi, daemon=True)
+                self.t.start()
+            except Exception:
+                self.proc = None
+            return
         try:
-            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.index}", f"--query-gpu={q}",
-                                          "--format=csv,noheader,nounits", "-lms", "200"],
-                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
-            self.t.start()
+            import pynvml
+            pynvml.nvmlInit()
+            self.nv = pynvml
+            self.h = pynvml.nvmlDeviceGetHandleByIndex(self.index)
+            self.smax = float(pynvml.nvmlDeviceGetMaxClockInfo(self.h, pynvml.NVML_CLOCK_SM))
         except Exception:
-            self.proc = None
+            self.nv = None
+            return
+        self.t = threading.Thread(target=self._poll_nvml, daemon=True)
+        self.t.start()
 
-    def _read(self):
-        for line in self.proc.stdout:
-            self.lines.append(line.strip())
+    def _poll_nvml(self):
+        nv = self.nv
+        while not self._stop.is_set():
+            try:
+                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                for name, bit in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+            except Exception:
+                pass
+            self._stop.wait(self.period)
 
-    def stop(self):
-        if not self.proc:
-            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
-        self.proc.terminate()
-        try:
-            self.proc.wait(timeout=5)
-        except Exception:
-            self.proc.kill()
-        sm, smax, reasons = [], None, set()
+    def _read_smi(self):
         names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            parts = [p.strip() for p in ln.split(",")]
+        for line in self.proc.stdout:
+            parts = [p.strip() for p in line.strip().split(",")]
             if len(parts) < 9:
                 continue
             try:
-                sm.append(float(parts[1]))
-                smax = float(parts[2])
+                self.samples.append(float(parts[1]))
+                self.smax = float(parts[2])
             except ValueError:
                 continue
             for n, v in zip(names, parts[5:9]):
                 if v.lower().startswith("active"):
-                    reasons.add(n)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": smax,
-                "reasons": sorted(reasons), "samples": len(sm)}
+                    self.reasons.add(n)
+
+    def stop(self):
+        if self.kind == "none":
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "sampler": "none"}
+        self._stop.set()
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+        elif getattr(self, "t", None):
+            self.t.join(timeout=2)
+        return {"sm_mhz": statistics.median(self.samples) if self.samples else None, "sm_max_mhz": self.smax,
+                "reasons": sorted(self.reasons), "samples": len(self.samples),
+                "sampler": "nvml" if self.kind == "nvml" else "nvidia-smi"}
 
 
 def dist_env():
@@ -117,7 +156,7 @@ def cpu_baseline(case, velocity, nsteps=20, threads=None):
     units = case.nx * case.ny * len(velocity[0]) * nsteps
     return {"value": units / el, "unit": UNIT, "cores": nthreads, "kind": "port",
             "sample": f"{nsteps} Explicit solver steps of the 8x64x1024 workload after 1 warm-up step "
-                      f"({el:.2f} s, C oracle -O2, {nthreads} OpenMP thread(s) over faces/cells)"}
+                      f"({el:.2f} s, C oracle -O2, {nthreads} pthread(s) over faces/cells)"}
 
 
 def run_reference_arm(args):
@@ -161,6 +200,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--sampler", default="nvml", choices=["nvml", "smi", "none"],
+                    help="clock sampler during the timed region")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -200,7 +241,7 @@ def main():
         s.step_explicit(SOLVER_STEPS)
     s.init_freestream()
     launches0 = s.launch_count
-    sampler = ClockSampler(local)
+    sampler = ClockSampler(local, args.sampler)
     sampler.start()
     barrier()
     ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
@@ -258,10 +299,12 @@ def main():
     s.step_explicit(20)
     s.profile(True)
     s.step_explicit(200)
-    tf, nf = s.profile_read("faces")
-    tc, ncl = s.profile_read("cells")
+    ktimes = {name: s.profile_read(short) for name, short in
+              (("k_lo_slopes", "slopes"), ("k_lo_faces", "faces"), ("k_lo_walls", "walls"), ("k_lo_cells", "cells"))}
     s.profile(False)
-    top, t_top, n_top = ("k_lo_faces", tf, nf) if tf >= tc else ("k_lo_cells", tc, ncl)
+    ktot = sum(t for t, _ in ktimes.values())
+    top = max(ktimes, key=lambda k: ktimes[k][0])
+    t_top, n_top = ktimes[top]
     avg_s = t_top / n_top * 1e-3
     peak, peak_kind = peaks()
     algo_bytes = BYTES_PER_UPDATE_EXPLICIT * nc * nv
@@ -269,7 +312,8 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": None, "kernel": top, "peak_source": peak_kind,
                 "kernel_avg_us": avg_s * 1e6,
-                "kernel_share": {"k_lo_faces": tf / (tf + tc), "k_lo_cells": tc / (tf + tc)},
+                "kernel_share": {k: t / ktot for k, (t, _) in ktimes.items()},
+                "kernel_avg_us_all": {k: 1e3 * t / max(n, 1) for k, (t, n) in ktimes.items()},
                 "algorithmic_bytes_per_launch": algo_bytes}
 
     cpu = None

@@ -148,7 +148,7 @@ class Oracle:
 
 
 def set_threads(n=None):
-    """Number of OpenMP threads the oracle uses (all host cores by default); returns the count."""
+    """Number of pthreads the oracle uses over faces and cells (all host cores by default)."""
     L = lib()
     if not hasattr(L, "uo_set_threads"):
         return 1

@@ -13,6 +13,9 @@
 #include <stdlib.h>
 #include <string.h>
 #include <float.h>
+#include <pthread.h>
+#include <stdatomic.h>
+#include <unistd.h>
 
 #define PI_D 3.14159265358979323846264338327950288
 static const double SMV = (double)FLT_MIN;   /* mod_Globaldata.f90:26 SMV = tiny(0.0_real32) */
@@ -32,9 +35,58 @@ struct uo_ctx {
     double *rate_w, *stream_h, *stream_b;
     double *peq_h, *peq_b, *pcol_h, *pcol_b;
     double *wall_aero;            /* [2][nx][3] */
-    /* scratch */
-    double *t[24];
+    double *cell_diag;            /* [nc][13] per-cell residual-norm terms, summed in cell order */
+    int *cell_err;                /* [nc] per-cell status */
+    /* scratch: 24 work vectors per OpenMP thread */
+    int nthr;
+    double **tt;
 };
+
+#define NSCR 24
+#define MAX_THREADS 256
+static int g_threads = 1;   /* threads used by par_for; set by uo_set_threads */
+
+static int host_cores(void) {
+    long n = sysconf(_SC_NPROCESSORS_ONLN);
+    return n < 1 ? 1 : (n > MAX_THREADS ? MAX_THREADS : (int)n);
+}
+
+int uo_set_threads(int n) {
+    g_threads = n > 0 ? (n > MAX_THREADS ? MAX_THREADS : n) : host_cores();
+    return g_threads;
+}
+
+/* Minimal parallel-for over independent items: each worker takes item indices from an atomic
+ * counter and passes its worker id (for per-thread scratch) to the body. */
+typedef void (*par_body)(void* arg, int item, int tid);
+typedef struct { par_body body; void* arg; int n, tid; atomic_int* next; } par_job;
+
+static void* par_worker(void* vp) {
+    par_job* j = (par_job*)vp;
+    for (;;) {
+        int i = atomic_fetch_add(j->next, 1);
+        if (i >= j->n) break;
+        j->body(j->arg, i, j->tid);
+    }
+    return NULL;
+}
+
+static void par_for(int n, par_body body, void* arg, int nthr) {
+    if (nthr <= 1 || n <= 1) {
+        for (int i = 0; i < n; ++i) body(arg, i, 0);
+        return;
+    }
+    if (nthr > n) nthr = n;
+    atomic_int next = 0;
+    pthread_t th[MAX_THREADS];
+    par_job jobs[MAX_THREADS];
+    for (int t = 0; t < nthr; ++t) { jobs[t].body = body; jobs[t].arg = arg; jobs[t].n = n; jobs[t].tid = t; jobs[t].next = &next; }
+    for (int t = 1; t < nthr; ++t) pthread_create(&th[t], NULL, par_worker, &jobs[t]);
+    par_worker(&jobs[0]);
+    for (int t = 1; t < nthr; ++t) pthread_join(th[t], NULL);
+}
+
+static double** scratch_t(uo_ctx* c, int tid) { return c->tt + (size_t)tid * NSCR; }
 
 /* ------------------------------------------------------------------ kinetic math library */
 
@@ -307,7 +359,11 @@ uo_ctx* uo_create(const uo_params* p, const double* u, const double* v, const do
     c->pcol_h = (double*)calloc(S, sizeof(double));
     c->pcol_b = (double*)calloc(S, sizeof(double));
     c->wall_aero = (double*)calloc((size_t)2 * nx * 3, sizeof(double));
-    for (int i = 0; i < 24; ++i) c->t[i] = (double*)calloc(nv, sizeof(double));
+    c->cell_diag = (double*)calloc((size_t)c->nc * 13, sizeof(double));
+    c->cell_err = (int*)calloc((size_t)c->nc, sizeof(int));
+    c->nthr = MAX_THREADS < host_cores() ? MAX_THREADS : host_cores();
+    c->tt = (double**)calloc((size_t)c->nthr * NSCR, sizeof(double*));
+    for (int i = 0; i < c->nthr * NSCR; ++i) c->tt[i] = (double*)calloc(nv, sizeof(double));
     return c;
 }
 
@@ -317,7 +373,10 @@ void uo_destroy(uo_ctx* c) {
                       c->fyRh, c->fyRb, c->fyLw, c->fyRw, c->res_w, c->res_h, c->res_b, c->rate_w, c->stream_h,
                       c->stream_b, c->peq_h, c->peq_b, c->pcol_h, c->pcol_b, c->wall_aero};
     for (size_t i = 0; i < sizeof(ptrs) / sizeof(ptrs[0]); ++i) free(ptrs[i]);
-    for (int i = 0; i < 24; ++i) free(c->t[i]);
+    for (int i = 0; i < c->nthr * NSCR; ++i) free(c->tt[i]);
+    free(c->tt);
+    free(c->cell_diag);
+    free(c->cell_err);
     free(c);
 }
 
@@ -355,7 +414,8 @@ int uo_init_freestream(uo_ctx* c, double rho, double U, double V, double tnative
     int nv = p->nvel;
     double prim[4] = {rho, U, V, 1.0 / tnative}, W[4];
     get_conserved(p, prim, W);
-    double *H = c->t[0], *B = c->t[1], *rh = c->t[2], *rb = c->t[3];
+    double** T = scratch_t(c, 0);
+    double *H = T[0], *B = T[1], *rh = T[2], *rb = T[3];
     maxwell(p, nv, c->u, c->v, prim, H, B);
     for (int cell = 0; cell < c->nc; ++cell) {
         memcpy(c->h + (size_t)cell * nv, H, sizeof(double) * nv);
@@ -452,15 +512,17 @@ static void global_frame(const double w[4], double cx, double cy, double o[4]) {
 /* CalcFlux_MultiDimension (mod_Evolution.f90:186-492) for an interior face.
  * dir 0: vertical face (normal x, cosx=1, cosy=-0); dir 1: horizontal face (cosx=-0, cosy=1).
  * Output: micro flux Fh,Fb (already times face length) and macro flux Fw (MomentConserved of it). */
-static int interior_face(uo_ctx* c, int dir, int cl, int cr, double dt, double* Fh, double* Fb, double Fw[4]) {
+static int interior_face(uo_ctx* c, int tid, int dir, int cl, int cr, double dt, double* Fh, double* Fb,
+                         double Fw[4]) {
     const uo_params* p = &c->p;
     int nv = p->nvel;
     double cx = dir == 0 ? 1.0 : -0.0, cy = dir == 0 ? -0.0 : 1.0;
     double flen = dir == 0 ? p->dy : p->dx;
     double len = dir == 0 ? p->dx : p->dy;   /* leftCell%length(idx) == rightCell%length(idx) */
-    double *vn = c->t[0], *vt = c->t[1], *dl = c->t[2], *hv = c->t[3], *bv = c->t[4], *shn = c->t[5], *sbn = c->t[6];
-    double *sht = c->t[7], *sbt = c->t[8], *H0 = c->t[9], *B0 = c->t[10], *Hp = c->t[11], *Bp = c->t[12];
-    double *rh = c->t[13], *rb = c->t[14];
+    double** T = scratch_t(c, tid);
+    double *vn = T[0], *vt = T[1], *dl = T[2], *hv = T[3], *bv = T[4], *shn = T[5], *sbn = T[6];
+    double *sht = T[7], *sbt = T[8], *H0 = T[9], *B0 = T[10], *Hp = T[11], *Bp = T[12];
+    double *rh = T[13], *rb = T[14];
     const double *hL = c->h + (size_t)cl * nv, *hR = c->h + (size_t)cr * nv;
     const double *bL = c->b + (size_t)cl * nv, *bR = c->b + (size_t)cr * nv;
     const double *shL = c->sh + (size_t)cl * 2 * nv, *shR = c->sh + (size_t)cr * 2 * nv;
@@ -559,15 +621,16 @@ static int interior_face(uo_ctx* c, int dir, int cl, int cr, double dt, double* 
 
 /* W2BMultiscaleFluxBoundary (mod_Evolution.f90:1888-2449) for the horizontal wall faces.
  * side = -1 (Lside, bottom wall, face below row 0) or +1 (Rside, top wall). */
-static int wall_face(uo_ctx* c, int side, int cell, int iw, double dt, double* Fh, double* Fb, double Fw[4],
+static int wall_face(uo_ctx* c, int tid, int side, int cell, int iw, double dt, double* Fh, double* Fb, double Fw[4],
                      double aero[3]) {
     const uo_params* p = &c->p;
     int nv = p->nvel;
     double cx = -0.0, cy = 1.0, flen = p->dx, len = p->dy;
     double rot = -(double)side;
-    double *vn = c->t[0], *vt = c->t[1], *dl = c->t[2], *hv = c->t[3], *bv = c->t[4], *shn = c->t[5], *sbn = c->t[6];
-    double *sht = c->t[7], *sbt = c->t[8], *Hg = c->t[9], *Bg = c->t[10], *Hp = c->t[11], *Bp = c->t[12];
-    double *rh = c->t[13], *rb = c->t[14], *Hw = c->t[15], *Bw = c->t[16];
+    double** T = scratch_t(c, tid);
+    double *vn = T[0], *vt = T[1], *dl = T[2], *hv = T[3], *bv = T[4], *shn = T[5], *sbn = T[6];
+    double *sht = T[7], *sbt = T[8], *Hg = T[9], *Bg = T[10], *Hp = T[11], *Bp = T[12];
+    double *rh = T[13], *rb = T[14], *Hw = T[15], *Bw = T[16];
     const double *h = c->h + (size_t)cell * nv, *b = c->b + (size_t)cell * nv;
     const double *sh = c->sh + (size_t)cell * 2 * nv, *sb = c->sb + (size_t)cell * 2 * nv;
     for (int k = 0; k < nv; ++k) {
@@ -676,36 +739,53 @@ static int wall_face(uo_ctx* c, int side, int cell, int iw, double dt, double* F
 }
 
 /* EvolutionNative (mod_Evolution.f90:46-177) for x-periodic + two walls. */
-int uo_evolution(uo_ctx* c, double dt) {
-    const uo_params* p = &c->p;
-    int nx = p->nx, ny = p->ny, nv = p->nvel;
-    for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) {
-            int cl = j * nx + (i + nx - 1) % nx, cr = j * nx + i;
-            size_t f = (size_t)j * nx + i;
-            int e = interior_face(c, 0, cl, cr, dt, c->fxh + f * nv, c->fxb + f * nv, c->fxw + f * 4);
-            if (e) return e;
+typedef struct { uo_ctx* c; double dt; int* err; } evo_arg;
+
+static void evo_body(void* vp, int f, int tid) {
+    evo_arg* a = (evo_arg*)vp;
+    uo_ctx* c = a->c;
+    double dt = a->dt;
+    int nx = c->p.nx, ny = c->p.ny, nv = c->p.nvel;
+    int nfx = nx * ny, nfy = nx * (ny - 1);
+    int e = 0;
+    if (f < nfx) {
+        int j = f / nx, i = f % nx;
+        int cl = j * nx + (i + nx - 1) % nx, cr = j * nx + i;
+        size_t o = (size_t)j * nx + i;
+        e = interior_face(c, tid, 0, cl, cr, dt, c->fxh + o * nv, c->fxb + o * nv, c->fxw + o * 4);
+    } else if (f < nfx + nfy) {
+        int g = f - nfx, jf = 1 + g / nx, i = g % nx;
+        int cl = (jf - 1) * nx + i, cr = jf * nx + i;
+        size_t o = (size_t)jf * nx + i;
+        e = interior_face(c, tid, 1, cl, cr, dt, c->fyLh + o * nv, c->fyLb + o * nv, c->fyLw + o * 4);
+        memcpy(c->fyRh + o * nv, c->fyLh + o * nv, sizeof(double) * nv);
+        memcpy(c->fyRb + o * nv, c->fyLb + o * nv, sizeof(double) * nv);
+        memcpy(c->fyRw + o * 4, c->fyLw + o * 4, sizeof(double) * 4);
+    } else {
+        int g = f - nfx - nfy, i = g % nx;
+        if (g < nx) {
+            size_t o = (size_t)i;
+            e = wall_face(c, tid, -1, i, 0, dt, c->fyLh + o * nv, c->fyLb + o * nv, c->fyLw + o * 4, c->wall_aero + i * 3);
+        } else {
+            size_t o = (size_t)ny * nx + i;
+            e = wall_face(c, tid, +1, (ny - 1) * nx + i, 1, dt, c->fyRh + o * nv, c->fyRb + o * nv, c->fyRw + o * 4,
+                          c->wall_aero + (nx + i) * 3);
         }
-    for (int jf = 1; jf < ny; ++jf)
-        for (int i = 0; i < nx; ++i) {
-            int cl = (jf - 1) * nx + i, cr = jf * nx + i;
-            size_t f = (size_t)jf * nx + i;
-            int e = interior_face(c, 1, cl, cr, dt, c->fyLh + f * nv, c->fyLb + f * nv, c->fyLw + f * 4);
-            if (e) return e;
-            memcpy(c->fyRh + f * nv, c->fyLh + f * nv, sizeof(double) * nv);
-            memcpy(c->fyRb + f * nv, c->fyLb + f * nv, sizeof(double) * nv);
-            memcpy(c->fyRw + f * 4, c->fyLw + f * 4, sizeof(double) * 4);
-        }
-    for (int i = 0; i < nx; ++i) {
-        size_t f = (size_t)i;
-        int e = wall_face(c, -1, i, 0, dt, c->fyLh + f * nv, c->fyLb + f * nv, c->fyLw + f * 4, c->wall_aero + i * 3);
-        if (e) return e;
-        f = (size_t)ny * nx + i;
-        e = wall_face(c, +1, (ny - 1) * nx + i, 1, dt, c->fyRh + f * nv, c->fyRb + f * nv, c->fyRw + f * 4,
-                      c->wall_aero + (nx + i) * 3);
-        if (e) return e;
     }
-    return 0;
+    a->err[f] = e;
+}
+
+/* EvolutionNative (mod_Evolution.f90:46-177) for x-periodic + two walls; faces are independent. */
+int uo_evolution(uo_ctx* c, double dt) {
+    int nx = c->p.nx, ny = c->p.ny;
+    int ntot = nx * ny + nx * (ny - 1) + 2 * nx;
+    int* err = (int*)calloc((size_t)ntot, sizeof(int));
+    evo_arg a = {c, dt, err};
+    par_for(ntot, evo_body, &a, g_threads < c->nthr ? g_threads : c->nthr);
+    int e = 0;
+    for (int f = 0; f < ntot && !e; ++f) e = err[f];
+    free(err);
+    return e;
 }
 
 /* ------------------------------------------------------------------ residual + update */
@@ -714,114 +794,153 @@ int uo_evolution(uo_ctx* c, double dt) {
  * AssembleMacroResidual, AssembleMicroFluxResidual, AssembleSteadyRateResiduals with the
  * EnforceStreamingMomentCompatibility projection (mod_ImplicitMicro.f90:293-306) and, when
  * with_collision, the physical equilibrium/collision used by the implicit paths. */
-int uo_compute_residual(uo_ctx* c, double dt, int with_collision) {
+typedef struct { uo_ctx* c; double dt; int with_collision; } res_arg;
+
+static void residual_body(void* vp, int cc, int tid) {
+    res_arg* a = (res_arg*)vp;
+    uo_ctx* c = a->c;
     const uo_params* p = &c->p;
-    int nx = p->nx, ny = p->ny, nv = p->nvel;
+    double dt = a->dt;
+    int with_collision = a->with_collision;
+    int nx = p->nx, nv = p->nvel;
     double area_inv = 1.0 / c->area;
-    for (int j = 0; j < ny; ++j)
-        for (int i = 0; i < nx; ++i) {
-            int cc = j * nx + i;
-            const double *vl = c->fxw + ((size_t)j * nx + i) * 4, *vr = c->fxw + ((size_t)j * nx + (i + 1) % nx) * 4;
-            const double *hl = c->fyLw + ((size_t)j * nx + i) * 4, *hr = c->fyRw + ((size_t)(j + 1) * nx + i) * 4;
-            for (int m = 0; m < 4; ++m) c->res_w[cc * 4 + m] = (vl[m] - vr[m] + hl[m] - hr[m]) / c->area;
-            const double *vlh = c->fxh + ((size_t)j * nx + i) * nv, *vrh = c->fxh + ((size_t)j * nx + (i + 1) % nx) * nv;
-            const double *vlb = c->fxb + ((size_t)j * nx + i) * nv, *vrb = c->fxb + ((size_t)j * nx + (i + 1) % nx) * nv;
-            const double *hlh = c->fyLh + ((size_t)j * nx + i) * nv, *hrh = c->fyRh + ((size_t)(j + 1) * nx + i) * nv;
-            const double *hlb = c->fyLb + ((size_t)j * nx + i) * nv, *hrb = c->fyRb + ((size_t)(j + 1) * nx + i) * nv;
-            for (int k = 0; k < nv; ++k) {
-                c->res_h[(size_t)cc * nv + k] = (vlh[k] - vrh[k] + hlh[k] - hrh[k]) * area_inv;
-                c->res_b[(size_t)cc * nv + k] = (vlb[k] - vrb[k] + hlb[k] - hrb[k]) * area_inv;
-            }
-        }
     double dti = 1.0 / dt;
-    for (int cc = 0; cc < c->nc; ++cc) {
+    {
+        double** T = scratch_t(c, tid);
+        int j = cc / nx, i = cc % nx;
+        const double *vl = c->fxw + ((size_t)j * nx + i) * 4, *vr = c->fxw + ((size_t)j * nx + (i + 1) % nx) * 4;
+        const double *hl = c->fyLw + ((size_t)j * nx + i) * 4, *hr = c->fyRw + ((size_t)(j + 1) * nx + i) * 4;
+        for (int m = 0; m < 4; ++m) c->res_w[cc * 4 + m] = (vl[m] - vr[m] + hl[m] - hr[m]) / c->area;
+        const double *vlh = c->fxh + ((size_t)j * nx + i) * nv, *vrh = c->fxh + ((size_t)j * nx + (i + 1) % nx) * nv;
+        const double *vlb = c->fxb + ((size_t)j * nx + i) * nv, *vrb = c->fxb + ((size_t)j * nx + (i + 1) % nx) * nv;
+        const double *hlh = c->fyLh + ((size_t)j * nx + i) * nv, *hrh = c->fyRh + ((size_t)(j + 1) * nx + i) * nv;
+        const double *hlb = c->fyLb + ((size_t)j * nx + i) * nv, *hrb = c->fyRb + ((size_t)(j + 1) * nx + i) * nv;
+        for (int k = 0; k < nv; ++k) {
+            c->res_h[(size_t)cc * nv + k] = (vlh[k] - vrh[k] + hlh[k] - hrh[k]) * area_inv;
+            c->res_b[(size_t)cc * nv + k] = (vlb[k] - vrb[k] + hlb[k] - hrb[k]) * area_inv;
+        }
         for (int m = 0; m < 4; ++m) c->rate_w[cc * 4 + m] = c->res_w[cc * 4 + m] * dti;
         for (int k = 0; k < nv; ++k) {
             c->stream_h[(size_t)cc * nv + k] = c->res_h[(size_t)cc * nv + k] * dti;
             c->stream_b[(size_t)cc * nv + k] = c->res_b[(size_t)cc * nv + k] * dti;
         }
-    }
-    int ok = 1;
-    for (int cc = 0; cc < c->nc; ++cc)
-        ok &= uo_project_moments(nv, c->stream_h + (size_t)cc * nv, c->stream_b + (size_t)cc * nv, c->rate_w + cc * 4,
-                                 c->u, c->v, c->w, c->h + (size_t)cc * nv, c->b + (size_t)cc * nv);
-    for (int cc = 0; cc < c->nc; ++cc) {
+        int e = 0;
+        if (!uo_project_moments(nv, c->stream_h + (size_t)cc * nv, c->stream_b + (size_t)cc * nv, c->rate_w + cc * 4,
+                                c->u, c->v, c->w, c->h + (size_t)cc * nv, c->b + (size_t)cc * nv))
+            e = 444;
         for (int k = 0; k < nv; ++k) {
             c->res_h[(size_t)cc * nv + k] = c->stream_h[(size_t)cc * nv + k] * dt;
             c->res_b[(size_t)cc * nv + k] = c->stream_b[(size_t)cc * nv + k] * dt;
         }
-        if (!with_collision) continue;
-        double prim[4], tau, q[2];
-        int e = get_primary(p, c->W + cc * 4, prim);
-        if (e) return e;
-        e = get_tau(p, prim, &tau);
-        if (e) return e;
-        const double *h = c->h + (size_t)cc * nv, *b = c->b + (size_t)cc * nv;
-        double *eh = c->peq_h + (size_t)cc * nv, *eb = c->peq_b + (size_t)cc * nv;
-        heat_flux(nv, h, b, c->u, c->v, c->w, prim, q);
-        maxwell(p, nv, c->u, c->v, prim, eh, eb);
-        shakhov(p, nv, eh, eb, c->u, c->v, q, prim, c->t[0], c->t[1]);
-        for (int k = 0; k < nv; ++k) { eh[k] = eh[k] + c->t[0][k]; eb[k] = eb[k] + c->t[1][k]; }
-        memcpy(c->t[2], eh, sizeof(double) * nv);
-        memcpy(c->t[3], eb, sizeof(double) * nv);
-        ok &= uo_project_moments(nv, eh, eb, c->W + cc * 4, c->u, c->v, c->w, c->t[2], c->t[3]);
-        for (int k = 0; k < nv; ++k) {
-            c->pcol_h[(size_t)cc * nv + k] = (eh[k] - h[k]) / tau;
-            c->pcol_b[(size_t)cc * nv + k] = (eb[k] - b[k]) / tau;
+        if (with_collision && !e) {
+            double prim[4], tau, q[2];
+            e = get_primary(p, c->W + cc * 4, prim);
+            if (!e) e = get_tau(p, prim, &tau);
+            if (!e) {
+                const double *h = c->h + (size_t)cc * nv, *b = c->b + (size_t)cc * nv;
+                double *eh = c->peq_h + (size_t)cc * nv, *eb = c->peq_b + (size_t)cc * nv;
+                heat_flux(nv, h, b, c->u, c->v, c->w, prim, q);
+                maxwell(p, nv, c->u, c->v, prim, eh, eb);
+                shakhov(p, nv, eh, eb, c->u, c->v, q, prim, T[0], T[1]);
+                for (int k = 0; k < nv; ++k) { eh[k] = eh[k] + T[0][k]; eb[k] = eb[k] + T[1][k]; }
+                memcpy(T[2], eh, sizeof(double) * nv);
+                memcpy(T[3], eb, sizeof(double) * nv);
+                if (!uo_project_moments(nv, eh, eb, c->W + cc * 4, c->u, c->v, c->w, T[2], T[3])) e = 444;
+                for (int k = 0; k < nv; ++k) {
+                    c->pcol_h[(size_t)cc * nv + k] = (eh[k] - h[k]) / tau;
+                    c->pcol_b[(size_t)cc * nv + k] = (eb[k] - b[k]) / tau;
+                }
+            }
         }
+        c->cell_err[cc] = e;
     }
-    return ok ? 0 : 444;
+}
+
+int uo_compute_residual(uo_ctx* c, double dt, int with_collision) {
+    res_arg a = {c, dt, with_collision};
+    par_for(c->nc, residual_body, &a, g_threads < c->nthr ? g_threads : c->nthr);
+    /* first failing cell in cell order, like the reference's per-rank loop order */
+    for (int cc = 0; cc < c->nc; ++cc) if (c->cell_err[cc]) return c->cell_err[cc];
+    return 0;
 }
 
 /* ApplyExplicitUpdate + ApplyMicroExplicitUpdate + residual norms
- * (mod_TimeIntegrator.f90:16-134,163-191,235-293). */
+ * (mod_TimeIntegrator.f90:16-134,163-191,235-293).  Cells update in parallel; the residual-norm
+ * terms are stored per cell and summed afterwards in cell order, as the single-rank loop does. */
+typedef struct { uo_ctx* c; double dt; } upd_arg;
+
+static void update_body(void* vp, int cc, int tid) {
+    upd_arg* a = (upd_arg*)vp;
+    uo_ctx* c = a->c;
+    const uo_params* p = &c->p;
+    double dt = a->dt;
+    int nv = p->nvel;
+    {
+        double** T = scratch_t(c, tid);
+        double *Ho = T[17], *Bo = T[18], *Hn = T[19], *Bn = T[20], *Hp = T[21], *Bp = T[22];
+        double *rh = T[13], *rb = T[14];
+        double Wold[4], po[4], pn[4], to, tn;
+        double* dg = c->cell_diag + (size_t)cc * 13;
+        int e = 0;
+        memcpy(Wold, c->W + cc * 4, sizeof Wold);
+        e = get_primary(p, Wold, po);
+        if (!e) { maxwell(p, nv, c->u, c->v, po, Ho, Bo); e = get_tau(p, po, &to); }
+        if (!e) {
+            for (int m = 0; m < 4; ++m) c->W[cc * 4 + m] = c->W[cc * 4 + m] + c->res_w[cc * 4 + m];
+            for (int m = 0; m < 4; ++m) if (!isfinite(c->W[cc * 4 + m])) e = 4;
+        }
+        if (!e) e = get_primary(p, c->W + cc * 4, pn);
+        if (!e) { maxwell(p, nv, c->u, c->v, pn, Hn, Bn); e = get_tau(p, pn, &tn); }
+        if (!e) {
+            for (int m = 0; m < 4; ++m) {
+                double d = (Wold[m] - c->W[cc * 4 + m]) * c->area / dt;
+                dg[m] = d * d;
+                dg[9 + m] = fabs(d);
+                dg[4 + m] = fabs(c->W[cc * 4 + m]) * c->area;
+            }
+            dg[8] = c->area * c->area;
+            double* h = c->h + (size_t)cc * nv;
+            double* b = c->b + (size_t)cc * nv;
+            double qf[2];
+            heat_flux(nv, h, b, c->u, c->v, c->w, po, qf);
+            shakhov(p, nv, Ho, Bo, c->u, c->v, qf, po, Hp, Bp);
+            for (int k = 0; k < nv; ++k) { Ho[k] = Ho[k] + Hp[k]; Bo[k] = Bo[k] + Bp[k]; }
+            shakhov(p, nv, Hn, Bn, c->u, c->v, qf, pn, Hp, Bp);
+            for (int k = 0; k < nv; ++k) { Hn[k] = Hn[k] + Hp[k]; Bn[k] = Bn[k] + Bp[k]; }
+            double tg[4];
+            get_conserved(p, po, tg);
+            memcpy(rh, Ho, sizeof(double) * nv); memcpy(rb, Bo, sizeof(double) * nv);
+            if (!uo_project_moments(nv, Ho, Bo, tg, c->u, c->v, c->w, rh, rb)) e = 444;
+            memcpy(rh, Hn, sizeof(double) * nv); memcpy(rb, Bn, sizeof(double) * nv);
+            if (!e && !uo_project_moments(nv, Hn, Bn, c->W + cc * 4, c->u, c->v, c->w, rh, rb)) e = 444;
+            if (!e) {
+                double inv = 1.0 / (1.0 + 0.5 * dt / tn);
+                const double *fh = c->res_h + (size_t)cc * nv, *fb = c->res_b + (size_t)cc * nv;
+                for (int k = 0; k < nv; ++k) {
+                    double ho = h[k], bo = b[k];
+                    h[k] = (ho + fh[k] + 0.5 * dt * (Hn[k] / tn + (Ho[k] - ho) / to)) * inv;
+                    b[k] = (bo + fb[k] + 0.5 * dt * (Bn[k] / tn + (Bo[k] - bo) / to)) * inv;
+                }
+            }
+        }
+        c->cell_err[cc] = e;
+    }
+}
+
 int uo_apply_explicit_update(uo_ctx* c, double dt, double* res_out) {
     const uo_params* p = &c->p;
-    int nv = p->nvel;
+    upd_arg a = {c, dt};
+    par_for(c->nc, update_body, &a, g_threads < c->nthr ? g_threads : c->nthr);
+    for (int cc = 0; cc < c->nc; ++cc) if (c->cell_err[cc]) return c->cell_err[cc];
     double sumRes[4] = {0, 0, 0, 0}, sumAvg[4] = {0, 0, 0, 0}, areaSq = 0.0, maxCell[4] = {0, 0, 0, 0};
-    double *Ho = c->t[17], *Bo = c->t[18], *Hn = c->t[19], *Bn = c->t[20], *Hp = c->t[21], *Bp = c->t[22];
-    double *rh = c->t[13], *rb = c->t[14];
     for (int cc = 0; cc < c->nc; ++cc) {
-        double Wold[4], po[4], pn[4], to, tn;
-        memcpy(Wold, c->W + cc * 4, sizeof Wold);
-        int e = get_primary(p, Wold, po);
-        if (e) return e;
-        maxwell(p, nv, c->u, c->v, po, Ho, Bo);
-        if ((e = get_tau(p, po, &to))) return e;
-        for (int m = 0; m < 4; ++m) c->W[cc * 4 + m] = c->W[cc * 4 + m] + c->res_w[cc * 4 + m];
-        for (int m = 0; m < 4; ++m) if (!isfinite(c->W[cc * 4 + m])) return 4;
-        if ((e = get_primary(p, c->W + cc * 4, pn))) return e;
-        maxwell(p, nv, c->u, c->v, pn, Hn, Bn);
-        if ((e = get_tau(p, pn, &tn))) return e;
+        const double* dg = c->cell_diag + (size_t)cc * 13;
         for (int m = 0; m < 4; ++m) {
-            double d = (Wold[m] - c->W[cc * 4 + m]) * c->area / dt;
-            double rc = fabs(d);
-            if (rc > maxCell[m]) maxCell[m] = rc;
-            sumRes[m] = sumRes[m] + d * d;
+            if (dg[9 + m] > maxCell[m]) maxCell[m] = dg[9 + m];
+            sumRes[m] = sumRes[m] + dg[m];
         }
-        for (int m = 0; m < 4; ++m) sumAvg[m] = sumAvg[m] + fabs(c->W[cc * 4 + m]) * c->area;
-        areaSq = areaSq + c->area * c->area;
-        double* h = c->h + (size_t)cc * nv;
-        double* b = c->b + (size_t)cc * nv;
-        double qf[2];
-        heat_flux(nv, h, b, c->u, c->v, c->w, po, qf);
-        shakhov(p, nv, Ho, Bo, c->u, c->v, qf, po, Hp, Bp);
-        for (int k = 0; k < nv; ++k) { Ho[k] = Ho[k] + Hp[k]; Bo[k] = Bo[k] + Bp[k]; }
-        shakhov(p, nv, Hn, Bn, c->u, c->v, qf, pn, Hp, Bp);
-        for (int k = 0; k < nv; ++k) { Hn[k] = Hn[k] + Hp[k]; Bn[k] = Bn[k] + Bp[k]; }
-        double tg[4];
-        get_conserved(p, po, tg);
-        memcpy(rh, Ho, sizeof(double) * nv); memcpy(rb, Bo, sizeof(double) * nv);
-        if (!uo_project_moments(nv, Ho, Bo, tg, c->u, c->v, c->w, rh, rb)) return 444;
-        memcpy(rh, Hn, sizeof(double) * nv); memcpy(rb, Bn, sizeof(double) * nv);
-        if (!uo_project_moments(nv, Hn, Bn, c->W + cc * 4, c->u, c->v, c->w, rh, rb)) return 444;
-        double inv = 1.0 / (1.0 + 0.5 * dt / tn);
-        const double *fh = c->res_h + (size_t)cc * nv, *fb = c->res_b + (size_t)cc * nv;
-        for (int k = 0; k < nv; ++k) {
-            double ho = h[k], bo = b[k];
-            h[k] = (ho + fh[k] + 0.5 * dt * (Hn[k] / tn + (Ho[k] - ho) / to)) * inv;
-            b[k] = (bo + fb[k] + 0.5 * dt * (Bn[k] / tn + (Bo[k] - bo) / to)) * inv;
-        }
+        for (int m = 0; m < 4; ++m) sumAvg[m] = sumAvg[m] + dg[4 + m];
+        areaSq = areaSq + dg[8];
     }
     /* residual norms (mod_TimeIntegrator.f90:102-127) */
     double ncell = (double)(p->nx * p->ny);

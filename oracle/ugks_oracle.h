@@ -85,6 +85,11 @@ int uo_solve_dense4(const double m[16], const double rhs[4], double sol[4]);
  * block-Jacobi seams.  out[] receives the diagnostics listed in ugks_oracle.c. */
 int uo_implicit_step(uo_ctx* c, double* out, int nout);
 
+/* Worker threads used over faces and cells (0 = all host cores); returns the count in use.
+ * Results do not depend on the thread count: faces and cells are independent and every sum over
+ * cells is taken afterwards in cell order. */
+int uo_set_threads(int n);
+
 #ifdef __cplusplus
 }
 #endif
