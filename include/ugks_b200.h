@@ -99,6 +99,24 @@ int ugks_apply_explicit_update(ugks_ctx* ctx, double* res_out);
  * from a CUDA graph.  dt_out / res_out (optional) report the last step. */
 int ugks_step_explicit(ugks_ctx* ctx, int nsteps, double* dt_out, double* res_out);
 
+/* The Explicit step of ugks_step_explicit for callers that cannot allocate device memory.  No
+ * counterpart in the reference (its Fortran solver owns module globals); added for host codes
+ * that manage every byte of device memory themselves (their own pre-sized pool, or a hard memory
+ * cap) and for latency-critical loops where cudaMalloc/cudaFree would synchronise the device.
+ * It creates no context and allocates nothing: u, v, w (nvel each), h, b ([ny][nx][nvel]) and W
+ * ([ny][nx][4]) are the caller's DEVICE arrays, updated in place by nsteps steps on `stream`
+ * (a cudaStream_t; NULL = legacy default stream); dt_out / res_out are optional host outputs as in
+ * ugks_step_explicit.  Working arrays live in one fixed 36 MiB __device__ array inside the library:
+ * a call whose working set (about 8*nx*ny*nvel + 2*nx*nvel + 22*nx*ny doubles; 33.8 MB for
+ * 8x64 cells x 32x32 velocities) does not fit returns UGKS_EINVAL before any GPU work.  Every
+ * GPU that loads the library keeps that array until the process exits.  The first call on a
+ * device looks up the array's device address with that device current, so make it before any
+ * stream capture.  All calls share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller. */
+int ugks_step_explicit_noalloc(const ugks_params* params, const double* u, const double* v, const double* w,
+                               double* h, double* b, double* W, int nsteps, void* stream, double* dt_out,
+                               double* res_out);
+
 /* Wall Aerodynamics of the last Evolution (src/mod_Evolution.f90:2402-2409): out[2][nx][3] =
  * local-frame (pnn, pnt, qn) per bottom/top wall face. */
 int ugks_wall_aero(ugks_ctx* ctx, double* out);

@@ -10,6 +10,12 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libugks_b200.so")
 
 UGKS_OK = 0
+UGKS_EINVAL = 1
+UGKS_ECUDA = 2
+UGKS_ENUMERIC = 3
+UGKS_ETIMEOUT = 4
+UGKS_ENOMEM = 5
+UGKS_EUNSUPPORTED = 6
 UGKS_METHOD_EXPLICIT = 0
 UGKS_METHOD_IMPLICIT_STEADY = 1
 
@@ -19,7 +25,7 @@ EXPORTS = [
     "ugks_timestep", "ugks_evolution", "ugks_compute_residual", "ugks_apply_explicit_update",
     "ugks_step_explicit", "ugks_wall_aero", "ugks_copy_array", "ugks_last_status", "ugks_status_reference_code",
     "ugks_error_string", "ugks_stream", "ugks_synchronize", "ugks_profile_enable", "ugks_profile_read",
-    "ugks_launch_count",
+    "ugks_launch_count", "ugks_step_explicit_noalloc",
 ]
 
 
@@ -83,6 +89,8 @@ def load(path=LIB_PATH):
     L.ugks_profile_read.argtypes = [vp, ctypes.c_char_p, dp, ctypes.POINTER(ctypes.c_longlong)]
     L.ugks_launch_count.argtypes = [vp]
     L.ugks_launch_count.restype = ctypes.c_longlong
+    L.ugks_step_explicit_noalloc.argtypes = [ctypes.POINTER(UgksParams), vp, vp, vp, vp, vp, vp, ctypes.c_int, vp,
+                                             dp, dp]
     _lib = L
     return L
 
