@@ -33,6 +33,8 @@ struct ugks_ctx {
     ugks_params prm;
     int device = 0;
     cudaStream_t stream = nullptr;
+    cudaStream_t stream2 = nullptr;          // side stream: wall faces run beside the interior faces
+    cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
     LoParams P{};
     LoBuffers B{};
     double* dmem = nullptr;      // one allocation backing every double buffer
@@ -139,6 +141,9 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     const size_t o_wa = take((size_t)2 * nx * 3);
     c->ndoubles = off;
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaStreamCreateWithFlags(&c->stream2, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_fork, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&c->ev_join, cudaEventDisableTiming);
     if (e == cudaSuccess) e = cudaMalloc(&c->dmem, off * sizeof(double));
     if (e == cudaSuccess) e = cudaMalloc(&c->dflags, 4 * sizeof(unsigned));
     if (e == cudaSuccess) e = cudaMemsetAsync(c->dmem, 0, off * sizeof(double), c->stream);
@@ -173,6 +178,9 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->dmem) cudaFree(c->dmem);
     if (c->dflags) cudaFree(c->dflags);
+    if (c->stream2) { cudaStreamSynchronize(c->stream2); cudaStreamDestroy(c->stream2); }
+    if (c->ev_fork) cudaEventDestroy(c->ev_fork);
+    if (c->ev_join) cudaEventDestroy(c->ev_join);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     return UGKS_OK;
@@ -280,15 +288,19 @@ extern "C" int ugks_apply_explicit_update(ugks_ctx* c, double* res_out) {
     return read_step_outputs(c, nullptr, res_out);
 }
 
+// One Explicit step per iteration: slopes, then the interior faces on the main stream while the
+// wall faces run on the side stream (they read only the slopes and the state), joined before the
+// cell update.  The fork/join is recorded into the CUDA graph as two parallel branches.
 static cudaError_t enqueue_explicit_steps(ugks_ctx* c, int n) {
     for (int s = 0; s < n; ++s) {
         cudaError_t e = launch_lo_slopes(c->P, c->B, c->stream);
-        if (e != cudaSuccess) return e;
-        e = launch_lo_faces(c->P, c->B, c->stream);
-        if (e != cudaSuccess) return e;
-        e = launch_lo_walls(c->P, c->B, c->stream);
-        if (e != cudaSuccess) return e;
-        e = launch_lo_cells(c->P, c->B, 3, false, c->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_fork, c->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream2, c->ev_fork, 0);
+        if (e == cudaSuccess) e = launch_lo_walls(c->P, c->B, c->stream2);
+        if (e == cudaSuccess) e = cudaEventRecord(c->ev_join, c->stream2);
+        if (e == cudaSuccess) e = launch_lo_faces(c->P, c->B, c->stream);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(c->stream, c->ev_join, 0);
+        if (e == cudaSuccess) e = launch_lo_cells(c->P, c->B, 3, false, c->stream);
         if (e != cudaSuccess) return e;
     }
     return cudaSuccess;

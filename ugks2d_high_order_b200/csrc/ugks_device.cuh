@@ -264,8 +264,11 @@ __device__ __forceinline__ double warp_halving(const double* v) {
     return t[0];   // the total of logical index (lane >> (5 - log2 NP)) when NP <= 32
 }
 
+// Reduce into shared memory only: on return out[0..NS+NM) holds the block totals and is visible
+// to every thread.  The next reduction writes `out` only after its first barrier, which no thread
+// passes before it has read this one, so no trailing barrier is needed.
 template <int NS, int NM>
-__device__ __forceinline__ void block_reduce(double* v, double* red, double* out) {
+__device__ __forceinline__ void block_reduce_smem(const double* v, double* red, double* out) {
     constexpr int PS = NS > 0 ? pow2_ceil(NS) : 0;
     constexpr int PM = NM > 0 ? pow2_ceil(NM) : 0;
     constexpr int W = PS + PM;
@@ -290,9 +293,13 @@ __device__ __forceinline__ void block_reduce(double* v, double* red, double* out
         out[i] = s;
     }
     __syncthreads();
+}
+
+template <int NS, int NM>
+__device__ __forceinline__ void block_reduce(double* v, double* red, double* out) {
+    block_reduce_smem<NS, NM>(v, red, out);
 #pragma unroll
     for (int i = 0; i < NS + NM; ++i) v[i] = out[i];
-    __syncthreads();
 }
 
 __device__ __forceinline__ void set_status(unsigned* status, unsigned bit) {

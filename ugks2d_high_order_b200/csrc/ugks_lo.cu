@@ -37,29 +37,27 @@ __device__ __forceinline__ Slot slot(int r, int nv) {
 // the wall rows the y slope is the one-sided (right-left)/dy of InterpBoundary (:100-117), and
 // UnifiedPhysicalOperators skips the Van-Leer inner loop there (:40-45,78-88).
 __global__ void __launch_bounds__(256) k_lo_slopes(LoParams P, LoBuffers B) {
+    // grid: x covers the velocity row, y = cell; 32-bit index arithmetic only
     const int nv = P.nvel, nx = P.nx, ny = P.ny;
-    const size_t n = (size_t)nx * ny * nv;
-    const size_t idx = (size_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx >= n) return;
-    const int k = (int)(idx % nv);
-    const int c = (int)(idx / nv), i = c % nx, j = c / nx;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= nv) return;
+    const int c = blockIdx.y, j = c / nx, i = c - j * nx;
+    const size_t row = (size_t)nx * nv;
+    const size_t idx = (size_t)c * nv + k;
     const size_t cm = (size_t)(j * nx + wrapx(i - 1, nx)) * nv + k, cp = (size_t)(j * nx + wrapx(i + 1, nx)) * nv + k;
     const double h0 = B.h[idx], b0 = B.b[idx];
     B.sxh[idx] = vanleer((h0 - B.h[cm]) * P.inv_dx, (B.h[cp] - h0) * P.inv_dx);
     B.sxb[idx] = vanleer((b0 - B.b[cm]) * P.inv_dx, (B.b[cp] - b0) * P.inv_dx);
     double syh, syb;
     if (j == 0) {
-        const size_t u = idx + (size_t)nx * nv;
-        syh = (B.h[u] - h0) * P.inv_dy;
-        syb = (B.b[u] - b0) * P.inv_dy;
+        syh = (B.h[idx + row] - h0) * P.inv_dy;
+        syb = (B.b[idx + row] - b0) * P.inv_dy;
     } else if (j == ny - 1) {
-        const size_t d = idx - (size_t)nx * nv;
-        syh = (h0 - B.h[d]) * P.inv_dy;
-        syb = (b0 - B.b[d]) * P.inv_dy;
+        syh = (h0 - B.h[idx - row]) * P.inv_dy;
+        syb = (b0 - B.b[idx - row]) * P.inv_dy;
     } else {
-        const size_t u = idx + (size_t)nx * nv, d = idx - (size_t)nx * nv;
-        syh = vanleer((h0 - B.h[d]) * P.inv_dy, (B.h[u] - h0) * P.inv_dy);
-        syb = vanleer((b0 - B.b[d]) * P.inv_dy, (B.b[u] - b0) * P.inv_dy);
+        syh = vanleer((h0 - B.h[idx - row]) * P.inv_dy, (B.h[idx + row] - h0) * P.inv_dy);
+        syb = vanleer((b0 - B.b[idx - row]) * P.inv_dy, (B.b[idx + row] - b0) * P.inv_dy);
     }
     B.syh[idx] = syh;
     B.syb[idx] = syb;
@@ -72,7 +70,7 @@ __global__ void __launch_bounds__(256) k_lo_slopes(LoParams P, LoBuffers B) {
 template <int VPT>
 __device__ __forceinline__ void lo_face_interior(const LoParams& P, const LoBuffers& B, int dir, int cL, int cR,
                                                  double dt, double* __restrict__ Fh, double* __restrict__ Fb,
-                                                 double* Fw, double* red, double* rout) {
+                                                 double* Fw, double* red, double* rout, double* sc) {
     const int nv = P.nvel, tid = threadIdx.x;
     const double len = dir == 0 ? P.dx : P.dy;      // cell length normal to the face
     const double flen = dir == 0 ? P.dy : P.dx;     // face length
@@ -107,27 +105,28 @@ __device__ __forceinline__ void lo_face_interior(const LoParams& P, const LoBuff
         acc[6] += wk * vt * sht;
         acc[7] += 0.5 * wk * (v2 * sht + sbt);
     }
-    block_reduce<8, 0>(acc, red, rout);
-    // face state, micro slopes aL, aR, b, A and the time coefficients (every thread, same values)
-    Prim pf;
-    const double cv[4] = {acc[0], acc[1], acc[2], acc[3]};
-    const bool ok = get_primary(P.gm1, cv, pf);
-    if (!ok) { pf.r = 1.0; pf.U = 0.0; pf.V = 0.0; pf.L = 1.0; }
-    const double* WL = B.W + cL * 4;
-    const double* WR = B.W + cR * 4;
-    double wl[4], wr[4];
-    wl[0] = WL[0]; wl[3] = WL[3]; wr[0] = WR[0]; wr[3] = WR[3];
-    if (dir == 0) { wl[1] = WL[1]; wl[2] = WL[2]; wr[1] = WR[1]; wr[2] = WR[2]; }
-    else { wl[1] = WL[2]; wl[2] = -WL[1]; wr[1] = WR[2]; wr[2] = -WR[1]; }
-    double sw[4], aL[4], aR[4], bs[4], aT[4], Mt[5], tau = 1.0, mxi2;
+    block_reduce_smem<8, 0>(acc, red, rout);
+    // face state, micro slopes aL, aR, b, A and the time coefficients: one thread computes them
+    // (GetPrimary, MicroSlope x4, CalcMoment, GetTau, Mt) and broadcasts through shared memory.
+    if (tid == 0) {
+        Prim pf;
+        const double cv[4] = {rout[0], rout[1], rout[2], rout[3]};
+        const bool ok = get_primary(P.gm1, cv, pf);
+        if (!ok) { pf.r = 1.0; pf.U = 0.0; pf.V = 0.0; pf.L = 1.0; }
+        const double* WL = B.W + cL * 4;
+        const double* WR = B.W + cR * 4;
+        double wl[4], wr[4];
+        wl[0] = WL[0]; wl[3] = WL[3]; wr[0] = WR[0]; wr[3] = WR[3];
+        if (dir == 0) { wl[1] = WL[1]; wl[2] = WL[2]; wr[1] = WR[1]; wr[2] = WR[2]; }
+        else { wl[1] = WL[2]; wl[2] = -WL[1]; wr[1] = WR[2]; wr[2] = -WR[1]; }
+        double sw[4], aL[4], aR[4], bs[4], aT[4], Mt[5], tau = 1.0;
 #pragma unroll
-    for (int m = 0; m < 4; ++m) sw[m] = (cv[m] - wl[m]) / hl;
-    micro_slope(P.ck, pf, sw, aL);
+        for (int m = 0; m < 4; ++m) sw[m] = (cv[m] - wl[m]) / hl;
+        micro_slope(P.ck, pf, sw, aL);
 #pragma unroll
-    for (int m = 0; m < 4; ++m) sw[m] = (wr[m] - cv[m]) / hl;
-    micro_slope(P.ck, pf, sw, aR);
-    {
-        const double swt[4] = {acc[4], acc[5], acc[6], acc[7]};
+        for (int m = 0; m < 4; ++m) sw[m] = (wr[m] - cv[m]) / hl;
+        micro_slope(P.ck, pf, sw, aR);
+        const double swt[4] = {rout[4], rout[5], rout[6], rout[7]};
         micro_slope(P.ck, pf, swt, bs);
         Moments M;
         calc_moment(P.ck, pf, M);
@@ -138,15 +137,26 @@ __device__ __forceinline__ void lo_face_interior(const LoParams& P, const LoBuff
 #pragma unroll
         for (int m = 0; m < 4; ++m) sw[m] = -pf.r * (MauL[m] + MauR[m] + Mbv[m]);
         micro_slope(P.ck, pf, sw, aT);
-        mxi2 = M.Mxi[2];
-    }
-    const bool tok = get_tau(P.mu_ref, P.omega, pf, tau);
-    if (!tok) tau = 1.0;
-    time_coeffs(dt, tau, Mt);
-    if (tid == 0) {
+        const bool tok = get_tau(P.mu_ref, P.omega, pf, tau);
+        if (!tok) tau = 1.0;
+        time_coeffs(dt, tau, Mt);
         if (!ok) set_status(B.status, ST_GETPRIMARY);
         if (ok && !tok) set_status(B.status, ST_TAU);
+        sc[0] = pf.r; sc[1] = pf.U; sc[2] = pf.V; sc[3] = pf.L;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { sc[4 + m] = aL[m]; sc[8 + m] = aR[m]; sc[12 + m] = bs[m]; sc[16 + m] = aT[m]; }
+#pragma unroll
+        for (int m = 0; m < 5; ++m) sc[20 + m] = Mt[m];
+        sc[25] = M.Mxi[2];
     }
+    __syncthreads();
+    const Prim pf{sc[0], sc[1], sc[2], sc[3]};
+    double aL[4], aR[4], bs[4], aT[4], Mt[5];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) { aL[m] = sc[4 + m]; aR[m] = sc[8 + m]; bs[m] = sc[12 + m]; aT[m] = sc[16 + m]; }
+#pragma unroll
+    for (int m = 0; m < 5; ++m) Mt[m] = sc[20 + m];
+    const double mxi2 = sc[25];
     // face equilibrium H0 (PrepareNativeFaceEquilibrium, mod_Evolution.f90:16-30) + heat flux
     const double pref = pf.r * (pf.L / kPi), bfac = (double)P.ck / (2.0 * pf.L);
 #pragma unroll
@@ -179,19 +189,24 @@ __device__ __forceinline__ void lo_face_interior(const LoParams& P, const LoBuff
         moment_add(wk, vn, vt, H0[r], b0, acc);
         gram_add(wk, fmax(fabs(H0[r]), kEps * sch), fmax(fabs(b0), kEps * scb), vn, vt, acc + 4);
     }
-    block_reduce<14, 0>(acc, red, rout);
+    block_reduce_smem<14, 0>(acc, red, rout);
     double tgt[4], lam[4];
     get_conserved(P.gm1, pf, tgt);
-    {
-        double rhs[4], gm[16];
+    if (tid == 0) {   // SolveDense4 once per face, broadcast
+        double rhs[4], gm[16], l[4];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) rhs[m] = tgt[m] - acc[m];
-        gram_expand(acc + 4, gm);
-        if (!solve_dense4(gm, rhs, lam)) {
-            lam[0] = lam[1] = lam[2] = lam[3] = 0.0;
-            if (tid == 0) set_status(B.status, ST_FACE_PROJECTION);
+        for (int m = 0; m < 4; ++m) rhs[m] = tgt[m] - rout[m];
+        gram_expand(rout + 4, gm);
+        if (!solve_dense4(gm, rhs, l)) {
+            l[0] = l[1] = l[2] = l[3] = 0.0;
+            set_status(B.status, ST_FACE_PROJECTION);
         }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) sc[26 + m] = l[m];
     }
+    __syncthreads();
+#pragma unroll
+    for (int m = 0; m < 4; ++m) lam[m] = sc[26 + m];
     // Shakhov part and the micro flux (mod_Evolution.f90:396-453), times the face length.
     const double coeff = 0.8 * (1.0 - P.pr) * pf.L * pf.L / pf.r;
     const double c2ck = 2.0 / (double)P.ck;
@@ -453,6 +468,7 @@ template <int VPT, int NTMAX>
 __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_faces(LoParams P, LoBuffers B) {
     __shared__ double red[16 * 64];
     __shared__ double rout[kRedSlots];
+    __shared__ double sc[32];
     const double dt = B.dt[0];
     const int nx = P.nx, ny = P.ny, nv = P.nvel;
     int f = blockIdx.x;
@@ -460,14 +476,14 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_faces(LoParams P, LoB
         const int j = f / nx, i = f % nx;
         const size_t o = (size_t)(j * nx + i);
         lo_face_interior<VPT>(P, B, 0, j * nx + wrapx(i - 1, nx), j * nx + i, dt, B.fxh + o * nv, B.fxb + o * nv,
-                              B.fxw + o * 4, red, rout);
+                              B.fxw + o * 4, red, rout, sc);
         return;
     }
     f -= nx * ny;
     const int jf = 1 + f / nx, i = f % nx;
     const size_t o = (size_t)(jf * nx + i);
     lo_face_interior<VPT>(P, B, 1, (jf - 1) * nx + i, jf * nx + i, dt, B.fyh + o * nv, B.fyb + o * nv, B.fyw + o * 4,
-                          red, rout);
+                          red, rout, sc);
 }
 
 template <int VPT, int NTMAX>
@@ -555,17 +571,54 @@ template <int VPT, int NTMAX, int MODE, bool COLLISION>
 __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoBuffers B) {
     __shared__ double red[16 * 64];
     __shared__ double rout[kRedSlots];
+    // per-cell scalars computed once (threads 0 and t1) and broadcast:
+    //  [0..3] prim_old  [4] tau_old  [5] ok_old  [8..11] res_w  [12..15] prim_new  [16] tau_new  [17] ok_new
+    //  [18..21] W_new  [22] dt_local(W_new)  [24..27] stream lambda  [28..31] old lambda  [32..35] new lambda
+    //  [36..39] collision lambda  [40] projection flags
+    __shared__ double sc[48];
     const int nv = P.nvel, tid = threadIdx.x, nx = P.nx;
+    const int t1 = blockDim.x > 32 ? 32 : 0;   // a thread of the second warp, so the two solves overlap
     const int c = blockIdx.x, i = c % nx, j = c / nx;
     const double dt = B.dt[0];
     const double* hc = B.h + (size_t)c * nv;
     const double* bc = B.b + (size_t)c * nv;
     double h[VPT], b[VPT], rh[VPT], rb[VPT];
-    double Wold[4];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) Wold[m] = B.W[c * 4 + m];
-    double resw[4];
     double acc[28];
+    const size_t fl = (size_t)(j * nx + i), fr = (size_t)(j * nx + wrapx(i + 1, nx));
+    const size_t gl = (size_t)(j * nx + i), gr = (size_t)((j + 1) * nx + i);
+    if (tid == 0) {
+        const double* Wo = B.W + c * 4;
+        Prim po;
+        double to = 1.0;
+        bool ok = get_primary(P.gm1, Wo, po);
+        ok = ok && get_tau(P.mu_ref, P.omega, po, to);
+        if (!ok) { po.r = 1.0; po.U = po.V = 0.0; po.L = 1.0; to = 1.0; }
+        sc[0] = po.r; sc[1] = po.U; sc[2] = po.V; sc[3] = po.L; sc[4] = to; sc[5] = ok ? 1.0 : 0.0;
+    }
+    if (tid == t1) {
+        double resw[4], Wn[4];
+        if (MODE & MODE_RESIDUAL) {
+            // AssembleMacroResidual (mod_Residual.f90:30-54)
+#pragma unroll
+            for (int m = 0; m < 4; ++m)
+                resw[m] = (B.fxw[fl * 4 + m] - B.fxw[fr * 4 + m] + B.fyw[gl * 4 + m] - B.fyw[gr * 4 + m]) / P.area;
+        } else {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) resw[m] = B.res_w[c * 4 + m];
+        }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { Wn[m] = B.W[c * 4 + m] + resw[m]; sc[8 + m] = resw[m]; sc[18 + m] = Wn[m]; }
+        if (MODE & MODE_UPDATE) {
+            Prim pn;
+            double tn = 1.0;
+            bool ok = get_primary(P.gm1, Wn, pn);
+            ok = ok && get_tau(P.mu_ref, P.omega, pn, tn);
+            if (!ok) { pn.r = 1.0; pn.U = pn.V = 0.0; pn.L = 1.0; tn = 1.0; }
+            sc[12] = pn.r; sc[13] = pn.U; sc[14] = pn.V; sc[15] = pn.L; sc[16] = tn; sc[17] = ok ? 1.0 : 0.0;
+            bool dok;
+            sc[22] = cell_dt(P, Wn, dok);
+        }
+    }
 #pragma unroll
     for (int r = 0; r < VPT; ++r) {
         const Slot s = slot(r, nv);
@@ -573,13 +626,8 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
         b[r] = bc[s.kk];
     }
     if (MODE & MODE_RESIDUAL) {
-        // AssembleMacroResidual / AssembleMicroFluxResidual (mod_Residual.f90:30-76)
-        const size_t fl = (size_t)(j * nx + i), fr = (size_t)(j * nx + wrapx(i + 1, nx));
-        const size_t gl = (size_t)(j * nx + i), gr = (size_t)((j + 1) * nx + i);
+        // AssembleMicroFluxResidual (mod_Residual.f90:60-76) and stream_h = res/dt (:81-95)
         const double area_inv = 1.0 / P.area;
-#pragma unroll
-        for (int m = 0; m < 4; ++m)
-            resw[m] = (B.fxw[fl * 4 + m] - B.fxw[fr * 4 + m] + B.fyw[gl * 4 + m] - B.fyw[gr * 4 + m]) / P.area;
         const double dti = 1.0 / dt;
 #pragma unroll
         for (int m = 0; m < 6; ++m) acc[m] = 0.0;
@@ -590,7 +638,7 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
             const double wk = s.ok ? B.w[k] : 0.0;
             const double sh = (B.fxh[fl * nv + k] - B.fxh[fr * nv + k] + B.fyh[gl * nv + k] - B.fyh[gr * nv + k]) * area_inv;
             const double sb = (B.fxb[fl * nv + k] - B.fxb[fr * nv + k] + B.fyb[gl * nv + k] - B.fyb[gr * nv + k]) * area_inv;
-            rh[r] = sh * dti;   // stream_h
+            rh[r] = sh * dti;
             rb[r] = sb * dti;
             moment_add(wk, B.u[k], B.v[k], rh[r], rb[r], acc);
             acc[4] = fmax(acc[4], s.ok ? fabs(h[r]) : 0.0);
@@ -598,9 +646,9 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
         }
         block_reduce<4, 2>(acc, red, rout);
         // EnforceStreamingMomentCompatibility (mod_ImplicitMicro.f90:293-306): stream onto rate_w
-        double rate[4], rhs[4], lam[4];
+        double mom[4];
 #pragma unroll
-        for (int m = 0; m < 4; ++m) { rate[m] = resw[m] * dti; rhs[m] = rate[m] - acc[m]; }
+        for (int m = 0; m < 4; ++m) mom[m] = acc[m];
         const double sh_ = fmax(acc[4], 1.0), sb_ = fmax(acc[5], 1.0);
 #pragma unroll
         for (int m = 0; m < 10; ++m) acc[m] = 0.0;
@@ -610,14 +658,21 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
             const double wk = s.ok ? B.w[s.kk] : 0.0;
             gram_add(wk, fmax(fabs(h[r]), kEps * sh_), fmax(fabs(b[r]), kEps * sb_), B.u[s.kk], B.v[s.kk], acc);
         }
-        block_reduce<10, 0>(acc, red, rout);
-        bool pok;
-        {
-            double gm[16];
-            gram_expand(acc, gm);
-            pok = solve_dense4(gm, rhs, lam);
+        block_reduce_smem<10, 0>(acc, red, rout);
+        if (tid == 0) {
+            double rhs[4], gm[16], lam[4];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) rhs[m] = sc[8 + m] * dti - mom[m];
+            gram_expand(rout, gm);
+            const bool pok = solve_dense4(gm, rhs, lam);
+#pragma unroll
+            for (int m = 0; m < 4; ++m) sc[24 + m] = pok ? lam[m] : 0.0;
+            sc[40] = pok ? 0.0 : 1.0;
         }
-        if (!pok) lam[0] = lam[1] = lam[2] = lam[3] = 0.0;
+        __syncthreads();
+        double lam[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) lam[m] = sc[24 + m];
 #pragma unroll
         for (int m = 0; m < 4; ++m) acc[m] = 0.0;
 #pragma unroll
@@ -631,13 +686,16 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
             rh[r] = rh[r] * dt;   // res_h_flux_store = stream_h * dt (mod_Residual.f90:114-115)
             rb[r] = rb[r] * dt;
         }
-        block_reduce<4, 0>(acc, red, rout);
+        block_reduce_smem<4, 0>(acc, red, rout);
         if (tid == 0) {
+            double rate[4];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) rate[m] = sc[8 + m] * dti;
             const double rs = fmax(fmax(fmax(fabs(rate[0]), fabs(rate[1])), fmax(fabs(rate[2]), fabs(rate[3]))), 1.0);
             double err = 0.0;
 #pragma unroll
-            for (int m = 0; m < 4; ++m) err = fmax(err, fabs(acc[m] - rate[m]));
-            if (!pok || !(err <= 1.0e-10 * rs)) set_status(B.status, ST_PROJECTION);
+            for (int m = 0; m < 4; ++m) err = fmax(err, fabs(rout[m] - rate[m]));
+            if (sc[40] != 0.0 || !(err <= 1.0e-10 * rs)) set_status(B.status, ST_PROJECTION);
         }
         if (MODE == MODE_RESIDUAL) {
 #pragma unroll
@@ -647,11 +705,10 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
                 B.res_h[(size_t)c * nv + s.k] = rh[r];
                 B.res_b[(size_t)c * nv + s.k] = rb[r];
             }
-            if (tid < 4) B.res_w[c * 4 + tid] = resw[tid];
+            if (tid < 4) B.res_w[c * 4 + tid] = sc[8 + tid];
         }
     } else {
-#pragma unroll
-        for (int m = 0; m < 4; ++m) resw[m] = B.res_w[c * 4 + m];
+        __syncthreads();   // the scalars written above
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
             const Slot s = slot(r, nv);
@@ -662,21 +719,18 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
 
     if (MODE == MODE_RESIDUAL && COLLISION) {
         // physical equilibrium and collision (mod_Residual.f90:116-127)
-        Prim p;
-        double tau = 1.0;
-        const bool ok = get_primary(P.gm1, Wold, p);
-        const bool tok = ok && get_tau(P.mu_ref, P.omega, p, tau);
-        if (!ok) { p.r = 1.0; p.U = p.V = 0.0; p.L = 1.0; }
-        if (!tok) tau = 1.0;
-        if (tid == 0 && !(ok && tok)) set_status(B.status, ok ? ST_TAU : ST_GETPRIMARY);
+        const Prim p{sc[0], sc[1], sc[2], sc[3]};
+        const double tau = sc[4];
+        if (tid == 0 && sc[5] == 0.0) set_status(B.status, ST_GETPRIMARY);
         acc[0] = acc[1] = 0.0;
 #pragma unroll
         for (int r = 0; r < VPT; ++r) {
             const Slot s = slot(r, nv);
             const double wk = s.ok ? B.w[s.kk] : 0.0;
             const double dvn = B.u[s.kk] - p.U, dvt = B.v[s.kk] - p.V, v2 = dvn * dvn + dvt * dvt;
-            acc[0] += 0.5 * wk * dvn * (v2 * h[r] + b[r]);
-            acc[1] += 0.5 * wk * dvt * (v2 * h[r] + b[r]);
+            const double t = 0.5 * wk * (v2 * h[r] + b[r]);
+            acc[0] += t * dvn;
+            acc[1] += t * dvt;
         }
         block_reduce<2, 0>(acc, red, rout);
         const double q0 = acc[0], q1 = acc[1];
@@ -706,17 +760,21 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
             moment_add(wk, B.u[s.kk], B.v[s.kk], E[r], F[r], acc);
             gram_add(wk, fmax(fabs(E[r]), kEps * se), fmax(fabs(F[r]), kEps * sf), B.u[s.kk], B.v[s.kk], acc + 4);
         }
-        block_reduce<14, 0>(acc, red, rout);
-        double lam[4];
-        bool pok;
-        {
-            double rhs[4], gm[16];
+        block_reduce_smem<14, 0>(acc, red, rout);
+        if (tid == 0) {
+            double rhs[4], gm[16], lam[4];
 #pragma unroll
-            for (int m = 0; m < 4; ++m) rhs[m] = Wold[m] - acc[m];
-            gram_expand(acc + 4, gm);
-            pok = solve_dense4(gm, rhs, lam);
+            for (int m = 0; m < 4; ++m) rhs[m] = B.W[c * 4 + m] - rout[m];
+            gram_expand(rout + 4, gm);
+            const bool pok = solve_dense4(gm, rhs, lam);
+#pragma unroll
+            for (int m = 0; m < 4; ++m) sc[36 + m] = pok ? lam[m] : 0.0;
+            if (!pok) set_status(B.status, ST_PROJECTION);
         }
-        if (!pok) lam[0] = lam[1] = lam[2] = lam[3] = 0.0;
+        __syncthreads();
+        double lam[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) lam[m] = sc[36 + m];
 #pragma unroll
         for (int m = 0; m < 4; ++m) acc[m] = 0.0;
 #pragma unroll
@@ -733,29 +791,22 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
                 B.pcol_b[(size_t)c * nv + s.k] = (Fp - b[r]) / tau;
             }
         }
-        block_reduce<4, 0>(acc, red, rout);
+        block_reduce_smem<4, 0>(acc, red, rout);
         if (tid == 0) {
-            const double rs = fmax(fmax(fmax(fabs(Wold[0]), fabs(Wold[1])), fmax(fabs(Wold[2]), fabs(Wold[3]))), 1.0);
+            const double* Wo = B.W + c * 4;
+            const double rs = fmax(fmax(fmax(fabs(Wo[0]), fabs(Wo[1])), fmax(fabs(Wo[2]), fabs(Wo[3]))), 1.0);
             double err = 0.0;
 #pragma unroll
-            for (int m = 0; m < 4; ++m) err = fmax(err, fabs(acc[m] - Wold[m]));
-            if (!pok || !(err <= 1.0e-10 * rs)) set_status(B.status, ST_PROJECTION);
+            for (int m = 0; m < 4; ++m) err = fmax(err, fabs(rout[m] - Wo[m]));
+            if (!(err <= 1.0e-10 * rs)) set_status(B.status, ST_PROJECTION);
         }
     }
     if (!(MODE & MODE_UPDATE)) return;
 
     // ---- ApplyExplicitUpdate (mod_TimeIntegrator.f90:16-134, 235-293)
-    Prim po, pn;
-    double to = 1.0, tn = 1.0, Wn[4];
-    bool ok = get_primary(P.gm1, Wold, po);
-    ok = ok && get_tau(P.mu_ref, P.omega, po, to);
-#pragma unroll
-    for (int m = 0; m < 4; ++m) Wn[m] = Wold[m] + resw[m];
-    bool ok2 = get_primary(P.gm1, Wn, pn);
-    ok2 = ok2 && get_tau(P.mu_ref, P.omega, pn, tn);
-    if (!ok) { po.r = 1.0; po.U = po.V = 0.0; po.L = 1.0; to = 1.0; }
-    if (!ok2) { pn.r = 1.0; pn.U = pn.V = 0.0; pn.L = 1.0; tn = 1.0; }
-    if (tid == 0 && !(ok && ok2)) set_status(B.status, ST_GETPRIMARY);
+    const Prim po{sc[0], sc[1], sc[2], sc[3]}, pn{sc[12], sc[13], sc[14], sc[15]};
+    const double to = sc[4], tn = sc[16];
+    if (tid == 0 && (sc[5] == 0.0 || sc[17] == 0.0)) set_status(B.status, ST_GETPRIMARY);
     // heat flux of the old state (GetHeatFlux_Vec with prim_old)
     acc[0] = acc[1] = 0.0;
 #pragma unroll
@@ -808,22 +859,33 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
         moment_add(wk, uk, vk, Hn[r], Bn[r], acc + 14);
         gram_add(wk, fmax(fabs(Hn[r]), kEps * sHn), fmax(fabs(Bn[r]), kEps * sBn), uk, vk, acc + 18);
     }
-    block_reduce<28, 0>(acc, red, rout);
-    double to4[4], lo[4], ln[4];
-    get_conserved(P.gm1, po, to4);
-    bool pok;
-    {
-        double rhs[4], gm[16];
+    block_reduce_smem<28, 0>(acc, red, rout);
+    // two ProjectToConservedMoments solves (mod_TimeIntegrator.f90:267-274), one per warp
+    if (tid == 0) {
+        double to4[4], rhs[4], gm[16], l[4];
+        get_conserved(P.gm1, po, to4);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) rhs[m] = to4[m] - acc[m];
-        gram_expand(acc + 4, gm);
-        pok = solve_dense4(gm, rhs, lo);
+        for (int m = 0; m < 4; ++m) rhs[m] = to4[m] - rout[m];
+        gram_expand(rout + 4, gm);
+        const bool ok = solve_dense4(gm, rhs, l);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) rhs[m] = Wn[m] - acc[14 + m];
-        gram_expand(acc + 18, gm);
-        pok = solve_dense4(gm, rhs, ln) && pok;
+        for (int m = 0; m < 4; ++m) sc[28 + m] = ok ? l[m] : 0.0;
+        if (!ok) set_status(B.status, ST_PROJECTION);
     }
-    if (!pok) lo[0] = lo[1] = lo[2] = lo[3] = ln[0] = ln[1] = ln[2] = ln[3] = 0.0;
+    if (tid == t1) {
+        double rhs[4], gm[16], l[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) rhs[m] = sc[18 + m] - rout[14 + m];
+        gram_expand(rout + 18, gm);
+        const bool ok = solve_dense4(gm, rhs, l);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) sc[32 + m] = ok ? l[m] : 0.0;
+        if (!ok) set_status(B.status, ST_PROJECTION);
+    }
+    __syncthreads();
+    double lo[4], ln[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) { lo[m] = sc[28 + m]; ln[m] = sc[32 + m]; }
     const double inv = 1.0 / (1.0 + 0.5 * dt / tn);
 #pragma unroll
     for (int m = 0; m < 8; ++m) acc[m] = 0.0;
@@ -844,13 +906,17 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
             B.b[(size_t)c * nv + s.k] = bnew;
         }
     }
-    block_reduce<8, 0>(acc, red, rout);
+    block_reduce_smem<8, 0>(acc, red, rout);
     if (tid == 0) {
+        double to4[4], Wn[4], Wold[4];
+        get_conserved(P.gm1, po, to4);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { Wn[m] = sc[18 + m]; Wold[m] = B.W[c * 4 + m]; }
         const double ro = fmax(fmax(fmax(fabs(to4[0]), fabs(to4[1])), fmax(fabs(to4[2]), fabs(to4[3]))), 1.0);
         const double rn = fmax(fmax(fmax(fabs(Wn[0]), fabs(Wn[1])), fmax(fabs(Wn[2]), fabs(Wn[3]))), 1.0);
         double eo = 0.0, en = 0.0;
-        for (int m = 0; m < 4; ++m) { eo = fmax(eo, fabs(acc[m] - to4[m])); en = fmax(en, fabs(acc[4 + m] - Wn[m])); }
-        if (!pok || !(eo <= 1.0e-10 * ro) || !(en <= 1.0e-10 * rn)) set_status(B.status, ST_PROJECTION);
+        for (int m = 0; m < 4; ++m) { eo = fmax(eo, fabs(rout[m] - to4[m])); en = fmax(en, fabs(rout[4 + m] - Wn[m])); }
+        if (!(eo <= 1.0e-10 * ro) || !(en <= 1.0e-10 * rn)) set_status(B.status, ST_PROJECTION);
         bool fin = true;
         for (int m = 0; m < 4; ++m) { B.W[c * 4 + m] = Wn[m]; fin = fin && isfinite(Wn[m]); }
         if (!fin) set_status(B.status, ST_NONFINITE_STATE);
@@ -863,8 +929,7 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_cells(LoParams P, LoB
             dg[9 + m] = fabs(d);
         }
         dg[8] = P.area * P.area;
-        bool dok;
-        B.dtl[c] = cell_dt(P, Wn, dok);
+        B.dtl[c] = sc[22];
     }
     last_cta_epilogue(P, B, true, true, red, rout);
 }
@@ -937,8 +1002,8 @@ int lo_threads(int nvel) {
 }
 
 cudaError_t launch_lo_slopes(const LoParams& P, const LoBuffers& B, cudaStream_t s) {
-    const size_t n = (size_t)P.nx * P.ny * P.nvel;
-    k_lo_slopes<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(P, B);
+    const dim3 grid((unsigned)((P.nvel + 255) / 256), (unsigned)(P.nx * P.ny));
+    k_lo_slopes<<<grid, 256, 0, s>>>(P, B);
     return cudaGetLastError();
 }
 
