@@ -56,6 +56,7 @@ def lib():
         L.uo_compute_residual.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.uo_apply_explicit_update.argtypes = [ctypes.c_void_p, ctypes.c_double, dp]
         L.uo_implicit_step.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
+        L.uo_implicit_init.argtypes = [ctypes.c_void_p]
         for name in ("uo_res_macro", "uo_res_h", "uo_res_b", "uo_wall_aero", "uo_face_x_h", "uo_face_y_h",
                      "uo_face_x_w", "uo_face_y_w", "uo_phys_eq_h", "uo_phys_col_h", "uo_phys_col_b"):
             f = getattr(L, name)
@@ -134,7 +135,12 @@ class Oracle:
             raise RuntimeError(f"oracle explicit step aborted with reference code {e}")
         return float(dt[0]), res
 
-    def implicit_step(self, nout=64):
+    def implicit_init(self):
+        e = lib().uo_implicit_init(self.ptr)
+        if e:
+            raise RuntimeError(f"oracle implicit init failed: {e}")
+
+    def implicit_step(self, nout=80):
         out = np.zeros(nout)
         e = lib().uo_implicit_step(self.ptr, _p(out), nout)
         if e:

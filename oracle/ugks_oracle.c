@@ -37,6 +37,19 @@ struct uo_ctx {
     double *wall_aero;            /* [2][nx][3] */
     double *cell_diag;            /* [nc][13] per-cell residual-norm terms, summed in cell order */
     int *cell_err;                /* [nc] per-cell status */
+    /* ImplicitSteady state (mod_ImplicitState.f90) */
+    double *dw, *dw_ghost;        /* delta_w [nc][4] and its halo snapshot from the last exchange */
+    double *wt, *tau_t;           /* w_tilde [nc][4], tau_tilde [nc] */
+    double *eq_h, *eq_b;          /* predicted equilibrium [nc][nvel] */
+    double *dh, *db;              /* delta_h, delta_b [nc][nvel] */
+    double *dh_ghost, *db_ghost;  /* halo snapshot of delta_h, delta_b */
+    double *save_h, *save_b, *save_W;
+    double ref_h, ref_b;          /* first-evaluation micro residual references */
+    int ref_init;
+    double m0;                    /* closed_mass_target (persistent M0) */
+    double mass_scale;
+    int streak;
+    double dt;
     /* scratch: 24 work vectors per OpenMP thread */
     int nthr;
     double **tt;
@@ -361,6 +374,20 @@ uo_ctx* uo_create(const uo_params* p, const double* u, const double* v, const do
     c->wall_aero = (double*)calloc((size_t)2 * nx * 3, sizeof(double));
     c->cell_diag = (double*)calloc((size_t)c->nc * 13, sizeof(double));
     c->cell_err = (int*)calloc((size_t)c->nc, sizeof(int));
+    c->dw = (double*)calloc((size_t)c->nc * 4, sizeof(double));
+    c->dw_ghost = (double*)calloc((size_t)c->nc * 4, sizeof(double));
+    c->wt = (double*)calloc((size_t)c->nc * 4, sizeof(double));
+    c->tau_t = (double*)calloc((size_t)c->nc, sizeof(double));
+    c->eq_h = (double*)calloc(S, sizeof(double));
+    c->eq_b = (double*)calloc(S, sizeof(double));
+    c->dh = (double*)calloc(S, sizeof(double));
+    c->db = (double*)calloc(S, sizeof(double));
+    c->dh_ghost = (double*)calloc(S, sizeof(double));
+    c->db_ghost = (double*)calloc(S, sizeof(double));
+    c->save_h = (double*)calloc(S, sizeof(double));
+    c->save_b = (double*)calloc(S, sizeof(double));
+    c->save_W = (double*)calloc((size_t)c->nc * 4, sizeof(double));
+    c->mass_scale = 1.0;
     c->nthr = MAX_THREADS < host_cores() ? MAX_THREADS : host_cores();
     c->tt = (double**)calloc((size_t)c->nthr * NSCR, sizeof(double*));
     for (int i = 0; i < c->nthr * NSCR; ++i) c->tt[i] = (double*)calloc(nv, sizeof(double));
@@ -377,6 +404,9 @@ void uo_destroy(uo_ctx* c) {
     free(c->tt);
     free(c->cell_diag);
     free(c->cell_err);
+    double* extra[] = {c->dw, c->dw_ghost, c->wt, c->tau_t, c->eq_h, c->eq_b, c->dh, c->db, c->dh_ghost, c->db_ghost,
+                       c->save_h, c->save_b, c->save_W};
+    for (size_t i = 0; i < sizeof(extra) / sizeof(extra[0]); ++i) free(extra[i]);
     free(c);
 }
 
@@ -971,4 +1001,516 @@ int uo_explicit_step(uo_ctx* c, double* dt_out, double* res_out) {
     e = uo_compute_residual(c, dt, 0);
     if (e) return e;
     return uo_apply_explicit_update(c, dt, res_out);
+}
+
+/* ================================================================== ImplicitSteady
+ * mod_SteadyImplicit.f90:379-462 with the closed-Couette mass rescale (mod_ClosedCouetteMass.f90)
+ * and the accepted-state re-evaluation (mod_R5Observe.f90:287-358).  The reference runs on NP_Y
+ * ranks stacked in y (nslab here); PR(2) and LU-SGS are Gauss-Seidel inside a rank and read the
+ * other ranks' corrections (and the x-periodic self-exchange) from halos refreshed only at the
+ * exchange points, so the emulation keeps a halo snapshot (dw_ghost, dh_ghost) refreshed at
+ * exactly those points. */
+
+static int uo_is_physical(const double w[4]) {            /* IsPhysicalState (mod_ImplicitCommon.f90:10-20) */
+    for (int m = 0; m < 4; ++m) if (!isfinite(w[m])) return 0;
+    if (w[0] <= 0.0) return 0;
+    double e = w[3] - 0.5 * (w[1] * w[1] + w[2] * w[2]) / w[0];
+    return isfinite(e) && e > 0.0;
+}
+
+static void euler_flux(double gamma, const double w[4], double nx, double ny, double f[4]) {   /* EulerFluxNormal */
+    double u = w[1] / w[0], v = w[2] / w[0], un = u * nx + v * ny;
+    double p = (gamma - 1.0) * (w[3] - 0.5 * (w[1] * w[1] + w[2] * w[2]) / w[0]);
+    f[0] = w[0] * un;
+    f[1] = w[1] * un + p * nx;
+    f[2] = w[2] * un + p * ny;
+    f[3] = (w[3] + p) * un;
+}
+
+static void zhu_map(const double w[4], double uw, double vw, double g[4]) {  /* ZhuMovingWallMap (mod_ImplicitBoundary.f90:187-194) */
+    g[0] = w[0];
+    g[1] = 2.0 * uw * w[0] - w[1];
+    g[2] = 2.0 * vw * w[0] - w[2];
+    g[3] = w[3] + 2.0 * (uw * uw + vw * vw) * w[0] - 2.0 * uw * w[1] - 2.0 * vw * w[2];
+}
+
+static int slab_rows(const uo_ctx* c) { return c->p.ny / (c->p.nslab > 0 ? c->p.nslab : 1); }
+static int same_slab(const uo_ctx* c, int j0, int j1) { return j0 / slab_rows(c) == j1 / slab_rows(c); }
+
+/* Face geometry of GetFaceGeometry (mod_ImplicitMacro.f90:236-263): face 0..3 = left, right,
+ * bottom, top; outward normal, face length, neighbour cell, and whether the neighbour is read from
+ * the halo (other rank or the x-periodic self-exchange) or is a physical wall. */
+typedef struct { double nx, ny, len; int nb; int ghost; int wall; double dist; } face_geo;
+
+static face_geo uo_face(const uo_ctx* c, int i, int j, int f) {
+    const uo_params* p = &c->p;
+    face_geo g;
+    int nx = p->nx, ny = p->ny;
+    double xi = (i + 0.5) * p->dx, yj = (j + 0.5) * p->dy;
+    g.wall = 0; g.ghost = 0;
+    if (f == 0) {
+        g.nx = -1.0; g.ny = 0.0; g.len = p->dy;
+        int ni = i - 1; g.ghost = ni < 0; if (ni < 0) ni += nx;
+        g.nb = j * nx + ni;
+        /* ghost centres on the outer ranks are re-extrapolated after the periodic copy
+         * (mod_InitializeFlow.f90:418-446), so the seam distance is one cell as well */
+        g.dist = fabs(((i - 1 + 0.5) * p->dx - xi) * g.nx + 0.0);
+    } else if (f == 1) {
+        g.nx = 1.0; g.ny = -0.0; g.len = p->dy;
+        int ni = i + 1; g.ghost = ni >= nx; if (ni >= nx) ni -= nx;
+        g.nb = j * nx + ni;
+        g.dist = fabs(((i + 1 + 0.5) * p->dx - xi) * g.nx + 0.0);
+    } else if (f == 2) {
+        g.nx = 0.0; g.ny = -1.0; g.len = p->dx;
+        if (j == 0) { g.wall = 1; g.nb = -1; g.dist = p->dy; }
+        else { g.nb = (j - 1) * nx + i; g.ghost = !same_slab(c, j, j - 1); g.dist = fabs(0.0 + (((j - 1) + 0.5) * p->dy - yj) * g.ny); }
+    } else {
+        g.nx = -0.0; g.ny = 1.0; g.len = p->dx;
+        if (j == ny - 1) { g.wall = 1; g.nb = -1; g.dist = p->dy; }
+        else { g.nb = (j + 1) * nx + i; g.ghost = !same_slab(c, j, j + 1); g.dist = fabs(0.0 + (((j + 1) + 0.5) * p->dy - yj) * g.ny); }
+    }
+    return g;
+}
+
+/* ImplicitSpectralRadius (mod_ImplicitMacro.f90:15-55) */
+static double spectral_radius(const uo_ctx* c, const double wi[4], const double wj[4], const face_geo* g) {
+    const uo_params* p = &c->p;
+    double pi_[4], pj[4], ti, tj;
+    if (get_primary(p, wi, pi_) || get_primary(p, wj, pj)) return NAN;
+    double rho_avg = 0.5 * (pi_[0] + pj[0]);
+    double u_avg = 0.5 * (pi_[1] + pj[1]);
+    double v_avg = 0.5 * (pi_[2] + pj[2]);
+    double p_i = 0.5 * pi_[0] / pi_[3], p_j = 0.5 * pj[0] / pj[3];
+    double p_avg = 0.5 * (p_i + p_j);
+    if (get_tau(p, pi_, &ti) || get_tau(p, pj, &tj)) return NAN;
+    double mu_avg = 0.5 * (ti * p_i + tj * p_j);
+    double sos = sqrt(p->gamma * p_avg / rho_avg);
+    return fabs(u_avg * g->nx + v_avg * g->ny) + sos + 2.0 * mu_avg / (rho_avg * fmax(g->dist, 1000.0 * DBL_EPSILON));
+}
+
+/* RelaxMacroPoint (mod_ImplicitMacro.f90:90-123) */
+static int relax_macro(uo_ctx* c, int i, int j, double dt_pseudo) {
+    const uo_params* p = &c->p;
+    int cc = j * p->nx + i;
+    double sdt[4] = {0, 0, 0, 0}, sgn[4] = {0, 0, 0, 0}, sg = 0.0;
+    for (int f = 0; f < 4; ++f) {
+        face_geo g = uo_face(c, i, j, f);
+        const double* wi = c->W + cc * 4;
+        double wj[4], dnb[4], fn[4], fo[4], dti[4], dtj[4], t[4];
+        if (g.wall) {
+            double uw = p->wall_ux[f == 2 ? 0 : 1], vw = 0.0;
+            zhu_map(wi, uw, vw, wj);
+            zhu_map(c->dw + cc * 4, uw, vw, dnb);
+        } else {
+            memcpy(wj, c->W + g.nb * 4, sizeof wj);
+            memcpy(dnb, (g.ghost ? c->dw_ghost : c->dw) + g.nb * 4, sizeof dnb);
+        }
+        for (int m = 0; m < 4; ++m) t[m] = wi[m] + c->dw[cc * 4 + m];
+        euler_flux(p->gamma, t, g.nx, g.ny, fn);
+        euler_flux(p->gamma, wi, g.nx, g.ny, fo);
+        for (int m = 0; m < 4; ++m) dti[m] = fn[m] - fo[m];
+        for (int m = 0; m < 4; ++m) t[m] = wj[m] + dnb[m];
+        euler_flux(p->gamma, t, g.nx, g.ny, fn);
+        euler_flux(p->gamma, wj, g.nx, g.ny, fo);
+        for (int m = 0; m < 4; ++m) dtj[m] = fn[m] - fo[m];
+        double gam = spectral_radius(c, wi, wj, &g);
+        if (!isfinite(gam) || !(gam > 0.0)) return 0;
+        for (int m = 0; m < 4; ++m) {
+            double s = dti[m] + dtj[m];
+            if (!isfinite(s)) return 0;
+            sdt[m] = sdt[m] + g.len * s;
+            sgn[m] = sgn[m] + g.len * gam * dnb[m];
+        }
+        sg = sg + g.len * gam;
+    }
+    double diag = 1.0 / dt_pseudo + 0.5 * sg / c->area;
+    double rhs[4];
+    for (int m = 0; m < 4; ++m)
+        rhs[m] = c->rate_w[cc * 4 + m] - 0.5 * 1.0 * sdt[m] / c->area + 0.5 * 1.0 * sgn[m] / c->area;
+    if (!(isfinite(diag) && diag > 0.0)) return 0;
+    for (int m = 0; m < 4; ++m) if (!isfinite(rhs[m])) return 0;
+    for (int m = 0; m < 4; ++m) c->dw[cc * 4 + m] = rhs[m] / diag;
+    return 1;
+}
+
+/* SolveMacroPR2 (mod_ImplicitMacro.f90:57-88) over nslab ranks */
+static int solve_macro_pr2(uo_ctx* c, double dt_pseudo) {
+    const uo_params* p = &c->p;
+    int rows = slab_rows(c), nx = p->nx;
+    memcpy(c->dw_ghost, c->dw, sizeof(double) * c->nc * 4);    /* MPIExchangeDeltaMacro */
+    for (int sweep = 0; sweep < p->macro_sweeps; ++sweep) {
+        for (int s = 0; s < p->nslab; ++s) {
+            for (int j = s * rows; j < (s + 1) * rows; ++j)
+                for (int i = 0; i < nx; ++i) if (!relax_macro(c, i, j, dt_pseudo)) return 0;
+            for (int j = (s + 1) * rows - 1; j >= s * rows; --j)
+                for (int i = nx - 1; i >= 0; --i) if (!relax_macro(c, i, j, dt_pseudo)) return 0;
+        }
+        memcpy(c->dw_ghost, c->dw, sizeof(double) * c->nc * 4);
+    }
+    for (int m = 0; m < c->nc * 4; ++m) if (!isfinite(c->dw[m])) return 0;
+    return 1;
+}
+
+/* ComputeDiffuseWallFaceDelta (mod_ImplicitBoundary.f90:282-326) for the wall face of cell cc:
+ * returns delta_rho (the reflected face correction is delta_rho * h_unit for vn < 0). */
+static int wall_delta_rho(uo_ctx* c, int cc, int top, double* drho) {
+    const uo_params* p = &c->p;
+    int nv = p->nvel;
+    double nxo = top ? -0.0 : 0.0, nyo = top ? 1.0 : -1.0;
+    double bc[4] = {1.0, p->wall_ux[top], 0.0, 1.0 / p->wall_tnative[top]}, pl[4];
+    local_frame(bc, nxo, nyo, pl);
+    pl[0] = 1.0;
+    double inc = 0.0, refl = 0.0, outs = 0.0;
+    for (int k = 0; k < nv; ++k) {
+        double vn = c->u[k] * nxo + c->v[k] * nyo, vt = -c->u[k] * nyo + c->v[k] * nxo;
+        double sel = vn < 0.0 ? 1.0 : 0.0;
+        double dvn = vn - pl[1], dvt = vt - pl[2];
+        double hu = pl[0] * (pl[3] / PI_D) * exp(-pl[3] * (dvn * dvn + dvt * dvt));
+        inc += c->w[k] * vn * c->dh[(size_t)cc * nv + k] * (1.0 - sel);
+        refl += c->w[k] * vn * hu * sel;
+        outs += fabs(c->w[k] * vn * hu * sel);
+    }
+    if (fabs(refl) <= 1000.0 * DBL_EPSILON * fmax(outs, DBL_MIN)) return 0;
+    *drho = -inc / refl;
+    return 1;
+}
+
+/* One LU-SGS stage over one slab (SolveMicroLUSGS / RelaxMicroPoint, mod_ImplicitMicro.f90:366-487) */
+static int lusgs_stage(uo_ctx* c, int s, int backward, double dt_pseudo) {
+    const uo_params* p = &c->p;
+    int nv = p->nvel, nx = p->nx, ny = p->ny, rows = slab_rows(c);
+    for (int jj = 0; jj < rows; ++jj) {
+        int j = backward ? (s + 1) * rows - 1 - jj : s * rows + jj;
+        for (int ii = 0; ii < nx; ++ii) {
+            int i = backward ? nx - 1 - ii : ii;
+            int cc = j * nx + i;
+            /* frozen wall closure from this cell's correction at the start of its velocity loop */
+            double drho[2] = {0.0, 0.0};
+            int haswall[2] = {j == 0, j == ny - 1};
+            for (int t = 0; t < 2; ++t)
+                if (haswall[t] && !wall_delta_rho(c, cc, t, &drho[t])) return 0;
+            face_geo g[4];
+            for (int f = 0; f < 4; ++f) g[f] = uo_face(c, i, j, f);
+            for (int kk = 0; kk < nv; ++kk) {
+                int k = backward ? nv - 1 - kk : kk;
+                size_t q = (size_t)cc * nv + k;
+                double rhs_h = c->stream_h[q] + (c->eq_h[q] - c->h[q]) / c->tau_t[cc];
+                double rhs_b = c->stream_b[q] + (c->eq_b[q] - c->b[q]) / c->tau_t[cc];
+                double diag = 1.0 / dt_pseudo + 1.0 / c->tau_t[cc];
+                for (int f = 0; f < 4; ++f) {
+                    double un = c->u[k] * g[f].nx + c->v[k] * g[f].ny;
+                    double nh, nb;
+                    if (g[f].wall) {
+                        int top = f == 3;
+                        double nxo = top ? -0.0 : 0.0, nyo = top ? 1.0 : -1.0;
+                        double vn = c->u[k] * nxo + c->v[k] * nyo, vt = -c->u[k] * nyo + c->v[k] * nxo;
+                        double bc[4] = {1.0, p->wall_ux[top], 0.0, 1.0 / p->wall_tnative[top]}, pl[4];
+                        local_frame(bc, nxo, nyo, pl);
+                        double dvn = vn - pl[1], dvt = vt - pl[2];
+                        double hu = 1.0 * (pl[3] / PI_D) * exp(-pl[3] * (dvn * dvn + dvt * dvt));
+                        double bu = hu * ((double)p->ck / (2.0 * pl[3]));
+                        double sel = vn < 0.0 ? 1.0 : 0.0;
+                        nh = drho[top] * hu * sel + c->dh[q] * (1.0 - sel);
+                        nb = drho[top] * bu * sel + c->db[q] * (1.0 - sel);
+                    } else {
+                        size_t qn = (size_t)g[f].nb * nv + k;
+                        nh = g[f].ghost ? c->dh_ghost[qn] : c->dh[qn];
+                        nb = g[f].ghost ? c->db_ghost[qn] : c->db[qn];
+                    }
+                    diag = diag + 1.0 * fmax(un, 0.0) * g[f].len / c->area;
+                    rhs_h = rhs_h - 1.0 * fmin(un, 0.0) * g[f].len * nh / c->area;
+                    rhs_b = rhs_b - 1.0 * fmin(un, 0.0) * g[f].len * nb / c->area;
+                }
+                if (!(diag > 0.0 && isfinite(diag) && isfinite(rhs_h) && isfinite(rhs_b))) return 0;
+                c->dh[q] = rhs_h / diag;
+                c->db[q] = rhs_b / diag;
+            }
+        }
+    }
+    return 1;
+}
+
+/* UpdateImplicitResidualDiagnostics (mod_ImplicitDiagnostics.f90:223-322); sci[22] = SciencePack
+ * (mod_R5Observe.f90:27-32) plus r5 raw values; sums taken per slab then over slabs. */
+static void implicit_diagnostics(uo_ctx* c, double dt, double sci[22]) {
+    const uo_params* p = &c->p;
+    int nv = p->nvel, nx = p->nx, rows = slab_rows(c);
+    double num[4] = {0}, den[4] = {0}, wgt = 0, mic[4] = {0}, mass = 0;
+    for (int s = 0; s < p->nslab; ++s) {
+        double ln[4] = {0}, ld[4] = {0}, lw = 0, lm[4] = {0}, lmass = 0;
+        for (int j = s * rows; j < (s + 1) * rows; ++j)
+            for (int i = 0; i < nx; ++i) {
+                int cc = j * nx + i;
+                for (int m = 0; m < 4; ++m) {
+                    double a = c->area * c->rate_w[cc * 4 + m];
+                    ln[m] = ln[m] + a * a;
+                    ld[m] = ld[m] + c->area * fabs(c->W[cc * 4 + m] + dt * c->rate_w[cc * 4 + m]);
+                }
+                lw = lw + c->area * c->area;
+                double s3 = 0.0, s4 = 0.0;
+                for (int k = 0; k < nv; ++k) {
+                    size_t q = (size_t)cc * nv + k;
+                    double dh = c->stream_h[q] + c->pcol_h[q], db = c->stream_b[q] + c->pcol_b[q];
+                    lm[0] = lm[0] + c->area * c->w[k] * dh * dh;
+                    lm[1] = lm[1] + c->area * c->w[k] * db * db;
+                    s3 += c->w[k] * fmax(c->h[q] * c->h[q], c->peq_h[q] * c->peq_h[q]);
+                    s4 += c->w[k] * fmax(c->b[q] * c->b[q], c->peq_b[q] * c->peq_b[q]);
+                }
+                lm[2] = lm[2] + c->area * s3;
+                lm[3] = lm[3] + c->area * s4;
+                lmass = lmass + c->rate_w[cc * 4] * c->area;
+            }
+        for (int m = 0; m < 4; ++m) { num[m] += ln[m]; den[m] += ld[m]; mic[m] += lm[m]; }
+        wgt += lw; mass += lmass;
+    }
+    double rel[4], absr[4], res[4];
+    double ncell = (double)(p->nx * p->ny);
+    for (int m = 0; m < 4; ++m) {
+        rel[m] = sqrt(ncell * num[m]) / (den[m] + SMV);
+        absr[m] = sqrt(num[m] / fmax(wgt, SMV));
+    }
+    double raw_h = sqrt(mic[0]), raw_b = sqrt(mic[1]);
+    double ords = fmax(fmax(den[0], den[3]), SMV);
+    for (int m = 0; m < 4; ++m) res[m] = (den[m] <= sqrt(DBL_EPSILON) * fmax(ords, DBL_MIN)) ? absr[m] : rel[m];
+    double h_raw = sqrt(mic[0] / fmax(mic[2], SMV)), b_raw = sqrt(mic[1] / fmax(mic[3], SMV));
+    if (!c->ref_init) { c->ref_h = h_raw; c->ref_b = b_raw; c->ref_init = 1; }
+    double h_rel = c->ref_h > DBL_MIN ? h_raw / c->ref_h : h_raw;
+    double b_rel = c->ref_b > DBL_MIN ? b_raw / c->ref_b : b_raw;
+    double nzr = fmax(100.0 * p->residual_tol, 1000.0 * DBL_EPSILON);
+    double h_norm = c->ref_h <= nzr ? h_raw : h_raw / c->ref_h;
+    double b_norm = c->ref_b <= nzr ? b_raw : b_raw / c->ref_b;
+    for (int m = 0; m < 4; ++m) { sci[m] = res[m]; sci[4 + m] = rel[m]; sci[8 + m] = absr[m]; }
+    sci[12] = h_norm; sci[13] = b_norm; sci[14] = h_rel; sci[15] = b_rel; sci[16] = h_raw; sci[17] = b_raw;
+    sci[18] = 0.0;   /* implicit_moment_error: filled by the caller */
+    sci[19] = fabs(mass); sci[20] = raw_h; sci[21] = raw_b;
+}
+
+/* MassStatistics (mod_ClosedCouetteMass.f90:173-204): totals[5], metrics[5] */
+static int mass_statistics(uo_ctx* c, double totals[5], double metrics[5]) {
+    const uo_params* p = &c->p;
+    int nv = p->nvel, nx = p->nx, rows = slab_rows(c);
+    int ok = 1;
+    double t[5] = {0}, mx[3] = {0}, mn[2] = {INFINITY, INFINITY};
+    for (int s = 0; s < p->nslab; ++s) {
+        double lt[5] = {0};
+        for (int j = s * rows; j < (s + 1) * rows; ++j)
+            for (int i = 0; i < nx; ++i) {
+                int cc = j * nx + i;
+                double mm[4];
+                const double *h = c->h + (size_t)cc * nv, *b = c->b + (size_t)cc * nv, *W = c->W + cc * 4;
+                moment_conserved(nv, h, b, c->u, c->v, c->w, mm);
+                for (int k = 0; k < nv; ++k) ok &= isfinite(h[k]) && isfinite(b[k]);
+                ok &= uo_is_physical(W) && uo_is_physical(mm);
+                for (int m = 0; m < 4; ++m) lt[m] = lt[m] + c->area * W[m];
+                lt[4] = lt[4] + c->area * mm[0];
+                double e1 = 0.0;
+                for (int m = 0; m < 4; ++m) e1 = fmax(e1, fabs(W[m] - mm[m]) / fmax(fabs(W[m]), 1.0));
+                mx[0] = fmax(mx[0], e1);
+                double nh1 = 0, nh2 = 0, nb1 = 0, nb2 = 0;
+                for (int k = 0; k < nv; ++k) {
+                    nh1 += c->w[k] * fmax(-h[k], 0.0); nh2 += c->w[k] * fabs(h[k]);
+                    nb1 += c->w[k] * fmax(-b[k], 0.0); nb2 += c->w[k] * fabs(b[k]);
+                }
+                mx[1] = fmax(mx[1], nh1 / fmax(nh2, DBL_MIN));
+                mx[2] = fmax(mx[2], nb1 / fmax(nb2, DBL_MIN));
+                if (isfinite(W[0]) && W[0] > 0.0) {
+                    double e = W[3] - 0.5 * (W[1] * W[1] + W[2] * W[2]) / W[0];
+                    mn[0] = fmin(mn[0], W[0]); mn[1] = fmin(mn[1], e);
+                }
+            }
+        for (int m = 0; m < 5; ++m) t[m] += lt[m];
+    }
+    memcpy(totals, t, sizeof t);
+    metrics[0] = mx[0]; metrics[1] = mx[1]; metrics[2] = mx[2]; metrics[3] = mn[0]; metrics[4] = mn[1];
+    return ok && metrics[0] <= p->moment_tol;
+}
+
+/* AssembleSteadyRateResiduals' rate/stream part run again on the cached residuals (the second call
+ * inside ApplyOriginalSteadyImplicitUpdate, mod_SteadyImplicit.f90:406, and after ComputeResidual
+ * in PhysicalDiagnostic): rate_w, stream_* from res_*, streaming projection, res_* = stream*dt. */
+static int reassemble_rates(uo_ctx* c, double dt) {
+    int nv = c->p.nvel;
+    double dti = 1.0 / dt;
+    int ok = 1;
+    for (int cc = 0; cc < c->nc; ++cc) {
+        for (int m = 0; m < 4; ++m) c->rate_w[cc * 4 + m] = c->res_w[cc * 4 + m] * dti;
+        for (int k = 0; k < nv; ++k) {
+            c->stream_h[(size_t)cc * nv + k] = c->res_h[(size_t)cc * nv + k] * dti;
+            c->stream_b[(size_t)cc * nv + k] = c->res_b[(size_t)cc * nv + k] * dti;
+        }
+        ok &= uo_project_moments(nv, c->stream_h + (size_t)cc * nv, c->stream_b + (size_t)cc * nv, c->rate_w + cc * 4,
+                                 c->u, c->v, c->w, c->h + (size_t)cc * nv, c->b + (size_t)cc * nv);
+        for (int k = 0; k < nv; ++k) {
+            c->res_h[(size_t)cc * nv + k] = c->stream_h[(size_t)cc * nv + k] * dt;
+            c->res_b[(size_t)cc * nv + k] = c->stream_b[(size_t)cc * nv + k] * dt;
+        }
+    }
+    return ok;
+}
+
+/* InitializeClosedMass (mod_ClosedCouetteMass.f90:212-241): persistent M0 of the cold start. */
+int uo_implicit_init(uo_ctx* c) {
+    double t[5], m[5];
+    if (!mass_statistics(c, t, m)) return 941;
+    c->m0 = t[0];
+    c->ref_init = 0;
+    c->streak = 0;
+    c->mass_scale = 1.0;
+    return 0;
+}
+
+/* One accepted ImplicitSteady pseudo-step of Solve_UGKS (mod_Solve.f90:84-293) with
+ * ClosedCouetteMassRescale: out[] = the sparse_residual.csv row of the accepted state
+ * [0] original_gate, [1] moment, [2] M_W, [3] M_h, [4..11] R1..R8, [12..33] science_1..22,
+ * [34..49] flux_1..16, [50] reference_h, [51] reference_b, [52] c_minus_1, then extras:
+ * [53] alpha, [54] macro_alpha, [55] dt, [56] verified streak, [57..78] science of the
+ * pre-update evaluation (the "Implicit iter=" line of the next step prints these). */
+int uo_implicit_step(uo_ctx* c, double* out, int nout) {
+    const uo_params* p = &c->p;
+    int nv = p->nvel, e;
+    double row[80];
+    memset(row, 0, sizeof row);
+    /* TimeStep, Interpolation, Evolution, ComputeResidual (mod_Solve.f90:95-117) */
+    double dt = uo_timestep(c);
+    if (!isfinite(dt)) return 101;
+    c->dt = dt;
+    uo_interpolation(c);
+    if ((e = uo_evolution(c, dt))) return e;
+    if ((e = uo_compute_residual(c, dt, 1))) return e;
+    /* ApplySteadyImplicitUpdate -> ApplyOriginalSteadyImplicitUpdate (mod_SteadyImplicit.f90:379-462) */
+    size_t S = (size_t)c->nc * nv;
+    memcpy(c->save_h, c->h, S * sizeof(double));
+    memcpy(c->save_b, c->b, S * sizeof(double));
+    memcpy(c->save_W, c->W, (size_t)c->nc * 4 * sizeof(double));
+    if (!reassemble_rates(c, dt)) return 444;
+    double sci0[22];
+    implicit_diagnostics(c, dt, sci0);
+    memcpy(row + 57, sci0, sizeof sci0);
+    double dtp = dt * p->ncfl / p->cfl;                     /* PseudoTimeStep */
+    memset(c->dw, 0, sizeof(double) * c->nc * 4);             /* ResetImplicitCorrections */
+    memset(c->dh, 0, S * sizeof(double));
+    memset(c->db, 0, S * sizeof(double));
+    if (!solve_macro_pr2(c, dtp)) return 420;
+    /* BuildPredictedMacroState (mod_ImplicitMacro.f90:159-185) */
+    double malpha = 1.0;
+    for (;;) {
+        int ok = 1;
+        for (int cc = 0; cc < c->nc && ok; ++cc) {
+            double t[4];
+            for (int m = 0; m < 4; ++m) t[m] = c->W[cc * 4 + m] + malpha * c->dw[cc * 4 + m];
+            ok = uo_is_physical(t);
+        }
+        if (ok) break;
+        malpha = 0.5 * malpha;
+        if (malpha < p->min_alpha) return 421;
+    }
+    for (int m = 0; m < c->nc * 4; ++m) c->dw[m] = malpha * c->dw[m];
+    for (int m = 0; m < c->nc * 4; ++m) c->wt[m] = c->W[m] + c->dw[m];
+    /* BuildPredictedEquilibrium (mod_ImplicitMicro.f90:43-88), low-order branch */
+    for (int cc = 0; cc < c->nc; ++cc) {
+        double po[4], pt[4], q[2];
+        if ((e = get_primary(p, c->W + cc * 4, po))) return e;
+        heat_flux(nv, c->h + (size_t)cc * nv, c->b + (size_t)cc * nv, c->u, c->v, c->w, po, q);
+        if ((e = get_primary(p, c->wt + cc * 4, pt))) return e;
+        if ((e = get_tau(p, pt, &c->tau_t[cc]))) return e;
+        double *eh = c->eq_h + (size_t)cc * nv, *eb = c->eq_b + (size_t)cc * nv;
+        double** T = scratch_t(c, 0);
+        maxwell(p, nv, c->u, c->v, pt, eh, eb);
+        shakhov(p, nv, eh, eb, c->u, c->v, q, pt, T[0], T[1]);
+        for (int k = 0; k < nv; ++k) { eh[k] = eh[k] + T[0][k]; eb[k] = eb[k] + T[1][k]; }
+        memcpy(T[2], eh, sizeof(double) * nv);
+        memcpy(T[3], eb, sizeof(double) * nv);
+        if (!uo_project_moments(nv, eh, eb, c->wt + cc * 4, c->u, c->v, c->w, T[2], T[3])) return 422;
+    }
+    /* SolveMicroLUSGS with the frozen wall closure, one sweep pair */
+    memset(c->dh_ghost, 0, S * sizeof(double));
+    memset(c->db_ghost, 0, S * sizeof(double));
+    for (int s = 0; s < p->nslab; ++s) if (!lusgs_stage(c, s, 0, dtp)) return 423;
+    memcpy(c->dh_ghost, c->dh, S * sizeof(double));           /* MPIExchangeDeltaMicro */
+    memcpy(c->db_ghost, c->db, S * sizeof(double));
+    for (int s = 0; s < p->nslab; ++s) if (!lusgs_stage(c, s, 1, dtp)) return 423;
+    /* FindAdmissibleMicroAlpha(enforce_negative_fraction=.false.) (mod_SteadyImplicit.f90:53-117) */
+    double alpha = 1.0;
+    double** T = scratch_t(c, 0);
+    for (;;) {
+        int ok = 1;
+        for (int cc = 0; cc < c->nc && ok; ++cc) {
+            double mm[4];
+            for (int k = 0; k < nv; ++k) {
+                size_t q = (size_t)cc * nv + k;
+                T[0][k] = c->h[q] + alpha * c->dh[q];
+                T[1][k] = c->b[q] + alpha * c->db[q];
+                ok &= isfinite(T[0][k]) && isfinite(T[1][k]);
+            }
+            moment_conserved(nv, T[0], T[1], c->u, c->v, c->w, mm);
+            ok &= uo_is_physical(mm);
+        }
+        if (ok) break;
+        alpha = 0.5 * alpha;
+        if (alpha < p->min_alpha) return 433;
+    }
+    for (size_t q = 0; q < S; ++q) { c->h[q] = c->h[q] + alpha * c->dh[q]; c->b[q] = c->b[q] + alpha * c->db[q]; }
+    /* RecoverMacroFromKineticState + moment gate (mod_ImplicitMicro.f90:628-645, mod_SteadyImplicit.f90:451-459) */
+    for (int cc = 0; cc < c->nc; ++cc) {
+        double mm[4];
+        moment_conserved(nv, c->h + (size_t)cc * nv, c->b + (size_t)cc * nv, c->u, c->v, c->w, mm);
+        if (!uo_is_physical(mm)) return 434;
+        memcpy(c->wt + cc * 4, mm, sizeof mm);
+    }
+    memcpy(c->W, c->wt, sizeof(double) * c->nc * 4);
+    double merr = 0.0;
+    for (int cc = 0; cc < c->nc; ++cc) {
+        double mm[4];
+        moment_conserved(nv, c->h + (size_t)cc * nv, c->b + (size_t)cc * nv, c->u, c->v, c->w, mm);
+        for (int m = 0; m < 4; ++m) merr = fmax(merr, fabs(c->W[cc * 4 + m] - mm[m]) / fmax(fabs(c->W[cc * 4 + m]), 1.0));
+    }
+    if (!(merr <= p->moment_tol)) return 451;
+    /* CheckR5Policy (mod_R5Observe.f90:248-256): the accepted update must be a full step */
+    if (alpha != 1.0 || malpha != 1.0) return 452;
+    /* RescaleClosedMass (mod_ClosedCouetteMass.f90:243-313) */
+    if (p->mass_rescale) {
+        double t[5], m[5];
+        if (!mass_statistics(c, t, m)) return 941;
+        c->mass_scale = c->m0 / t[0];
+        for (int q = 0; q < c->nc * 4; ++q) c->W[q] = c->mass_scale * c->W[q];
+        for (size_t q = 0; q < S; ++q) { c->h[q] = c->mass_scale * c->h[q]; c->b[q] = c->mass_scale * c->b[q]; }
+    }
+    /* AfterR5Accepted -> EvaluateSparseState (mod_R5Observe.f90:287-320) */
+    double totals[5], metrics[5];
+    if (!mass_statistics(c, totals, metrics)) return 941;
+    uo_interpolation(c);
+    if ((e = uo_evolution(c, dt))) return e;
+    if ((e = uo_compute_residual(c, dt, 1))) return e;
+    if (!reassemble_rates(c, dt)) return 444;
+    double sci[22];
+    implicit_diagnostics(c, dt, sci);
+    sci[18] = merr;   /* implicit_moment_error of this step (or the rescaled state's, below) */
+    if (p->mass_rescale) sci[18] = metrics[0];
+    /* flux_1..16: boundary-face totals per unit time (mod_R5Observe.f90:107-113) */
+    double fl[16] = {0};
+    int nx = p->nx, ny = p->ny;
+    for (int j = 0; j < ny; ++j)
+        for (int m = 0; m < 4; ++m) {
+            fl[m] = fl[m] - c->fxw[((size_t)j * nx + 0) * 4 + m] / dt;
+            fl[4 + m] = fl[4 + m] + c->fxw[((size_t)j * nx + 0) * 4 + m] / dt;
+        }
+    for (int i = 0; i < nx; ++i)
+        for (int m = 0; m < 4; ++m) {
+            fl[8 + m] = fl[8 + m] - c->fyLw[(size_t)i * 4 + m] / dt;
+            fl[12 + m] = fl[12 + m] + c->fyRw[((size_t)ny * nx + i) * 4 + m] / dt;
+        }
+    int pass = sci[0] <= p->residual_tol && sci[1] <= p->residual_tol && sci[2] <= p->residual_tol &&
+               sci[3] <= p->residual_tol && sci[12] <= p->residual_tol && sci[13] <= p->residual_tol &&
+               metrics[0] <= p->moment_tol;
+    c->streak = pass ? c->streak + 1 : 0;
+    row[0] = pass; row[1] = metrics[0]; row[2] = totals[0]; row[3] = totals[4];
+    row[4] = sci[8]; row[5] = sci[9]; row[6] = sci[10]; row[7] = sci[11];
+    row[8] = sci[20]; row[9] = sci[21]; row[10] = sci[16]; row[11] = sci[17];
+    memcpy(row + 12, sci, sizeof sci);
+    memcpy(row + 34, fl, sizeof fl);
+    row[50] = c->ref_h; row[51] = c->ref_b;
+    row[52] = p->mass_rescale ? c->mass_scale - 1.0 : 0.0;
+    row[53] = alpha; row[54] = malpha; row[55] = dt; row[56] = c->streak;
+    if (out) memcpy(out, row, sizeof(double) * (nout < 80 ? nout : 80));
+    return 0;
 }

@@ -84,6 +84,7 @@ int uo_solve_dense4(const double m[16], const double rhs[4], double sol[4]);
 /* ImplicitSteady pseudo-step (mod_SteadyImplicit.f90:379-462) with the reference's nslab
  * block-Jacobi seams.  out[] receives the diagnostics listed in ugks_oracle.c. */
 int uo_implicit_step(uo_ctx* c, double* out, int nout);
+int uo_implicit_init(uo_ctx* c);   /* persistent M0 of the cold start (InitializeClosedMass) */
 
 /* Worker threads used over faces and cells (0 = all host cores); returns the count in use.
  * Results do not depend on the thread count: faces and cells are independent and every sum over
