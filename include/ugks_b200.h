@@ -117,6 +117,24 @@ int ugks_step_explicit_noalloc(const ugks_params* params, const double* u, const
                                double* h, double* b, double* W, int nsteps, void* stream, double* dt_out,
                                double* res_out);
 
+/* ImplicitSteady with the closed-Couette mass rescale (method UGKS_METHOD_IMPLICIT_STEADY).
+ * ugks_implicit_init: InitializeClosedMass (src/mod_ClosedCouetteMass.f90:212-241) -- the persistent
+ * M0 from the current state and a fresh residual-reference epoch; call after the state is set.
+ * ugks_implicit_steps: up to max_steps pseudo-steps of Solve_UGKS (src/mod_Solve.f90:84-293), each
+ * TimeStep, Interpolation + Evolution, ComputeResidual, ApplySteadyImplicitUpdate (PR(2) + one
+ * LU-SGS sweep pair with the reference's nslab block-Jacobi seams, src/mod_SteadyImplicit.f90:379-462),
+ * RescaleClosedMass and the accepted-state re-evaluation with the five-state gate
+ * (src/mod_R5Observe.f90:287-320); stops early when the gate has passed 5 states in a row.
+ * report[80] (optional) = the last accepted state's sparse_residual.csv row: [0] gate pass,
+ * [1] moment, [2] M_W, [3] M_h, [4..11] R1..R8, [12..33] science_1..22, [34..49] flux_1..16,
+ * [50..51] reference_h/b, [52] c_minus_1, [53] alpha, [54] macro alpha, [55] dt, [56] streak,
+ * [57..78] science of the pre-update evaluation. */
+int ugks_implicit_init(ugks_ctx* ctx);
+int ugks_implicit_steps(ugks_ctx* ctx, int max_steps, int* steps_done, int* converged, double* report);
+/* state[16]: M0, reference_h, reference_b, reference set, mass_scale, streak, stop, steps, alpha,
+ * macro alpha, moment error, converged (see ugks_implicit.cuh); report[80] as above. */
+int ugks_implicit_state(ugks_ctx* ctx, double* state, double* report);
+
 /* Wall Aerodynamics of the last Evolution (src/mod_Evolution.f90:2402-2409): out[2][nx][3] =
  * local-frame (pnn, pnt, qn) per bottom/top wall face. */
 int ugks_wall_aero(ugks_ctx* ctx, double* out);

@@ -25,8 +25,10 @@ EXPORTS = [
     "ugks_timestep", "ugks_evolution", "ugks_compute_residual", "ugks_apply_explicit_update",
     "ugks_step_explicit", "ugks_wall_aero", "ugks_copy_array", "ugks_last_status", "ugks_status_reference_code",
     "ugks_error_string", "ugks_stream", "ugks_synchronize", "ugks_profile_enable", "ugks_profile_read",
-    "ugks_launch_count", "ugks_step_explicit_noalloc",
+    "ugks_launch_count", "ugks_step_explicit_noalloc", "ugks_implicit_init", "ugks_implicit_steps",
+    "ugks_implicit_state",
 ]
+REPORT_LEN = 80
 
 
 class UgksParams(ctypes.Structure):
@@ -91,6 +93,9 @@ def load(path=LIB_PATH):
     L.ugks_launch_count.restype = ctypes.c_longlong
     L.ugks_step_explicit_noalloc.argtypes = [ctypes.POINTER(UgksParams), vp, vp, vp, vp, vp, vp, ctypes.c_int, vp,
                                              dp, dp]
+    L.ugks_implicit_init.argtypes = [vp]
+    L.ugks_implicit_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), dp]
+    L.ugks_implicit_state.argtypes = [vp, dp, dp]
     _lib = L
     return L
 

@@ -9,7 +9,7 @@
 #include <string>
 
 #include "../../include/ugks_b200.h"
-#include "ugks_lo.cuh"
+#include "ugks_implicit.cuh"
 
 namespace ugks {
 int lo_threads(int nvel);
@@ -20,6 +20,11 @@ cudaError_t launch_lo_cells(const LoParams& P, const LoBuffers& B, int mode, boo
 cudaError_t launch_lo_timestep(const LoParams& P, const LoBuffers& B, cudaStream_t s);
 cudaError_t launch_lo_init(const LoParams& P, const LoBuffers& B, double rho, double U, double V, double tn,
                            cudaStream_t s);
+cudaError_t launch_im_init(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
+                           cudaStream_t s);
+cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
+                                  cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
+                                  long long* launches);
 }  // namespace ugks
 
 using namespace ugks;
@@ -45,6 +50,15 @@ struct ugks_ctx {
     // explicit-step graph
     cudaGraphExec_t graph = nullptr;
     int graph_steps = 0;
+    // ImplicitSteady
+    ImParams Q{};
+    ImBuffers I{};
+    double* imem = nullptr;
+    unsigned* iflags = nullptr;
+    bool implicit_ready = false;
+    cudaGraphExec_t igraph = nullptr;
+    int igraph_steps = 0;
+    long long igraph_launches = 0;
     // profiling
     bool profile = false;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -164,6 +178,38 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     if (e == cudaSuccess) e = cudaMemcpyAsync(d + o_v, v, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d + o_w, w, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
+    if (e == cudaSuccess && p->method == UGKS_METHOD_IMPLICIT_STEADY) {
+        // ImplicitSteady work arrays (mod_ImplicitState.f90:110-132)
+        ImParams& Q = c->Q;
+        Q.nslab = p->nslab > 0 ? p->nslab : 1;
+        Q.mass_rescale = p->mass_rescale;
+        Q.macro_sweeps = p->macro_sweeps > 0 ? p->macro_sweeps : 2;
+        Q.ncfl = p->ncfl; Q.residual_tol = p->residual_tol; Q.moment_tol = p->moment_tol; Q.min_alpha = p->min_alpha;
+        Q.wall_ux[0] = p->wall_ux[0]; Q.wall_ux[1] = p->wall_ux[1];
+        if (ny % Q.nslab != 0) { ugks_ctx_destroy(c); return UGKS_EINVAL; }
+        size_t io = 0;
+        auto itake = [&](size_t n) { size_t o = io; io += (n + 31) / 32 * 32; return o; };
+        const size_t i_sh = itake(S), i_sb = itake(S), i_rw = itake((size_t)nc * 4), i_da = itake((size_t)nc * 4);
+        const size_t i_db = itake((size_t)nc * 4), i_g = itake((size_t)nc * 4), i_fi = itake((size_t)nc * 16);
+        const size_t i_fj = itake((size_t)nc * 16), i_wt = itake((size_t)nc * 4), i_tt = itake(nc);
+        const size_t i_eh = itake(S), i_eb = itake(S), i_fh = itake(S), i_fb = itake(S), i_bh = itake(S), i_bb = itake(S);
+        const size_t i_hu = itake((size_t)2 * nv), i_bu = itake((size_t)2 * nv), i_dr = itake((size_t)2 * nx);
+        const size_t i_cell = itake((size_t)nc * kImCell), i_st = itake(IS_COUNT), i_rep = itake(kReport);
+        e = cudaMalloc(&c->imem, io * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&c->iflags, 4 * sizeof(unsigned));
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->imem, 0, io * sizeof(double), c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->iflags, 0, 4 * sizeof(unsigned), c->stream);
+        if (e == cudaSuccess) {
+            double* m = c->imem;
+            ImBuffers& I = c->I;
+            I.stream_h = m + i_sh; I.stream_b = m + i_sb; I.rate_w = m + i_rw; I.dwA = m + i_da; I.dwB = m + i_db;
+            I.pr_gamma = m + i_g; I.pr_foi = m + i_fi; I.pr_foj = m + i_fj; I.wt = m + i_wt; I.tau_t = m + i_tt;
+            I.eq_h = m + i_eh; I.eq_b = m + i_eb; I.dFh = m + i_fh; I.dFb = m + i_fb; I.dBh = m + i_bh; I.dBb = m + i_bb;
+            I.wall_hu = m + i_hu; I.wall_bu = m + i_bu; I.wall_drho = m + i_dr; I.cell = m + i_cell;
+            I.state = m + i_st; I.report = m + i_rep;
+            I.mask = c->iflags; I.counter = c->iflags + 2;
+        }
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { ugks_ctx_destroy(c); return cuda_fail(e); }
     *out = c;
@@ -175,6 +221,9 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     cudaSetDevice(c->device);
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
+    if (c->igraph) cudaGraphExecDestroy(c->igraph);
+    if (c->imem) cudaFree(c->imem);
+    if (c->iflags) cudaFree(c->iflags);
     for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     if (c->dmem) cudaFree(c->dmem);
     if (c->dflags) cudaFree(c->dflags);
@@ -435,3 +484,80 @@ extern "C" int ugks_profile_read(ugks_ctx* c, const char* kernel, double* total_
 }
 
 extern "C" long long ugks_launch_count(const ugks_ctx* c) { return c ? c->launches : 0; }
+
+// ---------------------------------------------------------------------------------------------
+// ImplicitSteady
+
+extern "C" int ugks_implicit_init(ugks_ctx* c) {
+    if (!c) return UGKS_EINVAL;
+    if (!c->imem) return UGKS_EUNSUPPORTED;
+    UGKS_CK(cudaSetDevice(c->device));
+    UGKS_CK(launch_im_init(c->P, c->B, c->Q, c->I, c->stream));
+    c->launches += 1;
+    c->implicit_ready = true;
+    return collect_status(c);
+}
+
+static int build_implicit_graph(ugks_ctx* c, int steps) {
+    if (c->igraph && c->igraph_steps == steps) return UGKS_OK;
+    if (c->igraph) { cudaGraphExecDestroy(c->igraph); c->igraph = nullptr; }
+    cudaGraph_t g;
+    long long n = 0;
+    UGKS_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = cudaSuccess;
+    for (int s = 0; s < steps && e == cudaSuccess; ++s)
+        e = enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork, c->ev_join, &n);
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) { if (e2 == cudaSuccess) cudaGraphDestroy(g); return cuda_fail(e); }
+    UGKS_CK(e2);
+    e = cudaGraphInstantiate(&c->igraph, g, 0);
+    cudaGraphDestroy(g);
+    UGKS_CK(e);
+    c->igraph_steps = steps;
+    c->igraph_launches = n;
+    return UGKS_OK;
+}
+
+extern "C" int ugks_implicit_steps(ugks_ctx* c, int max_steps, int* steps_done, int* converged, double* report) {
+    if (!c || max_steps < 0) return UGKS_EINVAL;
+    if (!c->imem) return UGKS_EUNSUPPORTED;
+    if (!c->implicit_ready) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    const int G = 8;
+    double st[IS_COUNT];
+    UGKS_CK(cudaMemcpyAsync(st, c->I.state, sizeof st, cudaMemcpyDeviceToHost, c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    const double start = st[IS_STEPS];
+    int left = max_steps;
+    while (left > 0 && st[IS_STOP] == 0.0) {
+        if (left >= G) {
+            int r = build_implicit_graph(c, G);
+            if (r) return r;
+            UGKS_CK(cudaGraphLaunch(c->igraph, c->stream));
+            c->launches += c->igraph_launches;
+            left -= G;
+        } else {
+            long long n = 0;
+            for (int s = 0; s < left; ++s)
+                UGKS_CK(enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork,
+                                              c->ev_join, &n));
+            c->launches += n;
+            left = 0;
+        }
+        UGKS_CK(cudaMemcpyAsync(st, c->I.state, sizeof st, cudaMemcpyDeviceToHost, c->stream));
+        UGKS_CK(cudaStreamSynchronize(c->stream));
+    }
+    if (steps_done) *steps_done = (int)(st[IS_STEPS] - start);
+    if (converged) *converged = st[IS_CONVERGED] != 0.0 ? 1 : 0;
+    if (report) UGKS_CK(cudaMemcpyAsync(report, c->I.report, kReport * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    return collect_status(c);
+}
+
+extern "C" int ugks_implicit_state(ugks_ctx* c, double* state, double* report) {
+    if (!c || !c->imem) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    if (state) UGKS_CK(cudaMemcpyAsync(state, c->I.state, IS_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (report) UGKS_CK(cudaMemcpyAsync(report, c->I.report, kReport * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    return UGKS_OK;
+}

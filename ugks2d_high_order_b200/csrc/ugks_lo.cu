@@ -17,21 +17,6 @@
 
 namespace ugks {
 
-__device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i >= nx ? i - nx : i); }
-
-// Velocity slot r of this thread: k, clamped index kk, and whether it is a real velocity.
-struct Slot {
-    int k, kk;
-    bool ok;
-};
-__device__ __forceinline__ Slot slot(int r, int nv) {
-    Slot s;
-    s.k = threadIdx.x + r * blockDim.x;
-    s.ok = s.k < nv;
-    s.kk = s.ok ? s.k : nv - 1;
-    return s;
-}
-
 // -------------------------------------------------------------------------------------------
 // Interpolation (mod_Interpolation.f90:26-90): slopes sx*, sy* of h and b.  x is periodic; on
 // the wall rows the y slope is the one-sided (right-left)/dy of InterpBoundary (:100-117), and
@@ -497,17 +482,6 @@ __global__ void __launch_bounds__(NTMAX) k_lo_walls(LoParams P, LoBuffers B) {
     const size_t o = (size_t)((side < 0 ? 0 : ny) * nx + i);
     lo_face_wall<VPT>(P, B, side, i, dt, B.fyh + o * nv, B.fyb + o * nv, B.fyw + o * 4,
                       B.wall_aero + ((side < 0 ? 0 : 1) * nx + i) * 3, red, rout);
-}
-
-// -------------------------------------------------------------------------------------------
-// Per-cell TimeStep (mod_Solve.f90:386-405): dt_local = CFL*area/(dy*max(U_MAX,|U|+c)+dx*max(V_MAX,|V|+c))
-__device__ __forceinline__ double cell_dt(const LoParams& P, const double w[4], bool& ok) {
-    Prim p;
-    ok = get_primary(P.gm1, w, p);
-    if (!ok) return 0.0;
-    const double sos = sqrt(0.5 * (P.gm1 + 1.0) / p.L);
-    const double a = fmax(P.umax, fabs(p.U) + sos), bq = fmax(P.vmax, fabs(p.V) + sos);
-    return P.cfl * P.area / (P.dy * a + P.dx * bq);
 }
 
 // Last-CTA epilogue: dt_global = min(dt_local) (MPI_AllReduce MIN, mod_Solve.f90:409-418) and

@@ -51,4 +51,30 @@ struct LoBuffers {
     unsigned* status;        // [1] error bits
 };
 
+__device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i >= nx ? i - nx : i); }
+
+// Velocity slot r of this thread: k, clamped index kk, and whether it is a real velocity.  Velocity
+// loops are branch-free: a slot beyond nvel reads a valid velocity with weight 0 and skips stores.
+struct Slot {
+    int k, kk;
+    bool ok;
+};
+__device__ __forceinline__ Slot slot(int r, int nv) {
+    Slot s;
+    s.k = threadIdx.x + r * blockDim.x;
+    s.ok = s.k < nv;
+    s.kk = s.ok ? s.k : nv - 1;
+    return s;
+}
+
+// Per-cell TimeStep (mod_Solve.f90:386-405): dt_local = CFL*area/(dy*max(U_MAX,|U|+c)+dx*max(V_MAX,|V|+c))
+__device__ __forceinline__ double cell_dt(const LoParams& P, const double w[4], bool& ok) {
+    Prim p;
+    ok = get_primary(P.gm1, w, p);
+    if (!ok) return 0.0;
+    const double sos = sqrt(0.5 * (P.gm1 + 1.0) / p.L);
+    const double a = fmax(P.umax, fabs(p.U) + sos), bq = fmax(P.vmax, fabs(p.V) + sos);
+    return P.cfl * P.area / (P.dy * a + P.dx * bq);
+}
+
 }  // namespace ugks

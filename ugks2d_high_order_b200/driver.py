@@ -37,6 +37,8 @@ def main(argv=None):
     case = case.with_(**kw) if kw else case
     s = Solver(case, *load_velocity_half32())
     s.init_freestream()
+    if a.method == "ImplicitSteady":
+        s.implicit_init()
     t0 = time.perf_counter()
     done = 0
     while done < a.steps:
@@ -46,9 +48,14 @@ def main(argv=None):
             done += n
             print(f"iter={done:8d} dt={dt:.7e} res={' '.join(f'{r:.7e}' for r in res)}", flush=True)
         else:
-            out = s.step_implicit(n)
+            got, conv, rep = s.step_implicit(n)
             done += n
-            print(f"iter={done:8d} {out}", flush=True)
+            print(f"iter={done:8d} Rrho={rep[12]:.4e} RrhoU={rep[13]:.4e} RrhoV={rep[14]:.4e} RE={rep[15]:.4e} "
+                  f"Rh={rep[24]:.4e} Rb={rep[25]:.4e} moment={rep[1]:.4e} c_minus_1={rep[52]:.6e} "
+                  f"streak={int(rep[56])}", flush=True)
+            if conv or got < n:
+                print(f"five-state gate reached after {int(s.implicit_state()[0][7])} accepted steps", flush=True)
+                break
     el = time.perf_counter() - t0
     print(f"{a.steps} steps in {el:.3f} s ({case.nx * case.ny * s.nvel * a.steps / el:.3e} cell-vel updates/s)")
     s.close()

@@ -112,6 +112,28 @@ class Solver:
         self._check(self.L.ugks_step_explicit(self.ctx, int(nsteps), _p(dt), _p(res)), "Explicit step")
         return float(dt[0]), res
 
+    # ---- ImplicitSteady (mod_SteadyImplicit.f90:379-462 + mod_ClosedCouetteMass.f90 + mod_R5Observe.f90)
+    def implicit_init(self):
+        """InitializeClosedMass: persistent M0 from the current state, new residual-reference epoch."""
+        self._check(self.L.ugks_implicit_init(self.ctx), "InitializeClosedMass")
+
+    def step_implicit(self, max_steps=1):
+        """Up to max_steps accepted pseudo-steps; stops when the five-state gate has passed 5 times.
+        Returns (steps_done, converged, report) where report is the last accepted state's
+        sparse_residual.csv row (layout in include/ugks_b200.h)."""
+        done = ctypes.c_int()
+        conv = ctypes.c_int()
+        rep = np.zeros(capi.REPORT_LEN)
+        self._check(self.L.ugks_implicit_steps(self.ctx, int(max_steps), ctypes.byref(done), ctypes.byref(conv),
+                                               _p(rep)), "ApplySteadyImplicitUpdate")
+        return done.value, bool(conv.value), rep
+
+    def implicit_state(self):
+        st = np.zeros(16)
+        rep = np.zeros(capi.REPORT_LEN)
+        self._check(self.L.ugks_implicit_state(self.ctx, _p(st), _p(rep)), "implicit_state")
+        return st, rep
+
     def wall_aero(self):
         out = np.empty((2, self.nx, 3))
         self._check(self.L.ugks_wall_aero(self.ctx, _p(out)), "wall_aero")
