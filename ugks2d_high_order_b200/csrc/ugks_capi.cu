@@ -22,6 +22,7 @@ cudaError_t launch_lo_init(const LoParams& P, const LoBuffers& B, double rho, do
                            cudaStream_t s);
 cudaError_t launch_im_init(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
                            cudaStream_t s);
+cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q);
 cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
                                   cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
                                   long long* launches);
@@ -131,6 +132,11 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     P.nx = nx; P.ny = ny; P.nvel = nv; P.ck = p->ck;
     P.dx = p->dx; P.dy = p->dy;
     P.area = std::fabs((-p->dx) * (-p->dy) - (p->dx) * (-p->dy)) * 0.5;
+    {
+        int e2 = 0;
+        const double m2 = std::frexp(P.area, &e2);
+        P.inv_area = (m2 == 0.5 && std::isfinite(P.area)) ? std::ldexp(1.0, 1 - e2) : 0.0;
+    }
     P.gm1 = (double)(p->ck + 4) / (double)(p->ck + 2) - 1.0;
     P.pr = p->pr; P.omega = p->omega; P.mu_ref = p->mu_ref; P.cfl = p->cfl;
     P.umax = -INFINITY; P.vmax = -INFINITY;
@@ -186,7 +192,8 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
         Q.macro_sweeps = p->macro_sweeps > 0 ? p->macro_sweeps : 2;
         Q.ncfl = p->ncfl; Q.residual_tol = p->residual_tol; Q.moment_tol = p->moment_tol; Q.min_alpha = p->min_alpha;
         Q.wall_ux[0] = p->wall_ux[0]; Q.wall_ux[1] = p->wall_ux[1];
-        if (ny % Q.nslab != 0) { ugks_ctx_destroy(c); return UGKS_EINVAL; }
+        if (ny % Q.nslab != 0 || (ny / Q.nslab) * nx > kMaxSlabCells) { ugks_ctx_destroy(c); return UGKS_EINVAL; }
+        e = prepare_implicit(c->P, Q);
         size_t io = 0;
         auto itake = [&](size_t n) { size_t o = io; io += (n + 31) / 32 * 32; return o; };
         const size_t i_sh = itake(S), i_sb = itake(S), i_rw = itake((size_t)nc * 4), i_da = itake((size_t)nc * 4);
@@ -195,7 +202,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
         const size_t i_eh = itake(S), i_eb = itake(S), i_fh = itake(S), i_fb = itake(S), i_bh = itake(S), i_bb = itake(S);
         const size_t i_hu = itake((size_t)2 * nv), i_bu = itake((size_t)2 * nv), i_dr = itake((size_t)2 * nx);
         const size_t i_cell = itake((size_t)nc * kImCell), i_st = itake(IS_COUNT), i_rep = itake(kReport);
-        e = cudaMalloc(&c->imem, io * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&c->imem, io * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&c->iflags, 4 * sizeof(unsigned));
         if (e == cudaSuccess) e = cudaMemsetAsync(c->imem, 0, io * sizeof(double), c->stream);
         if (e == cudaSuccess) e = cudaMemsetAsync(c->iflags, 0, 4 * sizeof(unsigned), c->stream);
@@ -204,7 +211,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
             ImBuffers& I = c->I;
             I.stream_h = m + i_sh; I.stream_b = m + i_sb; I.rate_w = m + i_rw; I.dwA = m + i_da; I.dwB = m + i_db;
             I.pr_gamma = m + i_g; I.pr_foi = m + i_fi; I.pr_foj = m + i_fj; I.wt = m + i_wt; I.tau_t = m + i_tt;
-            I.eq_h = m + i_eh; I.eq_b = m + i_eb; I.dFh = m + i_fh; I.dFb = m + i_fb; I.dBh = m + i_bh; I.dBb = m + i_bb;
+            I.rhs_h = m + i_eh; I.rhs_b = m + i_eb; I.dFh = m + i_fh; I.dFb = m + i_fb; I.dBh = m + i_bh; I.dBb = m + i_bb;
             I.wall_hu = m + i_hu; I.wall_bu = m + i_bu; I.wall_drho = m + i_dr; I.cell = m + i_cell;
             I.state = m + i_st; I.report = m + i_rep;
             I.mask = c->iflags; I.counter = c->iflags + 2;
@@ -241,9 +248,17 @@ static int kernel_timestep(ugks_ctx* c) {
     return UGKS_OK;
 }
 
+// Any call that changes the state, dt or the flux arrays outside the implicit step invalidates the
+// cached accepted-state evaluation the next implicit step would otherwise reuse.
+static int invalidate_eval(ugks_ctx* c) {
+    if (c->imem) UGKS_CK(cudaMemsetAsync(c->I.state + IS_EVAL_VALID, 0, sizeof(double), c->stream));
+    return UGKS_OK;
+}
+
 extern "C" int ugks_upload_state(ugks_ctx* c, const double* h, const double* b, const double* W) {
     if (!c || !h || !b || !W) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
+    if (int r = invalidate_eval(c)) return r;
     const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
     UGKS_CK(cudaMemcpyAsync(c->B.h, h, S * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     UGKS_CK(cudaMemcpyAsync(c->B.b, b, S * sizeof(double), cudaMemcpyHostToDevice, c->stream));
@@ -270,6 +285,7 @@ extern "C" int ugks_download_state(ugks_ctx* c, double* h, double* b, double* W)
 extern "C" int ugks_init_freestream(ugks_ctx* c, double rho, double U, double V, double tnative) {
     if (!c || !(rho > 0) || !(tnative > 0)) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
+    if (int r = invalidate_eval(c)) return r;
     UGKS_CK(launch_lo_init(c->P, c->B, rho, U, V, tnative, c->stream));
     c->launches += 1;
     int r = kernel_timestep(c);
@@ -280,6 +296,7 @@ extern "C" int ugks_init_freestream(ugks_ctx* c, double rho, double U, double V,
 extern "C" int ugks_timestep(ugks_ctx* c, double* dt_out) {
     if (!c) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
+    if (int r = invalidate_eval(c)) return r;
     int r = kernel_timestep(c);
     if (r) return r;
     if (dt_out) UGKS_CK(cudaMemcpyAsync(dt_out, c->B.dt, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -289,6 +306,7 @@ extern "C" int ugks_timestep(ugks_ctx* c, double* dt_out) {
 extern "C" int ugks_evolution(ugks_ctx* c) {
     if (!c) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
+    if (int r = invalidate_eval(c)) return r;
     UGKS_CK(launch_lo_slopes(c->P, c->B, c->stream));
     UGKS_CK(launch_lo_faces(c->P, c->B, c->stream));
     UGKS_CK(launch_lo_walls(c->P, c->B, c->stream));
@@ -299,6 +317,7 @@ extern "C" int ugks_evolution(ugks_ctx* c) {
 extern "C" int ugks_compute_residual(ugks_ctx* c, int with_collision) {
     if (!c) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
+    if (int r = invalidate_eval(c)) return r;
     UGKS_CK(launch_lo_cells(c->P, c->B, 1, with_collision != 0, c->stream));
     c->launches += 1;
     return collect_status(c);
@@ -332,6 +351,7 @@ static int read_step_outputs(ugks_ctx* c, double* dt_out, double* res_out) {
 extern "C" int ugks_apply_explicit_update(ugks_ctx* c, double* res_out) {
     if (!c) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
+    if (int r = invalidate_eval(c)) return r;
     UGKS_CK(launch_lo_cells(c->P, c->B, 2, false, c->stream));
     c->launches += 1;
     return read_step_outputs(c, nullptr, res_out);
@@ -374,6 +394,7 @@ static int build_graph(ugks_ctx* c, int steps) {
 extern "C" int ugks_step_explicit(ugks_ctx* c, int nsteps, double* dt_out, double* res_out) {
     if (!c || nsteps < 0) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
+    if (int r = invalidate_eval(c)) return r;
     if (nsteps == 0) return UGKS_OK;
     if (c->profile) {
         for (int s = 0; s < nsteps; ++s) {
@@ -556,7 +577,7 @@ extern "C" int ugks_implicit_steps(ugks_ctx* c, int max_steps, int* steps_done, 
 extern "C" int ugks_implicit_state(ugks_ctx* c, double* state, double* report) {
     if (!c || !c->imem) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
-    if (state) UGKS_CK(cudaMemcpyAsync(state, c->I.state, IS_COUNT * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (state) UGKS_CK(cudaMemcpyAsync(state, c->I.state, kStatePublic * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (report) UGKS_CK(cudaMemcpyAsync(report, c->I.report, kReport * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     UGKS_CK(cudaStreamSynchronize(c->stream));
     return UGKS_OK;

@@ -32,21 +32,43 @@ __device__ __forceinline__ bool is_physical(const double w[4]) {   // IsPhysical
 }
 
 // EulerFluxNormal (mod_ImplicitCommon.f90:22-30)
-__device__ __forceinline__ void euler_flux(double gm1, const double w[4], double nx, double ny, double f[4]) {
-    const double u = w[1] / w[0], v = w[2] / w[0], un = u * nx + v * ny;
-    const double p = gm1 * (w[3] - 0.5 * (w[1] * w[1] + w[2] * w[2]) / w[0]);
+// EulerFluxNormal (mod_ImplicitMacro.f90:265-280) split into the state's primitives (u, v, p), which
+// hold the divisions and are shared by every face of a cell, and the normal flux.  Products are
+// rounded before they are summed (no contraction), as in the reference's loop, so a flux built from
+// cached primitives equals one built from scratch.
+struct EulerPrim {
+    double u, v, p;
+};
+
+__device__ __forceinline__ EulerPrim euler_prim(double gm1, const double w[4]) {
+    EulerPrim e;
+    e.u = w[1] / w[0];
+    e.v = w[2] / w[0];
+    const double ke = __dadd_rn(__dmul_rn(w[1], w[1]), __dmul_rn(w[2], w[2]));
+    e.p = gm1 * (w[3] - 0.5 * ke / w[0]);
+    return e;
+}
+
+__device__ __forceinline__ void euler_flux_prim(const double w[4], const EulerPrim& e, double nx, double ny,
+                                                double f[4]) {
+    const double un = __dadd_rn(__dmul_rn(e.u, nx), __dmul_rn(e.v, ny));
     f[0] = w[0] * un;
-    f[1] = w[1] * un + p * nx;
-    f[2] = w[2] * un + p * ny;
-    f[3] = (w[3] + p) * un;
+    f[1] = __dadd_rn(__dmul_rn(w[1], un), __dmul_rn(e.p, nx));
+    f[2] = __dadd_rn(__dmul_rn(w[2], un), __dmul_rn(e.p, ny));
+    f[3] = (w[3] + e.p) * un;
+}
+
+__device__ __forceinline__ void euler_flux(double gm1, const double w[4], double nx, double ny, double f[4]) {
+    euler_flux_prim(w, euler_prim(gm1, w), nx, ny, f);
 }
 
 // ZhuMovingWallMap (mod_ImplicitBoundary.f90:187-194): ghost state and its exact tangent.
 __device__ __forceinline__ void zhu_map(const double w[4], double uw, double vw, double g[4]) {
     g[0] = w[0];
-    g[1] = 2.0 * uw * w[0] - w[1];
-    g[2] = 2.0 * vw * w[0] - w[2];
-    g[3] = w[3] + 2.0 * (uw * uw + vw * vw) * w[0] - 2.0 * uw * w[1] - 2.0 * vw * w[2];
+    g[1] = __dsub_rn(__dmul_rn(2.0 * uw, w[0]), w[1]);
+    g[2] = __dsub_rn(__dmul_rn(2.0 * vw, w[0]), w[2]);
+    const double t = __dadd_rn(w[3], __dmul_rn(2.0 * __dadd_rn(__dmul_rn(uw, uw), __dmul_rn(vw, vw)), w[0]));
+    g[3] = __dsub_rn(__dsub_rn(t, __dmul_rn(2.0 * uw, w[1])), __dmul_rn(2.0 * vw, w[2]));
 }
 
 // Face f (0 left, 1 right, 2 bottom, 3 top) of cell (i,j): outward normal of GetFaceGeometry
@@ -122,6 +144,10 @@ __device__ __forceinline__ void wall_frame(const LoParams& P, int top, double uk
 template <int VPT, int NTMAX, bool POST>
 __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_residual(LoParams P, LoBuffers B, ImParams Q, ImBuffers I) {
     if (I.state[IS_STOP] != 0.0) return;
+    if (!POST && eval_cached(B)) {   // the previous accepted-state evaluation is this evaluation
+        if (blockIdx.x == 0 && threadIdx.x < 22) I.report[57 + threadIdx.x] = I.state[IS_PRESCI + threadIdx.x];
+        return;
+    }
     __shared__ double red[16 * 64];
     __shared__ double rout[kRedSlots];
     __shared__ double sc[32];   // [0..3] res_w [4..7] prim [8] tau [9] ok [12..15] stream lambda [16..19] eq lambda
@@ -275,14 +301,10 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_residual(LoParams P, 
         acc[6] += wk * fmax(h[r] * h[r], Ep * Ep);
         acc[7] += wk * fmax(b[r] * b[r], Fp * Fp);
         moment_add(wk, uk, vk, h[r], b[r], acc + 8);
-        if (s.ok) {
+        if (s.ok) {   // the physical equilibrium and collision stay in registers: nothing later reads them
             const size_t q = (size_t)c * nv + s.k;
             I.stream_h[q] = sh[r];
             I.stream_b[q] = sb[r];
-            B.peq_h[q] = Ep;
-            B.peq_b[q] = Fp;
-            B.pcol_h[q] = ch;
-            B.pcol_b[q] = cb;
         }
     }
     block_reduce_smem<12, 0>(acc, red, rout);
@@ -324,16 +346,29 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_residual(LoParams P, 
     if (!s_last) return;
     __threadfence();
     const int nc = P.nx * P.ny;
-    double g[20];
+    // g[0..18]: sums of the per-cell terms; g[19..30]: boundary-face macro fluxes per unit time
+    // (x wrap face, bottom wall, top wall; PhysicalDiagnostic flux, mod_R5Observe.f90:107-113);
+    // g[31]: max moment error
+    double g[32];
 #pragma unroll
-    for (int m = 0; m < 19; ++m) g[m] = 0.0;
-    g[19] = 0.0;
+    for (int m = 0; m < 32; ++m) g[m] = 0.0;
     for (int cc = tid; cc < nc; cc += blockDim.x) {
 #pragma unroll
         for (int m = 0; m < 19; ++m) g[m] += __ldcg(I.cell + (size_t)cc * kImCell + m);
-        g[19] = fmax(g[19], __ldcg(I.cell + (size_t)cc * kImCell + 19));
+        g[31] = fmax(g[31], __ldcg(I.cell + (size_t)cc * kImCell + 19));
     }
-    block_reduce<19, 1>(g, red, rout);
+    if (POST) {
+        for (int jj = tid; jj < P.ny; jj += blockDim.x)
+#pragma unroll
+            for (int m = 0; m < 4; ++m) g[19 + m] += __ldcg(B.fxw + ((size_t)jj * nx + 0) * 4 + m) / dt;
+        for (int ii = tid; ii < nx; ii += blockDim.x)
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                g[23 + m] += __ldcg(B.fyw + (size_t)ii * 4 + m) / dt;
+                g[27 + m] += __ldcg(B.fyw + ((size_t)P.ny * nx + ii) * 4 + m) / dt;
+            }
+    }
+    block_reduce<31, 1>(g, red, rout);
     if (tid != 0) return;
     const double SMV = kSMV;
     double sci[22];
@@ -371,21 +406,20 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_residual(LoParams P, 
         *I.counter = 0u;
         return;
     }
-    const double moment = g[19];
+    const double moment = g[31];
+    for (int m = 0; m < 22; ++m) I.state[IS_PRESCI + m] = sci[m];
+    I.state[IS_EVAL_DT] = dt;
+    I.state[IS_EVAL_VALID] = 1.0;
     if (Q.mass_rescale) sci[18] = moment;   // implicit_moment_error = MassStatistics after the rescale
-    // boundary-face totals per unit time (PhysicalDiagnostic flux, mod_R5Observe.f90:107-113)
+    // boundary-face totals per unit time: outflow through the left x face, inflow through the right
+    // (the same periodic face), the bottom wall taken into the domain, the top wall out of it
     double flux[16];
-    for (int m = 0; m < 16; ++m) flux[m] = 0.0;
-    for (int jj = 0; jj < P.ny; ++jj)
-        for (int m = 0; m < 4; ++m) {
-            flux[m] = flux[m] - B.fxw[((size_t)jj * nx + 0) * 4 + m] / dt;
-            flux[4 + m] = flux[4 + m] + B.fxw[((size_t)jj * nx + 0) * 4 + m] / dt;
-        }
-    for (int ii = 0; ii < nx; ++ii)
-        for (int m = 0; m < 4; ++m) {
-            flux[8 + m] = flux[8 + m] - B.fyw[(size_t)ii * 4 + m] / dt;
-            flux[12 + m] = flux[12 + m] + B.fyw[((size_t)P.ny * nx + ii) * 4 + m] / dt;
-        }
+    for (int m = 0; m < 4; ++m) {
+        flux[m] = -g[19 + m];
+        flux[4 + m] = g[19 + m];
+        flux[8 + m] = -g[23 + m];
+        flux[12 + m] = g[27 + m];
+    }
     const double tol = Q.residual_tol;
     const bool pass = sci[0] <= tol && sci[1] <= tol && sci[2] <= tol && sci[3] <= tol && sci[12] <= tol &&
                       sci[13] <= tol && moment <= Q.moment_tol;
@@ -426,7 +460,7 @@ __global__ void k_im_pr2_prep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I) 
     for (int m = 0; m < 4; ++m) wi[m] = B.W[c * 4 + m];
     double dist;
     if (g.wall) {
-        zhu_map(wi, Q.wall_ux[f == 2 ? 0 : 1], 0.0, wj);
+        zhu_map(wi, (f == 2 ? Q.wall_ux[0] : Q.wall_ux[1]), 0.0, wj);
         dist = P.dy;   // ctr%length(dirc)
     } else {
 #pragma unroll
@@ -463,77 +497,176 @@ __global__ void k_im_pr2_prep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I) 
     }
 }
 
-// RelaxMacroPoint (mod_ImplicitMacro.f90:90-123) for cell c; X = halo buffer (previous sweep),
-// Y = this sweep's buffer (Gauss-Seidel inside the slab).
-__device__ __forceinline__ bool relax_macro(const LoParams& P, const LoBuffers& B, const ImParams& Q,
-                                            const ImBuffers& I, int rows, int i, int j, double dtp,
-                                            const double* X, double* Y) {
-    const int c = j * P.nx + i;
-    double wi[4], di[4];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) { wi[m] = B.W[c * 4 + m]; di[m] = Y[c * 4 + m]; }
-    double sdt[4] = {0.0, 0.0, 0.0, 0.0}, sgn[4] = {0.0, 0.0, 0.0, 0.0}, sg = 0.0;
-#pragma unroll
-    for (int f = 0; f < 4; ++f) {
-        const FaceGeo g = face_geo(P, rows, i, j, f);
-        double wj[4], dnb[4], t[4], fn[4];
-        if (g.wall) {
-            const double uw = Q.wall_ux[f == 2 ? 0 : 1];
-            zhu_map(wi, uw, 0.0, wj);
-            zhu_map(di, uw, 0.0, dnb);
-        } else {
-            const double* src = g.ghost ? X : Y;
-#pragma unroll
-            for (int m = 0; m < 4; ++m) { wj[m] = B.W[g.nb * 4 + m]; dnb[m] = src[g.nb * 4 + m]; }
-        }
-        const double gam = I.pr_gamma[c * 4 + f];
-        const double* foi = I.pr_foi + (c * 4 + f) * 4;
-        const double* foj = I.pr_foj + (c * 4 + f) * 4;
-        double dti[4];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) t[m] = wi[m] + di[m];
-        euler_flux(P.gm1, t, g.nx, g.ny, fn);
-#pragma unroll
-        for (int m = 0; m < 4; ++m) dti[m] = fn[m] - foi[m];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) t[m] = wj[m] + dnb[m];
-        euler_flux(P.gm1, t, g.nx, g.ny, fn);
-#pragma unroll
-        for (int m = 0; m < 4; ++m) {
-            const double s = dti[m] + (fn[m] - foj[m]);
-            if (!isfinite(s)) return false;
-            sdt[m] = sdt[m] + g.len * s;
-            sgn[m] = sgn[m] + g.len * gam * dnb[m];
-        }
-        sg = sg + g.len * gam;
-    }
-    const double diag = 1.0 / dtp + 0.5 * sg / P.area;
-    if (!(isfinite(diag) && diag > 0.0)) return false;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) {
-        const double rhs = I.rate_w[c * 4 + m] - 0.5 * 1.0 * sdt[m] / P.area + 0.5 * 1.0 * sgn[m] / P.area;
-        if (!isfinite(rhs)) return false;
-        Y[c * 4 + m] = rhs / diag;
-    }
-    return true;
+// Cells of anti-diagonal d of a rows x nx slab (local row jl = 0..rows-1, column i), t-th cell.
+__device__ __forceinline__ bool diag_cell(int d, int t, int rows, int nx, int& i, int& jl) {
+    const int jl0 = d - (nx - 1) > 0 ? d - (nx - 1) : 0;
+    jl = jl0 + t;
+    i = d - jl;
+    return jl < rows && i >= 0;
 }
 
-// One PR(2) sweep (forward then backward Gauss-Seidel) per slab.
+// One PR(2) sweep of one slab (SolveMacroPR2, mod_ImplicitMacro.f90:57-88; RelaxMacroPoint :90-123).
+// Lexicographic Gauss-Seidel on the 5-point stencil equals an anti-diagonal wavefront: cell (i,j)
+// reads the already-updated (i-1,j), (i,j-1) and the not-yet-updated (i+1,j), (i,j+1), and cells on
+// one anti-diagonal never read each other.  Four lanes per cell: as faces they build the face terms
+// len * (dF_i + dF_j) and len * gamma * delta_nb; as components they sum them in face order and
+// relax; three of them then refresh the cell's Euler primitives.  The state W + delta of a cell
+// is the neighbour state of every interior face that touches it, so its primitives (the divisions
+// of the Euler flux) are computed once per relaxation and shared.  Everything lives in shared
+// memory; the halo cells (x wrap, slab seams) hold the previous sweep's corrections X.
+// Y = this sweep's result.
+// shared doubles of one slab: corrections, states and primitives of interior + halo cells, then
+// W, rate, gamma, fixed fluxes and the diagonal of the interior cells
+__host__ __device__ constexpr int pr_smem_words(int rows, int nx) {
+    return (rows * nx + 2 * rows + 2 * nx) * 12 + rows * nx * 45;
+}
+
+// local index of the neighbour of interior cell (i, jl) across face f: interior cells first, then
+// the halo (left wrap [rows], right wrap [rows], row below the slab [nx], row above [nx]); -1: wall
+__device__ __forceinline__ int pr_neighbour(int i, int jl, int j, int f, int rows, int nx, int ny) {
+    const int ncs = rows * nx, cl = jl * nx + i;
+    if (f == 0) return i > 0 ? cl - 1 : ncs + jl;
+    if (f == 1) return i < nx - 1 ? cl + 1 : ncs + rows + jl;
+    if (f == 2) return j == 0 ? -1 : (jl > 0 ? cl - nx : ncs + 2 * rows + i);
+    return j == ny - 1 ? -1 : (jl < rows - 1 ? cl + nx : ncs + 2 * rows + nx + i);
+}
+
 __global__ void k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I, const double* X, double* Y) {
     if (I.state[IS_STOP] != 0.0) return;
-    const int s = blockIdx.x * blockDim.x + threadIdx.x;
-    if (s >= Q.nslab) return;
-    const int rows = P.ny / Q.nslab, nx = P.nx;
+    extern __shared__ double sm[];
+    __shared__ double part[32][4][8];
+    const int s = blockIdx.x, rows = P.ny / Q.nslab, nx = P.nx, ny = P.ny;
+    const int ncs = rows * nx, nall = ncs + 2 * rows + 2 * nx, c0 = s * ncs;
+    double* sY = sm;                  // [nall][4] corrections
+    double* sT = sY + nall * 4;       // [nall][4] W + correction
+    double* sP = sT + nall * 4;       // [nall][4] Euler primitives u, v, p of sT
+    double* sW = sP + nall * 4;       // [ncs][4]
+    double* sR = sW + ncs * 4;        // [ncs][4] rate_w
+    double* sG = sR + ncs * 4;        // [ncs][4] gamma per face
+    double* sFi = sG + ncs * 4;       // [ncs][4 faces][4] fixed Euler flux of the cell
+    double* sFj = sFi + ncs * 16;     // [ncs][4 faces][4] fixed Euler flux of the neighbour
+    double* sD = sFj + ncs * 16;      // [ncs] diagonal
+    const int f = threadIdx.x & 3, tc = threadIdx.x >> 2, D = blockDim.x >> 2;
+    const int wbase = threadIdx.x & ~31, wn = blockDim.x - wbase;
+    const unsigned wmask = wn >= 32 ? 0xffffffffu : ((1u << wn) - 1u);   // lanes of this warp
     const double dtp = B.dt[0] * Q.ncfl / P.cfl;   // PseudoTimeStep (mod_ImplicitCommon.f90:115-119)
-    for (int j = s * rows; j < (s + 1) * rows; ++j)
-        for (int i = 0; i < nx; ++i)
-            for (int m = 0; m < 4; ++m) Y[(j * nx + i) * 4 + m] = X[(j * nx + i) * 4 + m];
-    bool ok = true;
-    for (int j = s * rows; j < (s + 1) * rows && ok; ++j)
-        for (int i = 0; i < nx && ok; ++i) ok = relax_macro(P, B, Q, I, rows, i, j, dtp, X, Y);
-    for (int j = (s + 1) * rows - 1; j >= s * rows && ok; --j)
-        for (int i = nx - 1; i >= 0 && ok; --i) ok = relax_macro(P, B, Q, I, rows, i, j, dtp, X, Y);
-    if (!ok) stop_with(I, B.status, ST_NONFINITE_STATE);
+    int bad = 0;
+    for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) {
+        sW[q] = B.W[c0 * 4 + q];
+        sR[q] = I.rate_w[c0 * 4 + q];
+        sG[q] = I.pr_gamma[c0 * 4 + q];
+    }
+    for (int q = threadIdx.x; q < ncs * 16; q += blockDim.x) {
+        sFi[q] = I.pr_foi[c0 * 16 + q];
+        sFj[q] = I.pr_foj[c0 * 16 + q];
+    }
+    // interior and halo cells: correction, state, primitives (halo rows beyond a wall stay unused)
+    for (int l = threadIdx.x; l < nall; l += blockDim.x) {
+        int g;
+        if (l < ncs) g = c0 + l;
+        else if (l < ncs + rows) g = (s * rows + (l - ncs)) * nx + (nx - 1);
+        else if (l < ncs + 2 * rows) g = (s * rows + (l - ncs - rows)) * nx;
+        else if (l < ncs + 2 * rows + nx) g = s * rows > 0 ? (s * rows - 1) * nx + (l - ncs - 2 * rows) : -1;
+        else g = (s + 1) * rows < ny ? ((s + 1) * rows) * nx + (l - ncs - 2 * rows - nx) : -1;
+        double y[4] = {0.0, 0.0, 0.0, 0.0}, t[4] = {1.0, 0.0, 0.0, 1.0};
+        if (g >= 0) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) { y[m] = X[g * 4 + m]; t[m] = B.W[g * 4 + m] + y[m]; }
+        }
+        const EulerPrim e = euler_prim(P.gm1, t);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { sY[l * 4 + m] = y[m]; sT[l * 4 + m] = t[m]; }
+        sP[l * 4 + 0] = e.u; sP[l * 4 + 1] = e.v; sP[l * 4 + 2] = e.p;
+    }
+    // the diagonal 1/dt_ps + 0.5 * sum_faces(L * gamma) / area is fixed through the sweeps; the face
+    // products are rounded before they are summed in face order, as the reference loop does
+    for (int cl = threadIdx.x; cl < ncs; cl += blockDim.x) {
+        const double* gm = I.pr_gamma + (c0 + cl) * 4;
+        double sg = 0.0;
+        sg = sg + __dmul_rn(P.dy, gm[0]);
+        sg = sg + __dmul_rn(P.dy, gm[1]);
+        sg = sg + __dmul_rn(P.dx, gm[2]);
+        sg = sg + __dmul_rn(P.dx, gm[3]);
+        const double diag = 1.0 / dtp + div_area(0.5 * sg, P);
+        if (!(isfinite(diag) && diag > 0.0)) bad = 1;
+        sD[cl] = diag;
+    }
+    __syncthreads();
+    const double fnx = f == 0 ? -1.0 : (f == 1 ? 1.0 : 0.0);
+    const double fny = f == 2 ? -1.0 : (f == 3 ? 1.0 : (f == 1 ? -0.0 : 0.0));
+    const double flen = f < 2 ? P.dy : P.dx;
+    const double fnxs = f == 3 ? -0.0 : fnx;   // GetFaceGeometry's normals: (-1,0) (1,-0) (0,-1) (-0,1)
+    const int dcells = rows < nx ? rows : nx;
+    const int ndiag = rows + nx - 1;
+    for (int pass = 0; pass < 2; ++pass) {
+        for (int dd = 0; dd < ndiag; ++dd) {
+            const int d = pass == 0 ? dd : ndiag - 1 - dd;
+            for (int t0 = 0; t0 < dcells; t0 += D) {
+                int i = 0, jl = 0;
+                const bool act = diag_cell(d, tc + t0, rows, nx, i, jl);
+                const int j = s * rows + jl, cl = jl * nx + i;
+                if (act) {   // lane = face f
+                    double ti[4], fi[4], fj[4], dnb[4];
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) ti[m] = sT[cl * 4 + m];
+                    const EulerPrim ei{sP[cl * 4 + 0], sP[cl * 4 + 1], sP[cl * 4 + 2]};
+                    euler_flux_prim(ti, ei, fnxs, fny, fi);
+                    const int nl = pr_neighbour(i, jl, j, f, rows, nx, ny);
+                    if (nl < 0) {
+                        const double uw = (f == 2 ? Q.wall_ux[0] : Q.wall_ux[1]);
+                        double wi[4], di[4], wj[4], tj[4];
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) { wi[m] = sW[cl * 4 + m]; di[m] = sY[cl * 4 + m]; }
+                        zhu_map(wi, uw, 0.0, wj);
+                        zhu_map(di, uw, 0.0, dnb);
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) tj[m] = wj[m] + dnb[m];
+                        euler_flux(P.gm1, tj, fnxs, fny, fj);
+                    } else {
+                        double tj[4];
+#pragma unroll
+                        for (int m = 0; m < 4; ++m) { tj[m] = sT[nl * 4 + m]; dnb[m] = sY[nl * 4 + m]; }
+                        const EulerPrim ej{sP[nl * 4 + 0], sP[nl * 4 + 1], sP[nl * 4 + 2]};
+                        euler_flux_prim(tj, ej, fnxs, fny, fj);
+                    }
+                    const double gam = sG[cl * 4 + f];
+                    const double* foi = sFi + (cl * 4 + f) * 4;
+                    const double* foj = sFj + (cl * 4 + f) * 4;
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) {
+                        const double dti = fi[m] - foi[m];
+                        const double sm4 = dti + (fj[m] - foj[m]);
+                        if (!isfinite(sm4)) bad = 1;
+                        part[tc][f][m] = flen * sm4;
+                        part[tc][f][4 + m] = flen * gam * dnb[m];
+                    }
+                }
+                __syncwarp(wmask);
+                if (act) {   // lane = component m
+                    const int m = f;
+                    double sdt = 0.0, sgn = 0.0;
+#pragma unroll
+                    for (int ff = 0; ff < 4; ++ff) { sdt = sdt + part[tc][ff][m]; sgn = sgn + part[tc][ff][4 + m]; }
+                    const double rhs = sR[cl * 4 + m] - div_area(0.5 * 1.0 * sdt, P) + div_area(0.5 * 1.0 * sgn, P);
+                    if (!isfinite(rhs)) bad = 1;
+                    const double y = rhs / sD[cl];
+                    sY[cl * 4 + m] = y;
+                    sT[cl * 4 + m] = sW[cl * 4 + m] + y;
+                }
+                __syncwarp(wmask);
+                if (act && f < 3) {   // lanes 0..2: primitives of the relaxed state
+                    double t[4];
+#pragma unroll
+                    for (int m = 0; m < 4; ++m) t[m] = sT[cl * 4 + m];
+                    const EulerPrim e = euler_prim(P.gm1, t);
+                    sP[cl * 4 + f] = f == 0 ? e.u : (f == 1 ? e.v : e.p);
+                }
+            }
+            __syncthreads();
+        }
+    }
+    for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) Y[c0 * 4 + q] = sY[q];
+    if (__syncthreads_or(bad) && threadIdx.x == 0) stop_with(I, B.status, ST_NONFINITE_STATE);
 }
 
 // BuildPredictedMacroState (mod_ImplicitMacro.f90:159-185): admissible alpha levels per cell.
@@ -648,9 +781,10 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_equilibrium(LoParams 
         const double Ep = E[r] + fmax(fabs(E[r]), kEps * se) * (lam[0] + uk * lam[1] + vk * lam[2] + e * lam[3]);
         const double Fp = F[r] + 0.5 * fmax(fabs(F[r]), kEps * sf) * lam[3];
         moment_add(wk, uk, vk, Ep, Fp, acc);
-        if (s.ok) {
-            I.eq_h[(size_t)c * nv + s.k] = Ep;
-            I.eq_b[(size_t)c * nv + s.k] = Fp;
+        if (s.ok) {   // RelaxMicroPoint's velocity-local right-hand side (mod_ImplicitMicro.f90:458-460)
+            const size_t q = (size_t)c * nv + s.k;
+            I.rhs_h[q] = I.stream_h[q] + (Ep - B.h[q]) / sc[8];
+            I.rhs_b[q] = I.stream_b[q] + (Fp - B.b[q]) / sc[8];
         }
     }
     block_reduce_smem<4, 0>(acc, red, rout);
@@ -663,84 +797,134 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_equilibrium(LoParams 
 }
 
 // -------------------------------------------------------------------------------------------
-// One LU-SGS stage: RelaxMicroPoint (mod_ImplicitMicro.f90:444-487) over one slab for one velocity.
-// Forward: cells j up, i up; corrections not yet relaxed, the halos and the wall closures are 0
-// (everything was reset).  Backward: cells j down, i down; not-yet-relaxed neighbours, halos and the
-// x wrap read the forward result, walls use the closure frozen from the forward correction.
+// One LU-SGS stage: RelaxMicroPoint (mod_ImplicitMicro.f90:444-487) as a hyperplane wavefront.
+// Per velocity only upwind neighbours couple, and in the reference's sweep order (forward j up,
+// i up; backward j down, i down) a cell reads updated values only from the previous cells of its
+// row and column, so the cells of one anti-diagonal of a slab are independent.  A CTA owns one
+// slab and 32 velocities: lane = velocity, warp = cell of the current diagonal.  The slab's
+// corrections for those velocities stay in shared memory: zero at the start of the forward stage
+// (all corrections were reset); the forward result at the start of the backward stage, overwritten
+// cell by cell, so that a neighbour read there returns the backward value once that neighbour has
+// been relaxed and the forward value before.  Halos (seams and the x wrap) read the forward result
+// in global memory in the backward stage and 0 in the forward stage; wall faces use the closure
+// frozen from the forward correction.
+// A velocity has one inflow face per direction (u > 0: left, u < 0: right; v > 0: bottom, v < 0:
+// top); the outflow faces add exact zeros to the right-hand side and their u_n L / area to the
+// diagonal, so the sums below keep the reference's face order.  The next cell's right-hand side
+// and diagonal are prefetched one diagonal ahead.
 template <bool BACKWARD>
 __global__ void __launch_bounds__(256) k_im_lusgs(LoParams P, LoBuffers B, ImParams Q, ImBuffers I) {
     if (I.state[IS_STOP] != 0.0) return;
+    extern __shared__ double sm[];
     const int nv = P.nvel, nx = P.nx, ny = P.ny;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int s = t / nv, k = t - s * nv;
-    if (s >= Q.nslab) return;
-    const int rows = ny / Q.nslab;
+    const int s = blockIdx.y, rows = ny / Q.nslab, ncs = rows * nx, c0 = s * ncs;
+    const int lane = threadIdx.x & 31, k = blockIdx.x * 32 + lane, tc = threadIdx.x >> 5, D = blockDim.x >> 5;
+    const bool kok = k < nv;
+    const int kk = kok ? k : nv - 1;
+    double* sh = sm;              // [ncs][32]
+    double* sb = sm + ncs * 32;
+    for (int q = threadIdx.x; q < ncs * 32; q += blockDim.x) {
+        const int kq = blockIdx.x * 32 + (q & 31);
+        double vh = 0.0, vb = 0.0;
+        if (BACKWARD && kq < nv) {
+            const size_t g = (size_t)(c0 + (q >> 5)) * nv + kq;
+            vh = I.dFh[g];
+            vb = I.dFb[g];
+        }
+        sh[q] = vh;
+        sb[q] = vb;
+    }
     const double dtp = B.dt[0] * Q.ncfl / P.cfl;
-    const double uk = B.u[k], vk = B.v[k];
+    const double idtp = 1.0 / dtp;
+    const double uk = B.u[kk], vk = B.v[kk];
     const double un[4] = {-uk, uk, -vk, vk};   // u*nx_out + v*ny_out of faces left, right, bottom, top
     const double len[4] = {P.dy, P.dy, P.dx, P.dx};
-    double whu[2], wbu[2];
-    if (BACKWARD) {
+    double cd[4], cm[4];
 #pragma unroll
-        for (int w = 0; w < 2; ++w) { whu[w] = I.wall_hu[w * nv + k]; wbu[w] = I.wall_bu[w * nv + k]; }
+    for (int f = 0; f < 4; ++f) {
+        cd[f] = div_area(1.0 * fmax(un[f], 0.0) * len[f], P);   // outflow part of the diagonal
+        cm[f] = 1.0 * fmin(un[f], 0.0) * len[f];                 // inflow coupling (divided by area below)
     }
+    const int fx = un[0] < 0.0 ? 0 : (un[1] < 0.0 ? 1 : -1);   // inflow x face
+    const int fy = un[2] < 0.0 ? 2 : (un[3] < 0.0 ? 3 : -1);   // inflow y face
+    const double cmx = fx == 0 ? cm[0] : (fx == 1 ? cm[1] : 0.0);
+    const double cmy = fy == 2 ? cm[2] : (fy == 3 ? cm[3] : 0.0);
+    const double cdx = cd[0] + cd[1], cdy = cd[2] + cd[3];      // one of each pair is +0: exact
+    double whu = 0.0, wbu = 0.0;
+    if (BACKWARD && fy >= 2) { const int w = fy - 2; whu = I.wall_hu[w * nv + kk]; wbu = I.wall_bu[w * nv + kk]; }
     double* outh = BACKWARD ? I.dBh : I.dFh;
     double* outb = BACKWARD ? I.dBb : I.dFb;
+    const int dcells = rows < nx ? rows : nx;
+    const int nchunk = (dcells + D - 1) / D;
+    const int nit = (rows + nx - 1) * nchunk;
+    // work item `it`: diagonal it / nchunk, cell (it % nchunk) * D + tc of it (in sweep order)
+    auto locate = [&](int it, int& i, int& jl) -> bool {
+        const int d = it / nchunk;
+        const bool a = diag_cell(d, (it - d * nchunk) * D + tc, rows, nx, i, jl);
+        if (BACKWARD) { i = nx - 1 - i; jl = rows - 1 - jl; }
+        return a && kok;
+    };
+    int ni = 0, njl = 0;
+    bool nact = locate(0, ni, njl);
+    double nrh = 0.0, nrb = 0.0, ndg = 1.0;
+    if (nact) {
+        const int c = c0 + njl * nx + ni;
+        nrh = I.rhs_h[(size_t)c * nv + k]; nrb = I.rhs_b[(size_t)c * nv + k];
+        ndg = ((idtp + 1.0 / I.tau_t[c]) + cdx) + cdy;
+    }
+    __syncthreads();
     bool ok = true;
-    for (int jj = 0; jj < rows; ++jj) {
-        const int j = BACKWARD ? (s + 1) * rows - 1 - jj : s * rows + jj;
-        for (int ii = 0; ii < nx; ++ii) {
-            const int i = BACKWARD ? nx - 1 - ii : ii;
-            const int c = j * nx + i;
-            const size_t q = (size_t)c * nv + k;
-            const double tt = I.tau_t[c];
-            double rh = I.stream_h[q] + (I.eq_h[q] - B.h[q]) / tt;
-            double rb = I.stream_b[q] + (I.eq_b[q] - B.b[q]) / tt;
-            double diag = 1.0 / dtp + 1.0 / tt;
-#pragma unroll
-            for (int f = 0; f < 4; ++f) {
-                double nh = 0.0, nb = 0.0;
-                if (un[f] < 0.0) {   // only inflow faces couple (min(un,0) /= 0)
-                    if (f == 0) {
-                        const size_t qn = (size_t)(j * nx + wrapx(i - 1, nx)) * nv + k;
-                        if (!BACKWARD) { if (i > 0) { nh = outh[qn]; nb = outb[qn]; } }
-                        else { nh = I.dFh[qn]; nb = I.dFb[qn]; }
-                    } else if (f == 1) {
-                        const size_t qn = (size_t)(j * nx + wrapx(i + 1, nx)) * nv + k;
-                        if (BACKWARD) {
-                            if (i < nx - 1) { nh = outh[qn]; nb = outb[qn]; }
-                            else { nh = I.dFh[qn]; nb = I.dFb[qn]; }
-                        }
-                    } else if (f == 2) {
-                        if (j == 0) {
-                            if (BACKWARD) { nh = I.wall_drho[i] * whu[0]; nb = I.wall_drho[i] * wbu[0]; }
-                        } else {
-                            const size_t qn = (size_t)((j - 1) * nx + i) * nv + k;
-                            const bool same = (j - 1) / rows == j / rows;
-                            if (!BACKWARD) { if (same) { nh = outh[qn]; nb = outb[qn]; } }
-                            else { nh = I.dFh[qn]; nb = I.dFb[qn]; }
-                        }
-                    } else {
-                        if (j == ny - 1) {
-                            if (BACKWARD) { nh = I.wall_drho[nx + i] * whu[1]; nb = I.wall_drho[nx + i] * wbu[1]; }
-                        } else {
-                            const size_t qn = (size_t)((j + 1) * nx + i) * nv + k;
-                            const bool same = (j + 1) / rows == j / rows;
-                            if (BACKWARD) {
-                                if (same) { nh = outh[qn]; nb = outb[qn]; }
-                                else { nh = I.dFh[qn]; nb = I.dFb[qn]; }
-                            }
-                        }
-                    }
-                }
-                diag = diag + 1.0 * fmax(un[f], 0.0) * len[f] / P.area;
-                rh = rh - 1.0 * fmin(un[f], 0.0) * len[f] * nh / P.area;
-                rb = rb - 1.0 * fmin(un[f], 0.0) * len[f] * nb / P.area;
+    for (int it = 0; it < nit; ++it) {
+        const bool act = nact;
+        const int i = ni, jl = njl;
+        double rh = nrh, rb = nrb;
+        const double diag = ndg;
+        if (it + 1 < nit) {
+            nact = locate(it + 1, ni, njl);
+            if (nact) {
+                const int c = c0 + njl * nx + ni;
+                nrh = I.rhs_h[(size_t)c * nv + k]; nrb = I.rhs_b[(size_t)c * nv + k];
+                ndg = ((idtp + 1.0 / I.tau_t[c]) + cdx) + cdy;
             }
-            ok = ok && diag > 0.0 && isfinite(diag) && isfinite(rh) && isfinite(rb);
-            outh[q] = rh / diag;
-            outb[q] = rb / diag;
         }
+        if (act) {
+            const int j = s * rows + jl, cl = jl * nx + i;
+            double nh = 0.0, nb = 0.0;   // x inflow neighbour
+            if (fx == 0) {
+                if (i > 0) { nh = sh[(cl - 1) * 32 + lane]; nb = sb[(cl - 1) * 32 + lane]; }
+                else if (BACKWARD) { const size_t qn = (size_t)(j * nx + nx - 1) * nv + k; nh = I.dFh[qn]; nb = I.dFb[qn]; }
+            } else if (fx == 1 && BACKWARD) {
+                if (i < nx - 1) { nh = sh[(cl + 1) * 32 + lane]; nb = sb[(cl + 1) * 32 + lane]; }
+                else { const size_t qn = (size_t)(j * nx) * nv + k; nh = I.dFh[qn]; nb = I.dFb[qn]; }
+            }
+            rh = rh - div_area(cmx * nh, P);
+            rb = rb - div_area(cmx * nb, P);
+            nh = 0.0; nb = 0.0;          // y inflow neighbour
+            if (fy == 2) {
+                if (j == 0) {
+                    if (BACKWARD) { nh = I.wall_drho[i] * whu; nb = I.wall_drho[i] * wbu; }
+                } else if (jl > 0) {
+                    nh = sh[(cl - nx) * 32 + lane]; nb = sb[(cl - nx) * 32 + lane];
+                } else if (BACKWARD) {
+                    const size_t qn = (size_t)((j - 1) * nx + i) * nv + k;
+                    nh = I.dFh[qn]; nb = I.dFb[qn];
+                }
+            } else if (fy == 3 && BACKWARD) {
+                if (j == ny - 1) { nh = I.wall_drho[nx + i] * whu; nb = I.wall_drho[nx + i] * wbu; }
+                else if (jl < rows - 1) { nh = sh[(cl + nx) * 32 + lane]; nb = sb[(cl + nx) * 32 + lane]; }
+                else { const size_t qn = (size_t)((j + 1) * nx + i) * nv + k; nh = I.dFh[qn]; nb = I.dFb[qn]; }
+            }
+            rh = rh - div_area(cmy * nh, P);
+            rb = rb - div_area(cmy * nb, P);
+            ok = ok && diag > 0.0 && isfinite(diag) && isfinite(rh) && isfinite(rb);
+            const double oh = rh / diag, ob = rb / diag;
+            sh[cl * 32 + lane] = oh;
+            sb[cl * 32 + lane] = ob;
+            const size_t q = (size_t)(c0 + cl) * nv + k;
+            outh[q] = oh;
+            outb[q] = ob;
+        }
+        if ((it + 1) % nchunk == 0) __syncthreads();
     }
     if (!ok) stop_with(I, B.status, ST_NONFINITE_STATE);
 }
@@ -962,27 +1146,48 @@ static cudaError_t im_fluxes(const LoParams& P, const LoBuffers& B, cudaStream_t
 // One ImplicitSteady pseudo-step (mod_Solve.f90:84-293 with TimeIntegration_method =
 // 'ImplicitSteady' and ClosedCouetteMassRescale): 19 kernels, no host synchronisation.
 // Returns the number of kernels launched through *launches.
+// Shared-memory opt-in of the sweep kernels for this slab size (slab rows x nx <= kMaxSlabCells).
+cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q) {
+    const int rows = P.ny / Q.nslab, ncs = rows * P.nx;
+    const int pr_bytes = pr_smem_words(rows, P.nx) * (int)sizeof(double);
+    if (ncs > kMaxSlabCells || pr_bytes + 8192 > 227 * 1024) return cudaErrorInvalidValue;
+    cudaError_t e = cudaFuncSetAttribute(k_im_pr2_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, pr_bytes);
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_im_lusgs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ncs * 64 * (int)sizeof(double));
+    if (e == cudaSuccess)
+        e = cudaFuncSetAttribute(k_im_lusgs<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, ncs * 64 * (int)sizeof(double));
+    return e;
+}
+
 cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
                                   cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
                                   long long* launches) {
     const int nc = P.nx * P.ny;
+    // The pre-update evaluation reuses the previous accepted-state evaluation when the state and dt
+    // are unchanged since (dt is set by the velocity-table extent unless a cell outruns it).
+    LoBuffers Bpre = B;
+    Bpre.eval = I.state + IS_EVAL_VALID;
     cudaError_t e = launch_lo_timestep(P, B, s);                              // TimeStep
-    if (e == cudaSuccess) e = im_fluxes(P, B, s, s2, fork, join);            // Interpolation + Evolution
-    if (e == cudaSuccess) e = im_cell(0, P, B, Q, I, nullptr, s);             // ComputeResidual + diagnostics
+    if (e == cudaSuccess) e = im_fluxes(P, Bpre, s, s2, fork, join);         // Interpolation + Evolution
+    if (e == cudaSuccess) e = im_cell(0, P, Bpre, Q, I, nullptr, s);          // ComputeResidual + diagnostics
     if (e == cudaSuccess) { k_im_pr2_prep<<<(nc * 4 + 127) / 128, 128, 0, s>>>(P, B, Q, I); e = cudaGetLastError(); }
     const double* X = I.dwA;
     double* Y = I.dwB;
+    const int rows = P.ny / Q.nslab, ncs = rows * P.nx;
+    const int dcells = rows < P.nx ? rows : P.nx;                          // longest anti-diagonal
+    const int pr_threads = 4 * (dcells < 32 ? dcells : 32);
+    const int lu_warps = dcells < 8 ? dcells : 8;
     for (int sw = 0; sw < Q.macro_sweeps && e == cudaSuccess; ++sw) {        // SolveMacroPR2
-        k_im_pr2_sweep<<<(Q.nslab + 31) / 32, 32, 0, s>>>(P, B, Q, I, X, Y);
+        k_im_pr2_sweep<<<Q.nslab, pr_threads, (size_t)pr_smem_words(rows, P.nx) * sizeof(double), s>>>(P, B, Q, I, X, Y);
         e = cudaGetLastError();
         const double* t = Y; Y = const_cast<double*>(X); X = t;
     }
     if (e == cudaSuccess) { k_im_macro_alpha<<<(nc + 127) / 128, 128, 0, s>>>(P, B, Q, I, X); e = cudaGetLastError(); }
     if (e == cudaSuccess) e = im_cell(2, P, B, Q, I, X, s);                   // BuildPredictedEquilibrium
-    const int nl = Q.nslab * P.nvel;
-    if (e == cudaSuccess) { k_im_lusgs<false><<<(nl + 255) / 256, 256, 0, s>>>(P, B, Q, I); e = cudaGetLastError(); }
+    const dim3 lu_grid((unsigned)((P.nvel + 31) / 32), (unsigned)Q.nslab);
+    if (e == cudaSuccess) { k_im_lusgs<false><<<lu_grid, 32 * lu_warps, (size_t)ncs * 64 * sizeof(double), s>>>(P, B, Q, I); e = cudaGetLastError(); }
     if (e == cudaSuccess) e = im_cell(3, P, B, Q, I, nullptr, s);             // frozen wall closure
-    if (e == cudaSuccess) { k_im_lusgs<true><<<(nl + 255) / 256, 256, 0, s>>>(P, B, Q, I); e = cudaGetLastError(); }
+    if (e == cudaSuccess) { k_im_lusgs<true><<<lu_grid, 32 * lu_warps, (size_t)ncs * 64 * sizeof(double), s>>>(P, B, Q, I); e = cudaGetLastError(); }
     if (e == cudaSuccess) e = im_cell(4, P, B, Q, I, nullptr, s);             // FindAdmissibleMicroAlpha
     if (e == cudaSuccess) e = im_cell(5, P, B, Q, I, nullptr, s);             // update + RecoverMacro
     if (e == cudaSuccess) { k_im_rescale<<<148 * 4, 256, 0, s>>>(P, B, Q, I); e = cudaGetLastError(); }

@@ -18,8 +18,12 @@ enum : int {
     IS_MALPHA = 9,      // macro alpha of the last step
     IS_MOMENT = 10,     // implicit_moment_error of the last update
     IS_CONVERGED = 11,  // 1 once the streak reached 5
-    IS_COUNT = 16
+    IS_EVAL_VALID = 12, // 1: slopes, fluxes and steady rates still hold the evaluation of the current
+    IS_EVAL_DT = 13,    //    state at dt = state[IS_EVAL_DT] (written by the accepted-state evaluation)
+    IS_PRESCI = 16,     // [22] science_1..22 of that evaluation before the mass-rescale override
+    IS_COUNT = 40
 };
+constexpr int kStatePublic = 16;   // leading state slots copied out by ugks_implicit_state
 
 // Layout of the per-step report (the accepted state's sparse_residual.csv row):
 // [0] gate pass, [1] moment, [2] M_W, [3] M_h, [4..11] R1..R8, [12..33] science_1..22,
@@ -27,6 +31,7 @@ enum : int {
 // [54] macro alpha, [55] dt, [56] streak, [57..78] science of the pre-update evaluation.
 constexpr int kReport = 80;
 constexpr int kImCell = 20;   // per-cell diagnostic terms
+constexpr int kMaxSlabCells = 384;   // rows x nx of one slab held in shared memory by the sweep kernels
 
 struct ImParams {
     int nslab;              // ranks of the reference's 1 x NP_Y blocking (rows per slab = ny / nslab)
@@ -47,8 +52,8 @@ struct ImBuffers {
     double* pr_foj;         // [nc][4 faces][4] Euler normal flux of the neighbour (or Zhu ghost) state
     double* wt;             // [nc][4] w_tilde
     double* tau_t;          // [nc] tau_tilde
-    double* eq_h;           // [nc][nvel] predicted equilibrium
-    double* eq_b;
+    double* rhs_h;          // [nc][nvel] stream + (G_predicted - h) / tau_tilde: the velocity-local part of
+    double* rhs_b;          //            RelaxMicroPoint's right-hand side, shared by both LU-SGS stages
     double* dFh;            // [nc][nvel] forward-stage corrections
     double* dFb;
     double* dBh;            // [nc][nvel] backward-stage (final) corrections

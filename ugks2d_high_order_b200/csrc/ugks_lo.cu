@@ -22,6 +22,7 @@ namespace ugks {
 // the wall rows the y slope is the one-sided (right-left)/dy of InterpBoundary (:100-117), and
 // UnifiedPhysicalOperators skips the Van-Leer inner loop there (:40-45,78-88).
 __global__ void __launch_bounds__(256) k_lo_slopes(LoParams P, LoBuffers B) {
+    if (eval_cached(B)) return;
     // grid: x covers the velocity row, y = cell; 32-bit index arithmetic only
     const int nv = P.nvel, nx = P.nx, ny = P.ny;
     const int k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -451,6 +452,7 @@ __device__ __forceinline__ void lo_face_wall(const LoParams& P, const LoBuffers&
 
 template <int VPT, int NTMAX>
 __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_faces(LoParams P, LoBuffers B) {
+    if (eval_cached(B)) return;
     __shared__ double red[16 * 64];
     __shared__ double rout[kRedSlots];
     __shared__ double sc[32];
@@ -473,6 +475,7 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_faces(LoParams P, LoB
 
 template <int VPT, int NTMAX>
 __global__ void __launch_bounds__(NTMAX) k_lo_walls(LoParams P, LoBuffers B) {
+    if (eval_cached(B)) return;
     __shared__ double red[16 * 64];
     __shared__ double rout[kRedSlots];
     const double dt = B.dt[0];

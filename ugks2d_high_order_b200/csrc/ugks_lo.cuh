@@ -16,7 +16,14 @@ struct LoParams {
     double wall_lam[2];      // 1/Tw per wall
     double fixed_dt;         // > 0: Time_global_fixed
     double inv_dx, inv_dy;   // 1/dx, 1/dy for the slope stencils
+    double inv_area;         // 1/area when area is a power of two (then x/area == x*inv_area exactly), else 0
 };
+
+// x / area, as a multiplication when that is exact (area a power of two: both operations round the
+// same real number x * 2^-e once)
+__device__ __forceinline__ double div_area(double x, const LoParams& P) {
+    return P.inv_area != 0.0 ? x * P.inv_area : x / P.area;
+}
 
 struct LoBuffers {
     const double* u;         // [nvel] velocity table, k = i + j*Nu
@@ -49,7 +56,14 @@ struct LoBuffers {
     double* wall_aero;       // [2][nx][3] local-frame pnn, pnt, qn per wall face
     unsigned* counter;       // [1] last-CTA counter (self-resetting)
     unsigned* status;        // [1] error bits
+    const double* eval;      // [2] {valid, dt}: when valid and dt == dt[0], the slopes, fluxes and rates
+                             // of the current state are already in place and the evaluation returns
+                             // at entry (nullptr: always evaluate)
 };
+
+__device__ __forceinline__ bool eval_cached(const LoBuffers& B) {
+    return B.eval != nullptr && B.eval[0] != 0.0 && B.eval[1] == B.dt[0];
+}
 
 __device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i >= nx ? i - nx : i); }
 

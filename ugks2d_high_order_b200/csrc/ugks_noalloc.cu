@@ -114,6 +114,11 @@ extern "C" int ugks_step_explicit_noalloc(const ugks_params* prm, const double* 
     P.nx = nx; P.ny = ny; P.nvel = nv; P.ck = prm->ck;
     P.dx = prm->dx; P.dy = prm->dy;
     P.area = std::fabs((-prm->dx) * (-prm->dy) - (prm->dx) * (-prm->dy)) * 0.5;
+    {
+        int e2 = 0;
+        const double m2 = std::frexp(P.area, &e2);
+        P.inv_area = (m2 == 0.5 && std::isfinite(P.area)) ? std::ldexp(1.0, 1 - e2) : 0.0;
+    }
     P.gm1 = (double)(prm->ck + 4) / (double)(prm->ck + 2) - 1.0;
     P.pr = prm->pr; P.omega = prm->omega; P.mu_ref = prm->mu_ref; P.cfl = prm->cfl;
     P.umax = -INFINITY; P.vmax = -INFINITY;
