@@ -135,6 +135,11 @@ int ugks_implicit_steps(ugks_ctx* ctx, int max_steps, int* steps_done, int* conv
  * macro alpha, moment error, converged (see ugks_implicit.cuh); report[80] as above. */
 int ugks_implicit_state(ugks_ctx* ctx, double* state, double* report);
 
+/* Steady output fields of every cell, as Output writes them (src/mod_Output.f90:102-116):
+ * out[nc][10] = r, u, v, T (= 1/lambda), p (= r T / 2), sxx, sxy, syy (Get_Stress_Vec,
+ * src/mod_Tools.f90:409-432), qx, qy (GetHeatFlux_Vec, src/mod_Tools.f90:355-373). */
+int ugks_macro_fields(ugks_ctx* ctx, double* out);
+
 /* Wall Aerodynamics of the last Evolution (src/mod_Evolution.f90:2402-2409): out[2][nx][3] =
  * local-frame (pnn, pnt, qn) per bottom/top wall face. */
 int ugks_wall_aero(ugks_ctx* ctx, double* out);

@@ -15,6 +15,8 @@ Outputs (all small, committed):
      * the implicit "Implicit iter=2 ..." summary lines        (docs/release_checks/*/stdout.log)
      * converged 64-point profiles of the three methods        (docs/couette_results/profiles_three_methods.plt)
      * static-equilibrium residual / update maxima             (checks/VERIFICATION.json)
+     * end-of-run summaries of the explicit and implicit runs  (docs/couette_results/analysis.json):
+       step count, final selected residuals, c_final, per-wall native pnn/pnt/qn
 """
 import json
 import os
@@ -103,6 +105,15 @@ def main(ref):
     golden["profiles_columns"] = ["x", "y", "r", "u", "v", "T", "p", "sxx", "sxy", "syy", "qx", "qy"]
     ver = json.load(open(os.path.join(ref, "checks/VERIFICATION.json")))
     golden["static_equilibrium"] = {k: ver[k] for k in ("final_static_le", "static_le_19", "static_le_np1")}
+    summ = json.load(open(os.path.join(ref, "docs/couette_results/analysis.json")))["summary"]
+    for case in ("low_explicit", "low_implicit"):
+        c = summ[case]
+        keep = {k: c[k] for k in ("steps", "status", "selected_final", "c_final") if k in c}
+        if "final_walls" in c:
+            keep["final_walls"] = {w: {q: c["final_walls"][w][q] for q in ("native_pnn", "native_pnt", "native_qn")}
+                                   for w in c["final_walls"]}
+        keep["source"] = "docs/couette_results/analysis.json summary/" + case
+        golden[case + "_final"] = keep
     with open(os.path.join(HERE, "reference_golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
     print("wrote fixtures to", HERE)

@@ -23,12 +23,16 @@ UGKS_METHOD_IMPLICIT_STEADY = 1
 EXPORTS = [
     "ugks_ctx_create", "ugks_ctx_destroy", "ugks_upload_state", "ugks_download_state", "ugks_init_freestream",
     "ugks_timestep", "ugks_evolution", "ugks_compute_residual", "ugks_apply_explicit_update",
-    "ugks_step_explicit", "ugks_wall_aero", "ugks_copy_array", "ugks_last_status", "ugks_status_reference_code",
+    "ugks_step_explicit", "ugks_wall_aero", "ugks_macro_fields", "ugks_copy_array", "ugks_last_status", "ugks_status_reference_code",
     "ugks_error_string", "ugks_stream", "ugks_synchronize", "ugks_profile_enable", "ugks_profile_read",
     "ugks_launch_count", "ugks_step_explicit_noalloc", "ugks_implicit_init", "ugks_implicit_steps",
     "ugks_implicit_state",
 ]
 REPORT_LEN = 80
+# stages of one ImplicitSteady pseudo-step timed by the profile mode (kImStageNames in ugks_implicit.cuh)
+IMPLICIT_STAGES = ("timestep", "pre_evaluation", "pr2_prep", "pr2_sweep", "macro_alpha", "equilibrium",
+                   "lusgs_forward", "wall_closure", "lusgs_backward", "micro_alpha", "apply", "rescale",
+                   "post_fluxes", "post_residual")
 
 
 class UgksParams(ctypes.Structure):
@@ -78,6 +82,7 @@ def load(path=LIB_PATH):
     L.ugks_apply_explicit_update.argtypes = [vp, dp]
     L.ugks_step_explicit.argtypes = [vp, ctypes.c_int, dp, dp]
     L.ugks_wall_aero.argtypes = [vp, dp]
+    L.ugks_macro_fields.argtypes = [vp, dp]
     L.ugks_copy_array.argtypes = [vp, ctypes.c_char_p, dp, ctypes.c_size_t]
     L.ugks_last_status.argtypes = [vp]
     L.ugks_last_status.restype = ctypes.c_uint

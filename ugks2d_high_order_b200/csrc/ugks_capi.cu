@@ -18,6 +18,7 @@ cudaError_t launch_lo_faces(const LoParams& P, const LoBuffers& B, cudaStream_t 
 cudaError_t launch_lo_walls(const LoParams& P, const LoBuffers& B, cudaStream_t s);
 cudaError_t launch_lo_cells(const LoParams& P, const LoBuffers& B, int mode, bool collision, cudaStream_t s);
 cudaError_t launch_lo_timestep(const LoParams& P, const LoBuffers& B, cudaStream_t s);
+cudaError_t launch_lo_macro_fields(const LoParams& P, const LoBuffers& B, double* out, cudaStream_t s);
 cudaError_t launch_lo_init(const LoParams& P, const LoBuffers& B, double rho, double U, double V, double tn,
                            cudaStream_t s);
 cudaError_t launch_im_init(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
@@ -25,7 +26,7 @@ cudaError_t launch_im_init(const LoParams& P, const LoBuffers& B, const ImParams
 cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q);
 cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
                                   cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
-                                  long long* launches);
+                                  long long* launches, cudaEvent_t* marks);
 }  // namespace ugks
 
 using namespace ugks;
@@ -64,6 +65,8 @@ struct ugks_ctx {
     bool profile = false;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     KernelTimer t_slopes, t_faces, t_walls, t_cells;
+    cudaEvent_t im_ev[kImStages + 1] = {};
+    KernelTimer im_t[kImStages];
 };
 
 static int cuda_fail(cudaError_t e) {
@@ -232,6 +235,7 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->imem) cudaFree(c->imem);
     if (c->iflags) cudaFree(c->iflags);
     for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
+    for (int i = 0; i <= kImStages; ++i) if (c->im_ev[i]) cudaEventDestroy(c->im_ev[i]);
     if (c->dmem) cudaFree(c->dmem);
     if (c->dflags) cudaFree(c->dflags);
     if (c->stream2) { cudaStreamSynchronize(c->stream2); cudaStreamDestroy(c->stream2); }
@@ -434,6 +438,20 @@ extern "C" int ugks_step_explicit(ugks_ctx* c, int nsteps, double* dt_out, doubl
     return read_step_outputs(c, dt_out, res_out);
 }
 
+extern "C" int ugks_macro_fields(ugks_ctx* c, double* out) {
+    if (!c || !out) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    const size_t n = (size_t)c->P.nx * c->P.ny * 10;
+    double* d = nullptr;
+    UGKS_CK(cudaMallocAsync(&d, n * sizeof(double), c->stream));
+    cudaError_t e = launch_lo_macro_fields(c->P, c->B, d, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d, n * sizeof(double), cudaMemcpyDeviceToHost, c->stream);
+    cudaFreeAsync(d, c->stream);
+    UGKS_CK(e);
+    c->launches += 1;
+    return collect_status(c);
+}
+
 extern "C" int ugks_wall_aero(ugks_ctx* c, double* out) {
     if (!c || !out) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
@@ -488,6 +506,7 @@ extern "C" int ugks_profile_enable(ugks_ctx* c, int enable) {
     c->t_faces = KernelTimer();
     c->t_walls = KernelTimer();
     c->t_cells = KernelTimer();
+    for (int q = 0; q < kImStages; ++q) c->im_t[q] = KernelTimer();
     return UGKS_OK;
 }
 
@@ -498,7 +517,9 @@ extern "C" int ugks_profile_read(ugks_ctx* c, const char* kernel, double* total_
     else if (!std::strcmp(kernel, "faces")) t = &c->t_faces;
     else if (!std::strcmp(kernel, "walls")) t = &c->t_walls;
     else if (!std::strcmp(kernel, "cells")) t = &c->t_cells;
-    else return UGKS_EINVAL;
+    for (int q = 0; q < kImStages && !t; ++q)
+        if (!std::strcmp(kernel, kImStageNames[q])) t = &c->im_t[q];
+    if (!t) return UGKS_EINVAL;
     if (total_ms) *total_ms = t->total_ms;
     if (launches) *launches = t->launches;
     return UGKS_OK;
@@ -527,7 +548,7 @@ static int build_implicit_graph(ugks_ctx* c, int steps) {
     UGKS_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
     for (int s = 0; s < steps && e == cudaSuccess; ++s)
-        e = enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork, c->ev_join, &n);
+        e = enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork, c->ev_join, &n, nullptr);
     cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
     if (e != cudaSuccess) { if (e2 == cudaSuccess) cudaGraphDestroy(g); return cuda_fail(e); }
     UGKS_CK(e2);
@@ -551,7 +572,22 @@ extern "C" int ugks_implicit_steps(ugks_ctx* c, int max_steps, int* steps_done, 
     const double start = st[IS_STEPS];
     int left = max_steps;
     while (left > 0 && st[IS_STOP] == 0.0) {
-        if (left >= G) {
+        if (c->profile) {   // un-graphed, one step at a time, with an event after every stage
+            for (int q = 0; q <= kImStages; ++q)
+                if (!c->im_ev[q]) UGKS_CK(cudaEventCreate(&c->im_ev[q]));
+            long long n = 0;
+            UGKS_CK(enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork, c->ev_join, &n,
+                                          c->im_ev));
+            UGKS_CK(cudaEventSynchronize(c->im_ev[kImStages]));
+            for (int q = 0; q < kImStages; ++q) {
+                float ms = 0.f;
+                UGKS_CK(cudaEventElapsedTime(&ms, c->im_ev[q], c->im_ev[q + 1]));
+                c->im_t[q].total_ms += ms;
+                c->im_t[q].launches += 1;
+            }
+            c->launches += n;
+            left -= 1;
+        } else if (left >= G) {
             int r = build_implicit_graph(c, G);
             if (r) return r;
             UGKS_CK(cudaGraphLaunch(c->igraph, c->stream));
@@ -561,7 +597,7 @@ extern "C" int ugks_implicit_steps(ugks_ctx* c, int max_steps, int* steps_done, 
             long long n = 0;
             for (int s = 0; s < left; ++s)
                 UGKS_CK(enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork,
-                                              c->ev_join, &n));
+                                              c->ev_join, &n, nullptr));
             c->launches += n;
             left = 0;
         }

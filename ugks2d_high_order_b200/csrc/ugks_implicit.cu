@@ -1159,40 +1159,50 @@ cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q) {
     return e;
 }
 
+// One accepted pseudo-step.  marks (optional, profile runs only): kImStages + 1 events recorded on
+// s at the start and after each stage of kImStageNames.
 cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
                                   cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
-                                  long long* launches) {
+                                  long long* launches, cudaEvent_t* marks) {
     const int nc = P.nx * P.ny;
+    int stage = 0;
+    auto mark = [&](cudaError_t e) -> cudaError_t {
+        if (e == cudaSuccess && marks) e = cudaEventRecord(marks[stage++], s);
+        return e;
+    };
     // The pre-update evaluation reuses the previous accepted-state evaluation when the state and dt
     // are unchanged since (dt is set by the velocity-table extent unless a cell outruns it).
     LoBuffers Bpre = B;
     Bpre.eval = I.state + IS_EVAL_VALID;
-    cudaError_t e = launch_lo_timestep(P, B, s);                              // TimeStep
-    if (e == cudaSuccess) e = im_fluxes(P, Bpre, s, s2, fork, join);         // Interpolation + Evolution
-    if (e == cudaSuccess) e = im_cell(0, P, Bpre, Q, I, nullptr, s);          // ComputeResidual + diagnostics
-    if (e == cudaSuccess) { k_im_pr2_prep<<<(nc * 4 + 127) / 128, 128, 0, s>>>(P, B, Q, I); e = cudaGetLastError(); }
+    cudaError_t e = mark(cudaSuccess);
+    if (e == cudaSuccess) e = mark(launch_lo_timestep(P, B, s));                 // TimeStep
+    if (e == cudaSuccess) e = im_fluxes(P, Bpre, s, s2, fork, join);             // Interpolation + Evolution
+    if (e == cudaSuccess) e = mark(im_cell(0, P, Bpre, Q, I, nullptr, s));       // ComputeResidual + diagnostics
+    if (e == cudaSuccess) { k_im_pr2_prep<<<(nc * 4 + 127) / 128, 128, 0, s>>>(P, B, Q, I); e = mark(cudaGetLastError()); }
     const double* X = I.dwA;
     double* Y = I.dwB;
     const int rows = P.ny / Q.nslab, ncs = rows * P.nx;
-    const int dcells = rows < P.nx ? rows : P.nx;                          // longest anti-diagonal
+    const int dcells = rows < P.nx ? rows : P.nx;                              // longest anti-diagonal
     const int pr_threads = 4 * (dcells < 32 ? dcells : 32);
     const int lu_warps = dcells < 8 ? dcells : 8;
-    for (int sw = 0; sw < Q.macro_sweeps && e == cudaSuccess; ++sw) {        // SolveMacroPR2
+    for (int sw = 0; sw < Q.macro_sweeps && e == cudaSuccess; ++sw) {            // SolveMacroPR2
         k_im_pr2_sweep<<<Q.nslab, pr_threads, (size_t)pr_smem_words(rows, P.nx) * sizeof(double), s>>>(P, B, Q, I, X, Y);
         e = cudaGetLastError();
         const double* t = Y; Y = const_cast<double*>(X); X = t;
     }
-    if (e == cudaSuccess) { k_im_macro_alpha<<<(nc + 127) / 128, 128, 0, s>>>(P, B, Q, I, X); e = cudaGetLastError(); }
-    if (e == cudaSuccess) e = im_cell(2, P, B, Q, I, X, s);                   // BuildPredictedEquilibrium
+    e = mark(e);
+    if (e == cudaSuccess) { k_im_macro_alpha<<<(nc + 127) / 128, 128, 0, s>>>(P, B, Q, I, X); e = mark(cudaGetLastError()); }
+    if (e == cudaSuccess) e = mark(im_cell(2, P, B, Q, I, X, s));                // BuildPredictedEquilibrium
     const dim3 lu_grid((unsigned)((P.nvel + 31) / 32), (unsigned)Q.nslab);
-    if (e == cudaSuccess) { k_im_lusgs<false><<<lu_grid, 32 * lu_warps, (size_t)ncs * 64 * sizeof(double), s>>>(P, B, Q, I); e = cudaGetLastError(); }
-    if (e == cudaSuccess) e = im_cell(3, P, B, Q, I, nullptr, s);             // frozen wall closure
-    if (e == cudaSuccess) { k_im_lusgs<true><<<lu_grid, 32 * lu_warps, (size_t)ncs * 64 * sizeof(double), s>>>(P, B, Q, I); e = cudaGetLastError(); }
-    if (e == cudaSuccess) e = im_cell(4, P, B, Q, I, nullptr, s);             // FindAdmissibleMicroAlpha
-    if (e == cudaSuccess) e = im_cell(5, P, B, Q, I, nullptr, s);             // update + RecoverMacro
-    if (e == cudaSuccess) { k_im_rescale<<<148 * 4, 256, 0, s>>>(P, B, Q, I); e = cudaGetLastError(); }
-    if (e == cudaSuccess) e = im_fluxes(P, B, s, s2, fork, join);            // accepted-state evaluation
-    if (e == cudaSuccess) e = im_cell(1, P, B, Q, I, nullptr, s);
+    const size_t lu_smem = (size_t)ncs * 64 * sizeof(double);
+    if (e == cudaSuccess) { k_im_lusgs<false><<<lu_grid, 32 * lu_warps, lu_smem, s>>>(P, B, Q, I); e = mark(cudaGetLastError()); }
+    if (e == cudaSuccess) e = mark(im_cell(3, P, B, Q, I, nullptr, s));          // frozen wall closure
+    if (e == cudaSuccess) { k_im_lusgs<true><<<lu_grid, 32 * lu_warps, lu_smem, s>>>(P, B, Q, I); e = mark(cudaGetLastError()); }
+    if (e == cudaSuccess) e = mark(im_cell(4, P, B, Q, I, nullptr, s));          // FindAdmissibleMicroAlpha
+    if (e == cudaSuccess) e = mark(im_cell(5, P, B, Q, I, nullptr, s));          // update + RecoverMacro
+    if (e == cudaSuccess) { k_im_rescale<<<148 * 4, 256, 0, s>>>(P, B, Q, I); e = mark(cudaGetLastError()); }
+    if (e == cudaSuccess) e = mark(im_fluxes(P, B, s, s2, fork, join));         // accepted-state evaluation
+    if (e == cudaSuccess) e = mark(im_cell(1, P, B, Q, I, nullptr, s));
     if (launches) *launches += 16 + Q.macro_sweeps;
     return e;
 }

@@ -33,6 +33,12 @@ constexpr int kReport = 80;
 constexpr int kImCell = 20;   // per-cell diagnostic terms
 constexpr int kMaxSlabCells = 384;   // rows x nx of one slab held in shared memory by the sweep kernels
 
+// Stages of one pseudo-step, in launch order, for the per-stage event timing of profile runs.
+constexpr int kImStages = 14;
+constexpr const char* kImStageNames[kImStages] = {
+    "timestep", "pre_evaluation", "pr2_prep", "pr2_sweep", "macro_alpha", "equilibrium", "lusgs_forward",
+    "wall_closure", "lusgs_backward", "micro_alpha", "apply", "rescale", "post_fluxes", "post_residual"};
+
 struct ImParams {
     int nslab;              // ranks of the reference's 1 x NP_Y blocking (rows per slab = ny / nslab)
     int mass_rescale;

@@ -92,48 +92,83 @@ __device__ __forceinline__ void lo_face_interior(const LoParams& P, const LoBuff
         acc[7] += 0.5 * wk * (v2 * sht + sbt);
     }
     block_reduce_smem<8, 0>(acc, red, rout);
-    // face state, micro slopes aL, aR, b, A and the time coefficients: one thread computes them
-    // (GetPrimary, MicroSlope x4, CalcMoment, GetTau, Mt) and broadcasts through shared memory.
-    if (tid == 0) {
+    // face state, micro slopes aL, aR, b, A and the time coefficients (GetPrimary, MicroSlope x4,
+    // CalcMoment, GetTau, Mt): five independent scalar chains, each run by lane 0 of its own warp so
+    // they proceed concurrently, then the time slope A, which needs the first four.  Results go
+    // through shared memory: sc[0..3] face prim, [4..19] aL aR b A, [20..24] Mt, [25] Mxi[2],
+    // [32..61] the CalcMoment tables, [64..75] the three Moment_auvxi terms of A.
+    {
+        const int nw = blockDim.x >> 5, w = tid >> 5;
+        const bool lane0 = (tid & 31) == 0;
         Prim pf;
         const double cv[4] = {rout[0], rout[1], rout[2], rout[3]};
         const bool ok = get_primary(P.gm1, cv, pf);
         if (!ok) { pf.r = 1.0; pf.U = 0.0; pf.V = 0.0; pf.L = 1.0; }
-        const double* WL = B.W + cL * 4;
-        const double* WR = B.W + cR * 4;
-        double wl[4], wr[4];
-        wl[0] = WL[0]; wl[3] = WL[3]; wr[0] = WR[0]; wr[3] = WR[3];
-        if (dir == 0) { wl[1] = WL[1]; wl[2] = WL[2]; wr[1] = WR[1]; wr[2] = WR[2]; }
-        else { wl[1] = WL[2]; wl[2] = -WL[1]; wr[1] = WR[2]; wr[2] = -WR[1]; }
-        double sw[4], aL[4], aR[4], bs[4], aT[4], Mt[5], tau = 1.0;
+        if (lane0) {
+            for (int piece = w; piece < 5; piece += nw) {
+                if (piece <= 1) {            // aL from (W_face - W_L) / (dx/2), aR from (W_R - W_face) / (dx/2)
+                    const double* Wc = B.W + (piece == 0 ? cL : cR) * 4;
+                    double wc[4], sw[4], a4[4];
+                    wc[0] = Wc[0]; wc[3] = Wc[3];
+                    if (dir == 0) { wc[1] = Wc[1]; wc[2] = Wc[2]; }
+                    else { wc[1] = Wc[2]; wc[2] = -Wc[1]; }
 #pragma unroll
-        for (int m = 0; m < 4; ++m) sw[m] = (cv[m] - wl[m]) / hl;
-        micro_slope(P.ck, pf, sw, aL);
+                    for (int m = 0; m < 4; ++m) sw[m] = piece == 0 ? (cv[m] - wc[m]) / hl : (wc[m] - cv[m]) / hl;
+                    micro_slope(P.ck, pf, sw, a4);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) sw[m] = (wr[m] - cv[m]) / hl;
-        micro_slope(P.ck, pf, sw, aR);
-        const double swt[4] = {rout[4], rout[5], rout[6], rout[7]};
-        micro_slope(P.ck, pf, swt, bs);
-        Moments M;
-        calc_moment(P.ck, pf, M);
-        double MauL[4], MauR[4], Mbv[4];
-        moment_auvxi(aL, M.MuL, M.Mv, M.Mxi, 1, 0, MauL);
-        moment_auvxi(aR, M.MuR, M.Mv, M.Mxi, 1, 0, MauR);
-        moment_auvxi(bs, M.Mu, M.Mv, M.Mxi, 0, 1, Mbv);
+                    for (int m = 0; m < 4; ++m) sc[4 + 4 * piece + m] = a4[m];
+                    if (piece == 0) {
+                        sc[0] = pf.r; sc[1] = pf.U; sc[2] = pf.V; sc[3] = pf.L;
+                        if (!ok) set_status(B.status, ST_GETPRIMARY);
+                    }
+                } else if (piece == 2) {     // b from the tangential slope moments
+                    const double swt[4] = {rout[4], rout[5], rout[6], rout[7]};
+                    double a4[4];
+                    micro_slope(P.ck, pf, swt, a4);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) sw[m] = -pf.r * (MauL[m] + MauR[m] + Mbv[m]);
-        micro_slope(P.ck, pf, sw, aT);
-        const bool tok = get_tau(P.mu_ref, P.omega, pf, tau);
-        if (!tok) tau = 1.0;
-        time_coeffs(dt, tau, Mt);
-        if (!ok) set_status(B.status, ST_GETPRIMARY);
-        if (ok && !tok) set_status(B.status, ST_TAU);
-        sc[0] = pf.r; sc[1] = pf.U; sc[2] = pf.V; sc[3] = pf.L;
+                    for (int m = 0; m < 4; ++m) sc[12 + m] = a4[m];
+                } else if (piece == 3) {     // CalcMoment tables
+                    Moments M;
+                    calc_moment(P.ck, pf, M);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) { sc[4 + m] = aL[m]; sc[8 + m] = aR[m]; sc[12 + m] = bs[m]; sc[16 + m] = aT[m]; }
+                    for (int m = 0; m <= kMNUM; ++m) { sc[32 + m] = M.Mu[m]; sc[39 + m] = M.MuL[m]; sc[46 + m] = M.MuR[m]; }
 #pragma unroll
-        for (int m = 0; m < 5; ++m) sc[20 + m] = Mt[m];
-        sc[25] = M.Mxi[2];
+                    for (int m = 0; m <= kMTUM; ++m) sc[53 + m] = M.Mv[m];
+#pragma unroll
+                    for (int m = 0; m < 3; ++m) sc[59 + m] = M.Mxi[m];
+                    sc[25] = M.Mxi[2];
+                } else {                     // GetTau and Mt(1..5)
+                    double tau = 1.0, Mt[5];
+                    const bool tok = get_tau(P.mu_ref, P.omega, pf, tau);
+                    if (!tok) tau = 1.0;
+                    time_coeffs(dt, tau, Mt);
+#pragma unroll
+                    for (int m = 0; m < 5; ++m) sc[20 + m] = Mt[m];
+                    if (ok && !tok) set_status(B.status, ST_TAU);
+                }
+            }
+        }
+        __syncthreads();
+        if (lane0) {
+            for (int piece = w; piece < 3; piece += nw) {   // Moment_auvxi of aL (MuL), aR (MuR), b (Mu, v)
+                double a4[4], o4[4];
+#pragma unroll
+                for (int m = 0; m < 4; ++m) a4[m] = sc[4 + 4 * piece + m];
+                const double* Mu = sc + (piece == 0 ? 39 : (piece == 1 ? 46 : 32));
+                moment_auvxi(a4, Mu, sc + 53, sc + 59, piece == 2 ? 0 : 1, piece == 2 ? 1 : 0, o4);
+#pragma unroll
+                for (int m = 0; m < 4; ++m) sc[64 + 4 * piece + m] = o4[m];
+            }
+        }
+        __syncthreads();
+        if (tid == 0) {
+            double sw[4], aT[4];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) sw[m] = -pf.r * (sc[64 + m] + sc[68 + m] + sc[72 + m]);
+            micro_slope(P.ck, pf, sw, aT);
+#pragma unroll
+            for (int m = 0; m < 4; ++m) sc[16 + m] = aT[m];
+        }
     }
     __syncthreads();
     const Prim pf{sc[0], sc[1], sc[2], sc[3]};
@@ -455,7 +490,7 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_faces(LoParams P, LoB
     if (eval_cached(B)) return;
     __shared__ double red[16 * 64];
     __shared__ double rout[kRedSlots];
-    __shared__ double sc[32];
+    __shared__ double sc[80];
     const double dt = B.dt[0];
     const int nx = P.nx, ny = P.ny, nv = P.nvel;
     int f = blockIdx.x;
@@ -1016,6 +1051,54 @@ cudaError_t launch_lo_cells(const LoParams& P, const LoBuffers& B, int mode, boo
 
 cudaError_t launch_lo_timestep(const LoParams& P, const LoBuffers& B, cudaStream_t s) {
     k_lo_timestep<<<1, 256, 0, s>>>(P, B);
+    return cudaGetLastError();
+}
+
+// -------------------------------------------------------------------------------------------
+// Steady output fields of one cell (Output, mod_Output.f90:102-116): r, u, v, T = 1/lambda,
+// p = r T / 2, the stress tensor sxx, sxy, syy (Get_Stress_Vec with GetPressure_Vec,
+// mod_Tools.f90:326-347,409-432) and the heat flux qx, qy (GetHeatFlux_Vec, mod_Tools.f90:355-373).
+template <int VPT, int NTMAX>
+__global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_macro_fields(LoParams P, LoBuffers B, double* out) {
+    __shared__ double red[8 * 64];
+    __shared__ double rout[kRedSlots];
+    const int nv = P.nvel, c = blockIdx.x;
+    double w4[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) w4[m] = B.W[c * 4 + m];
+    Prim p;
+    const bool ok = get_primary(P.gm1, w4, p);
+    if (!ok) { p.r = 1.0; p.U = p.V = 0.0; p.L = 1.0; }
+    double acc[7] = {0.0, 0.0, 0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int r = 0; r < VPT; ++r) {
+        const Slot s = slot(r, nv);
+        const double wk = s.ok ? B.w[s.kk] : 0.0;
+        const double dvn = B.u[s.kk] - p.U, dvt = B.v[s.kk] - p.V, v2 = dvn * dvn + dvt * dvt;
+        const double h = B.h[(size_t)c * nv + s.kk], b = B.b[(size_t)c * nv + s.kk];
+        acc[0] += wk * v2 * h;                       // energy_sum
+        acc[1] += wk * b;                            // b_sum
+        acc[2] += wk * dvn * dvn * h;
+        acc[3] += wk * dvn * dvt * h;
+        acc[4] += wk * dvt * dvt * h;
+        acc[5] += 0.5 * wk * dvn * (v2 * h + b);
+        acc[6] += 0.5 * wk * dvt * (v2 * h + b);
+    }
+    block_reduce_smem<7, 0>(acc, red, rout);
+    if (threadIdx.x == 0) {
+        const double pr = (rout[0] + rout[1]) / ((double)P.ck + 2.0);
+        const double T = 1.0 / p.L;
+        double* o = out + (size_t)c * 10;
+        o[0] = p.r; o[1] = p.U; o[2] = p.V; o[3] = T; o[4] = 0.5 * p.r * T;
+        o[5] = rout[2] - pr; o[6] = rout[3]; o[7] = rout[4] - pr;
+        o[8] = rout[5]; o[9] = rout[6];
+        if (!ok) set_status(B.status, ST_GETPRIMARY);
+    }
+}
+
+cudaError_t launch_lo_macro_fields(const LoParams& P, const LoBuffers& B, double* out, cudaStream_t s) {
+    if (lo_vpt(P.nvel) == 4) k_lo_macro_fields<4, 256><<<P.nx * P.ny, lo_threads(P.nvel), 0, s>>>(P, B, out);
+    else k_lo_macro_fields<5, 512><<<P.nx * P.ny, lo_threads(P.nvel), 0, s>>>(P, B, out);
     return cudaGetLastError();
 }
 

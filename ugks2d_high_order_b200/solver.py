@@ -139,6 +139,19 @@ class Solver:
         self._check(self.L.ugks_wall_aero(self.ctx, _p(out)), "wall_aero")
         return out
 
+    FIELDS = ("r", "u", "v", "T", "p", "sxx", "sxy", "syy", "qx", "qy")
+
+    def macro_fields(self):
+        """Output's steady fields per cell (mod_Output.f90:102-116), computed on the device:
+        array [ny][nx][10] in the order of `FIELDS`."""
+        out = np.empty((self.ny, self.nx, 10))
+        self._check(self.L.ugks_macro_fields(self.ctx, _p(out)), "macro_fields")
+        return out
+
+    def profiles(self):
+        """x-averaged 64-point profiles of `FIELDS` (the rows of profiles_three_methods.plt)."""
+        return self.macro_fields().mean(axis=1)
+
     def array(self, name, shape):
         out = np.empty(int(np.prod(shape)))
         self._check(self.L.ugks_copy_array(self.ctx, name.encode(), _p(out), out.size), f"copy {name}")
