@@ -25,6 +25,7 @@ class UOParams(ctypes.Structure):
         ("ncfl", ctypes.c_double), ("nslab", ctypes.c_int), ("mass_rescale", ctypes.c_int),
         ("macro_sweeps", ctypes.c_int),
         ("residual_tol", ctypes.c_double), ("moment_tol", ctypes.c_double), ("min_alpha", ctypes.c_double),
+        ("high_order", ctypes.c_int),
     ]
 
 
@@ -57,6 +58,9 @@ def lib():
         L.uo_apply_explicit_update.argtypes = [ctypes.c_void_p, ctypes.c_double, dp]
         L.uo_implicit_step.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
         L.uo_implicit_init.argtypes = [ctypes.c_void_p]
+        L.uo_s2_evolution.argtypes = [ctypes.c_void_p, ctypes.c_double]
+        L.uo_s2_compute_residual.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
+        L.uo_s2_init_state.argtypes = [ctypes.c_void_p]
         for name in ("uo_res_macro", "uo_res_h", "uo_res_b", "uo_wall_aero", "uo_face_x_h", "uo_face_y_h",
                      "uo_face_x_w", "uo_face_y_w", "uo_phys_eq_h", "uo_phys_col_h", "uo_phys_col_b"):
             f = getattr(L, name)
@@ -93,6 +97,7 @@ class Oracle:
         p.mass_rescale = int(case.mass_rescale)
         p.macro_sweeps = case.macro_sweeps
         p.residual_tol, p.moment_tol, p.min_alpha = case.residual_tol, case.moment_tol, case.min_alpha
+        p.high_order = int(case.method == "HighOrderImplicit")
         self._params = p
         self.ptr = lib().uo_create(ctypes.byref(p), _p(self.u), _p(self.v), _p(self.w))
 
@@ -108,6 +113,8 @@ class Oracle:
     def init_freestream(self, rho=1.0, U=0.0, V=0.0, tnative=None):
         t = self.case.tinf if tnative is None else tnative
         e = lib().uo_init_freestream(self.ptr, rho, U, V, t)
+        if not e and self.case.method == "HighOrderImplicit":
+            e = lib().uo_s2_init_state(self.ptr)   # S2NativeInitializeState cold start
         if e:
             raise RuntimeError(f"oracle init failed: {e}")
 

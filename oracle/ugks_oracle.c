@@ -50,6 +50,13 @@ struct uo_ctx {
     double mass_scale;
     int streak;
     double dt;
+    /* high-order S2 path (ugks_oracle_s2.c) */
+    double *s2_rec;               /* reconstruction cache [nc][nvel][72] */
+    double *s2_mh, *s2_mb, *s2_kxh, *s2_kxb, *s2_kyh, *s2_kyb;   /* volume targets [nc][nvel] */
+    double *s2_kappa;             /* [nc][2x2] */
+    double *lco_h, *lco_b;        /* low_collision_old [nc][nvel] */
+    double *s2_facc;              /* per-cell face flux accumulators */
+    void *s2_scr;                 /* per-thread closure scratch */
     /* scratch: 24 work vectors per OpenMP thread */
     int nthr;
     double **tt;
@@ -394,8 +401,10 @@ uo_ctx* uo_create(const uo_params* p, const double* u, const double* v, const do
     return c;
 }
 
+static void s2_free(uo_ctx* c);
 void uo_destroy(uo_ctx* c) {
     if (!c) return;
+    s2_free(c);
     double* ptrs[] = {c->u, c->v, c->w, c->h, c->b, c->W, c->sh, c->sb, c->fxh, c->fxb, c->fxw, c->fyLh, c->fyLb,
                       c->fyRh, c->fyRb, c->fyLw, c->fyRw, c->res_w, c->res_h, c->res_b, c->rate_w, c->stream_h,
                       c->stream_b, c->peq_h, c->peq_b, c->pcol_h, c->pcol_b, c->wall_aero};
@@ -1196,6 +1205,10 @@ static int lusgs_stage(uo_ctx* c, int s, int backward, double dt_pseudo) {
                 size_t q = (size_t)cc * nv + k;
                 double rhs_h = c->stream_h[q] + (c->eq_h[q] - c->h[q]) / c->tau_t[cc];
                 double rhs_b = c->stream_b[q] + (c->eq_b[q] - c->b[q]) / c->tau_t[cc];
+                if (p->high_order) {   /* mod_ImplicitMicro.f90:467-470 */
+                    rhs_h = rhs_h + c->pcol_h[q] - c->lco_h[q];
+                    rhs_b = rhs_b + c->pcol_b[q] - c->lco_b[q];
+                }
                 double diag = 1.0 / dt_pseudo + 1.0 / c->tau_t[cc];
                 for (int f = 0; f < 4; ++f) {
                     double un = c->u[k] * g[f].nx + c->v[k] * g[f].ny;
@@ -1374,15 +1387,21 @@ int uo_implicit_step(uo_ctx* c, double* out, int nout) {
     double dt = uo_timestep(c);
     if (!isfinite(dt)) return 101;
     c->dt = dt;
-    uo_interpolation(c);
-    if ((e = uo_evolution(c, dt))) return e;
-    if ((e = uo_compute_residual(c, dt, 1))) return e;
+    if (p->high_order) {   /* S2NativeEvolution; Interpolation is skipped (mod_Solve.f90:108) */
+        if ((e = uo_s2_evolution(c, dt))) return e;
+        if ((e = uo_s2_compute_residual(c, dt, 0))) return e;
+    } else {
+        uo_interpolation(c);
+        if ((e = uo_evolution(c, dt))) return e;
+        if ((e = uo_compute_residual(c, dt, 1))) return e;
+    }
     /* ApplySteadyImplicitUpdate -> ApplyOriginalSteadyImplicitUpdate (mod_SteadyImplicit.f90:379-462) */
     size_t S = (size_t)c->nc * nv;
     memcpy(c->save_h, c->h, S * sizeof(double));
     memcpy(c->save_b, c->b, S * sizeof(double));
     memcpy(c->save_W, c->W, (size_t)c->nc * 4 * sizeof(double));
-    if (!reassemble_rates(c, dt)) return 444;
+    if (p->high_order) { if ((e = uo_s2_compute_residual(c, dt, 1))) return e; }
+    else if (!reassemble_rates(c, dt)) return 444;
     double sci0[22];
     implicit_diagnostics(c, dt, sci0);
     memcpy(row + 57, sci0, sizeof sci0);
@@ -1421,6 +1440,20 @@ int uo_implicit_step(uo_ctx* c, double* out, int nout) {
         memcpy(T[2], eh, sizeof(double) * nv);
         memcpy(T[3], eb, sizeof(double) * nv);
         if (!uo_project_moments(nv, eh, eb, c->wt + cc * 4, c->u, c->v, c->w, T[2], T[3])) return 422;
+        if (p->high_order) {   /* low_collision_old (mod_ImplicitMicro.f90:66-79) */
+            double tau_o;
+            maxwell(p, nv, c->u, c->v, po, T[4], T[5]);
+            shakhov(p, nv, T[4], T[5], c->u, c->v, q, po, T[0], T[1]);
+            for (int k = 0; k < nv; ++k) { T[4][k] = T[4][k] + T[0][k]; T[5][k] = T[5][k] + T[1][k]; }
+            memcpy(T[2], T[4], sizeof(double) * nv);
+            memcpy(T[3], T[5], sizeof(double) * nv);
+            if (!uo_project_moments(nv, T[4], T[5], c->W + cc * 4, c->u, c->v, c->w, T[2], T[3])) return 422;
+            if ((e = get_tau(p, po, &tau_o))) return e;
+            for (int k = 0; k < nv; ++k) {
+                c->lco_h[(size_t)cc * nv + k] = (T[4][k] - c->h[(size_t)cc * nv + k]) / tau_o;
+                c->lco_b[(size_t)cc * nv + k] = (T[5][k] - c->b[(size_t)cc * nv + k]) / tau_o;
+            }
+        }
     }
     /* SolveMicroLUSGS with the frozen wall closure, one sweep pair */
     memset(c->dh_ghost, 0, S * sizeof(double));
@@ -1478,10 +1511,16 @@ int uo_implicit_step(uo_ctx* c, double* out, int nout) {
     /* AfterR5Accepted -> EvaluateSparseState (mod_R5Observe.f90:287-320) */
     double totals[5], metrics[5];
     if (!mass_statistics(c, totals, metrics)) return 941;
-    uo_interpolation(c);
-    if ((e = uo_evolution(c, dt))) return e;
-    if ((e = uo_compute_residual(c, dt, 1))) return e;
-    if (!reassemble_rates(c, dt)) return 444;
+    if (p->high_order) {
+        if ((e = uo_s2_evolution(c, dt))) return e;
+        if ((e = uo_s2_compute_residual(c, dt, 0))) return e;
+        if ((e = uo_s2_compute_residual(c, dt, 1))) return e;
+    } else {
+        uo_interpolation(c);
+        if ((e = uo_evolution(c, dt))) return e;
+        if ((e = uo_compute_residual(c, dt, 1))) return e;
+        if (!reassemble_rates(c, dt)) return 444;
+    }
     double sci[22];
     implicit_diagnostics(c, dt, sci);
     sci[18] = merr;   /* implicit_moment_error of this step (or the rescaled state's, below) */
@@ -1514,3 +1553,5 @@ int uo_implicit_step(uo_ctx* c, double* out, int nout) {
     if (out) memcpy(out, row, sizeof(double) * (nout < 80 ? nout : 80));
     return 0;
 }
+
+#include "ugks_oracle_s2.c"

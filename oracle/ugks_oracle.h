@@ -34,6 +34,7 @@ typedef struct {
     int mass_rescale;         /* ClosedCouetteMassRescale */
     int macro_sweeps;         /* Implicit_MacroSweeps */
     double residual_tol, moment_tol, min_alpha;
+    int high_order;           /* 1: HighOrderImplicit (S2 evolution, S2 physical collision, HO micro RHS) */
 } uo_params;
 
 typedef struct uo_ctx uo_ctx;
@@ -85,6 +86,13 @@ int uo_solve_dense4(const double m[16], const double rhs[4], double sol[4]);
  * block-Jacobi seams.  out[] receives the diagnostics listed in ugks_oracle.c. */
 int uo_implicit_step(uo_ctx* c, double* out, int nout);
 int uo_implicit_init(uo_ctx* c);   /* persistent M0 of the cold start (InitializeClosedMass) */
+
+/* High-order S2 path (ugks_oracle_s2.c): the S2 Evolution of HighOrderImplicit (targets, WENO-AO
+ * reconstruction, Gauss-node UGKS fluxes, multiscale wall) publishing into the face arrays; the S2
+ * residual/rates/physical collision; the S2 cold start (h, b := discrete closure Maxwellian of W). */
+int uo_s2_evolution(uo_ctx* c, double dt);
+int uo_s2_compute_residual(uo_ctx* c, double dt, int rates_only);
+int uo_s2_init_state(uo_ctx* c);
 
 /* Worker threads used over faces and cells (0 = all host cores); returns the count in use.
  * Results do not depend on the thread count: faces and cells are independent and every sum over

@@ -94,3 +94,25 @@ def test_implicit_two_steps_match_sparse_residual(velocity, golden):
             else:
                 assert abs(row[i] - r) <= 1e-14, (step, k, row[i], r)
         assert row[53] == 1.0 and row[54] == 1.0   # full micro and macro steps (CheckR5Policy)
+
+
+def test_high_order_implicit_two_steps_match_sparse_residual(velocity, golden):
+    """docs/release_checks/high_implicit/sparse_residual.csv: accepted states 1 and 2 of the
+    HighOrderImplicit cold start (S2 tensor WENO-AO reconstruction, discrete-conservative Newton
+    closure, Gauss-node UGKS faces, multiscale diffuse wall, S2 physical collision, PR(2) + LU-SGS
+    with the high-order collision correction, closed-mass rescale).  Same bound as the
+    second-order rows: 1e-10 relative above 1e-10, 1e-14 absolute below."""
+    from oracle.oracle import set_threads
+    set_threads(None)
+    o = Oracle(reference_case("HighOrderImplicit"), *velocity)
+    o.init_freestream()
+    o.implicit_init()
+    for step, ref in enumerate(golden["high_implicit_sparse"]):
+        row = o.implicit_step()
+        for i, k in enumerate(SPARSE_KEYS):
+            r = ref[k]
+            if abs(r) > 1e-10:
+                assert abs(row[i] - r) <= 1e-10 * abs(r), (step, k, row[i], r)
+            else:
+                assert abs(row[i] - r) <= 1e-14, (step, k, row[i], r)
+        assert row[53] == 1.0 and row[54] == 1.0
