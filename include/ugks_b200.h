@@ -37,6 +37,7 @@ extern "C" {
 
 #define UGKS_METHOD_EXPLICIT 0
 #define UGKS_METHOD_IMPLICIT_STEADY 1
+#define UGKS_METHOD_HIGH_ORDER_IMPLICIT 2   /* S2 evolution + the implicit PR(2)/LU-SGS update */
 
 /* Subset of the reference's &config_para / &boundary_para that the hot path reads
  * (src/mod_ImportPara.f90:141-173, set_const_para :911-930). */
@@ -117,7 +118,10 @@ int ugks_step_explicit_noalloc(const ugks_params* params, const double* u, const
                                double* h, double* b, double* W, int nsteps, void* stream, double* dt_out,
                                double* res_out);
 
-/* ImplicitSteady with the closed-Couette mass rescale (method UGKS_METHOD_IMPLICIT_STEADY).
+/* ImplicitSteady / HighOrderImplicit with the closed-Couette mass rescale (methods
+ * UGKS_METHOD_IMPLICIT_STEADY, UGKS_METHOD_HIGH_ORDER_IMPLICIT; the latter evaluates the S2
+ * high-order residual, src/mod_S2NativeAdapter.f90:469-759, and adds the high-order collision
+ * correction to the micro right-hand side, src/mod_ImplicitMicro.f90:66-79,467-470).
  * ugks_implicit_init: InitializeClosedMass (src/mod_ClosedCouetteMass.f90:212-241) -- the persistent
  * M0 from the current state and a fresh residual-reference epoch; call after the state is set.
  * ugks_implicit_steps: up to max_steps pseudo-steps of Solve_UGKS (src/mod_Solve.f90:84-293), each

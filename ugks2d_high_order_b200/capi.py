@@ -18,6 +18,7 @@ UGKS_ENOMEM = 5
 UGKS_EUNSUPPORTED = 6
 UGKS_METHOD_EXPLICIT = 0
 UGKS_METHOD_IMPLICIT_STEADY = 1
+UGKS_METHOD_HIGH_ORDER_IMPLICIT = 2
 
 # every symbol include/ugks_b200.h declares (checked by the CPU test suite)
 EXPORTS = [

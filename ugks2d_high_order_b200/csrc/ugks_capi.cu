@@ -124,7 +124,9 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     if (p->nx < 1 || p->ny < 3 || p->nvel < 1 || p->nvel > kMaxVel || !(p->dx > 0) || !(p->dy > 0) ||
         p->ck < 1)
         return UGKS_EINVAL;
-    if (p->method != UGKS_METHOD_EXPLICIT && p->method != UGKS_METHOD_IMPLICIT_STEADY) return UGKS_EUNSUPPORTED;
+    if (p->method != UGKS_METHOD_EXPLICIT && p->method != UGKS_METHOD_IMPLICIT_STEADY &&
+        p->method != UGKS_METHOD_HIGH_ORDER_IMPLICIT)
+        return UGKS_EUNSUPPORTED;
     UGKS_CK(cudaSetDevice(device));
     ugks_ctx* c = new (std::nothrow) ugks_ctx();
     if (!c) return UGKS_ENOMEM;
@@ -187,12 +189,13 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     if (e == cudaSuccess) e = cudaMemcpyAsync(d + o_v, v, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d + o_w, w, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
-    if (e == cudaSuccess && p->method == UGKS_METHOD_IMPLICIT_STEADY) {
+    if (e == cudaSuccess && p->method != UGKS_METHOD_EXPLICIT) {
         // ImplicitSteady work arrays (mod_ImplicitState.f90:110-132)
         ImParams& Q = c->Q;
         Q.nslab = p->nslab > 0 ? p->nslab : 1;
         Q.mass_rescale = p->mass_rescale;
         Q.macro_sweeps = p->macro_sweeps > 0 ? p->macro_sweeps : 2;
+        Q.high_order = p->method == UGKS_METHOD_HIGH_ORDER_IMPLICIT ? 1 : 0;
         Q.ncfl = p->ncfl; Q.residual_tol = p->residual_tol; Q.moment_tol = p->moment_tol; Q.min_alpha = p->min_alpha;
         Q.wall_ux[0] = p->wall_ux[0]; Q.wall_ux[1] = p->wall_ux[1];
         if (ny % Q.nslab != 0 || (ny / Q.nslab) * nx > kMaxSlabCells) { ugks_ctx_destroy(c); return UGKS_EINVAL; }
@@ -205,6 +208,11 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
         const size_t i_eh = itake(S), i_eb = itake(S), i_fh = itake(S), i_fb = itake(S), i_bh = itake(S), i_bb = itake(S);
         const size_t i_hu = itake((size_t)2 * nv), i_bu = itake((size_t)2 * nv), i_dr = itake((size_t)2 * nx);
         const size_t i_cell = itake((size_t)nc * kImCell), i_st = itake(IS_COUNT), i_rep = itake(kReport);
+        // high order: reconstruction cache [nc][72][nv] and the six volume targets
+        const size_t i_rec = Q.high_order ? itake((size_t)nc * 72 * nv) : 0;
+        size_t i_tg[6] = {0, 0, 0, 0, 0, 0};
+        if (Q.high_order) for (int t = 0; t < 6; ++t) i_tg[t] = itake(S);
+        if (e == cudaSuccess && Q.high_order) e = prepare_s2();
         if (e == cudaSuccess) e = cudaMalloc(&c->imem, io * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&c->iflags, 4 * sizeof(unsigned));
         if (e == cudaSuccess) e = cudaMemsetAsync(c->imem, 0, io * sizeof(double), c->stream);
@@ -217,6 +225,11 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
             I.rhs_h = m + i_eh; I.rhs_b = m + i_eb; I.dFh = m + i_fh; I.dFb = m + i_fb; I.dBh = m + i_bh; I.dBb = m + i_bb;
             I.wall_hu = m + i_hu; I.wall_bu = m + i_bu; I.wall_drho = m + i_dr; I.cell = m + i_cell;
             I.state = m + i_st; I.report = m + i_rep;
+            if (Q.high_order) {
+                I.s2.rec = m + i_rec;
+                I.s2.mh = m + i_tg[0]; I.s2.mb = m + i_tg[1]; I.s2.kxh = m + i_tg[2];
+                I.s2.kxb = m + i_tg[3]; I.s2.kyh = m + i_tg[4]; I.s2.kyb = m + i_tg[5];
+            }
             I.mask = c->iflags; I.counter = c->iflags + 2;
         }
     }
@@ -292,6 +305,10 @@ extern "C" int ugks_init_freestream(ugks_ctx* c, double rho, double U, double V,
     if (int r = invalidate_eval(c)) return r;
     UGKS_CK(launch_lo_init(c->P, c->B, rho, U, V, tnative, c->stream));
     c->launches += 1;
+    if (c->imem && c->Q.high_order) {   // S2NativeInitializeState cold start: h, b := closure Maxwellian of W
+        UGKS_CK(s2_enqueue(0, c->P, c->B, c->I.s2, c->stream, c->stream2, c->ev_fork, c->ev_join));
+        c->launches += 1;
+    }
     int r = kernel_timestep(c);
     if (r) return r;
     return collect_status(c);

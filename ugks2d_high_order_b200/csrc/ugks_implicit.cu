@@ -141,6 +141,117 @@ __device__ __forceinline__ void wall_frame(const LoParams& P, int top, double uk
 // ComputeResidual's steady-rate assembly (mod_Residual.f90:81-132) + UpdateImplicitResidualDiagnostics
 // per cell.  POST = the accepted-state evaluation (PhysicalDiagnostic, mod_R5Observe.f90:40-141):
 // its last CTA writes the report row and advances the five-state streak.
+// Last-CTA part of the residual kernels: global sums (MPI_Allreduce SUM/MAX) of the per-cell
+// terms, the science / flux columns, the five-state streak and the report row.
+template <bool POST>
+__device__ void im_residual_epilogue(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
+                                     double* red, double* rout) {
+    const int tid = threadIdx.x, nx = P.nx;
+    const double dt = B.dt[0];
+    __shared__ unsigned s_last;
+    __threadfence();
+    __syncthreads();
+    if (tid == 0) s_last = (atomicAdd(I.counter, 1u) == (unsigned)(gridDim.x - 1)) ? 1u : 0u;
+    __syncthreads();
+    if (!s_last) return;
+    __threadfence();
+    const int nc = P.nx * P.ny;
+    // g[0..18]: sums of the per-cell terms; g[19..30]: boundary-face macro fluxes per unit time
+    // (x wrap face, bottom wall, top wall; PhysicalDiagnostic flux, mod_R5Observe.f90:107-113);
+    // g[31]: max moment error
+    double g[32];
+#pragma unroll
+    for (int m = 0; m < 32; ++m) g[m] = 0.0;
+    for (int cc = tid; cc < nc; cc += blockDim.x) {
+#pragma unroll
+        for (int m = 0; m < 19; ++m) g[m] += __ldcg(I.cell + (size_t)cc * kImCell + m);
+        g[31] = fmax(g[31], __ldcg(I.cell + (size_t)cc * kImCell + 19));
+    }
+    if (POST) {
+        for (int jj = tid; jj < P.ny; jj += blockDim.x)
+#pragma unroll
+            for (int m = 0; m < 4; ++m) g[19 + m] += __ldcg(B.fxw + ((size_t)jj * nx + 0) * 4 + m) / dt;
+        for (int ii = tid; ii < nx; ii += blockDim.x)
+#pragma unroll
+            for (int m = 0; m < 4; ++m) {
+                g[23 + m] += __ldcg(B.fyw + (size_t)ii * 4 + m) / dt;
+                g[27 + m] += __ldcg(B.fyw + ((size_t)P.ny * nx + ii) * 4 + m) / dt;
+            }
+    }
+    block_reduce<31, 1>(g, red, rout);
+    if (tid != 0) return;
+    const double SMV = kSMV;
+    double sci[22];
+    const double ncell = (double)nc;
+    double ords = fmax(fmax(g[4], g[7]), SMV);
+    for (int m = 0; m < 4; ++m) {
+        const double rel = sqrt(ncell * g[m]) / (g[4 + m] + SMV);
+        const double ab = sqrt(g[m] / fmax(g[8], SMV));
+        sci[4 + m] = rel;
+        sci[8 + m] = ab;
+        sci[m] = (g[4 + m] <= sqrt(kEps) * fmax(ords, DBL_MIN)) ? ab : rel;
+    }
+    const double raw_h = sqrt(g[9]), raw_b = sqrt(g[10]);
+    const double h_raw = sqrt(g[9] / fmax(g[11], SMV)), b_raw = sqrt(g[10] / fmax(g[12], SMV));
+    if (I.state[IS_REF_INIT] == 0.0) {
+        I.state[IS_REF_H] = h_raw;
+        I.state[IS_REF_B] = b_raw;
+        I.state[IS_REF_INIT] = 1.0;
+    }
+    const double rh = I.state[IS_REF_H], rb = I.state[IS_REF_B];
+    const double nzr = fmax(100.0 * Q.residual_tol, 1000.0 * kEps);
+    sci[12] = rh <= nzr ? h_raw : h_raw / rh;
+    sci[13] = rb <= nzr ? b_raw : b_raw / rb;
+    sci[14] = rh > DBL_MIN ? h_raw / rh : h_raw;
+    sci[15] = rb > DBL_MIN ? b_raw / rb : b_raw;
+    sci[16] = h_raw;
+    sci[17] = b_raw;
+    sci[18] = I.state[IS_MOMENT];
+    sci[19] = fabs(g[13]);
+    sci[20] = raw_h;
+    sci[21] = raw_b;
+    double* rep = I.report;
+    if (!POST) {
+        for (int m = 0; m < 22; ++m) rep[57 + m] = sci[m];
+        *I.counter = 0u;
+        return;
+    }
+    const double moment = g[31];
+    for (int m = 0; m < 22; ++m) I.state[IS_PRESCI + m] = sci[m];
+    I.state[IS_EVAL_DT] = dt;
+    I.state[IS_EVAL_VALID] = 1.0;
+    if (Q.mass_rescale) sci[18] = moment;   // implicit_moment_error = MassStatistics after the rescale
+    // boundary-face totals per unit time: outflow through the left x face, inflow through the right
+    // (the same periodic face), the bottom wall taken into the domain, the top wall out of it
+    double flux[16];
+    for (int m = 0; m < 4; ++m) {
+        flux[m] = -g[19 + m];
+        flux[4 + m] = g[19 + m];
+        flux[8 + m] = -g[23 + m];
+        flux[12 + m] = g[27 + m];
+    }
+    const double tol = Q.residual_tol;
+    const bool pass = sci[0] <= tol && sci[1] <= tol && sci[2] <= tol && sci[3] <= tol && sci[12] <= tol &&
+                      sci[13] <= tol && moment <= Q.moment_tol;
+    const double streak = pass ? I.state[IS_STREAK] + 1.0 : 0.0;
+    I.state[IS_STREAK] = streak;
+    I.state[IS_STEPS] = I.state[IS_STEPS] + 1.0;
+    const bool done = Q.mass_rescale ? streak >= 5.0 : pass;
+    if (done) { I.state[IS_CONVERGED] = 1.0; I.state[IS_STOP] = 1.0; }
+    rep[0] = pass ? 1.0 : 0.0;
+    rep[1] = moment;
+    rep[2] = g[14];
+    rep[3] = g[18];
+    for (int m = 0; m < 4; ++m) rep[4 + m] = sci[8 + m];
+    rep[8] = raw_h; rep[9] = raw_b; rep[10] = h_raw; rep[11] = b_raw;
+    for (int m = 0; m < 22; ++m) rep[12 + m] = sci[m];
+    for (int m = 0; m < 16; ++m) rep[34 + m] = flux[m];
+    rep[50] = rh; rep[51] = rb;
+    rep[52] = Q.mass_rescale ? I.state[IS_MASS_SCALE] - 1.0 : 0.0;
+    rep[53] = I.state[IS_ALPHA]; rep[54] = I.state[IS_MALPHA]; rep[55] = dt; rep[56] = streak;
+    *I.counter = 0u;
+}
+
 template <int VPT, int NTMAX, bool POST>
 __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_residual(LoParams P, LoBuffers B, ImParams Q, ImBuffers I) {
     if (I.state[IS_STOP] != 0.0) return;
@@ -337,109 +448,123 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_residual(LoParams P, 
         t[19] = merr;
     }
 
-    // ---- last CTA: global sums (MPI_Allreduce SUM/MAX) and the diagnostics derived from them
-    __shared__ unsigned s_last;
-    __threadfence();
-    __syncthreads();
-    if (tid == 0) s_last = (atomicAdd(I.counter, 1u) == (unsigned)(gridDim.x - 1)) ? 1u : 0u;
-    __syncthreads();
-    if (!s_last) return;
-    __threadfence();
-    const int nc = P.nx * P.ny;
-    // g[0..18]: sums of the per-cell terms; g[19..30]: boundary-face macro fluxes per unit time
-    // (x wrap face, bottom wall, top wall; PhysicalDiagnostic flux, mod_R5Observe.f90:107-113);
-    // g[31]: max moment error
-    double g[32];
-#pragma unroll
-    for (int m = 0; m < 32; ++m) g[m] = 0.0;
-    for (int cc = tid; cc < nc; cc += blockDim.x) {
-#pragma unroll
-        for (int m = 0; m < 19; ++m) g[m] += __ldcg(I.cell + (size_t)cc * kImCell + m);
-        g[31] = fmax(g[31], __ldcg(I.cell + (size_t)cc * kImCell + 19));
-    }
-    if (POST) {
-        for (int jj = tid; jj < P.ny; jj += blockDim.x)
-#pragma unroll
-            for (int m = 0; m < 4; ++m) g[19 + m] += __ldcg(B.fxw + ((size_t)jj * nx + 0) * 4 + m) / dt;
-        for (int ii = tid; ii < nx; ii += blockDim.x)
-#pragma unroll
-            for (int m = 0; m < 4; ++m) {
-                g[23 + m] += __ldcg(B.fyw + (size_t)ii * 4 + m) / dt;
-                g[27 + m] += __ldcg(B.fyw + ((size_t)P.ny * nx + ii) * 4 + m) / dt;
-            }
-    }
-    block_reduce<31, 1>(g, red, rout);
-    if (tid != 0) return;
-    const double SMV = kSMV;
-    double sci[22];
-    const double ncell = (double)nc;
-    double ords = fmax(fmax(g[4], g[7]), SMV);
-    for (int m = 0; m < 4; ++m) {
-        const double rel = sqrt(ncell * g[m]) / (g[4 + m] + SMV);
-        const double ab = sqrt(g[m] / fmax(g[8], SMV));
-        sci[4 + m] = rel;
-        sci[8 + m] = ab;
-        sci[m] = (g[4 + m] <= sqrt(kEps) * fmax(ords, DBL_MIN)) ? ab : rel;
-    }
-    const double raw_h = sqrt(g[9]), raw_b = sqrt(g[10]);
-    const double h_raw = sqrt(g[9] / fmax(g[11], SMV)), b_raw = sqrt(g[10] / fmax(g[12], SMV));
-    if (I.state[IS_REF_INIT] == 0.0) {
-        I.state[IS_REF_H] = h_raw;
-        I.state[IS_REF_B] = b_raw;
-        I.state[IS_REF_INIT] = 1.0;
-    }
-    const double rh = I.state[IS_REF_H], rb = I.state[IS_REF_B];
-    const double nzr = fmax(100.0 * Q.residual_tol, 1000.0 * kEps);
-    sci[12] = rh <= nzr ? h_raw : h_raw / rh;
-    sci[13] = rb <= nzr ? b_raw : b_raw / rb;
-    sci[14] = rh > DBL_MIN ? h_raw / rh : h_raw;
-    sci[15] = rb > DBL_MIN ? b_raw / rb : b_raw;
-    sci[16] = h_raw;
-    sci[17] = b_raw;
-    sci[18] = I.state[IS_MOMENT];
-    sci[19] = fabs(g[13]);
-    sci[20] = raw_h;
-    sci[21] = raw_b;
-    double* rep = I.report;
-    if (!POST) {
-        for (int m = 0; m < 22; ++m) rep[57 + m] = sci[m];
-        *I.counter = 0u;
+    im_residual_epilogue<POST>(P, B, Q, I, red, rout);
+}
+
+// ComputeResidual + AssembleSteadyRateResiduals for HighOrderImplicit (mod_Residual.f90:81-108,
+// IsS2CN2 branch) and S2NativePhysicalCollision (mod_S2NativeAdapter.f90:735-759): the steady rates
+// without the streaming projection (the stream moments must equal rate_w to 2e-12), the physical
+// collision C = (M + K_x q + K_y q - h) / tau with q = heat(h - M), tau = s2_tau(W), and the same
+// per-cell diagnostic terms as the second-order evaluation.
+template <int VPT, int NTMAX, bool POST>
+__global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_residual_s2(LoParams P, LoBuffers B, ImParams Q,
+                                                                       ImBuffers I) {
+    if (I.state[IS_STOP] != 0.0) return;
+    if (!POST && eval_cached(B)) {
+        if (blockIdx.x == 0 && threadIdx.x < 22) I.report[57 + threadIdx.x] = I.state[IS_PRESCI + threadIdx.x];
         return;
     }
-    const double moment = g[31];
-    for (int m = 0; m < 22; ++m) I.state[IS_PRESCI + m] = sci[m];
-    I.state[IS_EVAL_DT] = dt;
-    I.state[IS_EVAL_VALID] = 1.0;
-    if (Q.mass_rescale) sci[18] = moment;   // implicit_moment_error = MassStatistics after the rescale
-    // boundary-face totals per unit time: outflow through the left x face, inflow through the right
-    // (the same periodic face), the bottom wall taken into the domain, the top wall out of it
-    double flux[16];
-    for (int m = 0; m < 4; ++m) {
-        flux[m] = -g[19 + m];
-        flux[4 + m] = g[19 + m];
-        flux[8 + m] = -g[23 + m];
-        flux[12 + m] = g[27 + m];
+    __shared__ double red[16 * 64];
+    __shared__ double rout[kRedSlots];
+    __shared__ double sc[16];   // [0..3] res_w, [4] ux, [5] vy, [6] tau, [7] ok
+    const int nv = P.nvel, tid = threadIdx.x, nx = P.nx;
+    const int c = blockIdx.x, i = c % nx, j = c / nx;
+    const double dt = B.dt[0], dti = 1.0 / dt;
+    const size_t fl = (size_t)(j * nx + i), fr = (size_t)(j * nx + wrapx(i + 1, nx));
+    const size_t gl = (size_t)(j * nx + i), gr = (size_t)((j + 1) * nx + i);
+    const double* Wo = B.W + c * 4;
+    if (tid == 0) {
+#pragma unroll
+        for (int m = 0; m < 4; ++m)
+            sc[m] = (B.fxw[fl * 4 + m] - B.fxw[fr * 4 + m] + B.fyw[gl * 4 + m] - B.fyw[gr * 4 + m]) / P.area;
+        double tau = 1.0;
+        const bool ok = Wo[0] > 0.0 && s2_tau(P, Wo, tau);
+        sc[4] = Wo[1] / Wo[0]; sc[5] = Wo[2] / Wo[0]; sc[6] = ok ? tau : 1.0; sc[7] = ok ? 1.0 : 0.0;
     }
-    const double tol = Q.residual_tol;
-    const bool pass = sci[0] <= tol && sci[1] <= tol && sci[2] <= tol && sci[3] <= tol && sci[12] <= tol &&
-                      sci[13] <= tol && moment <= Q.moment_tol;
-    const double streak = pass ? I.state[IS_STREAK] + 1.0 : 0.0;
-    I.state[IS_STREAK] = streak;
-    I.state[IS_STEPS] = I.state[IS_STEPS] + 1.0;
-    const bool done = Q.mass_rescale ? streak >= 5.0 : pass;
-    if (done) { I.state[IS_CONVERGED] = 1.0; I.state[IS_STOP] = 1.0; }
-    rep[0] = pass ? 1.0 : 0.0;
-    rep[1] = moment;
-    rep[2] = g[14];
-    rep[3] = g[18];
-    for (int m = 0; m < 4; ++m) rep[4 + m] = sci[8 + m];
-    rep[8] = raw_h; rep[9] = raw_b; rep[10] = h_raw; rep[11] = b_raw;
-    for (int m = 0; m < 22; ++m) rep[12 + m] = sci[m];
-    for (int m = 0; m < 16; ++m) rep[34 + m] = flux[m];
-    rep[50] = rh; rep[51] = rb;
-    rep[52] = Q.mass_rescale ? I.state[IS_MASS_SCALE] - 1.0 : 0.0;
-    rep[53] = I.state[IS_ALPHA]; rep[54] = I.state[IS_MALPHA]; rep[55] = dt; rep[56] = streak;
-    *I.counter = 0u;
+    __syncthreads();
+    const double ux = sc[4], vy = sc[5], tau = sc[6];
+    const double area_inv = 1.0 / P.area;
+    double h[VPT], b[VPT], sh[VPT], sb[VPT], acc[12];
+#pragma unroll
+    for (int m = 0; m < 6; ++m) acc[m] = 0.0;
+#pragma unroll
+    for (int r = 0; r < VPT; ++r) {
+        const Slot s = slot(r, nv);
+        const int k = s.kk;
+        const size_t q = (size_t)c * nv + k;
+        const double wk = s.ok ? B.w[k] : 0.0, uk = B.u[k], vk = B.v[k];
+        h[r] = B.h[q];
+        b[r] = B.b[q];
+        sh[r] = (B.fxh[fl * nv + k] - B.fxh[fr * nv + k] + B.fyh[gl * nv + k] - B.fyh[gr * nv + k]) * area_inv * dti;
+        sb[r] = (B.fxb[fl * nv + k] - B.fxb[fr * nv + k] + B.fyb[gl * nv + k] - B.fyb[gr * nv + k]) * area_inv * dti;
+        moment_add(wk, uk, vk, sh[r], sb[r], acc);
+        const double cx = uk - ux, cy = vk - vy, c2 = cx * cx + cy * cy;
+        const double dh = h[r] - I.s2.mh[q], db = b[r] - I.s2.mb[q];
+        acc[4] += 0.5 * wk * cx * (c2 * dh + db);
+        acc[5] += 0.5 * wk * cy * (c2 * dh + db);
+    }
+    block_reduce<6, 0>(acc, red, rout);
+    if (tid == 0) {
+        double rs = 1.0, err = 0.0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { rs = fmax(rs, fabs(sc[m] * dti)); err = fmax(err, fabs(acc[m] - sc[m] * dti)); }
+        if (!(err / rs <= 2.0e-12)) stop_with(I, B.status, ST_PROJECTION);
+        if (sc[7] == 0.0) stop_with(I, B.status, ST_GETPRIMARY);
+    }
+    const double q0 = acc[4], q1 = acc[5];
+#pragma unroll
+    for (int m = 0; m < 12; ++m) acc[m] = 0.0;
+#pragma unroll
+    for (int r = 0; r < VPT; ++r) {
+        const Slot s = slot(r, nv);
+        const size_t q = (size_t)c * nv + s.kk;
+        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
+        const double Ep = I.s2.mh[q] + I.s2.kxh[q] * q0 + I.s2.kyh[q] * q1;
+        const double Fp = I.s2.mb[q] + I.s2.kxb[q] * q0 + I.s2.kyb[q] * q1;
+        const double ch = (Ep - h[r]) / tau, cb = (Fp - b[r]) / tau;
+        moment_add(wk, uk, vk, ch, cb, acc);
+        const double dh = sh[r] + ch, db = sb[r] + cb;
+        acc[4] += wk * dh * dh;
+        acc[5] += wk * db * db;
+        acc[6] += wk * fmax(h[r] * h[r], Ep * Ep);
+        acc[7] += wk * fmax(b[r] * b[r], Fp * Fp);
+        moment_add(wk, uk, vk, h[r], b[r], acc + 8);
+        if (s.ok) {
+            I.stream_h[(size_t)c * nv + s.k] = sh[r];
+            I.stream_b[(size_t)c * nv + s.k] = sb[r];
+            B.pcol_h[(size_t)c * nv + s.k] = ch;
+            B.pcol_b[(size_t)c * nv + s.k] = cb;
+        }
+    }
+    block_reduce_smem<12, 0>(acc, red, rout);
+    if (tid == 0) {
+        double ws = 1.0, mx = 0.0, merr = 0.0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { ws = fmax(ws, fabs(Wo[m])); mx = fmax(mx, fabs(rout[m])); }
+        if (tau * mx / ws > 2.0e-12) stop_with(I, B.status, ST_PROJECTION);   // S2 collision moment gate
+#pragma unroll
+        for (int m = 0; m < 4; ++m) merr = fmax(merr, fabs(Wo[m] - rout[8 + m]) / fmax(fabs(Wo[m]), 1.0));
+        double rate[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { rate[m] = sc[m] * dti; I.rate_w[c * 4 + m] = rate[m]; }
+        double* t = I.cell + (size_t)c * kImCell;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            const double a = P.area * rate[m];
+            t[m] = a * a;
+            t[4 + m] = P.area * fabs(Wo[m] + dt * rate[m]);
+            t[14 + m] = P.area * Wo[m];
+        }
+        t[8] = P.area * P.area;
+        t[9] = P.area * rout[4];
+        t[10] = P.area * rout[5];
+        t[11] = P.area * rout[6];
+        t[12] = P.area * rout[7];
+        t[13] = rate[0] * P.area;
+        t[18] = P.area * rout[8];
+        t[19] = merr;
+    }
+    im_residual_epilogue<POST>(P, B, Q, I, red, rout);
 }
 
 // -------------------------------------------------------------------------------------------
@@ -694,7 +819,8 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_equilibrium(LoParams 
     if (I.state[IS_STOP] != 0.0) return;
     __shared__ double red[16 * 64];
     __shared__ double rout[kRedSlots];
-    __shared__ double sc[24];   // [0..3] prim_old [4..7] prim_tilde [8] tau_tilde [9] ok [12..15] lambda
+    __shared__ double sc[32];   // [0..3] prim_old [4..7] prim_tilde [8] tau_tilde [9] ok [12..15] lambda
+                                // [16..19] old-state lambda, [20] tau_old (high order)
     const int nv = P.nvel, tid = threadIdx.x, c = blockIdx.x;
     if (tid == 0) {
         const int m = first_bit(I.mask[0]);
@@ -706,7 +832,10 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_equilibrium(LoParams 
         double tt = 1.0;
         bool ok = m >= 0 && get_primary(P.gm1, B.W + c * 4, po) && get_primary(P.gm1, wt, pt);
         ok = ok && get_tau(P.mu_ref, P.omega, pt, tt);
-        if (!ok) { po.r = pt.r = 1.0; po.U = po.V = pt.U = pt.V = 0.0; po.L = pt.L = 1.0; tt = 1.0; }
+        double to = 1.0;
+        if (Q.high_order) ok = ok && get_tau(P.mu_ref, P.omega, po, to);
+        sc[20] = to;
+        if (!ok) { po.r = pt.r = 1.0; po.U = po.V = pt.U = pt.V = 0.0; po.L = pt.L = 1.0; tt = 1.0; sc[20] = 1.0; }
         sc[0] = po.r; sc[1] = po.U; sc[2] = po.V; sc[3] = po.L;
         sc[4] = pt.r; sc[5] = pt.U; sc[6] = pt.V; sc[7] = pt.L; sc[8] = tt; sc[9] = ok ? 1.0 : 0.0;
         I.tau_t[c] = tt;
@@ -768,10 +897,56 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_equilibrium(LoParams 
         for (int m = 0; m < 4; ++m) sc[12 + m] = ok ? l[m] : 0.0;
         if (!ok) stop_with(I, B.status, ST_PROJECTION);
     }
+    // High order: the old-state Maxwell + Shakhov with q_frozen, projected onto W_old
+    // (low_collision_old, mod_ImplicitMicro.f90:66-79)
+    double Eo[VPT], Fo[VPT], seo = 1.0, sfo = 1.0;
+    if (Q.high_order) {
+        const double pref = po.r * (po.L / kPi), bfac = (double)P.ck / (2.0 * po.L);
+        const double coeff = 0.8 * (1.0 - P.pr) * po.L * po.L / po.r, c2ck = 2.0 / (double)P.ck;
+        double am[2] = {0.0, 0.0};
+#pragma unroll
+        for (int r = 0; r < VPT; ++r) {
+            const Slot s = slot(r, nv);
+            const double dvn = B.u[s.kk] - po.U, dvt = B.v[s.kk] - po.V, v2 = dvn * dvn + dvt * dvt;
+            const double H = pref * exp(-po.L * v2), Bm = H * bfac;
+            const double qd = dvn * q0 + dvt * q1, sH = 2.0 * po.L * v2 - 4.0;
+            Eo[r] = H + coeff * qd * sH * H;
+            Fo[r] = Bm + coeff * qd * (sH + c2ck) * Bm;
+            am[0] = fmax(am[0], s.ok ? fabs(Eo[r]) : 0.0);
+            am[1] = fmax(am[1], s.ok ? fabs(Fo[r]) : 0.0);
+        }
+        block_reduce<0, 2>(am, red, rout);
+        seo = fmax(am[0], 1.0); sfo = fmax(am[1], 1.0);
+        double ag[14];
+#pragma unroll
+        for (int m = 0; m < 14; ++m) ag[m] = 0.0;
+#pragma unroll
+        for (int r = 0; r < VPT; ++r) {
+            const Slot s = slot(r, nv);
+            const double wk = s.ok ? B.w[s.kk] : 0.0;
+            moment_add(wk, B.u[s.kk], B.v[s.kk], Eo[r], Fo[r], ag);
+            gram_add(wk, fmax(fabs(Eo[r]), kEps * seo), fmax(fabs(Fo[r]), kEps * sfo), B.u[s.kk], B.v[s.kk], ag + 4);
+        }
+        block_reduce_smem<14, 0>(ag, red, rout);
+        if (tid == 0) {
+            double rhs[4], gm[16], l[4];
+#pragma unroll
+            for (int m = 0; m < 4; ++m) rhs[m] = B.W[c * 4 + m] - rout[m];
+            gram_expand(rout + 4, gm);
+            const bool ok = solve_dense4(gm, rhs, l);
+#pragma unroll
+            for (int m = 0; m < 4; ++m) sc[16 + m] = ok ? l[m] : 0.0;
+            if (!ok) stop_with(I, B.status, ST_PROJECTION);
+        }
+    }
     __syncthreads();
     double lam[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) lam[m] = sc[12 + m];
+    double lamo[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) lamo[m] = sc[16 + m];
+    const double tau_old = sc[20];
 #pragma unroll
     for (int m = 0; m < 4; ++m) acc[m] = 0.0;
 #pragma unroll
@@ -781,10 +956,19 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_equilibrium(LoParams 
         const double Ep = E[r] + fmax(fabs(E[r]), kEps * se) * (lam[0] + uk * lam[1] + vk * lam[2] + e * lam[3]);
         const double Fp = F[r] + 0.5 * fmax(fabs(F[r]), kEps * sf) * lam[3];
         moment_add(wk, uk, vk, Ep, Fp, acc);
-        if (s.ok) {   // RelaxMicroPoint's velocity-local right-hand side (mod_ImplicitMicro.f90:458-460)
+        if (s.ok) {   // RelaxMicroPoint's velocity-local right-hand side (mod_ImplicitMicro.f90:458-470)
             const size_t q = (size_t)c * nv + s.k;
-            I.rhs_h[q] = I.stream_h[q] + (Ep - B.h[q]) / sc[8];
-            I.rhs_b[q] = I.stream_b[q] + (Fp - B.b[q]) / sc[8];
+            double rh = I.stream_h[q] + (Ep - B.h[q]) / sc[8];
+            double rb = I.stream_b[q] + (Fp - B.b[q]) / sc[8];
+            if (Q.high_order) {
+                const double Eop = Eo[r] + fmax(fabs(Eo[r]), kEps * seo) * (lamo[0] + uk * lamo[1] + vk * lamo[2] + e * lamo[3]);
+                const double Fop = Fo[r] + 0.5 * fmax(fabs(Fo[r]), kEps * sfo) * lamo[3];
+                const double lh = (Eop - B.h[q]) / tau_old, lb = (Fop - B.b[q]) / tau_old;
+                rh = rh + B.pcol_h[q] - lh;
+                rb = rb + B.pcol_b[q] - lb;
+            }
+            I.rhs_h[q] = rh;
+            I.rhs_b[q] = rb;
         }
     }
     block_reduce_smem<4, 0>(acc, red, rout);
@@ -1113,8 +1297,14 @@ static void im_cell_kernels(int which, const LoParams& P, const LoBuffers& B, co
                             const double* D, cudaStream_t s) {
     const int nc = P.nx * P.ny, nt = lo_threads(P.nvel);
     switch (which) {
-        case 0: k_im_residual<VPT, NTMAX, false><<<nc, nt, 0, s>>>(P, B, Q, I); break;
-        case 1: k_im_residual<VPT, NTMAX, true><<<nc, nt, 0, s>>>(P, B, Q, I); break;
+        case 0:
+            if (Q.high_order) k_im_residual_s2<VPT, NTMAX, false><<<nc, nt, 0, s>>>(P, B, Q, I);
+            else k_im_residual<VPT, NTMAX, false><<<nc, nt, 0, s>>>(P, B, Q, I);
+            break;
+        case 1:
+            if (Q.high_order) k_im_residual_s2<VPT, NTMAX, true><<<nc, nt, 0, s>>>(P, B, Q, I);
+            else k_im_residual<VPT, NTMAX, true><<<nc, nt, 0, s>>>(P, B, Q, I);
+            break;
         case 2: k_im_equilibrium<VPT, NTMAX><<<nc, nt, 0, s>>>(P, B, Q, I, D); break;
         case 3: k_im_wall_closure<VPT, NTMAX><<<2 * P.nx, nt, 0, s>>>(P, B, Q, I); break;
         case 4: k_im_micro_alpha<VPT, NTMAX><<<nc, nt, 0, s>>>(P, B, Q, I); break;
@@ -1176,7 +1366,8 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     Bpre.eval = I.state + IS_EVAL_VALID;
     cudaError_t e = mark(cudaSuccess);
     if (e == cudaSuccess) e = mark(launch_lo_timestep(P, B, s));                 // TimeStep
-    if (e == cudaSuccess) e = im_fluxes(P, Bpre, s, s2, fork, join);             // Interpolation + Evolution
+    if (e == cudaSuccess)                                                         // Interpolation + Evolution
+        e = Q.high_order ? s2_enqueue(1, P, Bpre, I.s2, s, s2, fork, join) : im_fluxes(P, Bpre, s, s2, fork, join);
     if (e == cudaSuccess) e = mark(im_cell(0, P, Bpre, Q, I, nullptr, s));       // ComputeResidual + diagnostics
     if (e == cudaSuccess) { k_im_pr2_prep<<<(nc * 4 + 127) / 128, 128, 0, s>>>(P, B, Q, I); e = mark(cudaGetLastError()); }
     const double* X = I.dwA;
@@ -1201,9 +1392,10 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     if (e == cudaSuccess) e = mark(im_cell(4, P, B, Q, I, nullptr, s));          // FindAdmissibleMicroAlpha
     if (e == cudaSuccess) e = mark(im_cell(5, P, B, Q, I, nullptr, s));          // update + RecoverMacro
     if (e == cudaSuccess) { k_im_rescale<<<148 * 4, 256, 0, s>>>(P, B, Q, I); e = mark(cudaGetLastError()); }
-    if (e == cudaSuccess) e = mark(im_fluxes(P, B, s, s2, fork, join));         // accepted-state evaluation
+    if (e == cudaSuccess)                                                         // accepted-state evaluation
+        e = mark(Q.high_order ? s2_enqueue(1, P, B, I.s2, s, s2, fork, join) : im_fluxes(P, B, s, s2, fork, join));
     if (e == cudaSuccess) e = mark(im_cell(1, P, B, Q, I, nullptr, s));
-    if (launches) *launches += 16 + Q.macro_sweeps;
+    if (launches) *launches += 16 + Q.macro_sweeps + (Q.high_order ? 2 : 0);
     return e;
 }
 

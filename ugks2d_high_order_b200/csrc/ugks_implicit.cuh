@@ -1,6 +1,7 @@
 // ugks_implicit.cuh -- device state of the ImplicitSteady pseudo-step (second order).
 #pragma once
 #include "ugks_lo.cuh"
+#include "ugks_s2.cuh"
 
 namespace ugks {
 
@@ -43,6 +44,7 @@ struct ImParams {
     int nslab;              // ranks of the reference's 1 x NP_Y blocking (rows per slab = ny / nslab)
     int mass_rescale;
     int macro_sweeps;
+    int high_order;         // 1: HighOrderImplicit (S2 evolution, S2 physical collision, HO micro RHS)
     double ncfl, residual_tol, moment_tol, min_alpha;
     double wall_ux[2];
 };
@@ -70,6 +72,7 @@ struct ImBuffers {
     double* cell;           // [nc][kImCell] per-cell terms for the global reductions
     double* state;          // [IS_COUNT]
     double* report;         // [kReport]
+    S2Buffers s2;           // high-order volume targets and reconstruction cache (HighOrderImplicit)
     unsigned* mask;         // [2] admissible macro / micro alpha bitmasks (bit m: alpha = 2^-m)
     unsigned* counter;      // [1] last-CTA counter of the implicit kernels
 };

@@ -38,7 +38,8 @@ class Solver:
         p.wall_ux[0], p.wall_ux[1] = case.wall_ux
         p.wall_tnative[0], p.wall_tnative[1] = case.wall_tnative
         p.fixed_dt = 0.0
-        p.method = capi.UGKS_METHOD_IMPLICIT_STEADY if case.method == "ImplicitSteady" else capi.UGKS_METHOD_EXPLICIT
+        p.method = {"ImplicitSteady": capi.UGKS_METHOD_IMPLICIT_STEADY,
+                    "HighOrderImplicit": capi.UGKS_METHOD_HIGH_ORDER_IMPLICIT}.get(case.method, capi.UGKS_METHOD_EXPLICIT)
         p.ncfl, p.nslab, p.mass_rescale, p.macro_sweeps = case.ncfl, case.nslab, int(case.mass_rescale), case.macro_sweeps
         p.residual_tol, p.moment_tol, p.min_alpha = case.residual_tol, case.moment_tol, case.min_alpha
         self._params = p
