@@ -14,7 +14,7 @@ from .solver import Solver
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--method", default="Explicit", choices=["Explicit", "ImplicitSteady"])
+    ap.add_argument("--method", default="Explicit", choices=["Explicit", "ImplicitSteady", "HighOrderImplicit"])
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--show", type=int, default=100)
     ap.add_argument("--cfl", type=float, default=None)
@@ -37,7 +37,7 @@ def main(argv=None):
     case = case.with_(**kw) if kw else case
     s = Solver(case, *load_velocity_half32())
     s.init_freestream()
-    if a.method == "ImplicitSteady":
+    if a.method != "Explicit":
         s.implicit_init()
     t0 = time.perf_counter()
     done = 0
