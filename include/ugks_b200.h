@@ -38,6 +38,7 @@ extern "C" {
 #define UGKS_METHOD_EXPLICIT 0
 #define UGKS_METHOD_IMPLICIT_STEADY 1
 #define UGKS_METHOD_HIGH_ORDER_IMPLICIT 2   /* S2 evolution + the implicit PR(2)/LU-SGS update */
+#define UGKS_METHOD_S2CN2 3                 /* explicit high-order step: S2 evolution + CN collision */
 
 /* Subset of the reference's &config_para / &boundary_para that the hot path reads
  * (src/mod_ImportPara.f90:141-173, set_const_para :911-930). */
@@ -138,6 +139,30 @@ int ugks_implicit_steps(ugks_ctx* ctx, int max_steps, int* steps_done, int* conv
 /* state[16]: M0, reference_h, reference_b, reference set, mass_scale, streak, stop, steps, alpha,
  * macro alpha, moment error, converged (see ugks_implicit.cuh); report[80] as above. */
 int ugks_implicit_state(ugks_ctx* ctx, double* state, double* report);
+
+/* S2CN2, the explicit high-order method (TimeIntegration_method='S2CN2', consistency/high_explicit).
+ * ugks_s2cn2_init: the ledger of S2NativeInitializeState (src/mod_S2NativeAdapter.f90:323-349;
+ * total0 = sum of W over the cells, empty wall balance) and the volume targets of the current state
+ * (build_targets, src/mod_S2D1.f90:1246-1300).  ugks_init_freestream does this itself after the S2
+ * cold start; call it after ugks_upload_state.
+ * ugks_s2cn2_steps: up to nsteps steps of Solve_UGKS (src/mod_Solve.f90:84-165), each TimeStep,
+ * S2NativeEvolution with the targets kept between steps (src/mod_S2NativeAdapter.f90:469-490),
+ * ComputeResidual, and S2NativeApplyUpdate (:867-940) whose advance_step
+ * (src/mod_S2D1.f90:1302-1435) rebuilds the targets of the stream state and applies the
+ * Crank-Nicolson collision, gated by cnres / mmerr <= 2e-12 and the global conservation drift
+ * against the wall ledger.  A rejected step (the reference aborts with 203) ends the sequence: the
+ * state stays the last accepted one, *steps_done counts the accepted steps and the call returns
+ * UGKS_ENUMERIC with ugks_status_reference_code 203.  report[24] (optional) = the last step:
+ * [0] dt, [1] cnres, [2] mmerr, [3] max 2 beta, [4] transport CFL, [5..8] min/max of h and b,
+ * [9] drift, [10..13] bottom and [14..17] top wall macro flux / dy, [18..21] wall balance,
+ * [22] accepted, [23] accepted steps of this call. */
+int ugks_s2cn2_init(ugks_ctx* ctx);
+int ugks_s2cn2_steps(ugks_ctx* ctx, int nsteps, int* steps_done, double* report);
+/* The reference's test hooks for a rejected S2CN2 step (S2D3_TEST_GLOBAL_REJECT,
+ * src/mod_S2NativeAdapter.f90:433-435,926; S2E3_TEST_REJECT_STEP, src/mod_S2CartesianMPI.f90:254-264):
+ * the conservation drift of step `step` (1-based) of the next ugks_s2cn2_steps call is forced above
+ * the gate, so that step is rejected.  One-shot; 0 clears it.  Host-side, numerical only. */
+int ugks_s2cn2_test_reject(ugks_ctx* ctx, int step);
 
 /* Steady output fields of every cell, as Output writes them (src/mod_Output.f90:102-116):
  * out[nc][10] = r, u, v, T (= 1/lambda), p (= r T / 2), sxx, sxy, syy (Get_Stress_Vec,

@@ -61,6 +61,8 @@ def lib():
         L.uo_s2_evolution.argtypes = [ctypes.c_void_p, ctypes.c_double]
         L.uo_s2_compute_residual.argtypes = [ctypes.c_void_p, ctypes.c_double, ctypes.c_int]
         L.uo_s2_init_state.argtypes = [ctypes.c_void_p]
+        L.uo_s2cn2_init.argtypes = [ctypes.c_void_p]
+        L.uo_s2cn2_step.argtypes = [ctypes.c_void_p, dp, ctypes.c_int]
         for name in ("uo_res_macro", "uo_res_h", "uo_res_b", "uo_wall_aero", "uo_face_x_h", "uo_face_y_h",
                      "uo_face_x_w", "uo_face_y_w", "uo_phys_eq_h", "uo_phys_col_h", "uo_phys_col_b"):
             f = getattr(L, name)
@@ -113,8 +115,10 @@ class Oracle:
     def init_freestream(self, rho=1.0, U=0.0, V=0.0, tnative=None):
         t = self.case.tinf if tnative is None else tnative
         e = lib().uo_init_freestream(self.ptr, rho, U, V, t)
-        if not e and self.case.method == "HighOrderImplicit":
+        if not e and self.case.method in ("HighOrderImplicit", "S2CN2"):
             e = lib().uo_s2_init_state(self.ptr)   # S2NativeInitializeState cold start
+        if not e and self.case.method == "S2CN2":
+            e = lib().uo_s2cn2_init(self.ptr)      # the conservation ledger of the cold start
         if e:
             raise RuntimeError(f"oracle init failed: {e}")
 
@@ -152,6 +156,22 @@ class Oracle:
         e = lib().uo_implicit_step(self.ptr, _p(out), nout)
         if e:
             raise RuntimeError(f"oracle implicit step aborted with reference code {e}")
+        return out
+
+    CN_OUT = 22
+
+    def s2cn2_init(self):
+        """Conservation ledger of the current state (total0, empty wall balance); targets not built."""
+        e = lib().uo_s2cn2_init(self.ptr)
+        if e:
+            raise RuntimeError(f"oracle S2CN2 init failed: {e}")
+
+    def s2cn2_step(self):
+        """One S2CN2 step; returns the diagnostics vector (dt, cnres, mmerr, ..., drift, ledger)."""
+        out = np.zeros(self.CN_OUT)
+        e = lib().uo_s2cn2_step(self.ptr, _p(out), self.CN_OUT)
+        if e:
+            raise RuntimeError(f"oracle S2CN2 step rejected with reference code {e}")
         return out
 
     def view(self, name, shape):

@@ -57,12 +57,20 @@ struct uo_ctx {
     double *lco_h, *lco_b;        /* low_collision_old [nc][nvel] */
     double *s2_facc;              /* per-cell face flux accumulators */
     void *s2_scr;                 /* per-thread closure scratch */
+    /* S2CN2 explicit high-order step (ugks_oracle_s2.c) */
+    int s2_ready;                 /* s2_mh.. hold the targets of the accepted state */
+    double *cn_mh, *cn_mb, *cn_kxh, *cn_kxb, *cn_kyh, *cn_kyb, *cn_kappa;   /* targets of the proposal */
+    double *cn_wn, *cn_hs, *cn_bs;   /* stream state W + res, h + res_h, b + res_b */
+    double *cn_hn, *cn_bn;        /* proposal after the CN collision */
+    double *cn_cell;              /* [nc][UO_CN_CELL] per-cell advance diagnostics */
+    double cn_total0[4], cn_balance[4];   /* conservation ledger: initial totals, cumulative wall balance */
     /* scratch: 24 work vectors per OpenMP thread */
     int nthr;
     double **tt;
 };
 
 #define NSCR 24
+#define UO_CN_CELL 8
 #define MAX_THREADS 256
 static int g_threads = 1;   /* threads used by par_for; set by uo_set_threads */
 
@@ -402,9 +410,11 @@ uo_ctx* uo_create(const uo_params* p, const double* u, const double* v, const do
 }
 
 static void s2_free(uo_ctx* c);
+static void cn_free(uo_ctx* c);
 void uo_destroy(uo_ctx* c) {
     if (!c) return;
     s2_free(c);
+    cn_free(c);
     double* ptrs[] = {c->u, c->v, c->w, c->h, c->b, c->W, c->sh, c->sb, c->fxh, c->fxb, c->fxw, c->fyLh, c->fyLb,
                       c->fyRh, c->fyRb, c->fyLw, c->fyRw, c->res_w, c->res_h, c->res_b, c->rate_w, c->stream_h,
                       c->stream_b, c->peq_h, c->peq_b, c->pcol_h, c->pcol_b, c->wall_aero};

@@ -94,6 +94,14 @@ int uo_s2_evolution(uo_ctx* c, double dt);
 int uo_s2_compute_residual(uo_ctx* c, double dt, int rates_only);
 int uo_s2_init_state(uo_ctx* c);
 
+/* S2CN2, the explicit high-order step (S2NativeEvolution + ComputeResidual + S2NativeApplyUpdate /
+ * advance_step): uo_s2cn2_init sets the conservation ledger of the current state; each
+ * uo_s2cn2_step advances one step or rejects it (state untouched).  out[UO_CN_OUT] is listed at
+ * uo_s2cn2_step in ugks_oracle_s2.c. */
+#define UO_CN_OUT 22
+int uo_s2cn2_init(uo_ctx* c);
+int uo_s2cn2_step(uo_ctx* c, double* out, int nout);
+
 /* Worker threads used over faces and cells (0 = all host cores); returns the count in use.
  * Results do not depend on the thread count: faces and cells are independent and every sum over
  * cells is taken afterwards in cell order. */

@@ -1034,23 +1034,32 @@ static int s2_cell9(const s2_field* F, int i, int j, double val[3][3]) {
     return 1;
 }
 
-/* build_targets (mod_S2D1.f90:1246-1300): Gauss-averaged M, K_x, K_y of every cell, kappa */
+/* build_targets (mod_S2D1.f90:1246-1300): Gauss-averaged M, K_x, K_y of every cell of the macro
+ * field Wsrc, and kappa = heat(Wsrc, K) */
+typedef struct {
+    uo_ctx* c;
+    int* err;
+    const double* Wsrc;
+    double *mh, *mb, *kxh, *kxb, *kyh, *kyb, *kappa;
+} s2tg_arg;
+
 static void s2_target_body(void* vp, int cc, int tid) {
-    s2_arg* a = (s2_arg*)vp;
+    s2tg_arg* a = (s2tg_arg*)vp;
     uo_ctx* c = a->c;
     const uo_params* p = &c->p;
+    const double* Wsrc = a->Wsrc;
     int nx = p->nx, ny = p->ny, nv = p->nvel, i = cc % nx, j = cc / nx;
     s2_scratch* S = s2_scr(c, tid);
     double* B = S->buf + S2_CALLER * (size_t)nv;
     double *tmh = B, *tmb = B + nv, *tkxh = B + 2 * nv, *tkxb = B + 3 * nv, *tkyh = B + 4 * nv, *tkyb = B + 5 * nv;
     double *tt = B + 6 * nv, *nscr = S->buf + 32 * (size_t)nv;
     double nodes[4][3][3], avg[4] = {0, 0, 0, 0}, kap[2][2];
-    double *mh = c->s2_mh + (size_t)cc * nv, *mb = c->s2_mb + (size_t)cc * nv;
-    double *kxh = c->s2_kxh + (size_t)cc * nv, *kxb = c->s2_kxb + (size_t)cc * nv;
-    double *kyh = c->s2_kyh + (size_t)cc * nv, *kyb = c->s2_kyb + (size_t)cc * nv;
+    double *mh = a->mh + (size_t)cc * nv, *mb = a->mb + (size_t)cc * nv;
+    double *kxh = a->kxh + (size_t)cc * nv, *kxb = a->kxb + (size_t)cc * nv;
+    double *kyh = a->kyh + (size_t)cc * nv, *kyb = a->kyb + (size_t)cc * nv;
     for (int k = 0; k < nv; ++k) mh[k] = mb[k] = kxh[k] = kxb[k] = kyh[k] = kyb[k] = 0.0;
     for (int m = 0; m < 4; ++m) {
-        s2_field Fw = {c->W + m, 4, nx, ny};
+        s2_field Fw = {Wsrc + m, 4, nx, ny};
         if (!s2_cell9(&Fw, i, j, nodes[m])) { a->err[cc] = 420; return; }
     }
     for (int cq = 0; cq < 3; ++cq)
@@ -1059,7 +1068,7 @@ static void s2_target_body(void* vp, int cc, int tid) {
     for (int cq = 0; cq < 3; ++cq)
         for (int aq = 0; aq < 3; ++aq) {
             double wq[4], wt2 = s2_gw[aq] * s2_gw[cq];
-            for (int m = 0; m < 4; ++m) wq[m] = nodes[m][aq][cq] + c->W[cc * 4 + m] - avg[m];
+            for (int m = 0; m < 4; ++m) wq[m] = nodes[m][aq][cq] + Wsrc[cc * 4 + m] - avg[m];
             if (!s2_closure_prepare(&S->C, wq, p->ck, nv, c->u, c->v, c->w, nscr) ||
                 !s2_make_mke(p, &S->C, wq, nv, c->u, c->v, c->w, tmh, tmb, tkxh, tkxb, tkyh, tkyb, kap, tt)) {
                 a->err[cc] = 420;
@@ -1072,10 +1081,10 @@ static void s2_target_body(void* vp, int cc, int tid) {
             }
         }
     double q[2];
-    if (!s2_heat(c->W + cc * 4, p->ck, nv, kxh, kxb, c->u, c->v, c->w, q)) { a->err[cc] = 420; return; }
-    c->s2_kappa[cc * 4 + 0] = q[0]; c->s2_kappa[cc * 4 + 1] = q[1];
-    if (!s2_heat(c->W + cc * 4, p->ck, nv, kyh, kyb, c->u, c->v, c->w, q)) { a->err[cc] = 420; return; }
-    c->s2_kappa[cc * 4 + 2] = q[0]; c->s2_kappa[cc * 4 + 3] = q[1];
+    if (!s2_heat(Wsrc + cc * 4, p->ck, nv, kxh, kxb, c->u, c->v, c->w, q)) { a->err[cc] = 420; return; }
+    a->kappa[cc * 4 + 0] = q[0]; a->kappa[cc * 4 + 1] = q[1];   /* kappa(1:2, 1) */
+    if (!s2_heat(Wsrc + cc * 4, p->ck, nv, kyh, kyb, c->u, c->v, c->w, q)) { a->err[cc] = 420; return; }
+    a->kappa[cc * 4 + 2] = q[0]; a->kappa[cc * 4 + 3] = q[1];   /* kappa(1:2, 2) */
 }
 
 static int s2_first_error(uo_ctx* c) {
@@ -1116,10 +1125,12 @@ static void s2_free(uo_ctx* c) {
     free(sc);
 }
 
-/* S2NativeEvolution for HighOrderImplicit (mod_S2NativeAdapter.f90:469-490 and CartesianEvolution,
- * mod_S2CartesianMPI.f90:182-234): rebuild the volume targets, reconstruct, evaluate every face,
- * and publish the face fluxes times the face length into the face arrays ComputeResidual reads. */
-int uo_s2_evolution(uo_ctx* c, double dt) {
+/* S2NativeEvolution (mod_S2NativeAdapter.f90:469-490 and CartesianEvolution,
+ * mod_S2CartesianMPI.f90:182-234): rebuild the volume targets of W when asked (HighOrderImplicit
+ * invalidates them every call, :479; S2CN2 only when they are not ready, :480-484), reconstruct,
+ * evaluate every face, and publish the face fluxes times the face length into the face arrays
+ * ComputeResidual reads. */
+static int s2_evolution_core(uo_ctx* c, double dt, int rebuild_targets) {
     const uo_params* p = &c->p;
     int nx = p->nx, ny = p->ny, nv = p->nvel;
     int nthr = g_threads < c->nthr ? g_threads : c->nthr;
@@ -1127,9 +1138,13 @@ int uo_s2_evolution(uo_ctx* c, double dt) {
     c->dt = dt;
     memset(c->cell_err, 0, sizeof(int) * c->nc);
     s2_arg a = {c, c->cell_err};
-    par_for(c->nc, s2_target_body, &a, nthr);
-    int e = s2_first_error(c);
-    if (e) return e;
+    if (rebuild_targets) {
+        s2tg_arg t = {c, c->cell_err, c->W, c->s2_mh, c->s2_mb, c->s2_kxh, c->s2_kxb, c->s2_kyh, c->s2_kyb, c->s2_kappa};
+        par_for(c->nc, s2_target_body, &t, nthr);
+        int e = s2_first_error(c);
+        if (e) return e;
+    }
+    int e;
     par_for(c->nc, s2_recon_body, &a, nthr);
     if ((e = s2_first_error(c))) return e;
     par_for(c->nc, s2_face_body, &a, nthr);
@@ -1162,6 +1177,8 @@ int uo_s2_evolution(uo_ctx* c, double dt) {
         }
     return 0;
 }
+
+int uo_s2_evolution(uo_ctx* c, double dt) { return s2_evolution_core(c, dt, 1); }
 
 /* ComputeResidual + AssembleSteadyRateResiduals for the S2 path (mod_Residual.f90:17-132, IsS2CN2
  * branch) and S2NativePhysicalCollision (mod_S2NativeAdapter.f90:735-759): residuals from the
@@ -1253,4 +1270,216 @@ int uo_s2_init_state(uo_ctx* c) {
     s2init_arg a = {c};
     par_for(c->nc, s2_init_body, &a, g_threads < c->nthr ? g_threads : c->nthr);
     return s2_first_error(c);
+}
+
+/* ---------------------------------------------------------------- S2CN2 explicit step */
+
+static void cn_alloc(uo_ctx* c) {
+    if (c->cn_wn) return;
+    size_t S = (size_t)c->nc * c->p.nvel;
+    c->cn_mh = (double*)calloc(S, sizeof(double)); c->cn_mb = (double*)calloc(S, sizeof(double));
+    c->cn_kxh = (double*)calloc(S, sizeof(double)); c->cn_kxb = (double*)calloc(S, sizeof(double));
+    c->cn_kyh = (double*)calloc(S, sizeof(double)); c->cn_kyb = (double*)calloc(S, sizeof(double));
+    c->cn_kappa = (double*)calloc((size_t)c->nc * 4, sizeof(double));
+    c->cn_wn = (double*)calloc((size_t)c->nc * 4, sizeof(double));
+    c->cn_hs = (double*)calloc(S, sizeof(double)); c->cn_bs = (double*)calloc(S, sizeof(double));
+    c->cn_hn = (double*)calloc(S, sizeof(double)); c->cn_bn = (double*)calloc(S, sizeof(double));
+    c->cn_cell = (double*)calloc((size_t)c->nc * UO_CN_CELL, sizeof(double));
+}
+
+static void cn_free(uo_ctx* c) {
+    if (!c->cn_wn) return;
+    double* ptrs[] = {c->cn_mh, c->cn_mb, c->cn_kxh, c->cn_kxb, c->cn_kyh, c->cn_kyb, c->cn_kappa,
+                      c->cn_wn, c->cn_hs, c->cn_bs, c->cn_hn, c->cn_bn, c->cn_cell};
+    for (size_t q = 0; q < sizeof ptrs / sizeof ptrs[0]; ++q) free(ptrs[q]);
+}
+
+/* the ledger of S2NativeInitializeState (mod_S2NativeAdapter.f90:323-349): total0 = sum of W over
+ * the cells, an empty wall balance, targets not yet built */
+int uo_s2cn2_init(uo_ctx* c) {
+    s2_alloc(c);
+    cn_alloc(c);
+    for (int m = 0; m < 4; ++m) {
+        double t = 0.0;
+        for (int cc = 0; cc < c->nc; ++cc) t = t + c->W[cc * 4 + m];
+        c->cn_total0[m] = t;
+        c->cn_balance[m] = 0.0;
+    }
+    c->s2_ready = 0;
+    return 0;
+}
+
+/* advance_step's per-cell Crank-Nicolson collision (mod_S2D1.f90:1355-1421, S2PhysicalGas=1):
+ * beta = dt / (2 tau), the old-state Shakhov correction from q_old = heat(w, h - M), the 2x2 solve
+ * for the new heat flux and h_new = (rh + beta eq) / (1 + beta); the cnres / mmerr gates. */
+typedef struct { uo_ctx* c; double dt; } cn_arg;
+
+static void s2_cn_body(void* vp, int cc, int tid) {
+    cn_arg* a = (cn_arg*)vp;
+    uo_ctx* c = a->c;
+    const uo_params* p = &c->p;
+    const int nv = p->nvel;
+    const double dt = a->dt;
+    const size_t o = (size_t)cc * nv;
+    const double *w = c->W + cc * 4, *wn = c->cn_wn + cc * 4;
+    const double *h = c->h + o, *b = c->b + o, *hs = c->cn_hs + o, *bs = c->cn_bs + o;
+    const double *mh = c->s2_mh + o, *mb = c->s2_mb + o, *kxh = c->s2_kxh + o, *kxb = c->s2_kxb + o;
+    const double *kyh = c->s2_kyh + o, *kyb = c->s2_kyb + o;
+    const double *mhn = c->cn_mh + o, *mbn = c->cn_mb + o, *kxhn = c->cn_kxh + o, *kxbn = c->cn_kxb + o;
+    const double *kyhn = c->cn_kyh + o, *kybn = c->cn_kyb + o, *kap = c->cn_kappa + cc * 4;
+    double *hn = c->cn_hn + o, *bn = c->cn_bn + o, *d = c->cn_cell + (size_t)cc * UO_CN_CELL;
+    double** T = scratch_t(c, tid);
+    double *rh = T[0], *rb = T[1], *eqh = T[2], *eqb = T[3], *th = T[4], *tb = T[5];
+    double tau_o, tau_n, rold[2], rhs[2], qtmp[2], rnew[2], rhat[2], mom[4];
+    c->cell_err[cc] = 0;
+    if (!s2_tau(p, w, &tau_o) || !s2_tau(p, wn, &tau_n)) { c->cell_err[cc] = 104; return; }
+    const double beta_old = dt / (2.0 * tau_o), beta = dt / (2.0 * tau_n);
+    d[0] = fmax(2.0 * beta_old, 2.0 * beta);
+    for (int k = 0; k < nv; ++k) { th[k] = h[k] - mh[k]; tb[k] = b[k] - mb[k]; }
+    if (!s2_heat(w, p->ck, nv, th, tb, c->u, c->v, c->w, rold)) { c->cell_err[cc] = 445; return; }
+    for (int k = 0; k < nv; ++k) {
+        rh[k] = hs[k] + beta_old * (mh[k] + kxh[k] * rold[0] + kyh[k] * rold[1] - h[k]);
+        rb[k] = bs[k] + beta_old * (mb[k] + kxb[k] * rold[0] + kyb[k] * rold[1] - b[k]);
+    }
+    if (!s2_heat(wn, p->ck, nv, rh, rb, c->u, c->v, c->w, rhs) ||
+        !s2_heat(wn, p->ck, nv, mhn, mbn, c->u, c->v, c->w, qtmp)) { c->cell_err[cc] = 445; return; }
+    rhs[0] = rhs[0] - qtmp[0];
+    rhs[1] = rhs[1] - qtmp[1];
+    /* a22 = -beta kappa; a22(1,1), a22(2,2) += 1 + beta; kappa(r, col) = kap[2 col + r] */
+    double a11 = -beta * kap[0], a21 = -beta * kap[1], a12 = -beta * kap[2], a22 = -beta * kap[3];
+    a11 = a11 + 1.0 + beta;
+    a22 = a22 + 1.0 + beta;
+    const double det = a11 * a22 - a12 * a21;
+    if (!isfinite(det) || det <= 0.0) { c->cell_err[cc] = 445; return; }
+    rnew[0] = (rhs[0] * a22 - a12 * rhs[1]) / det;
+    rnew[1] = (a11 * rhs[1] - rhs[0] * a21) / det;
+    double scale = 1.0, cres = 0.0;
+    for (int k = 0; k < nv; ++k) {
+        eqh[k] = mhn[k] + kxhn[k] * rnew[0] + kyhn[k] * rnew[1];
+        eqb[k] = mbn[k] + kxbn[k] * rnew[0] + kybn[k] * rnew[1];
+        hn[k] = (rh[k] + beta * eqh[k]) / (1.0 + beta);
+        bn[k] = (rb[k] + beta * eqb[k]) / (1.0 + beta);
+    }
+    /* scale = max(1, max|rh|, max|rb|, max|hn|, max|bn|), in the Fortran argument order */
+    double mrh = 0.0, mrb = 0.0, mhn_ = 0.0, mbn_ = 0.0, erh = 0.0, erb = 0.0;
+    for (int k = 0; k < nv; ++k) {
+        mrh = fmax(mrh, fabs(rh[k])); mrb = fmax(mrb, fabs(rb[k]));
+        mhn_ = fmax(mhn_, fabs(hn[k])); mbn_ = fmax(mbn_, fabs(bn[k]));
+        erh = fmax(erh, fabs((1.0 + beta) * hn[k] - rh[k] - beta * eqh[k]));
+        erb = fmax(erb, fabs((1.0 + beta) * bn[k] - rb[k] - beta * eqb[k]));
+    }
+    scale = fmax(fmax(fmax(fmax(1.0, mrh), mrb), mhn_), mbn_);
+    cres = fmax(erh, erb) / scale;
+    for (int k = 0; k < nv; ++k) { th[k] = hn[k] - mhn[k]; tb[k] = bn[k] - mbn[k]; }
+    if (!s2_heat(wn, p->ck, nv, th, tb, c->u, c->v, c->w, rhat)) { c->cell_err[cc] = 445; return; }
+    cres = fmax(cres, fmax(fabs(rhat[0] - rnew[0]), fabs(rhat[1] - rnew[1])) /
+                          fmax(fmax(1.0, fmax(fabs(rhat[0]), fabs(rhat[1]))), fmax(fabs(rnew[0]), fabs(rnew[1]))));
+    if (!s2_moment(nv, hn, bn, c->u, c->v, c->w, mom)) { c->cell_err[cc] = 445; return; }
+    double mx = 0.0, sc = 1.0;
+    for (int m = 0; m < 4; ++m) { mx = fmax(mx, fabs(mom[m] - wn[m])); sc = fmax(sc, fabs(wn[m])); }
+    d[1] = cres;
+    d[2] = mx / sc;
+    double lo_h = INFINITY, hi_h = -INFINITY, lo_b = INFINITY, hi_b = -INFINITY;
+    for (int k = 0; k < nv; ++k) {
+        lo_h = fmin(lo_h, hn[k]); hi_h = fmax(hi_h, hn[k]);
+        lo_b = fmin(lo_b, bn[k]); hi_b = fmax(hi_b, bn[k]);
+    }
+    d[3] = lo_h; d[4] = hi_h; d[5] = lo_b; d[6] = hi_b;
+}
+
+/* One S2CN2 step of the explicit high-order method (TimeStep; S2NativeEvolution with the targets
+ * kept between steps, mod_S2NativeAdapter.f90:469-490; ComputeResidual; S2NativeApplyUpdate,
+ * :867-940, with advance_step on the stream state, mod_S2D1.f90:1302-1435): the proposal
+ * wn = W + res, hs = h + res_h; targets of wn; the CN collision; the cnres / mmerr gates (2e-12);
+ * the global conservation drift with the wall ledger.  A rejected step leaves W, h, b, the targets
+ * and the ledger untouched and returns the reference abort code (203, AbortSteadyImplicit, for a rejection).
+ * out[UO_CN_OUT]: [0] dt, [1] cnres, [2] mmerr, [3] max 2 beta, [4] transport CFL, [5..8] min/max
+ * of h and b, [9] drift, [10..13] bottom wall flux / dy, [14..17] top wall flux / dy,
+ * [18..21] wall balance after the step. */
+int uo_s2cn2_step(uo_ctx* c, double* out, int nout) {
+    const uo_params* p = &c->p;
+    const int nx = p->nx, ny = p->ny, nv = p->nvel, nc = c->nc;
+    int nthr = g_threads < c->nthr ? g_threads : c->nthr;
+    s2_alloc(c);
+    cn_alloc(c);
+    double o[UO_CN_OUT];
+    for (int q = 0; q < UO_CN_OUT; ++q) o[q] = 0.0;
+    const double dt = uo_timestep(c);
+    if (!isfinite(dt)) return 101;
+    o[0] = dt;
+    int e;
+    if (!c->s2_ready) {   /* native_build_targets of the accepted state (:480-484) */
+        memset(c->cell_err, 0, sizeof(int) * nc);
+        s2tg_arg t = {c, c->cell_err, c->W, c->s2_mh, c->s2_mb, c->s2_kxh, c->s2_kxb, c->s2_kyh, c->s2_kyb, c->s2_kappa};
+        par_for(nc, s2_target_body, &t, nthr);
+        if ((e = s2_first_error(c))) return e;
+        c->s2_ready = 1;
+    }
+    if ((e = s2_evolution_core(c, dt, 0))) return e;
+    if ((e = uo_s2_compute_residual(c, dt, 0))) return e;
+    /* the stream state (S2NativeApplyUpdate :884-890) */
+    for (int cc = 0; cc < nc; ++cc) {
+        for (int m = 0; m < 4; ++m) c->cn_wn[cc * 4 + m] = c->W[cc * 4 + m] + c->res_w[cc * 4 + m];
+        for (int k = 0; k < nv; ++k) {
+            c->cn_hs[(size_t)cc * nv + k] = c->h[(size_t)cc * nv + k] + c->res_h[(size_t)cc * nv + k];
+            c->cn_bs[(size_t)cc * nv + k] = c->b[(size_t)cc * nv + k] + c->res_b[(size_t)cc * nv + k];
+        }
+    }
+    memset(c->cell_err, 0, sizeof(int) * nc);
+    s2tg_arg t = {c, c->cell_err, c->cn_wn, c->cn_mh, c->cn_mb, c->cn_kxh, c->cn_kxb, c->cn_kyh, c->cn_kyb, c->cn_kappa};
+    par_for(nc, s2_target_body, &t, nthr);
+    if ((e = s2_first_error(c))) return e;
+    cn_arg ca = {c, dt};
+    par_for(nc, s2_cn_body, &ca, nthr);
+    if ((e = s2_first_error(c))) return e;
+    double cnres = 0.0, mmerr = 0.0, b2 = 0.0, lo_h = INFINITY, hi_h = 0.0, lo_b = INFINITY, hi_b = 0.0;
+    double umx = 0.0, vmx = 0.0;
+    for (int cc = 0; cc < nc; ++cc) {
+        const double* d = c->cn_cell + (size_t)cc * UO_CN_CELL;
+        b2 = fmax(b2, d[0]); cnres = fmax(cnres, d[1]); mmerr = fmax(mmerr, d[2]);
+        lo_h = fmin(lo_h, d[3]); hi_h = fmax(hi_h, d[4]); lo_b = fmin(lo_b, d[5]); hi_b = fmax(hi_b, d[6]);
+    }
+    for (int k = 0; k < nv; ++k) { umx = fmax(umx, fabs(c->u[k])); vmx = fmax(vmx, fabs(c->v[k])); }
+    o[1] = cnres; o[2] = mmerr; o[3] = b2; o[4] = dt * (umx / p->dx + vmx / p->dy);
+    o[5] = lo_h; o[6] = hi_h; o[7] = lo_b; o[8] = hi_b;
+    int reject = !(cnres <= S2_GATE) || !(mmerr <= S2_GATE);
+    for (size_t q = 0; q < (size_t)nc * 4 && !reject; ++q) if (!isfinite(c->cn_wn[q])) reject = 1;
+    for (size_t q = 0; q < (size_t)nc * nv && !reject; ++q)
+        if (!isfinite(c->cn_hn[q]) || !isfinite(c->cn_bn[q])) reject = 1;
+    /* global conservation: total of the proposal plus the wall ledger against total0 (:907-926) */
+    double total[4], bottom[4] = {0, 0, 0, 0}, top[4] = {0, 0, 0, 0}, drift = 0.0;
+    const size_t st = 2 * (size_t)nv + 4;
+    for (int m = 0; m < 4; ++m) {
+        double s = 0.0;
+        for (int cc = 0; cc < nc; ++cc) s = s + c->cn_wn[cc * 4 + m];
+        total[m] = s;
+    }
+    for (int i = 0; i < nx; ++i) {
+        const double* lw = c->s2_facc + (size_t)i * 3 * st + 2 * st + 2 * nv;
+        const double* tw = c->s2_facc + ((size_t)(ny - 1) * nx + i) * 3 * st + st + 2 * nv;
+        for (int m = 0; m < 4; ++m) { bottom[m] = bottom[m] + lw[m] / p->dy; top[m] = top[m] + tw[m] / p->dy; }
+    }
+    for (int m = 0; m < 4; ++m) {
+        const double bal = c->cn_balance[m] + top[m] - bottom[m];
+        drift = fmax(drift, fabs(total[m] + bal - c->cn_total0[m]) / fmax(1.0, fabs(c->cn_total0[m])));
+        o[10 + m] = bottom[m]; o[14 + m] = top[m]; o[18 + m] = bal;
+    }
+    o[9] = drift;
+    if (!(drift <= S2_GATE)) reject = 1;
+    if (out) for (int q = 0; q < nout && q < UO_CN_OUT; ++q) out[q] = o[q];
+    if (reject) return 203;
+    /* accept: publish the proposal, keep its targets, advance the ledger */
+    memcpy(c->W, c->cn_wn, sizeof(double) * 4 * (size_t)nc);
+    memcpy(c->h, c->cn_hn, sizeof(double) * (size_t)nc * nv);
+    memcpy(c->b, c->cn_bn, sizeof(double) * (size_t)nc * nv);
+    double* sw;
+    sw = c->s2_mh; c->s2_mh = c->cn_mh; c->cn_mh = sw;
+    sw = c->s2_mb; c->s2_mb = c->cn_mb; c->cn_mb = sw;
+    sw = c->s2_kxh; c->s2_kxh = c->cn_kxh; c->cn_kxh = sw;
+    sw = c->s2_kxb; c->s2_kxb = c->cn_kxb; c->cn_kxb = sw;
+    sw = c->s2_kyh; c->s2_kyh = c->cn_kyh; c->cn_kyh = sw;
+    sw = c->s2_kyb; c->s2_kyb = c->cn_kyb; c->cn_kyb = sw;
+    sw = c->s2_kappa; c->s2_kappa = c->cn_kappa; c->cn_kappa = sw;
+    for (int m = 0; m < 4; ++m) c->cn_balance[m] = o[18 + m];
+    return 0;
 }

@@ -19,6 +19,7 @@ UGKS_EUNSUPPORTED = 6
 UGKS_METHOD_EXPLICIT = 0
 UGKS_METHOD_IMPLICIT_STEADY = 1
 UGKS_METHOD_HIGH_ORDER_IMPLICIT = 2
+UGKS_METHOD_S2CN2 = 3
 
 # every symbol include/ugks_b200.h declares (checked by the CPU test suite)
 EXPORTS = [
@@ -27,9 +28,11 @@ EXPORTS = [
     "ugks_step_explicit", "ugks_wall_aero", "ugks_macro_fields", "ugks_copy_array", "ugks_last_status", "ugks_status_reference_code",
     "ugks_error_string", "ugks_stream", "ugks_synchronize", "ugks_profile_enable", "ugks_profile_read",
     "ugks_launch_count", "ugks_step_explicit_noalloc", "ugks_implicit_init", "ugks_implicit_steps",
-    "ugks_implicit_state",
+    "ugks_implicit_state", "ugks_s2cn2_init", "ugks_s2cn2_steps",
+    "ugks_s2cn2_test_reject",
 ]
 REPORT_LEN = 80
+CN_REPORT_LEN = 24
 # stages of one ImplicitSteady pseudo-step timed by the profile mode (kImStageNames in ugks_implicit.cuh)
 IMPLICIT_STAGES = ("timestep", "pre_evaluation", "pr2_prep", "pr2_sweep", "macro_alpha", "equilibrium",
                    "lusgs_forward", "wall_closure", "lusgs_backward", "micro_alpha", "apply", "rescale",
@@ -102,6 +105,9 @@ def load(path=LIB_PATH):
     L.ugks_implicit_init.argtypes = [vp]
     L.ugks_implicit_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), dp]
     L.ugks_implicit_state.argtypes = [vp, dp, dp]
+    L.ugks_s2cn2_init.argtypes = [vp]
+    L.ugks_s2cn2_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), dp]
+    L.ugks_s2cn2_test_reject.argtypes = [vp, ctypes.c_int]
     _lib = L
     return L
 

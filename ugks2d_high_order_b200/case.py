@@ -50,7 +50,8 @@ class CouetteCase:
 
 
 def reference_case(method="Explicit"):
-    """The reference's delivered Ma3 Couette case (cases/low_explicit|low_implicit|high_implicit)."""
+    """The reference's delivered Ma3 Couette case (cases/low_explicit|low_implicit|high_implicit, and
+    consistency/high_explicit for the explicit high-order S2CN2 method: no mass rescale)."""
     c = CouetteCase(method=method)
     if method in ("ImplicitSteady", "HighOrderImplicit"):
         c.mass_rescale = True

@@ -10,6 +10,7 @@
 
 #include "../../include/ugks_b200.h"
 #include "ugks_implicit.cuh"
+#include "ugks_s2cn2.cuh"
 
 namespace ugks {
 int lo_threads(int nvel);
@@ -67,6 +68,15 @@ struct ugks_ctx {
     KernelTimer t_slopes, t_faces, t_walls, t_cells;
     cudaEvent_t im_ev[kImStages + 1] = {};
     KernelTimer im_t[kImStages];
+    // S2CN2: double-buffered state (set 0 is B's h, b, W) and volume targets
+    double* cmem = nullptr;
+    unsigned* cflags = nullptr;    // [0] halt, [1] last-CTA counter, [2] accepted steps
+    CnBuffers C{};
+    S2Buffers T[2] = {};
+    LoBuffers Bs[2] = {};          // state sets 0 and 1 with the halt flag
+    bool cn_ready = false;         // ledger and targets of the current state are in place
+    int cn_reject_at = 0;          // step of the next sequence forced to fail its conservation gate
+    cudaGraphExec_t cgraph = nullptr;
 };
 
 static int cuda_fail(cudaError_t e) {
@@ -101,6 +111,7 @@ extern "C" int ugks_status_reference_code(unsigned st) {
     if (st & ST_PROJECTION) return 444;
     if (st & ST_NONFINITE_FLUX) return 13;
     if (st & ST_NONFINITE_STATE) return 4;
+    if (st & ST_STEP_REJECTED) return 203;
     if (st & ST_MOMENT_GATE) return 451;
     if (st & ST_ALPHA) return 433;
     if (st & ST_TIMEOUT) return 999;
@@ -125,7 +136,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
         p->ck < 1)
         return UGKS_EINVAL;
     if (p->method != UGKS_METHOD_EXPLICIT && p->method != UGKS_METHOD_IMPLICIT_STEADY &&
-        p->method != UGKS_METHOD_HIGH_ORDER_IMPLICIT)
+        p->method != UGKS_METHOD_HIGH_ORDER_IMPLICIT && p->method != UGKS_METHOD_S2CN2)
         return UGKS_EUNSUPPORTED;
     UGKS_CK(cudaSetDevice(device));
     ugks_ctx* c = new (std::nothrow) ugks_ctx();
@@ -189,7 +200,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     if (e == cudaSuccess) e = cudaMemcpyAsync(d + o_v, v, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     if (e == cudaSuccess) e = cudaMemcpyAsync(d + o_w, w, nv * sizeof(double), cudaMemcpyHostToDevice, c->stream);
     for (int i = 0; i < 5 && e == cudaSuccess; ++i) e = cudaEventCreate(&c->ev[i]);
-    if (e == cudaSuccess && p->method != UGKS_METHOD_EXPLICIT) {
+    if (e == cudaSuccess && (p->method == UGKS_METHOD_IMPLICIT_STEADY || p->method == UGKS_METHOD_HIGH_ORDER_IMPLICIT)) {
         // ImplicitSteady work arrays (mod_ImplicitState.f90:110-132)
         ImParams& Q = c->Q;
         Q.nslab = p->nslab > 0 ? p->nslab : 1;
@@ -233,6 +244,42 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
             I.mask = c->iflags; I.counter = c->iflags + 2;
         }
     }
+    if (e == cudaSuccess && p->method == UGKS_METHOD_S2CN2) {
+        // S2CN2: reconstruction cache, two target sets, the second state set, the stream state and the
+        // CN right-hand side, per-cell diagnostics, ledger, report and raw wall fluxes
+        size_t co = 0;
+        auto ctake = [&](size_t n) { size_t o = co; co += (n + 31) / 32 * 32; return o; };
+        const size_t c_rec = ctake((size_t)nc * 72 * nv);
+        size_t c_tg[2][6];
+        for (int q = 0; q < 2; ++q) for (int t = 0; t < 6; ++t) c_tg[q][t] = ctake(S);
+        const size_t c_h1 = ctake(S), c_b1 = ctake(S), c_W1 = ctake((size_t)nc * 4);
+        const size_t c_ws = ctake((size_t)nc * 4), c_rh = ctake(S), c_rb = ctake(S);
+        const size_t c_cell = ctake((size_t)nc * kCnCell), c_led = ctake(16), c_rep = ctake(kCnReport);
+        const size_t c_wr = ctake((size_t)2 * nx * 4);
+        e = prepare_s2();
+        if (e == cudaSuccess) e = cudaMalloc(&c->cmem, co * sizeof(double));
+        if (e == cudaSuccess) e = cudaMalloc(&c->cflags, 4 * sizeof(unsigned));
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->cmem, 0, co * sizeof(double), c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->cflags, 0, 4 * sizeof(unsigned), c->stream);
+        if (e == cudaSuccess) {
+            double* m = c->cmem;
+            for (int q = 0; q < 2; ++q) {
+                S2Buffers& T = c->T[q];
+                T.rec = m + c_rec;
+                T.mh = m + c_tg[q][0]; T.mb = m + c_tg[q][1]; T.kxh = m + c_tg[q][2];
+                T.kxb = m + c_tg[q][3]; T.kyh = m + c_tg[q][4]; T.kyb = m + c_tg[q][5];
+                T.wall_raw = m + c_wr;
+            }
+            CnBuffers& C = c->C;
+            C.ws = m + c_ws; C.rh = m + c_rh; C.rb = m + c_rb; C.cell = m + c_cell; C.ledger = m + c_led;
+            C.report = m + c_rep; C.wall_raw = m + c_wr;
+            C.halt = c->cflags; C.counter = c->cflags + 1; C.accepted = c->cflags + 2;
+            c->Bs[0] = B;
+            c->Bs[0].halt = C.halt;
+            c->Bs[1] = c->Bs[0];
+            c->Bs[1].h = m + c_h1; c->Bs[1].b = m + c_b1; c->Bs[1].W = m + c_W1;
+        }
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { ugks_ctx_destroy(c); return cuda_fail(e); }
     *out = c;
@@ -245,6 +292,9 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->igraph) cudaGraphExecDestroy(c->igraph);
+    if (c->cgraph) cudaGraphExecDestroy(c->cgraph);
+    if (c->cmem) cudaFree(c->cmem);
+    if (c->cflags) cudaFree(c->cflags);
     if (c->imem) cudaFree(c->imem);
     if (c->iflags) cudaFree(c->iflags);
     for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
@@ -281,6 +331,7 @@ extern "C" int ugks_upload_state(ugks_ctx* c, const double* h, const double* b, 
     UGKS_CK(cudaMemcpyAsync(c->B.b, b, S * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     UGKS_CK(cudaMemcpyAsync(c->B.W, W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyHostToDevice,
                             c->stream));
+    c->cn_ready = false;   // an S2CN2 context needs ugks_s2cn2_init for the new state
     int r = kernel_timestep(c);
     if (r) return r;
     return collect_status(c);
@@ -308,6 +359,12 @@ extern "C" int ugks_init_freestream(ugks_ctx* c, double rho, double U, double V,
     if (c->imem && c->Q.high_order) {   // S2NativeInitializeState cold start: h, b := closure Maxwellian of W
         UGKS_CK(s2_enqueue(0, c->P, c->B, c->I.s2, c->stream, c->stream2, c->ev_fork, c->ev_join));
         c->launches += 1;
+    }
+    if (c->cmem) {   // the same cold start, then the S2CN2 ledger and the targets of the state
+        UGKS_CK(s2_enqueue(0, c->P, c->B, c->T[0], c->stream, c->stream2, c->ev_fork, c->ev_join));
+        UGKS_CK(enqueue_s2cn2_prepare(c->P, c->Bs[0], c->T[0], c->C, c->stream, &c->launches));
+        c->launches += 1;
+        c->cn_ready = true;
     }
     int r = kernel_timestep(c);
     if (r) return r;
@@ -634,4 +691,86 @@ extern "C" int ugks_implicit_state(ugks_ctx* c, double* state, double* report) {
     if (report) UGKS_CK(cudaMemcpyAsync(report, c->I.report, kReport * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     UGKS_CK(cudaStreamSynchronize(c->stream));
     return UGKS_OK;
+}
+
+// ---------------------------------------------------------------------------------------------
+// S2CN2
+
+extern "C" int ugks_s2cn2_init(ugks_ctx* c) {
+    if (!c) return UGKS_EINVAL;
+    if (!c->cmem) return UGKS_EUNSUPPORTED;
+    UGKS_CK(cudaSetDevice(c->device));
+    UGKS_CK(enqueue_s2cn2_prepare(c->P, c->Bs[0], c->T[0], c->C, c->stream, &c->launches));
+    const int r = collect_status(c);
+    c->cn_ready = r == UGKS_OK;
+    return r;
+}
+
+extern "C" int ugks_s2cn2_test_reject(ugks_ctx* c, int step) {
+    if (!c || step < 0) return UGKS_EINVAL;
+    if (!c->cmem) return UGKS_EUNSUPPORTED;
+    c->cn_reject_at = step;
+    return UGKS_OK;
+}
+
+static cudaError_t enqueue_cn_step(ugks_ctx* c, int from) {
+    return enqueue_s2cn2_step(c->P, c->Bs[from], c->T[from], c->Bs[1 - from], c->T[1 - from], c->C, c->stream,
+                              c->stream2, c->ev_fork, c->ev_join, nullptr);
+}
+
+// a pair of steps, set 0 -> set 1 -> set 0, captured once and replayed
+static int build_cn_graph(ugks_ctx* c) {
+    if (c->cgraph) return UGKS_OK;
+    cudaGraph_t g;
+    UGKS_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    cudaError_t e = enqueue_cn_step(c, 0);
+    if (e == cudaSuccess) e = enqueue_cn_step(c, 1);
+    cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+    if (e != cudaSuccess) { if (e2 == cudaSuccess) cudaGraphDestroy(g); return cuda_fail(e); }
+    UGKS_CK(e2);
+    e = cudaGraphInstantiate(&c->cgraph, g, 0);
+    cudaGraphDestroy(g);
+    UGKS_CK(e);
+    return UGKS_OK;
+}
+
+extern "C" int ugks_s2cn2_steps(ugks_ctx* c, int nsteps, int* steps_done, double* report) {
+    if (!c || nsteps < 0) return UGKS_EINVAL;
+    if (!c->cmem) return UGKS_EUNSUPPORTED;
+    if (!c->cn_ready) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    if (steps_done) *steps_done = 0;
+    // a new sequence: clear the halt flag and the accepted count, and any stale status
+    int r = collect_status(c);
+    if (r) return r;
+    UGKS_CK(cudaMemsetAsync(c->cflags, 0, 3 * sizeof(unsigned), c->stream));
+    const double inject = (double)c->cn_reject_at;
+    UGKS_CK(cudaMemcpyAsync(c->C.ledger + 8, &inject, sizeof inject, cudaMemcpyHostToDevice, c->stream));
+    c->cn_reject_at = 0;
+    const int pairs = nsteps / 2;
+    if (pairs > 0) {
+        r = build_cn_graph(c);
+        if (r) return r;
+        for (int q = 0; q < pairs; ++q) UGKS_CK(cudaGraphLaunch(c->cgraph, c->stream));
+    }
+    if (nsteps % 2) UGKS_CK(enqueue_cn_step(c, 0));
+    c->launches += 7LL * nsteps;
+    unsigned acc = 0;
+    UGKS_CK(cudaMemcpyAsync(&acc, c->C.accepted, sizeof acc, cudaMemcpyDeviceToHost, c->stream));
+    if (report) UGKS_CK(cudaMemcpyAsync(report, c->C.report, kCnReport * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    r = collect_status(c);
+    if (acc % 2) {   // the last accepted state is in set 1: bring it (and its targets) back to set 0
+        const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
+        UGKS_CK(cudaMemcpyAsync(c->Bs[0].h, c->Bs[1].h, S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        UGKS_CK(cudaMemcpyAsync(c->Bs[0].b, c->Bs[1].b, S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        UGKS_CK(cudaMemcpyAsync(c->Bs[0].W, c->Bs[1].W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double),
+                                cudaMemcpyDeviceToDevice, c->stream));
+        double* src[6] = {c->T[1].mh, c->T[1].mb, c->T[1].kxh, c->T[1].kxb, c->T[1].kyh, c->T[1].kyb};
+        double* dst[6] = {c->T[0].mh, c->T[0].mb, c->T[0].kxh, c->T[0].kxb, c->T[0].kyh, c->T[0].kyb};
+        for (int t = 0; t < 6; ++t)
+            UGKS_CK(cudaMemcpyAsync(dst[t], src[t], S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        UGKS_CK(cudaStreamSynchronize(c->stream));
+    }
+    if (steps_done) *steps_done = (int)acc;
+    return r;
 }

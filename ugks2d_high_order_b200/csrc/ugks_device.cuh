@@ -27,6 +27,7 @@ enum : unsigned {
     ST_TIMEOUT = 1u << 6,        // bounded wait expired
     ST_ALPHA = 1u << 7,          // implicit admissible alpha not found
     ST_MOMENT_GATE = 1u << 8,    // implicit moment gate (Implicit_MomentTol)
+    ST_STEP_REJECTED = 1u << 9,  // 203: an S2CN2 step failed its cnres / mmerr / conservation gates
 };
 
 struct Prim { double r, U, V, L; };   // [rho, U, V, lambda = 1/T_native]

@@ -561,6 +561,7 @@ __device__ void last_cta_epilogue(const LoParams& P, const LoBuffers& B, bool wr
 }
 
 __global__ void __launch_bounds__(256) k_lo_timestep(LoParams P, LoBuffers B) {
+    if (halted(B)) return;
     __shared__ double red[8 * 64];
     __shared__ double rout[kRedSlots];
     const int nc = P.nx * P.ny;

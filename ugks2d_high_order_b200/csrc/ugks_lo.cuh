@@ -59,10 +59,20 @@ struct LoBuffers {
     const double* eval;      // [2] {valid, dt}: when valid and dt == dt[0], the slopes, fluxes and rates
                              // of the current state are already in place and the evaluation returns
                              // at entry (nullptr: always evaluate)
+    const unsigned* halt;    // [1] nonzero after a rejected step of a multi-step launch sequence.  With
+                             // halt set, a kernel returns at entry once this flag or any status bit
+                             // is set, so a failure anywhere in a step ends the sequence there
+                             // (nullptr: never halted)
 };
 
+__device__ __forceinline__ bool halted(const LoBuffers& B) {
+    return B.halt != nullptr && (*B.halt != 0u || *B.status != 0u);
+}
+
+// true when the evaluation kernels have nothing to do: the cached evaluation is current, or the
+// launch sequence has halted
 __device__ __forceinline__ bool eval_cached(const LoBuffers& B) {
-    return B.eval != nullptr && B.eval[0] != 0.0 && B.eval[1] == B.dt[0];
+    return halted(B) || (B.eval != nullptr && B.eval[0] != 0.0 && B.eval[1] == B.dt[0]);
 }
 
 __device__ __forceinline__ int wrapx(int i, int nx) { return i < 0 ? i + nx : (i >= nx ? i - nx : i); }

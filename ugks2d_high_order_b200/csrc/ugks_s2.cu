@@ -373,20 +373,6 @@ __global__ void __launch_bounds__(128) k_s2_recon(LoParams P, LoBuffers B, S2Buf
 // ------------------------------------------------------------------------------------------
 // block-level discrete closure
 
-// mod_S2D1.f90 primitive (:66-79): theta_gas = p / rho
-__device__ __forceinline__ bool s2_primitive(const double w[4], int ck, double& rho, double& ux, double& vy,
-                                             double& th) {
-    rho = w[0];
-    if (!(isfinite(w[0]) && isfinite(w[1]) && isfinite(w[2]) && isfinite(w[3])) || w[0] <= 0.0) return false;
-    ux = w[1] / w[0];
-    vy = w[2] / w[0];
-    const double eint = w[3] - 0.5 * w[0] * (ux * ux + vy * vy);
-    if (eint <= 0.0) return false;
-    const double p = (2.0 / (double)(ck + 2)) * eint;
-    th = p / w[0];
-    return isfinite(th) && th > 0.0;
-}
-
 // solve_dense_4x4 (mod_CorrectedWF2DClosure.f90:631-661), m row-major
 __device__ bool s2_solve4(const double* m, const double rhs[4], double x[4]) {
     double a[4][4], b[4];
@@ -1213,8 +1199,11 @@ __global__ void __launch_bounds__(NT) k_s2_walls(LoParams P, LoBuffers B, S2Buff
         const Slot s = slot(r, nv);
         if (s.ok) { B.fyh[o * nv + s.k] = afh[r] * P.dx; B.fyb[o * nv + s.k] = afb[r] * P.dx; }
     }
-    if (threadIdx.x == 0)
+    if (threadIdx.x == 0) {
         for (int m = 0; m < 4; ++m) B.fyw[o * 4 + m] = afw[m] * P.dx;
+        if (SB.wall_raw != nullptr)
+            for (int m = 0; m < 4; ++m) SB.wall_raw[((size_t)top * nx + i) * 4 + m] = afw[m];
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1286,8 +1275,11 @@ static void s2_launch_all(int which, const LoParams& P, const LoBuffers& B, cons
         e = cudaGetLastError();
         return;
     }
-    k_s2_targets<VPT, NT><<<nc, NT, 0, s>>>(P, B, S);
-    e = cudaGetLastError();
+    if (which != 2) {
+        k_s2_targets<VPT, NT><<<nc, NT, 0, s>>>(P, B, S);
+        e = cudaGetLastError();
+        if (which == 3) return;
+    }
     if (e == cudaSuccess) {
         const dim3 grid((unsigned)((P.nvel + 127) / 128), (unsigned)nc);
         k_s2_recon<<<grid, 128, 0, s>>>(P, B, S);
@@ -1301,7 +1293,8 @@ static void s2_launch_all(int which, const LoParams& P, const LoBuffers& B, cons
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
 }
 
-// the S2 Evolution of one pseudo-step (targets, reconstruction, faces, walls), or the S2 cold start
+// which 0: the S2 cold start; 1: the S2 Evolution of one pseudo-step (targets, reconstruction, faces,
+// walls); 2: the Evolution with the targets kept (S2CN2); 3: the targets of B.W only
 cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S2Buffers& S, cudaStream_t s,
                        cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join) {
     cudaError_t e = cudaSuccess;

@@ -16,6 +16,8 @@ struct S2Maps {
 struct S2Buffers {
     double* rec;                        // [cell][72][nvel] limited face values / derivatives
     double *mh, *mb, *kxh, *kxb, *kyh, *kyb;   // [cell][nvel] volume targets
+    double* wall_raw;                   // [2][nx][4] wall macro fluxes before the face length (bottom,
+                                        // top), for the S2CN2 conservation ledger (nullptr: not kept)
 };
 
 // s2_tau (mod_S2PhysicalGas.f90:9-20): GetTau of (rho, U, V, 0.5 rho / p), p = 2/(ck+2) e
@@ -25,8 +27,23 @@ __device__ __forceinline__ bool s2_tau(const LoParams& P, const double w[4], dou
     return get_tau(P.mu_ref, P.omega, p, tau);
 }
 
+// mod_S2D1.f90 primitive (:66-79): theta_gas = p / rho
+__device__ __forceinline__ bool s2_primitive(const double w[4], int ck, double& rho, double& ux, double& vy,
+                                             double& th) {
+    rho = w[0];
+    if (!(isfinite(w[0]) && isfinite(w[1]) && isfinite(w[2]) && isfinite(w[3])) || w[0] <= 0.0) return false;
+    ux = w[1] / w[0];
+    vy = w[2] / w[0];
+    const double eint = w[3] - 0.5 * w[0] * (ux * ux + vy * vy);
+    if (eint <= 0.0) return false;
+    const double p = (2.0 / (double)(ck + 2)) * eint;
+    th = p / w[0];
+    return isfinite(th) && th > 0.0;
+}
+
 cudaError_t prepare_s2();
-// which 0: S2 cold start (h, b := discrete closure Maxwellian of W); 1: S2 Evolution
+// which 0: S2 cold start (h, b := discrete closure Maxwellian of W); 1: S2 Evolution (targets of B.W,
+// reconstruction, faces, walls); 2: S2 Evolution with the targets in S kept; 3: targets of B.W into S
 cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S2Buffers& S, cudaStream_t s,
                        cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join);
 

@@ -39,7 +39,8 @@ class Solver:
         p.wall_tnative[0], p.wall_tnative[1] = case.wall_tnative
         p.fixed_dt = 0.0
         p.method = {"ImplicitSteady": capi.UGKS_METHOD_IMPLICIT_STEADY,
-                    "HighOrderImplicit": capi.UGKS_METHOD_HIGH_ORDER_IMPLICIT}.get(case.method, capi.UGKS_METHOD_EXPLICIT)
+                    "HighOrderImplicit": capi.UGKS_METHOD_HIGH_ORDER_IMPLICIT,
+                    "S2CN2": capi.UGKS_METHOD_S2CN2}.get(case.method, capi.UGKS_METHOD_EXPLICIT)
         p.ncfl, p.nslab, p.mass_rescale, p.macro_sweeps = case.ncfl, case.nslab, int(case.mass_rescale), case.macro_sweeps
         p.residual_tol, p.moment_tol, p.min_alpha = case.residual_tol, case.moment_tol, case.min_alpha
         self._params = p
@@ -134,6 +135,28 @@ class Solver:
         rep = np.zeros(capi.REPORT_LEN)
         self._check(self.L.ugks_implicit_state(self.ctx, _p(st), _p(rep)), "implicit_state")
         return st, rep
+
+    # ---- S2CN2, the explicit high-order method (S2NativeEvolution + S2NativeApplyUpdate)
+    def s2cn2_init(self):
+        """S2NativeInitializeState's ledger and the volume targets of the current state (done by
+        init_freestream; needed after upload)."""
+        self._check(self.L.ugks_s2cn2_init(self.ctx), "S2CN2 init")
+
+    def step_s2cn2(self, nsteps=1):
+        """nsteps S2CN2 steps.  Returns (steps_done, report) with report the last step's
+        diagnostics (layout in include/ugks_b200.h).  A rejected step raises UgksError with
+        reference code 203 after the accepted ones are kept."""
+        done = ctypes.c_int()
+        rep = np.zeros(capi.CN_REPORT_LEN)
+        code = self.L.ugks_s2cn2_steps(self.ctx, int(nsteps), ctypes.byref(done), _p(rep))
+        self.last_steps_done = done.value
+        self._check(code, "S2NativeApplyUpdate")
+        return done.value, rep
+
+    def s2cn2_test_reject(self, step):
+        """Force step `step` (1-based) of the next step_s2cn2 call to fail its conservation gate
+        (the reference's S2D3_TEST_GLOBAL_REJECT / S2E3_TEST_REJECT_STEP hooks)."""
+        self._check(self.L.ugks_s2cn2_test_reject(self.ctx, int(step)), "S2CN2 test reject")
 
     def wall_aero(self):
         out = np.empty((2, self.nx, 3))
