@@ -223,6 +223,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
         const size_t i_rec = Q.high_order ? itake((size_t)nc * 72 * nv) : 0;
         size_t i_tg[6] = {0, 0, 0, 0, 0, 0};
         if (Q.high_order) for (int t = 0; t < 6; ++t) i_tg[t] = itake(S);
+        const size_t i_scr = Q.high_order ? itake(s2_scratch_doubles(nx, ny, nv)) : 0;
         if (e == cudaSuccess && Q.high_order) e = prepare_s2();
         if (e == cudaSuccess) e = cudaMalloc(&c->imem, io * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&c->iflags, 4 * sizeof(unsigned));
@@ -240,6 +241,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
                 I.s2.rec = m + i_rec;
                 I.s2.mh = m + i_tg[0]; I.s2.mb = m + i_tg[1]; I.s2.kxh = m + i_tg[2];
                 I.s2.kxb = m + i_tg[3]; I.s2.kyh = m + i_tg[4]; I.s2.kyb = m + i_tg[5];
+                s2_bind_scratch(I.s2, m + i_scr, nx, ny, nv);
             }
             I.mask = c->iflags; I.counter = c->iflags + 2;
         }
@@ -255,7 +257,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
         const size_t c_h1 = ctake(S), c_b1 = ctake(S), c_W1 = ctake((size_t)nc * 4);
         const size_t c_ws = ctake((size_t)nc * 4), c_rh = ctake(S), c_rb = ctake(S);
         const size_t c_cell = ctake((size_t)nc * kCnCell), c_led = ctake(16), c_rep = ctake(kCnReport);
-        const size_t c_wr = ctake((size_t)2 * nx * 4);
+        const size_t c_wr = ctake((size_t)2 * nx * 4), c_scr = ctake(s2_scratch_doubles(nx, ny, nv));
         e = prepare_s2();
         if (e == cudaSuccess) e = cudaMalloc(&c->cmem, co * sizeof(double));
         if (e == cudaSuccess) e = cudaMalloc(&c->cflags, 4 * sizeof(unsigned));
@@ -269,6 +271,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
                 T.mh = m + c_tg[q][0]; T.mb = m + c_tg[q][1]; T.kxh = m + c_tg[q][2];
                 T.kxb = m + c_tg[q][3]; T.kyh = m + c_tg[q][4]; T.kyb = m + c_tg[q][5];
                 T.wall_raw = m + c_wr;
+                s2_bind_scratch(T, m + c_scr, nx, ny, nv);   // one evaluation at a time: shared by both sets
             }
             CnBuffers& C = c->C;
             C.ws = m + c_ws; C.rh = m + c_rh; C.rb = m + c_rb; C.cell = m + c_cell; C.ledger = m + c_led;

@@ -1,22 +1,27 @@
-// ugks_s2.cu -- the high-order "S2" evolution of HighOrderImplicit on sm_100a (FP64).
+// ugks_s2.cu -- the high-order "S2" evolution of HighOrderImplicit and S2CN2 on sm_100a (FP64).
 //
-//   k_s2_init    : S2 cold start, h, b := discrete closure Maxwellian of W (S2NativeInitializeState,
-//                  mod_S2NativeAdapter.f90:192-445 with make_mke).
-//   k_s2_targets : build_targets (mod_S2D1.f90:1246-1300): per cell the Gauss-averaged closure
-//                  targets M, K_x, K_y of 9 volume nodes.  One CTA per cell.
-//   k_s2_recon   : tensor WENO-AO(5,3) reconstruction with one-sided wall quartics and the
-//                  positivity limiter (mod_S2D1Reconstruction.f90, limit_cell_outputs
-//                  mod_S2D1.f90:315-345).  One thread per (cell, velocity); writes the face cache.
-//   k_s2_faces   : compute_flux's interior faces (mod_S2D1.f90:757-878): 3 Gauss nodes of
-//                  ugks_node (:421-521) per face.  One CTA per face.
-//   k_s2_walls   : the multiscale diffuse wall nodes (s2w2_wall_node, mod_S2MultiscaleWall.f90:45-184).
+//   k_s2_init         : S2 cold start, h, b := discrete closure Maxwellian of W (S2NativeInitializeState,
+//                       mod_S2NativeAdapter.f90:192-445 with make_mke).  One warp per cell.
+//   k_s2_macro        : macro WENO of W: the normal / tangential slopes of every interior face at its 3
+//                       Gauss nodes (compute_flux :803-808,849-854) and the 9 mean-shifted volume node
+//                       states of every cell (build_targets, mod_S2D1.f90:1246-1300).
+//   k_s2_target_nodes : build_targets' closures: one warp per (cell, volume node) -> node scalars.
+//   k_s2_target_sum   : the Gauss-weighted targets M, K_x, K_y per (cell, velocity) from those scalars.
+//   k_s2_recon1/2     : tensor WENO-AO(5,3) reconstruction with one-sided wall quartics and the
+//                       positivity limiter (mod_S2D1Reconstruction.f90, limit_cell_outputs
+//                       mod_S2D1.f90:315-345): the shared first layer, then per cell the second-layer
+//                       templates and the limiter; writes the face cache.
+//   k_s2_face_nodes   : ugks_node (mod_S2D1.f90:421-521) at one Gauss node of one interior face per warp.
+//   k_s2_wall_nodes   : the multiscale diffuse wall node (s2w2_wall_node, mod_S2MultiscaleWall.f90:45-184)
+//                       per warp.
+//   k_s2_combine      : the Gauss-weighted node fluxes times the face length into the face arrays.
 //
-// The block-level discrete closure (solve_q_first, mod_CorrectedWF2DClosure.f90:331-426) runs its
-// Newton iteration with one CTA: every trial state is one block reduction of the 16 Jacobian
-// moments, the 4 moments and 2 flags; thread 0 keeps the reference's accept / backtrack / stop
-// logic and broadcasts the next trial through shared memory.  The closure Maxwellian and its
-// theta-derivatives are recomputed from theta where needed (the same rounded values), so a thread
-// holds only its velocities' working arrays.
+// The discrete closure (solve_q_first, mod_CorrectedWF2DClosure.f90:331-426) runs on one warp: its
+// lanes stride over the velocities, every moment sum is a per-lane sum and a fixed butterfly whose
+// totals every lane receives, and every lane runs the reference's accept / backtrack / stop logic on
+// those identical totals.  Per-velocity closure quantities (the Maxwellian, the Shakhov directions,
+// the slope directions) are recomputed from the closure's few scalars in each pass instead of being
+// stored.
 #include "ugks_implicit.cuh"
 #include "ugks_s2.cuh"
 
@@ -319,59 +324,148 @@ __device__ bool s2_cell9(const S2Field& F, int i, int j, double val[3][3]) {
 }
 
 // ------------------------------------------------------------------------------------------
-// reconstruction + limiter: one thread per (cell, velocity); cache layout
-// rec[((cell*72 + field*12 + side*3 + node)*nvel + k], fields: h, b, h_n, h_t, b_n, b_t
-__global__ void __launch_bounds__(128) k_s2_recon(LoParams P, LoBuffers B, S2Buffers S) {
+// reconstruction + limiter in two passes.  Cache layout rec[((cell*72 + field*12 + side*3 + node)*nvel + k],
+// fields: h, b, h_n, h_t, b_n, b_t; sides: x left, x right, y bottom, y top.
+//
+// k_s2_recon1, the first layer (prepare_first_layer_plane, mod_S2D1Reconstruction.f90:501-578):
+// per (cell, velocity, field) the 1-D WENO along x of the cell's own row -- values and derivatives
+// at xi = -1/2, +1/2 and values at the 3 Gauss nodes -- and, for rows away from the walls, along y
+// of the cell's own column -- values and derivatives at -1/2, +1/2.  These are the first-layer
+// results the tensor templates of the 5 neighbouring cells share.  l1[cell][field*11 + q][nvel]:
+// q 0..3 = x value/derivative at -1/2, +1/2; 4..6 = x Gauss values; 7..10 = y value/derivative.
+// CTA: 4 warps (field, direction) over 32 velocities of one cell.
+__global__ void __launch_bounds__(128) k_s2_recon1(LoParams P, LoBuffers B, S2Buffers S) {
     if (eval_cached(B)) return;
-    const int nv = P.nvel, nx = P.nx, ny = P.ny;
-    const int k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= nv) return;
+    const int nv = P.nvel, nx = P.nx, ny = P.ny, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int f = warp >> 1, dir = warp & 1;
+    const int k0 = blockIdx.x * 32 + lane;
+    const bool kok = k0 < nv;
+    const int k = kok ? k0 : nv - 1;
     const int cc = blockIdx.y, i = cc % nx, j = cc / nx;
-    const S2Field Fh{B.h + k, nv, nx, ny}, Fb{B.b + k, nv, nx, ny};
-    double hf[4][3], hn[4][3], ht[4][3], hv[3][3], bf[4][3], bn[4][3], bt[4][3], bv[3][3];
-    bool ok = s2_cell_faces9(Fh, i, j, hf, hn, ht, hv) && s2_cell_faces9(Fb, i, j, bf, bn, bt, bv);
-    const double hm = B.h[(size_t)cc * nv + k], bm = B.b[(size_t)cc * nv + k];
-    const double margin = 64.0 * kEps;
-    double theta = 1.0;
-    if (hm <= 0.0 || bm <= 0.0) {
-        theta = 0.0;
-    } else {
+    if (dir == 1 && s2_near_wall(j, ny)) return;   // walls use one-sided quartics instead
+    const S2Field F{(f == 0 ? B.h : B.b) + k, nv, nx, ny};
+    double q[5], fw[4], coef[4][5];
 #pragma unroll
-        for (int s = 0; s < 4; ++s)
+    for (int s = -2; s <= 2; ++s) q[s + 2] = dir == 0 ? F.at(i + s, j) : F.at(i, j + s);
+    const bool ok = s2_weno_coef(q, fw, coef);
+    double* o = S.l1 + ((size_t)cc * 22 + f * 11 + (dir == 0 ? 0 : 7)) * nv + k;
+    double v0, d0, v1, d1;
+    s2_eval(fw, coef, -0.5, v0, d0);
+    s2_eval(fw, coef, 0.5, v1, d1);
+    if (kok) {
+        o[0] = v0; o[(size_t)nv] = d0; o[2 * (size_t)nv] = v1; o[3 * (size_t)nv] = d1;
+        if (dir == 0)
 #pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                if (hf[s][a] < 0.0) theta = fmin(theta, (1.0 - margin) * hm / (hm - hf[s][a]));
-                if (bf[s][a] < 0.0) theta = fmin(theta, (1.0 - margin) * bm / (bm - bf[s][a]));
-            }
-#pragma unroll
-        for (int c = 0; c < 3; ++c)
-#pragma unroll
-            for (int a = 0; a < 3; ++a) {
-                if (hv[a][c] < 0.0) theta = fmin(theta, (1.0 - margin) * hm / (hm - hv[a][c]));
-                if (bv[a][c] < 0.0) theta = fmin(theta, (1.0 - margin) * bm / (bm - bv[a][c]));
-            }
-        theta = fmax(0.0, fmin(1.0, theta));
+            for (int a = 0; a < 3; ++a) o[(size_t)(4 + a) * nv] = s2_eval_v(fw, coef, c_s2.gnode[a]);
+        if (!ok) set_status(B.status, ST_NONFINITE_FLUX);
     }
-    double* r = S.rec + (size_t)cc * 72 * nv + k;
+}
+
+// k_s2_recon2, the second layer (tensor_velocity_tile, :723-792; reconstruct_wall_tile, :918-971) and
+// limit_cell_outputs (mod_S2D1.f90:315-345): CTA = 8 warps (field f = warp / 4, part p = warp % 4)
+// over 32 velocities of one cell.  Part p reconstructs face side p (x left, x right, y bottom, y top)
+// at its 3 Gauss nodes with value, normal and tangential derivative, and parts 0..2 also the volume
+// Gauss row p; the positivity factor theta is the minimum over the 8 warps (both fields, all face and
+// volume samples), then each warp writes its side's limited values.
+__global__ void __launch_bounds__(256) k_s2_recon2(LoParams P, LoBuffers B, S2Buffers S) {
+    if (eval_cached(B)) return;
+    __shared__ double s_th[8][32];
+    const int nv = P.nvel, nx = P.nx, ny = P.ny, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int f = warp >> 2, p = warp & 3;
+    const int k0 = blockIdx.x * 32 + lane;
+    const bool kok = k0 < nv;
+    const int k = kok ? k0 : nv - 1;
+    const int cc = blockIdx.y, i = cc % nx, j = cc / nx;
+    const bool nw = s2_near_wall(j, ny);
+    const int first = nw ? s2_wall_first(j, ny) : j - 2;   // rows of the x first layer
+    const double* L1 = S.l1 + (size_t)f * 11 * nv + k;
+    auto X = [&](int r, int q) { return L1[((size_t)((first + r) * nx + i) * 22 + q) * nv]; };
+    double face[3], dn[3], dt[3], vol[3];
+    bool ok = true;
+    if (p < 2) {   // x face p
+        double a5[5], b5[5];
 #pragma unroll
-    for (int s = 0; s < 4; ++s) {
-        const double nd = s < 2 ? P.dx : P.dy, td = s < 2 ? P.dy : P.dx;
+        for (int r = 0; r < 5; ++r) { a5[r] = X(r, 2 * p); b5[r] = X(r, 2 * p + 1); }
+        if (!nw) ok = s2_companion3(a5, b5, face, dt, dn);
+        else {
+            double dummy;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) {
-            const double v[6] = {hm + theta * (hf[s][a] - hm), bm + theta * (bf[s][a] - bm), theta * hn[s][a] / nd,
-                                 theta * ht[s][a] / td, theta * bn[s][a] / nd, theta * bt[s][a] / td};
-#pragma unroll
-            for (int f = 0; f < 6; ++f) {
-                r[(size_t)(f * 12 + s * 3 + a) * nv] = v[f];
-                ok = ok && isfinite(v[f]);
+            for (int a = 0; a < 3; ++a) {
+                s2_wall_eval(a5, j, ny, c_s2.gnode[a], face[a], dt[a]);
+                s2_wall_eval(b5, j, ny, c_s2.gnode[a], dn[a], dummy);
             }
         }
+    } else {       // y face p - 2
+        const int s = p - 2;
+        double a5[5], b5[5];
+        if (!nw) {
+#pragma unroll
+            for (int r = 0; r < 5; ++r) {
+                const double* y = L1 + ((size_t)(j * nx + wrapx(i + r - 2, nx)) * 22 + 7 + 2 * s) * nv;
+                a5[r] = y[0];
+                b5[r] = y[(size_t)nv];
+            }
+        } else {
+            const S2Field F{(f == 0 ? B.h : B.b) + k, nv, nx, ny};
+#pragma unroll
+            for (int r = -2; r <= 2; ++r) {
+                double q[5];
+#pragma unroll
+                for (int t = 0; t < 5; ++t) q[t] = F.at(i + r, first + t);
+                s2_wall_eval(q, j, ny, s == 0 ? -0.5 : 0.5, a5[r + 2], b5[r + 2]);
+            }
+        }
+        ok = s2_companion3(a5, b5, face, dt, dn);
     }
-    if (!ok) set_status(B.status, ST_NONFINITE_FLUX);
+    if (p < 3) {   // volume Gauss row p
+        double a5[5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) a5[r] = X(r, 4 + p);
+        if (!nw) {
+            double fw[4], coef[4][5];
+            ok = ok && s2_weno_coef(a5, fw, coef);
+#pragma unroll
+            for (int b = 0; b < 3; ++b) vol[b] = s2_eval_v(fw, coef, c_s2.gnode[b]);
+        } else {
+            double dummy;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) s2_wall_eval(a5, j, ny, c_s2.gnode[b], vol[b], dummy);
+        }
+    }
+    // positivity factor (limit_cell_outputs): min over both fields' face and volume samples
+    const double hm = B.h[(size_t)cc * nv + k], bm = B.b[(size_t)cc * nv + k];
+    const double mf = f == 0 ? hm : bm;
+    const double margin = 64.0 * kEps;
+    double cand = 1.0;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        if (face[a] < 0.0) cand = fmin(cand, (1.0 - margin) * mf / (mf - face[a]));
+        if (p < 3 && vol[a] < 0.0) cand = fmin(cand, (1.0 - margin) * mf / (mf - vol[a]));
+    }
+    s_th[warp][lane] = cand;
+    __syncthreads();
+    double theta = s_th[0][lane];
+#pragma unroll
+    for (int w = 1; w < 8; ++w) theta = fmin(theta, s_th[w][lane]);
+    theta = (hm <= 0.0 || bm <= 0.0) ? 0.0 : fmax(0.0, fmin(1.0, theta));
+    const double nd = p < 2 ? P.dx : P.dy, td = p < 2 ? P.dy : P.dx;
+    double* r = S.rec + (size_t)cc * 72 * nv + k;
+    const int fv = f == 0 ? 0 : 1, fn = f == 0 ? 2 : 4, ft = f == 0 ? 3 : 5;
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const double v = mf + theta * (face[a] - mf), n = theta * dn[a] / nd, t = theta * dt[a] / td;
+        if (kok) {
+            r[(size_t)(fv * 12 + p * 3 + a) * nv] = v;
+            r[(size_t)(fn * 12 + p * 3 + a) * nv] = n;
+            r[(size_t)(ft * 12 + p * 3 + a) * nv] = t;
+        }
+        ok = ok && isfinite(v) && isfinite(n) && isfinite(t);
+    }
+    if (!ok && kok) set_status(B.status, ST_NONFINITE_FLUX);
 }
 
 // ------------------------------------------------------------------------------------------
-// block-level discrete closure
+// closure helpers
 
 // solve_dense_4x4 (mod_CorrectedWF2DClosure.f90:631-661), m row-major
 __device__ bool s2_solve4(const double* m, const double rhs[4], double x[4]) {
@@ -439,152 +533,6 @@ __device__ __forceinline__ S2Q s2_q(const double th[4], int ck, double u, double
     return q;
 }
 
-// shared scalars of the block-level routines
-struct S2Shared {
-    double red[16 * 64];
-    double rout[kRedSlots];
-    double w[4];          // closure target
-    double th[4];         // converged theta
-    double trial[4];
-    double jac[16];       // converged Jacobian (row-major: moment r, theta a)
-    double tjac[16];
-    double res[4], step[4], alpha, norm;
-    double v[48];         // broadcast scalars of the callers
-    int act, iter;
-};
-
-enum { S2_EVAL_INIT = 0, S2_EVAL_TRIAL = 1, S2_DONE = 2, S2_FAIL = 3 };
-
-__device__ __forceinline__ double s2_scaled(const double r[4], const double w[4]) {
-    double s = 0.0;
-#pragma unroll
-    for (int m = 0; m < 4; ++m) s = fmax(s, fabs(r[m]) / fmax(1.0, fabs(w[m])));
-    return s;
-}
-
-// thread 0: choose the next trial after a rejected one or a new Newton iteration
-__device__ void s2_newton_next(S2Shared& S, bool new_iter) {
-    const double tol = 5.0e-13, floor_a = 9.5367431640625e-07;   // 2^-20
-    if (new_iter) {
-        if (S.norm <= tol) { S.act = S2_DONE; return; }
-        if (S.iter > 12) { S.act = S2_FAIL; return; }
-        const double mr[4] = {-S.res[0], -S.res[1], -S.res[2], -S.res[3]};
-        double st[4];
-        if (!s2_solve4(S.jac, mr, st)) { S.act = S2_FAIL; return; }
-#pragma unroll
-        for (int m = 0; m < 4; ++m) S.step[m] = st[m];
-        S.alpha = 1.0;
-    }
-    while (S.alpha >= floor_a) {
-        double nt[4];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) nt[m] = S.th[m] + S.alpha * S.step[m];
-        if (nt[0] > 0.0 && nt[3] > 0.0 && isfinite(nt[0]) && isfinite(nt[1]) && isfinite(nt[2]) && isfinite(nt[3])) {
-#pragma unroll
-            for (int m = 0; m < 4; ++m) S.trial[m] = nt[m];
-            S.act = S2_EVAL_TRIAL;
-            return;
-        }
-        S.alpha = 0.5 * S.alpha;
-    }
-    S.act = S2_FAIL;
-}
-
-// solve_q_first with one CTA.  w must be in S.w (written by the caller before a barrier).
-// Returns the converged theta / Jacobian in S.th / S.jac (uniform result).
-template <int VPT>
-__device__ bool s2_closure(const LoParams& P, const LoBuffers& B, S2Shared& S) {
-    const int nv = P.nvel, ck = P.ck;
-    if (threadIdx.x == 0) {
-        const double* w = S.w;
-        bool ok = isfinite(w[0]) && isfinite(w[1]) && isfinite(w[2]) && isfinite(w[3]) && w[0] > 0.0;
-        if (ok) {   // primitive_from_conserved_2d (mod_CorrectedWF2DEquilibrium.f90:25-41)
-            const double u = w[1] / w[0], v = w[2] / w[0];
-            const double kin = 0.5 * (u * u + v * v), ein = w[3] / w[0] - kin;
-            const double temp = 4.0 * ein / (double)(ck + 2);
-            ok = isfinite(u) && isfinite(v) && isfinite(temp) && temp > 0.0;
-            S.trial[0] = w[0]; S.trial[1] = u; S.trial[2] = v; S.trial[3] = temp;
-        }
-        S.act = ok ? S2_EVAL_INIT : S2_FAIL;
-    }
-    __syncthreads();
-    for (int guard = 0; guard < 1024; ++guard) {
-        const int act = S.act;
-        if (act == S2_DONE || act == S2_FAIL) break;
-        double th[4];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) th[m] = S.trial[m];
-        // 16 Jacobian moments, 4 moments of (qh, qb), flags: nonfinite, nonpositive
-        double acc[22];
-#pragma unroll
-        for (int m = 0; m < 22; ++m) acc[m] = 0.0;
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            const Slot s = slot(r, nv);
-            const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
-            const S2Q q = s2_q(th, ck, uk, vk);
-            const double e2 = uk * uk + vk * vk;
-#pragma unroll
-            for (int a = 0; a < 4; ++a) {
-                const double hk = q.qh * q.ld[a], bk = q.qb * q.ldb[a];
-                acc[0 * 4 + a] += wk * hk;
-                acc[1 * 4 + a] += wk * uk * hk;
-                acc[2 * 4 + a] += wk * vk * hk;
-                acc[3 * 4 + a] += 0.5 * wk * (e2 * hk + bk);
-            }
-            acc[16] += wk * q.qh;
-            acc[17] += wk * uk * q.qh;
-            acc[18] += wk * vk * q.qh;
-            acc[19] += 0.5 * wk * (e2 * q.qh + q.qb);
-            if (s.ok) {
-                acc[20] = fmax(acc[20], (isfinite(q.qh) && isfinite(q.qb)) ? 0.0 : 1.0);
-                acc[21] = fmax(acc[21], (q.qh > 0.0 && q.qb > 0.0) ? 0.0 : 1.0);
-            }
-        }
-        block_reduce_smem<20, 2>(acc, S.red, S.rout);
-        if (threadIdx.x == 0) {
-            const double* o = S.rout;
-            bool fin = o[20] == 0.0;
-#pragma unroll
-            for (int m = 0; m < 20; ++m) fin = fin && isfinite(o[m]);
-            double nres[4];
-#pragma unroll
-            for (int m = 0; m < 4; ++m) nres[m] = o[16 + m] - S.w[m];
-            if (act == S2_EVAL_INIT) {
-                if (!fin) S.act = S2_FAIL;
-                else {
-#pragma unroll
-                    for (int m = 0; m < 4; ++m) { S.th[m] = th[m]; S.res[m] = nres[m]; }
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) S.jac[m] = o[m];
-                    S.norm = s2_scaled(nres, S.w);
-                    S.iter = 1;
-                    s2_newton_next(S, true);
-                    if (S.act == S2_DONE && o[21] != 0.0) S.act = S2_FAIL;
-                }
-            } else {
-                const double nn = fin ? s2_scaled(nres, S.w) : INFINITY;
-                const bool accepted = fin && (nn < S.norm || nn <= 5.0e-13);
-                if (accepted) {
-#pragma unroll
-                    for (int m = 0; m < 4; ++m) { S.th[m] = th[m]; S.res[m] = nres[m]; }
-#pragma unroll
-                    for (int m = 0; m < 16; ++m) S.jac[m] = o[m];
-                    S.norm = nn;
-                    S.iter = S.iter + 1;
-                    s2_newton_next(S, true);
-                    if (S.act == S2_DONE && o[21] != 0.0) S.act = S2_FAIL;
-                } else {
-                    S.alpha = 0.5 * S.alpha;
-                    s2_newton_next(S, false);
-                }
-            }
-        }
-        __syncthreads();
-    }
-    return S.act == S2_DONE;
-}
-
 // dq for a moment direction m (closure_first_direction): td = solve(jac, m) by thread `who`,
 // broadcast through S.v[base..base+3]
 __device__ __forceinline__ void s2_dq(const S2Q& q, const double td[4], double& dh, double& db) {
@@ -596,387 +544,505 @@ __device__ __forceinline__ void s2_dq(const S2Q& q, const double td[4], double& 
     }
 }
 
-// make_mke_prepared (mod_S2D1.f90:111-151) after s2_closure on w = S.w: per velocity slot the
-// closure Maxwellian M and the projected Shakhov directions K_x, K_y.  Returns the uniform gate.
-template <int VPT>
-__device__ bool s2_make_mke(const LoParams& P, const LoBuffers& B, S2Shared& S, double mh[VPT], double mb[VPT],
-                            double kxh[VPT], double kxb[VPT], double kyh[VPT], double kyb[VPT]) {
-    const int nv = P.nvel, ck = P.ck;
-    double rho, ux, vy, th;
-    const double w[4] = {S.w[0], S.w[1], S.w[2], S.w[3]};
-    const bool pok = s2_primitive(w, ck, rho, ux, vy, th);
-    const double lam = 0.5 / th;
-    double thc[4];
+// ------------------------------------------------------------------------------------------
+// warp-level discrete closure.  One warp owns one closure-bearing node: lane l takes the
+// velocities k = l, l + 32, ...; every velocity sum is a per-lane sequential sum followed by a
+// fixed butterfly (warp_halving) and a broadcast, so all lanes hold bitwise-identical totals and
+// run the same Newton / gate logic.  No shared memory and no block barriers.
+
+struct WVel {
+    int k;       // velocity index, clamped to a valid one
+    bool ok;     // a real velocity of this lane
+    double u, v, w;
+};
+__device__ __forceinline__ WVel wvel(const LoBuffers& B, int nv, int r) {
+    WVel s;
+    const int k = (threadIdx.x & 31) + 32 * r;
+    s.ok = k < nv;
+    s.k = s.ok ? k : nv - 1;
+    s.u = __ldg(B.u + s.k);
+    s.v = __ldg(B.v + s.k);
+    s.w = s.ok ? __ldg(B.w + s.k) : 0.0;
+    return s;
+}
+
+template <int N>
+__device__ __forceinline__ void warp_sum_all(double* v) {
+    constexpr int sh = 5 - ilog2(pow2_ceil(N));
+    const double r = warp_halving<N, false>(v);
 #pragma unroll
-    for (int m = 0; m < 4; ++m) thc[m] = S.th[m];
+    for (int i = 0; i < N; ++i) v[i] = __shfl_sync(0xffffffffu, r, i << sh);
+}
+template <int N>
+__device__ __forceinline__ void warp_max_all(double* v) {
+    constexpr int sh = 5 - ilog2(pow2_ceil(N));
+    const double r = warp_halving<N, true>(v);
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = __shfl_sync(0xffffffffu, r, i << sh);
+}
+
+__device__ __forceinline__ double s2_scaled(const double r[4], const double w[4]) {
+    double s = 0.0;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) s = fmax(s, fabs(r[m]) / fmax(1.0, fabs(w[m])));
+    return s;
+}
+
+struct WClosure {
+    double th[4];    // converged (rho, u, v, T_native)
+    double jac[16];  // moment Jacobian at th, row-major (moment r, theta a)
+};
+
+enum { W_TRIAL = 0, W_DONE = 1, W_FAIL = 2 };
+
+// the next trial after an accepted evaluation (new_iter) or a rejected one
+__device__ __forceinline__ int w_newton_next(bool new_iter, const WClosure& C, const double res[4], double norm,
+                                             int iter, double step[4], double& alpha, double trial[4]) {
+    const double tol = 5.0e-13, floor_a = 9.5367431640625e-07;   // 2^-20
+    if (new_iter) {
+        if (norm <= tol) return W_DONE;
+        if (iter > 12) return W_FAIL;
+        const double mr[4] = {-res[0], -res[1], -res[2], -res[3]};
+        if (!s2_solve4(C.jac, mr, step)) return W_FAIL;
+        alpha = 1.0;
+    }
+    while (alpha >= floor_a) {
+        double nt[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) nt[m] = C.th[m] + alpha * step[m];
+        if (nt[0] > 0.0 && nt[3] > 0.0 && isfinite(nt[0]) && isfinite(nt[1]) && isfinite(nt[2]) && isfinite(nt[3])) {
+#pragma unroll
+            for (int m = 0; m < 4; ++m) trial[m] = nt[m];
+            return W_TRIAL;
+        }
+        alpha = 0.5 * alpha;
+    }
+    return W_FAIL;
+}
+
+// solve_q_first (mod_CorrectedWF2DClosure.f90:331-426) for the target moments w by one warp
+__device__ bool w_closure(const LoParams& P, const LoBuffers& B, const double w[4], WClosure& C) {
+    const int nv = P.nvel, ck = P.ck, nr = (nv + 31) >> 5;
+    double trial[4];
+    {   // primitive_from_conserved_2d (mod_CorrectedWF2DEquilibrium.f90:25-41)
+        if (!(isfinite(w[0]) && isfinite(w[1]) && isfinite(w[2]) && isfinite(w[3]) && w[0] > 0.0)) return false;
+        const double u = w[1] / w[0], v = w[2] / w[0];
+        const double kin = 0.5 * (u * u + v * v), ein = w[3] / w[0] - kin;
+        const double temp = 4.0 * ein / (double)(ck + 2);
+        if (!(isfinite(u) && isfinite(v) && isfinite(temp) && temp > 0.0)) return false;
+        trial[0] = w[0]; trial[1] = u; trial[2] = v; trial[3] = temp;
+    }
+    double res[4] = {0.0, 0.0, 0.0, 0.0}, step[4] = {0.0, 0.0, 0.0, 0.0}, alpha = 1.0, norm = 0.0;
+    int iter = 0;
+    bool first = true;
+    for (int guard = 0; guard < 1024; ++guard) {
+        // 16 Jacobian moments, the 4 moments of (qh, qb), flags: nonfinite, nonpositive
+        double acc[22];
+#pragma unroll
+        for (int m = 0; m < 22; ++m) acc[m] = 0.0;
+        for (int r = 0; r < nr; ++r) {
+            const WVel s = wvel(B, nv, r);
+            const S2Q q = s2_q(trial, ck, s.u, s.v);
+            const double e2 = s.u * s.u + s.v * s.v;
+#pragma unroll
+            for (int a = 0; a < 4; ++a) {
+                const double hk = q.qh * q.ld[a], bk = q.qb * q.ldb[a];
+                acc[0 * 4 + a] += s.w * hk;
+                acc[1 * 4 + a] += s.w * s.u * hk;
+                acc[2 * 4 + a] += s.w * s.v * hk;
+                acc[3 * 4 + a] += 0.5 * s.w * (e2 * hk + bk);
+            }
+            acc[16] += s.w * q.qh;
+            acc[17] += s.w * s.u * q.qh;
+            acc[18] += s.w * s.v * q.qh;
+            acc[19] += 0.5 * s.w * (e2 * q.qh + q.qb);
+            if (s.ok) {
+                acc[20] = fmax(acc[20], (isfinite(q.qh) && isfinite(q.qb)) ? 0.0 : 1.0);
+                acc[21] = fmax(acc[21], (q.qh > 0.0 && q.qb > 0.0) ? 0.0 : 1.0);
+            }
+        }
+        warp_sum_all<20>(acc);
+        warp_max_all<2>(acc + 20);
+        bool fin = acc[20] == 0.0;
+#pragma unroll
+        for (int m = 0; m < 20; ++m) fin = fin && isfinite(acc[m]);
+        double nres[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) nres[m] = acc[16 + m] - w[m];
+        int act;
+        const double nn = fin ? s2_scaled(nres, w) : INFINITY;
+        if (first ? fin : (fin && (nn < norm || nn <= 5.0e-13))) {   // accept the evaluation
+#pragma unroll
+            for (int m = 0; m < 4; ++m) { C.th[m] = trial[m]; res[m] = nres[m]; }
+#pragma unroll
+            for (int m = 0; m < 16; ++m) C.jac[m] = acc[m];
+            norm = nn;
+            iter = first ? 1 : iter + 1;
+            act = w_newton_next(true, C, res, norm, iter, step, alpha, trial);
+            if (act == W_DONE && acc[21] != 0.0) act = W_FAIL;
+        } else if (first) {
+            return false;
+        } else {
+            alpha = 0.5 * alpha;
+            act = w_newton_next(false, C, res, norm, iter, step, alpha, trial);
+        }
+        first = false;
+        if (act == W_DONE) return true;
+        if (act == W_FAIL) return false;
+    }
+    return false;
+}
+
+// make_mke_prepared (mod_S2D1.f90:111-151): the scalars that give, per velocity, the closure
+// Maxwellian M and the projected Shakhov directions K_x, K_y (w_mke_at)
+struct WMke {
+    double ux, vy, lam, coeff;   // primitive of w (theta_gas) and the Shakhov coefficient
+    double tdx[4], tdy[4];       // closure directions removed from the raw Shakhov terms
+};
+
+__device__ __forceinline__ void w_mke_raw(const WMke& M, const S2Q& q, int ck, double uk, double vk, double& kxh,
+                                          double& kxb, double& kyh, double& kyb) {
+    const double cx = uk - M.ux, cy = vk - M.vy, c2 = cx * cx + cy * cy;
+    const double shh = 2.0 * M.lam * c2 - 4.0, shb = shh + 2.0 / (double)ck;
+    kxh = M.coeff * cx * shh * q.qh; kxb = M.coeff * cx * shb * q.qb;
+    kyh = M.coeff * cy * shh * q.qh; kyb = M.coeff * cy * shb * q.qb;
+}
+
+// M, K_x, K_y of one velocity from the node scalars
+__device__ __forceinline__ void w_mke_at(const double th[4], const WMke& M, int ck, double uk, double vk, S2Q& q,
+                                         double& mh, double& mb, double& kxh, double& kxb, double& kyh, double& kyb) {
+    q = s2_q(th, ck, uk, vk);
+    mh = q.qh;
+    mb = q.qb;
+    w_mke_raw(M, q, ck, uk, vk, kxh, kxb, kyh, kyb);
+    double dh, db;
+    s2_dq(q, M.tdx, dh, db);
+    kxh = kxh - dh; kxb = kxb - db;
+    s2_dq(q, M.tdy, dh, db);
+    kyh = kyh - dh; kyb = kyb - db;
+}
+
+// Returns the gate (moments of M equal w, K_x, K_y moment-free, all finite, to 2e-12).
+__device__ bool w_make_mke(const LoParams& P, const LoBuffers& B, const double w[4], const WClosure& C, WMke& M) {
+    const int nv = P.nvel, ck = P.ck, nr = (nv + 31) >> 5;
+    double rho, th;
+    const bool pok = s2_primitive(w, ck, rho, M.ux, M.vy, th);
+    M.lam = 0.5 / th;
+    M.coeff = 0.8 * (1.0 - P.pr) * M.lam * M.lam / rho;
     double acc[16];
 #pragma unroll
     for (int m = 0; m < 8; ++m) acc[m] = 0.0;
-#pragma unroll
-    for (int r = 0; r < VPT; ++r) {
-        const Slot s = slot(r, nv);
-        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
-        const S2Q q = s2_q(thc, ck, uk, vk);
-        mh[r] = q.qh; mb[r] = q.qb;
-        const double cx = uk - ux, cy = vk - vy, c2 = cx * cx + cy * cy;
-        const double coeff = 0.8 * (1.0 - P.pr) * lam * lam / rho;
-        const double shh = 2.0 * lam * c2 - 4.0, shb = shh + 2.0 / (double)ck;
-        kxh[r] = coeff * cx * shh * mh[r]; kxb[r] = coeff * cx * shb * mb[r];
-        kyh[r] = coeff * cy * shh * mh[r]; kyb[r] = coeff * cy * shb * mb[r];
-        const double e2 = uk * uk + vk * vk;
-        acc[0] += wk * kxh[r]; acc[1] += wk * uk * kxh[r]; acc[2] += wk * vk * kxh[r]; acc[3] += 0.5 * wk * (e2 * kxh[r] + kxb[r]);
-        acc[4] += wk * kyh[r]; acc[5] += wk * uk * kyh[r]; acc[6] += wk * vk * kyh[r]; acc[7] += 0.5 * wk * (e2 * kyh[r] + kyb[r]);
+    for (int r = 0; r < nr; ++r) {
+        const WVel s = wvel(B, nv, r);
+        const S2Q q = s2_q(C.th, ck, s.u, s.v);
+        double kxh, kxb, kyh, kyb;
+        w_mke_raw(M, q, ck, s.u, s.v, kxh, kxb, kyh, kyb);
+        const double e2 = s.u * s.u + s.v * s.v;
+        acc[0] += s.w * kxh; acc[1] += s.w * s.u * kxh; acc[2] += s.w * s.v * kxh; acc[3] += 0.5 * s.w * (e2 * kxh + kxb);
+        acc[4] += s.w * kyh; acc[5] += s.w * s.u * kyh; acc[6] += s.w * s.v * kyh; acc[7] += 0.5 * s.w * (e2 * kyh + kyb);
     }
-    block_reduce_smem<8, 0>(acc, S.red, S.rout);
-    if (threadIdx.x == 0 || threadIdx.x == 32) {
-        const int d = threadIdx.x == 0 ? 0 : 1;
-        double m4[4], td[4];
+    warp_sum_all<8>(acc);
+    {
+        double td[4];
+        const bool okx = s2_solve4(C.jac, acc, td);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) m4[m] = S.rout[4 * d + m];
-        const bool ok = s2_solve4(S.jac, m4, td);
+        for (int m = 0; m < 4; ++m) M.tdx[m] = okx ? td[m] : NAN;
+        const bool oky = s2_solve4(C.jac, acc + 4, td);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) S.v[4 * d + m] = ok ? td[m] : NAN;
+        for (int m = 0; m < 4; ++m) M.tdy[m] = oky ? td[m] : NAN;
     }
-    __syncthreads();
-    double tdx[4], tdy[4];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) { tdx[m] = S.v[m]; tdy[m] = S.v[4 + m]; }
 #pragma unroll
     for (int m = 0; m < 16; ++m) acc[m] = 0.0;
-#pragma unroll
-    for (int r = 0; r < VPT; ++r) {
-        const Slot s = slot(r, nv);
-        const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
-        const S2Q q = s2_q(thc, ck, uk, vk);
-        double dh, db;
-        s2_dq(q, tdx, dh, db);
-        kxh[r] = kxh[r] - dh; kxb[r] = kxb[r] - db;
-        s2_dq(q, tdy, dh, db);
-        kyh[r] = kyh[r] - dh; kyb[r] = kyb[r] - db;
-        const double e2 = uk * uk + vk * vk, cx = uk - ux, cy = vk - vy, c2 = cx * cx + cy * cy;
-        acc[0] += wk * mh[r]; acc[1] += wk * uk * mh[r]; acc[2] += wk * vk * mh[r]; acc[3] += 0.5 * wk * (e2 * mh[r] + mb[r]);
-        acc[4] += wk * kxh[r]; acc[5] += wk * uk * kxh[r]; acc[6] += wk * vk * kxh[r]; acc[7] += 0.5 * wk * (e2 * kxh[r] + kxb[r]);
-        acc[8] += wk * kyh[r]; acc[9] += wk * uk * kyh[r]; acc[10] += wk * vk * kyh[r]; acc[11] += 0.5 * wk * (e2 * kyh[r] + kyb[r]);
-        acc[12] += 0.5 * wk * cx * (c2 * kxh[r] + kxb[r]);
-        acc[13] += 0.5 * wk * cy * (c2 * kxh[r] + kxb[r]);
-        acc[14] += 0.5 * wk * cx * (c2 * kyh[r] + kyb[r]);
-        acc[15] += 0.5 * wk * cy * (c2 * kyh[r] + kyb[r]);
+    for (int r = 0; r < nr; ++r) {
+        const WVel s = wvel(B, nv, r);
+        S2Q q;
+        double mh, mb, kxh, kxb, kyh, kyb;
+        w_mke_at(C.th, M, ck, s.u, s.v, q, mh, mb, kxh, kxb, kyh, kyb);
+        const double e2 = s.u * s.u + s.v * s.v, cx = s.u - M.ux, cy = s.v - M.vy, c2 = cx * cx + cy * cy;
+        acc[0] += s.w * mh; acc[1] += s.w * s.u * mh; acc[2] += s.w * s.v * mh; acc[3] += 0.5 * s.w * (e2 * mh + mb);
+        acc[4] += s.w * kxh; acc[5] += s.w * s.u * kxh; acc[6] += s.w * s.v * kxh; acc[7] += 0.5 * s.w * (e2 * kxh + kxb);
+        acc[8] += s.w * kyh; acc[9] += s.w * s.u * kyh; acc[10] += s.w * s.v * kyh; acc[11] += 0.5 * s.w * (e2 * kyh + kyb);
+        acc[12] += 0.5 * s.w * cx * (c2 * kxh + kxb);
+        acc[13] += 0.5 * s.w * cy * (c2 * kxh + kxb);
+        acc[14] += 0.5 * s.w * cx * (c2 * kyh + kyb);
+        acc[15] += 0.5 * s.w * cy * (c2 * kyh + kyb);
     }
-    block_reduce_smem<16, 0>(acc, S.red, S.rout);
-    const double* o = S.rout;
+    warp_sum_all<16>(acc);
     double res = 0.0, sc = 1.0;
 #pragma unroll
-    for (int m = 0; m < 4; ++m) { res = fmax(res, fabs(o[m] - w[m])); sc = fmax(sc, fabs(w[m])); }
+    for (int m = 0; m < 4; ++m) { res = fmax(res, fabs(acc[m] - w[m])); sc = fmax(sc, fabs(w[m])); }
     res = res / sc;
 #pragma unroll
-    for (int m = 4; m < 12; ++m) res = fmax(res, fabs(o[m]));
-    bool fin = isfinite(tdx[0]) && isfinite(tdy[0]);
+    for (int m = 4; m < 12; ++m) res = fmax(res, fabs(acc[m]));
+    bool fin = isfinite(M.tdx[0]) && isfinite(M.tdy[0]);
 #pragma unroll
-    for (int m = 12; m < 16; ++m) fin = fin && isfinite(o[m]);
+    for (int m = 12; m < 16; ++m) fin = fin && isfinite(acc[m]);
     return pok && fin && res <= 2.0e-12;
 }
 
-// ------------------------------------------------------------------------------------------
-// S2 cold start: one CTA per cell
-template <int VPT, int NT>
-__global__ void __launch_bounds__(NT) k_s2_init(LoParams P, LoBuffers B, S2Buffers SB) {
-    __shared__ S2Shared S;
-    const int nv = P.nvel, cc = blockIdx.x;
-    if (threadIdx.x < 4) S.w[threadIdx.x] = B.W[cc * 4 + threadIdx.x];
-    __syncthreads();
-    bool ok = s2_closure<VPT>(P, B, S);
-    if (ok) {
-        double mh[VPT], mb[VPT], kxh[VPT], kxb[VPT], kyh[VPT], kyb[VPT];
-        ok = s2_make_mke<VPT>(P, B, S, mh, mb, kxh, kxb, kyh, kyb);
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            const Slot s = slot(r, nv);
-            if (s.ok) { B.h[(size_t)cc * nv + s.k] = mh[r]; B.b[(size_t)cc * nv + s.k] = mb[r]; }
-        }
-    }
-    if (!ok && threadIdx.x == 0) set_status(B.status, ST_PROJECTION);
-}
+// node scalars of a volume target: th[4], tdx[4], tdy[4], ux, vy, lam, coeff
+constexpr int kS2TScal = 16;
 
-// build_targets: one CTA per cell, the 9 volume nodes in turn, accumulated in registers
-template <int VPT, int NT>
-__global__ void __launch_bounds__(NT) k_s2_targets(LoParams P, LoBuffers B, S2Buffers SB) {
-    if (eval_cached(B)) return;
-    __shared__ S2Shared S;
-    __shared__ double s_wq[9][4];
-    __shared__ int s_ok;
-    const int nv = P.nvel, nx = P.nx, ny = P.ny, cc = blockIdx.x, i = cc % nx, j = cc / nx;
-    if (threadIdx.x == 0) s_ok = 1;
-    __syncthreads();
-    if (threadIdx.x < 4) {   // s2d1_cell9 of the four macro fields
-        const int m = threadIdx.x;
-        const S2Field F{B.W + m, 4, nx, ny};
-        double nodes[3][3];
-        if (!s2_cell9(F, i, j, nodes)) s_ok = 0;
-        S.v[m * 9 + 0] = nodes[0][0];
+__device__ __forceinline__ void w_store_scalars(double* o, const WClosure& C, const WMke& M) {
 #pragma unroll
-        for (int a = 0; a < 3; ++a)
+    for (int m = 0; m < 4; ++m) { o[m] = C.th[m]; o[4 + m] = M.tdx[m]; o[8 + m] = M.tdy[m]; }
+    o[12] = M.ux; o[13] = M.vy; o[14] = M.lam; o[15] = M.coeff;
+}
+__device__ __forceinline__ void w_load_scalars(const double* o, double th[4], WMke& M) {
 #pragma unroll
-            for (int c = 0; c < 3; ++c) S.v[m * 9 + a * 3 + c] = nodes[a][c];
-    }
-    __syncthreads();
-    if (threadIdx.x < 4) {
-        const int m = threadIdx.x;
-        const double gw[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
-        double avg = 0.0;
-        for (int c = 0; c < 3; ++c)
-            for (int a = 0; a < 3; ++a) avg = avg + gw[a] * gw[c] * S.v[m * 9 + a * 3 + c];
-        for (int c = 0; c < 3; ++c)
-            for (int a = 0; a < 3; ++a) s_wq[c * 3 + a][m] = S.v[m * 9 + a * 3 + c] + B.W[cc * 4 + m] - avg;
-    }
-    __syncthreads();
-    double amh[VPT], amb[VPT], akxh[VPT], akxb[VPT], akyh[VPT], akyb[VPT];
-#pragma unroll
-    for (int r = 0; r < VPT; ++r) amh[r] = amb[r] = akxh[r] = akxb[r] = akyh[r] = akyb[r] = 0.0;
-    bool ok = s_ok != 0;
-    const double gw[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
-    for (int p = 0; p < 9 && ok; ++p) {
-        if (threadIdx.x < 4) S.w[threadIdx.x] = s_wq[p][threadIdx.x];
-        __syncthreads();
-        ok = s2_closure<VPT>(P, B, S);
-        if (!ok) break;
-        double mh[VPT], mb[VPT], kxh[VPT], kxb[VPT], kyh[VPT], kyb[VPT];
-        ok = s2_make_mke<VPT>(P, B, S, mh, mb, kxh, kxb, kyh, kyb);
-        const double wt2 = gw[p % 3] * gw[p / 3];
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            amh[r] = amh[r] + wt2 * mh[r]; amb[r] = amb[r] + wt2 * mb[r];
-            akxh[r] = akxh[r] + wt2 * kxh[r]; akxb[r] = akxb[r] + wt2 * kxb[r];
-            akyh[r] = akyh[r] + wt2 * kyh[r]; akyb[r] = akyb[r] + wt2 * kyb[r];
-        }
-        __syncthreads();
-    }
-#pragma unroll
-    for (int r = 0; r < VPT; ++r) {
-        const Slot s = slot(r, nv);
-        if (!s.ok) continue;
-        const size_t q = (size_t)cc * nv + s.k;
-        SB.mh[q] = amh[r]; SB.mb[q] = amb[r]; SB.kxh[q] = akxh[r]; SB.kxb[q] = akxb[r]; SB.kyh[q] = akyh[r]; SB.kyb[q] = akyb[r];
-    }
-    if (!ok && threadIdx.x == 0) set_status(B.status, ST_PROJECTION);
+    for (int m = 0; m < 4; ++m) { th[m] = o[m]; M.tdx[m] = o[4 + m]; M.tdy[m] = o[8 + m]; }
+    M.ux = o[12]; M.vy = o[13]; M.lam = o[14]; M.coeff = o[15];
 }
 
 // ------------------------------------------------------------------------------------------
-// interior faces: one CTA per face (the right x face of every cell, then the top y face of every
-// cell below the last row), the 3 Gauss nodes of ugks_node in turn
-template <int VPT, int NT>
-__global__ void __launch_bounds__(NT) k_s2_faces(LoParams P, LoBuffers B, S2Buffers SB) {
+// S2 cold start: one warp per cell, h, b := the discrete closure Maxwellian of W
+__global__ void __launch_bounds__(256, 2) k_s2_init(LoParams P, LoBuffers B, S2Buffers SB) {
+    const int nv = P.nvel, nc = P.nx * P.ny, lane = threadIdx.x & 31, nr = (nv + 31) >> 5;
+    const int cc = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (cc >= nc) return;
+    double w[4];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) w[m] = B.W[cc * 4 + m];
+    WClosure C;
+    WMke M;
+    const bool ok = w_closure(P, B, w, C) && w_make_mke(P, B, w, C, M);
+    if (ok)
+        for (int r = 0; r < nr; ++r) {
+            const WVel s = wvel(B, nv, r);
+            const S2Q q = s2_q(C.th, P.ck, s.u, s.v);
+            if (s.ok) { B.h[(size_t)cc * nv + s.k] = q.qh; B.b[(size_t)cc * nv + s.k] = q.qb; }
+        }
+    if (!ok && lane == 0) set_status(B.status, ST_PROJECTION);
+}
+
+// ------------------------------------------------------------------------------------------
+// macro WENO of W: per interior face and component the normal slopes of both sides and the
+// tangential slope at the 3 Gauss nodes (s2d1_face3, compute_flux :803-808,849-854), and per cell
+// and component the 3x3 Gauss values and the mean-shifted volume node states (build_targets
+// :1270-1279).  One thread per (face, component) and per (cell, component).
+__global__ void __launch_bounds__(128) k_s2_macro(LoParams P, LoBuffers B, S2Buffers SB, int faces, int cells) {
     if (eval_cached(B)) return;
-    __shared__ S2Shared S;
-    __shared__ double s_mac[3][4][3];   // [nl, nr, t][component][node]
-    __shared__ int s_ok;
-    const int nv = P.nvel, nx = P.nx, ny = P.ny;
-    int f = blockIdx.x;
-    const int axis = f < nx * ny ? 0 : 1;
-    if (axis == 1) f -= nx * ny;
-    const int cl = f, i = cl % nx, j = cl / nx;
-    const int cr = axis == 0 ? j * nx + (i + 1) % nx : (j + 1) * nx + i;
-    const double dt = B.dt[0];
-    if (threadIdx.x == 0) s_ok = 1;
-    __syncthreads();
-    if (threadIdx.x < 4) {   // s2d1_face3 of W component m (the macro normal/tangential slopes)
-        const int m = threadIdx.x;
+    const int nx = P.nx, ny = P.ny, nfx = nx * ny, nf = nfx + nx * (ny - 1), nc = nx * ny;
+    int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    const int nft = faces ? nf * 4 : 0;
+    if (t < nft) {
+        int f = t >> 2;
+        const int m = t & 3, fi = f, axis = f < nfx ? 0 : 1;
+        if (axis == 1) f -= nfx;
+        const int i = f % nx, j = f / nx;
         const S2Field F{B.W + m, 4, nx, ny};
         double vl[3], vr[3], nl[3], nr[3], tl[3], tr[3];
         bool ok;
         if (axis == 0) ok = s2_side3(F, 0, i, j, 0.5, vl, nl, tl) && s2_side3(F, 0, (i + 1) % nx, j, -0.5, vr, nr, tr);
         else ok = s2_side3(F, 1, j, i, 0.5, vl, nl, tl) && s2_side3(F, 1, j + 1, i, -0.5, vr, nr, tr);
-        if (!ok) s_ok = 0;
+        if (!ok) set_status(B.status, ST_NONFINITE_FLUX);
         const double dn = axis == 0 ? P.dx : P.dy, dtg = axis == 0 ? P.dy : P.dx;
 #pragma unroll
         for (int g = 0; g < 3; ++g) {
-            s_mac[0][m][g] = nl[g] / dn;
-            s_mac[1][m][g] = nr[g] / dn;
-            s_mac[2][m][g] = 0.5 * (tl[g] + tr[g]) / dtg;
+            double* o = SB.mac + (size_t)(fi * 3 + g) * 12;
+            o[m] = nl[g] / dn;
+            o[4 + m] = nr[g] / dn;
+            o[8 + m] = 0.5 * (tl[g] + tr[g]) / dtg;
         }
-    }
-    __syncthreads();
-    bool ok = s_ok != 0;
-    const int sl = axis == 0 ? 1 : 3, sr = axis == 0 ? 0 : 2;
-    const double gw[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
-    double afh[VPT], afb[VPT], afw[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int r = 0; r < VPT; ++r) afh[r] = afb[r] = 0.0;
-    for (int g = 0; g < 3 && ok; ++g) {
-        // inputs of this node: upwind face values and micro derivatives
-        double f0h[VPT], f0b[VPT], nh[VPT], nb[VPT], th_[VPT], tb_[VPT], acc[22];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) acc[m] = 0.0;
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            const Slot s = slot(r, nv);
-            const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
-            const double vn = axis == 0 ? uk : vk;
-            const bool left = vn >= 0.0;
-            const double* rc = SB.rec + (size_t)(left ? cl : cr) * 72 * nv + s.kk;
-            const int side = left ? sl : sr;
-            f0h[r] = rc[(size_t)(0 * 12 + side * 3 + g) * nv];
-            f0b[r] = rc[(size_t)(1 * 12 + side * 3 + g) * nv];
-            nh[r] = rc[(size_t)(2 * 12 + side * 3 + g) * nv];
-            th_[r] = rc[(size_t)(3 * 12 + side * 3 + g) * nv];
-            nb[r] = rc[(size_t)(4 * 12 + side * 3 + g) * nv];
-            tb_[r] = rc[(size_t)(5 * 12 + side * 3 + g) * nv];
-            const double e2 = uk * uk + vk * vk;
-            acc[0] += wk * f0h[r]; acc[1] += wk * uk * f0h[r]; acc[2] += wk * vk * f0h[r]; acc[3] += 0.5 * wk * (e2 * f0h[r] + f0b[r]);
-        }
-        block_reduce_smem<4, 0>(acc, S.red, S.rout);
-        if (threadIdx.x < 4) S.w[threadIdx.x] = S.rout[threadIdx.x];
-        __syncthreads();
-        double w0[4] = {S.w[0], S.w[1], S.w[2], S.w[3]};
-        ok = s2_closure<VPT>(P, B, S);
-        if (!ok) break;
-        double mh[VPT], mb[VPT], kxh[VPT], kxb[VPT], kyh[VPT], kyb[VPT];
-        ok = s2_make_mke<VPT>(P, B, S, mh, mb, kxh, kxb, kyh, kyb);
-        if (!ok) break;
-        // q0 = heat(w0, f0 - analytic Maxwellian)
-        double rho, ux, vy, thg;
-        s2_primitive(w0, P.ck, rho, ux, vy, thg);
-        double nrho = w0[0], nu = w0[1] / w0[0], nvv = w0[2] / w0[0];
-        const double temp = 4.0 * (w0[3] / w0[0] - 0.5 * (nu * nu + nvv * nvv)) / (double)(P.ck + 2);
-        const double lamn = 1.0 / temp;
-        acc[0] = acc[1] = 0.0;
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            const Slot s = slot(r, nv);
-            const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
-            const double du = uk - nu, dv = vk - nvv;
-            const double eah = nrho * lamn / kPi * exp(-lamn * (du * du + dv * dv));
-            const double eab = 0.5 * (double)P.ck * temp * eah;
-            const double cx = uk - ux, cy = vk - vy, c2 = cx * cx + cy * cy;
-            const double dh = f0h[r] - eah, db = f0b[r] - eab;
-            acc[0] += 0.5 * wk * cx * (c2 * dh + db);
-            acc[1] += 0.5 * wk * cy * (c2 * dh + db);
-        }
-        block_reduce_smem<2, 0>(acc, S.red, S.rout);
-        const double q0x = S.rout[0], q0y = S.rout[1];
-        double s0h[VPT], s0b[VPT];
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            s0h[r] = mh[r] + kxh[r] * q0x + kyh[r] * q0y;
-            s0b[r] = mb[r] + kxb[r] * q0x + kyb[r] * q0y;
-        }
-        // directions of the macro normal slopes (left, right) and the tangential slope
-        if (threadIdx.x == 0 || threadIdx.x == 32 || threadIdx.x == 64) {
-            const int d = threadIdx.x / 32;
-            double m4[4], td[4];
-#pragma unroll
-            for (int m = 0; m < 4; ++m) m4[m] = s_mac[d][m][g];
-            const bool sok = s2_solve4(S.jac, m4, td);
-#pragma unroll
-            for (int m = 0; m < 4; ++m) S.v[8 + 4 * d + m] = sok ? td[m] : NAN;
-        }
-        __syncthreads();
-        double thc[4], tdl[4], tdr[4], tdt[4];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) { thc[m] = S.th[m]; tdl[m] = S.v[8 + m]; tdr[m] = S.v[12 + m]; tdt[m] = S.v[16 + m]; }
-        double dlh[VPT], dlb[VPT], drh[VPT], drb[VPT], dth[VPT], dtb[VPT];
-#pragma unroll
-        for (int m = 0; m < 16; ++m) acc[m] = 0.0;
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            const Slot s = slot(r, nv);
-            const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
-            const S2Q q = s2_q(thc, P.ck, uk, vk);
-            s2_dq(q, tdl, dlh[r], dlb[r]);
-            s2_dq(q, tdr, drh[r], drb[r]);
-            s2_dq(q, tdt, dth[r], dtb[r]);
-            const double e2 = uk * uk + vk * vk;
-            acc[0] += wk * dlh[r]; acc[1] += wk * uk * dlh[r]; acc[2] += wk * vk * dlh[r]; acc[3] += 0.5 * wk * (e2 * dlh[r] + dlb[r]);
-            acc[4] += wk * drh[r]; acc[5] += wk * uk * drh[r]; acc[6] += wk * vk * drh[r]; acc[7] += 0.5 * wk * (e2 * drh[r] + drb[r]);
-            acc[8] += wk * dth[r]; acc[9] += wk * uk * dth[r]; acc[10] += wk * vk * dth[r]; acc[11] += 0.5 * wk * (e2 * dth[r] + dtb[r]);
-            const double vn = axis == 0 ? uk : vk, vt = axis == 0 ? vk : uk;
-            const double fh = vn * (vn >= 0.0 ? dlh[r] : drh[r]) + vt * dth[r];
-            const double fb = vn * (vn >= 0.0 ? dlb[r] : drb[r]) + vt * dtb[r];
-            acc[12] += wk * fh; acc[13] += wk * uk * fh; acc[14] += wk * vk * fh; acc[15] += 0.5 * wk * (e2 * fh + fb);
-        }
-        block_reduce_smem<16, 0>(acc, S.red, S.rout);
-        if (threadIdx.x == 0) {   // gates of the three directions; the time direction and Mt
-            bool gok = true;
-            for (int d = 0; d < 3; ++d) {
-                double mx = 0.0, sc = 1.0;
-                for (int m = 0; m < 4; ++m) {
-                    mx = fmax(mx, fabs(S.rout[4 * d + m] - s_mac[d][m][g]));
-                    sc = fmax(sc, fabs(s_mac[d][m][g]));
-                }
-                gok = gok && mx / sc <= 2.0e-12;
-            }
-            double wt[4], td[4];
-            for (int m = 0; m < 4; ++m) wt[m] = -S.rout[12 + m];
-            gok = gok && s2_solve4(S.jac, wt, td);
-            for (int m = 0; m < 4; ++m) { S.v[20 + m] = td[m]; S.v[24 + m] = wt[m]; }
-            double tau = 0.0;
-            gok = gok && s2_tau(P, w0, tau);
-            const double ex = exp(-dt / tau);
-            double mt[5];
-            mt[3] = tau * (1.0 - ex);
-            mt[4] = -tau * dt * ex + tau * mt[3];
-            mt[0] = dt - mt[3];
-            mt[1] = -tau * mt[0] + mt[4];
-            mt[2] = 0.5 * dt * dt - tau * mt[0];
-            for (int m = 0; m < 5; ++m) S.v[28 + m] = mt[m];
-            S.v[33] = gok ? 1.0 : 0.0;
-        }
-        __syncthreads();
-        if (S.v[33] == 0.0) { ok = false; break; }
-        double tdm[4], mt[5];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) tdm[m] = S.v[20 + m];
-#pragma unroll
-        for (int m = 0; m < 5; ++m) mt[m] = S.v[28 + m];
-#pragma unroll
-        for (int m = 0; m < 8; ++m) acc[m] = 0.0;
-        double fhv[VPT], fbv[VPT];
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            const Slot s = slot(r, nv);
-            const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
-            const S2Q q = s2_q(thc, P.ck, uk, vk);
-            double mth, mtb;
-            s2_dq(q, tdm, mth, mtb);
-            const double e2 = uk * uk + vk * vk;
-            acc[0] += wk * mth; acc[1] += wk * uk * mth; acc[2] += wk * vk * mth; acc[3] += 0.5 * wk * (e2 * mth + mtb);
-            const double vn = axis == 0 ? uk : vk, vt = axis == 0 ? vk : uk;
-            const double sh = vn * (vn >= 0.0 ? dlh[r] : drh[r]) + vt * dth[r];
-            const double sb = vn * (vn >= 0.0 ? dlb[r] : drb[r]) + vt * dtb[r];
-            fhv[r] = vn * (mt[0] * s0h[r] + mt[1] * sh + mt[2] * mth + mt[3] * f0h[r] - mt[4] * (vn * nh[r] + vt * th_[r]));
-            fbv[r] = vn * (mt[0] * s0b[r] + mt[1] * sb + mt[2] * mtb + mt[3] * f0b[r] - mt[4] * (vn * nb[r] + vt * tb_[r]));
-            acc[4] += wk * fhv[r]; acc[5] += wk * uk * fhv[r]; acc[6] += wk * vk * fhv[r]; acc[7] += 0.5 * wk * (e2 * fhv[r] + fbv[r]);
-            afh[r] = afh[r] + gw[g] * fhv[r];
-            afb[r] = afb[r] + gw[g] * fbv[r];
-            if (s.ok) ok = ok && isfinite(fhv[r]) && isfinite(fbv[r]);
-        }
-        block_reduce_smem<8, 0>(acc, S.red, S.rout);
-        {
-            double mx = 0.0, sc = 1.0;
-#pragma unroll
-            for (int m = 0; m < 4; ++m) { mx = fmax(mx, fabs(S.rout[m] - S.v[24 + m])); sc = fmax(sc, fabs(S.v[24 + m])); }
-            ok = ok && mx / sc <= 2.0e-12;
-        }
-#pragma unroll
-        for (int m = 0; m < 4; ++m) afw[m] = afw[m] + gw[g] * S.rout[4 + m];
-        ok = __syncthreads_and(ok) != 0;   // uniform before the loop test
-    }
-    if (!__syncthreads_and(ok)) {
-        if (threadIdx.x == 0) set_status(B.status, ST_NONFINITE_FLUX);
         return;
     }
-    // publish times the face length into the face arrays ComputeResidual reads
-    const double len = axis == 0 ? P.dy : P.dx;
-    size_t o;
-    double *Fh, *Fb, *Fw;
-    if (axis == 0) { o = (size_t)j * nx + (i + 1) % nx; Fh = B.fxh; Fb = B.fxb; Fw = B.fxw; }
-    else { o = (size_t)(j + 1) * nx + i; Fh = B.fyh; Fb = B.fyb; Fw = B.fyw; }
+    t -= nft;
+    if (!cells || t >= nc * 4) return;
+    const int cc = t >> 2, m = t & 3, i = cc % nx, j = cc / nx;
+    const S2Field F{B.W + m, 4, nx, ny};
+    double nodes[3][3];
+    if (!s2_cell9(F, i, j, nodes)) set_status(B.status, ST_PROJECTION);
+    const double gw[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
+    double avg = 0.0;
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a) avg = avg + gw[a] * gw[c] * nodes[a][c];
+    const double wc = B.W[cc * 4 + m];
+    for (int c = 0; c < 3; ++c)
+        for (int a = 0; a < 3; ++a) SB.wq[((size_t)cc * 9 + c * 3 + a) * 4 + m] = nodes[a][c] + wc - avg;
+}
+
+// build_targets, closure part: one warp per (cell, volume node) -> the node scalars
+__global__ void __launch_bounds__(256, 2) k_s2_target_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
+    if (eval_cached(B)) return;
+    const int nc = P.nx * P.ny, lane = threadIdx.x & 31;
+    const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (wid >= nc * 9) return;
+    double w[4];
 #pragma unroll
-    for (int r = 0; r < VPT; ++r) {
-        const Slot s = slot(r, nv);
-        if (s.ok) { Fh[o * nv + s.k] = afh[r] * len; Fb[o * nv + s.k] = afb[r] * len; }
+    for (int m = 0; m < 4; ++m) w[m] = SB.wq[(size_t)wid * 4 + m];
+    WClosure C;
+    WMke M;
+    const bool ok = w_closure(P, B, w, C) && w_make_mke(P, B, w, C, M);
+    if (lane == 0) {
+        if (ok) w_store_scalars(SB.tscal + (size_t)wid * kS2TScal, C, M);
+        else set_status(B.status, ST_PROJECTION);
     }
-    if (threadIdx.x == 0)
-        for (int m = 0; m < 4; ++m) Fw[o * 4 + m] = afw[m] * len;
+}
+
+// build_targets, sum part: per (cell, velocity) the Gauss-weighted M, K_x, K_y of the 9 nodes
+__global__ void __launch_bounds__(256) k_s2_target_sum(LoParams P, LoBuffers B, S2Buffers SB) {
+    if (eval_cached(B)) return;
+    const int nv = P.nvel, cc = blockIdx.y;
+    const int k = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (k >= nv) return;
+    const double uk = B.u[k], vk = B.v[k];
+    const double gw[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
+    double amh = 0.0, amb = 0.0, akxh = 0.0, akxb = 0.0, akyh = 0.0, akyb = 0.0;
+    for (int p = 0; p < 9; ++p) {
+        double th[4];
+        WMke M;
+        w_load_scalars(SB.tscal + ((size_t)cc * 9 + p) * kS2TScal, th, M);
+        S2Q q;
+        double mh, mb, kxh, kxb, kyh, kyb;
+        w_mke_at(th, M, P.ck, uk, vk, q, mh, mb, kxh, kxb, kyh, kyb);
+        const double wt2 = gw[p % 3] * gw[p / 3];
+        amh = amh + wt2 * mh; amb = amb + wt2 * mb;
+        akxh = akxh + wt2 * kxh; akxb = akxb + wt2 * kxb;
+        akyh = akyh + wt2 * kyh; akyb = akyb + wt2 * kyb;
+    }
+    const size_t q = (size_t)cc * nv + k;
+    SB.mh[q] = amh; SB.mb[q] = amb; SB.kxh[q] = akxh; SB.kxb[q] = akxb; SB.kyh[q] = akyh; SB.kyb[q] = akyb;
+}
+
+// ------------------------------------------------------------------------------------------
+// interior face nodes (ugks_node, mod_S2D1.f90:421-521): one warp per (face, Gauss node); the
+// right x face of every cell, then the top y face of every cell below the last row.  The node's
+// micro flux goes to SB.node[face][node][h|b][nvel] and its macro flux to SB.nodew.
+__global__ void __launch_bounds__(256, 2) k_s2_face_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
+    if (eval_cached(B)) return;
+    const int nv = P.nvel, nx = P.nx, ny = P.ny, ck = P.ck, lane = threadIdx.x & 31, nr = (nv + 31) >> 5;
+    const int nfx = nx * ny, nf = nfx + nx * (ny - 1);
+    const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (wid >= nf * 3) return;
+    const int fi = wid / 3, g = wid % 3;
+    const int axis = fi < nfx ? 0 : 1, f = axis == 0 ? fi : fi - nfx;
+    const int cl = f, i = cl % nx, j = cl / nx;
+    const int cr = axis == 0 ? j * nx + (i + 1) % nx : (j + 1) * nx + i;
+    const int sl = axis == 0 ? 1 : 3, sr = axis == 0 ? 0 : 2;
+    const double dt = B.dt[0];
+    const double* mac = SB.mac + (size_t)wid * 12;   // [nl | nr | t][component] of this node
+    auto upwind = [&](const WVel& s, int field) {
+        const double vn = axis == 0 ? s.u : s.v;
+        const bool left = vn >= 0.0;
+        return SB.rec[((size_t)(left ? cl : cr) * 72 + field * 12 + (left ? sl : sr) * 3 + g) * nv + s.k];
+    };
+    // W0: moments of the upwind face values
+    double acc[16];
+#pragma unroll
+    for (int m = 0; m < 4; ++m) acc[m] = 0.0;
+    for (int r = 0; r < nr; ++r) {
+        const WVel s = wvel(B, nv, r);
+        moment_add(s.w, s.u, s.v, upwind(s, 0), upwind(s, 1), acc);
+    }
+    warp_sum_all<4>(acc);
+    const double w0[4] = {acc[0], acc[1], acc[2], acc[3]};
+    WClosure C;
+    WMke M;
+    bool ok = w_closure(P, B, w0, C) && w_make_mke(P, B, w0, C, M);
+    double q0x = 0.0, q0y = 0.0, tdl[4], tdr[4], tdt[4], tdm[4], wt[4], mt[5];
+    if (ok) {   // q0 = heat(w0, f0 - analytic Maxwellian of w0)
+        const double nrho = w0[0], nu = w0[1] / w0[0], nvv = w0[2] / w0[0];
+        const double temp = 4.0 * (w0[3] / w0[0] - 0.5 * (nu * nu + nvv * nvv)) / (double)(ck + 2);
+        const double lamn = 1.0 / temp;
+        acc[0] = acc[1] = 0.0;
+        for (int r = 0; r < nr; ++r) {
+            const WVel s = wvel(B, nv, r);
+            const double du = s.u - nu, dv = s.v - nvv;
+            const double eah = nrho * lamn / kPi * exp(-lamn * (du * du + dv * dv));
+            const double eab = 0.5 * (double)ck * temp * eah;
+            const double cx = s.u - M.ux, cy = s.v - M.vy, c2 = cx * cx + cy * cy;
+            const double dh = upwind(s, 0) - eah, db = upwind(s, 1) - eab;
+            acc[0] += 0.5 * s.w * cx * (c2 * dh + db);
+            acc[1] += 0.5 * s.w * cy * (c2 * dh + db);
+        }
+        warp_sum_all<2>(acc);
+        q0x = acc[0];
+        q0y = acc[1];
+        // directions of the macro normal slopes (left, right) and the tangential slope
+        const bool okd = s2_solve4(C.jac, mac, tdl) & s2_solve4(C.jac, mac + 4, tdr) & s2_solve4(C.jac, mac + 8, tdt);
+        if (!okd)
+#pragma unroll
+            for (int m = 0; m < 4; ++m) tdl[m] = tdr[m] = tdt[m] = NAN;
+#pragma unroll
+        for (int m = 0; m < 16; ++m) acc[m] = 0.0;
+        for (int r = 0; r < nr; ++r) {
+            const WVel s = wvel(B, nv, r);
+            const S2Q q = s2_q(C.th, ck, s.u, s.v);
+            double dlh, dlb, drh, drb, dth, dtb;
+            s2_dq(q, tdl, dlh, dlb);
+            s2_dq(q, tdr, drh, drb);
+            s2_dq(q, tdt, dth, dtb);
+            moment_add(s.w, s.u, s.v, dlh, dlb, acc);
+            moment_add(s.w, s.u, s.v, drh, drb, acc + 4);
+            moment_add(s.w, s.u, s.v, dth, dtb, acc + 8);
+            const double vn = axis == 0 ? s.u : s.v, vt = axis == 0 ? s.v : s.u;
+            const double fh = vn * (vn >= 0.0 ? dlh : drh) + vt * dth;
+            const double fb = vn * (vn >= 0.0 ? dlb : drb) + vt * dtb;
+            moment_add(s.w, s.u, s.v, fh, fb, acc + 12);
+        }
+        warp_sum_all<16>(acc);
+        for (int d = 0; d < 3; ++d) {   // gates of the three directions
+            double mx = 0.0, sc = 1.0;
+            for (int m = 0; m < 4; ++m) {
+                mx = fmax(mx, fabs(acc[4 * d + m] - mac[4 * d + m]));
+                sc = fmax(sc, fabs(mac[4 * d + m]));
+            }
+            ok = ok && mx / sc <= 2.0e-12;
+        }
+        // the time direction and the time coefficients Mt (mod_Evolution.f90:346-350)
+#pragma unroll
+        for (int m = 0; m < 4; ++m) wt[m] = -acc[12 + m];
+        ok = ok && s2_solve4(C.jac, wt, tdm);
+        double tau = 0.0;
+        ok = ok && s2_tau(P, w0, tau);
+        const double ex = exp(-dt / tau);
+        mt[3] = tau * (1.0 - ex);
+        mt[4] = -tau * dt * ex + tau * mt[3];
+        mt[0] = dt - mt[3];
+        mt[1] = -tau * mt[0] + mt[4];
+        mt[2] = 0.5 * dt * dt - tau * mt[0];
+    }
+    if (ok) {   // node fluxes
+        double* outh = SB.node + (size_t)wid * 2 * nv;
+        double* outb = outh + nv;
+#pragma unroll
+        for (int m = 0; m < 8; ++m) acc[m] = 0.0;
+        for (int r = 0; r < nr; ++r) {
+            const WVel s = wvel(B, nv, r);
+            S2Q q;
+            double mh, mb, kxh, kxb, kyh, kyb;
+            w_mke_at(C.th, M, ck, s.u, s.v, q, mh, mb, kxh, kxb, kyh, kyb);
+            const double s0h = mh + kxh * q0x + kyh * q0y;
+            const double s0b = mb + kxb * q0x + kyb * q0y;
+            double dlh, dlb, drh, drb, dth, dtb, mth, mtb;
+            s2_dq(q, tdl, dlh, dlb);
+            s2_dq(q, tdr, drh, drb);
+            s2_dq(q, tdt, dth, dtb);
+            s2_dq(q, tdm, mth, mtb);
+            moment_add(s.w, s.u, s.v, mth, mtb, acc);
+            const double vn = axis == 0 ? s.u : s.v, vt = axis == 0 ? s.v : s.u;
+            const double sh = vn * (vn >= 0.0 ? dlh : drh) + vt * dth;
+            const double sb = vn * (vn >= 0.0 ? dlb : drb) + vt * dtb;
+            const double f0h = upwind(s, 0), f0b = upwind(s, 1), nh = upwind(s, 2), th_ = upwind(s, 3);
+            const double nb = upwind(s, 4), tb_ = upwind(s, 5);
+            const double fhv = vn * (mt[0] * s0h + mt[1] * sh + mt[2] * mth + mt[3] * f0h - mt[4] * (vn * nh + vt * th_));
+            const double fbv = vn * (mt[0] * s0b + mt[1] * sb + mt[2] * mtb + mt[3] * f0b - mt[4] * (vn * nb + vt * tb_));
+            moment_add(s.w, s.u, s.v, fhv, fbv, acc + 4);
+            if (s.ok) {
+                outh[s.k] = fhv;
+                outb[s.k] = fbv;
+                ok = ok && isfinite(fhv) && isfinite(fbv);
+            }
+        }
+        warp_sum_all<8>(acc);
+        double mx = 0.0, sc = 1.0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { mx = fmax(mx, fabs(acc[m] - wt[m])); sc = fmax(sc, fabs(wt[m])); }
+        ok = ok && mx / sc <= 2.0e-12;
+        if (lane < 4) SB.nodew[(size_t)wid * 4 + lane] = lane == 0 ? acc[4] : (lane == 1 ? acc[5] : (lane == 2 ? acc[6] : acc[7]));
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    if (!ok && lane == 0) set_status(B.status, ST_NONFINITE_FLUX);
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1048,15 +1114,20 @@ __device__ void s2w_time_coeffs(double dt, double tau, double mt[5]) {
     }
 }
 
-// wall faces: one CTA per wall face (bottom faces of row 0, then top faces of row ny-1), the 3
-// Gauss nodes of s2w2_wall_node in turn
-template <int VPT, int NT>
-__global__ void __launch_bounds__(NT) k_s2_walls(LoParams P, LoBuffers B, S2Buffers SB) {
+
+// wall face nodes (s2w2_wall_node, mod_S2MultiscaleWall.f90:45-184): one warp per (wall face,
+// Gauss node); bottom faces of row 0, then top faces of row ny-1.  Node fluxes go to the node
+// buffers after the interior faces.
+__global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
     if (eval_cached(B)) return;
-    __shared__ S2Shared S;
-    const int nv = P.nvel, nx = P.nx, ny = P.ny, ck = P.ck;
-    const int top = blockIdx.x >= nx ? 1 : 0, i = blockIdx.x - top * nx;
+    const int nv = P.nvel, nx = P.nx, ny = P.ny, ck = P.ck, lane = threadIdx.x & 31, nr = (nv + 31) >> 5;
+    const int nf = nx * ny + nx * (ny - 1);
+    const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    if (wid >= 2 * nx * 3) return;
+    const int wf = wid / 3, g = wid % 3;
+    const int top = wf >= nx ? 1 : 0, i = wf - top * nx;
     const int cc = top ? (ny - 1) * nx + i : i, sidx = top ? 3 : 2;
+    const size_t node = (size_t)(nf + wf) * 3 + g;
     const double side = top ? 1.0 : -1.0;
     const double ux = P.wall_ux[top], theta = 0.5 / P.wall_lam[top];
     const double dt = B.dt[0];
@@ -1066,143 +1137,158 @@ __global__ void __launch_bounds__(NT) k_s2_walls(LoParams P, LoBuffers B, S2Buff
     const double prim_g[4] = {pp / theta, 0.0, -ux, lambda};
     const double wc[4] = {wcell[0], wcell[2], -wcell[1], wcell[3]};
     const double wg[4] = {prim_g[0], 0.0, -prim_g[0] * ux, prim_g[0] * ((double)(ck + 2) / (4.0 * lambda) + 0.5 * ux * ux)};
-    // wall_equilibrium: the discrete closure of the wall state (the same for the 3 nodes)
-    if (threadIdx.x == 0) {
-        S.w[0] = prim_g[0]; S.w[1] = prim_g[0] * ux; S.w[2] = 0.0;
-        S.w[3] = prim_g[0] * ((double)(ck + 2) * theta / 2.0 + ux * ux / 2.0);
-    }
-    __syncthreads();
-    bool ok = pp > 0.0 && isfinite(pp) && s2_closure<VPT>(P, B, S);
-    const double gw[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
-    double afh[VPT], afb[VPT], afw[4] = {0.0, 0.0, 0.0, 0.0};
-#pragma unroll
-    for (int r = 0; r < VPT; ++r) afh[r] = afb[r] = 0.0;
-    double thc[4];
-#pragma unroll
-    for (int m = 0; m < 4; ++m) thc[m] = S.th[m];
-    for (int g = 0; g < 3 && ok; ++g) {
-        double hin[VPT], bin[VPT], hn[VPT], bn[VPT], ht[VPT], bt[VPT], acc[8];
+    // wall_equilibrium: the discrete closure of the wall state
+    const double wwall[4] = {prim_g[0], prim_g[0] * ux, 0.0, prim_g[0] * ((double)(ck + 2) * theta / 2.0 + ux * ux / 2.0)};
+    WClosure C;
+    bool ok = pp > 0.0 && isfinite(pp) && w_closure(P, B, wwall, C);
+    auto rec = [&](const WVel& s, int field) {
+        return SB.rec[((size_t)cc * 72 + field * 12 + sidx * 3 + g) * nv + s.k];
+    };
+    double acc[8];
+    double an[4], at[4], atime[4], mt[5], mxi2 = 0.0, coeff = 0.0, hlx = 0.0, hly = 0.0;
+    if (ok) {
 #pragma unroll
         for (int m = 0; m < 6; ++m) acc[m] = 0.0;
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            const Slot s = slot(r, nv);
-            const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
-            const double* rc = SB.rec + (size_t)cc * 72 * nv + s.kk;
-            hin[r] = rc[(size_t)(0 * 12 + sidx * 3 + g) * nv];
-            bin[r] = rc[(size_t)(1 * 12 + sidx * 3 + g) * nv];
-            hn[r] = rc[(size_t)(2 * 12 + sidx * 3 + g) * nv];
-            ht[r] = rc[(size_t)(3 * 12 + sidx * 3 + g) * nv];
-            bn[r] = rc[(size_t)(4 * 12 + sidx * 3 + g) * nv];
-            bt[r] = rc[(size_t)(5 * 12 + sidx * 3 + g) * nv];
-            const double vn = vk, vt = -uk, v2 = vn * vn + vt * vt;
-            acc[0] += wk * (-ht[r]);
-            acc[1] += wk * (-(vn * ht[r]));
-            acc[2] += wk * (-(vt * ht[r]));
-            acc[3] += wk * (-(0.5 * (v2 * ht[r] + bt[r])));
-            const double vt2 = -uk + ux, w2 = vn * vn + vt2 * vt2;
-            acc[4] += 0.5 * wk * vn * (w2 * hin[r] + bin[r]);
-            acc[5] += 0.5 * wk * vt2 * (w2 * hin[r] + bin[r]);
+        for (int r = 0; r < nr; ++r) {
+            const WVel s = wvel(B, nv, r);
+            const double hin = rec(s, 0), bin = rec(s, 1), ht = rec(s, 3), bt = rec(s, 5);
+            const double vn = s.v, vt = -s.u, v2 = vn * vn + vt * vt;
+            acc[0] += s.w * (-ht);
+            acc[1] += s.w * (-(vn * ht));
+            acc[2] += s.w * (-(vt * ht));
+            acc[3] += s.w * (-(0.5 * (v2 * ht + bt)));
+            const double vt2 = -s.u + ux, w2 = vn * vn + vt2 * vt2;
+            acc[4] += 0.5 * s.w * vn * (w2 * hin + bin);
+            acc[5] += 0.5 * s.w * vt2 * (w2 * hin + bin);
         }
-        block_reduce_smem<6, 0>(acc, S.red, S.rout);
-        if (threadIdx.x == 0) {
-            double sw[4], sw_t[4], an[4], at[4], atime[4], Mu[7], Mv[6], Mxi[3], m1[4], m2[4], mt[5];
-            for (int m = 0; m < 4; ++m) { sw[m] = (wg[m] - wc[m]) / (side * 0.5 * P.dy); sw_t[m] = S.rout[m]; }
-            s2w_micro_slope(ck, prim_g, sw, an);
-            s2w_micro_slope(ck, prim_g, sw_t, at);
-            s2w_moments(ck, prim_g, Mu, Mv, Mxi);
-            s2w_auvxi(an, Mu, Mv, Mxi, 1, 0, m1);
-            s2w_auvxi(at, Mu, Mv, Mxi, 0, 1, m2);
-            for (int m = 0; m < 4; ++m) sw[m] = -prim_g[0] * (m1[m] + m2[m]);
-            s2w_micro_slope(ck, prim_g, sw, atime);
-            double tau_wall = 0.0;
-            const double wgg[4] = {wg[0], -wg[2], wg[1], wg[3]};
-            const bool tok = s2_tau(P, wgg, tau_wall);
-            s2w_time_coeffs(dt, tau_wall, mt);
-            const double coeff = P.pr != 1.0 ? 0.8 * (1.0 - P.pr) * lambda * lambda / prim_g[0] : 0.0;
-            for (int m = 0; m < 4; ++m) { S.v[m] = an[m]; S.v[4 + m] = at[m]; S.v[8 + m] = atime[m]; }
-            for (int m = 0; m < 5; ++m) S.v[12 + m] = mt[m];
-            S.v[17] = Mxi[2]; S.v[18] = coeff; S.v[19] = S.rout[4]; S.v[20] = S.rout[5]; S.v[21] = tok ? 1.0 : 0.0;
+        warp_sum_all<6>(acc);
+        double sw[4], sw_t[4], Mu[7], Mv[6], Mxi[3], m1[4], m2[4];
+        for (int m = 0; m < 4; ++m) { sw[m] = (wg[m] - wc[m]) / (side * 0.5 * P.dy); sw_t[m] = acc[m]; }
+        s2w_micro_slope(ck, prim_g, sw, an);
+        s2w_micro_slope(ck, prim_g, sw_t, at);
+        s2w_moments(ck, prim_g, Mu, Mv, Mxi);
+        s2w_auvxi(an, Mu, Mv, Mxi, 1, 0, m1);
+        s2w_auvxi(at, Mu, Mv, Mxi, 0, 1, m2);
+        for (int m = 0; m < 4; ++m) sw[m] = -prim_g[0] * (m1[m] + m2[m]);
+        s2w_micro_slope(ck, prim_g, sw, atime);
+        double tau_wall = 0.0;
+        const double wgg[4] = {wg[0], -wg[2], wg[1], wg[3]};
+        ok = s2_tau(P, wgg, tau_wall);
+        s2w_time_coeffs(dt, tau_wall, mt);
+        coeff = P.pr != 1.0 ? 0.8 * (1.0 - P.pr) * lambda * lambda / prim_g[0] : 0.0;
+        mxi2 = Mxi[2];
+        hlx = acc[4];
+        hly = acc[5];
+    }
+    // the incident micro flux g_in and the reflected wall Maxwellian of one velocity
+    auto gin = [&](const WVel& s, double& ginh, double& ginb, double& wallh, double& wallb) {
+        const S2Q q = s2_q(C.th, ck, s.u, s.v);
+        const double mh = q.qh, mb = q.qb;
+        wallh = mh / prim_g[0];
+        wallb = mb / prim_g[0];
+        double corrh = 0.0, corrb = 0.0;
+        if (P.pr != 1.0) {
+            const double vn = s.v, vt = -s.u + ux, v2 = vn * vn + vt * vt;
+            const double qdot = vn * hlx + vt * hly, shh = 2.0 * lambda * v2 - 4.0;
+            corrh = coeff * qdot * shh * mh;
+            corrb = coeff * qdot * (shh + 2.0 / (double)ck) * mb;
         }
-        __syncthreads();
-        if (S.v[21] == 0.0) { ok = false; break; }
-        double an[4], at[4], atime[4], mt[5];
-#pragma unroll
-        for (int m = 0; m < 4; ++m) { an[m] = S.v[m]; at[m] = S.v[4 + m]; atime[m] = S.v[8 + m]; }
-#pragma unroll
-        for (int m = 0; m < 5; ++m) mt[m] = S.v[12 + m];
-        const double mxi2 = S.v[17], coeff = S.v[18], hlx = S.v[19], hly = S.v[20];
-        double ginh[VPT], ginb[VPT], wallh[VPT], wallb[VPT];
+        const double vn = s.v, vt = -s.u, v2 = vn * vn + vt * vt;
+        const double Han = (an[0] + an[1] * vn + an[2] * vt) * mh + 0.5 * an[3] * (v2 * mh + mb);
+        const double Hatan = (at[0] + at[1] * vn + at[2] * vt) * mh + 0.5 * at[3] * (v2 * mh + mb);
+        const double Hatime = (atime[0] + atime[1] * vn + atime[2] * vt) * mh + 0.5 * atime[3] * (v2 * mh + mb);
+        const double Ban = (an[0] + an[1] * vn + an[2] * vt) * mb + 0.5 * an[3] * (v2 * mb + mxi2 * mh);
+        const double Batan = (at[0] + at[1] * vn + at[2] * vt) * mb + 0.5 * at[3] * (v2 * mb + mxi2 * mh);
+        const double Batime = (atime[0] + atime[1] * vn + atime[2] * vt) * mb + 0.5 * atime[3] * (v2 * mb + mxi2 * mh);
+        ginh = mt[0] * mh + mt[1] * (vn * Han + vt * Hatan) + mt[2] * Hatime + mt[3] * rec(s, 0) -
+               mt[4] * (vn * rec(s, 2) + s.u * rec(s, 3));
+        ginb = mt[0] * mb + mt[1] * (vn * Ban + vt * Batan) + mt[2] * Batime + mt[3] * rec(s, 1) -
+               mt[4] * (vn * rec(s, 4) + s.u * rec(s, 5));
+        ginh = ginh + mt[0] * corrh;
+        ginb = ginb + mt[0] * corrb;
+    };
+    double inc = 0.0, rhow = 0.0;
+    if (ok) {   // incidence and reflection -> wall density
         acc[0] = acc[1] = 0.0;
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            const Slot s = slot(r, nv);
-            const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
-            const S2Q q = s2_q(thc, ck, uk, vk);
-            const double mh = q.qh, mb = q.qb;
-            wallh[r] = mh / prim_g[0]; wallb[r] = mb / prim_g[0];
-            double corrh = 0.0, corrb = 0.0;
-            if (P.pr != 1.0) {
-                const double vn = vk, vt = -uk + ux, v2 = vn * vn + vt * vt;
-                const double qdot = vn * hlx + vt * hly, shh = 2.0 * lambda * v2 - 4.0;
-                corrh = coeff * qdot * shh * mh;
-                corrb = coeff * qdot * (shh + 2.0 / (double)ck) * mb;
-            }
-            const double vn = vk, vt = -uk, v2 = vn * vn + vt * vt;
-            const double Han = (an[0] + an[1] * vn + an[2] * vt) * mh + 0.5 * an[3] * (v2 * mh + mb);
-            const double Hatan = (at[0] + at[1] * vn + at[2] * vt) * mh + 0.5 * at[3] * (v2 * mh + mb);
-            const double Hatime = (atime[0] + atime[1] * vn + atime[2] * vt) * mh + 0.5 * atime[3] * (v2 * mh + mb);
-            const double Ban = (an[0] + an[1] * vn + an[2] * vt) * mb + 0.5 * an[3] * (v2 * mb + mxi2 * mh);
-            const double Batan = (at[0] + at[1] * vn + at[2] * vt) * mb + 0.5 * at[3] * (v2 * mb + mxi2 * mh);
-            const double Batime = (atime[0] + atime[1] * vn + atime[2] * vt) * mb + 0.5 * atime[3] * (v2 * mb + mxi2 * mh);
-            ginh[r] = mt[0] * mh + mt[1] * (vn * Han + vt * Hatan) + mt[2] * Hatime + mt[3] * hin[r] -
-                      mt[4] * (vn * hn[r] + uk * ht[r]);
-            ginb[r] = mt[0] * mb + mt[1] * (vn * Ban + vt * Batan) + mt[2] * Batime + mt[3] * bin[r] -
-                      mt[4] * (vn * bn[r] + uk * bt[r]);
-            ginh[r] = ginh[r] + mt[0] * corrh;
-            ginb[r] = ginb[r] + mt[0] * corrb;
-            if (side * vn > 0.0) acc[0] += wk * vn * ginh[r];
-            else acc[1] += dt * wk * vn * wallh[r];
+        for (int r = 0; r < nr; ++r) {
+            const WVel s = wvel(B, nv, r);
+            double ginh, ginb, wallh, wallb;
+            gin(s, ginh, ginb, wallh, wallb);
+            if (side * s.v > 0.0) acc[0] += s.w * s.v * ginh;
+            else acc[1] += dt * s.w * s.v * wallh;
         }
-        block_reduce_smem<2, 0>(acc, S.red, S.rout);
-        const double inc = S.rout[0], refl = S.rout[1];
-        const double rhow = -inc / refl;
-        if (!isfinite(refl) || fabs(refl) <= DBL_MIN || !isfinite(rhow) || rhow <= 0.0) { ok = false; break; }
+        warp_sum_all<2>(acc);
+        inc = acc[0];
+        const double refl = acc[1];
+        rhow = -inc / refl;
+        ok = isfinite(refl) && fabs(refl) > DBL_MIN && isfinite(rhow) && rhow > 0.0;
+    }
+    if (ok) {
+        double* outh = SB.node + node * 2 * nv;
+        double* outb = outh + nv;
 #pragma unroll
         for (int m = 0; m < 4; ++m) acc[m] = 0.0;
-#pragma unroll
-        for (int r = 0; r < VPT; ++r) {
-            const Slot s = slot(r, nv);
-            const double uk = B.u[s.kk], vk = B.v[s.kk], wk = s.ok ? B.w[s.kk] : 0.0;
-            double fh, fb;
-            if (side * vk > 0.0) { fh = vk * ginh[r]; fb = vk * ginb[r]; }
-            else { fh = dt * vk * rhow * wallh[r]; fb = dt * vk * rhow * wallb[r]; }
-            acc[0] += wk * fh; acc[1] += wk * (uk * fh); acc[2] += wk * (vk * fh);
-            acc[3] += wk * (0.5 * ((uk * uk + vk * vk) * fh + fb));
-            afh[r] = afh[r] + gw[g] * fh;
-            afb[r] = afb[r] + gw[g] * fb;
-            if (s.ok) ok = ok && isfinite(fh) && isfinite(fb);
+        for (int r = 0; r < nr; ++r) {
+            const WVel s = wvel(B, nv, r);
+            double ginh, ginb, wallh, wallb, fh, fb;
+            gin(s, ginh, ginb, wallh, wallb);
+            if (side * s.v > 0.0) { fh = s.v * ginh; fb = s.v * ginb; }
+            else { fh = dt * s.v * rhow * wallh; fb = dt * s.v * rhow * wallb; }
+            acc[0] += s.w * fh; acc[1] += s.w * (s.u * fh); acc[2] += s.w * (s.v * fh);
+            acc[3] += s.w * (0.5 * ((s.u * s.u + s.v * s.v) * fh + fb));
+            if (s.ok) {
+                outh[s.k] = fh;
+                outb[s.k] = fb;
+                ok = ok && isfinite(fh) && isfinite(fb);
+            }
         }
-        block_reduce_smem<4, 0>(acc, S.red, S.rout);
-        ok = ok && isfinite(S.rout[0]) && fabs(S.rout[0]) <= 2.0e-12 * fmax(1.0, fabs(inc));
+        warp_sum_all<4>(acc);
+        ok = ok && isfinite(acc[0]) && fabs(acc[0]) <= 2.0e-12 * fmax(1.0, fabs(inc));
+        if (lane < 4) SB.nodew[node * 4 + lane] = lane == 0 ? acc[0] : (lane == 1 ? acc[1] : (lane == 2 ? acc[2] : acc[3]));
+    }
+    ok = __all_sync(0xffffffffu, ok);
+    if (!ok && lane == 0) set_status(B.status, ST_NONFINITE_FLUX);
+}
+
+// Gauss-weighted sum of the node fluxes of every face (interior, then the walls) times the face
+// length, into the face arrays ComputeResidual reads; the walls' macro fluxes also unscaled into
+// SB.wall_raw.  One thread per (face, velocity); threads k < 4 also do the macro flux.
+__global__ void __launch_bounds__(256) k_s2_combine(LoParams P, LoBuffers B, S2Buffers SB) {
+    if (eval_cached(B)) return;
+    const int nv = P.nvel, nx = P.nx, ny = P.ny, nfx = nx * ny, nf = nfx + nx * (ny - 1);
+    const int fi = blockIdx.y;
+    const int k = (int)(blockIdx.x * blockDim.x + threadIdx.x);
+    if (k >= nv) return;
+    const double gw[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
+    size_t o;
+    double len, *Fh, *Fb, *Fw;
+    int wall = -1;
+    if (fi < nfx) {
+        const int i = fi % nx, j = fi / nx;
+        o = (size_t)j * nx + (i + 1) % nx; len = P.dy; Fh = B.fxh; Fb = B.fxb; Fw = B.fxw;
+    } else if (fi < nf) {
+        const int f = fi - nfx, i = f % nx, j = f / nx;
+        o = (size_t)(j + 1) * nx + i; len = P.dx; Fh = B.fyh; Fb = B.fyb; Fw = B.fyw;
+    } else {
+        wall = fi - nf;
+        const int top = wall >= nx ? 1 : 0, i = wall - top * nx;
+        o = top ? (size_t)ny * nx + i : (size_t)i; len = P.dx; Fh = B.fyh; Fb = B.fyb; Fw = B.fyw;
+    }
+    const double* nd = SB.node + (size_t)fi * 3 * 2 * nv;
+    double afh = 0.0, afb = 0.0;
 #pragma unroll
-        for (int m = 0; m < 4; ++m) afw[m] = afw[m] + gw[g] * S.rout[m];
-        ok = __syncthreads_and(ok) != 0;   // uniform before the loop test
+    for (int g = 0; g < 3; ++g) {
+        afh = afh + gw[g] * nd[(size_t)(2 * g) * nv + k];
+        afb = afb + gw[g] * nd[(size_t)(2 * g + 1) * nv + k];
     }
-    if (!__syncthreads_and(ok)) {
-        if (threadIdx.x == 0) set_status(B.status, ST_NONFINITE_FLUX);
-        return;
-    }
-    const size_t o = top ? (size_t)ny * nx + i : (size_t)i;
+    Fh[o * nv + k] = afh * len;
+    Fb[o * nv + k] = afb * len;
+    if (k < 4) {
+        double afw = 0.0;
 #pragma unroll
-    for (int r = 0; r < VPT; ++r) {
-        const Slot s = slot(r, nv);
-        if (s.ok) { B.fyh[o * nv + s.k] = afh[r] * P.dx; B.fyb[o * nv + s.k] = afb[r] * P.dx; }
-    }
-    if (threadIdx.x == 0) {
-        for (int m = 0; m < 4; ++m) B.fyw[o * 4 + m] = afw[m] * P.dx;
-        if (SB.wall_raw != nullptr)
-            for (int m = 0; m < 4; ++m) SB.wall_raw[((size_t)top * nx + i) * 4 + m] = afw[m];
+        for (int g = 0; g < 3; ++g) afw = afw + gw[g] * SB.nodew[((size_t)fi * 3 + g) * 4 + k];
+        Fw[o * 4 + k] = afw * len;
+        if (wall >= 0 && SB.wall_raw != nullptr) SB.wall_raw[(size_t)wall * 4 + k] = afw;
     }
 }
 
@@ -1266,40 +1352,44 @@ cudaError_t prepare_s2() {
     return cudaMemcpyToSymbol(c_s2, &m, sizeof m);
 }
 
-template <int VPT, int NT>
-static void s2_launch_all(int which, const LoParams& P, const LoBuffers& B, const S2Buffers& S, cudaStream_t s,
-                          cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join, cudaError_t& e) {
-    const int nc = P.nx * P.ny;
-    if (which == 0) {
-        k_s2_init<VPT, NT><<<nc, NT, 0, s>>>(P, B, S);
-        e = cudaGetLastError();
-        return;
-    }
-    if (which != 2) {
-        k_s2_targets<VPT, NT><<<nc, NT, 0, s>>>(P, B, S);
-        e = cudaGetLastError();
-        if (which == 3) return;
-    }
-    if (e == cudaSuccess) {
-        const dim3 grid((unsigned)((P.nvel + 127) / 128), (unsigned)nc);
-        k_s2_recon<<<grid, 128, 0, s>>>(P, B, S);
-        e = cudaGetLastError();
-    }
-    if (e == cudaSuccess) e = cudaEventRecord(fork, s);
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
-    if (e == cudaSuccess) { k_s2_walls<VPT, NT><<<2 * P.nx, NT, 0, s2>>>(P, B, S); e = cudaGetLastError(); }
-    if (e == cudaSuccess) e = cudaEventRecord(join, s2);
-    if (e == cudaSuccess) { k_s2_faces<VPT, NT><<<P.nx * P.ny + P.nx * (P.ny - 1), NT, 0, s>>>(P, B, S); e = cudaGetLastError(); }
-    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
-}
 
-// which 0: the S2 cold start; 1: the S2 Evolution of one pseudo-step (targets, reconstruction, faces,
-// walls); 2: the Evolution with the targets kept (S2CN2); 3: the targets of B.W only
+// which 0: the S2 cold start; 1: the S2 Evolution of one pseudo-step (targets, reconstruction,
+// faces, walls); 2: the Evolution with the targets kept (S2CN2); 3: the targets of B.W only
 cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S2Buffers& S, cudaStream_t s,
                        cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join) {
-    cudaError_t e = cudaSuccess;
-    if (P.nvel <= 1024) s2_launch_all<2, 512>(which, P, B, S, s, s2, fork, join, e);
-    else s2_launch_all<5, 512>(which, P, B, S, s, s2, fork, join, e);
+    const int nx = P.nx, ny = P.ny, nv = P.nvel, nc = nx * ny, nf = nx * ny + nx * (ny - 1);
+    auto warps = [](long long n) { return (unsigned)((n * 32 + 255) / 256); };
+    if (which == 0) {
+        k_s2_init<<<warps(nc), 256, 0, s>>>(P, B, S);
+        return cudaGetLastError();
+    }
+    const int faces = which != 3, targets = which != 2;
+    const long long nmac = (faces ? (long long)nf * 4 : 0) + (targets ? (long long)nc * 4 : 0);
+    k_s2_macro<<<(unsigned)((nmac + 127) / 128), 128, 0, s>>>(P, B, S, faces, targets);
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && targets) {
+        k_s2_target_nodes<<<warps((long long)nc * 9), 256, 0, s>>>(P, B, S);
+        e = cudaGetLastError();
+        if (e == cudaSuccess) {
+            k_s2_target_sum<<<dim3((unsigned)((nv + 255) / 256), (unsigned)nc), 256, 0, s>>>(P, B, S);
+            e = cudaGetLastError();
+        }
+    }
+    if (e != cudaSuccess || which == 3) return e;
+    const dim3 grid((unsigned)((nv + 31) / 32), (unsigned)nc);
+    k_s2_recon1<<<grid, 128, 0, s>>>(P, B, S);
+    e = cudaGetLastError();
+    if (e == cudaSuccess) { k_s2_recon2<<<grid, 256, 0, s>>>(P, B, S); e = cudaGetLastError(); }
+    if (e == cudaSuccess) e = cudaEventRecord(fork, s);
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
+    if (e == cudaSuccess) { k_s2_wall_nodes<<<warps(2LL * nx * 3), 256, 0, s2>>>(P, B, S); e = cudaGetLastError(); }
+    if (e == cudaSuccess) e = cudaEventRecord(join, s2);
+    if (e == cudaSuccess) { k_s2_face_nodes<<<warps((long long)nf * 3), 256, 0, s>>>(P, B, S); e = cudaGetLastError(); }
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
+    if (e == cudaSuccess) {
+        k_s2_combine<<<dim3((unsigned)((nv + 255) / 256), (unsigned)(nf + 2 * nx)), 256, 0, s>>>(P, B, S);
+        e = cudaGetLastError();
+    }
     return e;
 }
 

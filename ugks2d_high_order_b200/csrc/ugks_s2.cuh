@@ -18,7 +18,31 @@ struct S2Buffers {
     double *mh, *mb, *kxh, *kxb, *kyh, *kyb;   // [cell][nvel] volume targets
     double* wall_raw;                   // [2][nx][4] wall macro fluxes before the face length (bottom,
                                         // top), for the S2CN2 conservation ledger (nullptr: not kept)
+    // evaluation scratch (s2_bind_scratch)
+    double* node;    // [face][3 nodes][h | b][nvel] Gauss-node micro fluxes; faces: interior x, interior y, walls
+    double* nodew;   // [face][3][4] Gauss-node macro fluxes
+    double* mac;     // [interior face][3][normal left | normal right | tangential][4] macro slopes
+    double* wq;      // [cell][9][4] mean-shifted volume node states
+    double* tscal;   // [cell][9][16] volume node scalars (closure theta, directions, primitive)
+    double* l1;      // [cell][22][nvel] first-layer WENO values of h and b (k_s2_recon1)
 };
+
+// doubles of evaluation scratch one S2Buffers needs, and their layout
+inline size_t s2_scratch_doubles(int nx, int ny, int nv) {
+    const size_t nf = (size_t)nx * ny + (size_t)nx * (ny - 1), nfw = nf + 2 * (size_t)nx, nc = (size_t)nx * ny;
+    auto r = [](size_t n) { return (n + 31) / 32 * 32; };
+    return r(nfw * 3 * 2 * nv) + r(nfw * 3 * 4) + r(nf * 3 * 12) + r(nc * 9 * 4) + r(nc * 9 * 16) + r(nc * 22 * nv);
+}
+inline void s2_bind_scratch(S2Buffers& S, double* base, int nx, int ny, int nv) {
+    const size_t nf = (size_t)nx * ny + (size_t)nx * (ny - 1), nfw = nf + 2 * (size_t)nx, nc = (size_t)nx * ny;
+    auto r = [](size_t n) { return (n + 31) / 32 * 32; };
+    S.node = base; base += r(nfw * 3 * 2 * nv);
+    S.nodew = base; base += r(nfw * 3 * 4);
+    S.mac = base; base += r(nf * 3 * 12);
+    S.wq = base; base += r(nc * 9 * 4);
+    S.tscal = base; base += r(nc * 9 * 16);
+    S.l1 = base;
+}
 
 // s2_tau (mod_S2PhysicalGas.f90:9-20): GetTau of (rho, U, V, 0.5 rho / p), p = 2/(ck+2) e
 __device__ __forceinline__ bool s2_tau(const LoParams& P, const double w[4], double& tau) {
