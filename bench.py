@@ -17,6 +17,10 @@ itself prescribes), no dataset is involved.
   cpu_baseline   the C oracle (a restatement of the reference's Fortran; the Fortran itself does not
                  build on this image) timed on a bounded number of pseudo-steps of the same case.
   explicit_plain the plain second-order Explicit step (1000 steps, CFL 0.5, omega 0.81) for context.
+  high_order_implicit  HighOrderImplicit (WENO5-AO S2 evolution + LU-SGS) from the cold start to its
+                 3000-pseudo-step cap, c_minus_1 recorded, with a bounded oracle sample beside it.
+  s2cn2          the explicit high-order S2CN2 step (S2 evolution + Crank-Nicolson collision) on the same
+                 case, with a bounded oracle sample beside it.
 
 Multi-GPU: a single instance does not shard (one domain per GPU); N ranks run N independent
 replicas ("scaling": "weak").  --impl reference times the CPU restatement of the reference on host
@@ -41,6 +45,8 @@ UNIT = "cell·vel updates/s"
 MAX_PSEUDO_STEPS = 3000
 TOL10_MAX_PSEUDO_STEPS = 20000
 EXPLICIT_STEPS = 1000
+HO_MAX_PSEUDO_STEPS = 3000     # HighOrderImplicit cap (cases/high_implicit/Config.ini MAX_ITER)
+S2CN2_STEPS = 400
 # algorithmic bytes per cell*velocity of the stages (FP64 h and b):
 #   lusgs_forward  reads the right-hand side (h, b) and writes the correction (h, b)      32 B
 #   lusgs_backward also reads the forward correction                                   48 B
@@ -180,6 +186,45 @@ def cpu_baseline(case, velocity, nsteps=30, threads=None):
             "seconds_per_pseudo_step": el / nsteps,
             "sample": f"{nsteps} ImplicitSteady pseudo-steps of the 8x64x1024 cold start after 1 warm-up step "
                       f"({el:.2f} s, C oracle -O2, {nthreads} pthread(s) over cells, faces and slabs)"}
+
+
+def cpu_sample_high_order(velocity, nsteps=2, threads=None):
+    """The oracle on `nsteps` HighOrderImplicit pseudo-steps of the cold start (after one warm-up step)."""
+    from oracle.oracle import Oracle, set_threads
+    from ugks2d_high_order_b200.case import reference_case
+    nthreads = set_threads(threads)
+    case = reference_case("HighOrderImplicit")
+    o = Oracle(case, *velocity)
+    o.init_freestream()
+    o.implicit_init()
+    o.implicit_step()
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        o.implicit_step()
+    el = time.perf_counter() - t0
+    units = case.nx * case.ny * len(velocity[0]) * nsteps
+    return {"value": units / el, "unit": UNIT, "cores": nthreads, "kind": "port", "seconds_per_pseudo_step": el / nsteps,
+            "sample": f"{nsteps} HighOrderImplicit pseudo-steps of the cold start ({el:.2f} s, C oracle -O2, "
+                      f"{nthreads} pthread(s)); the reference's published figure is 1.8153 s per pseudo-step on 8 "
+                      f"MPI ranks (analysis.json high_implicit: 5445.8 s for 3000)"}
+
+
+def cpu_sample_s2cn2(velocity, nsteps=3, threads=None):
+    """The oracle on `nsteps` S2CN2 steps of the cold start (after one warm-up step)."""
+    from oracle.oracle import Oracle, set_threads
+    from ugks2d_high_order_b200.case import reference_case
+    nthreads = set_threads(threads)
+    case = reference_case("S2CN2")
+    o = Oracle(case, *velocity)
+    o.init_freestream()
+    o.s2cn2_step()
+    t0 = time.perf_counter()
+    for _ in range(nsteps):
+        o.s2cn2_step()
+    el = time.perf_counter() - t0
+    units = case.nx * case.ny * len(velocity[0]) * nsteps
+    return {"value": units / el, "unit": UNIT, "cores": nthreads, "kind": "port", "seconds_per_step": el / nsteps,
+            "sample": f"{nsteps} S2CN2 steps of the cold start ({el:.2f} s, C oracle -O2, {nthreads} pthread(s))"}
 
 
 def run_reference_arm(args):
@@ -412,6 +457,53 @@ def main():
                 "kernel_avg_us": {k: 1e3 * t / max(n, 1) for k, (t, n) in kt.items()},
                 "faces_roofline_frac": (BYTES_PER_UPDATE_EXPLICIT * nc * nv / (kt["faces"][0] / kt["faces"][1] * 1e-3) / 1e9) / peak}
 
+    # ---------------- HighOrderImplicit: the cold start to the 3000 pseudo-step cap (the reference run
+    # also stops at its iteration limit, analysis.json high_implicit status)
+    sh = Solver(reference_case("HighOrderImplicit"), *vel, device=local)
+    sh.init_freestream()
+    sh.implicit_init()
+    sh.step_implicit(16)                      # graph capture and warm-up
+    sh.init_freestream()
+    sh.implicit_init()
+    hstream = torch.cuda.ExternalStream(sh.stream)
+    h0, h1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(hstream):
+        h0.record(hstream)
+        done_h, conv_h, rep_h = sh.step_implicit(HO_MAX_PSEUDO_STEPS)
+        h1.record(hstream)
+    h1.synchronize()
+    hms = h0.elapsed_time(h1)
+    ho_value = nc * nv * done_h / (hms * 1e-3)
+    high_order = {"value": ho_value, "unit": UNIT, "pseudo_steps": int(done_h), "converged": bool(conv_h),
+                  "wall_s": hms * 1e-3, "ms_per_pseudo_step": hms / max(done_h, 1),
+                  "c_minus_1": float(rep_h[52]), "science_1_4": [float(x) for x in rep_h[12:16]],
+                  "Rh_Rb": [float(rep_h[24]), float(rep_h[25])],
+                  "hbm_roofline_frac": BYTES_PER_UPDATE_PSEUDO_STEP * ho_value / 1e9 / peak,
+                  "config": "HighOrderImplicit 8x64x1024 (WENO5-AO S2 evolution, PR2 + LU-SGS, 8 slabs), CFL 0.1, "
+                            "nCFL 1000, mass rescale on, cold start, 3000 pseudo-step cap; FP64-bound (the "
+                            "closures and WENO templates), so the HBM fraction is small by construction"}
+    sh.close()
+
+    # ---------------- S2CN2, the explicit high-order step
+    sc = Solver(reference_case("S2CN2"), *vel, device=local)
+    sc.init_freestream()
+    sc.step_s2cn2(8)
+    cstream = torch.cuda.ExternalStream(sc.stream)
+    c0, c1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(cstream):
+        c0.record(cstream)
+        done_c2, rep_c2 = sc.step_s2cn2(S2CN2_STEPS)
+        c1.record(cstream)
+    c1.synchronize()
+    cms = c0.elapsed_time(c1)
+    sc.close()
+    cn_value = nc * nv * done_c2 / (cms * 1e-3)
+    s2cn2 = {"value": cn_value, "unit": UNIT, "steps": int(done_c2), "ms_per_step": cms / max(done_c2, 1),
+             "cnres": float(rep_c2[1]), "mmerr": float(rep_c2[2]), "drift": float(rep_c2[9]),
+             "hbm_roofline_frac": BYTES_PER_UPDATE_EXPLICIT * cn_value / 1e9 / peak,
+             "config": "S2CN2 8x64x1024, CFL 0.1, 8 steps warm-up then 400 steps, two steps per CUDA graph; "
+                       "FP64-bound"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -419,6 +511,11 @@ def main():
             cpu["time_to_steady_estimate_s"] = cpu["seconds_per_pseudo_step"] * (sum(pseudo) / len(pseudo))
         except Exception as e:   # the checker is optional for the device number
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
+        try:
+            high_order["cpu_baseline"] = cpu_sample_high_order(vel)
+            s2cn2["cpu_baseline"] = cpu_sample_s2cn2(vel)
+        except Exception as e:
+            high_order["cpu_baseline"] = s2cn2["cpu_baseline"] = {"value": None, "sample": f"unavailable: {e}"}
 
     if rank == 0:
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -436,6 +533,8 @@ def main():
                 "cpu_baseline": cpu,
                 "explicit_plain": explicit,
                 "tol_1e-10": tol10,
+                "high_order_implicit": high_order,
+                "s2cn2": s2cn2,
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
     s.close()

@@ -169,8 +169,10 @@ int ugks_s2cn2_test_reject(ugks_ctx* ctx, int step);
  * src/mod_Tools.f90:409-432), qx, qy (GetHeatFlux_Vec, src/mod_Tools.f90:355-373). */
 int ugks_macro_fields(ugks_ctx* ctx, double* out);
 
-/* Wall Aerodynamics of the last Evolution (src/mod_Evolution.f90:2402-2409): out[2][nx][3] =
- * local-frame (pnn, pnt, qn) per bottom/top wall face. */
+/* Wall Aerodynamics of the last Evolution: out[2][nx][3] = (pnn, pnt, qn) per bottom/top wall face.
+ * Second-order methods: the local frame of W2BMultiscaleFluxBoundary (src/mod_Evolution.f90:2402-2409);
+ * high-order methods: the native frame n = +y, t = -x of PublishWallDiagnostics
+ * (src/mod_S2NativeAdapter.f90:1075-1097), qn net of the moving wall's work. */
 int ugks_wall_aero(ugks_ctx* ctx, double* out);
 
 /* Copy a named device work array to the host (diagnostics / parity tests).  Names:

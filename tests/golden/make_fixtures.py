@@ -106,12 +106,14 @@ def main(ref):
     ver = json.load(open(os.path.join(ref, "checks/VERIFICATION.json")))
     golden["static_equilibrium"] = {k: ver[k] for k in ("final_static_le", "static_le_19", "static_le_np1")}
     summ = json.load(open(os.path.join(ref, "docs/couette_results/analysis.json")))["summary"]
-    for case in ("low_explicit", "low_implicit"):
+    for case in ("low_explicit", "low_implicit", "high_implicit"):
         c = summ[case]
         keep = {k: c[k] for k in ("steps", "status", "selected_final", "c_final") if k in c}
         if "final_walls" in c:
             keep["final_walls"] = {w: {q: c["final_walls"][w][q] for q in ("native_pnn", "native_pnt", "native_qn")}
                                    for w in c["final_walls"]}
+        if case == "high_implicit":
+            keep["x_spread"] = c["x_spread"]
         keep["source"] = "docs/couette_results/analysis.json summary/" + case
         golden[case + "_final"] = keep
     with open(os.path.join(HERE, "reference_golden.json"), "w") as f:

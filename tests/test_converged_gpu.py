@@ -66,3 +66,33 @@ def test_explicit_limit_matches_reference_profiles(velocity, golden):
         assert not bad, bad
     finally:
         s.close()
+
+
+@pytest.mark.gpu
+def test_high_order_implicit_reaches_reference_limit_state(velocity, golden):
+    """HighOrderImplicit from the cold start to its 3000 pseudo-step cap (the reference run also stops
+    at the iteration limit, not at the gate).  The state is still relaxing there, so the bound is the
+    reference's own x-spread of each profile column (analysis.json high_implicit/x_spread): every
+    x-averaged profile value lies within it of "S2 implicit: limit"."""
+    from ugks2d_high_order_b200.solver import Solver
+    fin = golden["high_implicit_final"]
+    s = Solver(reference_case("HighOrderImplicit"), *velocity)
+    try:
+        s.init_freestream()
+        s.implicit_init()
+        done, conv, rep = s.step_implicit(fin["steps"])
+        assert done == fin["steps"] and not conv
+        ref = np.array(golden["profiles"]["S2 implicit: limit"])[:, 2:]
+        dev = np.abs(s.profiles() - ref).max(axis=0)
+        bad = {c: (d, fin["x_spread"][c]) for c, d in zip(COLS, dev) if not d <= fin["x_spread"][c]}
+        assert not bad, bad
+        assert abs(rep[52]) <= 1e-9, rep[52]              # c_minus_1 (reference: -2.2e-10)
+        assert rep[1] <= 1e-12                            # moment gate of the last accepted state
+        # wall shear and heat in the native frame (PublishWallDiagnostics), x-averaged
+        aero = s.wall_aero().mean(axis=1)
+        for w, row in (("1", 0), ("2", 1)):
+            r = fin["final_walls"][w]
+            for q, col in (("native_pnn", 0), ("native_pnt", 1), ("native_qn", 2)):
+                assert abs(aero[row, col] - r[q]) <= 1e-7 * abs(r[q]), (w, q, aero[row, col], r[q])
+    finally:
+        s.close()

@@ -1252,7 +1252,8 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
 
 // Gauss-weighted sum of the node fluxes of every face (interior, then the walls) times the face
 // length, into the face arrays ComputeResidual reads; the walls' macro fluxes also unscaled into
-// SB.wall_raw.  One thread per (face, velocity); threads k < 4 also do the macro flux.
+// SB.wall_raw, and the walls' (pnn, pnt, qn) into B.wall_aero.  One thread per (face, velocity);
+// threads k < 4 also do the macro flux.
 __global__ void __launch_bounds__(256) k_s2_combine(LoParams P, LoBuffers B, S2Buffers SB) {
     if (eval_cached(B)) return;
     const int nv = P.nvel, nx = P.nx, ny = P.ny, nfx = nx * ny, nf = nfx + nx * (ny - 1);
@@ -1289,6 +1290,23 @@ __global__ void __launch_bounds__(256) k_s2_combine(LoParams P, LoBuffers B, S2B
         for (int g = 0; g < 3; ++g) afw = afw + gw[g] * SB.nodew[((size_t)fi * 3 + g) * 4 + k];
         Fw[o * 4 + k] = afw * len;
         if (wall >= 0 && SB.wall_raw != nullptr) SB.wall_raw[(size_t)wall * 4 + k] = afw;
+    }
+    if (wall >= 0 && k == 0) {   // PublishWallDiagnostics (mod_S2NativeAdapter.f90:1075-1097)
+        const int top = wall >= nx ? 1 : 0;
+        const double measure = B.dt[0] * len;
+        double rate[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) {
+            double afw = 0.0;
+#pragma unroll
+            for (int g = 0; g < 3; ++g) afw = afw + gw[g] * SB.nodew[((size_t)fi * 3 + g) * 4 + m];
+            rate[m] = afw * len / measure;
+        }
+        // native frame n = +y, t = -x; the heat removes the moving wall's mechanical work
+        double* a = B.wall_aero + (size_t)wall * 3;
+        a[0] = rate[2];
+        a[1] = -rate[1];
+        a[2] = rate[3] - P.wall_ux[top] * rate[1];
     }
 }
 
