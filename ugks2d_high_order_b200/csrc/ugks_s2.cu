@@ -518,18 +518,32 @@ __device__ bool s2_solve4(const double* m, const double rhs[4], double x[4]) {
 }
 
 // the closure Maxwellian at theta for velocity (u, v) and its log-derivatives (q_state_first,
-// mod_CorrectedWF2DClosure.f90:389-426)
+// mod_CorrectedWF2DClosure.f90:389-426).  The velocity-independent factors are formed once per
+// theta (S2Th); the divisions by T and rho of the reference become multiplications by 1/T and 1/rho,
+// which moves each value by at most an ulp.
+struct S2Th {
+    double r, u, v, tw;          // theta = (rho, u, v, T_native)
+    double pref, itw, ir, ckh;   // rho / (pi T), 1 / T, 1 / rho, ck T / 2
+};
+__device__ __forceinline__ S2Th s2_th(const double th[4], int ck) {
+    S2Th t;
+    t.r = th[0]; t.u = th[1]; t.v = th[2]; t.tw = th[3];
+    t.pref = t.r / (kPi * t.tw);
+    t.itw = 1.0 / t.tw;
+    t.ir = 1.0 / t.r;
+    t.ckh = 0.5 * (double)ck * t.tw;
+    return t;
+}
 struct S2Q {
     double qh, qb, ld[4], ldb[4];
 };
-__device__ __forceinline__ S2Q s2_q(const double th[4], int ck, double u, double v) {
+__device__ __forceinline__ S2Q s2_q(const S2Th& t, double u, double v) {
     S2Q q;
-    const double r = th[0], tw = th[3];
-    const double du = u - th[1], dv = v - th[2], c2 = du * du + dv * dv;
-    q.qh = r / (kPi * tw) * exp(-c2 / tw);
-    q.ld[0] = 1.0 / r; q.ld[1] = 2.0 * du / tw; q.ld[2] = 2.0 * dv / tw; q.ld[3] = -1.0 / tw + c2 / (tw * tw);
-    q.qb = 0.5 * (double)ck * tw * q.qh;
-    q.ldb[0] = q.ld[0]; q.ldb[1] = q.ld[1]; q.ldb[2] = q.ld[2]; q.ldb[3] = q.ld[3] + 1.0 / tw;
+    const double du = u - t.u, dv = v - t.v, c2 = du * du + dv * dv;
+    q.qh = t.pref * exp(-c2 * t.itw);
+    q.ld[0] = t.ir; q.ld[1] = 2.0 * du * t.itw; q.ld[2] = 2.0 * dv * t.itw; q.ld[3] = -t.itw + c2 * (t.itw * t.itw);
+    q.qb = t.ckh * q.qh;
+    q.ldb[0] = q.ld[0]; q.ldb[1] = q.ld[1]; q.ldb[2] = q.ld[2]; q.ldb[3] = q.ld[3] + t.itw;
     return q;
 }
 
@@ -640,9 +654,10 @@ __device__ bool w_closure(const LoParams& P, const LoBuffers& B, const double w[
         double acc[22];
 #pragma unroll
         for (int m = 0; m < 22; ++m) acc[m] = 0.0;
+        const S2Th tt = s2_th(trial, ck);
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
-            const S2Q q = s2_q(trial, ck, s.u, s.v);
+            const S2Q q = s2_q(tt, s.u, s.v);
             const double e2 = s.u * s.u + s.v * s.v;
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
@@ -709,9 +724,9 @@ __device__ __forceinline__ void w_mke_raw(const WMke& M, const S2Q& q, int ck, d
 }
 
 // M, K_x, K_y of one velocity from the node scalars
-__device__ __forceinline__ void w_mke_at(const double th[4], const WMke& M, int ck, double uk, double vk, S2Q& q,
+__device__ __forceinline__ void w_mke_at(const S2Th& th, const WMke& M, int ck, double uk, double vk, S2Q& q,
                                          double& mh, double& mb, double& kxh, double& kxb, double& kyh, double& kyb) {
-    q = s2_q(th, ck, uk, vk);
+    q = s2_q(th, uk, vk);
     mh = q.qh;
     mb = q.qb;
     w_mke_raw(M, q, ck, uk, vk, kxh, kxb, kyh, kyb);
@@ -732,9 +747,10 @@ __device__ bool w_make_mke(const LoParams& P, const LoBuffers& B, const double w
     double acc[16];
 #pragma unroll
     for (int m = 0; m < 8; ++m) acc[m] = 0.0;
+    const S2Th tt = s2_th(C.th, ck);
     for (int r = 0; r < nr; ++r) {
         const WVel s = wvel(B, nv, r);
-        const S2Q q = s2_q(C.th, ck, s.u, s.v);
+        const S2Q q = s2_q(tt, s.u, s.v);
         double kxh, kxb, kyh, kyb;
         w_mke_raw(M, q, ck, s.u, s.v, kxh, kxb, kyh, kyb);
         const double e2 = s.u * s.u + s.v * s.v;
@@ -757,7 +773,7 @@ __device__ bool w_make_mke(const LoParams& P, const LoBuffers& B, const double w
         const WVel s = wvel(B, nv, r);
         S2Q q;
         double mh, mb, kxh, kxb, kyh, kyb;
-        w_mke_at(C.th, M, ck, s.u, s.v, q, mh, mb, kxh, kxb, kyh, kyb);
+        w_mke_at(tt, M, ck, s.u, s.v, q, mh, mb, kxh, kxb, kyh, kyb);
         const double e2 = s.u * s.u + s.v * s.v, cx = s.u - M.ux, cy = s.v - M.vy, c2 = cx * cx + cy * cy;
         acc[0] += s.w * mh; acc[1] += s.w * s.u * mh; acc[2] += s.w * s.v * mh; acc[3] += 0.5 * s.w * (e2 * mh + mb);
         acc[4] += s.w * kxh; acc[5] += s.w * s.u * kxh; acc[6] += s.w * s.v * kxh; acc[7] += 0.5 * s.w * (e2 * kxh + kxb);
@@ -806,10 +822,11 @@ __global__ void __launch_bounds__(256, 2) k_s2_init(LoParams P, LoBuffers B, S2B
     WClosure C;
     WMke M;
     const bool ok = w_closure(P, B, w, C) && w_make_mke(P, B, w, C, M);
+    const S2Th tt = s2_th(C.th, P.ck);
     if (ok)
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
-            const S2Q q = s2_q(C.th, P.ck, s.u, s.v);
+            const S2Q q = s2_q(tt, s.u, s.v);
             if (s.ok) { B.h[(size_t)cc * nv + s.k] = q.qh; B.b[(size_t)cc * nv + s.k] = q.qb; }
         }
     if (!ok && lane == 0) set_status(B.status, ST_PROJECTION);
@@ -894,7 +911,7 @@ __global__ void __launch_bounds__(256) k_s2_target_sum(LoParams P, LoBuffers B, 
         w_load_scalars(SB.tscal + ((size_t)cc * 9 + p) * kS2TScal, th, M);
         S2Q q;
         double mh, mb, kxh, kxb, kyh, kyb;
-        w_mke_at(th, M, P.ck, uk, vk, q, mh, mb, kxh, kxb, kyh, kyb);
+        w_mke_at(s2_th(th, P.ck), M, P.ck, uk, vk, q, mh, mb, kxh, kxb, kyh, kyb);
         const double wt2 = gw[p % 3] * gw[p / 3];
         amh = amh + wt2 * mh; amb = amb + wt2 * mb;
         akxh = akxh + wt2 * kxh; akxb = akxb + wt2 * kxb;
@@ -965,9 +982,10 @@ __global__ void __launch_bounds__(256, 2) k_s2_face_nodes(LoParams P, LoBuffers 
             for (int m = 0; m < 4; ++m) tdl[m] = tdr[m] = tdt[m] = NAN;
 #pragma unroll
         for (int m = 0; m < 16; ++m) acc[m] = 0.0;
+        const S2Th tt = s2_th(C.th, ck);
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
-            const S2Q q = s2_q(C.th, ck, s.u, s.v);
+            const S2Q q = s2_q(tt, s.u, s.v);
             double dlh, dlb, drh, drb, dth, dtb;
             s2_dq(q, tdl, dlh, dlb);
             s2_dq(q, tdr, drh, drb);
@@ -1007,11 +1025,12 @@ __global__ void __launch_bounds__(256, 2) k_s2_face_nodes(LoParams P, LoBuffers 
         double* outb = outh + nv;
 #pragma unroll
         for (int m = 0; m < 8; ++m) acc[m] = 0.0;
+        const S2Th tt = s2_th(C.th, ck);
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
             S2Q q;
             double mh, mb, kxh, kxb, kyh, kyb;
-            w_mke_at(C.th, M, ck, s.u, s.v, q, mh, mb, kxh, kxb, kyh, kyb);
+            w_mke_at(tt, M, ck, s.u, s.v, q, mh, mb, kxh, kxb, kyh, kyb);
             const double s0h = mh + kxh * q0x + kyh * q0y;
             const double s0b = mb + kxb * q0x + kyb * q0y;
             double dlh, dlb, drh, drb, dth, dtb, mth, mtb;
@@ -1181,8 +1200,9 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
         hly = acc[5];
     }
     // the incident micro flux g_in and the reflected wall Maxwellian of one velocity
+    const S2Th tt = s2_th(C.th, ck);
     auto gin = [&](const WVel& s, double& ginh, double& ginb, double& wallh, double& wallb) {
-        const S2Q q = s2_q(C.th, ck, s.u, s.v);
+        const S2Q q = s2_q(tt, s.u, s.v);
         const double mh = q.qh, mb = q.qb;
         wallh = mh / prim_g[0];
         wallb = mb / prim_g[0];
