@@ -56,11 +56,13 @@ __device__ __forceinline__ bool s2_weno_coef(const double q[5], double fw[4], do
     s = s + 8209 * q1 * q5;
     s = s - 51001 * q4 * q5;
     s = s + 6908 * (q5 * q5);
-    beta[3] = s / 5040.0;
+    // the reference's divisions by 5040, 3, sum(alpha) and gamma_4 are multiplications by the
+    // reciprocals here (each weight moves by at most an ulp); tau / (beta + 1e-8) stays a division
+    beta[3] = s * (1.0 / 5040.0);
     double tau = fabs(beta[3] - beta[0]);
     tau = tau + fabs(beta[3] - beta[1]);
     tau = tau + fabs(beta[3] - beta[2]);
-    tau = tau / 3.0;
+    tau = tau * (1.0 / 3.0);
     const double gam[4] = {0.01125, 0.1275, 0.01125, 0.85};
     double alpha[4], sa = 0.0;
 #pragma unroll
@@ -69,9 +71,10 @@ __device__ __forceinline__ bool s2_weno_coef(const double q[5], double fw[4], do
         alpha[c] = gam[c] * (1.0 + r * r);
         sa = sa + alpha[c];
     }
-    fw[3] = (alpha[3] / sa) / gam[3];
+    const double isa = 1.0 / sa;
+    fw[3] = (alpha[3] * isa) * (1.0 / 0.85);
 #pragma unroll
-    for (int c = 0; c < 3; ++c) fw[c] = alpha[c] / sa - fw[3] * gam[c];
+    for (int c = 0; c < 3; ++c) fw[c] = alpha[c] * isa - fw[3] * gam[c];
 #pragma unroll
     for (int c = 0; c < 4; ++c)
 #pragma unroll
@@ -367,7 +370,7 @@ __global__ void __launch_bounds__(128) k_s2_recon1(LoParams P, LoBuffers B, S2Bu
 // at its 3 Gauss nodes with value, normal and tangential derivative, and parts 0..2 also the volume
 // Gauss row p; the positivity factor theta is the minimum over the 8 warps (both fields, all face and
 // volume samples), then each warp writes its side's limited values.
-__global__ void __launch_bounds__(256) k_s2_recon2(LoParams P, LoBuffers B, S2Buffers S) {
+__global__ void __launch_bounds__(256, 3) k_s2_recon2(LoParams P, LoBuffers B, S2Buffers S) {
     if (eval_cached(B)) return;
     __shared__ double s_th[8][32];
     const int nv = P.nvel, nx = P.nx, ny = P.ny, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
