@@ -21,6 +21,10 @@ itself prescribes), no dataset is involved.
                  3000-pseudo-step cap, c_minus_1 recorded, with a bounded oracle sample beside it.
   s2cn2          the explicit high-order S2CN2 step (S2 evolution + Crank-Nicolson collision) on the same
                  case, with a bounded oracle sample beside it.
+  batched        256 S2CN2 instances of the batched distribution (Kn log-uniform in [0.01, 1], wall Mach
+                 in [0.5, 3], wall temperature ratio in [0.8, 1.2], 8x{32,64,128} cells, {24,32,48}^2
+                 velocities, PCG64(20261203)) advanced together (one graph launch per two steps, stream
+                 count picked by the autotuner); aggregate updates/s and the ratio to s2cn2's plain rate.
 
 Multi-GPU: a single instance does not shard (one domain per GPU); N ranks run N independent
 replicas ("scaling": "weak").  --impl reference times the CPU restatement of the reference on host
@@ -47,6 +51,7 @@ TOL10_MAX_PSEUDO_STEPS = 20000
 EXPLICIT_STEPS = 1000
 HO_MAX_PSEUDO_STEPS = 3000     # HighOrderImplicit cap (cases/high_implicit/Config.ini MAX_ITER)
 S2CN2_STEPS = 400
+BATCH_STEPS = 4               # batched steps timed (each advances all 256 instances by one step)
 # algorithmic bytes per cell*velocity of the stages (FP64 h and b):
 #   lusgs_forward  reads the right-hand side (h, b) and writes the correction (h, b)      32 B
 #   lusgs_backward also reads the forward correction                                   48 B
@@ -504,6 +509,38 @@ def main():
              "config": "S2CN2 8x64x1024, CFL 0.1, 8 steps warm-up then 400 steps, two steps per CUDA graph; "
                        "FP64-bound"}
 
+    # ---------------- batched S2CN2: 256 instances of uneven sizes
+    from ugks2d_high_order_b200.batch import Batch
+    from ugks2d_high_order_b200.case import batched_cases, velocity_table
+    bcases = batched_cases()
+    tables = {n: velocity_table(n) for n in (24, 32, 48)}
+    bt = Batch([(c, tables[n]) for c, n in bcases], device=local, max_streams=16)
+    bt.init_freestream()
+    k_tuned, tune_ms = bt.tune(steps=2)
+    bt.init_freestream()
+    bt.run(2)
+    bstream = torch.cuda.ExternalStream(bt.stream)
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    blaunch0 = bt.launch_count
+    with torch.cuda.stream(bstream):
+        b0.record(bstream)
+        bdone, bst = bt.run(BATCH_STEPS)
+        b1.record(bstream)
+    b1.synchronize()
+    bms = b0.elapsed_time(b1)
+    bcv = bt.cell_velocities
+    b_value = bcv * BATCH_STEPS / (bms * 1e-3)
+    batched = {"value": b_value, "unit": UNIT, "instances": len(bcases), "cell_velocities_per_step": int(bcv),
+               "steps": BATCH_STEPS, "ms_per_batched_step": bms / BATCH_STEPS, "streams": int(k_tuned),
+               "all_accepted": bool((bdone == BATCH_STEPS).all() and not bst.any()),
+               "vs_plain_s2cn2": b_value / s2cn2["value"],
+               "gpu_launches": int(bt.launch_count - blaunch0),
+               "full_run_estimate_s": 2000 * bms / BATCH_STEPS * 1e-3,
+               "config": "256 S2CN2 instances, seed PCG64(20261203), CFL 0.1, omega 0.5, cold start; 2 steps "
+                         "warm-up after the autotuner; each bench step advances every instance by one step "
+                         "(the distribution's full run is 2000 steps)"}
+    bt.close()
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -535,6 +572,7 @@ def main():
                 "tol_1e-10": tol10,
                 "high_order_implicit": high_order,
                 "s2cn2": s2cn2,
+                "batched": batched,
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
     s.close()

@@ -164,6 +164,39 @@ int ugks_s2cn2_steps(ugks_ctx* ctx, int nsteps, int* steps_done, double* report)
  * the gate, so that step is rejected.  One-shot; 0 clears it.  Host-side, numerical only. */
 int ugks_s2cn2_test_reject(ugks_ctx* ctx, int step);
 
+/* Batched S2CN2: many independent Couette instances of uneven grid and velocity-set sizes advanced
+ * together (BASELINE's batched form; no counterpart routine in the reference, whose runs are one case
+ * per job).  Each instance is described by ugks_params (method UGKS_METHOD_S2CN2) and its velocity
+ * table.  Instances own their persistent state (two state sets, two target sets, ledger: about 16
+ * doubles per cell-velocity); the per-step scratch lives in up to max_streams slots sized for the
+ * largest instance, instances being assigned to slots largest-first.  One CUDA graph launch advances
+ * every instance by two steps, the slots running concurrently.
+ * ugks_batch_init_freestream: InitFlow_Freestream + the S2 cold start + the ledger of every instance.
+ * ugks_batch_run: nsteps steps of every instance; steps_done[n] / status[n] (optional) per instance;
+ *   an instance whose step is rejected stops at its last accepted state (status bit of reference
+ *   code 203 or the gate's own code), the others continue; returns UGKS_ENUMERIC if any stopped.
+ * ugks_batch_tune: times `steps` steps at 1, 2, 4, ... max_streams slots on the live batch (the
+ *   instances advance) and keeps the fastest; *chosen and *ms_per_step report it.
+ * ugks_batch_upload / download / report / wall_aero: per-instance state, last-step report[24] (as
+ *   ugks_s2cn2_steps) and wall (pnn, pnt, qn). */
+typedef struct ugks_instance_desc {
+    ugks_params params;
+    const double *u, *v, *w;   /* host velocity table, params.nvel entries */
+} ugks_instance_desc;
+typedef struct ugks_batch ugks_batch;
+int ugks_batch_create(int n, const ugks_instance_desc* desc, int device, int max_streams, ugks_batch** out);
+int ugks_batch_destroy(ugks_batch* batch);
+int ugks_batch_init_freestream(ugks_batch* batch, double rho, double U, double V, double tnative);
+int ugks_batch_run(ugks_batch* batch, int nsteps, int* steps_done, unsigned* status);
+int ugks_batch_tune(ugks_batch* batch, int steps, int* chosen, double* ms_per_step);
+int ugks_batch_set_streams(ugks_batch* batch, int streams);
+int ugks_batch_upload(ugks_batch* batch, int i, const double* h, const double* b, const double* W);
+int ugks_batch_download(ugks_batch* batch, int i, double* h, double* b, double* W);
+int ugks_batch_report(ugks_batch* batch, int i, double* report);
+int ugks_batch_wall_aero(ugks_batch* batch, int i, double* out);
+long long ugks_batch_launch_count(const ugks_batch* batch);
+void* ugks_batch_stream(ugks_batch* batch);
+
 /* Steady output fields of every cell, as Output writes them (src/mod_Output.f90:102-116):
  * out[nc][10] = r, u, v, T (= 1/lambda), p (= r T / 2), sxx, sxy, syy (Get_Stress_Vec,
  * src/mod_Tools.f90:409-432), qx, qy (GetHeatFlux_Vec, src/mod_Tools.f90:355-373). */

@@ -50,6 +50,25 @@ def read_mesh(path):
     return nx0, ny0, gx.copy(), gy.copy()
 
 
+def parse_velocity_tables(path):
+    """raw_node / raw_weight of the half16 and half32 rules (mod_VelocityTables.f90:40-96)."""
+    import re
+    txt = open(path).read()
+    out = {}
+    for name in ("half16", "half32"):
+        body = txt[txt.index("case('%s')" % name):]
+        body = body[:body.index("case(", 5) if "case(" in body[5:] else body.index("end select")]
+        arrays = {}
+        for key in ("raw_node", "raw_weight"):
+            seg = body[body.index(key + "=["):]
+            seg = seg[:seg.index("]")]
+            arrays[key] = [float(x.replace("_KREAL", "").replace("d", "e"))
+                           for x in re.findall(r"[-+]?\d\.\d+e[-+]\d+_KREAL", seg)]
+        out[name] = arrays
+    out["source"] = "src/mod_VelocityTables.f90 FillVelocity raw rules"
+    return out
+
+
 def parse_profiles(path):
     zones = {}
     name = None
@@ -116,6 +135,7 @@ def main(ref):
             keep["x_spread"] = c["x_spread"]
         keep["source"] = "docs/couette_results/analysis.json summary/" + case
         golden[case + "_final"] = keep
+    golden["velocity_tables"] = parse_velocity_tables(os.path.join(ref, "src/mod_VelocityTables.f90"))
     with open(os.path.join(HERE, "reference_golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
     print("wrote fixtures to", HERE)

@@ -10,7 +10,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libugks_b200.so")
-SOURCES = ["ugks_lo.cu", "ugks_implicit.cu", "ugks_s2.cu", "ugks_s2cn2.cu", "ugks_capi.cu", "ugks_noalloc.cu"]
+SOURCES = ["ugks_lo.cu", "ugks_implicit.cu", "ugks_s2.cu", "ugks_s2cn2.cu", "ugks_batch.cu", "ugks_capi.cu", "ugks_noalloc.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 FLAGS = ["-gencode", "arch=compute_100a,code=sm_100a", "-O3", "-lineinfo", "-std=c++17",
          "-Xcompiler", "-fPIC", "-shared", "--expt-relaxed-constexpr", "-I" + os.path.join(ROOT, "include")]

@@ -29,7 +29,9 @@ EXPORTS = [
     "ugks_error_string", "ugks_stream", "ugks_synchronize", "ugks_profile_enable", "ugks_profile_read",
     "ugks_launch_count", "ugks_step_explicit_noalloc", "ugks_implicit_init", "ugks_implicit_steps",
     "ugks_implicit_state", "ugks_s2cn2_init", "ugks_s2cn2_steps",
-    "ugks_s2cn2_test_reject",
+    "ugks_s2cn2_test_reject", "ugks_batch_create", "ugks_batch_destroy", "ugks_batch_init_freestream",
+    "ugks_batch_run", "ugks_batch_tune", "ugks_batch_set_streams", "ugks_batch_upload", "ugks_batch_download",
+    "ugks_batch_report", "ugks_batch_wall_aero", "ugks_batch_launch_count", "ugks_batch_stream",
 ]
 REPORT_LEN = 80
 CN_REPORT_LEN = 24
@@ -52,6 +54,10 @@ class UgksParams(ctypes.Structure):
         ("macro_sweeps", ctypes.c_int),
         ("residual_tol", ctypes.c_double), ("moment_tol", ctypes.c_double), ("min_alpha", ctypes.c_double),
     ]
+
+
+class UgksInstanceDesc(ctypes.Structure):
+    _fields_ = [("params", UgksParams), ("u", ctypes.c_void_p), ("v", ctypes.c_void_p), ("w", ctypes.c_void_p)]
 
 
 class UgksError(RuntimeError):
@@ -108,6 +114,22 @@ def load(path=LIB_PATH):
     L.ugks_s2cn2_init.argtypes = [vp]
     L.ugks_s2cn2_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), dp]
     L.ugks_s2cn2_test_reject.argtypes = [vp, ctypes.c_int]
+    ip = ctypes.POINTER(ctypes.c_int)
+    L.ugks_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(UgksInstanceDesc), ctypes.c_int, ctypes.c_int,
+                                    ctypes.POINTER(vp)]
+    L.ugks_batch_destroy.argtypes = [vp]
+    L.ugks_batch_init_freestream.argtypes = [vp] + [ctypes.c_double] * 4
+    L.ugks_batch_run.argtypes = [vp, ctypes.c_int, ip, ctypes.POINTER(ctypes.c_uint)]
+    L.ugks_batch_tune.argtypes = [vp, ctypes.c_int, ip, dp]
+    L.ugks_batch_set_streams.argtypes = [vp, ctypes.c_int]
+    L.ugks_batch_upload.argtypes = [vp, ctypes.c_int, dp, dp, dp]
+    L.ugks_batch_download.argtypes = [vp, ctypes.c_int, dp, dp, dp]
+    L.ugks_batch_report.argtypes = [vp, ctypes.c_int, dp]
+    L.ugks_batch_wall_aero.argtypes = [vp, ctypes.c_int, dp]
+    L.ugks_batch_launch_count.argtypes = [vp]
+    L.ugks_batch_launch_count.restype = ctypes.c_longlong
+    L.ugks_batch_stream.argtypes = [vp]
+    L.ugks_batch_stream.restype = vp
     _lib = L
     return L
 

@@ -67,3 +67,34 @@ def load_velocity_half32():
     """The reference's velocity_half32_scale2.dat table (u, v, w), k = i + (j-1)*Nu."""
     t = np.load(os.path.join(_GOLDEN, "velocity_half32_scale2.npy"))
     return t[:, 0].copy(), t[:, 1].copy(), t[:, 2].copy()
+
+
+def velocity_table(n_per_axis, scale=2.0):
+    """(u, v, w) of an n x n half-range table with the given scale: the reference's own file for
+    32 x 32 at scale 2, otherwise generated (ugks2d_high_order_b200.velocity)."""
+    if n_per_axis == 32 and scale == 2.0:
+        return load_velocity_half32()
+    from .velocity import structured_table
+    return structured_table(n_per_axis, scale)
+
+
+def batched_cases(n=256, seed=20261203, ny_choices=(32, 64, 128), nvel_choices=(24, 32, 48)):
+    """The batched Couette distribution: Kn log-uniform in [0.01, 1] (mu_ref = Kn / sqrt(pi),
+    mod_ImportPara.f90:926), wall Mach uniform in [0.5, 3] (WallUx = -/+ Ma sqrt(5/3 theta_w) per
+    wall), wall temperature ratio uniform in [0.8, 1.2] (T_native,wall = 2 ratio, gas T_native 2),
+    grids 8 x {32, 64, 128} on the unit square, velocity sets {24^2, 32^2, 48^2}, all uniform, from
+    numpy's PCG64(seed).  Method S2CN2 at CFL 0.1.  Returns [(CouetteCase, n_per_axis)]."""
+    rng = np.random.Generator(np.random.PCG64(seed))
+    out = []
+    for _ in range(n):
+        kn = 10.0 ** rng.uniform(-2.0, 0.0)
+        ma = rng.uniform(0.5, 3.0)
+        ratio = rng.uniform(0.8, 1.2)
+        ny = int(rng.choice(ny_choices))
+        nva = int(rng.choice(nvel_choices))
+        tw = 2.0 * ratio
+        ux = ma * math.sqrt(5.0 / 3.0 * (0.5 * tw))
+        c = CouetteCase(ny=ny, dy=1.0 / ny, mu_ref=kn / math.sqrt(math.pi), wall_ux=(-ux, ux),
+                        wall_tnative=(tw, tw), method="S2CN2")
+        out.append((c, nva))
+    return out

@@ -30,8 +30,18 @@ class Solver:
         self.v = np.ascontiguousarray(v, dtype=np.float64)
         self.w = np.ascontiguousarray(w, dtype=np.float64)
         self.nx, self.ny, self.nvel = case.nx, case.ny, len(self.u)
+        p = self.params_for(case, self.nvel)
+        self._params = p
+        ctx = ctypes.c_void_p()
+        self._check(self.L.ugks_ctx_create(ctypes.byref(p), _p(self.u), _p(self.v), _p(self.w), device,
+                                           ctypes.byref(ctx)), "ugks_ctx_create", None)
+        self.ctx = ctx
+
+    @staticmethod
+    def params_for(case, nvel):
+        """ugks_params of a case (the C ABI's view of Config.ini)."""
         p = capi.UgksParams()
-        p.nx, p.ny, p.nvel = case.nx, case.ny, self.nvel
+        p.nx, p.ny, p.nvel = case.nx, case.ny, nvel
         p.dx, p.dy = case.dx, case.dy
         p.ck = case.ck
         p.pr, p.omega, p.mu_ref, p.cfl = case.pr, case.omega, case.mu_ref, case.cfl
@@ -43,11 +53,7 @@ class Solver:
                     "S2CN2": capi.UGKS_METHOD_S2CN2}.get(case.method, capi.UGKS_METHOD_EXPLICIT)
         p.ncfl, p.nslab, p.mass_rescale, p.macro_sweeps = case.ncfl, case.nslab, int(case.mass_rescale), case.macro_sweeps
         p.residual_tol, p.moment_tol, p.min_alpha = case.residual_tol, case.moment_tol, case.min_alpha
-        self._params = p
-        ctx = ctypes.c_void_p()
-        self._check(self.L.ugks_ctx_create(ctypes.byref(p), _p(self.u), _p(self.v), _p(self.w), device,
-                                           ctypes.byref(ctx)), "ugks_ctx_create", None)
-        self.ctx = ctx
+        return p
 
     def _check(self, code, what, ctx="self"):
         capi.check(self.L, self.ctx if ctx == "self" else ctx, code, what)
