@@ -73,3 +73,31 @@ def test_high_order_ten_steps_match_oracle(velocity):
         assert abs(rep[52] - row[52]) <= HO_TOL * max(abs(row[52]), 1e-3)   # c_minus_1
     finally:
         s.close()
+
+
+@pytest.mark.gpu
+def test_refined_high_order_two_steps_match_oracle():
+    """The refined variant (16 x 128 cells, generated 48^2 table, 8 slabs of 16 rows): 2 pseudo-steps
+    against the oracle; no reference output exists at this size."""
+    from oracle.oracle import Oracle, set_threads
+    from ugks2d_high_order_b200.case import refined_high_order_case, velocity_table
+    from ugks2d_high_order_b200.solver import Solver
+    set_threads(None)
+    case = refined_high_order_case()
+    table = velocity_table(48)
+    s = Solver(case, *table)
+    o = Oracle(case, *table)
+    try:
+        s.init_freestream(); s.implicit_init()
+        o.init_freestream(); o.implicit_init()
+        for step in range(2):
+            done, conv, rep = s.step_implicit(1)
+            row = o.implicit_step()
+            assert done == 1
+            hg, bg, Wg = s.download()
+            ho, bo, Wo = o.get_state()
+            assert _rel(Wg, Wo) <= HO_TOL and _rel(hg, ho) <= HO_TOL, (step, _rel(Wg, Wo), _rel(hg, ho))
+            for i in (12, 13, 15, 24, 25):   # science_1, 2, 4 and the micro residuals
+                assert abs(rep[i] - row[i]) <= 1e-8 * abs(row[i]), (step, i, rep[i], row[i])
+    finally:
+        s.close()

@@ -58,6 +58,14 @@ def reference_case(method="Explicit"):
     return c
 
 
+def refined_high_order_case():
+    """The refined HighOrderImplicit variant: 16 x 128 cells on the unit square (uniform mesh) with a
+    48 x 48 velocity set (generated half-range table, scale 2); otherwise the high_implicit case.
+    The reference has no 48^2 table and no run at this size, so only the oracle checks it."""
+    c = reference_case("HighOrderImplicit")
+    return c.with_(nx=16, ny=128, dx=1.0 / 16.0, dy=1.0 / 128.0)
+
+
 def baseline_explicit_case():
     """Throughput variant of the explicit case: CFL 0.5, omega 0.81 (same mesh, walls, Kn)."""
     return CouetteCase(cfl=0.5, omega=0.81)
