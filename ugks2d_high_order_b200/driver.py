@@ -1,6 +1,7 @@
 """Command-line driver for the Couette case (the role of the reference's run.sh + Solve_UGKS loop).
 
     python -m ugks2d_high_order_b200.driver --method Explicit --steps 200 [--cfl 0.5 --omega 0.81]
+    python -m ugks2d_high_order_b200.driver --method S2CN2 --steps 20 [--nvel 48 --ny 128]
 
 Runs the case on cuda:0 and prints the residual line every --show steps, as Write_residuals does
 (src/mod_Solve.f90:427-461).  Also the small, self-contained command used for ncu captures.
@@ -8,19 +9,21 @@ Runs the case on cuda:0 and prints the residual line every --show steps, as Writ
 import argparse
 import time
 
-from .case import CouetteCase, load_velocity_half32, reference_case
+from .case import CouetteCase, reference_case, velocity_table
 from .solver import Solver
 
 
 def main(argv=None):
     ap = argparse.ArgumentParser()
-    ap.add_argument("--method", default="Explicit", choices=["Explicit", "ImplicitSteady", "HighOrderImplicit"])
+    ap.add_argument("--method", default="Explicit",
+                    choices=["Explicit", "ImplicitSteady", "HighOrderImplicit", "S2CN2"])
     ap.add_argument("--steps", type=int, default=100)
     ap.add_argument("--show", type=int, default=100)
     ap.add_argument("--cfl", type=float, default=None)
     ap.add_argument("--omega", type=float, default=None)
     ap.add_argument("--ny", type=int, default=None)
     ap.add_argument("--nx", type=int, default=None)
+    ap.add_argument("--nvel", type=int, default=32, help="velocities per axis (32: the reference's table)")
     a = ap.parse_args(argv)
     case = reference_case(a.method)
     kw = {}
@@ -35,9 +38,9 @@ def main(argv=None):
         kw["nx"] = a.nx
         kw["dx"] = 1.0 / a.nx
     case = case.with_(**kw) if kw else case
-    s = Solver(case, *load_velocity_half32())
+    s = Solver(case, *velocity_table(a.nvel))
     s.init_freestream()
-    if a.method != "Explicit":
+    if a.method in ("ImplicitSteady", "HighOrderImplicit"):
         s.implicit_init()
     t0 = time.perf_counter()
     done = 0
@@ -47,6 +50,11 @@ def main(argv=None):
             dt, res = s.step_explicit(n)
             done += n
             print(f"iter={done:8d} dt={dt:.7e} res={' '.join(f'{r:.7e}' for r in res)}", flush=True)
+        elif a.method == "S2CN2":
+            got, rep = s.step_s2cn2(n)
+            done += n
+            print(f"iter={done:8d} dt={rep[0]:.7e} cnres={rep[1]:.3e} mmerr={rep[2]:.3e} drift={rep[9]:.3e} "
+                  f"wall_balance_rho={rep[18]:.6e}", flush=True)
         else:
             got, conv, rep = s.step_implicit(n)
             done += n
