@@ -21,7 +21,9 @@ itself prescribes), no dataset is involved.
                  3000-pseudo-step cap, c_minus_1 recorded, with a bounded oracle sample beside it.
   s2cn2          the explicit high-order S2CN2 step (S2 evolution + Crank-Nicolson collision) on the same
                  case, with a bounded oracle sample beside it.
-  batched        256 S2CN2 instances of the batched distribution (Kn log-uniform in [0.01, 1], wall Mach
+  batched        (N > 1: the instances are split over the ranks by an LPT greedy on cells x velocities,
+                 no collective; time = max over ranks; value = all instances' work / that time)
+                 256 S2CN2 instances of the batched distribution (Kn log-uniform in [0.01, 1], wall Mach
                  in [0.5, 3], wall temperature ratio in [0.8, 1.2], 8x{32,64,128} cells, {24,32,48}^2
                  velocities, PCG64(20261203)) advanced together (one graph launch per two steps, stream
                  count picked by the autotuner); aggregate updates/s and the ratio to s2cn2's plain rate.
@@ -539,7 +541,10 @@ def main():
     # ---------------- batched S2CN2: 256 instances of uneven sizes
     from ugks2d_high_order_b200.batch import Batch
     from ugks2d_high_order_b200.case import batched_cases, velocity_table
-    bcases = batched_cases()
+    from ugks2d_high_order_b200.shard import instance_cost, shard
+    bcases_all = batched_cases()
+    bcosts = [instance_cost(c, n * n) for c, n in bcases_all]
+    bcases, _ = shard(bcases_all, bcosts, rank, world)     # this rank's LPT share (all of it at N=1)
     tables = {n: velocity_table(n) for n in (24, 32, 48)}
     bt = Batch([(c, tables[n]) for c, n in bcases], device=local, max_streams=16)
     bt.init_freestream()
@@ -549,18 +554,21 @@ def main():
     bstream = torch.cuda.ExternalStream(bt.stream)
     b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     blaunch0 = bt.launch_count
+    barrier()
     with torch.cuda.stream(bstream):
         b0.record(bstream)
         bdone, bst = bt.run(BATCH_STEPS)
         b1.record(bstream)
     b1.synchronize()
-    bms = b0.elapsed_time(b1)
-    bcv = bt.cell_velocities
+    barrier()
+    bms = max_over_ranks(b0.elapsed_time(b1))
+    bcv = sum(bcosts)                                       # all instances, all ranks
     b_value = bcv * BATCH_STEPS / (bms * 1e-3)
-    batched = {"value": b_value, "unit": UNIT, "instances": len(bcases), "cell_velocities_per_step": int(bcv),
+    batched = {"value": b_value, "unit": UNIT, "instances": len(bcases_all), "instances_this_rank": len(bcases),
+               "cell_velocities_per_step": int(bcv), "scaling": "strong" if world > 1 else None,
                "steps": BATCH_STEPS, "ms_per_batched_step": bms / BATCH_STEPS, "streams": int(k_tuned),
                "all_accepted": bool((bdone == BATCH_STEPS).all() and not bst.any()),
-               "vs_plain_s2cn2": b_value / s2cn2["value"],
+               "vs_plain_s2cn2": b_value / (world * s2cn2["value"]),
                "gpu_launches": int(bt.launch_count - blaunch0),
                "full_run_estimate_s": 2000 * bms / BATCH_STEPS * 1e-3,
                "config": "256 S2CN2 instances, seed PCG64(20261203), CFL 0.1, omega 0.5, cold start; 2 steps "

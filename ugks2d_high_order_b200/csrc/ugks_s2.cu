@@ -1408,11 +1408,20 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     const long long nmac = (faces ? (long long)nf * 4 : 0) + (targets ? (long long)nc * 4 : 0);
     k_s2_macro<<<(unsigned)((nmac + 127) / 128), 128, 0, s>>>(P, B, S, faces, targets);
     cudaError_t e = cudaGetLastError();
+    // which 1: the targets need only the macro pass and are first read after the face combine, so
+    // they run on the side stream beside the reconstruction and the face nodes (the wall nodes
+    // follow them there); which 3: on the main stream
+    const bool side_targets = targets && faces;
+    if (e == cudaSuccess && side_targets) {
+        e = cudaEventRecord(fork, s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
+    }
     if (e == cudaSuccess && targets) {
-        k_s2_target_nodes<<<warps((long long)nc * 9), 256, 0, s>>>(P, B, S);
+        cudaStream_t ts = side_targets ? s2 : s;
+        k_s2_target_nodes<<<warps((long long)nc * 9), 256, 0, ts>>>(P, B, S);
         e = cudaGetLastError();
         if (e == cudaSuccess) {
-            k_s2_target_sum<<<dim3((unsigned)((nv + 255) / 256), (unsigned)nc), 256, 0, s>>>(P, B, S);
+            k_s2_target_sum<<<dim3((unsigned)((nv + 255) / 256), (unsigned)nc), 256, 0, ts>>>(P, B, S);
             e = cudaGetLastError();
         }
     }
