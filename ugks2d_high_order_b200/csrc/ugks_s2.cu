@@ -32,12 +32,28 @@ __constant__ S2Maps c_s2;
 // ------------------------------------------------------------------------------------------
 // per-thread reconstruction arithmetic (mod_S2D1Reconstruction.f90), in the reference's order
 
-__device__ __forceinline__ double s2_powi(double x, int n) {
-    return n == 0 ? 1.0 : (n == 1 ? x : (n == 2 ? x * x : (n == 3 ? x * x * x : (x * x) * (x * x))));
-}
+// Every evaluation of the S2 path is at xi = -1/2, +1/2 or a Gauss node, so the value (or the
+// xi-derivative) of candidate polynomial c at point p is a fixed linear combination of its stencil,
+// sum_k E[p][c][k] q[k] with E = sum_d cmap[c][k][d] xi_p^d, tabulated on the host from the same
+// maps.  The reference forms the polynomial coefficients first and then evaluates them
+// (prepared_eval, :247-262); the same sums taken in this order agree to an ulp.
+enum { S2_XM = 0, S2_XP = 1, S2_G0 = 2 };   // points -1/2, +1/2, then the Gauss nodes 0..2
+struct S2PointW {
+    double E[5][4][5];   // value weights [point][candidate][stencil sample]
+    double D[5][4][5];   // derivative weights
+};
+__constant__ S2PointW c_s2p;
 
-// weno_coefficients (:168-204)
-__device__ __forceinline__ bool s2_weno_coef(const double q[5], double fw[4], double coef[4][5]) {
+struct S2Weno {
+    double fw[4];   // final weights of the 4 candidates
+    double q[5];    // the stencil
+};
+
+// weno_coefficients (:168-204): the nonlinear weights of stencil q
+__device__ __forceinline__ bool s2_weno(const double q[5], S2Weno& w) {
+    double* fw = w.fw;
+#pragma unroll
+    for (int k = 0; k < 5; ++k) w.q[k] = q[k];
     const double q1 = q[0], q2 = q[1], q3 = q[2], q4 = q[3], q5 = q[4];
     double beta[4];
     double t = q1 - 2 * q2 + q3, u0 = q1 - 4 * q2 + 3 * q3;
@@ -75,83 +91,37 @@ __device__ __forceinline__ bool s2_weno_coef(const double q[5], double fw[4], do
     fw[3] = (alpha[3] * isa) * (1.0 / 0.85);
 #pragma unroll
     for (int c = 0; c < 3; ++c) fw[c] = alpha[c] * isa - fw[3] * gam[c];
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-#pragma unroll
-        for (int d = 0; d < 5; ++d) coef[c][d] = 0.0;
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int k = c; k <= c + 2; ++k)
-#pragma unroll
-            for (int d = 0; d <= 2; ++d) coef[c][d] = coef[c][d] + c_s2.cmap[c][k][d] * q[k];
-#pragma unroll
-    for (int k = 0; k < 5; ++k)
-#pragma unroll
-        for (int d = 0; d <= 4; ++d) coef[3][d] = coef[3][d] + c_s2.cmap[3][k][d] * q[k];
     return isfinite(fw[0]) && isfinite(fw[1]) && isfinite(fw[2]) && isfinite(fw[3]);
 }
 
-// prepared_eval (:247-262)
-__device__ __forceinline__ void s2_eval(const double fw[4], const double coef[4][5], double xi, double& val,
-                                        double& der) {
-    double pw[5], dp[5];
-    pw[0] = 1.0; dp[0] = 0.0;
-#pragma unroll
-    for (int d = 1; d <= 4; ++d) { pw[d] = pw[d - 1] * xi; dp[d] = (double)d * s2_powi(xi, d - 1); }
-    double v = 0.0, dv = 0.0;
-#pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        double cand = 0.0, dcand = 0.0;
-#pragma unroll
-        for (int d = 0; d < 5; ++d) { cand = cand + coef[c][d] * pw[d]; dcand = dcand + coef[c][d] * dp[d]; }
-        v = v + fw[c] * cand;
-        dv = dv + fw[c] * dcand;
-    }
-    val = v;
-    der = dv;
-}
-
-__device__ __forceinline__ double s2_eval_v(const double fw[4], const double coef[4][5], double xi) {
-    double pw[5];
-    pw[0] = 1.0;
-#pragma unroll
-    for (int d = 1; d <= 4; ++d) pw[d] = pw[d - 1] * xi;
-    double v = 0.0;
+// sum_c fw[c] sum_k T[c][k] v[k] over each candidate's stencil samples (prepared_eval, :247-262)
+__device__ __forceinline__ double s2_cand_sum(const double fw[4], const double v[5], const double (*T)[5]) {
+    double r = 0.0;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         double cand = 0.0;
 #pragma unroll
-        for (int d = 0; d < 5; ++d) cand = cand + coef[c][d] * pw[d];
-        v = v + fw[c] * cand;
+        for (int k = (c < 3 ? c : 0); k <= (c < 3 ? c + 2 : 4); ++k) cand = cand + T[c][k] * v[k];
+        r = r + fw[c] * cand;
     }
-    return v;
+    return r;
 }
+__device__ __forceinline__ void s2_at(const S2Weno& w, int p, double& val, double& der) {
+    val = s2_cand_sum(w.fw, w.q, c_s2p.E[p]);
+    der = s2_cand_sum(w.fw, w.q, c_s2p.D[p]);
+}
+__device__ __forceinline__ double s2_at_v(const S2Weno& w, int p) { return s2_cand_sum(w.fw, w.q, c_s2p.E[p]); }
 
-// companion_eval3 (:287-318)
+// companion_eval3 (:287-318): the weights of q applied to the companion samples comp as well
 __device__ __forceinline__ bool s2_companion3(const double q[5], const double comp[5], double val[3], double der[3],
                                               double cval[3]) {
-    double fw[4], coef[4][5], ccoef[4][5];
-    if (!s2_weno_coef(q, fw, coef)) return false;
-#pragma unroll
-    for (int c = 0; c < 4; ++c)
-#pragma unroll
-        for (int d = 0; d < 5; ++d) ccoef[c][d] = 0.0;
-#pragma unroll
-    for (int c = 0; c < 3; ++c)
-#pragma unroll
-        for (int k = c; k <= c + 2; ++k)
-#pragma unroll
-            for (int d = 0; d <= 2; ++d) ccoef[c][d] = ccoef[c][d] + c_s2.cmap[c][k][d] * comp[k];
-#pragma unroll
-    for (int k = 0; k < 5; ++k)
-#pragma unroll
-        for (int d = 0; d <= 4; ++d) ccoef[3][d] = ccoef[3][d] + c_s2.cmap[3][k][d] * comp[k];
+    S2Weno w;
+    if (!s2_weno(q, w)) return false;
     bool ok = true;
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
-        s2_eval(fw, coef, c_s2.gnode[s], val[s], der[s]);
-        cval[s] = s2_eval_v(fw, ccoef, c_s2.gnode[s]);
+        s2_at(w, S2_G0 + s, val[s], der[s]);
+        cval[s] = s2_cand_sum(w.fw, comp, c_s2p.E[S2_G0 + s]);
         ok = ok && isfinite(val[s]) && isfinite(der[s]) && isfinite(cval[s]);
     }
     return ok;
@@ -191,24 +161,25 @@ struct S2Field {
 // s2d1_cell_faces9 / s2d1_cell_faces9_wall (:409-498)
 __device__ bool s2_cell_faces9(const S2Field& F, int i, int j, double face[4][3], double dn[4][3], double dt[4][3],
                                double vol[3][3]) {
-    double xv[5][2], xd[5][2], yv[5][2], yd[5][2], rows[5][3], q[5], fw[4], coef[4][5];
+    double xv[5][2], xd[5][2], yv[5][2], yd[5][2], rows[5][3], q[5];
+    S2Weno ww;
     const int ny = F.ny;
     if (!s2_near_wall(j, ny)) {
         for (int r = -2; r <= 2; ++r) {
 #pragma unroll
             for (int s = -2; s <= 2; ++s) q[s + 2] = F.at(i + s, j + r);
-            if (!s2_weno_coef(q, fw, coef)) return false;
-            s2_eval(fw, coef, -0.5, xv[r + 2][0], xd[r + 2][0]);
-            s2_eval(fw, coef, 0.5, xv[r + 2][1], xd[r + 2][1]);
+            if (!s2_weno(q, ww)) return false;
+            s2_at(ww, S2_XM, xv[r + 2][0], xd[r + 2][0]);
+            s2_at(ww, S2_XP, xv[r + 2][1], xd[r + 2][1]);
 #pragma unroll
-            for (int a = 0; a < 3; ++a) rows[r + 2][a] = s2_eval_v(fw, coef, c_s2.gnode[a]);
+            for (int a = 0; a < 3; ++a) rows[r + 2][a] = s2_at_v(ww, S2_G0 + a);
         }
         for (int r = -2; r <= 2; ++r) {
 #pragma unroll
             for (int s = -2; s <= 2; ++s) q[s + 2] = F.at(i + r, j + s);
-            if (!s2_weno_coef(q, fw, coef)) return false;
-            s2_eval(fw, coef, -0.5, yv[r + 2][0], yd[r + 2][0]);
-            s2_eval(fw, coef, 0.5, yv[r + 2][1], yd[r + 2][1]);
+            if (!s2_weno(q, ww)) return false;
+            s2_at(ww, S2_XM, yv[r + 2][0], yd[r + 2][0]);
+            s2_at(ww, S2_XP, yv[r + 2][1], yd[r + 2][1]);
         }
 #pragma unroll
         for (int s = 0; s < 2; ++s) {
@@ -225,20 +196,20 @@ __device__ bool s2_cell_faces9(const S2Field& F, int i, int j, double face[4][3]
             double a5[5];
 #pragma unroll
             for (int r = 0; r < 5; ++r) a5[r] = rows[r][a];
-            if (!s2_weno_coef(a5, fw, coef)) return false;
+            if (!s2_weno(a5, ww)) return false;
 #pragma unroll
-            for (int b = 0; b < 3; ++b) vol[a][b] = s2_eval_v(fw, coef, c_s2.gnode[b]);
+            for (int b = 0; b < 3; ++b) vol[a][b] = s2_at_v(ww, S2_G0 + b);
         }
     } else {
         const int first = s2_wall_first(j, ny);
         for (int r = 0; r < 5; ++r) {
 #pragma unroll
             for (int s = -2; s <= 2; ++s) q[s + 2] = F.at(i + s, first + r);
-            if (!s2_weno_coef(q, fw, coef)) return false;
-            s2_eval(fw, coef, -0.5, xv[r][0], xd[r][0]);
-            s2_eval(fw, coef, 0.5, xv[r][1], xd[r][1]);
+            if (!s2_weno(q, ww)) return false;
+            s2_at(ww, S2_XM, xv[r][0], xd[r][0]);
+            s2_at(ww, S2_XP, xv[r][1], xd[r][1]);
 #pragma unroll
-            for (int a = 0; a < 3; ++a) rows[r][a] = s2_eval_v(fw, coef, c_s2.gnode[a]);
+            for (int a = 0; a < 3; ++a) rows[r][a] = s2_at_v(ww, S2_G0 + a);
         }
         for (int r = -2; r <= 2; ++r) {
 #pragma unroll
@@ -290,12 +261,13 @@ __device__ bool s2_side3(const S2Field& F, int axis, int cell, int tangent, doub
         for (int a = 0; a < 3; ++a) { val[a] = f[slot][a]; dn[a] = n[slot][a]; dt[a] = t[slot][a]; }
         return true;
     }
-    double nv5[5], nd5[5], q[5], fw[4], coef[4][5];
+    double nv5[5], nd5[5], q[5];
+    S2Weno ww;
     for (int r = -2; r <= 2; ++r) {
 #pragma unroll
         for (int s = -2; s <= 2; ++s) q[s + 2] = axis == 0 ? F.at(cell + s, tangent + r) : F.at(tangent + r, cell + s);
-        if (!s2_weno_coef(q, fw, coef)) return false;
-        s2_eval(fw, coef, side, nv5[r + 2], nd5[r + 2]);
+        if (!s2_weno(q, ww)) return false;
+        s2_at(ww, side < 0.0 ? S2_XM : S2_XP, nv5[r + 2], nd5[r + 2]);
     }
     return s2_companion3(nv5, nd5, val, dt, dn);
 }
@@ -306,22 +278,23 @@ __device__ bool s2_cell9(const S2Field& F, int i, int j, double val[3][3]) {
         double f[4][3], n[4][3], t[4][3];
         return s2_cell_faces9(F, i, j, f, n, t, val);
     }
-    double rows[5][3], q[5], fw[4], coef[4][5];
+    double rows[5][3], q[5];
+    S2Weno ww;
     for (int r = -2; r <= 2; ++r) {
 #pragma unroll
         for (int s = -2; s <= 2; ++s) q[s + 2] = F.at(i + s, j + r);
-        if (!s2_weno_coef(q, fw, coef)) return false;
+        if (!s2_weno(q, ww)) return false;
 #pragma unroll
-        for (int a = 0; a < 3; ++a) rows[r + 2][a] = s2_eval_v(fw, coef, c_s2.gnode[a]);
+        for (int a = 0; a < 3; ++a) rows[r + 2][a] = s2_at_v(ww, S2_G0 + a);
     }
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         double a5[5];
 #pragma unroll
         for (int r = 0; r < 5; ++r) a5[r] = rows[r][a];
-        if (!s2_weno_coef(a5, fw, coef)) return false;
+        if (!s2_weno(a5, ww)) return false;
 #pragma unroll
-        for (int b = 0; b < 3; ++b) val[a][b] = s2_eval_v(fw, coef, c_s2.gnode[b]);
+        for (int b = 0; b < 3; ++b) val[a][b] = s2_at_v(ww, S2_G0 + b);
     }
     return true;
 }
@@ -347,19 +320,20 @@ __global__ void __launch_bounds__(128) k_s2_recon1(LoParams P, LoBuffers B, S2Bu
     const int cc = blockIdx.y, i = cc % nx, j = cc / nx;
     if (dir == 1 && s2_near_wall(j, ny)) return;   // walls use one-sided quartics instead
     const S2Field F{(f == 0 ? B.h : B.b) + k, nv, nx, ny};
-    double q[5], fw[4], coef[4][5];
+    double q[5];
+    S2Weno ww;
 #pragma unroll
     for (int s = -2; s <= 2; ++s) q[s + 2] = dir == 0 ? F.at(i + s, j) : F.at(i, j + s);
-    const bool ok = s2_weno_coef(q, fw, coef);
+    const bool ok = s2_weno(q, ww);
     double* o = S.l1 + ((size_t)cc * 22 + f * 11 + (dir == 0 ? 0 : 7)) * nv + k;
     double v0, d0, v1, d1;
-    s2_eval(fw, coef, -0.5, v0, d0);
-    s2_eval(fw, coef, 0.5, v1, d1);
+    s2_at(ww, S2_XM, v0, d0);
+    s2_at(ww, S2_XP, v1, d1);
     if (kok) {
         o[0] = v0; o[(size_t)nv] = d0; o[2 * (size_t)nv] = v1; o[3 * (size_t)nv] = d1;
         if (dir == 0)
 #pragma unroll
-            for (int a = 0; a < 3; ++a) o[(size_t)(4 + a) * nv] = s2_eval_v(fw, coef, c_s2.gnode[a]);
+            for (int a = 0; a < 3; ++a) o[(size_t)(4 + a) * nv] = s2_at_v(ww, S2_G0 + a);
         if (!ok) set_status(B.status, ST_NONFINITE_FLUX);
     }
 }
@@ -425,10 +399,10 @@ __global__ void __launch_bounds__(256, 3) k_s2_recon2(LoParams P, LoBuffers B, S
 #pragma unroll
         for (int r = 0; r < 5; ++r) a5[r] = X(r, 4 + p);
         if (!nw) {
-            double fw[4], coef[4][5];
-            ok = ok && s2_weno_coef(a5, fw, coef);
+            S2Weno ww;
+            ok = ok && s2_weno(a5, ww);
 #pragma unroll
-            for (int b = 0; b < 3; ++b) vol[b] = s2_eval_v(fw, coef, c_s2.gnode[b]);
+            for (int b = 0; b < 3; ++b) vol[b] = s2_at_v(ww, S2_G0 + b);
         } else {
             double dummy;
 #pragma unroll
@@ -1390,7 +1364,25 @@ cudaError_t prepare_s2() {
     }
     const double g = 0.5 * std::sqrt(3.0 / 5.0);
     m.gnode[0] = -g; m.gnode[1] = 0.0; m.gnode[2] = g;
-    return cudaMemcpyToSymbol(c_s2, &m, sizeof m);
+    // value and derivative weights of every candidate at the 5 evaluation points
+    static S2PointW pw;
+    const double xs[5] = {-0.5, 0.5, m.gnode[0], m.gnode[1], m.gnode[2]};
+    for (int p = 0; p < 5; ++p)
+        for (int c = 0; c < 4; ++c)
+            for (int k = 0; k < 5; ++k) {
+                double e = 0.0, d = 0.0, x = 1.0, xd = 0.0;   // x = xi^d, xd = d xi^(d-1)
+                for (int q = 0; q < 5; ++q) {
+                    e = e + m.cmap[c][k][q] * x;
+                    d = d + m.cmap[c][k][q] * xd;
+                    xd = (double)(q + 1) * x;
+                    x = x * xs[p];
+                }
+                pw.E[p][c][k] = e;
+                pw.D[p][c][k] = d;
+            }
+    cudaError_t e = cudaMemcpyToSymbol(c_s2, &m, sizeof m);
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(c_s2p, &pw, sizeof pw);
+    return e;
 }
 
 
