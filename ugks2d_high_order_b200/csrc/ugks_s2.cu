@@ -581,7 +581,8 @@ __device__ __forceinline__ double s2_scaled(const double r[4], const double w[4]
 
 struct WClosure {
     double th[4];    // converged (rho, u, v, T_native)
-    double jac[16];  // moment Jacobian at th, row-major (moment r, theta a)
+    double* jac;     // [16] moment Jacobian at th, row-major (moment r, theta a), in the warp's slice of
+                     // shared memory: lane 0 writes it, every lane reads it (it is warp-uniform)
 };
 
 enum { W_TRIAL = 0, W_DONE = 1, W_FAIL = 2 };
@@ -666,8 +667,10 @@ __device__ bool w_closure(const LoParams& P, const LoBuffers& B, const double w[
         if (first ? fin : (fin && (nn < norm || nn <= 5.0e-13))) {   // accept the evaluation
 #pragma unroll
             for (int m = 0; m < 4; ++m) { C.th[m] = trial[m]; res[m] = nres[m]; }
+            if ((threadIdx.x & 31) == 0)
 #pragma unroll
-            for (int m = 0; m < 16; ++m) C.jac[m] = acc[m];
+                for (int m = 0; m < 16; ++m) C.jac[m] = acc[m];
+            __syncwarp();
             norm = nn;
             iter = first ? 1 : iter + 1;
             act = w_newton_next(true, C, res, norm, iter, step, alpha, trial);
@@ -793,10 +796,12 @@ __global__ void __launch_bounds__(256, 2) k_s2_init(LoParams P, LoBuffers B, S2B
     const int nv = P.nvel, nc = P.nx * P.ny, lane = threadIdx.x & 31, nr = (nv + 31) >> 5;
     const int cc = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (cc >= nc) return;
+    __shared__ double s_jac[8][16];
     double w[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) w[m] = B.W[cc * 4 + m];
     WClosure C;
+    C.jac = s_jac[threadIdx.x >> 5];
     WMke M;
     const bool ok = w_closure(P, B, w, C) && w_make_mke(P, B, w, C, M);
     const S2Th tt = s2_th(C.th, P.ck);
@@ -861,10 +866,12 @@ __global__ void __launch_bounds__(256, 2) k_s2_target_nodes(LoParams P, LoBuffer
     const int nc = P.nx * P.ny, lane = threadIdx.x & 31;
     const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (wid >= nc * 9) return;
+    __shared__ double s_jac[8][16];
     double w[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) w[m] = SB.wq[(size_t)wid * 4 + m];
     WClosure C;
+    C.jac = s_jac[threadIdx.x >> 5];
     WMke M;
     const bool ok = w_closure(P, B, w, C) && w_make_mke(P, B, w, C, M);
     if (lane == 0) {
@@ -930,7 +937,9 @@ __global__ void __launch_bounds__(256, 2) k_s2_face_nodes(LoParams P, LoBuffers 
     }
     warp_sum_all<4>(acc);
     const double w0[4] = {acc[0], acc[1], acc[2], acc[3]};
+    __shared__ double s_jac[8][16];
     WClosure C;
+    C.jac = s_jac[threadIdx.x >> 5];
     WMke M;
     bool ok = w_closure(P, B, w0, C) && w_make_mke(P, B, w0, C, M);
     double q0x = 0.0, q0y = 0.0, tdl[4], tdr[4], tdt[4], tdm[4], wt[4], mt[5];
@@ -1135,7 +1144,9 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
     const double wg[4] = {prim_g[0], 0.0, -prim_g[0] * ux, prim_g[0] * ((double)(ck + 2) / (4.0 * lambda) + 0.5 * ux * ux)};
     // wall_equilibrium: the discrete closure of the wall state
     const double wwall[4] = {prim_g[0], prim_g[0] * ux, 0.0, prim_g[0] * ((double)(ck + 2) * theta / 2.0 + ux * ux / 2.0)};
+    __shared__ double s_jac[8][16];
     WClosure C;
+    C.jac = s_jac[threadIdx.x >> 5];
     bool ok = pp > 0.0 && isfinite(pp) && w_closure(P, B, wwall, C);
     auto rec = [&](const WVel& s, int field) {
         return SB.rec[((size_t)cc * 72 + field * 12 + sidx * 3 + g) * nv + s.k];
