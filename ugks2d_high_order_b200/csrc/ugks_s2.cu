@@ -11,7 +11,9 @@
 //                       positivity limiter (mod_S2D1Reconstruction.f90, limit_cell_outputs
 //                       mod_S2D1.f90:315-345): the shared first layer, then per cell the second-layer
 //                       templates and the limiter; writes the face cache.
-//   k_s2_face_nodes   : ugks_node (mod_S2D1.f90:421-521) at one Gauss node of one interior face per warp.
+//   k_s2_face_nodes   : ugks_node (mod_S2D1.f90:421-521) at one Gauss node of one interior face per warp:
+//                       closure, directions and time coefficients -> node scalars.
+//   k_s2_face_flux    : the node's micro flux from those scalars, one CTA per face node.
 //   k_s2_wall_nodes   : the multiscale diffuse wall node (s2w2_wall_node, mod_S2MultiscaleWall.f90:45-184)
 //                       per warp.
 //   k_s2_combine      : the Gauss-weighted node fluxes times the face length into the face arrays.
@@ -906,9 +908,13 @@ __global__ void __launch_bounds__(256) k_s2_target_sum(LoParams P, LoBuffers B, 
 }
 
 // ------------------------------------------------------------------------------------------
-// interior face nodes (ugks_node, mod_S2D1.f90:421-521): one warp per (face, Gauss node); the
-// right x face of every cell, then the top y face of every cell below the last row.  The node's
-// micro flux goes to SB.node[face][node][h|b][nvel] and its macro flux to SB.nodew.
+// interior face nodes (ugks_node, mod_S2D1.f90:421-521), scalar part: one warp per (face, Gauss
+// node) -- the right x face of every cell, then the top y face of every cell below the last row --
+// computes W0, the closure, make_mke, q0, the slope and time directions and Mt, and stores them as
+// the node's scalars (SB.fscal) for k_s2_face_flux.
+constexpr int kS2FScal = 48;   // [0] ok, [1..4] theta, [5..12] K directions, [13..16] ux vy lam coeff,
+                               // [17..18] q0, [19..34] left/right/tangential/time directions, [35..39] Mt,
+                               // [40..43] the time-direction moments wt
 __global__ void __launch_bounds__(256, 2) k_s2_face_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
     if (eval_cached(B)) return;
     const int nv = P.nvel, nx = P.nx, ny = P.ny, ck = P.ck, lane = threadIdx.x & 31, nr = (nv + 31) >> 5;
@@ -1006,48 +1012,104 @@ __global__ void __launch_bounds__(256, 2) k_s2_face_nodes(LoParams P, LoBuffers 
         mt[1] = -tau * mt[0] + mt[4];
         mt[2] = 0.5 * dt * dt - tau * mt[0];
     }
-    if (ok) {   // node fluxes
-        double* outh = SB.node + (size_t)wid * 2 * nv;
-        double* outb = outh + nv;
+    // the node scalars of the flux pass (k_s2_face_flux)
+    if (lane == 0) {
+        double* o = SB.fscal + (size_t)wid * kS2FScal;
+        o[0] = ok ? 1.0 : 0.0;
+        if (ok) {
 #pragma unroll
-        for (int m = 0; m < 8; ++m) acc[m] = 0.0;
-        const S2Th tt = s2_th(C.th, ck);
-        for (int r = 0; r < nr; ++r) {
-            const WVel s = wvel(B, nv, r);
-            S2Q q;
-            double mh, mb, kxh, kxb, kyh, kyb;
-            w_mke_at(tt, M, ck, s.u, s.v, q, mh, mb, kxh, kxb, kyh, kyb);
-            const double s0h = mh + kxh * q0x + kyh * q0y;
-            const double s0b = mb + kxb * q0x + kyb * q0y;
-            double dlh, dlb, drh, drb, dth, dtb, mth, mtb;
-            s2_dq(q, tdl, dlh, dlb);
-            s2_dq(q, tdr, drh, drb);
-            s2_dq(q, tdt, dth, dtb);
-            s2_dq(q, tdm, mth, mtb);
-            moment_add(s.w, s.u, s.v, mth, mtb, acc);
-            const double vn = axis == 0 ? s.u : s.v, vt = axis == 0 ? s.v : s.u;
-            const double sh = vn * (vn >= 0.0 ? dlh : drh) + vt * dth;
-            const double sb = vn * (vn >= 0.0 ? dlb : drb) + vt * dtb;
-            const double f0h = upwind(s, 0), f0b = upwind(s, 1), nh = upwind(s, 2), th_ = upwind(s, 3);
-            const double nb = upwind(s, 4), tb_ = upwind(s, 5);
-            const double fhv = vn * (mt[0] * s0h + mt[1] * sh + mt[2] * mth + mt[3] * f0h - mt[4] * (vn * nh + vt * th_));
-            const double fbv = vn * (mt[0] * s0b + mt[1] * sb + mt[2] * mtb + mt[3] * f0b - mt[4] * (vn * nb + vt * tb_));
-            moment_add(s.w, s.u, s.v, fhv, fbv, acc + 4);
-            if (s.ok) {
-                outh[s.k] = fhv;
-                outb[s.k] = fbv;
-                ok = ok && isfinite(fhv) && isfinite(fbv);
+            for (int m = 0; m < 4; ++m) {
+                o[1 + m] = C.th[m]; o[5 + m] = M.tdx[m]; o[9 + m] = M.tdy[m];
+                o[19 + m] = tdl[m]; o[23 + m] = tdr[m]; o[27 + m] = tdt[m]; o[31 + m] = tdm[m]; o[40 + m] = wt[m];
             }
-        }
-        warp_sum_all<8>(acc);
-        double mx = 0.0, sc = 1.0;
+            o[13] = M.ux; o[14] = M.vy; o[15] = M.lam; o[16] = M.coeff; o[17] = q0x; o[18] = q0y;
 #pragma unroll
-        for (int m = 0; m < 4; ++m) { mx = fmax(mx, fabs(acc[m] - wt[m])); sc = fmax(sc, fabs(wt[m])); }
-        ok = ok && mx / sc <= 2.0e-12;
-        if (lane < 4) SB.nodew[(size_t)wid * 4 + lane] = lane == 0 ? acc[4] : (lane == 1 ? acc[5] : (lane == 2 ? acc[6] : acc[7]));
+            for (int m = 0; m < 5; ++m) o[35 + m] = mt[m];
+        } else {
+            set_status(B.status, ST_NONFINITE_FLUX);
+        }
     }
-    ok = __all_sync(0xffffffffu, ok);
-    if (!ok && lane == 0) set_status(B.status, ST_NONFINITE_FLUX);
+}
+
+// ugks_node's flux at one face Gauss node (mod_S2D1.f90:486-507): one CTA per (face, node), VPT
+// velocities per thread, from the node scalars; the node micro flux goes to SB.node, its moments to
+// SB.nodew, and the time-direction moment gate (2e-12) is checked on the block-reduced moments.
+template <int VPT>
+__global__ void __launch_bounds__(256) k_s2_face_flux(LoParams P, LoBuffers B, S2Buffers SB) {
+    if (eval_cached(B)) return;
+    __shared__ double sc[kS2FScal];
+    __shared__ double red[8 * 8];
+    __shared__ double rout[kRedSlots];
+    const int nv = P.nvel, nx = P.nx, ny = P.ny, ck = P.ck;
+    const int nfx = nx * ny;
+    const int wid = blockIdx.x, fi = wid / 3, g = wid % 3;
+    const int axis = fi < nfx ? 0 : 1, f = axis == 0 ? fi : fi - nfx;
+    const int cl = f, i = cl % nx, j = cl / nx;
+    const int cr = axis == 0 ? j * nx + (i + 1) % nx : (j + 1) * nx + i;
+    const int sl = axis == 0 ? 1 : 3, sr = axis == 0 ? 0 : 2;
+    if (threadIdx.x < kS2FScal) sc[threadIdx.x] = SB.fscal[(size_t)wid * kS2FScal + threadIdx.x];
+    __syncthreads();
+    if (sc[0] == 0.0) return;   // the scalars kernel failed (status set there)
+    double th[4], tdl[4], tdr[4], tdt[4], tdm[4], mt[5];
+    WMke M;
+#pragma unroll
+    for (int m = 0; m < 4; ++m) {
+        th[m] = sc[1 + m]; M.tdx[m] = sc[5 + m]; M.tdy[m] = sc[9 + m];
+        tdl[m] = sc[19 + m]; tdr[m] = sc[23 + m]; tdt[m] = sc[27 + m]; tdm[m] = sc[31 + m];
+    }
+    M.ux = sc[13]; M.vy = sc[14]; M.lam = sc[15]; M.coeff = sc[16];
+    const double q0x = sc[17], q0y = sc[18];
+#pragma unroll
+    for (int m = 0; m < 5; ++m) mt[m] = sc[35 + m];
+    const S2Th tt = s2_th(th, ck);
+    double* outh = SB.node + (size_t)wid * 2 * nv;
+    double* outb = outh + nv;
+    double acc[8];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) acc[m] = 0.0;
+    int bad = 0;
+#pragma unroll
+    for (int r = 0; r < VPT; ++r) {
+        const Slot sl_ = slot(r, nv);
+        const int k = sl_.kk;
+        const double uk = B.u[k], vk = B.v[k], wk = sl_.ok ? B.w[k] : 0.0;
+        S2Q q;
+        double mh, mb, kxh, kxb, kyh, kyb;
+        w_mke_at(tt, M, ck, uk, vk, q, mh, mb, kxh, kxb, kyh, kyb);
+        const double s0h = mh + kxh * q0x + kyh * q0y;
+        const double s0b = mb + kxb * q0x + kyb * q0y;
+        double dlh, dlb, drh, drb, dth, dtb, mth, mtb;
+        s2_dq(q, tdl, dlh, dlb);
+        s2_dq(q, tdr, drh, drb);
+        s2_dq(q, tdt, dth, dtb);
+        s2_dq(q, tdm, mth, mtb);
+        moment_add(wk, uk, vk, mth, mtb, acc);
+        const double vn = axis == 0 ? uk : vk, vt = axis == 0 ? vk : uk;
+        const bool left = vn >= 0.0;
+        const double* rc = SB.rec + ((size_t)(left ? cl : cr) * 72 + (left ? sl : sr) * 3 + g) * nv + k;
+        const double f0h = rc[0], f0b = rc[(size_t)12 * nv], nh = rc[(size_t)24 * nv], th_ = rc[(size_t)36 * nv];
+        const double nb = rc[(size_t)48 * nv], tb_ = rc[(size_t)60 * nv];
+        const double sh = vn * (left ? dlh : drh) + vt * dth;
+        const double sb = vn * (left ? dlb : drb) + vt * dtb;
+        const double fhv = vn * (mt[0] * s0h + mt[1] * sh + mt[2] * mth + mt[3] * f0h - mt[4] * (vn * nh + vt * th_));
+        const double fbv = vn * (mt[0] * s0b + mt[1] * sb + mt[2] * mtb + mt[3] * f0b - mt[4] * (vn * nb + vt * tb_));
+        moment_add(wk, uk, vk, fhv, fbv, acc + 4);
+        if (sl_.ok) {
+            outh[sl_.k] = fhv;
+            outb[sl_.k] = fbv;
+            if (!(isfinite(fhv) && isfinite(fbv))) bad = 1;
+        }
+    }
+    block_reduce_smem<8, 0>(acc, red, rout);
+    bad = __syncthreads_or(bad);
+    if (threadIdx.x == 0) {
+        double mx = 0.0, scl = 1.0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { mx = fmax(mx, fabs(rout[m] - sc[40 + m])); scl = fmax(scl, fabs(sc[40 + m])); }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) SB.nodew[(size_t)wid * 4 + m] = rout[4 + m];
+        if (bad || !(mx / scl <= 2.0e-12)) set_status(B.status, ST_NONFINITE_FLUX);
+    }
 }
 
 // ------------------------------------------------------------------------------------------
@@ -1438,6 +1500,11 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     if (e == cudaSuccess) { k_s2_wall_nodes<<<warps(2LL * nx * 3), 256, 0, s2>>>(P, B, S); e = cudaGetLastError(); }
     if (e == cudaSuccess) e = cudaEventRecord(join, s2);
     if (e == cudaSuccess) { k_s2_face_nodes<<<warps((long long)nf * 3), 256, 0, s>>>(P, B, S); e = cudaGetLastError(); }
+    if (e == cudaSuccess) {
+        if (nv <= 1024) k_s2_face_flux<4><<<(unsigned)(nf * 3), 256, 0, s>>>(P, B, S);
+        else k_s2_face_flux<10><<<(unsigned)(nf * 3), 256, 0, s>>>(P, B, S);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
     if (e == cudaSuccess) {
         k_s2_combine<<<dim3((unsigned)((nv + 255) / 256), (unsigned)(nf + 2 * nx)), 256, 0, s>>>(P, B, S);

@@ -25,13 +25,14 @@ struct S2Buffers {
     double* wq;      // [cell][9][4] mean-shifted volume node states
     double* tscal;   // [cell][9][16] volume node scalars (closure theta, directions, primitive)
     double* l1;      // [cell][22][nvel] first-layer WENO values of h and b (k_s2_recon1)
+    double* fscal;   // [interior face][3][48] face-node scalars (k_s2_face_nodes -> k_s2_face_flux)
 };
 
 // doubles of evaluation scratch one S2Buffers needs, and their layout
 inline size_t s2_scratch_doubles(int nx, int ny, int nv) {
     const size_t nf = (size_t)nx * ny + (size_t)nx * (ny - 1), nfw = nf + 2 * (size_t)nx, nc = (size_t)nx * ny;
     auto r = [](size_t n) { return (n + 31) / 32 * 32; };
-    return r(nfw * 3 * 2 * nv) + r(nfw * 3 * 4) + r(nf * 3 * 12) + r(nc * 9 * 4) + r(nc * 9 * 16) + r(nc * 22 * nv);
+    return r(nfw * 3 * 2 * nv) + r(nfw * 3 * 4) + r(nf * 3 * 12) + r(nc * 9 * 4) + r(nc * 9 * 16) + r(nc * 22 * nv) + r(nf * 3 * 48);
 }
 inline void s2_bind_scratch(S2Buffers& S, double* base, int nx, int ny, int nv) {
     const size_t nf = (size_t)nx * ny + (size_t)nx * (ny - 1), nfw = nf + 2 * (size_t)nx, nc = (size_t)nx * ny;
@@ -41,7 +42,8 @@ inline void s2_bind_scratch(S2Buffers& S, double* base, int nx, int ny, int nv) 
     S.mac = base; base += r(nf * 3 * 12);
     S.wq = base; base += r(nc * 9 * 4);
     S.tscal = base; base += r(nc * 9 * 16);
-    S.l1 = base;
+    S.l1 = base; base += r(nc * 22 * nv);
+    S.fscal = base;
 }
 
 // s2_tau (mod_S2PhysicalGas.f90:9-20): GetTau of (rho, U, V, 0.5 rho / p), p = 2/(ck+2) e
