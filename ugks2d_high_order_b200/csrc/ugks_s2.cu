@@ -817,49 +817,164 @@ __global__ void __launch_bounds__(256, 2) k_s2_init(LoParams P, LoBuffers B, S2B
 }
 
 // ------------------------------------------------------------------------------------------
+// Macro WENO of W in 8-lane groups: the 5 first-layer samples of a template are computed by lanes
+// 0..4 of the group at once and gathered by shuffles, and lane 0 (or lanes 0..2) finish the template.
+//
+// s2d1_side3 with wall_y (:320-354) of one side: normal and tangential derivatives at the 3 Gauss
+// nodes, valid in lane 0 of the group.  Near a wall the x faces take the one-sided quartic across the
+// 5 true rows and the y faces the companion template of the columns' one-sided quartics
+// (s2d1_cell_faces9_wall, :456-499), the same cases s2_side3 takes through s2_cell_faces9.
+__device__ bool s2_side3_group(const S2Field& F, int axis, int cell, int tangent, double side, int gl, double dn[3],
+                               double dt[3]) {
+    const int ny = F.ny, j = axis == 0 ? tangent : cell, base = (threadIdx.x & 31) & ~7;
+    const bool nw = s2_near_wall(j, ny);
+    const int first = nw ? s2_wall_first(j, ny) : 0;
+    double v = 0.0, d = 0.0;
+    bool ok = true;
+    if (gl < 5) {
+        double q[5];
+        if (nw && axis == 1) {   // column tangent + gl - 2, one-sided across the 5 true rows
+#pragma unroll
+            for (int t = 0; t < 5; ++t) q[t] = F.at(tangent + gl - 2, first + t);
+            s2_wall_eval(q, j, ny, side, v, d);
+        } else {
+#pragma unroll
+            for (int s = -2; s <= 2; ++s)
+                q[s + 2] = nw ? F.at(cell + s, first + gl)
+                              : (axis == 0 ? F.at(cell + s, tangent + gl - 2) : F.at(tangent + gl - 2, cell + s));
+            S2Weno ww;
+            ok = s2_weno(q, ww);
+            s2_at(ww, side < 0.0 ? S2_XM : S2_XP, v, d);
+        }
+    }
+    double v5[5], d5[5];
+    int okc = ok ? 1 : 0;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+        v5[r] = __shfl_sync(0xffffffffu, v, base + r);
+        d5[r] = __shfl_sync(0xffffffffu, d, base + r);
+        okc &= __shfl_sync(0xffffffffu, okc, base + r);
+    }
+    ok = okc != 0;
+    if (gl == 0) {
+        if (nw && axis == 0) {
+            double dummy;
+#pragma unroll
+            for (int a = 0; a < 3; ++a) {
+                s2_wall_eval(v5, j, ny, c_s2.gnode[a], dummy, dt[a]);
+                s2_wall_eval(d5, j, ny, c_s2.gnode[a], dn[a], dummy);
+            }
+        } else {
+            double val[3];
+            ok = ok && s2_companion3(v5, d5, val, dt, dn);
+        }
+#pragma unroll
+        for (int a = 0; a < 3; ++a) ok = ok && isfinite(dn[a]) && isfinite(dt[a]);
+    }
+    return ok;
+}
+
+// s2d1_cell9 (:378-403; near a wall the volume part of s2d1_cell_faces9_wall) of one field: lanes
+// 0..2 of the group return vol[gl][0..2]
+__device__ bool s2_cell9_group(const S2Field& F, int i, int j, int gl, double vol[3]) {
+    const int ny = F.ny, base = (threadIdx.x & 31) & ~7;
+    const bool nw = s2_near_wall(j, ny);
+    const int first = nw ? s2_wall_first(j, ny) : j - 2;
+    double rw[3] = {0.0, 0.0, 0.0};
+    bool ok = true;
+    if (gl < 5) {   // the x first layer of row first + gl at the 3 Gauss nodes
+        double q[5];
+#pragma unroll
+        for (int s = -2; s <= 2; ++s) q[s + 2] = F.at(i + s, first + gl);
+        S2Weno ww;
+        ok = s2_weno(q, ww);
+#pragma unroll
+        for (int a = 0; a < 3; ++a) rw[a] = s2_at_v(ww, S2_G0 + a);
+    }
+    double rows[5][3];
+    int okc = ok ? 1 : 0;
+#pragma unroll
+    for (int r = 0; r < 5; ++r) {
+#pragma unroll
+        for (int a = 0; a < 3; ++a) rows[r][a] = __shfl_sync(0xffffffffu, rw[a], base + r);
+        okc &= __shfl_sync(0xffffffffu, okc, base + r);
+    }
+    ok = okc != 0;
+    if (gl < 3) {
+        double a5[5];
+#pragma unroll
+        for (int r = 0; r < 5; ++r) a5[r] = rows[r][gl];
+        if (!nw) {
+            S2Weno ww;
+            ok = ok && s2_weno(a5, ww);
+#pragma unroll
+            for (int b = 0; b < 3; ++b) vol[b] = s2_at_v(ww, S2_G0 + b);
+        } else {
+            double dummy;
+#pragma unroll
+            for (int b = 0; b < 3; ++b) s2_wall_eval(a5, j, ny, c_s2.gnode[b], vol[b], dummy);
+        }
+    }
+    return ok;
+}
+
 // macro WENO of W: per interior face and component the normal slopes of both sides and the
 // tangential slope at the 3 Gauss nodes (s2d1_face3, compute_flux :803-808,849-854), and per cell
 // and component the 3x3 Gauss values and the mean-shifted volume node states (build_targets
-// :1270-1279).  One thread per (face, component) and per (cell, component).
+// :1270-1279).  Faces: 2 warps per face, an 8-lane group per (component, side); cells: one warp per
+// cell, an 8-lane group per component.
 __global__ void __launch_bounds__(128) k_s2_macro(LoParams P, LoBuffers B, S2Buffers SB, int faces, int cells) {
     if (eval_cached(B)) return;
     const int nx = P.nx, ny = P.ny, nfx = nx * ny, nf = nfx + nx * (ny - 1), nc = nx * ny;
-    int t = (int)(blockIdx.x * blockDim.x + threadIdx.x);
-    const int nft = faces ? nf * 4 : 0;
-    if (t < nft) {
-        int f = t >> 2;
-        const int m = t & 3, fi = f, axis = f < nfx ? 0 : 1;
-        if (axis == 1) f -= nfx;
+    int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
+    const int lane = threadIdx.x & 31, grp = lane >> 3, gl = lane & 7;
+    const int nfw = faces ? nf * 2 : 0;
+    if (wid < nfw) {
+        const int fi = wid >> 1, m = (wid & 1) * 2 + (grp >> 1), right = grp & 1;
+        const int axis = fi < nfx ? 0 : 1, f = axis == 0 ? fi : fi - nfx;
         const int i = f % nx, j = f / nx;
         const S2Field F{B.W + m, 4, nx, ny};
-        double vl[3], vr[3], nl[3], nr[3], tl[3], tr[3];
+        double dn[3] = {0.0, 0.0, 0.0}, dt[3] = {0.0, 0.0, 0.0};
         bool ok;
-        if (axis == 0) ok = s2_side3(F, 0, i, j, 0.5, vl, nl, tl) && s2_side3(F, 0, (i + 1) % nx, j, -0.5, vr, nr, tr);
-        else ok = s2_side3(F, 1, j, i, 0.5, vl, nl, tl) && s2_side3(F, 1, j + 1, i, -0.5, vr, nr, tr);
-        if (!ok) set_status(B.status, ST_NONFINITE_FLUX);
-        const double dn = axis == 0 ? P.dx : P.dy, dtg = axis == 0 ? P.dy : P.dx;
+        if (axis == 0) ok = s2_side3_group(F, 0, right ? (i + 1) % nx : i, j, right ? -0.5 : 0.5, gl, dn, dt);
+        else ok = s2_side3_group(F, 1, right ? j + 1 : j, i, right ? -0.5 : 0.5, gl, dn, dt);
+        // the right side's tangential derivatives to the left side's lane 0
+        double tr[3];
 #pragma unroll
-        for (int g = 0; g < 3; ++g) {
-            double* o = SB.mac + (size_t)(fi * 3 + g) * 12;
-            o[m] = nl[g] / dn;
-            o[4 + m] = nr[g] / dn;
-            o[8 + m] = 0.5 * (tl[g] + tr[g]) / dtg;
+        for (int g = 0; g < 3; ++g) tr[g] = __shfl_down_sync(0xffffffffu, dt[g], 8);
+        if (gl == 0) {
+            if (!ok) set_status(B.status, ST_NONFINITE_FLUX);
+            const double dnrm = axis == 0 ? P.dx : P.dy, dtg = axis == 0 ? P.dy : P.dx;
+#pragma unroll
+            for (int g = 0; g < 3; ++g) {
+                double* o = SB.mac + (size_t)(fi * 3 + g) * 12;
+                o[(right ? 4 : 0) + m] = dn[g] / dnrm;
+                if (!right) o[8 + m] = 0.5 * (dt[g] + tr[g]) / dtg;
+            }
         }
         return;
     }
-    t -= nft;
-    if (!cells || t >= nc * 4) return;
-    const int cc = t >> 2, m = t & 3, i = cc % nx, j = cc / nx;
+    wid -= nfw;
+    if (!cells || wid >= nc) return;
+    const int cc = wid, m = grp, i = cc % nx, j = cc / nx;
     const S2Field F{B.W + m, 4, nx, ny};
+    double vol[3] = {0.0, 0.0, 0.0};
+    const bool ok = s2_cell9_group(F, i, j, gl, vol);
+    if (__any_sync(0xffffffffu, !ok) && lane == 0) set_status(B.status, ST_PROJECTION);
+    // nodes[a][c] = vol of lane a, entry c; the mean over the 9 nodes in the reference's order
+    const int base = lane & ~7;
     double nodes[3][3];
-    if (!s2_cell9(F, i, j, nodes)) set_status(B.status, ST_PROJECTION);
+#pragma unroll
+    for (int a = 0; a < 3; ++a)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) nodes[a][c] = __shfl_sync(0xffffffffu, vol[c], base + a);
     const double gw[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
     double avg = 0.0;
     for (int c = 0; c < 3; ++c)
         for (int a = 0; a < 3; ++a) avg = avg + gw[a] * gw[c] * nodes[a][c];
     const double wc = B.W[cc * 4 + m];
-    for (int c = 0; c < 3; ++c)
-        for (int a = 0; a < 3; ++a) SB.wq[((size_t)cc * 9 + c * 3 + a) * 4 + m] = nodes[a][c] + wc - avg;
+    if (gl < 3)
+        for (int c = 0; c < 3; ++c) SB.wq[((size_t)cc * 9 + c * 3 + gl) * 4 + m] = nodes[gl][c] + wc - avg;
 }
 
 // build_targets, closure part: one warp per (cell, volume node) -> the node scalars
@@ -1470,8 +1585,8 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
         return cudaGetLastError();
     }
     const int faces = which != 3, targets = which != 2;
-    const long long nmac = (faces ? (long long)nf * 4 : 0) + (targets ? (long long)nc * 4 : 0);
-    k_s2_macro<<<(unsigned)((nmac + 127) / 128), 128, 0, s>>>(P, B, S, faces, targets);
+    const long long nmacw = (faces ? (long long)nf * 2 : 0) + (targets ? (long long)nc : 0);   // warps
+    k_s2_macro<<<(unsigned)((nmacw * 32 + 127) / 128), 128, 0, s>>>(P, B, S, faces, targets);
     cudaError_t e = cudaGetLastError();
     // which 1: the targets need only the macro pass and are first read after the face combine, so
     // they run on the side stream beside the reconstruction and the face nodes (the wall nodes
