@@ -340,8 +340,8 @@ cudaError_t enqueue_s2cn2_step(const LoParams& P, const LoBuffers& B, const S2Bu
     cudaError_t e = launch_lo_timestep(P, B, s);
     if (e == cudaSuccess) e = s2_enqueue(2, P, B, T, s, s2, fork, join);
     if (e == cudaSuccess) {
-        if (P.nvel <= 1024) e = cn_launch<2, 512>(P, B, T, Bo, To, C, s);
-        else e = cn_launch<5, 512>(P, B, T, Bo, To, C, s);
+        if (P.nvel <= 1024) e = cn_launch<4, 256>(P, B, T, Bo, To, C, s);
+        else e = cn_launch<10, 256>(P, B, T, Bo, To, C, s);
     }
     if (launches) *launches += 7;
     return e;
