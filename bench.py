@@ -279,7 +279,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--sampler", default="nvml", choices=["nvml", "smi", "none"],
                     help="clock sampler during the timed region")
-    ap.add_argument("--sampler-period", type=float, default=0.2, help="seconds between clock samples")
+    ap.add_argument("--sampler-period", type=float, default=0.5, help="seconds between clock samples")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference_arm(args)
@@ -546,7 +546,7 @@ def main():
     bcosts = [instance_cost(c, n * n) for c, n in bcases_all]
     bcases, _ = shard(bcases_all, bcosts, rank, world)     # this rank's LPT share (all of it at N=1)
     tables = {n: velocity_table(n) for n in (24, 32, 48)}
-    bt = Batch([(c, tables[n]) for c, n in bcases], device=local, max_streams=16)
+    bt = Batch([(c, tables[n]) for c, n in bcases], device=local, max_streams=32)
     bt.init_freestream()
     k_tuned, tune_ms = bt.tune(steps=2)
     bt.init_freestream()

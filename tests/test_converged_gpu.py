@@ -96,3 +96,25 @@ def test_high_order_implicit_reaches_reference_limit_state(velocity, golden):
                 assert abs(aero[row, col] - r[q]) <= 1e-7 * abs(r[q]), (w, q, aero[row, col], r[q])
     finally:
         s.close()
+
+
+@pytest.mark.gpu
+def test_repeated_solves_on_one_context_are_identical(velocity):
+    """Two cold-start ImplicitSteady solves to the five-state gate on one context (as bench.py runs
+    them): the second sees none of the first's stop state and reproduces it bitwise."""
+    from ugks2d_high_order_b200.solver import Solver
+    s = Solver(reference_case("ImplicitSteady"), *velocity)
+    try:
+        out = []
+        for _ in range(2):
+            s.init_freestream()
+            s.implicit_init()
+            done, conv, rep = s.step_implicit(3000)
+            assert conv
+            out.append((done, rep.copy(), s.download()))
+        assert out[0][0] == out[1][0]
+        assert np.array_equal(out[0][1], out[1][1])
+        for x, y in zip(out[0][2], out[1][2]):
+            assert np.array_equal(x, y)
+    finally:
+        s.close()

@@ -243,7 +243,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
                 I.s2.kxb = m + i_tg[3]; I.s2.kyh = m + i_tg[4]; I.s2.kyb = m + i_tg[5];
                 s2_bind_scratch(I.s2, m + i_scr, nx, ny, nv);
             }
-            I.mask = c->iflags; I.counter = c->iflags + 2;
+            I.mask = c->iflags; I.counter = c->iflags + 2; I.stopw = c->iflags + 3;
         }
     }
     if (e == cudaSuccess && p->method == UGKS_METHOD_S2CN2) {
@@ -665,11 +665,14 @@ extern "C" int ugks_implicit_steps(ugks_ctx* c, int max_steps, int* steps_done, 
             c->launches += n;
             left -= 1;
         } else if (left >= G) {
+            // up to 4 graphs per readback of the stop flag: after a stop the queued steps' kernels
+            // return at entry, so the state and the counts are those of the stopping step
             int r = build_implicit_graph(c, G);
             if (r) return r;
-            UGKS_CK(cudaGraphLaunch(c->igraph, c->stream));
-            c->launches += c->igraph_launches;
-            left -= G;
+            const int ng = left / G < 4 ? left / G : 4;
+            for (int q = 0; q < ng; ++q) UGKS_CK(cudaGraphLaunch(c->igraph, c->stream));
+            c->launches += c->igraph_launches * ng;
+            left -= G * ng;
         } else {
             long long n = 0;
             for (int s = 0; s < left; ++s)

@@ -121,6 +121,7 @@ __device__ __forceinline__ int alpha_levels(double min_alpha) {
 __device__ __forceinline__ void stop_with(const ImBuffers& I, unsigned* status, unsigned bit) {
     set_status(status, bit);
     I.state[IS_STOP] = 1.0;
+    *I.stopw = 1u;
 }
 
 // Wall frame of ComputeDiffuseWallFaceDelta: top = wall above row ny-1 (normal +y), else bottom.
@@ -237,7 +238,7 @@ __device__ void im_residual_epilogue(const LoParams& P, const LoBuffers& B, cons
     I.state[IS_STREAK] = streak;
     I.state[IS_STEPS] = I.state[IS_STEPS] + 1.0;
     const bool done = Q.mass_rescale ? streak >= 5.0 : pass;
-    if (done) { I.state[IS_CONVERGED] = 1.0; I.state[IS_STOP] = 1.0; }
+    if (done) { I.state[IS_CONVERGED] = 1.0; I.state[IS_STOP] = 1.0; *I.stopw = 1u; }
     rep[0] = pass ? 1.0 : 0.0;
     rep[1] = moment;
     rep[2] = g[14];
@@ -1267,6 +1268,7 @@ __global__ void k_im_init(LoParams P, LoBuffers B, ImParams Q, ImBuffers I) {
         I.state[IS_ALPHA] = 1.0;
         I.state[IS_MALPHA] = 1.0;
         *I.counter = 0u;
+        *I.stopw = 0u;
     }
     for (int k = threadIdx.x; k < P.nvel; k += blockDim.x) {
         for (int w = 0; w < 2; ++w) {
@@ -1362,10 +1364,12 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     };
     // The pre-update evaluation reuses the previous accepted-state evaluation when the state and dt
     // are unchanged since (dt is set by the velocity-table extent unless a cell outruns it).
-    LoBuffers Bpre = B;
+    LoBuffers Bh = B;          // the evaluation kernels return at entry once the sequence has stopped
+    Bh.halt = I.stopw;
+    LoBuffers Bpre = Bh;
     Bpre.eval = I.state + IS_EVAL_VALID;
     cudaError_t e = mark(cudaSuccess);
-    if (e == cudaSuccess) e = mark(launch_lo_timestep(P, B, s));                 // TimeStep
+    if (e == cudaSuccess) e = mark(launch_lo_timestep(P, Bh, s));                // TimeStep
     if (e == cudaSuccess)                                                         // Interpolation + Evolution
         e = Q.high_order ? s2_enqueue(1, P, Bpre, I.s2, s, s2, fork, join) : im_fluxes(P, Bpre, s, s2, fork, join);
     if (e == cudaSuccess) e = mark(im_cell(0, P, Bpre, Q, I, nullptr, s));       // ComputeResidual + diagnostics
@@ -1393,7 +1397,7 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     if (e == cudaSuccess) e = mark(im_cell(5, P, B, Q, I, nullptr, s));          // update + RecoverMacro
     if (e == cudaSuccess) { k_im_rescale<<<148 * 4, 256, 0, s>>>(P, B, Q, I); e = mark(cudaGetLastError()); }
     if (e == cudaSuccess)                                                         // accepted-state evaluation
-        e = mark(Q.high_order ? s2_enqueue(1, P, B, I.s2, s, s2, fork, join) : im_fluxes(P, B, s, s2, fork, join));
+        e = mark(Q.high_order ? s2_enqueue(1, P, Bh, I.s2, s, s2, fork, join) : im_fluxes(P, Bh, s, s2, fork, join));
     if (e == cudaSuccess) e = mark(im_cell(1, P, B, Q, I, nullptr, s));
     if (launches) *launches += 16 + Q.macro_sweeps + (Q.high_order ? 2 : 0);
     return e;

@@ -75,6 +75,8 @@ struct ImBuffers {
     S2Buffers s2;           // high-order volume targets and reconstruction cache (HighOrderImplicit)
     unsigned* mask;         // [2] admissible macro / micro alpha bitmasks (bit m: alpha = 2^-m)
     unsigned* counter;      // [1] last-CTA counter of the implicit kernels
+    unsigned* stopw;        // [1] nonzero once the stop flag is set: the evaluation kernels of the step
+                            // sequence see it through LoBuffers::halt and return at entry
 };
 
 }  // namespace ugks
