@@ -657,7 +657,19 @@ __device__ __forceinline__ int pr_neighbour(int i, int jl, int j, int f, int row
     return j == ny - 1 ? -1 : (jl < rows - 1 ? cl + nx : ncs + 2 * rows + nx + i);
 }
 
-__global__ void k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I, const double* X, double* Y) {
+// Barrier of the wavefront warps alone (named barrier 1); the other warps of the CTA only fill
+// and drain the slab's shared memory and meet the wavefront at barrier 0 afterwards.
+__device__ __forceinline__ void pr_wave_sync(int warps) {
+    if (warps == 1) __syncwarp();
+    else asm volatile("bar.sync 1, %0;" ::"r"(warps * 32) : "memory");
+}
+
+// Launched with kPrThreads threads: all of them stage the slab (about 120 global loads a warp
+// when one warp did it alone), the first 4 x min(dcells, 32) relax.
+constexpr int kPrThreads = 256;
+
+__global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I,
+                                                             const double* X, double* Y) {
     if (I.state[IS_STOP] != 0.0) return;
     extern __shared__ double sm[];
     __shared__ double part[32][4][8];
@@ -672,9 +684,10 @@ __global__ void k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I,
     double* sFi = sG + ncs * 4;       // [ncs][4 faces][4] fixed Euler flux of the cell
     double* sFj = sFi + ncs * 16;     // [ncs][4 faces][4] fixed Euler flux of the neighbour
     double* sD = sFj + ncs * 16;      // [ncs] diagonal
-    const int f = threadIdx.x & 3, tc = threadIdx.x >> 2, D = blockDim.x >> 2;
-    const int wbase = threadIdx.x & ~31, wn = blockDim.x - wbase;
-    const unsigned wmask = wn >= 32 ? 0xffffffffu : ((1u << wn) - 1u);   // lanes of this warp
+    const int dcells = rows < nx ? rows : nx;                  // longest anti-diagonal
+    const int wave = 4 * (dcells < 32 ? dcells : 32);          // relaxing lanes: 4 per cell
+    const int wave_warps = (wave + 31) >> 5;
+    const int f = threadIdx.x & 3, tc = threadIdx.x >> 2, D = wave >> 2;
     const double dtp = B.dt[0] * Q.ncfl / P.cfl;   // PseudoTimeStep (mod_ImplicitCommon.f90:115-119)
     int bad = 0;
     for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) {
@@ -722,14 +735,13 @@ __global__ void k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I,
     const double fny = f == 2 ? -1.0 : (f == 3 ? 1.0 : (f == 1 ? -0.0 : 0.0));
     const double flen = f < 2 ? P.dy : P.dx;
     const double fnxs = f == 3 ? -0.0 : fnx;   // GetFaceGeometry's normals: (-1,0) (1,-0) (0,-1) (-0,1)
-    const int dcells = rows < nx ? rows : nx;
     const int ndiag = rows + nx - 1;
-    for (int pass = 0; pass < 2; ++pass) {
+    for (int pass = 0; pass < 2 && (int)threadIdx.x < wave_warps * 32; ++pass) {
         for (int dd = 0; dd < ndiag; ++dd) {
             const int d = pass == 0 ? dd : ndiag - 1 - dd;
             for (int t0 = 0; t0 < dcells; t0 += D) {
                 int i = 0, jl = 0;
-                const bool act = diag_cell(d, tc + t0, rows, nx, i, jl);
+                const bool act = (int)threadIdx.x < wave && diag_cell(d, tc + t0, rows, nx, i, jl);
                 const int j = s * rows + jl, cl = jl * nx + i;
                 if (act) {   // lane = face f
                     double ti[4], fi[4], fj[4], dnb[4];
@@ -767,7 +779,7 @@ __global__ void k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I,
                         part[tc][f][4 + m] = flen * gam * dnb[m];
                     }
                 }
-                __syncwarp(wmask);
+                __syncwarp();
                 if (act) {   // lane = component m
                     const int m = f;
                     double sdt = 0.0, sgn = 0.0;
@@ -779,7 +791,7 @@ __global__ void k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I,
                     sY[cl * 4 + m] = y;
                     sT[cl * 4 + m] = sW[cl * 4 + m] + y;
                 }
-                __syncwarp(wmask);
+                __syncwarp();
                 if (act && f < 3) {   // lanes 0..2: primitives of the relaxed state
                     double t[4];
 #pragma unroll
@@ -788,9 +800,10 @@ __global__ void k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I,
                     sP[cl * 4 + f] = f == 0 ? e.u : (f == 1 ? e.v : e.p);
                 }
             }
-            __syncthreads();
+            pr_wave_sync(wave_warps);
         }
     }
+    __syncthreads();
     for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) Y[c0 * 4 + q] = sY[q];
     if (__syncthreads_or(bad) && threadIdx.x == 0) stop_with(I, B.status, ST_NONFINITE_STATE);
 }
@@ -1378,10 +1391,9 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     double* Y = I.dwB;
     const int rows = P.ny / Q.nslab, ncs = rows * P.nx;
     const int dcells = rows < P.nx ? rows : P.nx;                              // longest anti-diagonal
-    const int pr_threads = 4 * (dcells < 32 ? dcells : 32);
     const int lu_warps = dcells < 8 ? dcells : 8;
     for (int sw = 0; sw < Q.macro_sweeps && e == cudaSuccess; ++sw) {            // SolveMacroPR2
-        k_im_pr2_sweep<<<Q.nslab, pr_threads, (size_t)pr_smem_words(rows, P.nx) * sizeof(double), s>>>(P, B, Q, I, X, Y);
+        k_im_pr2_sweep<<<Q.nslab, kPrThreads, (size_t)pr_smem_words(rows, P.nx) * sizeof(double), s>>>(P, B, Q, I, X, Y);
         e = cudaGetLastError();
         const double* t = Y; Y = const_cast<double*>(X); X = t;
     }
