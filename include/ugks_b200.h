@@ -135,6 +135,13 @@ int ugks_step_explicit_noalloc(const ugks_params* params, const double* u, const
  * [50..51] reference_h/b, [52] c_minus_1, [53] alpha, [54] macro alpha, [55] dt, [56] streak,
  * [57..78] science of the pre-update evaluation. */
 int ugks_implicit_init(ugks_ctx* ctx);
+/* Resume from a restart (InitFlow_Restart + ReadMassRestart, src/mod_ClosedCouetteMass.f90:352-393, and
+ * the residual-reference inheritance of src/mod_R5Observe.f90:176-186): like ugks_implicit_init but
+ * with the persistent M0 read from closed_mass_rank*.bin instead of the current mass, and, when
+ * have_reference is nonzero, the residual references (reference_h, reference_b) of
+ * residual_reference.in instead of those of the first evaluation.  UGKS_EINVAL if M0 is not finite
+ * and positive or an inherited reference is not finite.  Call after the state is uploaded. */
+int ugks_implicit_restore(ugks_ctx* ctx, double m0, double reference_h, double reference_b, int have_reference);
 int ugks_implicit_steps(ugks_ctx* ctx, int max_steps, int* steps_done, int* converged, double* report);
 /* state[16]: M0, reference_h, reference_b, reference set, mass_scale, streak, stop, steps, alpha,
  * macro alpha, moment error, converged (see ugks_implicit.cuh); report[80] as above. */

@@ -9,7 +9,7 @@ Outputs (all small, committed):
                                 parsed to float64 exactly (18 significant digits in the file).
   mesh_8x64.npy               - gridx, gridy node arrays decoded from cases/*/Mesh2d.dat
                                 (Fortran unformatted, records "9 65" then gridx, gridy).
-  reference_golden.json       - numbers the reference itself printed for this hot path:
+  reference_golden.json       - numbers the reference itself printed for this hot path, and its case inputs:
      * low_explicit 2-step `dtPhysical` and `res:` line  (docs/release_checks/low_explicit/stdout.log)
      * low_implicit / high_implicit sparse_residual.csv rows  (docs/release_checks/*/sparse_residual.csv)
      * the implicit "Implicit iter=2 ..." summary lines        (docs/release_checks/*/stdout.log)
@@ -17,6 +17,9 @@ Outputs (all small, committed):
      * static-equilibrium residual / update maxima             (checks/VERIFICATION.json)
      * end-of-run summaries of the explicit and implicit runs  (docs/couette_results/analysis.json):
        step count, final selected residuals, c_final, per-wall native pnn/pnt/qn
+     * the namelist assignments of cases/*/Config.ini as raw tokens   (case_namelists)
+     * SHA-256 of cases/low_implicit/Mesh2d.dat and the velocity file  (case_file_sha256)
+     * the text lines of docs/release_checks/*/sparse_residual.csv     (sparse_lines)
 """
 import json
 import os
@@ -87,6 +90,29 @@ def parse_profiles(path):
     return zones
 
 
+def namelist_tokens(path):
+    """The assignments of a Config.ini's namelist groups as raw value tokens, comments dropped (the
+    delivered cases put no '!' inside a string and one assignment on a line)."""
+    out, group = {}, None
+    with open(path, encoding="utf-8") as f:
+        for line in f:
+            line = line.split("!")[0].strip()
+            if line.startswith("&"):
+                group = line[1:].strip().lower()
+                out[group] = {}
+            elif line == "/":
+                group = None
+            elif group and "=" in line:
+                k, v = line.split("=", 1)
+                out[group][k.strip()] = v.split()
+    return out
+
+
+def sha256(path):
+    import hashlib
+    return hashlib.sha256(open(path, "rb").read()).hexdigest()
+
+
 def parse_sparse(path):
     with open(path) as f:
         header = f.readline().strip().split(",")
@@ -136,6 +162,12 @@ def main(ref):
         keep["source"] = "docs/couette_results/analysis.json summary/" + case
         golden[case + "_final"] = keep
     golden["velocity_tables"] = parse_velocity_tables(os.path.join(ref, "src/mod_VelocityTables.f90"))
+    golden["case_namelists"] = {c: namelist_tokens(os.path.join(ref, f"cases/{c}/Config.ini"))
+                                for c in ("low_explicit", "low_implicit", "high_implicit")}
+    golden["case_file_sha256"] = {f: sha256(os.path.join(ref, "cases/low_implicit", f))
+                                  for f in ("Mesh2d.dat", "velocity_half32_scale2.dat")}
+    golden["sparse_lines"] = {c: open(os.path.join(ref, f"docs/release_checks/{c}/sparse_residual.csv")).read().splitlines()
+                              for c in ("low_implicit", "high_implicit")}
     with open(os.path.join(HERE, "reference_golden.json"), "w") as f:
         json.dump(golden, f, indent=1)
     print("wrote fixtures to", HERE)

@@ -27,7 +27,7 @@ EXPORTS = [
     "ugks_timestep", "ugks_evolution", "ugks_compute_residual", "ugks_apply_explicit_update",
     "ugks_step_explicit", "ugks_wall_aero", "ugks_macro_fields", "ugks_copy_array", "ugks_last_status", "ugks_status_reference_code",
     "ugks_error_string", "ugks_stream", "ugks_synchronize", "ugks_profile_enable", "ugks_profile_read",
-    "ugks_launch_count", "ugks_step_explicit_noalloc", "ugks_implicit_init", "ugks_implicit_steps",
+    "ugks_launch_count", "ugks_step_explicit_noalloc", "ugks_implicit_init", "ugks_implicit_restore", "ugks_implicit_steps",
     "ugks_implicit_state", "ugks_s2cn2_init", "ugks_s2cn2_steps",
     "ugks_s2cn2_test_reject", "ugks_batch_create", "ugks_batch_destroy", "ugks_batch_init_freestream",
     "ugks_batch_run", "ugks_batch_tune", "ugks_batch_set_streams", "ugks_batch_upload", "ugks_batch_download",
@@ -109,6 +109,7 @@ def load(path=LIB_PATH):
     L.ugks_step_explicit_noalloc.argtypes = [ctypes.POINTER(UgksParams), vp, vp, vp, vp, vp, vp, ctypes.c_int, vp,
                                              dp, dp]
     L.ugks_implicit_init.argtypes = [vp]
+    L.ugks_implicit_restore.argtypes = [vp, ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int]
     L.ugks_implicit_steps.argtypes = [vp, ctypes.c_int, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int), dp]
     L.ugks_implicit_state.argtypes = [vp, dp, dp]
     L.ugks_s2cn2_init.argtypes = [vp]

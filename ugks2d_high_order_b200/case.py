@@ -35,7 +35,7 @@ class CouetteCase:
     residual_tol: float = 1.0e-8     # Implicit_ResidualTol
     moment_tol: float = 1.0e-12      # Implicit_MomentTol
     min_alpha: float = 1.0e-6        # Implicit_MinAlpha
-    max_iter: int = 3000
+    max_iter: int = 3000             # MAX_ITER (the loop cap; 200000 in the explicit case)
 
     @property
     def gamma(self):
@@ -55,6 +55,8 @@ def reference_case(method="Explicit"):
     c = CouetteCase(method=method)
     if method in ("ImplicitSteady", "HighOrderImplicit"):
         c.mass_rescale = True
+    if method == "Explicit":
+        c.max_iter = 200000
     return c
 
 

@@ -617,6 +617,26 @@ extern "C" int ugks_implicit_init(ugks_ctx* c) {
     return collect_status(c);
 }
 
+extern "C" int ugks_implicit_restore(ugks_ctx* c, double m0, double reference_h, double reference_b,
+                                     int have_reference) {
+    if (!c) return UGKS_EINVAL;
+    if (!c->imem) return UGKS_EUNSUPPORTED;
+    // ValidMass (finite, positive) for M0; the references must be finite when inherited
+    if (!(std::isfinite(m0) && m0 > 0.0)) return UGKS_EINVAL;
+    if (have_reference && !(std::isfinite(reference_h) && std::isfinite(reference_b))) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    UGKS_CK(launch_im_init(c->P, c->B, c->Q, c->I, c->stream));
+    c->launches += 1;
+    static_assert(IS_REF_H == IS_M0 + 1 && IS_REF_B == IS_M0 + 2 && IS_REF_INIT == IS_M0 + 3,
+                  "M0 and the residual references are contiguous state words");
+    const double v[4] = {m0, have_reference ? reference_h : 0.0, have_reference ? reference_b : 0.0,
+                         have_reference ? 1.0 : 0.0};
+    UGKS_CK(cudaMemcpyAsync(c->I.state + IS_M0, v, sizeof v, cudaMemcpyHostToDevice, c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    c->implicit_ready = true;
+    return collect_status(c);
+}
+
 static int build_implicit_graph(ugks_ctx* c, int steps) {
     if (c->igraph && c->igraph_steps == steps) return UGKS_OK;
     if (c->igraph) { cudaGraphExecDestroy(c->igraph); c->igraph = nullptr; }

@@ -2,6 +2,11 @@
 
     python -m ugks2d_high_order_b200.driver --method Explicit --steps 200 [--cfl 0.5 --omega 0.81]
     python -m ugks2d_high_order_b200.driver --method S2CN2 --steps 20 [--nvel 48 --ny 128]
+    python -m ugks2d_high_order_b200.driver --case-dir CASE [--out DIR] [--steps N]
+
+The last form runs a reference case directory unchanged (Config.ini, Mesh2d.dat, velocity file;
+restart files when Iflag_InitFlow = 2) and writes sparse_residual.csv and the restart set
+(ugks2d_high_order_b200.caserun).
 
 Runs the case on cuda:0 and prints the residual line every --show steps, as Write_residuals does
 (src/mod_Solve.f90:427-461).  Also the small, self-contained command used for ncu captures.
@@ -17,14 +22,24 @@ def main(argv=None):
     ap = argparse.ArgumentParser()
     ap.add_argument("--method", default="Explicit",
                     choices=["Explicit", "ImplicitSteady", "HighOrderImplicit", "S2CN2"])
-    ap.add_argument("--steps", type=int, default=100)
+    ap.add_argument("--steps", type=int, default=None, help="steps to run (default 100; --case-dir: MAX_ITER)")
     ap.add_argument("--show", type=int, default=100)
     ap.add_argument("--cfl", type=float, default=None)
     ap.add_argument("--omega", type=float, default=None)
     ap.add_argument("--ny", type=int, default=None)
     ap.add_argument("--nx", type=int, default=None)
     ap.add_argument("--nvel", type=int, default=32, help="velocities per axis (32: the reference's table)")
+    ap.add_argument("--case-dir", default=None, help="run this reference case directory instead")
+    ap.add_argument("--out", default=None, help="output directory of --case-dir (default: the case directory)")
     a = ap.parse_args(argv)
+    if a.case_dir:
+        from .caserun import run_case_dir
+        t0 = time.perf_counter()
+        done, conv, _ = run_case_dir(a.case_dir, a.out, a.steps, log=lambda m: print(m, flush=True))
+        print(f"{done} steps in {time.perf_counter() - t0:.3f} s" + ("" if conv is None else f", converged={conv}"))
+        return
+    if a.steps is None:
+        a.steps = 100
     case = reference_case(a.method)
     kw = {}
     if a.cfl is not None:

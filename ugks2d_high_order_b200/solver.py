@@ -125,6 +125,13 @@ class Solver:
         """InitializeClosedMass: persistent M0 from the current state, new residual-reference epoch."""
         self._check(self.L.ugks_implicit_init(self.ctx), "InitializeClosedMass")
 
+    def implicit_restore(self, m0, reference=None):
+        """Resume a restarted run: the persistent M0 of closed_mass_rank*.bin and, when given, the
+        (reference_h, reference_b) pair of residual_reference.in instead of a new epoch."""
+        rh, rb = reference if reference is not None else (0.0, 0.0)
+        self._check(self.L.ugks_implicit_restore(self.ctx, float(m0), float(rh), float(rb), int(reference is not None)),
+                    "ReadMassRestart")
+
     def step_implicit(self, max_steps=1):
         """Up to max_steps accepted pseudo-steps; stops when the five-state gate has passed 5 times.
         Returns (steps_done, converged, report) where report is the last accepted state's
