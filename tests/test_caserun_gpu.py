@@ -65,3 +65,27 @@ def test_restart_continues_bitwise(tmp_path, method):
         assert rows[-1] == refio.sparse_row(N2, N1 + N2, rep2, case.mass_rescale)
         m0, _, step = refio.read_mass_restart(b, refio.load_case_dir(b).config, u, w, case.nx, case.ny, len(u))
         assert step == N1 + N2 and m0 > 0.0
+        plt = open(os.path.join(b, "ResidualImplicit.plt")).read().splitlines()
+        assert plt[0] == refio.RESIDUAL_IMPLICIT_HEADER and len(plt) == 1 + N2 // 5
+        assert plt[-1] == refio.residual_implicit_row(N2, rep2, case.ncfl, True, float(plt[-1][12 + 11 * 18 + 8:][:18]))
+
+
+@pytest.mark.gpu
+def test_delivered_implicit_case_runs_to_the_gate(tmp_path):
+    """The delivered low_implicit case directory, run by the driver from the cold start: 1097 accepted
+    states (the reference: 1096), the last five passing the gate, one sparse row per state and the
+    restart set at the end."""
+    from ugks2d_high_order_b200.caserun import run_case_dir
+    case = reference_case("ImplicitSteady")
+    u, v, w = load_velocity_half32()
+    d = str(tmp_path / "low_implicit")
+    refio.write_case_dir(d, case, u, v, w, extra={"Nstep_restart": 100, "Iflag_WriteRestart": 1, "Nstep_show": 100})
+    done, conv, rep = run_case_dir(d, log=lambda m: None)
+    assert conv and done == 1097
+    rows = open(os.path.join(d, "sparse_residual.csv")).read().splitlines()[1:]
+    assert len(rows) == done
+    gate = [float(r.split(",")[3]) for r in rows]
+    assert gate[-5:] == [1.0] * 5 and gate[-6] == 0.0
+    assert rows[-1] == refio.sparse_row(done, done, rep, True)
+    m0, _, step = refio.read_mass_restart(d, refio.load_case_dir(d).config, u, w, case.nx, case.ny, len(u))
+    assert step == done and abs(m0 - 1.0) < 1e-14

@@ -229,3 +229,39 @@ def test_residual_reference_keeps_its_epoch(tmp_path):
         f.write(text.replace("0 ", "7 ", 1))
     refio.write_residual_reference(p, 1.0, 2.0, 1e-8, 1e-12)
     assert refio.read_residual_reference(p)[:3] == (7, 1.0, 2.0)
+
+
+def _report_from_sparse(rows):
+    """A device report vector carrying the pre-update science of step 2 (the view of accepted state 1)
+    and the moment error of step 2's update (the accepted state 2's)."""
+    rep = np.zeros(80)
+    rep[57:79] = [rows[0][f"science_{k}"] for k in range(1, 23)]
+    rep[1] = rows[1]["moment"]
+    rep[53] = 1.0
+    return rep
+
+
+@pytest.mark.parametrize("case", ["low_implicit", "high_implicit"])
+def test_implicit_stdout_line_reproduces_the_reference(case):
+    g = golden()
+    line = g[case + "_summary"][0]
+    wall = float(line.split("wall=")[1].split()[0])
+    rep = _report_from_sparse(g[case + "_sparse"])
+    assert refio.implicit_stdout_line(2, rep, 1000.0, wall) == line
+
+
+def test_residual_implicit_rows_follow_the_fortran_format(tmp_path):
+    g = golden()
+    rep = _report_from_sparse(g["low_implicit_sparse"])
+    rep[55], rep[52] = 8.6528e-5, -1.25e-10
+    w = refio.ResidualImplicitWriter(str(tmp_path), 1000.0, True)
+    w.append(1, rep, 0.5)
+    w.append(2, rep, 1.0)
+    lines = open(tmp_path / "ResidualImplicit.plt").read().splitlines()
+    assert lines[0] == refio.RESIDUAL_IMPLICIT_HEADER and len(lines) == 3
+    row = lines[2]
+    assert len(row) == 12 + 11 * 18 + 8 + 5 * 18 + 12 + 15 * 18 + 2 * 25
+    assert len(lines[0].split()) - 2 == 36                      # 36 columns after "VARIABLES ="
+    f = [float(row[0:12])] + [float(row[12 + 18 * k: 30 + 18 * k]) for k in range(11)]
+    assert f[0] == 2 and f[1] == 8.6528e-5 and f[2] == 1000.0 and f[4] == float(f"{rep[57]:.9E}")
+    assert float(row[-50:-25]) == -1.25e-10 and float(row[-25:]) == 1.0

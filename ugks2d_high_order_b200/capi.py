@@ -36,9 +36,8 @@ EXPORTS = [
 REPORT_LEN = 80
 CN_REPORT_LEN = 24
 # stages of one ImplicitSteady pseudo-step timed by the profile mode (kImStageNames in ugks_implicit.cuh)
-IMPLICIT_STAGES = ("timestep", "pre_evaluation", "pr2_prep", "pr2_sweep", "macro_alpha", "equilibrium",
-                   "lusgs_forward", "wall_closure", "lusgs_backward", "micro_alpha", "apply", "rescale",
-                   "post_fluxes", "post_residual")
+IMPLICIT_STAGES = ("timestep", "pre_evaluation", "pr2_sweep", "equilibrium", "lusgs_forward", "wall_closure",
+                   "lusgs_backward", "micro_alpha", "apply", "rescale", "post_fluxes", "post_residual")
 
 
 class UgksParams(ctypes.Structure):

@@ -5,6 +5,8 @@ from the cold start (Iflag_InitFlow = 0) or from the restart files of the direct
 MAX_ITER steps (implicit methods stop earlier at the five-state gate), and writes what the
 reference writes for this path:
   sparse_residual.csv          every Nstep_monitor-th accepted state (implicit methods),
+  ResidualImplicit.plt         every Nstep_show-th step (implicit methods), with the reference's
+                               'Implicit iter=' line on the log,
   flow2d.dat, vdf2d.dat,       every Nstep_restart steps and at the end when Iflag_WriteRestart = 1
   grid2d.grd                   (Output_restart_only, mod_Output.f90:30-56),
   closed_mass_rank<r>.bin,     with the mass rescale on (WriteMassRestart), and
@@ -13,6 +15,7 @@ The correction ledger of closed_mass_rank<r>.bin is written as zeros: the device
 (the reference uses it only for its light_steps.csv audit columns).
 """
 import os
+import time
 
 import numpy as np
 
@@ -83,6 +86,8 @@ def run_case_dir(path, out=None, steps=None, log=print):
     try:
         origin = start(d, s)
         sparse = refio.SparseResidualWriter(out, c.mass_rescale) if c.method in IMPLICIT else None
+        plt = refio.ResidualImplicitWriter(out, c.ncfl, c.mass_rescale) if c.method in IMPLICIT else None
+        t0 = time.perf_counter()
         done, conv, rep = 0, None, None
         while done < nsteps:
             if c.method in IMPLICIT:
@@ -92,9 +97,10 @@ def run_case_dir(path, out=None, steps=None, log=print):
                 done += got
                 if (origin + done) % monitor == 0:
                     sparse.append(done, origin + done, rep)
-                if done % show == 0 or conv:
-                    log(f"iter={origin + done:8d} Rrho={rep[12]:.4e} RrhoU={rep[13]:.4e} RrhoV={rep[14]:.4e} "
-                        f"RE={rep[15]:.4e} Rh={rep[24]:.4e} Rb={rep[25]:.4e} c_minus_1={rep[52]:.6e}")
+                if done % show == 0:
+                    wall = time.perf_counter() - t0
+                    plt.append(done, rep, wall)
+                    log(refio.implicit_stdout_line(done, rep, c.ncfl, wall))
             else:
                 n = min(show, nsteps - done)
                 if every > 0 and write_restart:

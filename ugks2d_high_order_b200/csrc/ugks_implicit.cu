@@ -569,16 +569,13 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_residual_s2(LoParams 
 }
 
 // -------------------------------------------------------------------------------------------
-// PR(2) set-up: per (cell, face) the spectral radius (ImplicitSpectralRadius, mod_ImplicitMacro.f90:
-// 15-55) and the Euler normal fluxes of the unperturbed cell and neighbour states, which stay fixed
-// through the sweeps; zero the first correction buffer and reset the admissible-alpha masks.
-__global__ void k_im_pr2_prep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I) {
-    if (I.state[IS_STOP] != 0.0) return;
-    const int t = blockIdx.x * blockDim.x + threadIdx.x;
-    const int nc = P.nx * P.ny;
-    if (t == 0) { I.mask[0] = 0xffffffffu; I.mask[1] = 0xffffffffu; }
-    if (t >= nc * 4) return;
-    const int c = t >> 2, f = t & 3, i = c % P.nx, j = c / P.nx;
+// PR(2) set-up of one (cell, face): the spectral radius (ImplicitSpectralRadius,
+// mod_ImplicitMacro.f90:15-55) and the Euler normal fluxes of the unperturbed cell and neighbour
+// states, which stay fixed through the sweeps.  Written to global memory for the later sweeps.
+// Returns false (after stopping the sequence) when gamma is not finite and positive.
+__device__ __forceinline__ bool pr_prep_item(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I, int c,
+                             int f, double& gam, double foi[4], double foj[4]) {
+    const int i = c % P.nx, j = c / P.nx;
     const int rows = P.ny / Q.nslab;
     const FaceGeo g = face_geo(P, rows, i, j, f);
     double wi[4], wj[4];
@@ -598,7 +595,7 @@ __global__ void k_im_pr2_prep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I) 
     double ti = 1.0, tj = 1.0;
     bool ok = get_primary(P.gm1, wi, pi_) && get_primary(P.gm1, wj, pj);
     ok = ok && get_tau(P.mu_ref, P.omega, pi_, ti) && get_tau(P.mu_ref, P.omega, pj, tj);
-    double gam = NAN;
+    gam = NAN;
     if (ok) {
         const double rho_avg = 0.5 * (pi_.r + pj.r);
         const double u_avg = 0.5 * (pi_.U + pj.U), v_avg = 0.5 * (pi_.V + pj.V);
@@ -608,19 +605,17 @@ __global__ void k_im_pr2_prep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I) 
         const double sos = sqrt((P.gm1 + 1.0) * p_avg / rho_avg);
         gam = fabs(u_avg * g.nx + v_avg * g.ny) + sos + 2.0 * mu_avg / (rho_avg * fmax(dist, 1000.0 * kEps));
     }
-    if (!(isfinite(gam) && gam > 0.0)) stop_with(I, B.status, ST_GETPRIMARY);
+    const bool good = isfinite(gam) && gam > 0.0;
+    if (!good) stop_with(I, B.status, ST_GETPRIMARY);
     I.pr_gamma[c * 4 + f] = gam;
-    double fo[4];
-    euler_flux(P.gm1, wi, g.nx, g.ny, fo);
+    euler_flux(P.gm1, wi, g.nx, g.ny, foi);
+    euler_flux(P.gm1, wj, g.nx, g.ny, foj);
 #pragma unroll
-    for (int m = 0; m < 4; ++m) I.pr_foi[(c * 4 + f) * 4 + m] = fo[m];
-    euler_flux(P.gm1, wj, g.nx, g.ny, fo);
-#pragma unroll
-    for (int m = 0; m < 4; ++m) I.pr_foj[(c * 4 + f) * 4 + m] = fo[m];
-    if (f == 0) {
-#pragma unroll
-        for (int m = 0; m < 4; ++m) I.dwA[c * 4 + m] = 0.0;
+    for (int m = 0; m < 4; ++m) {
+        I.pr_foi[(c * 4 + f) * 4 + m] = foi[m];
+        I.pr_foj[(c * 4 + f) * 4 + m] = foj[m];
     }
+    return good;
 }
 
 // Cells of anti-diagonal d of a rows x nx slab (local row jl = 0..rows-1, column i), t-th cell.
@@ -668,8 +663,13 @@ __device__ __forceinline__ void pr_wave_sync(int warps) {
 // when one warp did it alone), the first 4 x min(dcells, 32) relax.
 constexpr int kPrThreads = 256;
 
+// first: the sweep also does the PR(2) set-up of its slab (pr_prep_item, straight into shared memory)
+// and starts from the zero correction (X unused); when it is not also the last sweep, CTA 0 resets
+// the admissible-alpha masks.  last: the sweep also does BuildPredictedMacroState
+// (mod_ImplicitMacro.f90:159-185) for its cells: the admissible alpha levels of W + alpha Y,
+// ANDed into the macro mask.
 __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I,
-                                                             const double* X, double* Y) {
+                                                             const double* X, double* Y, int first, int last) {
     if (I.state[IS_STOP] != 0.0) return;
     extern __shared__ double sm[];
     __shared__ double part[32][4][8];
@@ -693,11 +693,24 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
     for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) {
         sW[q] = B.W[c0 * 4 + q];
         sR[q] = I.rate_w[c0 * 4 + q];
-        sG[q] = I.pr_gamma[c0 * 4 + q];
     }
-    for (int q = threadIdx.x; q < ncs * 16; q += blockDim.x) {
-        sFi[q] = I.pr_foi[c0 * 16 + q];
-        sFj[q] = I.pr_foj[c0 * 16 + q];
+    if (first) {
+        if (!last && s == 0 && threadIdx.x == 0) { I.mask[0] = 0xffffffffu; I.mask[1] = 0xffffffffu; }
+        int prep_bad = 0;
+        for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) {
+            double gam, foi[4], foj[4];
+            if (!pr_prep_item(P, B, Q, I, c0 + (q >> 2), q & 3, gam, foi, foj)) prep_bad = 1;
+            sG[q] = gam;
+#pragma unroll
+            for (int m = 0; m < 4; ++m) { sFi[q * 4 + m] = foi[m]; sFj[q * 4 + m] = foj[m]; }
+        }
+        if (__syncthreads_or(prep_bad)) return;   // the sequence has stopped (ST_GETPRIMARY)
+    } else {
+        for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) sG[q] = I.pr_gamma[c0 * 4 + q];
+        for (int q = threadIdx.x; q < ncs * 16; q += blockDim.x) {
+            sFi[q] = I.pr_foi[c0 * 16 + q];
+            sFj[q] = I.pr_foj[c0 * 16 + q];
+        }
     }
     // interior and halo cells: correction, state, primitives (halo rows beyond a wall stay unused)
     for (int l = threadIdx.x; l < nall; l += blockDim.x) {
@@ -710,7 +723,7 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
         double y[4] = {0.0, 0.0, 0.0, 0.0}, t[4] = {1.0, 0.0, 0.0, 1.0};
         if (g >= 0) {
 #pragma unroll
-            for (int m = 0; m < 4; ++m) { y[m] = X[g * 4 + m]; t[m] = B.W[g * 4 + m] + y[m]; }
+            for (int m = 0; m < 4; ++m) { y[m] = first ? 0.0 : X[g * 4 + m]; t[m] = B.W[g * 4 + m] + y[m]; }
         }
         const EulerPrim e = euler_prim(P.gm1, t);
 #pragma unroll
@@ -719,8 +732,9 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
     }
     // the diagonal 1/dt_ps + 0.5 * sum_faces(L * gamma) / area is fixed through the sweeps; the face
     // products are rounded before they are summed in face order, as the reference loop does
+    __syncthreads();
     for (int cl = threadIdx.x; cl < ncs; cl += blockDim.x) {
-        const double* gm = I.pr_gamma + (c0 + cl) * 4;
+        const double* gm = sG + cl * 4;
         double sg = 0.0;
         sg = sg + __dmul_rn(P.dy, gm[0]);
         sg = sg + __dmul_rn(P.dy, gm[1]);
@@ -805,25 +819,22 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
     }
     __syncthreads();
     for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) Y[c0 * 4 + q] = sY[q];
-    if (__syncthreads_or(bad) && threadIdx.x == 0) stop_with(I, B.status, ST_NONFINITE_STATE);
-}
-
-// BuildPredictedMacroState (mod_ImplicitMacro.f90:159-185): admissible alpha levels per cell.
-__global__ void k_im_macro_alpha(LoParams P, LoBuffers B, ImParams Q, ImBuffers I, const double* D) {
-    if (I.state[IS_STOP] != 0.0) return;
-    const int c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c >= P.nx * P.ny) return;
-    const int lv = alpha_levels(Q.min_alpha);
-    unsigned mask = 0u;
-    double a = 1.0;
-    for (int m = 0; m <= lv; ++m) {
-        double t[4];
+    if (last) {
+        const int lv = alpha_levels(Q.min_alpha);
+        for (int cl = threadIdx.x; cl < ncs; cl += blockDim.x) {
+            unsigned mask = 0u;
+            double a = 1.0;
+            for (int m = 0; m <= lv; ++m) {
+                double t[4];
 #pragma unroll
-        for (int q = 0; q < 4; ++q) t[q] = B.W[c * 4 + q] + a * D[c * 4 + q];
-        if (is_physical(t)) mask |= 1u << m;
-        a = 0.5 * a;
+                for (int q = 0; q < 4; ++q) t[q] = sW[cl * 4 + q] + a * sY[cl * 4 + q];
+                if (is_physical(t)) mask |= 1u << m;
+                a = 0.5 * a;
+            }
+            atomicAnd(I.mask, mask);
+        }
     }
-    atomicAnd(I.mask, mask);
+    if (__syncthreads_or(bad) && threadIdx.x == 0) stop_with(I, B.status, ST_NONFINITE_STATE);
 }
 
 // BuildPredictedEquilibrium (mod_ImplicitMicro.f90:43-88), second-order branch.
@@ -1369,7 +1380,6 @@ cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q) {
 cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
                                   cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
                                   long long* launches, cudaEvent_t* marks) {
-    const int nc = P.nx * P.ny;
     int stage = 0;
     auto mark = [&](cudaError_t e) -> cudaError_t {
         if (e == cudaSuccess && marks) e = cudaEventRecord(marks[stage++], s);
@@ -1386,19 +1396,21 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     if (e == cudaSuccess)                                                         // Interpolation + Evolution
         e = Q.high_order ? s2_enqueue(1, P, Bpre, I.s2, s, s2, fork, join) : im_fluxes(P, Bpre, s, s2, fork, join);
     if (e == cudaSuccess) e = mark(im_cell(0, P, Bpre, Q, I, nullptr, s));       // ComputeResidual + diagnostics
-    if (e == cudaSuccess) { k_im_pr2_prep<<<(nc * 4 + 127) / 128, 128, 0, s>>>(P, B, Q, I); e = mark(cudaGetLastError()); }
     const double* X = I.dwA;
     double* Y = I.dwB;
     const int rows = P.ny / Q.nslab, ncs = rows * P.nx;
     const int dcells = rows < P.nx ? rows : P.nx;                              // longest anti-diagonal
     const int lu_warps = dcells < 8 ? dcells : 8;
-    for (int sw = 0; sw < Q.macro_sweeps && e == cudaSuccess; ++sw) {            // SolveMacroPR2
-        k_im_pr2_sweep<<<Q.nslab, kPrThreads, (size_t)pr_smem_words(rows, P.nx) * sizeof(double), s>>>(P, B, Q, I, X, Y);
+    // SolveMacroPR2 with its set-up fused into the first sweep and BuildPredictedMacroState into the
+    // last; a single sweep resets the alpha masks beforehand (its CTAs AND into them as they finish)
+    if (e == cudaSuccess && Q.macro_sweeps == 1) e = cudaMemsetAsync(I.mask, 0xff, 2 * sizeof(unsigned), s);
+    for (int sw = 0; sw < Q.macro_sweeps && e == cudaSuccess; ++sw) {
+        k_im_pr2_sweep<<<Q.nslab, kPrThreads, (size_t)pr_smem_words(rows, P.nx) * sizeof(double), s>>>(
+            P, B, Q, I, X, Y, sw == 0, sw == Q.macro_sweeps - 1);
         e = cudaGetLastError();
         const double* t = Y; Y = const_cast<double*>(X); X = t;
     }
     e = mark(e);
-    if (e == cudaSuccess) { k_im_macro_alpha<<<(nc + 127) / 128, 128, 0, s>>>(P, B, Q, I, X); e = mark(cudaGetLastError()); }
     if (e == cudaSuccess) e = mark(im_cell(2, P, B, Q, I, X, s));                // BuildPredictedEquilibrium
     const dim3 lu_grid((unsigned)((P.nvel + 31) / 32), (unsigned)Q.nslab);
     const size_t lu_smem = (size_t)ncs * 64 * sizeof(double);
@@ -1411,7 +1423,7 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     if (e == cudaSuccess)                                                         // accepted-state evaluation
         e = mark(Q.high_order ? s2_enqueue(1, P, Bh, I.s2, s, s2, fork, join) : im_fluxes(P, Bh, s, s2, fork, join));
     if (e == cudaSuccess) e = mark(im_cell(1, P, B, Q, I, nullptr, s));
-    if (launches) *launches += 16 + Q.macro_sweeps + (Q.high_order ? 2 : 0);
+    if (launches) *launches += 14 + Q.macro_sweeps + (Q.high_order ? 2 : 0);
     return e;
 }
 

@@ -35,10 +35,10 @@ constexpr int kImCell = 20;   // per-cell diagnostic terms
 constexpr int kMaxSlabCells = 384;   // rows x nx of one slab held in shared memory by the sweep kernels
 
 // Stages of one pseudo-step, in launch order, for the per-stage event timing of profile runs.
-constexpr int kImStages = 14;
+constexpr int kImStages = 12;
 constexpr const char* kImStageNames[kImStages] = {
-    "timestep", "pre_evaluation", "pr2_prep", "pr2_sweep", "macro_alpha", "equilibrium", "lusgs_forward",
-    "wall_closure", "lusgs_backward", "micro_alpha", "apply", "rescale", "post_fluxes", "post_residual"};
+    "timestep", "pre_evaluation", "pr2_sweep", "equilibrium", "lusgs_forward", "wall_closure",
+    "lusgs_backward", "micro_alpha", "apply", "rescale", "post_fluxes", "post_residual"};
 
 struct ImParams {
     int nslab;              // ranks of the reference's 1 x NP_Y blocking (rows per slab = ny / nslab)

@@ -16,7 +16,9 @@ Restart and monitor files written and read here:
                                       (mod_ClosedCouetteMass.f90:315-393);
   residual_reference.in               WriteRestartReference (mod_Output.f90:58-76), read back in
                                       mod_R5Observe.f90:176-186;
-  sparse_residual.csv                 WriteMonitorRows (mod_R5Observe.f90:322-350).
+  sparse_residual.csv                 WriteMonitorRows (mod_R5Observe.f90:322-350);
+  ResidualImplicit.plt, the           WriteImplicitResidual (mod_ImplicitDiagnostics.f90:356-399).
+  'Implicit iter=' stdout line
 
 Fortran unformatted sequential files are framed as gfortran frames them: every record carries its
 byte length as a little-endian int32 before and after the data.  closed_mass_rank<r>.bin is a
@@ -716,3 +718,75 @@ class SparseResidualWriter:
             if new:
                 f.write(SPARSE_HEADER + "\n")
             f.write(sparse_row(local_state, cumulative_state, report, self.mass_rescale) + "\n")
+
+
+# ------------------------------------------------------------------------------------------------
+# ResidualImplicit.plt and the implicit stdout line (WriteImplicitResidual,
+# mod_ImplicitDiagnostics.f90:356-399).  Both print the science of the pre-update evaluation
+# (SciencePack, mod_R5Observe.f90:27-32: the view of the accepted state is restored away before
+# they are written) with the moment error of the update (after the rescale, the accepted state's).
+
+RESIDUAL_IMPLICIT_HEADER = (
+    "VARIABLES = iter dtPhysicalMin nCFL alpha rhoResidual rhoUResidual rhoVResidual energyResidual "
+    "hResidual bResidual momentError massDefect retries wallTime prSeconds lusgsSeconds "
+    "correctionExchangeSeconds evolutionSeconds retryTotal rhoRelative rhoURelative rhoVRelative "
+    "energyRelative rhoAbsolute rhoUAbsolute rhoVAbsolute energyAbsolute hRelative bRelative hAbsolute "
+    "bAbsolute microForwardSeconds microBackwardSeconds microForwardBackwardExchangeSeconds c_minus_1 "
+    "mass_rescale_enabled")
+
+PRE_SCIENCE = 57   # report[57..78]: science_1..22 of the pre-update evaluation
+
+
+def _fe(x, width, digits):
+    """Fortran 1PEw.d: d.ddd, then E+dd (E dropped for a 3-digit exponent)."""
+    x = float(x)
+    if not math.isfinite(x):
+        return ("NaN" if math.isnan(x) else ("Infinity" if x > 0 else "-Infinity")).rjust(width)
+    mant, ex = f"{x:.{digits}E}".split("E")
+    e = int(ex)
+    tail = f"E{'+' if e >= 0 else '-'}{abs(e):02d}" if abs(e) <= 99 else f"{'+' if e >= 0 else '-'}{abs(e):03d}"
+    return (mant + tail).rjust(width)
+
+
+def _implicit_values(report, ncfl):
+    r = np.asarray(report, dtype=np.float64)
+    sci = r[PRE_SCIENCE:PRE_SCIENCE + 22]
+    return r, sci, {"dt": r[55], "ncfl": ncfl, "alpha": r[53], "moment": r[1], "mass": sci[19]}
+
+
+def residual_implicit_row(it, report, ncfl, mass_rescale, wall_time=0.0):
+    """One ResidualImplicit.plt row: '(I12,1P,11E18.9,I8,5E18.9,I12,15E18.9,2ES25.16E3)'.  The
+    reference's phase timers (PR, LU-SGS, exchange, evolution, micro sweeps) are written as 0: the
+    device pseudo-step is one graph launch and is timed only as a whole (wall_time)."""
+    r, sci, v = _implicit_values(report, ncfl)
+    a = [v["dt"], v["ncfl"], v["alpha"], *sci[0:4], sci[12], sci[13], v["moment"], v["mass"]]
+    b = [wall_time, 0.0, 0.0, 0.0, 0.0]
+    c = [*sci[4:8], *sci[8:12], sci[14], sci[15], sci[16], sci[17], 0.0, 0.0, 0.0]
+    return (f"{int(it):12d}" + "".join(_fe(x, 18, 9) for x in a) + f"{0:8d}" + "".join(_fe(x, 18, 9) for x in b)
+            + f"{0:12d}" + "".join(_fe(x, 18, 9) for x in c)
+            + _es(r[52] if mass_rescale else 0.0, 16, 25) + _es(1.0 if mass_rescale else 0.0, 16, 25))
+
+
+def implicit_stdout_line(it, report, ncfl, wall_time=0.0):
+    """The 'Implicit iter=...' line: '(A,I0,1P,11(A,E12.4),2(A,I0))'."""
+    r, sci, v = _implicit_values(report, ncfl)
+    names = (("nCFL", v["ncfl"]), ("alpha", v["alpha"]), ("Rrho", sci[0]), ("RrhoU", sci[1]), ("RrhoV", sci[2]),
+             ("RE", sci[3]), ("Rh", sci[12]), ("Rb", sci[13]), ("moment", v["moment"]), ("mass", v["mass"]),
+             ("wall", wall_time))
+    return f"Implicit iter={int(it)}" + "".join(f" {k}={_fe(x, 12, 4)}" for k, x in names) + " retries=0 retryTotal=0"
+
+
+class ResidualImplicitWriter:
+    """ResidualImplicit.plt: replaced by the first row of a run, appended afterwards."""
+
+    def __init__(self, path, ncfl, mass_rescale):
+        self.fn = os.path.join(path, "ResidualImplicit.plt")
+        self.ncfl, self.mass_rescale = ncfl, mass_rescale
+        self.started = False
+
+    def append(self, it, report, wall_time):
+        with open(self.fn, "a" if self.started else "w") as f:
+            if not self.started:
+                f.write(RESIDUAL_IMPLICIT_HEADER + "\n")
+            f.write(residual_implicit_row(it, report, self.ncfl, self.mass_rescale, wall_time) + "\n")
+        self.started = True
