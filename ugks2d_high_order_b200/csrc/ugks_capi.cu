@@ -62,6 +62,8 @@ struct ugks_ctx {
     cudaGraphExec_t igraph = nullptr;
     int igraph_steps = 0;
     long long igraph_launches = 0;
+    double* hstate = nullptr;                  // pinned [2][IS_COUNT]: the state after each graph batch
+    cudaEvent_t rb_ev[2] = {nullptr, nullptr};  // its copy has landed
     // profiling
     bool profile = false;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -300,6 +302,8 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->cflags) cudaFree(c->cflags);
     if (c->imem) cudaFree(c->imem);
     if (c->iflags) cudaFree(c->iflags);
+    if (c->hstate) cudaFreeHost(c->hstate);
+    for (int i = 0; i < 2; ++i) if (c->rb_ev[i]) cudaEventDestroy(c->rb_ev[i]);
     for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (int i = 0; i <= kImStages; ++i) if (c->im_ev[i]) cudaEventDestroy(c->im_ev[i]);
     if (c->dmem) cudaFree(c->dmem);
@@ -685,14 +689,43 @@ extern "C" int ugks_implicit_steps(ugks_ctx* c, int max_steps, int* steps_done, 
             c->launches += n;
             left -= 1;
         } else if (left >= G) {
-            // up to 4 graphs per readback of the stop flag: after a stop the queued steps' kernels
-            // return at entry, so the state and the counts are those of the stopping step
+            // Batches of up to 2 graphs, each followed by a copy of the state into a pinned slot.  The
+            // next batch is queued before the host waits for the previous batch's copy, so the device
+            // never idles on the host between batches.  After a stop the queued steps' kernels return
+            // at entry, so the state and the counts stay those of the stopping step.
             int r = build_implicit_graph(c, G);
             if (r) return r;
-            const int ng = left / G < 4 ? left / G : 4;
-            for (int q = 0; q < ng; ++q) UGKS_CK(cudaGraphLaunch(c->igraph, c->stream));
-            c->launches += c->igraph_launches * ng;
-            left -= G * ng;
+            if (!c->hstate) {
+                UGKS_CK(cudaMallocHost((void**)&c->hstate, 2 * IS_COUNT * sizeof(double)));
+                for (int i = 0; i < 2; ++i) UGKS_CK(cudaEventCreateWithFlags(&c->rb_ev[i], cudaEventDisableTiming));
+            }
+            auto queue_batch = [&](int slot) -> cudaError_t {
+                const int ng = left / G < 2 ? left / G : 2;
+                for (int q = 0; q < ng; ++q) {
+                    const cudaError_t e = cudaGraphLaunch(c->igraph, c->stream);
+                    if (e != cudaSuccess) return e;
+                }
+                c->launches += c->igraph_launches * ng;
+                left -= G * ng;
+                const cudaError_t e = cudaMemcpyAsync(c->hstate + slot * IS_COUNT, c->I.state, IS_COUNT * sizeof(double),
+                                                      cudaMemcpyDeviceToHost, c->stream);
+                return e != cudaSuccess ? e : cudaEventRecord(c->rb_ev[slot], c->stream);
+            };
+            int cur = 0;
+            UGKS_CK(queue_batch(cur));
+            for (;;) {
+                const int prev = cur;
+                cur = left >= G ? 1 - prev : -1;
+                if (cur >= 0) UGKS_CK(queue_batch(cur));
+                UGKS_CK(cudaEventSynchronize(c->rb_ev[prev]));
+                std::memcpy(st, c->hstate + prev * IS_COUNT, sizeof st);
+                if (st[IS_STOP] != 0.0 || cur < 0) break;
+            }
+            if (cur >= 0) {   // a batch queued past the stop: let it drain, then read the final state
+                UGKS_CK(cudaMemcpyAsync(st, c->I.state, sizeof st, cudaMemcpyDeviceToHost, c->stream));
+                UGKS_CK(cudaStreamSynchronize(c->stream));
+            }
+            continue;
         } else {
             long long n = 0;
             for (int s = 0; s < left; ++s)

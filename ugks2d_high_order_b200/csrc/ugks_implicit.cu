@@ -672,7 +672,9 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
                                                              const double* X, double* Y, int first, int last) {
     if (I.state[IS_STOP] != 0.0) return;
     extern __shared__ double sm[];
-    __shared__ double part[32][4][8];
+    // face terms of the cells of one diagonal, [term][writer lane]: the faces lanes write a contiguous
+    // row, and the odd row length puts the components lanes' reads of a column on distinct banks
+    __shared__ double part[8][4 * 32 + 1];
     const int s = blockIdx.x, rows = P.ny / Q.nslab, nx = P.nx, ny = P.ny;
     const int ncs = rows * nx, nall = ncs + 2 * rows + 2 * nx, c0 = s * ncs;
     double* sY = sm;                  // [nall][4] corrections
@@ -681,8 +683,9 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
     double* sW = sP + nall * 4;       // [ncs][4]
     double* sR = sW + ncs * 4;        // [ncs][4] rate_w
     double* sG = sR + ncs * 4;        // [ncs][4] gamma per face
-    double* sFi = sG + ncs * 4;       // [ncs][4 faces][4] fixed Euler flux of the cell
-    double* sFj = sFi + ncs * 16;     // [ncs][4 faces][4] fixed Euler flux of the neighbour
+    double* sFi = sG + ncs * 4;       // [4 components][ncs * 4 faces] fixed Euler flux of the cell
+    double* sFj = sFi + ncs * 16;     // [4 components][ncs * 4 faces] fixed Euler flux of the neighbour
+    const int ncf = ncs * 4;          // component-major: the cells of a diagonal fall on distinct banks
     double* sD = sFj + ncs * 16;      // [ncs] diagonal
     const int dcells = rows < nx ? rows : nx;                  // longest anti-diagonal
     const int wave = 4 * (dcells < 32 ? dcells : 32);          // relaxing lanes: 4 per cell
@@ -702,14 +705,14 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
             if (!pr_prep_item(P, B, Q, I, c0 + (q >> 2), q & 3, gam, foi, foj)) prep_bad = 1;
             sG[q] = gam;
 #pragma unroll
-            for (int m = 0; m < 4; ++m) { sFi[q * 4 + m] = foi[m]; sFj[q * 4 + m] = foj[m]; }
+            for (int m = 0; m < 4; ++m) { sFi[m * ncf + q] = foi[m]; sFj[m * ncf + q] = foj[m]; }
         }
         if (__syncthreads_or(prep_bad)) return;   // the sequence has stopped (ST_GETPRIMARY)
     } else {
         for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) sG[q] = I.pr_gamma[c0 * 4 + q];
         for (int q = threadIdx.x; q < ncs * 16; q += blockDim.x) {
-            sFi[q] = I.pr_foi[c0 * 16 + q];
-            sFj[q] = I.pr_foj[c0 * 16 + q];
+            sFi[(q & 3) * ncf + (q >> 2)] = I.pr_foi[c0 * 16 + q];
+            sFj[(q & 3) * ncf + (q >> 2)] = I.pr_foj[c0 * 16 + q];
         }
     }
     // interior and halo cells: correction, state, primitives (halo rows beyond a wall stay unused)
@@ -782,37 +785,41 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
                         euler_flux_prim(tj, ej, fnxs, fny, fj);
                     }
                     const double gam = sG[cl * 4 + f];
-                    const double* foi = sFi + (cl * 4 + f) * 4;
-                    const double* foj = sFj + (cl * 4 + f) * 4;
+                    const double* foi = sFi + cl * 4 + f;
+                    const double* foj = sFj + cl * 4 + f;
 #pragma unroll
                     for (int m = 0; m < 4; ++m) {
-                        const double dti = fi[m] - foi[m];
-                        const double sm4 = dti + (fj[m] - foj[m]);
+                        const double dti = fi[m] - foi[m * ncf];
+                        const double sm4 = dti + (fj[m] - foj[m * ncf]);
                         if (!isfinite(sm4)) bad = 1;
-                        part[tc][f][m] = flen * sm4;
-                        part[tc][f][4 + m] = flen * gam * dnb[m];
+                        part[m][threadIdx.x] = flen * sm4;
+                        part[4 + m][threadIdx.x] = flen * gam * dnb[m];
                     }
                 }
                 __syncwarp();
+                double tm = 0.0;
                 if (act) {   // lane = component m
                     const int m = f;
                     double sdt = 0.0, sgn = 0.0;
 #pragma unroll
-                    for (int ff = 0; ff < 4; ++ff) { sdt = sdt + part[tc][ff][m]; sgn = sgn + part[tc][ff][4 + m]; }
+                    for (int ff = 0; ff < 4; ++ff) { sdt = sdt + part[m][tc * 4 + ff]; sgn = sgn + part[4 + m][tc * 4 + ff]; }
                     const double rhs = sR[cl * 4 + m] - div_area(0.5 * 1.0 * sdt, P) + div_area(0.5 * 1.0 * sgn, P);
                     if (!isfinite(rhs)) bad = 1;
                     const double y = rhs / sD[cl];
+                    tm = sW[cl * 4 + m] + y;
                     sY[cl * 4 + m] = y;
-                    sT[cl * 4 + m] = sW[cl * 4 + m] + y;
+                    sT[cl * 4 + m] = tm;
                 }
-                __syncwarp();
-                if (act && f < 3) {   // lanes 0..2: primitives of the relaxed state
-                    double t[4];
+                // lanes 0..2 of the cell: primitives of the relaxed state, its components gathered from
+                // the cell's 4 lanes (every lane of the warp takes part in the shuffles)
+                double t[4];
 #pragma unroll
-                    for (int m = 0; m < 4; ++m) t[m] = sT[cl * 4 + m];
+                for (int m = 0; m < 4; ++m) t[m] = __shfl_sync(0xffffffffu, tm, (threadIdx.x & ~3) + m);
+                if (act && f < 3) {
                     const EulerPrim e = euler_prim(P.gm1, t);
                     sP[cl * 4 + f] = f == 0 ? e.u : (f == 1 ? e.v : e.p);
                 }
+                if (t0 + D < dcells) __syncwarp();   // the next chunk rewrites part[]
             }
             pr_wave_sync(wave_warps);
         }
@@ -1366,7 +1373,8 @@ static cudaError_t im_fluxes(const LoParams& P, const LoBuffers& B, cudaStream_t
 cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q) {
     const int rows = P.ny / Q.nslab, ncs = rows * P.nx;
     const int pr_bytes = pr_smem_words(rows, P.nx) * (int)sizeof(double);
-    if (ncs > kMaxSlabCells || pr_bytes + 8192 > 227 * 1024) return cudaErrorInvalidValue;
+    const int pr_static = 8 * (4 * 32 + 1) * (int)sizeof(double);   // k_im_pr2_sweep's face-term array
+    if (ncs > kMaxSlabCells || pr_bytes + pr_static > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(k_im_pr2_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, pr_bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_im_lusgs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ncs * 64 * (int)sizeof(double));
