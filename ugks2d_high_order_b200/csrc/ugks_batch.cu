@@ -104,6 +104,7 @@ static void bind_scratch(ugks_batch* b, Inst& I) {
         S2Buffers& T = I.T[q];
         T.rec = rec;
         T.wall_raw = wraw;
+        T.concurrent = 1;
         s2_bind_scratch(T, s2s, nx, ny, nv);
     }
     I.C.ws = ws; I.C.rh = rh; I.C.rb = rb; I.C.cell = cell; I.C.wall_raw = wraw;

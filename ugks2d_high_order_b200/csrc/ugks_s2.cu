@@ -977,18 +977,21 @@ __global__ void __launch_bounds__(128) k_s2_macro(LoParams P, LoBuffers B, S2Buf
         for (int c = 0; c < 3; ++c) SB.wq[((size_t)cc * 9 + c * 3 + gl) * 4 + m] = nodes[gl][c] + wc - avg;
 }
 
-// The warp-per-node closure kernels run in 128-thread CTAs, three per SM: up to 170 registers a
-// thread (no spills) at 12 warps per SM.  Two 256-thread CTAs per SM capped them at 128 registers,
-// which spilled the closure's state, and ran 2-3 % slower per step.
+// The warp-per-node closure kernels come in two CTA shapes.  A single instance runs them in
+// 128-thread CTAs, three per SM: up to 170 registers a thread (no spills) at 12 warps per SM, 2-3 %
+// faster per step than two 256-thread CTAs per SM capped at 128 registers (which spill the closure's
+// state).  Many instances on concurrent streams (S2Buffers::concurrent) gain more from the 16
+// resident warps of the 256-thread shape, which they keep.
 constexpr int kS2NodeThreads = 128;
 
 // build_targets, closure part: one warp per (cell, volume node) -> the node scalars
-__global__ void __launch_bounds__(kS2NodeThreads, 3) k_s2_target_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_s2_target_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
     if (eval_cached(B)) return;
     const int nc = P.nx * P.ny, lane = threadIdx.x & 31;
     const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (wid >= nc * 9) return;
-    __shared__ double s_jac[kS2NodeThreads / 32][16];
+    __shared__ double s_jac[NT / 32][16];
     double w[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) w[m] = SB.wq[(size_t)wid * 4 + m];
@@ -1035,7 +1038,8 @@ __global__ void __launch_bounds__(256) k_s2_target_sum(LoParams P, LoBuffers B, 
 constexpr int kS2FScal = 48;   // [0] ok, [1..4] theta, [5..12] K directions, [13..16] ux vy lam coeff,
                                // [17..18] q0, [19..34] left/right/tangential/time directions, [35..39] Mt,
                                // [40..43] the time-direction moments wt
-__global__ void __launch_bounds__(kS2NodeThreads, 3) k_s2_face_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
+template <int NT, int MINB>
+__global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
     if (eval_cached(B)) return;
     const int nv = P.nvel, nx = P.nx, ny = P.ny, ck = P.ck, lane = threadIdx.x & 31, nr = (nv + 31) >> 5;
     const int nfx = nx * ny, nf = nfx + nx * (ny - 1);
@@ -1063,7 +1067,7 @@ __global__ void __launch_bounds__(kS2NodeThreads, 3) k_s2_face_nodes(LoParams P,
     }
     warp_sum_all<4>(acc);
     const double w0[4] = {acc[0], acc[1], acc[2], acc[3]};
-    __shared__ double s_jac[kS2NodeThreads / 32][16];
+    __shared__ double s_jac[NT / 32][16];
     WClosure C;
     C.jac = s_jac[threadIdx.x >> 5];
     WMke M;
@@ -1604,7 +1608,8 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     }
     if (e == cudaSuccess && targets) {
         cudaStream_t ts = side_targets ? s2 : s;
-        k_s2_target_nodes<<<node_ctas((long long)nc * 9), kS2NodeThreads, 0, ts>>>(P, B, S);
+        if (S.concurrent) k_s2_target_nodes<256, 2><<<warps((long long)nc * 9), 256, 0, ts>>>(P, B, S);
+        else k_s2_target_nodes<kS2NodeThreads, 3><<<node_ctas((long long)nc * 9), kS2NodeThreads, 0, ts>>>(P, B, S);
         e = cudaGetLastError();
         if (e == cudaSuccess) {
             k_s2_target_sum<<<dim3((unsigned)((nv + 255) / 256), (unsigned)nc), 256, 0, ts>>>(P, B, S);
@@ -1620,7 +1625,11 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
     if (e == cudaSuccess) { k_s2_wall_nodes<<<warps(2LL * nx * 3), 256, 0, s2>>>(P, B, S); e = cudaGetLastError(); }
     if (e == cudaSuccess) e = cudaEventRecord(join, s2);
-    if (e == cudaSuccess) { k_s2_face_nodes<<<node_ctas((long long)nf * 3), kS2NodeThreads, 0, s>>>(P, B, S); e = cudaGetLastError(); }
+    if (e == cudaSuccess) {
+        if (S.concurrent) k_s2_face_nodes<256, 2><<<warps((long long)nf * 3), 256, 0, s>>>(P, B, S);
+        else k_s2_face_nodes<kS2NodeThreads, 3><<<node_ctas((long long)nf * 3), kS2NodeThreads, 0, s>>>(P, B, S);
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess) {
         if (nv <= 1024) k_s2_face_flux<4><<<(unsigned)(nf * 3), 256, 0, s>>>(P, B, S);
         else k_s2_face_flux<10><<<(unsigned)(nf * 3), 256, 0, s>>>(P, B, S);

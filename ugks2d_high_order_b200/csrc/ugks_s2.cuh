@@ -26,6 +26,8 @@ struct S2Buffers {
     double* tscal;   // [cell][9][16] volume node scalars (closure theta, directions, primitive)
     double* l1;      // [cell][22][nvel] first-layer WENO values of h and b (k_s2_recon1)
     double* fscal;   // [interior face][3][48] face-node scalars (k_s2_face_nodes -> k_s2_face_flux)
+    int concurrent;  // 1: one of many instances on concurrent streams (the batch): the closure kernels
+                     // take the CTA shape with more resident warps
 };
 
 // doubles of evaluation scratch one S2Buffers needs, and their layout
