@@ -1158,8 +1158,10 @@ __global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffer
 // ugks_node's flux at one face Gauss node (mod_S2D1.f90:486-507): one CTA per (face, node), VPT
 // velocities per thread, from the node scalars; the node micro flux goes to SB.node, its moments to
 // SB.nodew, and the time-direction moment gate (2e-12) is checked on the block-reduced moments.
+// Three CTAs per SM (80 registers, small spills): the kernel waits on its face-cache loads, and 24
+// resident warps hide that better than 16.
 template <int VPT>
-__global__ void __launch_bounds__(256) k_s2_face_flux(LoParams P, LoBuffers B, S2Buffers SB) {
+__global__ void __launch_bounds__(256, 3) k_s2_face_flux(LoParams P, LoBuffers B, S2Buffers SB) {
     if (eval_cached(B)) return;
     __shared__ double sc[kS2FScal];
     __shared__ double red[8 * 8];
