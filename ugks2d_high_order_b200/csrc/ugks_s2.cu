@@ -977,21 +977,21 @@ __global__ void __launch_bounds__(128) k_s2_macro(LoParams P, LoBuffers B, S2Buf
         for (int c = 0; c < 3; ++c) SB.wq[((size_t)cc * 9 + c * 3 + gl) * 4 + m] = nodes[gl][c] + wc - avg;
 }
 
-// The warp-per-node closure kernels come in two CTA shapes.  A single instance runs them in
-// 128-thread CTAs, three per SM: up to 170 registers a thread (no spills) at 12 warps per SM, 2-3 %
-// faster per step than two 256-thread CTAs per SM capped at 128 registers (which spill the closure's
-// state).  Many instances on concurrent streams (S2Buffers::concurrent) gain more from the 16
-// resident warps of the 256-thread shape, which they keep.
+// The face-node closure kernel comes in two CTA shapes.  A single instance runs it in 128-thread
+// CTAs, three per SM: up to 170 registers a thread (no spills) at 12 warps per SM, faster per step
+// than two 256-thread CTAs per SM capped at 128 registers (which spill the closure's state).  Many
+// instances on concurrent streams (S2Buffers::concurrent) gain more from the 16 resident warps of
+// the 256-thread shape, which they keep.  The volume-node kernel is fastest in the 256-thread shape
+// in both cases.
 constexpr int kS2NodeThreads = 128;
 
 // build_targets, closure part: one warp per (cell, volume node) -> the node scalars
-template <int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_s2_target_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
+__global__ void __launch_bounds__(256, 2) k_s2_target_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
     if (eval_cached(B)) return;
     const int nc = P.nx * P.ny, lane = threadIdx.x & 31;
     const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (wid >= nc * 9) return;
-    __shared__ double s_jac[NT / 32][16];
+    __shared__ double s_jac[8][16];
     double w[4];
 #pragma unroll
     for (int m = 0; m < 4; ++m) w[m] = SB.wq[(size_t)wid * 4 + m];
@@ -1610,8 +1610,7 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     }
     if (e == cudaSuccess && targets) {
         cudaStream_t ts = side_targets ? s2 : s;
-        if (S.concurrent) k_s2_target_nodes<256, 2><<<warps((long long)nc * 9), 256, 0, ts>>>(P, B, S);
-        else k_s2_target_nodes<kS2NodeThreads, 3><<<node_ctas((long long)nc * 9), kS2NodeThreads, 0, ts>>>(P, B, S);
+        k_s2_target_nodes<<<warps((long long)nc * 9), 256, 0, ts>>>(P, B, S);
         e = cudaGetLastError();
         if (e == cudaSuccess) {
             k_s2_target_sum<<<dim3((unsigned)((nv + 255) / 256), (unsigned)nc), 256, 0, ts>>>(P, B, S);
