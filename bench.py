@@ -14,6 +14,9 @@ itself prescribes), no dataset is involved.
                  from pinned host memory, runs to the gate and downloads the final state.
   roofline       the dominant stage of the pseudo-step (per-stage CUDA events in a separate
                  profiling pass, same stream) against its algorithmic bytes.
+  fp64           (in roofline and in each method's object) algorithmic FP64 operations per update
+                 (counted by oracle/count_flops.py) x updates/s, against a cuBLAS float64 GEMM
+                 measured in the same run; the S2 paths are bound by FP64, not by HBM.
   cpu_baseline   the C oracle (a restatement of the reference's Fortran; the Fortran itself does not
                  build on this image) timed on a bounded number of pseudo-steps of the same case.
   explicit_plain the plain second-order Explicit step (1000 steps, CFL 0.5, omega 0.81) for context.
@@ -67,6 +70,11 @@ BYTES_PER_UPDATE_EXPLICIT = 32
 # pr2_sweep works on the macroscopic fields: per cell W, X, rate, gamma (4 each), two 16-value face
 # flux tables, and writes Y (4): 52 doubles per cell per launch
 PR2_BYTES_PER_CELL = 52 * 8
+# Algorithmic FP64 operations per cell*velocity update (add/sub + mul + div + sqrt), counted by the
+# op-counting build of the oracle on the 8x64x1024 cases (python oracle/count_flops.py).  The
+# implicit pseudo-steps count one evaluation less than the reference runs: the device reuses the
+# accepted-state evaluation as the next pre-update one (reference: 3568 and 58725).
+FLOPS_PER_UPDATE = {"explicit": 1565.9, "implicit_steady": 2211.5, "high_order_implicit": 29736.7, "s2cn2": 29241.7}
 WORKLOAD = ("ImplicitSteady 2nd-order UGKS Couette 8x64 cells, 32x32 velocities (velocity_half32_scale2), "
             "CFL 0.1, nCFL 1000, Kn 0.1, mass rescale on, cold start to the five-state gate (tol 1e-8)")
 
@@ -78,6 +86,33 @@ def peaks():
         return float(p["hbm_gbs"]), "measured"
     except Exception:
         return 6650.0, "fallback"
+
+
+def fp64_peak(device):
+    """FP64 throughput of this GPU in TFLOP/s: a cuBLAS float64 GEMM (8192^3) through torch, the
+    denominator of the FP64 fractions (B200's nominal FP64 and FP64 tensor peaks are both 37 TFLOP/s)."""
+    import torch
+    n = 8192
+    a = torch.randn(n, n, dtype=torch.float64, device=device)
+    b = torch.randn(n, n, dtype=torch.float64, device=device)
+    for _ in range(2):
+        torch.matmul(a, b)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record()
+    for _ in range(5):
+        torch.matmul(a, b)
+    e1.record()
+    e1.synchronize()
+    t = e0.elapsed_time(e1) * 1e-3 / 5
+    del a, b
+    torch.cuda.empty_cache()
+    return 2.0 * n ** 3 / t / 1e12
+
+
+def fp64_fraction(flops_per_update, updates_per_s, peak_tflops):
+    achieved = flops_per_update * updates_per_s / 1e12
+    return {"flops_per_update": flops_per_update, "achieved_tflops": achieved, "peak_tflops": peak_tflops,
+            "frac": achieved / peak_tflops, "peak_source": "cuBLAS float64 GEMM 8192^3 measured in this run"}
 
 
 class ClockSampler:
@@ -417,7 +452,7 @@ def main():
     achieved = BYTES_PER_UPDATE_PSEUDO_STEP * value / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": None, "kernel": "ImplicitSteady pseudo-step (one CUDA graph node group, %d launches)"
-                % (16 + case.macro_sweeps),
+                % (14 + case.macro_sweeps),
                 "bytes_per_update": BYTES_PER_UPDATE_PSEUDO_STEP, "peak_source": peak_kind,
                 "pseudo_step_us": ms / args.steps / (sum(pseudo) / len(pseudo)) * 1e3,
                 "dominant_stage": {"stage": top, "kernel": kname, "avg_us_per_launch": avg_s * 1e6,
@@ -428,6 +463,8 @@ def main():
                 "note": "one 8.4 MB instance is L2-resident and the step is latency-bound: pr2_sweep and "
                         "the LU-SGS stages are Gauss-Seidel wavefronts, chains of (rows+nx-1) dependent "
                         "relaxations per pass; stage times come from an un-graphed event pass"}
+    fpk = fp64_peak(f"cuda:{local}")
+    roofline["fp64"] = fp64_fraction(FLOPS_PER_UPDATE["implicit_steady"], value / world, fpk)
 
     # ---------------- BASELINE's tolerance 1e-10 (the reference's case file uses 1e-8)
     s10 = Solver(case.with_(residual_tol=1e-10), *vel, device=local)
@@ -464,6 +501,7 @@ def main():
                 "config": "Explicit 8x64x1024, CFL 0.5, omega 0.81, 1000 steps from the cold start, CUDA graphs",
                 "kernel_avg_us": {k: 1e3 * t / max(n, 1) for k, (t, n) in kt.items()},
                 "faces_roofline_frac": (BYTES_PER_UPDATE_EXPLICIT * nc * nv / (kt["faces"][0] / kt["faces"][1] * 1e-3) / 1e9) / peak}
+    explicit["fp64"] = fp64_fraction(FLOPS_PER_UPDATE["explicit"], explicit["value"], fpk)
 
     # ---------------- HighOrderImplicit: the cold start to the 3000 pseudo-step cap (the reference run
     # also stops at its iteration limit, analysis.json high_implicit status)
@@ -487,6 +525,7 @@ def main():
                   "c_minus_1": float(rep_h[52]), "science_1_4": [float(x) for x in rep_h[12:16]],
                   "Rh_Rb": [float(rep_h[24]), float(rep_h[25])],
                   "hbm_roofline_frac": BYTES_PER_UPDATE_PSEUDO_STEP * ho_value / 1e9 / peak,
+                  "fp64": fp64_fraction(FLOPS_PER_UPDATE["high_order_implicit"], ho_value, fpk),
                   "config": "HighOrderImplicit 8x64x1024 (WENO5-AO S2 evolution, PR2 + LU-SGS, 8 slabs), CFL 0.1, "
                             "nCFL 1000, mass rescale on, cold start, 3000 pseudo-step cap; FP64-bound (the "
                             "closures and WENO templates), so the HBM fraction is small by construction"}
@@ -535,6 +574,7 @@ def main():
     s2cn2 = {"value": cn_value, "unit": UNIT, "steps": int(done_c2), "ms_per_step": cms / max(done_c2, 1),
              "cnres": float(rep_c2[1]), "mmerr": float(rep_c2[2]), "drift": float(rep_c2[9]),
              "hbm_roofline_frac": BYTES_PER_UPDATE_EXPLICIT * cn_value / 1e9 / peak,
+             "fp64": fp64_fraction(FLOPS_PER_UPDATE["s2cn2"], cn_value, fpk),
              "config": "S2CN2 8x64x1024, CFL 0.1, 8 steps warm-up then 400 steps, two steps per CUDA graph; "
                        "FP64-bound"}
 
@@ -569,6 +609,9 @@ def main():
                "steps": BATCH_STEPS, "ms_per_batched_step": bms / BATCH_STEPS, "streams": int(k_tuned),
                "all_accepted": bool((bdone == BATCH_STEPS).all() and not bst.any()),
                "vs_plain_s2cn2": b_value / (world * s2cn2["value"]),
+               "fp64": dict(fp64_fraction(FLOPS_PER_UPDATE["s2cn2"], b_value / world, fpk),
+                            note="flops per update counted on the 8x64x1024 S2CN2 case and applied to every "
+                                 "instance size"),
                "gpu_launches": int(bt.launch_count - blaunch0),
                "full_run_estimate_s": 2000 * bms / BATCH_STEPS * 1e-3,
                "config": "256 S2CN2 instances, seed PCG64(20261203), CFL 0.1, omega 0.5, cold start; 2 steps "
