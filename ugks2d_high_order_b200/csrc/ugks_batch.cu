@@ -292,7 +292,7 @@ extern "C" int ugks_batch_init_freestream(ugks_batch* b, double rho, double U, d
         BCK(launch_lo_init(I.P, I.B[0], rho, U, V, tnative, S.s));
         BCK(s2_enqueue(0, I.P, I.B[0], I.T[0], S.s, S.s2, S.fork, S.join));
         BCK(enqueue_s2cn2_prepare(I.P, I.B[0], I.T[0], I.C, S.s, nullptr));
-        b->launches += 4;
+        b->launches += 1 + s2_enqueue_kernels(0) + 1 + s2_enqueue_kernels(3);   // init, cold start, prepare
     }
     BCK(cudaDeviceSynchronize());
     std::vector<unsigned> f((size_t)b->n * 4);
@@ -327,7 +327,7 @@ extern "C" int ugks_batch_run(ugks_batch* b, int nsteps, int* steps_done, unsign
         for (int q = 0; q < pairs; ++q) BCK(cudaGraphLaunch(b->graph, b->origin));
     }
     if (nsteps % 2) BCK(enqueue_all(b, 1));
-    b->launches += 7LL * nsteps * b->n;
+    b->launches += (long long)kCnStepKernels * nsteps * b->n;
     std::vector<unsigned> f((size_t)b->n * 4);
     BCK(cudaMemcpyAsync(f.data(), b->flags, f.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, b->origin));
     BCK(cudaStreamSynchronize(b->origin));

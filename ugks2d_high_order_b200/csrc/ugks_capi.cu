@@ -365,12 +365,12 @@ extern "C" int ugks_init_freestream(ugks_ctx* c, double rho, double U, double V,
     c->launches += 1;
     if (c->imem && c->Q.high_order) {   // S2NativeInitializeState cold start: h, b := closure Maxwellian of W
         UGKS_CK(s2_enqueue(0, c->P, c->B, c->I.s2, c->stream, c->stream2, c->ev_fork, c->ev_join));
-        c->launches += 1;
+        c->launches += s2_enqueue_kernels(0);
     }
     if (c->cmem) {   // the same cold start, then the S2CN2 ledger and the targets of the state
         UGKS_CK(s2_enqueue(0, c->P, c->B, c->T[0], c->stream, c->stream2, c->ev_fork, c->ev_join));
         UGKS_CK(enqueue_s2cn2_prepare(c->P, c->Bs[0], c->T[0], c->C, c->stream, &c->launches));
-        c->launches += 1;
+        c->launches += s2_enqueue_kernels(0);
         c->cn_ready = true;
     }
     int r = kernel_timestep(c);
@@ -813,7 +813,7 @@ extern "C" int ugks_s2cn2_steps(ugks_ctx* c, int nsteps, int* steps_done, double
         for (int q = 0; q < pairs; ++q) UGKS_CK(cudaGraphLaunch(c->cgraph, c->stream));
     }
     if (nsteps % 2) UGKS_CK(enqueue_cn_step(c, 0));
-    c->launches += 7LL * nsteps;
+    c->launches += (long long)kCnStepKernels * nsteps;
     unsigned acc = 0;
     UGKS_CK(cudaMemcpyAsync(&acc, c->C.accepted, sizeof acc, cudaMemcpyDeviceToHost, c->stream));
     if (report) UGKS_CK(cudaMemcpyAsync(report, c->C.report, kCnReport * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

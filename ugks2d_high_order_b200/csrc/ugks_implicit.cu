@@ -1366,9 +1366,6 @@ static cudaError_t im_fluxes(const LoParams& P, const LoBuffers& B, cudaStream_t
     return e;
 }
 
-// One ImplicitSteady pseudo-step (mod_Solve.f90:84-293 with TimeIntegration_method =
-// 'ImplicitSteady' and ClosedCouetteMassRescale): 19 kernels, no host synchronisation.
-// Returns the number of kernels launched through *launches.
 // Shared-memory opt-in of the sweep kernels for this slab size (slab rows x nx <= kMaxSlabCells).
 cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q) {
     const int rows = P.ny / Q.nslab, ncs = rows * P.nx;
@@ -1383,8 +1380,13 @@ cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q) {
     return e;
 }
 
-// One accepted pseudo-step.  marks (optional, profile runs only): kImStages + 1 events recorded on
-// s at the start and after each stage of kImStageNames.
+// One ImplicitSteady pseudo-step (mod_Solve.f90:84-293 with TimeIntegration_method =
+// 'ImplicitSteady' and ClosedCouetteMassRescale): 16 + macro_sweeps kernels with the second-order
+// evaluations (3 kernels each), 6 more per evaluation with the S2 one of HighOrderImplicit, no host
+// synchronisation.
+// Returns the number of kernels launched through *launches.
+// marks (optional, profile runs only): kImStages + 1 events recorded on s at the start and after
+// each stage of kImStageNames.
 cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
                                   cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
                                   long long* launches, cudaEvent_t* marks) {
@@ -1431,7 +1433,8 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     if (e == cudaSuccess)                                                         // accepted-state evaluation
         e = mark(Q.high_order ? s2_enqueue(1, P, Bh, I.s2, s, s2, fork, join) : im_fluxes(P, Bh, s, s2, fork, join));
     if (e == cudaSuccess) e = mark(im_cell(1, P, B, Q, I, nullptr, s));
-    if (launches) *launches += 14 + Q.macro_sweeps + (Q.high_order ? 2 : 0);
+    const int evaluation = Q.high_order ? s2_enqueue_kernels(1) : 3;   // im_fluxes: slopes, faces, walls
+    if (launches) *launches += 10 + Q.macro_sweeps + 2 * evaluation;
     return e;
 }
 

@@ -74,5 +74,11 @@ cudaError_t prepare_s2();
 // reconstruction, faces, walls); 2: S2 Evolution with the targets in S kept; 3: targets of B.W into S
 cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S2Buffers& S, cudaStream_t s,
                        cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join);
+// kernels s2_enqueue(which, ...) launches: the cold start 1; the macro pass, then 2 for the targets
+// (volume nodes, sum) and 6 for the evolution (reconstruction x2, wall nodes, face nodes, face flux,
+// combine)
+constexpr int s2_enqueue_kernels(int which) {
+    return which == 0 ? 1 : 1 + (which != 2 ? 2 : 0) + (which != 3 ? 6 : 0);
+}
 
 }  // namespace ugks

@@ -2,7 +2,7 @@
 //
 // One step (TimeStep; S2NativeEvolution with the volume targets kept between steps,
 // mod_S2NativeAdapter.f90:469-490; ComputeResidual; S2NativeApplyUpdate, :867-940, whose
-// advance_step, mod_S2D1.f90:1302-1435, runs on the stream state) is seven launches:
+// advance_step, mod_S2D1.f90:1302-1435, runs on the stream state) is 13 launches:
 //   k_lo_timestep  : dt of the accepted state.
 //   S2 evolution   : reconstruction, interior faces and (side stream) walls of ugks_s2.cu, with the
 //                    accepted state's targets.
@@ -343,7 +343,7 @@ cudaError_t enqueue_s2cn2_step(const LoParams& P, const LoBuffers& B, const S2Bu
         if (P.nvel <= 1024) e = cn_launch<4, 256>(P, B, T, Bo, To, C, s);
         else e = cn_launch<10, 256>(P, B, T, Bo, To, C, s);
     }
-    if (launches) *launches += 7;
+    if (launches) *launches += kCnStepKernels;
     return e;
 }
 
@@ -352,7 +352,7 @@ cudaError_t enqueue_s2cn2_prepare(const LoParams& P, const LoBuffers& B, const S
     k_cn_ledger<<<1, 256, 0, s>>>(P, B, C);
     cudaError_t e = cudaGetLastError();
     if (e == cudaSuccess) e = s2_enqueue(3, P, B, T, s, s, nullptr, nullptr);
-    if (launches) *launches += 2;
+    if (launches) *launches += 1 + s2_enqueue_kernels(3);
     return e;
 }
 

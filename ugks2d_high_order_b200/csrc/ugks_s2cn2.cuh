@@ -6,6 +6,10 @@ namespace ugks {
 
 constexpr int kCnCell = 8;     // per-cell advance diagnostics
 constexpr int kCnReport = 24;  // report of the last step (layout at enqueue_s2cn2_step)
+// kernels of one S2CN2 step: timestep, the evolution keeping the targets, k_cn_stream, the targets of
+// the stream state, k_cn_collide
+constexpr int kCnStepKernels = 1 + s2_enqueue_kernels(2) + 1 + s2_enqueue_kernels(3) + 1;
+static_assert(kCnStepKernels == 13, "one S2CN2 step launches 13 kernels");
 
 struct CnBuffers {
     double* ws;          // [nc][4]    stream state W + res_w (the proposal's W)
