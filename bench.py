@@ -452,7 +452,7 @@ def main():
     achieved = BYTES_PER_UPDATE_PSEUDO_STEP * value / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": None, "kernel": "ImplicitSteady pseudo-step (one CUDA graph node group, %d launches)"
-                % (14 + case.macro_sweeps),
+                % (16 + case.macro_sweeps),
                 "bytes_per_update": BYTES_PER_UPDATE_PSEUDO_STEP, "peak_source": peak_kind,
                 "pseudo_step_us": ms / args.steps / (sum(pseudo) / len(pseudo)) * 1e3,
                 "dominant_stage": {"stage": top, "kernel": kname, "avg_us_per_launch": avg_s * 1e6,
