@@ -24,6 +24,8 @@ itself prescribes), no dataset is involved.
                  3000-pseudo-step cap, c_minus_1 recorded, with a bounded oracle sample beside it.
   s2cn2          the explicit high-order S2CN2 step (S2 evolution + Crank-Nicolson collision) on the same
                  case, with a bounded oracle sample beside it.
+  adjoint_shape  the adjoint config's 64 cases (8x64x1024): the adjoint is not built; the batch gives the
+                 gradients by central differences (7 instances per case), timed against the forward batch.
   batched        (N > 1: the instances are split over the ranks by an LPT greedy on cells x velocities,
                  no collective; time = max over ranks; value = all instances' work / that time)
                  256 S2CN2 instances of the batched distribution (Kn log-uniform in [0.01, 1], wall Mach
@@ -58,6 +60,7 @@ HO_MAX_PSEUDO_STEPS = 3000     # HighOrderImplicit cap (cases/high_implicit/Conf
 S2CN2_STEPS = 400
 REFINED_PSEUDO_STEPS = 100   # timed pseudo-steps of the refined HighOrderImplicit variant
 BATCH_STEPS = 4               # batched steps timed (each advances all 256 instances by one step)
+C5_STEPS = 2                  # steps timed at the adjoint config's shape (64 cases, 8x64x1024)
 # algorithmic bytes per cell*velocity of the stages (FP64 h and b):
 #   lusgs_forward  reads the right-hand side (h, b) and writes the correction (h, b)      32 B
 #   lusgs_backward also reads the forward correction                                   48 B
@@ -619,6 +622,43 @@ def main():
                          "(the distribution's full run is 2000 steps)"}
     bt.close()
 
+    # ---------------- the adjoint config's shape: 64 cases of the batched distribution at 8x64 cells and
+    # 32^2 velocities.  The adjoint is not built; the wall-output gradients come from central
+    # differences on the batch (7 instances per case, ugks2d_high_order_b200.sensitivity), timed here
+    # against the forward batch of the same cases.
+    from ugks2d_high_order_b200.sensitivity import sensitivity_instances
+
+    def batch_ms_per_step(instances, steps):
+        bb = Batch(instances, device=local, max_streams=32)
+        try:
+            bb.init_freestream()
+            bb.run(1)
+            st_ = torch.cuda.ExternalStream(bb.stream)
+            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            with torch.cuda.stream(st_):
+                f0.record(st_)
+                bb.run(steps)
+                f1.record(st_)
+            f1.synchronize()
+            return f0.elapsed_time(f1) / steps
+        finally:
+            bb.close()
+
+    c5_all = [(c.with_(ny=64, dy=1.0 / 64), 32) for c, _ in batched_cases(64)]
+    c5, _ = shard(c5_all, [1] * len(c5_all), rank, world)
+    fwd_ms = batch_ms_per_step([(c, tables[n]) for c, n in c5], C5_STEPS)
+    sens_ms = batch_ms_per_step(sensitivity_instances(c5), C5_STEPS)
+    barrier()
+    fwd_ms, sens_ms = max_over_ranks(fwd_ms), max_over_ranks(sens_ms)
+    adjoint_shape = {"adjoint": "not built", "gradients": "central differences on the batch: per case the base "
+                     "instance and +-1e-6 relative steps of wall speed, wall temperature and the tau scale",
+                     "cases": len(c5_all), "steps": C5_STEPS, "forward_ms_per_step": fwd_ms,
+                     "gradients_ms_per_step": sens_ms, "cost_vs_forward": sens_ms / fwd_ms,
+                     "full_run_estimate_s": 2000 * sens_ms * 1e-3,
+                     "config": "64 S2CN2 cases of the batched distribution at 8x64 cells, 32x32 velocities, "
+                               "cold start; 1 step warm-up, then the timed steps (the config's run is 2000 "
+                               "steps)"}
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
@@ -651,6 +691,7 @@ def main():
                 "high_order_implicit": high_order,
                 "s2cn2": s2cn2,
                 "batched": batched,
+                "adjoint_shape": adjoint_shape,
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
     s.close()
