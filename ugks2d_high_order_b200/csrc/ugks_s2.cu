@@ -427,12 +427,14 @@ __global__ void __launch_bounds__(256, 3) k_s2_recon2(LoParams P, LoBuffers B, S
 #pragma unroll
     for (int w = 1; w < 8; ++w) theta = fmin(theta, s_th[w][lane]);
     theta = (hm <= 0.0 || bm <= 0.0) ? 0.0 : fmax(0.0, fmin(1.0, theta));
-    const double nd = p < 2 ? P.dx : P.dy, td = p < 2 ? P.dy : P.dx;
+    // the derivatives are divided by the cell sizes (limit_cell_outputs): multiplied by the reciprocals
+    // here, exact when dx and dy are powers of two (the delivered meshes), within an ulp otherwise
+    const double ind = 1.0 / (p < 2 ? P.dx : P.dy), itd = 1.0 / (p < 2 ? P.dy : P.dx);
     double* r = S.rec + (size_t)cc * 72 * nv + k;
     const int fv = f == 0 ? 0 : 1, fn = f == 0 ? 2 : 4, ft = f == 0 ? 3 : 5;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const double v = mf + theta * (face[a] - mf), n = theta * dn[a] / nd, t = theta * dt[a] / td;
+        const double v = mf + theta * (face[a] - mf), n = theta * dn[a] * ind, t = theta * dt[a] * itd;
         if (kok) {
             r[(size_t)(fv * 12 + p * 3 + a) * nv] = v;
             r[(size_t)(fn * 12 + p * 3 + a) * nv] = n;
