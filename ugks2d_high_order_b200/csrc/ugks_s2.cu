@@ -75,17 +75,29 @@ __device__ __forceinline__ bool s2_weno(const double q[5], S2Weno& w) {
     s = s - 51001 * q4 * q5;
     s = s + 6908 * (q5 * q5);
     // the reference's divisions by 5040, 3, sum(alpha) and gamma_4 are multiplications by the
-    // reciprocals here (each weight moves by at most an ulp); tau / (beta + 1e-8) stays a division
+    // reciprocals here (each weight moves by at most an ulp)
     beta[3] = s * (1.0 / 5040.0);
     double tau = fabs(beta[3] - beta[0]);
     tau = tau + fabs(beta[3] - beta[1]);
     tau = tau + fabs(beta[3] - beta[2]);
     tau = tau * (1.0 / 3.0);
     const double gam[4] = {0.01125, 0.1275, 0.01125, 0.85};
+    // tau / (beta_c + 1e-8) for the 4 candidates from one reciprocal of the product of the 4
+    // denominators (each quotient within a few ulps of the division); the product of values in
+    // [1e-8, ~1e7] cannot leave the normal range, and a non-finite reciprocal falls back to division
+    const double d0 = beta[0] + 1.0e-8, d1 = beta[1] + 1.0e-8, d2 = beta[2] + 1.0e-8, d3 = beta[3] + 1.0e-8;
+    const double p01 = d0 * d1, p23 = d2 * d3, ip = 1.0 / (p01 * p23);
+    double inv[4];
+    if (isfinite(ip) && ip > 0.0) {
+        const double a = p23 * ip, b = p01 * ip;
+        inv[0] = d1 * a; inv[1] = d0 * a; inv[2] = d3 * b; inv[3] = d2 * b;
+    } else {
+        inv[0] = 1.0 / d0; inv[1] = 1.0 / d1; inv[2] = 1.0 / d2; inv[3] = 1.0 / d3;
+    }
     double alpha[4], sa = 0.0;
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-        const double r = tau / (beta[c] + 1.0e-8);
+        const double r = tau * inv[c];
         alpha[c] = gam[c] * (1.0 + r * r);
         sa = sa + alpha[c];
     }
