@@ -27,7 +27,7 @@ cudaError_t launch_im_init(const LoParams& P, const LoBuffers& B, const ImParams
 cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q);
 cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
                                   cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
-                                  long long* launches, cudaEvent_t* marks);
+                                  long long* launches, cudaEvent_t* marks, const ImCapture* cond = nullptr);
 }  // namespace ugks
 
 using namespace ugks;
@@ -62,6 +62,7 @@ struct ugks_ctx {
     cudaGraphExec_t igraph = nullptr;
     int igraph_steps = 0;
     long long igraph_launches = 0;
+    ImCapture icap{};                          // body capture of the conditional pre-update evaluation
     double* hstate = nullptr;                  // pinned [2][IS_COUNT]: the state after each graph batch
     cudaEvent_t rb_ev[2] = {nullptr, nullptr};  // its copy has landed
     // profiling
@@ -303,6 +304,10 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->imem) cudaFree(c->imem);
     if (c->iflags) cudaFree(c->iflags);
     if (c->hstate) cudaFreeHost(c->hstate);
+    if (c->icap.s) cudaStreamDestroy(c->icap.s);
+    if (c->icap.s2) cudaStreamDestroy(c->icap.s2);
+    if (c->icap.fork) cudaEventDestroy(c->icap.fork);
+    if (c->icap.join) cudaEventDestroy(c->icap.join);
     for (int i = 0; i < 2; ++i) if (c->rb_ev[i]) cudaEventDestroy(c->rb_ev[i]);
     for (int i = 0; i < 5; ++i) if (c->ev[i]) cudaEventDestroy(c->ev[i]);
     for (int i = 0; i <= kImStages; ++i) if (c->im_ev[i]) cudaEventDestroy(c->im_ev[i]);
@@ -616,7 +621,8 @@ extern "C" int ugks_implicit_init(ugks_ctx* c) {
     if (!c->imem) return UGKS_EUNSUPPORTED;
     UGKS_CK(cudaSetDevice(c->device));
     UGKS_CK(launch_im_init(c->P, c->B, c->Q, c->I, c->stream));
-    c->launches += 1;
+    // + the first pseudo-step's pre-update S2 evaluation and residual (in graphs a conditional body)
+    c->launches += 1 + (c->Q.high_order ? 1 + s2_enqueue_kernels(1) : 0);
     c->implicit_ready = true;
     return collect_status(c);
 }
@@ -630,7 +636,8 @@ extern "C" int ugks_implicit_restore(ugks_ctx* c, double m0, double reference_h,
     if (have_reference && !(std::isfinite(reference_h) && std::isfinite(reference_b))) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
     UGKS_CK(launch_im_init(c->P, c->B, c->Q, c->I, c->stream));
-    c->launches += 1;
+    // + the first pseudo-step's pre-update S2 evaluation and residual (in graphs a conditional body)
+    c->launches += 1 + (c->Q.high_order ? 1 + s2_enqueue_kernels(1) : 0);
     static_assert(IS_REF_H == IS_M0 + 1 && IS_REF_B == IS_M0 + 2 && IS_REF_INIT == IS_M0 + 3,
                   "M0 and the residual references are contiguous state words");
     const double v[4] = {m0, have_reference ? reference_h : 0.0, have_reference ? reference_b : 0.0,
@@ -644,12 +651,22 @@ extern "C" int ugks_implicit_restore(ugks_ctx* c, double m0, double reference_h,
 static int build_implicit_graph(ugks_ctx* c, int steps) {
     if (c->igraph && c->igraph_steps == steps) return UGKS_OK;
     if (c->igraph) { cudaGraphExecDestroy(c->igraph); c->igraph = nullptr; }
+    if (!c->icap.s) {
+        UGKS_CK(cudaStreamCreateWithFlags(&c->icap.s, cudaStreamNonBlocking));
+        UGKS_CK(cudaStreamCreateWithFlags(&c->icap.s2, cudaStreamNonBlocking));
+        UGKS_CK(cudaEventCreateWithFlags(&c->icap.fork, cudaEventDisableTiming));
+        UGKS_CK(cudaEventCreateWithFlags(&c->icap.join, cudaEventDisableTiming));
+    }
     cudaGraph_t g;
     long long n = 0;
     UGKS_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
     cudaError_t e = cudaSuccess;
     for (int s = 0; s < steps && e == cudaSuccess; ++s)
-        e = enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork, c->ev_join, &n, nullptr);
+        // the S2 pre-update evaluation goes into a conditional body (its skipped kernels launch grids of
+        // 16k CTAs); the second-order one keeps its launches, which return at entry more cheaply than the
+        // conditional node costs
+        e = enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork, c->ev_join, &n, nullptr,
+                                  c->Q.high_order ? &c->icap : nullptr);
     cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
     if (e != cudaSuccess) { if (e2 == cudaSuccess) cudaGraphDestroy(g); return cuda_fail(e); }
     UGKS_CK(e2);

@@ -1387,9 +1387,23 @@ cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q) {
 // Returns the number of kernels launched through *launches.
 // marks (optional, profile runs only): kImStages + 1 events recorded on s at the start and after
 // each stage of kImStageNames.
+// Sets the condition of the pre-update evaluation's conditional graph node: 1 when the evaluation must
+// run (the previous accepted-state evaluation does not apply: first pseudo-step, or dt changed), 0
+// when it is reused, in which case its science columns are copied into the report here, as the
+// skipped residual kernel would have done.  One warp.
+__global__ void k_im_pre_gate(LoBuffers Bpre, ImBuffers I, cudaGraphConditionalHandle h) {
+    const bool cached = eval_cached(Bpre);
+    if (threadIdx.x == 0) cudaGraphSetConditional(h, cached ? 0u : 1u);
+    if (cached && I.state[IS_STOP] == 0.0 && threadIdx.x < 22)
+        I.report[57 + threadIdx.x] = I.state[IS_PRESCI + threadIdx.x];
+}
+
+// cond (graph capture only): the pre-update evaluation and its residual go into the body of a
+// conditional node that k_im_pre_gate enables, so a reused evaluation launches none of its kernels;
+// without it they are launched and return at entry.
 cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const ImParams& Q, const ImBuffers& I,
                                   cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
-                                  long long* launches, cudaEvent_t* marks) {
+                                  long long* launches, cudaEvent_t* marks, const ImCapture* cond) {
     int stage = 0;
     auto mark = [&](cudaError_t e) -> cudaError_t {
         if (e == cudaSuccess && marks) e = cudaEventRecord(marks[stage++], s);
@@ -1403,9 +1417,40 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     Bpre.eval = I.state + IS_EVAL_VALID;
     cudaError_t e = mark(cudaSuccess);
     if (e == cudaSuccess) e = mark(launch_lo_timestep(P, Bh, s));                // TimeStep
-    if (e == cudaSuccess)                                                         // Interpolation + Evolution
-        e = Q.high_order ? s2_enqueue(1, P, Bpre, I.s2, s, s2, fork, join) : im_fluxes(P, Bpre, s, s2, fork, join);
-    if (e == cudaSuccess) e = mark(im_cell(0, P, Bpre, Q, I, nullptr, s));       // ComputeResidual + diagnostics
+    if (e == cudaSuccess && cond) {
+        cudaStreamCaptureStatus cs;
+        cudaGraph_t g = nullptr;
+        const cudaGraphNode_t* deps = nullptr;
+        size_t nd = 0;
+        cudaGraphConditionalHandle h = 0;
+        e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd);
+        if (e == cudaSuccess && cs != cudaStreamCaptureStatusActive) e = cudaErrorStreamCaptureInvalidated;
+        if (e == cudaSuccess) e = cudaGraphConditionalHandleCreate(&h, g, 0, cudaGraphCondAssignDefault);
+        if (e == cudaSuccess) { k_im_pre_gate<<<1, 32, 0, s>>>(Bpre, I, h); e = cudaGetLastError(); }
+        if (e == cudaSuccess) e = cudaStreamGetCaptureInfo(s, &cs, nullptr, &g, &deps, &nd);
+        cudaGraphNodeParams np = {};
+        np.type = cudaGraphNodeTypeConditional;
+        np.conditional.handle = h;
+        np.conditional.type = cudaGraphCondTypeIf;
+        np.conditional.size = 1;
+        cudaGraphNode_t node = nullptr;
+        if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, deps, nd, &np);
+        if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(cond->s, np.conditional.phGraph_out[0], nullptr,
+                                                                nullptr, 0, cudaStreamCaptureModeThreadLocal);
+        if (e == cudaSuccess) {
+            cudaError_t eb = Q.high_order ? s2_enqueue(1, P, Bpre, I.s2, cond->s, cond->s2, cond->fork, cond->join)
+                                          : im_fluxes(P, Bpre, cond->s, cond->s2, cond->fork, cond->join);
+            if (eb == cudaSuccess) eb = im_cell(0, P, Bpre, Q, I, nullptr, cond->s);
+            cudaGraph_t body = nullptr;
+            e = cudaStreamEndCapture(cond->s, &body);
+            if (eb != cudaSuccess) e = eb;
+        }
+        if (e == cudaSuccess) e = cudaStreamUpdateCaptureDependencies(s, &node, 1, cudaStreamSetCaptureDependencies);
+    } else {
+        if (e == cudaSuccess)                                                     // Interpolation + Evolution
+            e = Q.high_order ? s2_enqueue(1, P, Bpre, I.s2, s, s2, fork, join) : im_fluxes(P, Bpre, s, s2, fork, join);
+        if (e == cudaSuccess) e = mark(im_cell(0, P, Bpre, Q, I, nullptr, s));   // ComputeResidual + diagnostics
+    }
     const double* X = I.dwA;
     double* Y = I.dwB;
     const int rows = P.ny / Q.nslab, ncs = rows * P.nx;
@@ -1433,8 +1478,12 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     if (e == cudaSuccess)                                                         // accepted-state evaluation
         e = mark(Q.high_order ? s2_enqueue(1, P, Bh, I.s2, s, s2, fork, join) : im_fluxes(P, Bh, s, s2, fork, join));
     if (e == cudaSuccess) e = mark(im_cell(1, P, B, Q, I, nullptr, s));
-    const int evaluation = Q.high_order ? s2_enqueue_kernels(1) : 3;   // im_fluxes: slopes, faces, walls
-    if (launches) *launches += 10 + Q.macro_sweeps + 2 * evaluation;
+    // im_fluxes: slopes, faces, walls.  With cond the pre-update evaluation (and its residual) are a
+    // conditional body, not counted here: it runs only when no accepted-state evaluation applies
+    // (counted once per sequence by ugks_implicit_init / ugks_implicit_restore); the gate replaces the
+    // pre-update residual in the count
+    const int evaluation = Q.high_order ? s2_enqueue_kernels(1) : 3;
+    if (launches) *launches += 10 + Q.macro_sweeps + (cond ? evaluation : 2 * evaluation);
     return e;
 }
 

@@ -40,6 +40,12 @@ constexpr const char* kImStageNames[kImStages] = {
     "timestep", "pre_evaluation", "pr2_sweep", "equilibrium", "lusgs_forward", "wall_closure",
     "lusgs_backward", "micro_alpha", "apply", "rescale", "post_fluxes", "post_residual"};
 
+// Streams and events of the pre-update evaluation's conditional graph body (graph capture only).
+struct ImCapture {
+    cudaStream_t s, s2;
+    cudaEvent_t fork, join;
+};
+
 struct ImParams {
     int nslab;              // ranks of the reference's 1 x NP_Y blocking (rows per slab = ny / nslab)
     int mass_rescale;
