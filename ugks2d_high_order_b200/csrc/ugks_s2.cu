@@ -1091,30 +1091,28 @@ __global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffer
         const double nrho = w0[0], nu = w0[1] / w0[0], nvv = w0[2] / w0[0];
         const double temp = 4.0 * (w0[3] / w0[0] - 0.5 * (nu * nu + nvv * nvv)) / (double)(ck + 2);
         const double lamn = 1.0 / temp;
-        acc[0] = acc[1] = 0.0;
-        for (int r = 0; r < nr; ++r) {
-            const WVel s = wvel(B, nv, r);
-            const double du = s.u - nu, dv = s.v - nvv;
-            const double eah = nrho * lamn / kPi * exp(-lamn * (du * du + dv * dv));
-            const double eab = 0.5 * (double)ck * temp * eah;
-            const double cx = s.u - M.ux, cy = s.v - M.vy, c2 = cx * cx + cy * cy;
-            const double dh = upwind(s, 0) - eah, db = upwind(s, 1) - eab;
-            acc[0] += 0.5 * s.w * cx * (c2 * dh + db);
-            acc[1] += 0.5 * s.w * cy * (c2 * dh + db);
-        }
-        warp_sum_all<2>(acc);
-        q0x = acc[0];
-        q0y = acc[1];
         // directions of the macro normal slopes (left, right) and the tangential slope
         const bool okd = s2_solve4(C.jac, mac, tdl) & s2_solve4(C.jac, mac + 4, tdr) & s2_solve4(C.jac, mac + 8, tdt);
         if (!okd)
 #pragma unroll
             for (int m = 0; m < 4; ++m) tdl[m] = tdr[m] = tdt[m] = NAN;
+        // one pass over the velocities for q0 (qacc) and the direction moments (acc): two independent
+        // chains per velocity, each summed in velocity order and reduced on its own
+        double qacc[2] = {0.0, 0.0};
 #pragma unroll
         for (int m = 0; m < 16; ++m) acc[m] = 0.0;
         const S2Th tt = s2_th(C.th, ck);
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
+            {
+                const double du = s.u - nu, dv = s.v - nvv;
+                const double eah = nrho * lamn / kPi * exp(-lamn * (du * du + dv * dv));
+                const double eab = 0.5 * (double)ck * temp * eah;
+                const double cx = s.u - M.ux, cy = s.v - M.vy, c2 = cx * cx + cy * cy;
+                const double dh = upwind(s, 0) - eah, db = upwind(s, 1) - eab;
+                qacc[0] += 0.5 * s.w * cx * (c2 * dh + db);
+                qacc[1] += 0.5 * s.w * cy * (c2 * dh + db);
+            }
             const S2Q q = s2_q(tt, s.u, s.v);
             double dlh, dlb, drh, drb, dth, dtb;
             s2_dq(q, tdl, dlh, dlb);
@@ -1128,6 +1126,9 @@ __global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffer
             const double fb = vn * (vn >= 0.0 ? dlb : drb) + vt * dtb;
             moment_add(s.w, s.u, s.v, fh, fb, acc + 12);
         }
+        warp_sum_all<2>(qacc);
+        q0x = qacc[0];
+        q0y = qacc[1];
         warp_sum_all<16>(acc);
         for (int d = 0; d < 3; ++d) {   // gates of the three directions
             double mx = 0.0, sc = 1.0;
