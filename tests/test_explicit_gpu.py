@@ -3,7 +3,7 @@
 Tolerances: the device uses CUDA's exp/erfc/pow and tree-ordered FP64 reductions where the oracle
 (and the reference) use libm and sequential sums, so results agree to rounding, not bitwise.
   * per-operator arrays after one step:  max|gpu-oracle| <= 1e-12 * max|oracle|
-  * state after 40 steps:                max|gpu-oracle| <= 1e-11 * max|oracle|   (north_star: 1e-11)
+  * state after 40 steps:                max|gpu-oracle| <= 1e-11 * max|oracle|   (the required 1e-11)
   * reference 2-step `res` line:         equal at its 7 printed digits
 """
 import numpy as np

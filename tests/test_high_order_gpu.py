@@ -3,7 +3,7 @@
 The S2 evolution (closure targets, WENO-AO reconstruction, Gauss-node UGKS faces, multiscale wall)
 and the implicit update with the high-order collision correction, through the C ABI.  The GPU sums
 velocity moments in a tree and the oracle sequentially, and each Newton closure amplifies that
-rounding, so the bound is 1e-9 relative (north_star: the reference's own run-to-run tolerance for
+rounding, so the bound is 1e-9 relative (the required tolerance is the reference's own run-to-run one for
 the high-order path; the oracle itself matches the reference's printed rows to 5e-13).
 """
 import numpy as np

@@ -17,7 +17,6 @@ from ugks2d_high_order_b200.case import (batched_cases, load_velocity_half32, re
                                          refined_high_order_case, velocity_table)
 
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden")
-REF_CASES = "/root/reference/cases"
 METHOD = {"low_explicit": "Explicit", "low_implicit": "ImplicitSteady", "high_implicit": "HighOrderImplicit"}
 
 
@@ -64,19 +63,33 @@ $DIS_para
         refio.parse_namelists("&config_para\n A = 1\n")
 
 
+def config_text(name):
+    """Config.ini of a delivered case, rebuilt from its fixture assignments."""
+    nml = golden()["case_namelists"][name]
+    return "\n".join(f"&{g}\n" + "\n".join(f"{k} = {' '.join(v)}" for k, v in kv.items()) + "\n/"
+                      for g, kv in nml.items()) + "\n"
+
+
 @pytest.mark.parametrize("name", ["low_explicit", "low_implicit", "high_implicit"])
 def test_delivered_namelists_load_as_the_reference_cases(name):
-    nml = golden()["case_namelists"][name]
-    text = "\n".join(f"&{g}\n" + "\n".join(f"{k} = {' '.join(v)}" for k, v in kv.items()) + "\n/"
-                     for g, kv in nml.items())
-    case = refio.case_from_config(refio.parse_namelists(text), mesh())
+    case = refio.case_from_config(refio.parse_namelists(config_text(name)), mesh())
     assert case == reference_case(METHOD[name])
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_CASES), reason="reference case directories not present")
 @pytest.mark.parametrize("name", ["low_explicit", "low_implicit", "high_implicit"])
-def test_reference_case_directories_load_unchanged(name):
-    d = refio.load_case_dir(os.path.join(REF_CASES, name))
+def test_reference_case_directories_load_unchanged(name, tmp_path):
+    """A delivered case directory (the three share one Mesh2d.dat and one velocity file): the binary
+    files are written by the writers and checked against the delivered files' SHA-256, Config.ini
+    holds the delivered assignments; load_case_dir gives the case the GPU tests run."""
+    want = golden()["case_file_sha256"]
+    gx, gy = mesh()
+    refio.write_mesh(str(tmp_path / "Mesh2d.dat"), gx, gy)
+    u, v, w = load_velocity_half32()
+    refio.write_velocity_file(str(tmp_path / "velocity_half32_scale2.dat"), u, v, w, 32, 32)
+    for f in ("Mesh2d.dat", "velocity_half32_scale2.dat"):
+        assert sha(tmp_path / f) == want[f]
+    (tmp_path / "Config.ini").write_text(config_text(name))
+    d = refio.load_case_dir(str(tmp_path))
     assert d.case == reference_case(METHOD[name])
     for x, y in zip((d.u, d.v, d.w), load_velocity_half32()):
         assert np.array_equal(x, y)
