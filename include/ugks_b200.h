@@ -5,7 +5,7 @@
  * argument-less subroutines that act on module globals, called from Solve_UGKS
  * (src/mod_Solve.f90:84-186).  Each entry point below replaces one of them; the citation on each
  * declaration names the routine it stands in for.  Plain pointers and sizes only: a Fortran
- * `bind(C)` interface (see INTEGRATION.md) or ctypes can call every function.
+ * `bind(C)` interface or ctypes can call every function.
  *
  * Host arrays use the reference's backing-store layout with the halo stripped:
  *   h, b : [ny][nx][nvel]  (Fortran cell_h_store(Nvel, 1:nx, 1:ny), velocity fastest)
