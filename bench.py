@@ -69,6 +69,11 @@ C5_STEPS = 2                  # steps timed at the adjoint config's shape (64 ca
 #   post_fluxes    reads h, b and their slopes, writes the face fluxes                   64 B
 #   explicit step  reads h, b, writes h, b                                              32 B
 BYTES_PER_UPDATE_PSEUDO_STEP = 240   # compulsory traffic of one implicit pseudo-step per cell*velocity
+# DRAM bytes (read + write) of one ImplicitSteady pseudo-step at 8x64x1024: the sum over its launches in
+# the ncu launch list of 16 pseudo-steps (dram__bytes_read.sum + dram__bytes_write.sum, 289 launches,
+# init kernels excluded).  ncu flushes the caches before every launch, so this is the cold-cache upper
+# bound of the graph-replayed step, in which the 8.4 MB state and the work arrays stay in L2.
+TRAFFIC_PER_PSEUDO_STEP_8X64X1024 = 149_164_656
 STAGE_BYTES_PER_UPDATE = {"lusgs_forward": 32, "lusgs_backward": 48, "post_residual": 80, "post_fluxes": 64}
 BYTES_PER_UPDATE_EXPLICIT = 32
 # pr2_sweep works on the macroscopic fields: per cell W, X, rate, gamma (4 each), two 16-value face
@@ -455,7 +460,9 @@ def main():
     # device-resident pseudo-step rate
     achieved = BYTES_PER_UPDATE_PSEUDO_STEP * value / 1e9
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                "traffic": None, "kernel": "ImplicitSteady pseudo-step (one CUDA graph node group, %d launches)"
+                "traffic": TRAFFIC_PER_PSEUDO_STEP_8X64X1024 if (case.nx, case.ny, nv) == (8, 64, 1024) else None,
+                "traffic_source": "ncu launch list, cold-cache sum over one pseudo-step's launches",
+                "kernel": "ImplicitSteady pseudo-step (one CUDA graph node group, %d launches)"
                 % (16 + case.macro_sweeps),
                 "bytes_per_update": BYTES_PER_UPDATE_PSEUDO_STEP, "peak_source": peak_kind,
                 "pseudo_step_us": ms / args.steps / (sum(pseudo) / len(pseudo)) * 1e3,
