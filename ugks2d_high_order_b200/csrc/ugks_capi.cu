@@ -65,6 +65,10 @@ struct ugks_ctx {
     ImCapture icap{};                          // body capture of the conditional pre-update evaluation
     double* hstate = nullptr;                  // pinned [2][IS_COUNT]: the state after each graph batch
     cudaEvent_t rb_ev[2] = {nullptr, nullptr};  // its copy has landed
+    cudaGraphExec_t iloop = nullptr;           // WHILE node over the batch graph: the device runs the batches
+    unsigned* iloop_ctr = nullptr;             // device: batches the WHILE node may still run
+    long long iloop_launches = 0;              // kernels per loop iteration
+    bool iloop_unavailable = false;            // its build failed: the host pipeline runs the batches
     // profiling
     bool profile = false;
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
@@ -298,6 +302,8 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->igraph) cudaGraphExecDestroy(c->igraph);
+    if (c->iloop) cudaGraphExecDestroy(c->iloop);
+    if (c->iloop_ctr) cudaFree(c->iloop_ctr);
     if (c->cgraph) cudaGraphExecDestroy(c->cgraph);
     if (c->cmem) cudaFree(c->cmem);
     if (c->cflags) cudaFree(c->cflags);
@@ -678,6 +684,70 @@ static int build_implicit_graph(ugks_ctx* c, int steps) {
     return UGKS_OK;
 }
 
+// Batch budget of the device-driven pseudo-step loop, armed by the host before each loop launch.
+__global__ void k_im_loop_arm(unsigned* ctr, unsigned batches) { *ctr = batches; }
+
+// Last node of every loop iteration: spends one batch of the budget and continues only while budget
+// remains and the sequence has not stopped.  It sets the condition on every iteration, so the loop
+// ends after at most the armed number of batches whatever the state holds.
+__global__ void k_im_loop_cond(cudaGraphConditionalHandle h, unsigned* ctr, const double* state) {
+    const unsigned left = *ctr;
+    const unsigned next = left > 0u ? left - 1u : 0u;
+    *ctr = next;
+    cudaGraphSetConditional(h, (next > 0u && state[IS_STOP] == 0.0) ? 1u : 0u);
+}
+
+// The device-driven form of the batch loop (second-order path): a graph whose WHILE node runs a body
+// of `steps` pseudo-steps followed by k_im_loop_cond, so a whole call runs without the host.
+static cudaError_t build_implicit_loop(ugks_ctx* c, int steps) {
+    cudaError_t e = cudaSuccess;
+    if (!c->iloop_ctr) e = cudaMalloc((void**)&c->iloop_ctr, sizeof(unsigned));
+    cudaGraph_t g = nullptr;
+    if (e == cudaSuccess) e = cudaGraphCreate(&g, 0);
+    if (e != cudaSuccess) return e;
+    cudaGraphConditionalHandle h = 0;
+    e = cudaGraphConditionalHandleCreate(&h, g, 1, cudaGraphCondAssignDefault);
+    cudaGraphNodeParams np = {};
+    np.type = cudaGraphNodeTypeConditional;
+    np.conditional.handle = h;
+    np.conditional.type = cudaGraphCondTypeWhile;
+    np.conditional.size = 1;
+    cudaGraphNode_t node = nullptr;
+    if (e == cudaSuccess) e = cudaGraphAddNode(&node, g, nullptr, 0, &np);
+    long long n = 0;
+    if (e == cudaSuccess) e = cudaStreamBeginCaptureToGraph(c->stream, np.conditional.phGraph_out[0], nullptr, nullptr,
+                                                           0, cudaStreamCaptureModeThreadLocal);
+    if (e == cudaSuccess) {
+        cudaError_t eb = cudaSuccess;
+        for (int s = 0; s < steps && eb == cudaSuccess; ++s)
+            eb = enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork, c->ev_join, &n,
+                                       nullptr, nullptr);
+        if (eb == cudaSuccess) {
+            k_im_loop_cond<<<1, 1, 0, c->stream>>>(h, c->iloop_ctr, c->I.state);
+            eb = cudaGetLastError();
+        }
+        cudaGraph_t body = nullptr;
+        e = cudaStreamEndCapture(c->stream, &body);
+        if (eb != cudaSuccess) e = eb;
+    }
+    if (e == cudaSuccess) e = cudaGraphInstantiate(&c->iloop, g, 0);
+    cudaGraphDestroy(g);
+    if (e == cudaSuccess) c->iloop_launches = n + 1;
+    return e;
+}
+
+// Whether the device-driven loop runs this context's batches: the second-order path only (the S2 step
+// holds a conditional node of its own), built on first use; if that build fails the host pipeline runs
+// the batches instead.
+static bool use_implicit_loop(ugks_ctx* c, int steps) {
+    if (c->Q.high_order || c->iloop_unavailable) return false;
+    if (c->iloop) return true;
+    if (build_implicit_loop(c, steps) == cudaSuccess) return true;
+    cudaGetLastError();
+    c->iloop_unavailable = true;
+    return false;
+}
+
 extern "C" int ugks_implicit_steps(ugks_ctx* c, int max_steps, int* steps_done, int* converged, double* report) {
     if (!c || max_steps < 0) return UGKS_EINVAL;
     if (!c->imem) return UGKS_EUNSUPPORTED;
@@ -705,6 +775,22 @@ extern "C" int ugks_implicit_steps(ugks_ctx* c, int max_steps, int* steps_done, 
             }
             c->launches += n;
             left -= 1;
+        } else if (left >= G && use_implicit_loop(c, G)) {
+            // The device runs the batches: one launch of the WHILE-node graph, bounded by the batch budget
+            // (after a stop, the rest of the stopping batch's kernels return at entry)
+            const unsigned nb = (unsigned)(left / G);
+            unsigned rest = 0;
+            k_im_loop_arm<<<1, 1, 0, c->stream>>>(c->iloop_ctr, nb);
+            UGKS_CK(cudaGetLastError());
+            UGKS_CK(cudaGraphLaunch(c->iloop, c->stream));
+            UGKS_CK(cudaMemcpyAsync(&rest, c->iloop_ctr, sizeof rest, cudaMemcpyDeviceToHost, c->stream));
+            UGKS_CK(cudaMemcpyAsync(st, c->I.state, sizeof st, cudaMemcpyDeviceToHost, c->stream));
+            UGKS_CK(cudaStreamSynchronize(c->stream));
+            const long long ran = (long long)nb - (long long)rest;
+            if (ran < 1 || ran > (long long)nb) return cuda_fail(cudaErrorUnknown);   // the loop body did not run
+            c->launches += 1 + c->iloop_launches * ran;
+            left -= G * (int)ran;
+            continue;
         } else if (left >= G) {
             // Batches of up to 2 graphs, each followed by a copy of the state into a pinned slot.  The
             // next batch is queued before the host waits for the previous batch's copy, so the device
