@@ -130,6 +130,8 @@ int ugks_step_explicit_noalloc(const ugks_params* params, const double* u, const
  * LU-SGS sweep pair with the reference's nslab block-Jacobi seams, src/mod_SteadyImplicit.f90:379-462),
  * RescaleClosedMass and the accepted-state re-evaluation with the five-state gate
  * (src/mod_R5Observe.f90:287-320); stops early when the gate has passed 5 states in a row.
+ * On the second-order path whole batches of 8 steps run on the device under one graph launch (a
+ * conditional WHILE node bounded by max_steps / 8 batches), and the host waits once per call.
  * report[80] (optional) = the last accepted state's sparse_residual.csv row: [0] gate pass,
  * [1] moment, [2] M_W, [3] M_h, [4..11] R1..R8, [12..33] science_1..22, [34..49] flux_1..16,
  * [50..51] reference_h/b, [52] c_minus_1, [53] alpha, [54] macro alpha, [55] dt, [56] streak,
