@@ -68,6 +68,10 @@ C5_STEPS = 2                  # steps timed at the adjoint config's shape (64 ca
 #   post_residual  reads h, b, the x- and y-face fluxes (h, b) and writes stream (h, b)   80 B
 #   post_fluxes    reads h, b and their slopes, writes the face fluxes                   64 B
 #   explicit step  reads h, b, writes h, b                                              32 B
+# accepted pseudo-steps of the delivered ImplicitSteady case to its five-state gate on the B200 (the C
+# oracle stops at the same step; the reference's own run stopped at 1096): the reference arm, which
+# samples pseudo-steps, extrapolates its time to steady with it
+PSEUDO_STEPS_TO_GATE = 1097
 BYTES_PER_UPDATE_PSEUDO_STEP = 240   # compulsory traffic of one implicit pseudo-step per cell*velocity
 # DRAM bytes (read + write) of one ImplicitSteady pseudo-step at 8x64x1024: the sum over its launches in
 # the ncu launch list of 16 pseudo-steps (dram__bytes_read.sum + dram__bytes_write.sum, 289 launches,
@@ -221,6 +225,21 @@ def dist_env():
     return world, rank, local
 
 
+def host_cpu():
+    """The host CPU the baselines ran on: the model name of /proc/cpuinfo (what lscpu prints) and the
+    logical CPUs of the host."""
+    model = "unknown"
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.lower().startswith("model name"):
+                    model = line.split(":", 1)[1].strip()
+                    break
+    except OSError:
+        pass
+    return {"cpu_model": model, "host_cpus": os.cpu_count()}
+
+
 def cpu_baseline(case, velocity, nsteps=30, threads=None):
     """The oracle (single-domain restatement of the reference Fortran) on `nsteps` pseudo-steps."""
     from oracle.oracle import Oracle, set_threads
@@ -234,7 +253,7 @@ def cpu_baseline(case, velocity, nsteps=30, threads=None):
         o.implicit_step()
     el = time.perf_counter() - t0
     units = case.nx * case.ny * len(velocity[0]) * nsteps
-    return {"value": units / el, "unit": UNIT, "cores": nthreads, "kind": "port",
+    return {"value": units / el, "unit": UNIT, "cores": nthreads, "kind": "port", **host_cpu(),
             "seconds_per_pseudo_step": el / nsteps,
             "sample": f"{nsteps} ImplicitSteady pseudo-steps of the 8x64x1024 cold start after 1 warm-up step "
                       f"({el:.2f} s, C oracle -O2, {nthreads} pthread(s) over cells, faces and slabs)"}
@@ -255,7 +274,8 @@ def cpu_sample_high_order(velocity, nsteps=2, threads=None):
         o.implicit_step()
     el = time.perf_counter() - t0
     units = case.nx * case.ny * len(velocity[0]) * nsteps
-    return {"value": units / el, "unit": UNIT, "cores": nthreads, "kind": "port", "seconds_per_pseudo_step": el / nsteps,
+    return {"value": units / el, "unit": UNIT, "cores": nthreads, "kind": "port", **host_cpu(),
+            "seconds_per_pseudo_step": el / nsteps,
             "sample": f"{nsteps} HighOrderImplicit pseudo-steps of the cold start ({el:.2f} s, C oracle -O2, "
                       f"{nthreads} pthread(s)); the reference's published figure is 1.8153 s per pseudo-step on 8 "
                       f"MPI ranks (analysis.json high_implicit: 5445.8 s for 3000)"}
@@ -275,7 +295,8 @@ def cpu_sample_s2cn2(velocity, nsteps=3, threads=None):
         o.s2cn2_step()
     el = time.perf_counter() - t0
     units = case.nx * case.ny * len(velocity[0]) * nsteps
-    return {"value": units / el, "unit": UNIT, "cores": nthreads, "kind": "port", "seconds_per_step": el / nsteps,
+    return {"value": units / el, "unit": UNIT, "cores": nthreads, "kind": "port", **host_cpu(),
+            "seconds_per_step": el / nsteps,
             "sample": f"{nsteps} S2CN2 steps of the cold start ({el:.2f} s, C oracle -O2, {nthreads} pthread(s))"}
 
 
@@ -306,12 +327,88 @@ def run_reference_arm(args):
             "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
             "impl": "reference",
             "config": {"workload": WORKLOAD, "pseudo_steps_per_bench_step": per_step,
-                       "seconds_per_pseudo_step": el / (per_step * args.steps), "parallelism": "host threads"},
-            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port",
+                       "sampled": f"each bench step times {per_step} pseudo-steps of the solve (from the cold "
+                                  f"start, {args.warmup * per_step} warm-up pseudo-steps first), not a solve to the "
+                                  f"gate; the rate is per cell-velocity update, the unit of the GPU arm's value",
+                       "seconds_per_pseudo_step": el / (per_step * args.steps),
+                       "time_to_steady_estimate_s": el / (per_step * args.steps) * PSEUDO_STEPS_TO_GATE,
+                       "parallelism": "host threads"},
+            "cpu_baseline": {"value": v, "unit": UNIT, "cores": nthreads, "kind": "port", **host_cpu(),
                              "sample": f"{per_step} pseudo-steps of the cold start per bench step (the Fortran "
                                        f"reference cannot be built on this image; its C restatement is timed)"},
             "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line), flush=True)
+
+
+def run_long(args):
+    """The configurations at their full stated length, run once (not part of the default bench, whose
+    timed work stays near a minute): the 256-instance batch for its 2000 steps, and the refined
+    HighOrderImplicit variant (16x128 cells, 48x48 velocities) to its 3000 pseudo-step cap.  Prints one
+    JSON line with "mode": "long"."""
+    import torch
+    _, _, local = dist_env()
+    torch.cuda.set_device(local)
+    from ugks2d_high_order_b200.batch import Batch
+    from ugks2d_high_order_b200.case import batched_cases, refined_high_order_case, velocity_table
+    from ugks2d_high_order_b200.solver import Solver
+    out = {"mode": "long"}
+    tables = {n: velocity_table(n) for n in (24, 32, 48)}
+
+    # the refined HighOrderImplicit variant from the cold start to the cap
+    rcase = refined_high_order_case()
+    sr = Solver(rcase, *tables[48], device=local)
+    sr.init_freestream()
+    sr.implicit_init()
+    st = torch.cuda.ExternalStream(sr.stream)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    with torch.cuda.stream(st):
+        e0.record(st)
+        done, conv, rep = sr.step_implicit(HO_MAX_PSEUDO_STEPS)
+        e1.record(st)
+    e1.synchronize()
+    ms = e0.elapsed_time(e1)
+    sr.close()
+    out["refined_high_order_implicit"] = {
+        "pseudo_steps": int(done), "converged": bool(conv), "wall_s": ms * 1e-3,
+        "ms_per_pseudo_step": ms / max(done, 1),
+        "updates_per_s": rcase.nx * rcase.ny * len(tables[48][0]) * done / (ms * 1e-3),
+        "c_minus_1": float(rep[52]), "moment": float(rep[1]), "R1_R8": [float(x) for x in rep[4:12]],
+        "science_1_4": [float(x) for x in rep[12:16]], "Rh_Rb": [float(rep[24]), float(rep[25])],
+        "config": "HighOrderImplicit 16x128 cells, 48x48 velocities (generated half-range table), 8 slabs, "
+                  "CFL 0.1, nCFL 1000, mass rescale on, cold start to the 3000 pseudo-step cap"}
+
+    # the batched distribution for its full 2000 steps
+    cases = batched_cases()
+    bt = Batch([(c, tables[n]) for c, n in cases], device=local, max_streams=32)
+    bt.init_freestream()
+    k_tuned, _ = bt.tune(steps=2)
+    bt.init_freestream()
+    bs = torch.cuda.ExternalStream(bt.stream)
+    b0, b1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    nsteps = 2000
+    with torch.cuda.stream(bs):
+        b0.record(bs)
+        bdone, bst = bt.run(nsteps)
+        b1.record(bs)
+    b1.synchronize()
+    bms = b0.elapsed_time(b1)
+    reps = np.stack([bt.report(i) for i in range(len(cases))])
+    kn = np.array([c.mu_ref * np.sqrt(np.pi) for c, _ in cases])
+    cv = sum(c.nx * c.ny * n * n for c, n in cases)
+    out["batched_full"] = {
+        "instances": len(cases), "steps": nsteps, "streams": int(k_tuned),
+        "all_accepted": bool((bdone == nsteps).all() and not bst.any()),
+        "steps_done_min": int(bdone.min()), "wall_s": bms * 1e-3, "updates_per_s": cv * nsteps / (bms * 1e-3),
+        "final_drift_max": float(reps[:, 9].max()), "final_drift_median": float(np.median(reps[:, 9])),
+        "final_cnres_max": float(reps[:, 1].max()), "final_mmerr_max": float(reps[:, 2].max()),
+        "min_h_min": float(reps[:, 5].min()), "min_b_min": float(reps[:, 7].min()),
+        "kn_range": [float(kn.min()), float(kn.max())],
+        "config": "256 S2CN2 instances, seed PCG64(20261203), Kn log-uniform [0.01, 1], wall Mach [0.5, 3], "
+                  "Tw ratio [0.8, 1.2], 8x{32,64,128} cells, {24,32,48}^2 velocities, CFL 0.1, cold start, "
+                  "2000 steps; drift is each instance's conservation drift against its wall ledger at the last "
+                  "step (every step is gated at 2e-12)"}
+    bt.close()
+    print(json.dumps(out), flush=True)
 
 
 def main():
@@ -324,7 +421,12 @@ def main():
     ap.add_argument("--sampler", default="nvml", choices=["nvml", "smi", "none"],
                     help="clock sampler during the timed region")
     ap.add_argument("--sampler-period", type=float, default=0.5, help="seconds between clock samples")
+    ap.add_argument("--long", action="store_true",
+                    help="run the batched and refined configurations once at their full length instead")
     args = ap.parse_args()
+    if args.long:
+        run_long(args)
+        return
     if args.impl == "reference":
         run_reference_arm(args)
         return

@@ -76,6 +76,13 @@ int ugks_ctx_destroy(ugks_ctx* ctx);
 /* Copy state host <-> device (the only PCIe crossings). */
 int ugks_upload_state(ugks_ctx* ctx, const double* h, const double* b, const double* W);
 int ugks_download_state(ugks_ctx* ctx, double* h, double* b, double* W);
+/* The same with h and b in the reference's own backing stores, halo included: cell_h_store(Nvel,
+ * 1-LAP:nx+LAP, 1-LAP:ny+LAP) and cell_b_store (src/mod_InitializeFlow.f90:109-110), that is host arrays
+ * [ny + 2 lap][nx + 2 lap][nvel] with the interior at (lap, lap); W as above (ctr%conVars packed).  Only
+ * the interior is read or written, so the Fortran driver passes its stores as they are (lap = LAP = 2,
+ * src/mod_Globaldata.f90:95) and keeps filling its halo itself. */
+int ugks_upload_state_halo(ugks_ctx* ctx, const double* h, const double* b, const double* W, int lap);
+int ugks_download_state_halo(ugks_ctx* ctx, double* h, double* b, double* W, int lap);
 
 /* InitFlow_Freestream + cold-start EnforceAcceptedMomentCompatibility
  * (src/mod_InitializeFlow.f90:826-856; src/mod_SteadyImplicit.f90:28-42). */
@@ -84,16 +91,40 @@ int ugks_init_freestream(ugks_ctx* ctx, double rho, double U, double V, double t
 /* TimeStep (src/mod_Solve.f90:373-421): computes dt_global on the device; *dt_out optional. */
 int ugks_timestep(ugks_ctx* ctx, double* dt_out);
 
-/* Interpolation() + Evolution() (src/mod_Interpolation.f90:26, src/mod_Evolution.f90:35-177):
- * Van-Leer slopes fused into the UGKS face fluxes (interior faces and W2B moving walls). */
+/* Interpolation() + Evolution() (src/mod_Interpolation.f90:26, src/mod_Evolution.f90:35-41), which
+ * dispatches on the method as the reference does: Explicit / ImplicitSteady run EvolutionNative, the
+ * Van-Leer slopes fused into the UGKS face fluxes (interior faces and W2B moving walls); S2CN2 and
+ * HighOrderImplicit run S2NativeEvolution (src/mod_S2NativeAdapter.f90:469-490), as ugks_evolution_s2
+ * with the reference's target rule: HighOrderImplicit rebuilds the volume targets every time, S2CN2
+ * keeps those of the accepted state (UGKS_EINVAL before ugks_s2cn2_init or ugks_init_freestream). */
 int ugks_evolution(ugks_ctx* ctx);
 
+/* S2NativeEvolution (src/mod_S2NativeAdapter.f90:469-599 -> CartesianEvolution
+ * src/mod_S2CartesianMPI.f90:182-234 -> compute_flux src/mod_S2D1.f90:632-959) on an S2CN2 or
+ * HighOrderImplicit context: the WENO-AO face and wall fluxes of the current state into the face arrays
+ * (ugks_copy_array "fxh", "fyw", ...) and the wall aerodynamics.  rebuild_targets nonzero rebuilds the
+ * volume targets of the current W first (build_targets, src/mod_S2D1.f90:1246-1300; always on
+ * HighOrderImplicit, whose targets the reference invalidates at every evaluation, :479); zero keeps the
+ * S2CN2 targets of the accepted state.  On S2CN2 this starts a per-operator step: ugks_timestep,
+ * ugks_evolution (or this), ugks_compute_residual, ugks_apply_explicit_update advance the state exactly
+ * as one step of ugks_s2cn2_steps.  UGKS_EUNSUPPORTED on a second-order context. */
+int ugks_evolution_s2(ugks_ctx* ctx, int rebuild_targets);
+
 /* ComputeResidual() (src/mod_Residual.f90:17-132) with the unified streaming-moment projection;
- * with_collision also forms the physical equilibrium/collision used by the implicit paths. */
+ * with_collision also forms the physical equilibrium/collision used by the implicit paths.
+ * S2CN2 (after the evolution of the step): the residual, the stream state, the S2 physical collision
+ * and its moment gate (S2NativePhysicalCollision, src/mod_S2NativeAdapter.f90:735-759) and the
+ * Crank-Nicolson right-hand side of advance_step (src/mod_S2D1.f90:1376-1390); UGKS_EINVAL out of that
+ * order.  HighOrderImplicit: UGKS_EUNSUPPORTED, its residual runs inside ugks_implicit_steps. */
 int ugks_compute_residual(ugks_ctx* ctx, int with_collision);
 
 /* ApplyExplicitUpdate() (src/mod_TimeIntegrator.f90:16-134): macro update, CN Shakhov
- * collision with variable tau, residual norms; res_out[4] optional = the reference `res`. */
+ * collision with variable tau, residual norms; res_out[4] optional = the reference `res`.
+ * S2CN2 (after ugks_compute_residual): S2NativeApplyUpdate (src/mod_S2NativeAdapter.f90:867-940), the
+ * targets of the stream state, the CN collision, the cnres / mmerr / conservation gates and the
+ * acceptance; a rejected step keeps the accepted state and returns UGKS_ENUMERIC (reference code 203);
+ * res_out is not written (ugks_s2cn2_report gives the step's report).  HighOrderImplicit:
+ * UGKS_EUNSUPPORTED (ugks_implicit_steps). */
 int ugks_apply_explicit_update(ugks_ctx* ctx, double* res_out);
 
 /* nsteps full Explicit steps (TimeStep, Interpolation, Evolution, ComputeResidual,
@@ -110,11 +141,14 @@ int ugks_step_explicit(ugks_ctx* ctx, int nsteps, double* dt_out, double* res_ou
  * (a cudaStream_t; NULL = legacy default stream); dt_out / res_out are optional host outputs as in
  * ugks_step_explicit.  Working arrays live in one fixed 36 MiB __device__ array inside the library:
  * a call whose working set (about 8*nx*ny*nvel + 2*nx*nvel + 22*nx*ny doubles; 33.8 MB for
- * 8x64 cells x 32x32 velocities) does not fit returns UGKS_EINVAL before any GPU work.  Every
- * GPU that loads the library keeps that array until the process exits.  The first call on a
- * device looks up the array's device address with that device current, so make it before any
- * stream capture.  All calls share the array: calls that overlap on the GPU race and must be
- * serialised by the caller. */
+ * 8x64 cells x 32x32 velocities) does not fit returns UGKS_EINVAL before any GPU work.  The array is
+ * loaded on a device, and its 36 MiB taken there, at the first call on that device (CUDA loads modules
+ * lazily), so callers that size their own device pool or run under a memory cap make one call per
+ * device before they do; the array then stays until the process exits.  Each call synchronises
+ * `stream` twice (it reads the velocity table's extent, which sets dt, and then the status), so it
+ * cannot be captured in a CUDA graph.  All calls on one device share the array: calls that overlap on
+ * that GPU (other streams, other host threads) race and must be serialised by the caller; host threads
+ * driving different devices share nothing. */
 int ugks_step_explicit_noalloc(const ugks_params* params, const double* u, const double* v, const double* w,
                                double* h, double* b, double* W, int nsteps, void* stream, double* dt_out,
                                double* res_out);
@@ -172,6 +206,9 @@ int ugks_s2cn2_steps(ugks_ctx* ctx, int nsteps, int* steps_done, double* report)
  * the conservation drift of step `step` (1-based) of the next ugks_s2cn2_steps call is forced above
  * the gate, so that step is rejected.  One-shot; 0 clears it.  Host-side, numerical only. */
 int ugks_s2cn2_test_reject(ugks_ctx* ctx, int step);
+/* report[24] of the last S2CN2 step (layout of ugks_s2cn2_steps), whether it ran through
+ * ugks_s2cn2_steps or the per-operator calls. */
+int ugks_s2cn2_report(ugks_ctx* ctx, double* report);
 
 /* Batched S2CN2: many independent Couette instances of uneven grid and velocity-set sizes advanced
  * together (BASELINE's batched form; no counterpart routine in the reference, whose runs are one case

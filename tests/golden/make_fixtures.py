@@ -2,7 +2,7 @@
 
 Run once in a container that has the reference checkout (the GPU host does not):
 
-    python tests/golden/make_fixtures.py /root/reference
+    python tests/golden/make_fixtures.py <the reference checkout>
 
 Outputs (all small, committed):
   velocity_half32_scale2.npy  - the 1024-row (u, v, w) table of cases/*/velocity_half32_scale2.dat,

@@ -50,11 +50,15 @@ def test_noalloc_matches_context_path_two_calls_in_a_row(velocity):
         hc, bc, Wc = s.download()
         dt_n = np.zeros(1)
         res_n = np.zeros(4)
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info(dev)[0]
         rc = L.ugks_step_explicit_noalloc(ctypes.byref(s._params), vp(u), vp(v), vp(w), vp(h), vp(b), vp(W),
                                           nsteps, ctypes.c_void_p(stream), dt_n.ctypes.data_as(dp),
                                           res_n.ctypes.data_as(dp))
         assert rc == capi.UGKS_OK, f"call {call}: {L.ugks_error_string(rc).decode()}"
         torch.cuda.synchronize()
+        if call > 0:   # the first call may load the library's scratch array; later calls take nothing
+            assert torch.cuda.mem_get_info(dev)[0] == free_before, "a repeated call changed the free device memory"
         assert relmax(h.cpu().numpy(), hc) <= TOL, call
         assert relmax(b.cpu().numpy(), bc) <= TOL, call
         assert relmax(W.cpu().numpy(), Wc) <= TOL, call

@@ -32,6 +32,7 @@ EXPORTS = [
     "ugks_s2cn2_test_reject", "ugks_batch_create", "ugks_batch_destroy", "ugks_batch_init_freestream",
     "ugks_batch_run", "ugks_batch_tune", "ugks_batch_set_streams", "ugks_batch_upload", "ugks_batch_download",
     "ugks_batch_report", "ugks_batch_wall_aero", "ugks_batch_launch_count", "ugks_batch_stream",
+    "ugks_evolution_s2", "ugks_upload_state_halo", "ugks_download_state_halo", "ugks_s2cn2_report",
 ]
 REPORT_LEN = 80
 CN_REPORT_LEN = 24
@@ -87,6 +88,10 @@ def load(path=LIB_PATH):
     L.ugks_init_freestream.argtypes = [vp] + [ctypes.c_double] * 4
     L.ugks_timestep.argtypes = [vp, dp]
     L.ugks_evolution.argtypes = [vp]
+    L.ugks_evolution_s2.argtypes = [vp, ctypes.c_int]
+    L.ugks_upload_state_halo.argtypes = [vp, dp, dp, dp, ctypes.c_int]
+    L.ugks_download_state_halo.argtypes = [vp, dp, dp, dp, ctypes.c_int]
+    L.ugks_s2cn2_report.argtypes = [vp, dp]
     L.ugks_compute_residual.argtypes = [vp, ctypes.c_int]
     L.ugks_apply_explicit_update.argtypes = [vp, dp]
     L.ugks_step_explicit.argtypes = [vp, ctypes.c_int, dp, dp]

@@ -157,18 +157,9 @@ extern "C" int ugks_batch_create(int n, const ugks_instance_desc* desc, int devi
         const ugks_params* p = &desc[i].params;
         Inst& I = b->inst[i];
         LoParams& P = I.P;
-        P.nx = p->nx; P.ny = p->ny; P.nvel = p->nvel; P.ck = p->ck; P.dx = p->dx; P.dy = p->dy;
-        P.area = std::fabs((-p->dx) * (-p->dy) - (p->dx) * (-p->dy)) * 0.5;
-        int e2 = 0;
-        const double m2 = std::frexp(P.area, &e2);
-        P.inv_area = (m2 == 0.5 && std::isfinite(P.area)) ? std::ldexp(1.0, 1 - e2) : 0.0;
-        P.gm1 = (double)(p->ck + 4) / (double)(p->ck + 2) - 1.0;
-        P.pr = p->pr; P.omega = p->omega; P.mu_ref = p->mu_ref; P.cfl = p->cfl;
-        P.umax = -INFINITY; P.vmax = -INFINITY;
-        for (int k = 0; k < p->nvel; ++k) { P.umax = std::fmax(P.umax, desc[i].u[k]); P.vmax = std::fmax(P.vmax, desc[i].v[k]); }
-        for (int s = 0; s < 2; ++s) { P.wall_ux[s] = p->wall_ux[s]; P.wall_lam[s] = 1.0 / p->wall_tnative[s]; }
-        P.fixed_dt = p->fixed_dt;
-        P.inv_dx = 1.0 / p->dx; P.inv_dy = 1.0 / p->dy;
+        double umax = -INFINITY, vmax = -INFINITY;
+        for (int k = 0; k < p->nvel; ++k) { umax = std::fmax(umax, desc[i].u[k]); vmax = std::fmax(vmax, desc[i].v[k]); }
+        P = make_lo_params(*p, umax, vmax);
         const int nx = p->nx, ny = p->ny, nv = p->nvel;
         const size_t nc = (size_t)nx * ny, S = nc * nv;
         I.S = S;

@@ -83,6 +83,7 @@ struct ugks_ctx {
     LoBuffers Bs[2] = {};          // state sets 0 and 1 with the halt flag
     bool cn_ready = false;         // ledger and targets of the current state are in place
     int cn_reject_at = 0;          // step of the next sequence forced to fail its conservation gate
+    int cn_stage = 0;              // per-operator S2CN2 step: 1 after the evolution, 2 after the residual
     cudaGraphExec_t cgraph = nullptr;
 };
 
@@ -151,23 +152,9 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
     c->prm = *p;
     c->device = device;
     const int nx = p->nx, ny = p->ny, nv = p->nvel, nc = nx * ny;
-    LoParams& P = c->P;
-    P.nx = nx; P.ny = ny; P.nvel = nv; P.ck = p->ck;
-    P.dx = p->dx; P.dy = p->dy;
-    P.area = std::fabs((-p->dx) * (-p->dy) - (p->dx) * (-p->dy)) * 0.5;
-    {
-        int e2 = 0;
-        const double m2 = std::frexp(P.area, &e2);
-        P.inv_area = (m2 == 0.5 && std::isfinite(P.area)) ? std::ldexp(1.0, 1 - e2) : 0.0;
-    }
-    P.gm1 = (double)(p->ck + 4) / (double)(p->ck + 2) - 1.0;
-    P.pr = p->pr; P.omega = p->omega; P.mu_ref = p->mu_ref; P.cfl = p->cfl;
-    P.umax = -INFINITY; P.vmax = -INFINITY;
-    for (int k = 0; k < nv; ++k) { P.umax = std::fmax(P.umax, u[k]); P.vmax = std::fmax(P.vmax, v[k]); }
-    for (int s = 0; s < 2; ++s) { P.wall_ux[s] = p->wall_ux[s]; P.wall_lam[s] = 1.0 / p->wall_tnative[s]; }
-    P.fixed_dt = p->fixed_dt;
-    P.inv_dx = 1.0 / p->dx;
-    P.inv_dy = 1.0 / p->dy;
+    double umax = -INFINITY, vmax = -INFINITY;
+    for (int k = 0; k < nv; ++k) { umax = std::fmax(umax, u[k]); vmax = std::fmax(vmax, v[k]); }
+    c->P = make_lo_params(*p, umax, vmax);
 
     // buffer plan (doubles)
     const size_t S = (size_t)nc * nv, SY = (size_t)(ny + 1) * nx * nv;
@@ -350,6 +337,7 @@ extern "C" int ugks_upload_state(ugks_ctx* c, const double* h, const double* b, 
     UGKS_CK(cudaMemcpyAsync(c->B.W, W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyHostToDevice,
                             c->stream));
     c->cn_ready = false;   // an S2CN2 context needs ugks_s2cn2_init for the new state
+    c->cn_stage = 0;
     int r = kernel_timestep(c);
     if (r) return r;
     return collect_status(c);
@@ -361,6 +349,43 @@ extern "C" int ugks_download_state(ugks_ctx* c, double* h, double* b, double* W)
     const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
     if (h) UGKS_CK(cudaMemcpyAsync(h, c->B.h, S * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
     if (b) UGKS_CK(cudaMemcpyAsync(b, c->B.b, S * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (W)
+        UGKS_CK(cudaMemcpyAsync(W, c->B.W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                                c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    return UGKS_OK;
+}
+
+// h, b with the reference's LAP halo: host arrays [ny + 2 lap][nx + 2 lap][nvel], interior at (lap, lap).
+// One strided copy per array; the halo of the host arrays is neither read nor written.
+static cudaError_t copy_halo(double* dst, const double* src, const ugks_ctx* c, int lap, cudaMemcpyKind kind) {
+    const size_t nv = (size_t)c->P.nvel, nx = (size_t)c->P.nx, ny = (size_t)c->P.ny;
+    const size_t row = nx * nv * sizeof(double), hpitch = (nx + 2 * (size_t)lap) * nv * sizeof(double);
+    const size_t hoff = ((size_t)lap * (nx + 2 * (size_t)lap) + (size_t)lap) * nv;
+    if (kind == cudaMemcpyHostToDevice) return cudaMemcpy2DAsync(dst, row, src + hoff, hpitch, row, ny, kind, c->stream);
+    return cudaMemcpy2DAsync(dst + hoff, hpitch, src, row, row, ny, kind, c->stream);
+}
+
+extern "C" int ugks_upload_state_halo(ugks_ctx* c, const double* h, const double* b, const double* W, int lap) {
+    if (!c || !h || !b || !W || lap < 0) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    if (int r = invalidate_eval(c)) return r;
+    UGKS_CK(copy_halo(c->B.h, h, c, lap, cudaMemcpyHostToDevice));
+    UGKS_CK(copy_halo(c->B.b, b, c, lap, cudaMemcpyHostToDevice));
+    UGKS_CK(cudaMemcpyAsync(c->B.W, W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyHostToDevice,
+                            c->stream));
+    c->cn_ready = false;
+    c->cn_stage = 0;
+    int r = kernel_timestep(c);
+    if (r) return r;
+    return collect_status(c);
+}
+
+extern "C" int ugks_download_state_halo(ugks_ctx* c, double* h, double* b, double* W, int lap) {
+    if (!c || lap < 0) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    if (h) UGKS_CK(copy_halo(h, c->B.h, c, lap, cudaMemcpyDeviceToHost));
+    if (b) UGKS_CK(copy_halo(b, c->B.b, c, lap, cudaMemcpyDeviceToHost));
     if (W)
         UGKS_CK(cudaMemcpyAsync(W, c->B.W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyDeviceToHost,
                                 c->stream));
@@ -399,10 +424,42 @@ extern "C" int ugks_timestep(ugks_ctx* c, double* dt_out) {
     return collect_status(c);
 }
 
+// The S2 evolution of the current state (S2NativeEvolution, mod_S2NativeAdapter.f90:469-490): the
+// high-order faces, walls and their macro fluxes, with the volume targets rebuilt (HighOrderImplicit
+// always, S2CN2 when asked) or kept (S2CN2: the accepted state's targets from the last step or from
+// ugks_s2cn2_init).  An S2CN2 evaluation starts a per-operator step: the halt flag, the accepted count
+// and the rejection hook are armed as ugks_s2cn2_steps arms them for a sequence of one step.
+static int s2_evolution(ugks_ctx* c, bool rebuild_targets) {
+    if (c->cmem) {
+        if (!c->cn_ready && !rebuild_targets) return UGKS_EINVAL;   // no targets: ugks_s2cn2_init first
+        int r = collect_status(c);
+        if (r) return r;
+        UGKS_CK(cudaMemsetAsync(c->cflags, 0, 3 * sizeof(unsigned), c->stream));
+        const double inject = (double)c->cn_reject_at;
+        UGKS_CK(cudaMemcpyAsync(c->C.ledger + 8, &inject, sizeof inject, cudaMemcpyHostToDevice, c->stream));
+        c->cn_reject_at = 0;
+        const int which = rebuild_targets ? 1 : 2;
+        UGKS_CK(s2_enqueue(which, c->P, c->Bs[0], c->T[0], c->stream, c->stream2, c->ev_fork, c->ev_join));
+        c->launches += s2_enqueue_kernels(which);
+        r = collect_status(c);
+        c->cn_ready = c->cn_ready || (rebuild_targets && r == UGKS_OK);
+        c->cn_stage = r == UGKS_OK ? 1 : 0;
+        return r;
+    }
+    UGKS_CK(s2_enqueue(1, c->P, c->B, c->I.s2, c->stream, c->stream2, c->ev_fork, c->ev_join));
+    c->launches += s2_enqueue_kernels(1);
+    return collect_status(c);
+}
+
+static bool is_s2(const ugks_ctx* c) {
+    return c->prm.method == UGKS_METHOD_S2CN2 || c->prm.method == UGKS_METHOD_HIGH_ORDER_IMPLICIT;
+}
+
 extern "C" int ugks_evolution(ugks_ctx* c) {
     if (!c) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
     if (int r = invalidate_eval(c)) return r;
+    if (is_s2(c)) return s2_evolution(c, c->prm.method == UGKS_METHOD_HIGH_ORDER_IMPLICIT);
     UGKS_CK(launch_lo_slopes(c->P, c->B, c->stream));
     UGKS_CK(launch_lo_faces(c->P, c->B, c->stream));
     UGKS_CK(launch_lo_walls(c->P, c->B, c->stream));
@@ -410,44 +467,73 @@ extern "C" int ugks_evolution(ugks_ctx* c) {
     return collect_status(c);
 }
 
-extern "C" int ugks_compute_residual(ugks_ctx* c, int with_collision) {
+extern "C" int ugks_evolution_s2(ugks_ctx* c, int rebuild_targets) {
     if (!c) return UGKS_EINVAL;
+    if (!is_s2(c)) return UGKS_EUNSUPPORTED;
     UGKS_CK(cudaSetDevice(c->device));
     if (int r = invalidate_eval(c)) return r;
+    return s2_evolution(c, rebuild_targets != 0 || c->prm.method == UGKS_METHOD_HIGH_ORDER_IMPLICIT);
+}
+
+extern "C" int ugks_compute_residual(ugks_ctx* c, int with_collision) {
+    if (!c) return UGKS_EINVAL;
+    if (c->prm.method == UGKS_METHOD_HIGH_ORDER_IMPLICIT) return UGKS_EUNSUPPORTED;
+    UGKS_CK(cudaSetDevice(c->device));
+    if (int r = invalidate_eval(c)) return r;
+    if (c->cmem) {   // S2CN2: residual, stream state, S2 physical collision gate, CN right-hand side
+        if (c->cn_stage != 1) return UGKS_EINVAL;
+        UGKS_CK(enqueue_cn_stream(c->P, c->Bs[0], c->T[0], c->C, c->stream));
+        c->launches += 1;
+        const int r = collect_status(c);
+        c->cn_stage = r == UGKS_OK ? 2 : 0;
+        return r;
+    }
     UGKS_CK(launch_lo_cells(c->P, c->B, 1, with_collision != 0, c->stream));
     c->launches += 1;
     return collect_status(c);
 }
 
-// residual vector of ApplyExplicitUpdate (mod_TimeIntegrator.f90:108-127) from the reduced sums
-static void finish_res(const ugks_ctx* c, const double* dg, double* res) {
-    const double SMV = 1.1754943508222875e-38;
-    const double ncell = (double)(c->P.nx * c->P.ny);
-    double sumRes[4], sumAvg[4];
-    for (int m = 0; m < 4; ++m) { sumRes[m] = dg[m]; sumAvg[m] = dg[4 + m]; }
-    const double areaSq = dg[8];
-    const double ords = std::fmax(std::fmax(sumAvg[0], sumAvg[3]), SMV);
-    for (int m = 0; m < 4; ++m) {
-        const double rel = std::sqrt(ncell * sumRes[m]) / (sumAvg[m] + SMV);
-        const double ab = std::sqrt(sumRes[m] / std::fmax(areaSq, SMV));
-        const bool near0 = sumAvg[m] <= std::sqrt(2.220446049250313e-16) * std::fmax(ords, 2.2250738585072014e-308);
-        res[m] = near0 ? ab : rel;
+// S2NativeApplyUpdate (mod_S2NativeAdapter.f90:867-940) of a per-operator S2CN2 step: the targets of
+// the stream state and the CN collision into state set 1, the gates and the acceptance; an accepted
+// state (and its targets) is brought back to set 0.
+static int s2cn2_apply(ugks_ctx* c) {
+    if (c->cn_stage != 2) return UGKS_EINVAL;
+    c->cn_stage = 0;
+    UGKS_CK(enqueue_cn_apply(c->P, c->Bs[0], c->Bs[1], c->T[1], c->C, c->stream));
+    c->launches += 1 + s2_enqueue_kernels(3);
+    unsigned acc = 0;
+    UGKS_CK(cudaMemcpyAsync(&acc, c->C.accepted, sizeof acc, cudaMemcpyDeviceToHost, c->stream));
+    const int r = collect_status(c);
+    if (acc == 1u) {
+        const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
+        UGKS_CK(cudaMemcpyAsync(c->Bs[0].h, c->Bs[1].h, S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        UGKS_CK(cudaMemcpyAsync(c->Bs[0].b, c->Bs[1].b, S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        UGKS_CK(cudaMemcpyAsync(c->Bs[0].W, c->Bs[1].W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double),
+                                cudaMemcpyDeviceToDevice, c->stream));
+        double* src[6] = {c->T[1].mh, c->T[1].mb, c->T[1].kxh, c->T[1].kxb, c->T[1].kyh, c->T[1].kyb};
+        double* dst[6] = {c->T[0].mh, c->T[0].mb, c->T[0].kxh, c->T[0].kxb, c->T[0].kyh, c->T[0].kyb};
+        for (int t = 0; t < 6; ++t)
+            UGKS_CK(cudaMemcpyAsync(dst[t], src[t], S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+        UGKS_CK(cudaStreamSynchronize(c->stream));
     }
+    return r;
 }
 
 static int read_step_outputs(ugks_ctx* c, double* dt_out, double* res_out) {
     double dg[kNDiag];
     if (res_out) UGKS_CK(cudaMemcpyAsync(dg, c->B.diag, sizeof dg, cudaMemcpyDeviceToHost, c->stream));
     int r = collect_status(c);
-    if (res_out) finish_res(c, dg, res_out);
+    if (res_out) finish_explicit_res(c->P.nx, c->P.ny, dg, res_out);
     (void)dt_out;
     return r;
 }
 
 extern "C" int ugks_apply_explicit_update(ugks_ctx* c, double* res_out) {
     if (!c) return UGKS_EINVAL;
+    if (c->prm.method == UGKS_METHOD_HIGH_ORDER_IMPLICIT) return UGKS_EUNSUPPORTED;
     UGKS_CK(cudaSetDevice(c->device));
     if (int r = invalidate_eval(c)) return r;
+    if (c->cmem) return s2cn2_apply(c);
     UGKS_CK(launch_lo_cells(c->P, c->B, 2, false, c->stream));
     c->launches += 1;
     return read_step_outputs(c, nullptr, res_out);
@@ -688,13 +774,16 @@ static int build_implicit_graph(ugks_ctx* c, int steps) {
 __global__ void k_im_loop_arm(unsigned* ctr, unsigned batches) { *ctr = batches; }
 
 // Last node of every loop iteration: spends one batch of the budget and continues only while budget
-// remains and the sequence has not stopped.  It sets the condition on every iteration, so the loop
-// ends after at most the armed number of batches whatever the state holds.
-__global__ void k_im_loop_cond(cudaGraphConditionalHandle h, unsigned* ctr, const double* state) {
+// remains, the sequence has not stopped and no kernel has raised a status bit (a failed gate of the
+// evaluation kernels raises one without stopping the sequence; the call returns that failure, so
+// nothing after the failing batch runs).  It sets the condition on every iteration, so the loop ends
+// after at most the armed number of batches whatever the state holds.
+__global__ void k_im_loop_cond(cudaGraphConditionalHandle h, unsigned* ctr, const double* state,
+                               const unsigned* status) {
     const unsigned left = *ctr;
     const unsigned next = left > 0u ? left - 1u : 0u;
     *ctr = next;
-    cudaGraphSetConditional(h, (next > 0u && state[IS_STOP] == 0.0) ? 1u : 0u);
+    cudaGraphSetConditional(h, (next > 0u && state[IS_STOP] == 0.0 && *status == 0u) ? 1u : 0u);
 }
 
 // The device-driven form of the batch loop (second-order path): a graph whose WHILE node runs a body
@@ -723,7 +812,7 @@ static cudaError_t build_implicit_loop(ugks_ctx* c, int steps) {
             eb = enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork, c->ev_join, &n,
                                        nullptr, nullptr);
         if (eb == cudaSuccess) {
-            k_im_loop_cond<<<1, 1, 0, c->stream>>>(h, c->iloop_ctr, c->I.state);
+            k_im_loop_cond<<<1, 1, 0, c->stream>>>(h, c->iloop_ctr, c->I.state, c->B.status);
             eb = cudaGetLastError();
         }
         cudaGraph_t body = nullptr;
@@ -865,6 +954,7 @@ extern "C" int ugks_s2cn2_init(ugks_ctx* c) {
     UGKS_CK(enqueue_s2cn2_prepare(c->P, c->Bs[0], c->T[0], c->C, c->stream, &c->launches));
     const int r = collect_status(c);
     c->cn_ready = r == UGKS_OK;
+    c->cn_stage = 0;
     return r;
 }
 
@@ -872,6 +962,15 @@ extern "C" int ugks_s2cn2_test_reject(ugks_ctx* c, int step) {
     if (!c || step < 0) return UGKS_EINVAL;
     if (!c->cmem) return UGKS_EUNSUPPORTED;
     c->cn_reject_at = step;
+    return UGKS_OK;
+}
+
+extern "C" int ugks_s2cn2_report(ugks_ctx* c, double* report) {
+    if (!c || !report) return UGKS_EINVAL;
+    if (!c->cmem) return UGKS_EUNSUPPORTED;
+    UGKS_CK(cudaSetDevice(c->device));
+    UGKS_CK(cudaMemcpyAsync(report, c->C.report, kCnReport * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
     return UGKS_OK;
 }
 
@@ -902,6 +1001,7 @@ extern "C" int ugks_s2cn2_steps(ugks_ctx* c, int nsteps, int* steps_done, double
     if (!c->cn_ready) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
     if (steps_done) *steps_done = 0;
+    c->cn_stage = 0;
     // a new sequence: clear the halt flag and the accepted count, and any stale status
     int r = collect_status(c);
     if (r) return r;

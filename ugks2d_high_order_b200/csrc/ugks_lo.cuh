@@ -1,6 +1,9 @@
 // ugks_lo.cuh -- device-side state of one Couette domain and the second-order (Van-Leer UGKS)
 // kernels' parameter blocks.
 #pragma once
+#include <cmath>
+
+#include "../../include/ugks_b200.h"
 #include "ugks_device.cuh"
 
 namespace ugks {
@@ -89,6 +92,43 @@ __device__ __forceinline__ Slot slot(int r, int nv) {
     s.ok = s.k < nv;
     s.kk = s.ok ? s.k : nv - 1;
     return s;
+}
+
+// The kernels' parameter block of a domain described by the C ABI's ugks_params, with U_MAX / V_MAX
+// of its velocity table (InitVelocityFromStructuredFile, mod_InitializeFlow.f90:508).  Host only;
+// shared by the context path and the allocation-free entry point so that both derive the same block.
+inline LoParams make_lo_params(const ugks_params& p, double umax, double vmax) {
+    LoParams P{};
+    P.nx = p.nx; P.ny = p.ny; P.nvel = p.nvel; P.ck = p.ck;
+    P.dx = p.dx; P.dy = p.dy;
+    P.area = std::fabs((-p.dx) * (-p.dy) - (p.dx) * (-p.dy)) * 0.5;
+    {
+        int e2 = 0;
+        const double m2 = std::frexp(P.area, &e2);
+        P.inv_area = (m2 == 0.5 && std::isfinite(P.area)) ? std::ldexp(1.0, 1 - e2) : 0.0;
+    }
+    P.gm1 = (double)(p.ck + 4) / (double)(p.ck + 2) - 1.0;
+    P.pr = p.pr; P.omega = p.omega; P.mu_ref = p.mu_ref; P.cfl = p.cfl;
+    P.umax = umax; P.vmax = vmax;
+    for (int s = 0; s < 2; ++s) { P.wall_ux[s] = p.wall_ux[s]; P.wall_lam[s] = 1.0 / p.wall_tnative[s]; }
+    P.fixed_dt = p.fixed_dt;
+    P.inv_dx = 1.0 / p.dx;
+    P.inv_dy = 1.0 / p.dy;
+    return P;
+}
+
+// The residual vector `res` of ApplyExplicitUpdate (mod_TimeIntegrator.f90:108-127) from the cell-reduced
+// sums dg[kNDiag] (sum of squared rates [0..3], of |W| [4..7], of area^2 [8]).  Host only.
+inline void finish_explicit_res(int nx, int ny, const double* dg, double* res) {
+    const double SMV = 1.1754943508222875e-38;
+    const double ncell = (double)nx * (double)ny;
+    const double ords = std::fmax(std::fmax(dg[4], dg[7]), SMV);
+    for (int m = 0; m < 4; ++m) {
+        const double rel = std::sqrt(ncell * dg[m]) / (dg[4 + m] + SMV);
+        const double ab = std::sqrt(dg[m] / std::fmax(dg[8], SMV));
+        const bool near0 = dg[4 + m] <= std::sqrt(2.220446049250313e-16) * std::fmax(ords, 2.2250738585072014e-308);
+        res[m] = near0 ? ab : rel;
+    }
 }
 
 // Per-cell TimeStep (mod_Solve.f90:386-405): dt_local = CFL*area/(dy*max(U_MAX,|U|+c)+dx*max(V_MAX,|V|+c))

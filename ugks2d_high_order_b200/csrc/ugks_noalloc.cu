@@ -11,16 +11,24 @@
 // Limits and behaviour (also stated in include/ugks_b200.h):
 //   * The scratch array is kNoAllocBytes = 36 MiB.  A call whose working set does not fit is
 //     rejected with UGKS_EINVAL before any GPU work; the reference's delivered case (8x64 cells,
-//     32x32 velocities) needs 33.8 MB.  The array is part of the library's device image, so every
-//     GPU on which it is loaded keeps those 36 MiB until the process exits.
+//     32x32 velocities) needs 33.8 MB.  The array belongs to this file's device module.  Under
+//     CUDA's lazy module loading (the default) that module, and with it the 36 MiB, is loaded on a
+//     device at the first call there, so a caller that sizes its own device pool or runs under a
+//     memory cap makes one call on each device before it does so.  The array then stays until the
+//     process exits.
 //   * The first call on a device looks the array's device address up (cudaGetSymbolAddress) with
-//     that device current; make that first call before any stream capture begins.
+//     that device current.
+//   * Every call synchronises its stream twice: once after copying the velocity table to the host
+//     (U_MAX / V_MAX set the time step) and once after reading the status and the outputs.  The
+//     call therefore cannot be captured in a CUDA graph.
 //   * Every call uses the same array and it keeps the previous call's contents; this call clears
 //     what must start at zero (the last-CTA counter and the status word).  Calls that overlap on
-//     the GPU (other streams, other host threads) race on the array and must be serialised by the
-//     caller.
+//     the GPU (other streams, other host threads driving the same device) race on the array and
+//     must be serialised by the caller.  Host threads that drive different devices use different
+//     arrays and share no host state.
 #include <cuda_runtime.h>
 
+#include <atomic>
 #include <cmath>
 #include <cstdio>
 
@@ -47,8 +55,10 @@ constexpr int kMaxDevices = 64;
 // host-side shadow, so only the address returned by cudaGetSymbolAddress is passed to kernels.
 static __device__ __align__(256) double g_noalloc_scratch[kNoAllocDoubles];
 
-double* g_scratch_addr[kMaxDevices] = {nullptr};
-double g_host_u[kMaxVel], g_host_v[kMaxVel];   // velocity-table staging for U_MAX / V_MAX
+// Device address of the scratch per device, filled on the first call on that device.  Every lookup of
+// one device yields the same address, so two host threads filling one entry at once store the same
+// value; the entries are atomic so that such a store is well defined.
+std::atomic<double*> g_scratch_addr[kMaxDevices];
 
 struct Plan {
     size_t flags, sxh, syh, sxb, syb, fxh, fxb, fxw, fyh, fyb, fyw, dtl, dt, cd, dg, wa, total;
@@ -96,37 +106,27 @@ extern "C" int ugks_step_explicit_noalloc(const ugks_params* prm, const double* 
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return fail(e);
     if (dev < 0 || dev >= kMaxDevices) return UGKS_EINVAL;
-    if (!g_scratch_addr[dev]) {   // once per device, with that device current
+    double* base = g_scratch_addr[dev].load(std::memory_order_acquire);
+    if (!base) {   // once per device, with that device current
         void* ptr = nullptr;
         e = cudaGetSymbolAddress(&ptr, g_noalloc_scratch);
         if (e != cudaSuccess) return fail(e);
-        g_scratch_addr[dev] = static_cast<double*>(ptr);
+        base = static_cast<double*>(ptr);
+        g_scratch_addr[dev].store(base, std::memory_order_release);
     }
-    double* base = g_scratch_addr[dev];
     cudaStream_t s = static_cast<cudaStream_t>(stream);
 
-    // U_MAX, V_MAX of the table (InitVelocityFromStructuredFile, mod_InitializeFlow.f90:508)
-    e = cudaMemcpyAsync(g_host_u, u, nv * sizeof(double), cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(g_host_v, v, nv * sizeof(double), cudaMemcpyDeviceToHost, s);
+    // U_MAX, V_MAX of the table (InitVelocityFromStructuredFile, mod_InitializeFlow.f90:508), staged in
+    // this call's own stack buffers (40 KB at the largest table), so concurrent calls from other host
+    // threads share no host memory
+    double hu[kMaxVel], hv[kMaxVel];
+    e = cudaMemcpyAsync(hu, u, nv * sizeof(double), cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(hv, v, nv * sizeof(double), cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(e);
-    LoParams P{};
-    P.nx = nx; P.ny = ny; P.nvel = nv; P.ck = prm->ck;
-    P.dx = prm->dx; P.dy = prm->dy;
-    P.area = std::fabs((-prm->dx) * (-prm->dy) - (prm->dx) * (-prm->dy)) * 0.5;
-    {
-        int e2 = 0;
-        const double m2 = std::frexp(P.area, &e2);
-        P.inv_area = (m2 == 0.5 && std::isfinite(P.area)) ? std::ldexp(1.0, 1 - e2) : 0.0;
-    }
-    P.gm1 = (double)(prm->ck + 4) / (double)(prm->ck + 2) - 1.0;
-    P.pr = prm->pr; P.omega = prm->omega; P.mu_ref = prm->mu_ref; P.cfl = prm->cfl;
-    P.umax = -INFINITY; P.vmax = -INFINITY;
-    for (int k = 0; k < nv; ++k) { P.umax = std::fmax(P.umax, g_host_u[k]); P.vmax = std::fmax(P.vmax, g_host_v[k]); }
-    for (int i = 0; i < 2; ++i) { P.wall_ux[i] = prm->wall_ux[i]; P.wall_lam[i] = 1.0 / prm->wall_tnative[i]; }
-    P.fixed_dt = prm->fixed_dt;
-    P.inv_dx = 1.0 / prm->dx;
-    P.inv_dy = 1.0 / prm->dy;
+    double umax = -INFINITY, vmax = -INFINITY;
+    for (int k = 0; k < nv; ++k) { umax = std::fmax(umax, hu[k]); vmax = std::fmax(vmax, hv[k]); }
+    const LoParams P = make_lo_params(*prm, umax, vmax);
 
     LoBuffers B{};
     B.u = u; B.v = v; B.w = w; B.h = h; B.b = b; B.W = W;
@@ -159,16 +159,6 @@ extern "C" int ugks_step_explicit_noalloc(const ugks_params* prm, const double* 
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) return fail(e);
     if (dt_out) *dt_out = nsteps > 0 ? dt2[1] : dt2[0];
-    if (res_out && nsteps > 0) {
-        // residual vector of ApplyExplicitUpdate (mod_TimeIntegrator.f90:108-127)
-        const double SMV = 1.1754943508222875e-38, ncell = (double)nx * ny;
-        const double ords = std::fmax(std::fmax(dg[4], dg[7]), SMV);
-        for (int m = 0; m < 4; ++m) {
-            const double rel = std::sqrt(ncell * dg[m]) / (dg[4 + m] + SMV);
-            const double ab = std::sqrt(dg[m] / std::fmax(dg[8], SMV));
-            const bool near0 = dg[4 + m] <= std::sqrt(2.220446049250313e-16) * std::fmax(ords, 2.2250738585072014e-308);
-            res_out[m] = near0 ? ab : rel;
-        }
-    }
+    if (res_out && nsteps > 0) finish_explicit_res(nx, ny, dg, res_out);
     return status ? UGKS_ENUMERIC : UGKS_OK;
 }

@@ -317,18 +317,31 @@ __global__ void __launch_bounds__(256) k_cn_ledger(LoParams P, LoBuffers B, CnBu
 }
 
 template <int VPT, int NT>
-static cudaError_t cn_launch(const LoParams& P, const LoBuffers& B, const S2Buffers& T, const LoBuffers& Bo,
-                             const S2Buffers& To, const CnBuffers& C, cudaStream_t s) {
-    const int nc = P.nx * P.ny;
-    k_cn_stream<VPT, NT><<<nc, NT, 0, s>>>(P, B, T, C);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
+static cudaError_t cn_stream_launch(const LoParams& P, const LoBuffers& B, const S2Buffers& T, const CnBuffers& C,
+                                    cudaStream_t s) {
+    k_cn_stream<VPT, NT><<<P.nx * P.ny, NT, 0, s>>>(P, B, T, C);
+    return cudaGetLastError();
+}
+
+template <int VPT, int NT>
+static cudaError_t cn_apply_launch(const LoParams& P, const LoBuffers& B, const LoBuffers& Bo, const S2Buffers& To,
+                                   const CnBuffers& C, cudaStream_t s) {
     LoBuffers Bw = B;   // the targets of the stream state
     Bw.W = C.ws;
-    e = s2_enqueue(3, P, Bw, To, s, s, nullptr, nullptr);
+    cudaError_t e = s2_enqueue(3, P, Bw, To, s, s, nullptr, nullptr);
     if (e != cudaSuccess) return e;
-    k_cn_collide<VPT, NT><<<nc, NT, 0, s>>>(P, B, To, C, Bo);
+    k_cn_collide<VPT, NT><<<P.nx * P.ny, NT, 0, s>>>(P, B, To, C, Bo);
     return cudaGetLastError();
+}
+
+cudaError_t enqueue_cn_stream(const LoParams& P, const LoBuffers& B, const S2Buffers& T, const CnBuffers& C,
+                              cudaStream_t s) {
+    return P.nvel <= 1024 ? cn_stream_launch<4, 256>(P, B, T, C, s) : cn_stream_launch<10, 256>(P, B, T, C, s);
+}
+
+cudaError_t enqueue_cn_apply(const LoParams& P, const LoBuffers& B, const LoBuffers& Bo, const S2Buffers& To,
+                             const CnBuffers& C, cudaStream_t s) {
+    return P.nvel <= 1024 ? cn_apply_launch<4, 256>(P, B, Bo, To, C, s) : cn_apply_launch<10, 256>(P, B, Bo, To, C, s);
 }
 
 // Report (C.report) of the step: [0] dt, [1] cnres, [2] mmerr, [3] max 2 beta, [4] transport CFL,
@@ -339,10 +352,8 @@ cudaError_t enqueue_s2cn2_step(const LoParams& P, const LoBuffers& B, const S2Bu
                                cudaEvent_t fork, cudaEvent_t join, long long* launches) {
     cudaError_t e = launch_lo_timestep(P, B, s);
     if (e == cudaSuccess) e = s2_enqueue(2, P, B, T, s, s2, fork, join);
-    if (e == cudaSuccess) {
-        if (P.nvel <= 1024) e = cn_launch<4, 256>(P, B, T, Bo, To, C, s);
-        else e = cn_launch<10, 256>(P, B, T, Bo, To, C, s);
-    }
+    if (e == cudaSuccess) e = enqueue_cn_stream(P, B, T, C, s);
+    if (e == cudaSuccess) e = enqueue_cn_apply(P, B, Bo, To, C, s);
     if (launches) *launches += kCnStepKernels;
     return e;
 }

@@ -29,6 +29,13 @@ struct CnBuffers {
 cudaError_t enqueue_s2cn2_step(const LoParams& P, const LoBuffers& B, const S2Buffers& T, const LoBuffers& Bo,
                                const S2Buffers& To, const CnBuffers& C, cudaStream_t s, cudaStream_t s2,
                                cudaEvent_t fork, cudaEvent_t join, long long* launches);
+// The two halves of the step after the evolution, for the per-operator C ABI (ComputeResidual, then
+// S2NativeApplyUpdate): k_cn_stream of set (B, T); then the targets of the stream state into To and
+// k_cn_collide into Bo with the acceptance.  enqueue_s2cn2_step launches exactly these.
+cudaError_t enqueue_cn_stream(const LoParams& P, const LoBuffers& B, const S2Buffers& T, const CnBuffers& C,
+                              cudaStream_t s);
+cudaError_t enqueue_cn_apply(const LoParams& P, const LoBuffers& B, const LoBuffers& Bo, const S2Buffers& To,
+                             const CnBuffers& C, cudaStream_t s);
 // S2NativeInitializeState's ledger of the state in B (total0 = sum of W, empty wall balance) and the
 // volume targets of that state into T.
 cudaError_t enqueue_s2cn2_prepare(const LoParams& P, const LoBuffers& B, const S2Buffers& T, const CnBuffers& C,

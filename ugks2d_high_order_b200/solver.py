@@ -92,6 +92,25 @@ class Solver:
         self._check(self.L.ugks_download_state(self.ctx, _p(h), _p(b), _p(W)), "ugks_download_state")
         return h, b, W
 
+    def upload_halo(self, h, b, W, lap=2):
+        """Upload from the reference's backing stores with their LAP halo: h, b of shape
+        [ny + 2 lap][nx + 2 lap][nvel] (cell_h_store(Nvel, 1-LAP:nx+LAP, 1-LAP:ny+LAP)); the halo is not read."""
+        h = np.ascontiguousarray(h, dtype=np.float64)
+        b = np.ascontiguousarray(b, dtype=np.float64)
+        W = np.ascontiguousarray(W, dtype=np.float64)
+        assert h.shape == (self.ny + 2 * lap, self.nx + 2 * lap, self.nvel) and h.shape == b.shape
+        assert W.size == self.ncell * 4
+        self._check(self.L.ugks_upload_state_halo(self.ctx, _p(h), _p(b), _p(W), int(lap)), "ugks_upload_state_halo")
+
+    def download_halo(self, h, b, W=None, lap=2):
+        """Download into backing stores with a LAP halo (the arrays' halo is left as it is)."""
+        assert h.flags.c_contiguous and b.flags.c_contiguous and h.dtype == np.float64 and b.dtype == np.float64
+        assert h.shape == (self.ny + 2 * lap, self.nx + 2 * lap, self.nvel) and h.shape == b.shape
+        if W is not None:
+            assert W.flags.c_contiguous and W.dtype == np.float64 and W.size == self.ncell * 4
+        self._check(self.L.ugks_download_state_halo(self.ctx, _p(h), _p(b), _p(W) if W is not None else None, int(lap)),
+                    "ugks_download_state_halo")
+
     # ---- reference operators
     def time_step(self):
         """TimeStep (mod_Solve.f90:373-421): global CFL dt, computed on the device."""
@@ -100,8 +119,13 @@ class Solver:
         return float(dt[0])
 
     def evolution(self):
-        """Interpolation + Evolution (mod_Interpolation.f90:26-90, mod_Evolution.f90:35-177)."""
+        """Interpolation + Evolution (mod_Interpolation.f90:26-90, mod_Evolution.f90:35-41): the
+        second-order evolution, or S2NativeEvolution on the S2 methods as the reference dispatches."""
         self._check(self.L.ugks_evolution(self.ctx), "Evolution")
+
+    def evolution_s2(self, rebuild_targets=False):
+        """S2NativeEvolution (mod_S2NativeAdapter.f90:469-599) with the volume targets rebuilt or kept."""
+        self._check(self.L.ugks_evolution_s2(self.ctx, int(rebuild_targets)), "S2NativeEvolution")
 
     def compute_residual(self, with_collision=False):
         """ComputeResidual (mod_Residual.f90:17-132)."""
@@ -165,6 +189,12 @@ class Solver:
         self.last_steps_done = done.value
         self._check(code, "S2NativeApplyUpdate")
         return done.value, rep
+
+    def s2cn2_report(self):
+        """The last S2CN2 step's report (layout in include/ugks_b200.h)."""
+        rep = np.zeros(capi.CN_REPORT_LEN)
+        self._check(self.L.ugks_s2cn2_report(self.ctx, _p(rep)), "S2CN2 report")
+        return rep
 
     def s2cn2_test_reject(self, step):
         """Force step `step` (1-based) of the next step_s2cn2 call to fail its conservation gate
