@@ -30,7 +30,8 @@ class UOParams(ctypes.Structure):
 
 
 def build():
-    subprocess.run(["make", "-s", "-C", HERE], check=True)
+    """The oracle and its tangent build (oracle/tangent.py)."""
+    subprocess.run(["make", "-s", "-C", HERE, "all", "tangent"], check=True)
 
 
 _lib = None
