@@ -210,6 +210,32 @@ int ugks_s2cn2_test_reject(ugks_ctx* ctx, int step);
  * ugks_s2cn2_steps or the per-operator calls. */
 int ugks_s2cn2_report(ugks_ctx* ctx, double* report);
 
+/* Gradients of the S2CN2 wall outputs by the discrete adjoint of the step (no counterpart routine in the
+ * reference, which has no derivatives; the gradient of its S2CN2 trajectory, mod_S2D1.f90:1302-1435 with
+ * compute_flux :632-959 and the walls of mod_S2MultiscaleWall.f90:45-184).  The outputs are the wall
+ * aerodynamics of the last step's evaluation averaged over each wall (PublishWallDiagnostics,
+ * src/mod_S2NativeAdapter.f90:1075-1097): out[4] = bottom shear (pnt), bottom heat flux (qn), top shear,
+ * top heat flux.  The parameters are grad[5] = d/d(mu_ref, wall_ux[0], wall_ux[1], wall_tnative[0],
+ * wall_tnative[1]) of the seeded output combination sum_i seed[i] out[i].
+ * ugks_s2cn2_forward_checkpointed: nsteps accepted S2CN2 steps from the current state (as
+ *   ugks_s2cn2_steps), storing the state and the conservation ledger every `every` steps (device memory
+ *   for the checkpoints and one segment of `every` states with their targets is reserved on first use);
+ *   out[4] optional.  A rejected step returns UGKS_ENUMERIC (reference code 203) and leaves no trajectory.
+ * ugks_s2cn2_backward: the reverse sweep over that trajectory: each segment's states are recomputed from
+ *   its checkpoint, then every step is re-run for its evaluation scratch and transposed.  grad[5]
+ *   optional; gh0, gb0 [ny][nx][nvel] and gW0 [ny][nx][4] (optional) receive the cotangent of the initial
+ *   state (its targets' dependence on W included).  The adjoint holds the time step fixed: it returns
+ *   UGKS_ENUMERIC with ugks_last_status bit 0x400 if a state's dt is set by |U| + c instead of the
+ *   velocity table's extent.  The context's state (the last forward state) is not changed.
+ * ugks_s2cn2_step_vjp: the vector-Jacobian product of one step at the current state (not advanced): the
+ *   cotangents gh, gb [ny][nx][nvel], gW [ny][nx][4] of the step's outputs (NULL = zero) and seed[4] of
+ *   the step's wall outputs (NULL = zero) give the input cotangents gh_in, gb_in, gW_in (optional) and
+ *   grad[5] (optional). */
+int ugks_s2cn2_forward_checkpointed(ugks_ctx* ctx, int nsteps, int every, double* out);
+int ugks_s2cn2_backward(ugks_ctx* ctx, const double* seed, double* grad, double* gh0, double* gb0, double* gW0);
+int ugks_s2cn2_step_vjp(ugks_ctx* ctx, const double* gh, const double* gb, const double* gW, const double* seed,
+                        double* gh_in, double* gb_in, double* gW_in, double* grad);
+
 /* Batched S2CN2: many independent Couette instances of uneven grid and velocity-set sizes advanced
  * together (BASELINE's batched form; no counterpart routine in the reference, whose runs are one case
  * per job).  Each instance is described by ugks_params (method UGKS_METHOD_S2CN2) and its velocity

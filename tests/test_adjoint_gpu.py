@@ -1,0 +1,191 @@
+"""The discrete adjoint of the S2CN2 step on the GPU, through the C ABI.
+
+The adjoint is the transpose of the step's Jacobian.  It is checked three ways:
+  * the dot-product identity <J v, u> = <v, J^T u> at one step, with J v from the oracle's tangent build
+    (the oracle itself run with (value, derivative) numbers, oracle/tangent.py) and J^T u from the
+    device's vector-Jacobian product, for directions in h, b, W and in each parameter;
+  * gradients through several steps (checkpoint-and-recompute) against central differences of the GPU
+    forward and against the tangent oracle's exact forward-mode derivatives;
+  * the checkpoint interval does not change the gradient.
+The GPU and the oracle evaluate the same step with differently ordered moment sums, so their Jacobians
+agree to the tolerance of the high-order parity tests, not bit for bit.
+"""
+import numpy as np
+import pytest
+
+from ugks2d_high_order_b200.case import reference_case, velocity_table
+
+pytestmark = pytest.mark.gpu
+
+PARAMS = ("mu_ref", "wall_ux0", "wall_ux1", "wall_tnative0", "wall_tnative1")
+DOT_TOL = 1e-8      # <J v, u> vs <v, J^T u>, GPU adjoint against the oracle's tangent, relative
+FD_TOL = 1e-6       # gradient vs central differences (h = 1e-6 relative), relative to the gradient's norm
+
+
+def _case():
+    return reference_case("S2CN2").with_(ny=16, dy=1.0 / 16.0)
+
+
+def _perturbed(case, p, d):
+    if p == "mu_ref":
+        return case.with_(mu_ref=case.mu_ref + d)
+    if p.startswith("wall_ux"):
+        w = int(p[-1])
+        ux = list(case.wall_ux)
+        ux[w] += d
+        return case.with_(wall_ux=tuple(ux))
+    w = int(p[-1])
+    tw = list(case.wall_tnative)
+    tw[w] += d
+    return case.with_(wall_tnative=tuple(tw))
+
+
+def _param_value(case, p):
+    return {"mu_ref": case.mu_ref, "wall_ux0": case.wall_ux[0], "wall_ux1": case.wall_ux[1],
+            "wall_tnative0": case.wall_tnative[0], "wall_tnative1": case.wall_tnative[1]}[p]
+
+
+def _dparams(p):
+    if p == "mu_ref":
+        return {"mu_ref": 1.0}
+    w = int(p[-1])
+    d = [0.0, 0.0]
+    d[w] = 1.0
+    return {"wall_ux": tuple(d)} if p.startswith("wall_ux") else {"wall_tnative": tuple(d)}
+
+
+@pytest.fixture(scope="module")
+def developed_state():
+    """A state with developed wall layers: 3 S2CN2 steps of the cold start."""
+    from ugks2d_high_order_b200.solver import Solver
+    vel = velocity_table(24)
+    s = Solver(_case(), *vel)
+    try:
+        s.init_freestream()
+        s.step_s2cn2(3)
+        return vel, s.download()
+    finally:
+        s.close()
+
+
+def _tangent_step(case, vel, state, dstate=(None, None, None), dparams=None):
+    """J v of one step by the tangent oracle: (dh', db', dW', d wall outputs[4])."""
+    from oracle.tangent import TangentOracle
+    t = TangentOracle(case, *vel, dparams=dparams)
+    h, b, W = state
+    t.set_state(h, b, W, *dstate)
+    out = t.s2cn2_step()
+    _, dh, _, db, _, dW = t.get_state()
+    _, dwall = t.wall_outputs(out[0])
+    return dh, db, dW, dwall.reshape(4)
+
+
+def test_step_vjp_dot_product_with_the_tangent_oracle(developed_state):
+    from ugks2d_high_order_b200.solver import Solver
+    vel, state = developed_state
+    case = _case()
+    rng = np.random.default_rng(20261204)
+    h, b, W = state
+    u = [rng.standard_normal(h.shape), rng.standard_normal(b.shape), rng.standard_normal(W.shape)]
+    seed = rng.standard_normal(4)
+    s = Solver(case, *vel)
+    try:
+        s.upload(h, b, W)
+        s.s2cn2_init()
+        lh, lb, lW, grad = s.s2cn2_step_vjp(u[0], u[1], u[2], seed)
+    finally:
+        s.close()
+    lam = (lh, lb, lW)
+
+    def lhs(jv):
+        return sum(float(np.sum(a * c)) for a, c in zip(u, jv[:3])) + float(np.dot(seed, jv[3]))
+
+    # state directions, one field at a time (h, b, W)
+    for which in range(3):
+        v = [None, None, None]
+        v[which] = rng.standard_normal(state[which].shape) * np.abs(state[which]).max()
+        jv = _tangent_step(case, vel, state, tuple(v))
+        a, c = lhs(jv), float(np.sum(v[which] * lam[which]))
+        assert abs(a - c) <= DOT_TOL * max(abs(a), abs(c)), (which, a, c)
+    # parameter directions: d(<u, x'> + seed . out) / dp = grad[p]
+    for q, p in enumerate(PARAMS):
+        jv = _tangent_step(case, vel, state, dparams=_dparams(p))
+        a = lhs(jv)
+        assert abs(a - grad[q]) <= DOT_TOL * max(abs(a), 1e-12), (p, a, grad[q])
+
+
+def _gpu_outputs(case, vel, nsteps):
+    from ugks2d_high_order_b200.sensitivity import wall_outputs
+    from ugks2d_high_order_b200.solver import Solver
+    s = Solver(case, *vel)
+    try:
+        s.init_freestream()
+        done, _ = s.step_s2cn2(nsteps)
+        assert done == nsteps
+        return wall_outputs(s.wall_aero()).reshape(4)
+    finally:
+        s.close()
+
+
+def test_gradient_through_steps_matches_central_differences_and_the_tangent_oracle():
+    from oracle.tangent import TangentOracle
+    from ugks2d_high_order_b200.solver import Solver
+    case, vel, nsteps = _case(), velocity_table(24), 6
+    seed = np.array([0.7, -1.3, 0.4, 0.9])
+    s = Solver(case, *vel)
+    try:
+        s.init_freestream()
+        out = s.s2cn2_forward_checkpointed(nsteps, every=4)
+        grad = s.s2cn2_backward(seed)
+    finally:
+        s.close()
+    assert np.array_equal(out, _gpu_outputs(case, vel, nsteps))   # the checkpointed run is the plain run
+    fd, exact = np.zeros(5), np.zeros(5)
+    for q, p in enumerate(PARAMS):
+        d = 1e-6 * abs(_param_value(case, p))
+        fd[q] = float(np.dot(seed, _gpu_outputs(_perturbed(case, p, d), vel, nsteps) -
+                             _gpu_outputs(_perturbed(case, p, -d), vel, nsteps))) / (2.0 * d)
+        t = TangentOracle(case, *vel, dparams=_dparams(p))
+        t.init_freestream()
+        for _ in range(nsteps):
+            o = t.s2cn2_step()
+        exact[q] = float(np.dot(seed, t.wall_outputs(o[0])[1].reshape(4)))
+    scale = np.abs(grad).max()
+    assert np.abs(grad - fd).max() <= FD_TOL * scale, (grad, fd)
+    assert np.abs(grad - exact).max() <= FD_TOL * scale, (grad, exact)
+
+
+def test_checkpoint_interval_does_not_change_the_gradient():
+    from ugks2d_high_order_b200.solver import Solver
+    case, vel, nsteps = _case(), velocity_table(24), 7
+    seed = np.array([1.0, 0.5, -0.25, 2.0])
+    grads = []
+    for every in (7, 3, 1):
+        s = Solver(case, *vel)
+        try:
+            s.init_freestream()
+            s.s2cn2_forward_checkpointed(nsteps, every=every)
+            grads.append(s.s2cn2_backward(seed))
+        finally:
+            s.close()
+    for g in grads[1:]:
+        assert np.abs(g - grads[0]).max() <= 1e-12 * np.abs(grads[0]).max(), (g, grads[0])
+
+
+def test_one_step_backward_equals_the_step_vjp():
+    from ugks2d_high_order_b200.solver import Solver
+    case, vel = _case(), velocity_table(24)
+    seed = np.array([0.3, 1.1, -0.8, 0.6])
+    s = Solver(case, *vel)
+    try:
+        s.init_freestream()
+        h0, b0, W0 = s.download()
+        s.s2cn2_forward_checkpointed(1, every=1)
+        grad, (gh, gb, gW) = s.s2cn2_backward(seed, initial_state=True)
+        s.upload(h0, b0, W0)
+        s.s2cn2_init()
+        vh, vb, vW, vgrad = s.s2cn2_step_vjp(seed=seed)
+    finally:
+        s.close()
+    for a, c in ((grad, vgrad), (gh, vh), (gb, vb), (gW, vW)):
+        assert np.abs(a - c).max() <= 1e-12 * max(np.abs(c).max(), 1e-300)

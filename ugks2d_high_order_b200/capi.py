@@ -33,6 +33,7 @@ EXPORTS = [
     "ugks_batch_run", "ugks_batch_tune", "ugks_batch_set_streams", "ugks_batch_upload", "ugks_batch_download",
     "ugks_batch_report", "ugks_batch_wall_aero", "ugks_batch_launch_count", "ugks_batch_stream",
     "ugks_evolution_s2", "ugks_upload_state_halo", "ugks_download_state_halo", "ugks_s2cn2_report",
+    "ugks_s2cn2_forward_checkpointed", "ugks_s2cn2_backward", "ugks_s2cn2_step_vjp",
 ]
 REPORT_LEN = 80
 CN_REPORT_LEN = 24
@@ -92,6 +93,9 @@ def load(path=LIB_PATH):
     L.ugks_upload_state_halo.argtypes = [vp, dp, dp, dp, ctypes.c_int]
     L.ugks_download_state_halo.argtypes = [vp, dp, dp, dp, ctypes.c_int]
     L.ugks_s2cn2_report.argtypes = [vp, dp]
+    L.ugks_s2cn2_forward_checkpointed.argtypes = [vp, ctypes.c_int, ctypes.c_int, dp]
+    L.ugks_s2cn2_backward.argtypes = [vp, dp, dp, dp, dp, dp]
+    L.ugks_s2cn2_step_vjp.argtypes = [vp, dp, dp, dp, dp, dp, dp, dp, dp]
     L.ugks_compute_residual.argtypes = [vp, ctypes.c_int]
     L.ugks_apply_explicit_update.argtypes = [vp, dp]
     L.ugks_step_explicit.argtypes = [vp, ctypes.c_int, dp, dp]

@@ -10,6 +10,7 @@
 
 #include "../../include/ugks_b200.h"
 #include "ugks_implicit.cuh"
+#include "ugks_s2_adjoint.cuh"
 #include "ugks_s2cn2.cuh"
 
 namespace ugks {
@@ -85,6 +86,19 @@ struct ugks_ctx {
     int cn_reject_at = 0;          // step of the next sequence forced to fail its conservation gate
     int cn_stage = 0;              // per-operator S2CN2 step: 1 after the evolution, 2 after the residual
     cudaGraphExec_t cgraph = nullptr;
+    // S2CN2 adjoint (ugks_s2cn2_forward_checkpointed / ugks_s2cn2_backward / ugks_s2cn2_step_vjp)
+    double* amem = nullptr;        // checkpoints, segment slots, cotangent sets, adjoint work
+    unsigned* aflags = nullptr;    // [0..2] halt, counter, accepted of the re-runs, [3] adjoint status
+    size_t amem_doubles = 0;
+    int adj_capacity_ckpt = 0, adj_capacity_seg = 0;
+    double* ckpt = nullptr;        // [ckpt][h | b | W | ledger]
+    double* seg = nullptr;         // [slot][h | b | W | 6 targets | ledger]
+    double* cot[2] = {nullptr, nullptr};   // [h | b | W | 6 targets] cotangent sets
+    double* adj_seed = nullptr;    // [4]
+    double* adj_ledger = nullptr;  // [16] the re-runs' ledger
+    double* adj_report = nullptr;  // [kCnReport]
+    AdjBuffers A{};
+    int adj_nsteps = 0, adj_every = 0;   // the trajectory the checkpoints hold (0: none)
 };
 
 static int cuda_fail(cudaError_t e) {
@@ -292,6 +306,8 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->iloop) cudaGraphExecDestroy(c->iloop);
     if (c->iloop_ctr) cudaFree(c->iloop_ctr);
     if (c->cgraph) cudaGraphExecDestroy(c->cgraph);
+    if (c->amem) cudaFree(c->amem);
+    if (c->aflags) cudaFree(c->aflags);
     if (c->cmem) cudaFree(c->cmem);
     if (c->cflags) cudaFree(c->cflags);
     if (c->imem) cudaFree(c->imem);
@@ -1035,4 +1051,291 @@ extern "C" int ugks_s2cn2_steps(ugks_ctx* c, int nsteps, int* steps_done, double
     }
     if (steps_done) *steps_done = (int)acc;
     return r;
+}
+
+// ---------------------------------------------------------------------------------------------
+// S2CN2 adjoint: checkpointed forward, reverse sweep with recompute, one-step VJP
+
+namespace {
+
+size_t rnd32(size_t n) { return (n + 31) / 32 * 32; }
+
+struct SlotView {
+    double *h, *b, *W, *T[6], *ledger;
+};
+
+size_t state_doubles(const ugks_ctx* c) {
+    const size_t nc = (size_t)c->P.nx * c->P.ny, S = nc * c->P.nvel;
+    return 2 * rnd32(S) + rnd32(nc * 4);
+}
+size_t ckpt_doubles(const ugks_ctx* c) { return state_doubles(c) + 32; }
+size_t seg_doubles(const ugks_ctx* c) {
+    const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
+    return state_doubles(c) + 6 * rnd32(S) + 32;
+}
+size_t cot_doubles(const ugks_ctx* c) {
+    const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
+    return state_doubles(c) + 6 * rnd32(S);
+}
+
+// h, b, W (and, with targets, the six targets) of a block laid out as state_doubles + 6 targets
+SlotView view_of(const ugks_ctx* c, double* base, bool targets, bool ledger) {
+    const size_t nc = (size_t)c->P.nx * c->P.ny, S = nc * c->P.nvel;
+    SlotView v{};
+    v.h = base; base += rnd32(S);
+    v.b = base; base += rnd32(S);
+    v.W = base; base += rnd32(nc * 4);
+    for (int t = 0; t < 6; ++t) {
+        v.T[t] = targets ? base : nullptr;
+        if (targets) base += rnd32(S);
+    }
+    v.ledger = ledger ? base : nullptr;
+    return v;
+}
+SlotView ckpt_view(const ugks_ctx* c, int q) { return view_of(c, c->ckpt + (size_t)q * ckpt_doubles(c), false, true); }
+SlotView seg_view(const ugks_ctx* c, int m) { return view_of(c, c->seg + (size_t)m * seg_doubles(c), true, true); }
+SlotView cot_view(const ugks_ctx* c, int i) { return view_of(c, c->cot[i], true, false); }
+
+// the state set of a slot: the context's set 0 with the slot's arrays and the re-runs' halt flag
+LoBuffers slot_lo(const ugks_ctx* c, const SlotView& v) {
+    LoBuffers B = c->Bs[0];
+    B.h = v.h; B.b = v.b; B.W = v.W;
+    B.halt = c->aflags;
+    return B;
+}
+S2Buffers slot_targets(const ugks_ctx* c, const SlotView& v) {
+    S2Buffers T = c->T[0];
+    T.mh = v.T[0]; T.mb = v.T[1]; T.kxh = v.T[2]; T.kxb = v.T[3]; T.kyh = v.T[4]; T.kyb = v.T[5];
+    return T;
+}
+// the re-runs' step buffers: the shared stream state and right-hand side, a ledger, report and flags of
+// their own, so that a re-run never touches the accepted sequence's ledger
+CnBuffers rerun_cn(const ugks_ctx* c) {
+    CnBuffers C = c->C;
+    C.ledger = c->adj_ledger;
+    C.report = c->adj_report;
+    C.halt = c->aflags;
+    C.counter = c->aflags + 1;
+    C.accepted = c->aflags + 2;
+    return C;
+}
+AdjBuffers adj_bind(const ugks_ctx* c, int out, const double* seed) {
+    AdjBuffers A = c->A;
+    const SlotView o = cot_view(c, out), in = cot_view(c, 1 - out);
+    A.gho = o.h; A.gbo = o.b; A.gWo = o.W;
+    A.ghi = in.h; A.gbi = in.b; A.gWi = in.W;
+    for (int t = 0; t < 6; ++t) { A.gTo[t] = o.T[t]; A.gTi[t] = in.T[t]; }
+    A.seed = seed;
+    return A;
+}
+
+cudaError_t copy_state(const ugks_ctx* c, const SlotView& dst, const double* h, const double* b, const double* W) {
+    const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
+    cudaError_t e = cudaMemcpyAsync(dst.h, h, S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(dst.b, b, S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(dst.W, W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    return e;
+}
+// a ledger copy without the test-rejection hook (slot 8)
+cudaError_t copy_ledger(const ugks_ctx* c, double* dst, const double* src) {
+    cudaError_t e = cudaMemcpyAsync(dst, src, 8 * sizeof(double), cudaMemcpyDeviceToDevice, c->stream);
+    if (e == cudaSuccess) e = cudaMemsetAsync(dst + 8, 0, sizeof(double), c->stream);
+    return e;
+}
+
+// one step of the S2CN2 sequence from (Bin, Tin) into (Bout, Tout) with the ledger `ledger`, as
+// enqueue_s2cn2_step, on the re-runs' buffers
+cudaError_t rerun_step(ugks_ctx* c, const LoBuffers& Bin, const S2Buffers& Tin, const LoBuffers& Bout,
+                       const S2Buffers& Tout, const double* ledger) {
+    cudaError_t e = cudaMemsetAsync(c->aflags, 0, 3 * sizeof(unsigned), c->stream);
+    if (e == cudaSuccess) e = copy_ledger(c, c->adj_ledger, ledger);
+    if (e == cudaSuccess)
+        e = enqueue_s2cn2_step(c->P, Bin, Tin, Bout, Tout, rerun_cn(c), c->stream, c->stream2, c->ev_fork, c->ev_join,
+                               &c->launches);
+    return e;
+}
+
+int adj_reserve(ugks_ctx* c, int nckpt, int nseg) {
+    if (c->amem && c->adj_capacity_ckpt >= nckpt && c->adj_capacity_seg >= nseg) return UGKS_OK;
+    if (c->amem) { cudaFree(c->amem); c->amem = nullptr; }
+    const size_t nx = c->P.nx, ny = c->P.ny, nv = c->P.nvel;
+    const size_t tot = (size_t)nckpt * ckpt_doubles(c) + (size_t)nseg * seg_doubles(c) + 2 * cot_doubles(c) +
+                       rnd32(adj_work_doubles((int)nx, (int)ny, (int)nv)) + 3 * 32;
+    UGKS_CK(prepare_s2_adjoint());
+    UGKS_CK(cudaMalloc(&c->amem, tot * sizeof(double)));
+    if (!c->aflags) UGKS_CK(cudaMalloc(&c->aflags, 4 * sizeof(unsigned)));
+    UGKS_CK(cudaMemsetAsync(c->amem, 0, tot * sizeof(double), c->stream));
+    UGKS_CK(cudaMemsetAsync(c->aflags, 0, 4 * sizeof(unsigned), c->stream));
+    double* m = c->amem;
+    c->ckpt = m; m += (size_t)nckpt * ckpt_doubles(c);
+    c->seg = m; m += (size_t)nseg * seg_doubles(c);
+    c->cot[0] = m; m += cot_doubles(c);
+    c->cot[1] = m; m += cot_doubles(c);
+    adj_bind_work(c->A, m, (int)nx, (int)ny, (int)nv);
+    m += rnd32(adj_work_doubles((int)nx, (int)ny, (int)nv));
+    c->adj_seed = m; m += 32;
+    c->adj_ledger = m; m += 32;
+    c->adj_report = m;
+    c->A.status = c->aflags + 3;
+    c->amem_doubles = tot;
+    c->adj_capacity_ckpt = nckpt;
+    c->adj_capacity_seg = nseg;
+    return UGKS_OK;
+}
+
+// cotangent sets, parameter cotangents and the seed for a new reverse sweep
+int adj_clear(ugks_ctx* c, const double* seed) {
+    UGKS_CK(cudaMemsetAsync(c->cot[0], 0, 2 * cot_doubles(c) * sizeof(double), c->stream));
+    UGKS_CK(cudaMemsetAsync(c->A.gpar, 0, GP_COUNT * sizeof(double), c->stream));
+    UGKS_CK(cudaMemsetAsync(c->aflags + 3, 0, sizeof(unsigned), c->stream));
+    double sd[4] = {0.0, 0.0, 0.0, 0.0};
+    if (seed) for (int q = 0; q < 4; ++q) sd[q] = seed[q];
+    UGKS_CK(cudaMemcpyAsync(c->adj_seed, sd, sizeof sd, cudaMemcpyHostToDevice, c->stream));
+    return UGKS_OK;
+}
+
+// synchronise; the forward status word and the adjoint's own
+int adj_status(ugks_ctx* c) {
+    unsigned ast = 0;
+    UGKS_CK(cudaMemcpyAsync(&ast, c->aflags + 3, sizeof ast, cudaMemcpyDeviceToHost, c->stream));
+    const int r = collect_status(c);
+    if (r) return r;
+    c->last_status = ast;
+    return ast ? UGKS_ENUMERIC : UGKS_OK;
+}
+
+int adj_outputs(ugks_ctx* c, double* out) {
+    if (!out) return UGKS_OK;
+    const int nx = c->P.nx;
+    double* a = new (std::nothrow) double[(size_t)2 * nx * 3];
+    if (!a) return UGKS_ENOMEM;
+    cudaError_t e = cudaMemcpyAsync(a, c->B.wall_aero, (size_t)2 * nx * 3 * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
+    if (e == cudaSuccess)
+        for (int w = 0; w < 2; ++w) {
+            double sh = 0.0, ht = 0.0;
+            for (int i = 0; i < nx; ++i) { sh += a[((size_t)w * nx + i) * 3 + 1]; ht += a[((size_t)w * nx + i) * 3 + 2]; }
+            out[2 * w] = sh / nx;
+            out[2 * w + 1] = ht / nx;
+        }
+    delete[] a;
+    return cuda_fail(e);
+}
+
+int adj_download(ugks_ctx* c, const SlotView& v, double* gh, double* gb, double* gW, double* grad) {
+    const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
+    if (gh) UGKS_CK(cudaMemcpyAsync(gh, v.h, S * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (gb) UGKS_CK(cudaMemcpyAsync(gb, v.b, S * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    if (gW) UGKS_CK(cudaMemcpyAsync(gW, v.W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyDeviceToHost,
+                                    c->stream));
+    if (grad) UGKS_CK(cudaMemcpyAsync(grad, c->A.gpar, 5 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    return UGKS_OK;
+}
+
+}  // namespace
+
+extern "C" int ugks_s2cn2_forward_checkpointed(ugks_ctx* c, int nsteps, int every, double* outputs) {
+    if (!c || nsteps < 1 || every < 1) return UGKS_EINVAL;
+    if (!c->cmem) return UGKS_EUNSUPPORTED;
+    if (!c->cn_ready) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    const int nckpt = (nsteps + every - 1) / every, nseg = every < nsteps ? every : nsteps;
+    if (int r = adj_reserve(c, nckpt, nseg)) return r;
+    c->adj_nsteps = 0;
+    for (int q = 0; q < nckpt; ++q) {
+        const SlotView v = ckpt_view(c, q);
+        UGKS_CK(copy_state(c, v, c->Bs[0].h, c->Bs[0].b, c->Bs[0].W));
+        UGKS_CK(copy_ledger(c, v.ledger, c->C.ledger));
+        const int n = (q + 1) * every <= nsteps ? every : nsteps - q * every;
+        int done = 0;
+        const int r = ugks_s2cn2_steps(c, n, &done, nullptr);
+        if (r) return r;
+        if (done != n) return UGKS_ENUMERIC;
+    }
+    c->adj_nsteps = nsteps;
+    c->adj_every = every;
+    return adj_outputs(c, outputs);
+}
+
+extern "C" int ugks_s2cn2_backward(ugks_ctx* c, const double* seed, double* grad, double* gh0, double* gb0,
+                                   double* gW0) {
+    if (!c || !seed) return UGKS_EINVAL;
+    if (!c->cmem) return UGKS_EUNSUPPORTED;
+    if (c->adj_nsteps < 1) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    if (int r = collect_status(c)) return r;
+    if (int r = adj_clear(c, seed)) return r;
+    const int nsteps = c->adj_nsteps, every = c->adj_every, nckpt = (nsteps + every - 1) / every;
+    const CnBuffers Cr = rerun_cn(c);
+    int cur = 0;
+    for (int q = nckpt - 1; q >= 0; --q) {
+        const int n0 = q * every, len = n0 + every <= nsteps ? every : nsteps - n0;
+        const SlotView ck = ckpt_view(c, q), s0 = seg_view(c, 0);
+        UGKS_CK(copy_state(c, s0, ck.h, ck.b, ck.W));
+        UGKS_CK(copy_ledger(c, s0.ledger, ck.ledger));
+        UGKS_CK(s2_enqueue(3, c->P, slot_lo(c, s0), slot_targets(c, s0), c->stream, c->stream, nullptr, nullptr));
+        c->launches += s2_enqueue_kernels(3);
+        for (int m = 0; m + 1 < len; ++m) {   // the segment's states, recomputed from its checkpoint
+            const SlotView a = seg_view(c, m), b = seg_view(c, m + 1);
+            UGKS_CK(rerun_step(c, slot_lo(c, a), slot_targets(c, a), slot_lo(c, b), slot_targets(c, b), a.ledger));
+            UGKS_CK(copy_ledger(c, b.ledger, c->adj_ledger));
+        }
+        for (int m = len - 1; m >= 0; --m) {   // reverse: re-run the step for its scratch, then its adjoint
+            const SlotView a = seg_view(c, m);
+            const LoBuffers Ba = slot_lo(c, a);
+            const S2Buffers Ta = slot_targets(c, a);
+            LoBuffers Bs1 = c->Bs[1];
+            Bs1.halt = c->aflags;
+            UGKS_CK(rerun_step(c, Ba, Ta, Bs1, c->T[1], a.ledger));
+            const bool last = q == nckpt - 1 && m == len - 1;
+            const AdjBuffers A = adj_bind(c, cur, last ? c->adj_seed : nullptr);
+            UGKS_CK(enqueue_s2cn2_adjoint(c->P, Ba, c->T[0], Ta, c->T[1], Cr, A, c->stream));
+            c->launches += kAdjStepKernels;
+            cur = 1 - cur;
+        }
+        if (int r = adj_status(c)) return r;
+    }
+    const SlotView g = cot_view(c, cur);
+    if (gh0 || gb0 || gW0) {   // x_0's targets depend on its W: their cotangent goes to W
+        const SlotView s0 = seg_view(c, 0);
+        UGKS_CK(s2_enqueue(3, c->P, slot_lo(c, s0), c->T[1], c->stream, c->stream, nullptr, nullptr));
+        const AdjBuffers A = adj_bind(c, 1 - cur, nullptr);
+        UGKS_CK(enqueue_targets_adjoint(c->P, slot_lo(c, s0), c->T[0], g.T, g.W, A, c->stream));
+        c->launches += s2_enqueue_kernels(3) + 2;
+        if (int r = adj_status(c)) return r;
+    }
+    return adj_download(c, g, gh0, gb0, gW0, grad);
+}
+
+extern "C" int ugks_s2cn2_step_vjp(ugks_ctx* c, const double* gh, const double* gb, const double* gW, const double* seed,
+                                   double* gh_in, double* gb_in, double* gW_in, double* grad) {
+    if (!c) return UGKS_EINVAL;
+    if (!c->cmem) return UGKS_EUNSUPPORTED;
+    if (!c->cn_ready) return UGKS_EINVAL;
+    UGKS_CK(cudaSetDevice(c->device));
+    if (int r = adj_reserve(c, c->adj_capacity_ckpt > 0 ? c->adj_capacity_ckpt : 1,
+                            c->adj_capacity_seg > 0 ? c->adj_capacity_seg : 1)) return r;
+    if (int r = collect_status(c)) return r;
+    if (int r = adj_clear(c, seed)) return r;
+    const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
+    const SlotView o = cot_view(c, 0), in = cot_view(c, 1);
+    if (gh) UGKS_CK(cudaMemcpyAsync(o.h, gh, S * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (gb) UGKS_CK(cudaMemcpyAsync(o.b, gb, S * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    if (gW) UGKS_CK(cudaMemcpyAsync(o.W, gW, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyHostToDevice,
+                                    c->stream));
+    LoBuffers B0 = c->Bs[0];
+    B0.halt = c->aflags;
+    LoBuffers Bs1 = c->Bs[1];
+    Bs1.halt = c->aflags;
+    UGKS_CK(rerun_step(c, B0, c->T[0], Bs1, c->T[1], c->C.ledger));
+    const AdjBuffers A = adj_bind(c, 0, c->adj_seed);
+    UGKS_CK(enqueue_s2cn2_adjoint(c->P, B0, c->T[0], c->T[0], c->T[1], rerun_cn(c), A, c->stream));
+    UGKS_CK(s2_enqueue(3, c->P, B0, c->T[1], c->stream, c->stream, nullptr, nullptr));   // W's targets, for their adjoint
+    UGKS_CK(enqueue_targets_adjoint(c->P, B0, c->T[0], in.T, in.W, A, c->stream));
+    c->launches += kAdjStepKernels + s2_enqueue_kernels(3) + 2;
+    if (int r = adj_status(c)) return r;
+    return adj_download(c, in, gh_in, gb_in, gW_in, grad);
 }

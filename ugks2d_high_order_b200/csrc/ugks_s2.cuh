@@ -30,11 +30,19 @@ struct S2Buffers {
                      // take the CTA shape with more resident warps
 };
 
+// Node scalar records.  Volume target nodes (tscal): [0..3] closure theta, [4..11] the K_x, K_y
+// closure directions, [12..15] ux vy lam coeff, [16..31] the closure's moment Jacobian (row-major).
+// Interior face nodes (fscal): [0] ok, [1..4] theta, [5..12] K directions, [13..16] ux vy lam coeff,
+// [17..18] q0, [19..34] left/right/tangential/time directions, [35..39] Mt, [40..43] the time-direction
+// moments wt, [44..59] the closure's moment Jacobian.  The Jacobians serve the adjoint (ugks_s2_adjoint.cu).
+constexpr int kS2TScal = 32;
+constexpr int kS2FScal = 64;
+
 // doubles of evaluation scratch one S2Buffers needs, and their layout
 inline size_t s2_scratch_doubles(int nx, int ny, int nv) {
     const size_t nf = (size_t)nx * ny + (size_t)nx * (ny - 1), nfw = nf + 2 * (size_t)nx, nc = (size_t)nx * ny;
     auto r = [](size_t n) { return (n + 31) / 32 * 32; };
-    return r(nfw * 3 * 2 * nv) + r(nfw * 3 * 4) + r(nf * 3 * 12) + r(nc * 9 * 4) + r(nc * 9 * 16) + r(nc * 22 * nv) + r(nf * 3 * 48);
+    return r(nfw * 3 * 2 * nv) + r(nfw * 3 * 4) + r(nf * 3 * 12) + r(nc * 9 * 4) + r(nc * 9 * kS2TScal) + r(nc * 22 * nv) + r(nf * 3 * kS2FScal);
 }
 inline void s2_bind_scratch(S2Buffers& S, double* base, int nx, int ny, int nv) {
     const size_t nf = (size_t)nx * ny + (size_t)nx * (ny - 1), nfw = nf + 2 * (size_t)nx, nc = (size_t)nx * ny;
@@ -43,7 +51,7 @@ inline void s2_bind_scratch(S2Buffers& S, double* base, int nx, int ny, int nv) 
     S.nodew = base; base += r(nfw * 3 * 4);
     S.mac = base; base += r(nf * 3 * 12);
     S.wq = base; base += r(nc * 9 * 4);
-    S.tscal = base; base += r(nc * 9 * 16);
+    S.tscal = base; base += r(nc * 9 * kS2TScal);
     S.l1 = base; base += r(nc * 22 * nv);
     S.fscal = base;
 }

@@ -196,6 +196,49 @@ class Solver:
         self._check(self.L.ugks_s2cn2_report(self.ctx, _p(rep)), "S2CN2 report")
         return rep
 
+    # ---- the S2CN2 adjoint: gradients of the wall outputs (bottom shear, bottom heat, top shear, top heat)
+    # with respect to (mu_ref, wall_ux[0], wall_ux[1], wall_tnative[0], wall_tnative[1])
+    def s2cn2_forward_checkpointed(self, nsteps, every=50):
+        """nsteps S2CN2 steps storing a checkpoint every `every` steps; returns the wall outputs [4]."""
+        out = np.zeros(4)
+        self._check(self.L.ugks_s2cn2_forward_checkpointed(self.ctx, int(nsteps), int(every), _p(out)),
+                    "S2CN2 checkpointed forward")
+        return out
+
+    def s2cn2_backward(self, seed, initial_state=False):
+        """The reverse sweep of the last checkpointed forward: the gradient [5] of sum(seed * outputs),
+        and, with initial_state, the cotangents (h, b, W) of the initial state."""
+        seed = np.ascontiguousarray(seed, dtype=np.float64)
+        assert seed.size == 4
+        grad = np.zeros(5)
+        if initial_state:
+            gh = np.zeros((self.ny, self.nx, self.nvel))
+            gb = np.zeros_like(gh)
+            gW = np.zeros((self.ny, self.nx, 4))
+            self._check(self.L.ugks_s2cn2_backward(self.ctx, _p(seed), _p(grad), _p(gh), _p(gb), _p(gW)),
+                        "S2CN2 backward")
+            return grad, (gh, gb, gW)
+        self._check(self.L.ugks_s2cn2_backward(self.ctx, _p(seed), _p(grad), None, None, None), "S2CN2 backward")
+        return grad
+
+    def s2cn2_step_vjp(self, gh=None, gb=None, gW=None, seed=None):
+        """The vector-Jacobian product of one S2CN2 step at the current state: output cotangents (gh, gb,
+        gW; None = 0) and the wall outputs' seed [4] -> (gh_in, gb_in, gW_in, grad[5])."""
+        def opt(a, shape):
+            if a is None:
+                return None
+            a = np.ascontiguousarray(a, dtype=np.float64)
+            assert a.size == int(np.prod(shape))
+            return a
+        S = (self.ny, self.nx, self.nvel)
+        gh, gb, gW = opt(gh, S), opt(gb, S), opt(gW, (self.ny, self.nx, 4))
+        seed = opt(seed, (4,))
+        oh, ob, oW, grad = np.zeros(S), np.zeros(S), np.zeros((self.ny, self.nx, 4)), np.zeros(5)
+        P = lambda a: _p(a) if a is not None else None
+        self._check(self.L.ugks_s2cn2_step_vjp(self.ctx, P(gh), P(gb), P(gW), P(seed), _p(oh), _p(ob), _p(oW), _p(grad)),
+                    "S2CN2 step VJP")
+        return oh, ob, oW, grad
+
     def s2cn2_test_reject(self, step):
         """Force step `step` (1-based) of the next step_s2cn2 call to fail its conservation gate
         (the reference's S2D3_TEST_GLOBAL_REJECT / S2E3_TEST_REJECT_STEP hooks)."""
