@@ -218,11 +218,12 @@ int ugks_s2cn2_report(ugks_ctx* ctx, double* report);
  * top heat flux.  The parameters are grad[5] = d/d(mu_ref, wall_ux[0], wall_ux[1], wall_tnative[0],
  * wall_tnative[1]) of the seeded output combination sum_i seed[i] out[i].
  * ugks_s2cn2_forward_checkpointed: nsteps accepted S2CN2 steps from the current state (as
- *   ugks_s2cn2_steps), storing the state and the conservation ledger every `every` steps (device memory
- *   for the checkpoints and one segment of `every` states with their targets is reserved on first use);
- *   out[4] optional.  A rejected step returns UGKS_ENUMERIC (reference code 203) and leaves no trajectory.
+ *   ugks_s2cn2_steps), storing the state and the conservation ledger every `every` steps in device memory
+ *   the context keeps (about (nsteps / every) x 16 doubles per cell-velocity); out[4] optional.  A rejected step returns UGKS_ENUMERIC (reference code 203) and leaves no trajectory.
  * ugks_s2cn2_backward: the reverse sweep over that trajectory: each segment's states are recomputed from
- *   its checkpoint, then every step is re-run for its evaluation scratch and transposed.  grad[5]
+ *   its checkpoint, then every step is re-run for its evaluation scratch and transposed.  Its work memory
+ *   (`every` states with their targets, about 64 doubles per cell-velocity more) is reserved by the first
+ *   backward and kept with the context.  grad[5]
  *   optional; gh0, gb0 [ny][nx][nvel] and gW0 [ny][nx][4] (optional) receive the cotangent of the initial
  *   state (its targets' dependence on W included).  The adjoint holds the time step fixed: it returns
  *   UGKS_ENUMERIC with ugks_last_status bit 0x400 if a state's dt is set by |U| + c instead of the

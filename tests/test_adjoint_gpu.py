@@ -189,3 +189,36 @@ def test_one_step_backward_equals_the_step_vjp():
         s.close()
     for a, c in ((grad, vgrad), (gh, vh), (gb, vb), (gW, vW)):
         assert np.abs(a - c).max() <= 1e-12 * max(np.abs(c).max(), 1e-300)
+
+
+def test_autograd_function_gives_the_parameter_gradients():
+    """WallOutputs (torch.autograd.Function over the C ABI): the gradient of a loss of the wall outputs in
+    (wall speed, wall temperature, tau scale) of two cases against central differences of the loss."""
+    import torch
+    from ugks2d_high_order_b200.adjoint import case_at, wall_outputs
+    vel = velocity_table(24)
+    base = _case()
+    cases = [(base, vel), (base.with_(mu_ref=base.mu_ref * 2.0), vel)]
+    p0 = np.array([[abs(base.wall_ux[1]), base.wall_tnative[0], 1.0],
+                   [0.7 * abs(base.wall_ux[1]), 1.1 * base.wall_tnative[0], 0.8]])
+    wts = torch.tensor([[[1.0, -0.5], [0.25, 2.0]], [[-1.0, 0.3], [0.7, 1.5]]], dtype=torch.float64)
+    nsteps = 5
+    params = torch.tensor(p0, dtype=torch.float64, requires_grad=True)
+    out = wall_outputs(params, cases, nsteps, every=2)
+    loss = (wts * out).sum()
+    loss.backward()
+
+    def loss_at(p):
+        return float((wts * wall_outputs(torch.tensor(p, dtype=torch.float64), cases, nsteps, every=nsteps)).sum())
+
+    fd = np.zeros_like(p0)
+    for n in range(2):
+        for q in range(3):
+            d = 1e-6 * abs(p0[n, q])
+            pp, pm = p0.copy(), p0.copy()
+            pp[n, q] += d
+            pm[n, q] -= d
+            fd[n, q] = (loss_at(pp) - loss_at(pm)) / (2.0 * d)
+    g = params.grad.numpy()
+    assert np.abs(g - fd).max() <= FD_TOL * np.abs(g).max(), (g, fd)
+    assert case_at(base, 1.0, 2.0, 3.0).mu_ref == 3.0 * base.mu_ref

@@ -87,9 +87,9 @@ struct ugks_ctx {
     int cn_stage = 0;              // per-operator S2CN2 step: 1 after the evolution, 2 after the residual
     cudaGraphExec_t cgraph = nullptr;
     // S2CN2 adjoint (ugks_s2cn2_forward_checkpointed / ugks_s2cn2_backward / ugks_s2cn2_step_vjp)
-    double* amem = nullptr;        // checkpoints, segment slots, cotangent sets, adjoint work
+    double* amem = nullptr;        // checkpoints (held from the checkpointed forward to the context's end)
+    double* bmem = nullptr;        // segment slots, cotangent sets, adjoint work (reserved by the backward)
     unsigned* aflags = nullptr;    // [0..2] halt, counter, accepted of the re-runs, [3] adjoint status
-    size_t amem_doubles = 0;
     int adj_capacity_ckpt = 0, adj_capacity_seg = 0;
     double* ckpt = nullptr;        // [ckpt][h | b | W | ledger]
     double* seg = nullptr;         // [slot][h | b | W | 6 targets | ledger]
@@ -307,6 +307,7 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->iloop_ctr) cudaFree(c->iloop_ctr);
     if (c->cgraph) cudaGraphExecDestroy(c->cgraph);
     if (c->amem) cudaFree(c->amem);
+    if (c->bmem) cudaFree(c->bmem);
     if (c->aflags) cudaFree(c->aflags);
     if (c->cmem) cudaFree(c->cmem);
     if (c->cflags) cudaFree(c->cflags);
@@ -1156,30 +1157,41 @@ cudaError_t rerun_step(ugks_ctx* c, const LoBuffers& Bin, const S2Buffers& Tin, 
     return e;
 }
 
-int adj_reserve(ugks_ctx* c, int nckpt, int nseg) {
-    if (c->amem && c->adj_capacity_ckpt >= nckpt && c->adj_capacity_seg >= nseg) return UGKS_OK;
-    if (c->amem) { cudaFree(c->amem); c->amem = nullptr; }
+// the checkpoints of a trajectory (the checkpointed forward); kept until the next reservation or the
+// context's end
+int adj_reserve_ckpt(ugks_ctx* c, int nckpt) {
+    if (c->amem && c->adj_capacity_ckpt >= nckpt) return UGKS_OK;
+    if (c->amem) { cudaFree(c->amem); c->amem = nullptr; c->adj_capacity_ckpt = 0; }
+    UGKS_CK(cudaMalloc(&c->amem, (size_t)nckpt * ckpt_doubles(c) * sizeof(double)));
+    c->ckpt = c->amem;
+    c->adj_capacity_ckpt = nckpt;
+    return UGKS_OK;
+}
+
+// the reverse sweep's work: nseg segment slots, the two cotangent sets and the adjoint's arrays
+int adj_reserve_bwd(ugks_ctx* c, int nseg) {
+    if (!c->aflags) {
+        UGKS_CK(cudaMalloc(&c->aflags, 4 * sizeof(unsigned)));
+        UGKS_CK(cudaMemsetAsync(c->aflags, 0, 4 * sizeof(unsigned), c->stream));
+    }
+    if (c->bmem && c->adj_capacity_seg >= nseg) return UGKS_OK;
+    if (c->bmem) { cudaFree(c->bmem); c->bmem = nullptr; c->adj_capacity_seg = 0; }
     const size_t nx = c->P.nx, ny = c->P.ny, nv = c->P.nvel;
-    const size_t tot = (size_t)nckpt * ckpt_doubles(c) + (size_t)nseg * seg_doubles(c) + 2 * cot_doubles(c) +
-                       rnd32(adj_work_doubles((int)nx, (int)ny, (int)nv)) + 3 * 32;
+    const size_t work = rnd32(adj_work_doubles((int)nx, (int)ny, (int)nv));
+    const size_t tot = (size_t)nseg * seg_doubles(c) + 2 * cot_doubles(c) + work + 3 * 32;
     UGKS_CK(prepare_s2_adjoint());
-    UGKS_CK(cudaMalloc(&c->amem, tot * sizeof(double)));
-    if (!c->aflags) UGKS_CK(cudaMalloc(&c->aflags, 4 * sizeof(unsigned)));
-    UGKS_CK(cudaMemsetAsync(c->amem, 0, tot * sizeof(double), c->stream));
-    UGKS_CK(cudaMemsetAsync(c->aflags, 0, 4 * sizeof(unsigned), c->stream));
-    double* m = c->amem;
-    c->ckpt = m; m += (size_t)nckpt * ckpt_doubles(c);
+    UGKS_CK(cudaMalloc(&c->bmem, tot * sizeof(double)));
+    UGKS_CK(cudaMemsetAsync(c->bmem, 0, tot * sizeof(double), c->stream));
+    double* m = c->bmem;
     c->seg = m; m += (size_t)nseg * seg_doubles(c);
     c->cot[0] = m; m += cot_doubles(c);
     c->cot[1] = m; m += cot_doubles(c);
     adj_bind_work(c->A, m, (int)nx, (int)ny, (int)nv);
-    m += rnd32(adj_work_doubles((int)nx, (int)ny, (int)nv));
+    m += work;
     c->adj_seed = m; m += 32;
     c->adj_ledger = m; m += 32;
     c->adj_report = m;
     c->A.status = c->aflags + 3;
-    c->amem_doubles = tot;
-    c->adj_capacity_ckpt = nckpt;
     c->adj_capacity_seg = nseg;
     return UGKS_OK;
 }
@@ -1242,8 +1254,8 @@ extern "C" int ugks_s2cn2_forward_checkpointed(ugks_ctx* c, int nsteps, int ever
     if (!c->cmem) return UGKS_EUNSUPPORTED;
     if (!c->cn_ready) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
-    const int nckpt = (nsteps + every - 1) / every, nseg = every < nsteps ? every : nsteps;
-    if (int r = adj_reserve(c, nckpt, nseg)) return r;
+    const int nckpt = (nsteps + every - 1) / every;
+    if (int r = adj_reserve_ckpt(c, nckpt)) return r;
     c->adj_nsteps = 0;
     for (int q = 0; q < nckpt; ++q) {
         const SlotView v = ckpt_view(c, q);
@@ -1267,8 +1279,9 @@ extern "C" int ugks_s2cn2_backward(ugks_ctx* c, const double* seed, double* grad
     if (c->adj_nsteps < 1) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
     if (int r = collect_status(c)) return r;
-    if (int r = adj_clear(c, seed)) return r;
     const int nsteps = c->adj_nsteps, every = c->adj_every, nckpt = (nsteps + every - 1) / every;
+    if (int r = adj_reserve_bwd(c, every < nsteps ? every : nsteps)) return r;
+    if (int r = adj_clear(c, seed)) return r;
     const CnBuffers Cr = rerun_cn(c);
     int cur = 0;
     for (int q = nckpt - 1; q >= 0; --q) {
@@ -1316,8 +1329,7 @@ extern "C" int ugks_s2cn2_step_vjp(ugks_ctx* c, const double* gh, const double* 
     if (!c->cmem) return UGKS_EUNSUPPORTED;
     if (!c->cn_ready) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
-    if (int r = adj_reserve(c, c->adj_capacity_ckpt > 0 ? c->adj_capacity_ckpt : 1,
-                            c->adj_capacity_seg > 0 ? c->adj_capacity_seg : 1)) return r;
+    if (int r = adj_reserve_bwd(c, c->adj_capacity_seg > 0 ? c->adj_capacity_seg : 1)) return r;
     if (int r = collect_status(c)) return r;
     if (int r = adj_clear(c, seed)) return r;
     const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
