@@ -118,3 +118,34 @@ def test_repeated_solves_on_one_context_are_identical(velocity):
             assert np.array_equal(x, y)
     finally:
         s.close()
+
+
+@pytest.mark.gpu
+def test_implicit_steady_follows_the_oracle_past_the_gate(velocity):
+    """3000 accepted pseudo-steps of the delivered case with BASELINE's 1e-10 gate, against the oracle's
+    trajectory (tests/golden/oracle_implicit_3000.json, from make_oracle_trajectory.py).
+
+    The 1e-10 gate is not reached: science_3 (the rho*V residual relative to its near-zero reference)
+    still sits above it at 3000 pseudo-steps.  The device follows the oracle's trajectory: the macro and
+    micro residual columns within 1e-6 relative at every recorded step, and c_minus_1 at round-off."""
+    import json
+    import os
+    from ugks2d_high_order_b200.solver import Solver
+    with open(os.path.join(os.path.dirname(__file__), "golden", "oracle_implicit_3000.json")) as f:
+        rows = {int(k): np.array(v) for k, v in json.load(f)["rows"].items()}
+    s = Solver(reference_case("ImplicitSteady").with_(residual_tol=1e-10), *velocity)
+    try:
+        s.init_freestream()
+        s.implicit_init()
+        at = 0
+        for n in sorted(rows):
+            done, conv, rep = s.step_implicit(n - at)
+            assert done == n - at and not conv
+            at = n
+            o = rows[n]
+            for col in (12, 13, 14, 15, 24, 25):       # science_1..4, R_h, R_b
+                assert abs(rep[col] - o[col]) <= 1e-6 * abs(o[col]), (n, col, rep[col], o[col])
+            assert abs(rep[52]) <= 1e-14 and abs(o[52]) <= 1e-14
+        assert rows[3000][14] > 1e-10   # the 1e-10 gate is still not met by the oracle either
+    finally:
+        s.close()
