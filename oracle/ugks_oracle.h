@@ -102,6 +102,19 @@ int uo_s2_init_state(uo_ctx* c);
 int uo_s2cn2_init(uo_ctx* c);
 int uo_s2cn2_step(uo_ctx* c, double* out, int nout);
 
+/* The reference's tangent routines of the high-order path, restated (ugks_oracle_reftan.c): return 1
+ * when every output is finite.  n velocities u, v with weights wt; w the conserved state. */
+int uo_ref_maxwellian_direction(const double w[4], const double dw[4], int ck, int n, const double* u, const double* v,
+                                double* mh, double* mb, double* dmh, double* dmb);
+int uo_ref_dq_direction(const double w[4], const double dw[4], const double m[4], const double dm[4], int ck, int n,
+                        const double* u, const double* v, const double* wt, double* ch, double* cb, double* dch,
+                        double* dcb);
+int uo_ref_projector_direction(const double w[4], const double dw[4], const double* zh, const double* zb,
+                               const double* dzh, const double* dzb, int ck, int n, const double* u, const double* v,
+                               const double* wt, double* ph, double* pb, double* dph, double* dpb);
+int uo_ref_weno_direction(const double q[5], const double dq[5], double xi, double* val, double* dval,
+                          int* differentiable);
+
 /* Worker threads used over faces and cells (0 = all host cores); returns the count in use.
  * Results do not depend on the thread count: faces and cells are independent and every sum over
  * cells is taken afterwards in cell order. */

@@ -1483,3 +1483,5 @@ int uo_s2cn2_step(uo_ctx* c, double* out, int nout) {
     for (int m = 0; m < 4; ++m) c->cn_balance[m] = o[18 + m];
     return 0;
 }
+
+#include "ugks_oracle_reftan.c"
