@@ -24,8 +24,8 @@ itself prescribes), no dataset is involved.
                  3000-pseudo-step cap, c_minus_1 recorded, with a bounded oracle sample beside it.
   s2cn2          the explicit high-order S2CN2 step (S2 evolution + Crank-Nicolson collision) on the same
                  case, with a bounded oracle sample beside it.
-  adjoint_shape  the adjoint config's 64 cases (8x64x1024): the adjoint is not built; the batch gives the
-                 gradients by central differences (7 instances per case), timed against the forward batch.
+  adjoint        the adjoint config's cases (8x64x1024): the gradient of the wall outputs by the discrete
+                 adjoint (checkpointed forward + reverse sweep), timed against the plain forward of the same cases.
   batched        (N > 1: the instances are split over the ranks by an LPT greedy on cells x velocities,
                  no collective; time = max over ranks; value = all instances' work / that time)
                  256 S2CN2 instances of the batched distribution (Kn log-uniform in [0.01, 1], wall Mach
@@ -60,6 +60,9 @@ HO_MAX_PSEUDO_STEPS = 3000     # HighOrderImplicit cap (cases/high_implicit/Conf
 S2CN2_STEPS = 400
 REFINED_PSEUDO_STEPS = 100   # timed pseudo-steps of the refined HighOrderImplicit variant
 BATCH_STEPS = 4               # batched steps timed (each advances all 256 instances by one step)
+ADJ_STEPS = 50                # adjoint timing: one checkpoint segment of 50 steps per case
+ADJ_EVERY = 50
+ADJ_CASES = 4                 # cases of the 64 timed (each gradient is an independent instance)
 C5_STEPS = 2                  # steps timed at the adjoint config's shape (64 cases, 8x64x1024); even:
                               # one replay of the two-step graph
 # algorithmic bytes per cell*velocity of the stages (FP64 h and b):
@@ -579,7 +582,7 @@ def main():
     fpk = fp64_peak(f"cuda:{local}")
     roofline["fp64"] = fp64_fraction(FLOPS_PER_UPDATE["implicit_steady"], value / world, fpk)
 
-    # ---------------- BASELINE's tolerance 1e-10 (the reference's case file uses 1e-8)
+    # ---------------- the 1e-10 residual tolerance of the headline metric (the reference's case file uses 1e-8)
     s10 = Solver(case.with_(residual_tol=1e-10), *vel, device=local)
     s10.init_freestream()
     s10.implicit_init()
@@ -732,42 +735,65 @@ def main():
                          "(the distribution's full run is 2000 steps)"}
     bt.close()
 
-    # ---------------- the adjoint config's shape: 64 cases of the batched distribution at 8x64 cells and
-    # 32^2 velocities.  The adjoint is not built; the wall-output gradients come from central
-    # differences on the batch (7 instances per case, ugks2d_high_order_b200.sensitivity), timed here
-    # against the forward batch of the same cases.
-    from ugks2d_high_order_b200.sensitivity import sensitivity_instances
-
-    def batch_ms_per_step(instances, steps):
-        bb = Batch(instances, device=local, max_streams=32)
-        try:
-            bb.init_freestream()
-            bb.run(2)   # warm-up: builds and runs the two-step graph outside the timed region
-            st_ = torch.cuda.ExternalStream(bb.stream)
-            f0, f1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            with torch.cuda.stream(st_):
-                f0.record(st_)
-                bb.run(steps)
-                f1.record(st_)
-            f1.synchronize()
-            return f0.elapsed_time(f1) / steps
-        finally:
-            bb.close()
-
+    # ---------------- the adjoint workload: gradients of the wall shear and heat flux with respect
+    # to wall speed, wall temperature and the tau scale through the S2CN2 steps of 64 cases of the batched
+    # distribution at 8x64 cells and 32^2 velocities, checkpoint every 50 steps.  ADJ_CASES of them are timed
+    # over one full checkpoint segment: the plain forward, and the gradient (the checkpointed forward and the
+    # reverse sweep with recompute), each on the case's own stream with CUDA events.
     c5_all = [(c.with_(ny=64, dy=1.0 / 64), 32) for c, _ in batched_cases(64)]
     c5, _ = shard(c5_all, [1] * len(c5_all), rank, world)
-    fwd_ms = batch_ms_per_step([(c, tables[n]) for c, n in c5], C5_STEPS)
-    sens_ms = batch_ms_per_step(sensitivity_instances(c5), C5_STEPS)
+    seed = np.array([1.0, 1.0, 1.0, 1.0])
+    grads = []
+    fwd_list, fc_list, bw_list = [], [], []
+    for case, nva in c5[:ADJ_CASES]:
+        sv = Solver(case, *tables[nva], device=local)
+        try:
+            st_ = torch.cuda.ExternalStream(sv.stream)
+            sv.init_freestream(tnative=2.0)
+            sv.step_s2cn2(2)   # graph capture; then a full-size gradient reserves the adjoint's memory
+            sv.init_freestream(tnative=2.0)
+            sv.s2cn2_forward_checkpointed(ADJ_STEPS, every=ADJ_EVERY)
+            sv.s2cn2_backward(seed)
+            sv.init_freestream(tnative=2.0)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+            with torch.cuda.stream(st_):
+                ev[0].record(st_)
+                sv.step_s2cn2(ADJ_STEPS)
+                ev[1].record(st_)
+            ev[1].synchronize()
+            sv.init_freestream(tnative=2.0)
+            with torch.cuda.stream(st_):
+                ev[2].record(st_)
+                sv.s2cn2_forward_checkpointed(ADJ_STEPS, every=ADJ_EVERY)
+                ev[3].record(st_)
+                g = sv.s2cn2_backward(seed)
+                ev[4].record(st_)
+            ev[4].synchronize()
+            fwd_list.append(ev[0].elapsed_time(ev[1]))
+            fc_list.append(ev[2].elapsed_time(ev[3]))
+            bw_list.append(ev[3].elapsed_time(ev[4]))
+            grads.append([float(x) for x in g])
+        finally:
+            sv.close()
+    fwd_ms, fc_ms, bw_ms = sum(fwd_list), sum(fc_list), sum(bw_list)
     barrier()
-    fwd_ms, sens_ms = max_over_ranks(fwd_ms), max_over_ranks(sens_ms)
-    adjoint_shape = {"adjoint": "not built", "gradients": "central differences on the batch: per case the base "
-                     "instance and +-1e-6 relative steps of wall speed, wall temperature and the tau scale",
-                     "cases": len(c5_all), "steps": C5_STEPS, "forward_ms_per_step": fwd_ms,
-                     "gradients_ms_per_step": sens_ms, "cost_vs_forward": sens_ms / fwd_ms,
-                     "full_run_estimate_s": 2000 * sens_ms * 1e-3,
-                     "config": "64 S2CN2 cases of the batched distribution at 8x64 cells, 32x32 velocities, "
-                               "cold start; 2 steps warm-up (graph built), then the timed steps (the config's "
-                               "run is 2000 steps)"}
+    fwd_ms, fc_ms, bw_ms = max_over_ranks(fwd_ms), max_over_ranks(fc_ms), max_over_ranks(bw_ms)
+    n_t = len(fwd_list)
+    adjoint = {"gradients": "hand-written discrete adjoint of the S2CN2 step (ugks_s2cn2_forward_checkpointed + "
+                            "ugks_s2cn2_backward: checkpoint every %d steps, each segment recomputed, each step "
+                            "re-run for its scratch and transposed)" % ADJ_EVERY,
+               "cases": len(c5_all), "cases_timed": n_t, "steps": ADJ_STEPS,
+               "forward_ms_per_step": fwd_ms / (n_t * ADJ_STEPS),
+               "checkpointed_forward_ms_per_step": fc_ms / (n_t * ADJ_STEPS),
+               "backward_ms_per_step": bw_ms / (n_t * ADJ_STEPS),
+               "gradient_ms_per_step": (fc_ms + bw_ms) / (n_t * ADJ_STEPS),
+               "cost_vs_forward": (fc_ms + bw_ms) / fwd_ms,
+               "backward_vs_forward": bw_ms / fwd_ms,
+               "full_run_estimate_s": 2000 * len(c5_all) * (fc_ms + bw_ms) / (n_t * ADJ_STEPS) * 1e-3,
+               "grad_first_case": grads[0] if grads else None,
+               "config": "%d of the 64 cases of the batched distribution at 8x64 cells, 32x32 velocities, from the "
+                         "cold start; one checkpoint segment of %d steps each; seed = sum of the four wall "
+                         "outputs; every case runs on its own context and stream" % (n_t, ADJ_STEPS)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -801,7 +827,7 @@ def main():
                 "high_order_implicit": high_order,
                 "s2cn2": s2cn2,
                 "batched": batched,
-                "adjoint_shape": adjoint_shape,
+                "adjoint": adjoint,
                 "clocks": clocks}
         print(json.dumps(line), flush=True)
     s.close()

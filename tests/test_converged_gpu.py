@@ -122,7 +122,7 @@ def test_repeated_solves_on_one_context_are_identical(velocity):
 
 @pytest.mark.gpu
 def test_implicit_steady_follows_the_oracle_past_the_gate(velocity):
-    """3000 accepted pseudo-steps of the delivered case with BASELINE's 1e-10 gate, against the oracle's
+    """3000 accepted pseudo-steps of the delivered case with the headline metric's 1e-10 gate, against the oracle's
     trajectory (tests/golden/oracle_implicit_3000.json, from make_oracle_trajectory.py).
 
     The 1e-10 gate is not reached: science_3 (the rho*V residual relative to its near-zero reference)
