@@ -13,7 +13,7 @@ from ugks2d_high_order_b200.case import reference_case, velocity_table
 
 pytestmark = pytest.mark.gpu
 
-HO_TOL = 1e-9   # GPU S2 evaluation vs the oracle (tree-ordered vs sequential moment sums)
+HO_TOL = 1e-11   # GPU S2 evaluation vs the oracle (per-lane + butterfly vs sequential moment sums)
 
 
 def _s2cn2_case():

@@ -122,17 +122,26 @@ def test_repeated_solves_on_one_context_are_identical(velocity):
 
 @pytest.mark.gpu
 def test_implicit_steady_follows_the_oracle_past_the_gate(velocity):
-    """3000 accepted pseudo-steps of the delivered case with the headline metric's 1e-10 gate, against the oracle's
-    trajectory (tests/golden/oracle_implicit_3000.json, from make_oracle_trajectory.py).
+    """3000 accepted pseudo-steps of the delivered case with the headline metric's 1e-10 gate, against the
+    oracle's trajectory (tests/golden/oracle_implicit_3000.json, from make_oracle_trajectory.py).
 
-    The 1e-10 gate is not reached: science_3 (the rho*V residual relative to its near-zero reference)
-    still sits above it at 3000 pseudo-steps.  The device follows the oracle's trajectory: the macro and
-    micro residual columns within 1e-6 relative at every recorded step, and c_minus_1 at round-off."""
+    The residual columns are norms of the change of one pseudo-step.  While they are far above rounding
+    the device and the oracle give the same numbers (within 1e-9 to step 100, 2e-6 at step 500, where the
+    macro residuals are 1e-7).  From step 1000 on they are made of rounding: the device and the oracle
+    each sit on their own round-off floor, and the columns agree in magnitude only.  science_3, the
+    rho*V residual relative to a near-zero reference, crosses 1e-8 near step 1100 and then stays between
+    1e-10 and 1e-8 on that floor in both:
+    the 1e-10 gate is never reached (the reference's own explicit run stalls the same way, at a rho*V
+    residual of 6.7e-9 after 200,000 steps).  The state itself is converged and the same: W at steps 1100
+    and 3000 agrees with the oracle's to 1e-12 of its largest component."""
     import json
     import os
     from ugks2d_high_order_b200.solver import Solver
     with open(os.path.join(os.path.dirname(__file__), "golden", "oracle_implicit_3000.json")) as f:
-        rows = {int(k): np.array(v) for k, v in json.load(f)["rows"].items()}
+        fx = json.load(f)
+    rows = {int(k): np.array(v) for k, v in fx["rows"].items()}
+    states = {int(k): np.array(v) for k, v in fx["W"].items()}
+    cols = (12, 13, 14, 15, 24, 25)   # science_1..4, R_h, R_b
     s = Solver(reference_case("ImplicitSteady").with_(residual_tol=1e-10), *velocity)
     try:
         s.init_freestream()
@@ -143,9 +152,18 @@ def test_implicit_steady_follows_the_oracle_past_the_gate(velocity):
             assert done == n - at and not conv
             at = n
             o = rows[n]
-            for col in (12, 13, 14, 15, 24, 25):       # science_1..4, R_h, R_b
-                assert abs(rep[col] - o[col]) <= 1e-6 * abs(o[col]), (n, col, rep[col], o[col])
-            assert abs(rep[52]) <= 1e-14 and abs(o[52]) <= 1e-14
-        assert rows[3000][14] > 1e-10   # the 1e-10 gate is still not met by the oracle either
+            if n <= 500:
+                tol = 1e-9 if n <= 100 else 2e-6
+                for col in cols:
+                    assert abs(rep[col] - o[col]) <= tol * abs(o[col]), (n, col, rep[col], o[col])
+            else:
+                for col in (12, 13, 15, 24, 25):
+                    assert rep[col] <= 1e-10 and o[col] <= 1e-10, (n, col, rep[col], o[col])
+                assert 1e-10 < rep[14] < (1e-7 if n <= 1100 else 1e-8), (n, rep[14])
+                assert 1e-10 < o[14], (n, o[14])
+            assert abs(rep[52] - o[52]) <= 1e-13, (n, rep[52], o[52])   # c_minus_1
+            if n in states:
+                W = s.download()[2].reshape(-1)
+                assert np.abs(W - states[n]).max() <= 1e-12 * np.abs(states[n]).max(), n
     finally:
         s.close()

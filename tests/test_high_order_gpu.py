@@ -2,9 +2,9 @@
 
 The S2 evolution (closure targets, WENO-AO reconstruction, Gauss-node UGKS faces, multiscale wall)
 and the implicit update with the high-order collision correction, through the C ABI.  The GPU sums
-velocity moments in a tree and the oracle sequentially, and each Newton closure amplifies that
-rounding, so the bound is 1e-9 relative (the required tolerance is the reference's own run-to-run one for
-the high-order path; the oracle itself matches the reference's printed rows to 5e-13).
+velocity moments per lane and in a butterfly, the oracle sequentially; over ten pseudo-steps the states
+differ by 3e-14 (W) and 6e-13 (h) relative and the printed rows by at most 1.3e-11, so the bound is 1e-11
+for the states and 5e-11 for the rows (the oracle itself matches the reference's printed rows to 5e-13).
 """
 import numpy as np
 import pytest
@@ -12,7 +12,8 @@ import pytest
 from ugks2d_high_order_b200.case import reference_case
 from tests.test_oracle_golden import SPARSE_KEYS
 
-HO_TOL = 1e-9
+HO_TOL = 1e-11    # states against the oracle, relative to the largest component
+ROW_TOL = 5e-11   # printed report rows (against the reference and the oracle)
 
 
 def _rel(a, b):
@@ -42,7 +43,7 @@ def test_high_order_two_steps_match_oracle_and_reference(velocity, golden):
             for i, k in enumerate(SPARSE_KEYS):
                 r = ref[k]
                 if abs(r) > 1e-10:
-                    assert abs(rep[i] - r) <= HO_TOL * abs(r), (step, k, rep[i], r)
+                    assert abs(rep[i] - r) <= ROW_TOL * abs(r), (step, k, rep[i], r)
                 else:
                     assert abs(rep[i] - r) <= 1e-13, (step, k, rep[i], r)
             hg, bg, Wg = s.download()
@@ -70,7 +71,7 @@ def test_high_order_ten_steps_match_oracle(velocity):
         ho, bo, Wo = o.get_state()
         assert done == 10
         assert _rel(Wg, Wo) <= HO_TOL and _rel(hg, ho) <= HO_TOL, (_rel(Wg, Wo), _rel(hg, ho))
-        assert abs(rep[52] - row[52]) <= HO_TOL * max(abs(row[52]), 1e-3)   # c_minus_1
+        assert abs(rep[52] - row[52]) <= ROW_TOL * max(abs(row[52]), 1e-3)   # c_minus_1
     finally:
         s.close()
 
@@ -98,6 +99,6 @@ def test_refined_high_order_two_steps_match_oracle():
             ho, bo, Wo = o.get_state()
             assert _rel(Wg, Wo) <= HO_TOL and _rel(hg, ho) <= HO_TOL, (step, _rel(Wg, Wo), _rel(hg, ho))
             for i in (12, 13, 15, 24, 25):   # science_1, 2, 4 and the micro residuals
-                assert abs(rep[i] - row[i]) <= 1e-8 * abs(row[i]), (step, i, rep[i], row[i])
+                assert abs(rep[i] - row[i]) <= ROW_TOL * abs(row[i]), (step, i, rep[i], row[i])
     finally:
         s.close()

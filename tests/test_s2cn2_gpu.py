@@ -4,16 +4,17 @@ The step is TimeStep, S2NativeEvolution with the volume targets kept between ste
 and S2NativeApplyUpdate's advance_step on the stream state (mod_S2NativeAdapter.f90:469-490,867-940;
 mod_S2D1.f90:1302-1435), through the C ABI.  The reference ships no S2CN2 output for this case
 (consistency/high_explicit holds inputs only), so the oracle is the checker; its S2 evolution is the
-code pinned to the reference's high_implicit rows.  GPU moment sums are tree-ordered and the oracle's
-sequential, and every Newton closure amplifies that rounding: the bound is 1e-9 relative, as for the
-other high-order tests.
+code pinned to the reference's high_implicit rows.  GPU moment sums are per lane and in a butterfly, the
+oracle's sequential; over a dozen steps the states differ by 3e-16 (W) and 1.4e-15 (h, b) relative and the
+wall fluxes by 4e-13, so the bounds are 1e-12 for the states and 1e-11 for the report.
 """
 import numpy as np
 import pytest
 
 from ugks2d_high_order_b200.case import reference_case
 
-HO_TOL = 1e-9
+HO_TOL = 1e-12    # states against the oracle, relative to the largest component
+REP_TOL = 1e-11   # report entries
 GATE = 2e-12
 
 
@@ -46,9 +47,9 @@ def test_s2cn2_steps_match_oracle(velocity):
             assert rep[1] <= GATE and rep[2] <= GATE and rep[9] <= GATE
             assert abs(rep[4] - out[4]) <= 1e-14             # transport CFL
             for q in (5, 6, 7, 8):                           # min/max of h and b
-                assert abs(rep[q] - out[q]) <= HO_TOL * max(abs(out[q]), 1e-6), (step, q, rep[q], out[q])
+                assert abs(rep[q] - out[q]) <= REP_TOL * max(abs(out[q]), 1e-6), (step, q, rep[q], out[q])
             for q in range(10, 22):                          # wall fluxes and the ledger
-                assert abs(rep[q] - out[q]) <= HO_TOL * max(abs(out[q]), 1e-3), (step, q, rep[q], out[q])
+                assert abs(rep[q] - out[q]) <= REP_TOL * max(abs(out[q]), 1e-3), (step, q, rep[q], out[q])
             hg, bg, Wg = s.download()
             ho, bo, Wo = o.get_state()
             assert _rel(Wg, Wo) <= HO_TOL and _rel(hg, ho) <= HO_TOL and _rel(bg, bo) <= HO_TOL, \
@@ -75,7 +76,7 @@ def test_s2cn2_graph_pairs_and_odd_tail_match_oracle(velocity):
             assert _rel(Wg, Wo) <= HO_TOL and _rel(hg, ho) <= HO_TOL and _rel(bg, bo) <= HO_TOL, \
                 (n, _rel(Wg, Wo), _rel(hg, ho), _rel(bg, bo))
             for q in range(10, 22):
-                assert abs(rep[q] - out[q]) <= HO_TOL * max(abs(out[q]), 1e-3), (n, q, rep[q], out[q])
+                assert abs(rep[q] - out[q]) <= REP_TOL * max(abs(out[q]), 1e-3), (n, q, rep[q], out[q])
     finally:
         s.close()
 

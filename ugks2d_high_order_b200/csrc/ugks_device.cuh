@@ -265,6 +265,22 @@ __device__ __forceinline__ double warp_halving(const double* v) {
     return t[0];   // the total of logical index (lane >> (5 - log2 NP)) when NP <= 32
 }
 
+// Warp-wide sums (maxima) of N values per lane; every lane returns with the totals in v[0..N).
+template <int N>
+__device__ __forceinline__ void warp_sum_all(double* v) {
+    constexpr int sh = 5 - ilog2(pow2_ceil(N));
+    const double r = warp_halving<N, false>(v);
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = __shfl_sync(0xffffffffu, r, i << sh);
+}
+template <int N>
+__device__ __forceinline__ void warp_max_all(double* v) {
+    constexpr int sh = 5 - ilog2(pow2_ceil(N));
+    const double r = warp_halving<N, true>(v);
+#pragma unroll
+    for (int i = 0; i < N; ++i) v[i] = __shfl_sync(0xffffffffu, r, i << sh);
+}
+
 // Reduce into shared memory only: on return out[0..NS+NM) holds the block totals and is visible
 // to every thread.  The next reduction writes `out` only after its first barrier, which no thread
 // passes before it has read this one, so no trailing barrier is needed.

@@ -13,8 +13,9 @@
 // The reference runs NP_Y ranks stacked in y.  PR(2) and LU-SGS are Gauss-Seidel inside a rank and
 // read the other ranks' corrections, and the x-periodic self-exchange, from halos refreshed only at
 // the exchange points, so the device keeps the same seams ("slabs"):
-//   * PR(2): one thread per slab; each sweep reads other slabs / the x wrap from the previous
-//     sweep's complete buffer and its own cells Gauss-Seidel from the current one (double buffer);
+//   * PR(2): one CTA per slab, an anti-diagonal wavefront of its cells; each sweep reads other slabs /
+//     the x wrap from the previous sweep's complete buffer and its own cells Gauss-Seidel from the
+//     current one (double buffer);
 //   * LU-SGS: one thread per (slab, velocity) -- the per-velocity upwind sweep -- forward with zero
 //     halos, backward with the forward result as halo, the diffuse-wall closure frozen per cell from
 //     the forward correction between the two stages.
@@ -629,17 +630,24 @@ __device__ __forceinline__ bool diag_cell(int d, int t, int rows, int nx, int& i
 // One PR(2) sweep of one slab (SolveMacroPR2, mod_ImplicitMacro.f90:57-88; RelaxMacroPoint :90-123).
 // Lexicographic Gauss-Seidel on the 5-point stencil equals an anti-diagonal wavefront: cell (i,j)
 // reads the already-updated (i-1,j), (i,j-1) and the not-yet-updated (i+1,j), (i,j+1), and cells on
-// one anti-diagonal never read each other.  Four lanes per cell: as faces they build the face terms
-// len * (dF_i + dF_j) and len * gamma * delta_nb; as components they sum them in face order and
-// relax; three of them then refresh the cell's Euler primitives.  The state W + delta of a cell
-// is the neighbour state of every interior face that touches it, so its primitives (the divisions
-// of the Euler flux) are computed once per relaxation and shared.  Everything lives in shared
-// memory; the halo cells (x wrap, slab seams) hold the previous sweep's corrections X.
-// Y = this sweep's result.
-// shared doubles of one slab: corrections, states and primitives of interior + halo cells, then
-// W, rate, gamma, fixed fluxes and the diagonal of the interior cells
+// one anti-diagonal never read each other.  Four lanes per cell, one per component: each sums its
+// component of the four face terms len * (dF_i + dF_j) and len * gamma * delta_nb in face order and
+// relaxes it.  The chain of dependent relaxations is kept short: what a relaxation reads is ready in
+// shared memory when the wavefront reaches the cell.
+//   * Every cell's normal Euler fluxes are kept as two vectors, F(T, (1,-0)) and F(T, (-0,1)) with
+//     T = W + correction; the lanes that relax a cell refresh them for its new state (primitives and
+//     fluxes, the divisions of EulerFluxNormal, once per relaxation).  A face with the opposite normal
+//     (left, bottom) takes the negated vector: the products are rounded one by one (no contraction),
+//     so F(T, -n) = -F(T, n) exactly, up to the sign of a zero.
+//   * The wall faces' ghost-state flux and ghost correction depend on the cell's own correction only,
+//     which changes only when the cell itself relaxes: they are built before each pass.
+//   * The diagonal 1/dt_ps + 0.5 sum(L gamma)/area is fixed through the sweeps; the division by it is
+//     a multiplication by its reciprocal with one remainder correction (div_by_recip).
+// The halo cells (x wrap, slab seams) hold the previous sweep's corrections X; Y = this sweep's result.
+// shared doubles of one slab: corrections, states and flux pairs of interior + halo cells, then W, rate,
+// gamma, fixed fluxes, diagonal and its reciprocal of the interior cells, then the wall-face terms
 __host__ __device__ constexpr int pr_smem_words(int rows, int nx) {
-    return (rows * nx + 2 * rows + 2 * nx) * 12 + rows * nx * 45;
+    return (rows * nx + 2 * rows + 2 * nx) * 16 + rows * nx * 46 + nx * 16;
 }
 
 // local index of the neighbour of interior cell (i, jl) across face f: interior cells first, then
@@ -650,6 +658,45 @@ __device__ __forceinline__ int pr_neighbour(int i, int jl, int j, int f, int row
     if (f == 1) return i < nx - 1 ? cl + 1 : ncs + rows + jl;
     if (f == 2) return j == 0 ? -1 : (jl > 0 ? cl - nx : ncs + 2 * rows + i);
     return j == ny - 1 ? -1 : (jl < rows - 1 ? cl + nx : ncs + 2 * rows + nx + i);
+}
+
+// a / d for a divisor used many times, from r = 1/d (correctly rounded, computed once): q0 = a r, the
+// remainder a - d q0 is exact in one fused multiply-add, and q0 + remainder * r rounds to a/d
+// (Markstein's division correction, IBM J. Res. Develop. 34(1):111-119, 1990).  Finite operands away
+// from overflow and underflow, which the callers check.
+__device__ __forceinline__ double div_by_recip(double a, double d, double r) {
+    const double q0 = __dmul_rn(a, r);
+    return __fma_rn(__fma_rn(-d, q0, a), r, q0);
+}
+
+// F(t, (1,-0)) and F(t, (-0,1)) of a state and its primitives (EulerFluxNormal with those normals)
+__device__ __forceinline__ void euler_flux_pair(const double t[4], const EulerPrim& e, double fx[4], double fy[4]) {
+    euler_flux_prim(t, e, 1.0, -0.0, fx);
+    euler_flux_prim(t, e, -0.0, 1.0, fy);
+}
+
+// Wall-face terms of the wall rows of this slab: the ghost state Zhu(W) + Zhu(delta) of the cell's
+// current correction, its Euler flux with the wall face's normal, and the ghost correction Zhu(delta).
+// [side][i][4], side 0 the bottom wall (face 2, normal (0,-1)), 1 the top wall (face 3, normal (-0,1)).
+__device__ __forceinline__ void pr_wall_terms(const LoParams& P, const ImParams& Q, int s, int rows, const double* sW,
+                                              const double* sY, double* sWf, double* sWd) {
+    for (int q = threadIdx.x; q < 2 * P.nx; q += blockDim.x) {
+        const int side = q / P.nx, i = q - side * P.nx;
+        const int jl = side == 0 ? 0 : rows - 1, j = s * rows + jl;
+        if (side == 0 ? j != 0 : j != P.ny - 1) continue;
+        const int cl = jl * P.nx + i;
+        const double uw = side == 0 ? Q.wall_ux[0] : Q.wall_ux[1];
+        double wi[4], di[4], wj[4], dnb[4], tj[4], fj[4];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { wi[m] = sW[cl * 4 + m]; di[m] = sY[cl * 4 + m]; }
+        zhu_map(wi, uw, 0.0, wj);
+        zhu_map(di, uw, 0.0, dnb);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) tj[m] = wj[m] + dnb[m];
+        euler_flux(P.gm1, tj, side == 0 ? 0.0 : -0.0, side == 0 ? -1.0 : 1.0, fj);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { sWf[q * 4 + m] = fj[m]; sWd[q * 4 + m] = dnb[m]; }
+    }
 }
 
 // Barrier of the wavefront warps alone (named barrier 1); the other warps of the CTA only fill
@@ -668,29 +715,29 @@ constexpr int kPrThreads = 256;
 // the admissible-alpha masks.  last: the sweep also does BuildPredictedMacroState
 // (mod_ImplicitMacro.f90:159-185) for its cells: the admissible alpha levels of W + alpha Y,
 // ANDed into the macro mask.
-__global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I,
+__global__ void __launch_bounds__(kPrThreads, 1) k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I,
                                                              const double* X, double* Y, int first, int last) {
     if (I.state[IS_STOP] != 0.0) return;
     extern __shared__ double sm[];
-    // face terms of the cells of one diagonal, [term][writer lane]: the faces lanes write a contiguous
-    // row, and the odd row length puts the components lanes' reads of a column on distinct banks
-    __shared__ double part[8][4 * 32 + 1];
     const int s = blockIdx.x, rows = P.ny / Q.nslab, nx = P.nx, ny = P.ny;
     const int ncs = rows * nx, nall = ncs + 2 * rows + 2 * nx, c0 = s * ncs;
     double* sY = sm;                  // [nall][4] corrections
     double* sT = sY + nall * 4;       // [nall][4] W + correction
-    double* sP = sT + nall * 4;       // [nall][4] Euler primitives u, v, p of sT
-    double* sW = sP + nall * 4;       // [ncs][4]
+    double* sF = sT + nall * 4;       // [nall][8] F(T, (1,-0)), F(T, (-0,1))
+    double* sW = sF + nall * 8;       // [ncs][4]
     double* sR = sW + ncs * 4;        // [ncs][4] rate_w
     double* sG = sR + ncs * 4;        // [ncs][4] gamma per face
     double* sFi = sG + ncs * 4;       // [4 components][ncs * 4 faces] fixed Euler flux of the cell
     double* sFj = sFi + ncs * 16;     // [4 components][ncs * 4 faces] fixed Euler flux of the neighbour
     const int ncf = ncs * 4;          // component-major: the cells of a diagonal fall on distinct banks
     double* sD = sFj + ncs * 16;      // [ncs] diagonal
+    double* sRd = sD + ncs;           // [ncs] 1 / diagonal
+    double* sWf = sRd + ncs;          // [2][nx][4] wall-face flux (pr_wall_terms)
+    double* sWd = sWf + nx * 8;       // [2][nx][4] wall-face ghost correction
     const int dcells = rows < nx ? rows : nx;                  // longest anti-diagonal
     const int wave = 4 * (dcells < 32 ? dcells : 32);          // relaxing lanes: 4 per cell
     const int wave_warps = (wave + 31) >> 5;
-    const int f = threadIdx.x & 3, tc = threadIdx.x >> 2, D = wave >> 2;
+    const int m = threadIdx.x & 3, tc = threadIdx.x >> 2, D = wave >> 2;
     const double dtp = B.dt[0] * Q.ncfl / P.cfl;   // PseudoTimeStep (mod_ImplicitCommon.f90:115-119)
     int bad = 0;
     for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) {
@@ -705,7 +752,7 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
             if (!pr_prep_item(P, B, Q, I, c0 + (q >> 2), q & 3, gam, foi, foj)) prep_bad = 1;
             sG[q] = gam;
 #pragma unroll
-            for (int m = 0; m < 4; ++m) { sFi[m * ncf + q] = foi[m]; sFj[m * ncf + q] = foj[m]; }
+            for (int k = 0; k < 4; ++k) { sFi[k * ncf + q] = foi[k]; sFj[k * ncf + q] = foj[k]; }
         }
         if (__syncthreads_or(prep_bad)) return;   // the sequence has stopped (ST_GETPRIMARY)
     } else {
@@ -715,7 +762,7 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
             sFj[(q & 3) * ncf + (q >> 2)] = I.pr_foj[c0 * 16 + q];
         }
     }
-    // interior and halo cells: correction, state, primitives (halo rows beyond a wall stay unused)
+    // interior and halo cells: correction, state, flux pair (halo rows beyond a wall stay unused)
     for (int l = threadIdx.x; l < nall; l += blockDim.x) {
         int g;
         if (l < ncs) g = c0 + l;
@@ -726,12 +773,17 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
         double y[4] = {0.0, 0.0, 0.0, 0.0}, t[4] = {1.0, 0.0, 0.0, 1.0};
         if (g >= 0) {
 #pragma unroll
-            for (int m = 0; m < 4; ++m) { y[m] = first ? 0.0 : X[g * 4 + m]; t[m] = B.W[g * 4 + m] + y[m]; }
+            for (int k = 0; k < 4; ++k) { y[k] = first ? 0.0 : X[g * 4 + k]; t[k] = B.W[g * 4 + k] + y[k]; }
         }
-        const EulerPrim e = euler_prim(P.gm1, t);
+        double fx[4], fy[4];
+        euler_flux_pair(t, euler_prim(P.gm1, t), fx, fy);
 #pragma unroll
-        for (int m = 0; m < 4; ++m) { sY[l * 4 + m] = y[m]; sT[l * 4 + m] = t[m]; }
-        sP[l * 4 + 0] = e.u; sP[l * 4 + 1] = e.v; sP[l * 4 + 2] = e.p;
+        for (int k = 0; k < 4; ++k) {
+            sY[l * 4 + k] = y[k];
+            sT[l * 4 + k] = t[k];
+            sF[l * 8 + k] = fx[k];
+            sF[l * 8 + 4 + k] = fy[k];
+        }
     }
     // the diagonal 1/dt_ps + 0.5 * sum_faces(L * gamma) / area is fixed through the sweeps; the face
     // products are rounded before they are summed in face order, as the reference loop does
@@ -746,80 +798,69 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
         const double diag = 1.0 / dtp + div_area(0.5 * sg, P);
         if (!(isfinite(diag) && diag > 0.0)) bad = 1;
         sD[cl] = diag;
+        sRd[cl] = 1.0 / diag;
     }
+    pr_wall_terms(P, Q, s, rows, sW, sY, sWf, sWd);
     __syncthreads();
-    const double fnx = f == 0 ? -1.0 : (f == 1 ? 1.0 : 0.0);
-    const double fny = f == 2 ? -1.0 : (f == 3 ? 1.0 : (f == 1 ? -0.0 : 0.0));
-    const double flen = f < 2 ? P.dy : P.dx;
-    const double fnxs = f == 3 ? -0.0 : fnx;   // GetFaceGeometry's normals: (-1,0) (1,-0) (0,-1) (-0,1)
     const int ndiag = rows + nx - 1;
-    for (int pass = 0; pass < 2 && (int)threadIdx.x < wave_warps * 32; ++pass) {
+    for (int pass = 0; pass < 2; ++pass) {
+        if (pass == 1) {   // the wall-row cells relaxed in the first pass
+            __syncthreads();
+            pr_wall_terms(P, Q, s, rows, sW, sY, sWf, sWd);
+            __syncthreads();
+        }
+        if ((int)threadIdx.x >= wave_warps * 32) continue;
         for (int dd = 0; dd < ndiag; ++dd) {
             const int d = pass == 0 ? dd : ndiag - 1 - dd;
             for (int t0 = 0; t0 < dcells; t0 += D) {
                 int i = 0, jl = 0;
                 const bool act = (int)threadIdx.x < wave && diag_cell(d, tc + t0, rows, nx, i, jl);
                 const int j = s * rows + jl, cl = jl * nx + i;
-                if (act) {   // lane = face f
-                    double ti[4], fi[4], fj[4], dnb[4];
-#pragma unroll
-                    for (int m = 0; m < 4; ++m) ti[m] = sT[cl * 4 + m];
-                    const EulerPrim ei{sP[cl * 4 + 0], sP[cl * 4 + 1], sP[cl * 4 + 2]};
-                    euler_flux_prim(ti, ei, fnxs, fny, fi);
-                    const int nl = pr_neighbour(i, jl, j, f, rows, nx, ny);
-                    if (nl < 0) {
-                        const double uw = (f == 2 ? Q.wall_ux[0] : Q.wall_ux[1]);
-                        double wi[4], di[4], wj[4], tj[4];
-#pragma unroll
-                        for (int m = 0; m < 4; ++m) { wi[m] = sW[cl * 4 + m]; di[m] = sY[cl * 4 + m]; }
-                        zhu_map(wi, uw, 0.0, wj);
-                        zhu_map(di, uw, 0.0, dnb);
-#pragma unroll
-                        for (int m = 0; m < 4; ++m) tj[m] = wj[m] + dnb[m];
-                        euler_flux(P.gm1, tj, fnxs, fny, fj);
-                    } else {
-                        double tj[4];
-#pragma unroll
-                        for (int m = 0; m < 4; ++m) { tj[m] = sT[nl * 4 + m]; dnb[m] = sY[nl * 4 + m]; }
-                        const EulerPrim ej{sP[nl * 4 + 0], sP[nl * 4 + 1], sP[nl * 4 + 2]};
-                        euler_flux_prim(tj, ej, fnxs, fny, fj);
-                    }
-                    const double gam = sG[cl * 4 + f];
-                    const double* foi = sFi + cl * 4 + f;
-                    const double* foj = sFj + cl * 4 + f;
-#pragma unroll
-                    for (int m = 0; m < 4; ++m) {
-                        const double dti = fi[m] - foi[m * ncf];
-                        const double sm4 = dti + (fj[m] - foj[m * ncf]);
-                        if (!isfinite(sm4)) bad = 1;
-                        part[m][threadIdx.x] = flen * sm4;
-                        part[4 + m][threadIdx.x] = flen * gam * dnb[m];
-                    }
-                }
-                __syncwarp();
                 double tm = 0.0;
-                if (act) {   // lane = component m
-                    const int m = f;
+                if (act) {   // lane = component m of cell (i, j)
                     double sdt = 0.0, sgn = 0.0;
 #pragma unroll
-                    for (int ff = 0; ff < 4; ++ff) { sdt = sdt + part[m][tc * 4 + ff]; sgn = sgn + part[4 + m][tc * 4 + ff]; }
+                    for (int f = 0; f < 4; ++f) {
+                        const int dir = (f >> 1) * 4 + m;
+                        const bool neg = (f & 1) == 0;   // left and bottom faces: normals (-1,0), (0,-1)
+                        const double flen = f < 2 ? P.dy : P.dx;
+                        const double fo = sF[cl * 8 + dir];
+                        const double fi = neg ? -fo : fo;
+                        const int nl = pr_neighbour(i, jl, j, f, rows, nx, ny);
+                        double fj, dnb;
+                        if (nl < 0) {
+                            const int w = (f == 3 ? nx : 0) + i;
+                            fj = sWf[w * 4 + m];
+                            dnb = sWd[w * 4 + m];
+                        } else {
+                            const double fn = sF[nl * 8 + dir];
+                            fj = neg ? -fn : fn;
+                            dnb = sY[nl * 4 + m];
+                        }
+                        const double dti = fi - sFi[m * ncf + cl * 4 + f];
+                        const double sm4 = dti + (fj - sFj[m * ncf + cl * 4 + f]);
+                        if (!isfinite(sm4)) bad = 1;
+                        sdt = __dadd_rn(sdt, __dmul_rn(flen, sm4));
+                        sgn = __dadd_rn(sgn, __dmul_rn(__dmul_rn(flen, sG[cl * 4 + f]), dnb));
+                    }
                     const double rhs = sR[cl * 4 + m] - div_area(0.5 * 1.0 * sdt, P) + div_area(0.5 * 1.0 * sgn, P);
                     if (!isfinite(rhs)) bad = 1;
-                    const double y = rhs / sD[cl];
+                    const double y = div_by_recip(rhs, sD[cl], sRd[cl]);
                     tm = sW[cl * 4 + m] + y;
                     sY[cl * 4 + m] = y;
                     sT[cl * 4 + m] = tm;
                 }
-                // lanes 0..2 of the cell: primitives of the relaxed state, its components gathered from
-                // the cell's 4 lanes (every lane of the warp takes part in the shuffles)
+                // the relaxed state's flux pair, its components gathered from the cell's 4 lanes (every
+                // lane of the warp takes part in the shuffles)
                 double t[4];
 #pragma unroll
-                for (int m = 0; m < 4; ++m) t[m] = __shfl_sync(0xffffffffu, tm, (threadIdx.x & ~3) + m);
-                if (act && f < 3) {
-                    const EulerPrim e = euler_prim(P.gm1, t);
-                    sP[cl * 4 + f] = f == 0 ? e.u : (f == 1 ? e.v : e.p);
+                for (int k = 0; k < 4; ++k) t[k] = __shfl_sync(0xffffffffu, tm, (threadIdx.x & ~3) + k);
+                if (act) {
+                    double fx[4], fy[4];
+                    euler_flux_pair(t, euler_prim(P.gm1, t), fx, fy);
+                    sF[cl * 8 + m] = m == 0 ? fx[0] : (m == 1 ? fx[1] : (m == 2 ? fx[2] : fx[3]));
+                    sF[cl * 8 + 4 + m] = m == 0 ? fy[0] : (m == 1 ? fy[1] : (m == 2 ? fy[2] : fy[3]));
                 }
-                if (t0 + D < dcells) __syncwarp();   // the next chunk rewrites part[]
             }
             pr_wave_sync(wave_warps);
         }
@@ -831,11 +872,11 @@ __global__ void __launch_bounds__(kPrThreads) k_im_pr2_sweep(LoParams P, LoBuffe
         for (int cl = threadIdx.x; cl < ncs; cl += blockDim.x) {
             unsigned mask = 0u;
             double a = 1.0;
-            for (int m = 0; m <= lv; ++m) {
+            for (int k = 0; k <= lv; ++k) {
                 double t[4];
 #pragma unroll
                 for (int q = 0; q < 4; ++q) t[q] = sW[cl * 4 + q] + a * sY[cl * 4 + q];
-                if (is_physical(t)) mask |= 1u << m;
+                if (is_physical(t)) mask |= 1u << k;
                 a = 0.5 * a;
             }
             atomicAnd(I.mask, mask);
@@ -1370,8 +1411,7 @@ static cudaError_t im_fluxes(const LoParams& P, const LoBuffers& B, cudaStream_t
 cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q) {
     const int rows = P.ny / Q.nslab, ncs = rows * P.nx;
     const int pr_bytes = pr_smem_words(rows, P.nx) * (int)sizeof(double);
-    const int pr_static = 8 * (4 * 32 + 1) * (int)sizeof(double);   // k_im_pr2_sweep's face-term array
-    if (ncs > kMaxSlabCells || pr_bytes + pr_static > 227 * 1024) return cudaErrorInvalidValue;
+    if (ncs > kMaxSlabCells || pr_bytes > 227 * 1024) return cudaErrorInvalidValue;
     cudaError_t e = cudaFuncSetAttribute(k_im_pr2_sweep, cudaFuncAttributeMaxDynamicSharedMemorySize, pr_bytes);
     if (e == cudaSuccess)
         e = cudaFuncSetAttribute(k_im_lusgs<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, ncs * 64 * (int)sizeof(double));

@@ -282,6 +282,200 @@ __device__ __forceinline__ void lo_face_interior(const LoParams& P, const LoBuff
 }
 
 // -------------------------------------------------------------------------------------------
+// Interior face, one warp per face (nvel <= 1024): the arithmetic of lo_face_interior, with every
+// velocity sum a per-lane sum over k = lane, lane + 32, ... followed by a warp butterfly whose totals
+// every lane holds.  The face's scalar chain (GetPrimary, MicroSlope x4, CalcMoment, GetTau, Mt) then
+// runs on every lane alike, so the face needs no barrier; H0 of the lane's velocities waits in the
+// warp's slice of shared memory (sH, 1024 doubles) between the passes that use it.
+__device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const LoBuffers& B, int dir, int cL, int cR,
+                                                      double dt, double* __restrict__ Fh, double* __restrict__ Fb,
+                                                      double* Fw, double* sH) {
+    const int nv = P.nvel, lane = threadIdx.x & 31, nr = (nv + 31) >> 5;
+    const double len = dir == 0 ? P.dx : P.dy, flen = dir == 0 ? P.dy : P.dx, hl = 0.5 * len;
+    const double* sN_h = dir == 0 ? B.sxh : B.syh;
+    const double* sN_b = dir == 0 ? B.sxb : B.syb;
+    const double* sT_h = dir == 0 ? B.syh : B.sxh;
+    const double* sT_b = dir == 0 ? B.syb : B.sxb;
+    const double tsg = dir == 0 ? 1.0 : -1.0;
+    double acc[14];
+#pragma unroll
+    for (int m = 0; m < 8; ++m) acc[m] = 0.0;
+#pragma unroll 4
+    for (int r = 0; r < nr; ++r) {
+        const int k = lane + 32 * r;
+        const bool kok = k < nv;
+        const int kk = kok ? k : nv - 1;
+        const double uk = B.u[kk], vk = B.v[kk], wk = kok ? B.w[kk] : 0.0;
+        const double vn = dir == 0 ? uk : vk, vt = dir == 0 ? vk : -uk;
+        const bool left = copysign(1.0, vn) > 0.0;
+        const size_t q = (size_t)(left ? cL : cR) * nv + kk;
+        const double sg = left ? hl : -hl;
+        const double hv = B.h[q] + sg * sN_h[q], bv = B.b[q] + sg * sN_b[q];
+        const double sht = tsg * sT_h[q], sbt = tsg * sT_b[q];
+        const double v2 = vn * vn + vt * vt;
+        acc[0] += wk * hv;
+        acc[1] += wk * vn * hv;
+        acc[2] += wk * vt * hv;
+        acc[3] += 0.5 * wk * (v2 * hv + bv);
+        acc[4] += wk * sht;
+        acc[5] += wk * vn * sht;
+        acc[6] += wk * vt * sht;
+        acc[7] += 0.5 * wk * (v2 * sht + sbt);
+    }
+    warp_sum_all<8>(acc);
+    // the face's scalar chain, on every lane
+    Prim pf;
+    const double cv[4] = {acc[0], acc[1], acc[2], acc[3]};
+    const bool ok = get_primary(P.gm1, cv, pf);
+    if (!ok) { pf.r = 1.0; pf.U = 0.0; pf.V = 0.0; pf.L = 1.0; }
+    double aL[4], aR[4], bs[4], aT[4], Mt[5];
+    for (int piece = 0; piece < 2; ++piece) {   // aL from (W_face - W_L) / (dx/2), aR from (W_R - W_face) / (dx/2)
+        const double* Wc = B.W + (piece == 0 ? cL : cR) * 4;
+        double wc[4], sw[4];
+        wc[0] = Wc[0]; wc[3] = Wc[3];
+        if (dir == 0) { wc[1] = Wc[1]; wc[2] = Wc[2]; }
+        else { wc[1] = Wc[2]; wc[2] = -Wc[1]; }
+#pragma unroll
+        for (int m = 0; m < 4; ++m) sw[m] = piece == 0 ? (cv[m] - wc[m]) / hl : (wc[m] - cv[m]) / hl;
+        micro_slope(P.ck, pf, sw, piece == 0 ? aL : aR);
+    }
+    {
+        const double swt[4] = {acc[4], acc[5], acc[6], acc[7]};
+        micro_slope(P.ck, pf, swt, bs);
+    }
+    Moments M;
+    calc_moment(P.ck, pf, M);
+    double tau = 1.0;
+    const bool tok = get_tau(P.mu_ref, P.omega, pf, tau);
+    if (!tok) tau = 1.0;
+    time_coeffs(dt, tau, Mt);
+    if (lane == 0) {
+        if (!ok) set_status(B.status, ST_GETPRIMARY);
+        if (ok && !tok) set_status(B.status, ST_TAU);
+    }
+    {
+        double o0[4], o1[4], o2[4], sw[4];
+        moment_auvxi(aL, M.MuL, M.Mv, M.Mxi, 1, 0, o0);
+        moment_auvxi(aR, M.MuR, M.Mv, M.Mxi, 1, 0, o1);
+        moment_auvxi(bs, M.Mu, M.Mv, M.Mxi, 0, 1, o2);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) sw[m] = -pf.r * (o0[m] + o1[m] + o2[m]);
+        micro_slope(P.ck, pf, sw, aT);
+    }
+    const double mxi2 = M.Mxi[2];
+    // face equilibrium H0 (PrepareNativeFaceEquilibrium, mod_Evolution.f90:16-30) + heat flux
+    const double pref = pf.r * (pf.L / kPi), bfac = (double)P.ck / (2.0 * pf.L);
+#pragma unroll
+    for (int m = 0; m < 4; ++m) acc[m] = 0.0;
+#pragma unroll 4
+    for (int r = 0; r < nr; ++r) {
+        const int k = lane + 32 * r;
+        const bool kok = k < nv;
+        const int kk = kok ? k : nv - 1;
+        const double uk = B.u[kk], vk = B.v[kk], wk = kok ? B.w[kk] : 0.0;
+        const double vn = dir == 0 ? uk : vk, vt = dir == 0 ? vk : -uk;
+        const bool left = copysign(1.0, vn) > 0.0;
+        const size_t q = (size_t)(left ? cL : cR) * nv + kk;
+        const double sg = left ? hl : -hl;
+        const double hv = B.h[q] + sg * sN_h[q], bv = B.b[q] + sg * sN_b[q];
+        const double dvn = vn - pf.U, dvt = vt - pf.V, v2 = dvn * dvn + dvt * dvt;
+        const double H0 = pref * exp(-pf.L * v2);
+        sH[r * 32 + lane] = H0;
+        const double t = 0.5 * wk * (v2 * hv + bv);
+        acc[0] += t * dvn;
+        acc[1] += t * dvt;
+        acc[2] = fmax(acc[2], kok ? fabs(H0) : 0.0);
+        acc[3] = fmax(acc[3], kok ? fabs(H0 * bfac) : 0.0);
+    }
+    warp_sum_all<2>(acc);
+    warp_max_all<2>(acc + 2);
+    const double qf0 = acc[0], qf1 = acc[1];
+    const double sch = fmax(acc[2], 1.0), scb = fmax(acc[3], 1.0);
+    // ProjectToConservedMoments of (H0, B0) onto GetConserved(pf), local frame (mod_ImplicitCommon.f90:42-82)
+#pragma unroll
+    for (int m = 0; m < 14; ++m) acc[m] = 0.0;
+#pragma unroll 4
+    for (int r = 0; r < nr; ++r) {
+        const int k = lane + 32 * r;
+        const bool kok = k < nv;
+        const int kk = kok ? k : nv - 1;
+        const double uk = B.u[kk], vk = B.v[kk], wk = kok ? B.w[kk] : 0.0;
+        const double vn = dir == 0 ? uk : vk, vt = dir == 0 ? vk : -uk;
+        const double H0 = sH[r * 32 + lane], b0 = H0 * bfac;
+        moment_add(wk, vn, vt, H0, b0, acc);
+        gram_add(wk, fmax(fabs(H0), kEps * sch), fmax(fabs(b0), kEps * scb), vn, vt, acc + 4);
+    }
+    warp_sum_all<14>(acc);
+    double tgt[4], lam[4];
+    get_conserved(P.gm1, pf, tgt);
+    {
+        double rhs[4], gm[16];
+#pragma unroll
+        for (int m = 0; m < 4; ++m) rhs[m] = tgt[m] - acc[m];
+        gram_expand(acc + 4, gm);
+        if (!solve_dense4(gm, rhs, lam)) {
+            lam[0] = lam[1] = lam[2] = lam[3] = 0.0;
+            if (lane == 0) set_status(B.status, ST_FACE_PROJECTION);
+        }
+    }
+    // Shakhov part and the micro flux (mod_Evolution.f90:396-453), times the face length
+    const double coeff = 0.8 * (1.0 - P.pr) * pf.L * pf.L / pf.r;
+    const double c2ck = 2.0 / (double)P.ck;
+#pragma unroll
+    for (int m = 0; m < 8; ++m) acc[m] = 0.0;
+#pragma unroll 2
+    for (int r = 0; r < nr; ++r) {
+        const int k = lane + 32 * r;
+        const bool kok = k < nv;
+        const int kk = kok ? k : nv - 1;
+        const double uk = B.u[kk], vk = B.v[kk], wk = kok ? B.w[kk] : 0.0;
+        const double a = dir == 0 ? uk : vk, t = dir == 0 ? vk : -uk;
+        const double H0 = sH[r * 32 + lane], b0 = H0 * bfac;
+        const double e = 0.5 * (a * a + t * t);
+        const double H = H0 + fmax(fabs(H0), kEps * sch) * (lam[0] + a * lam[1] + t * lam[2] + e * lam[3]);
+        const double Bq = b0 + 0.5 * fmax(fabs(b0), kEps * scb) * lam[3];
+        moment_add(wk, a, t, H, Bq, acc);   // projection gate
+        const bool left = copysign(1.0, a) > 0.0;
+        const size_t q = (size_t)(left ? cL : cR) * nv + kk;
+        const double sg = left ? hl : -hl;
+        const double shn = sN_h[q], sbn = sN_b[q], sht = tsg * sT_h[q], sbt = tsg * sT_b[q];
+        const double hv = B.h[q] + sg * shn, bv = B.b[q] + sg * sbn;
+        const double dvn = a - pf.U, dvt = t - pf.V, dv2 = dvn * dvn + dvt * dvt;
+        const double qdot = dvn * qf0 + dvt * qf1;
+        const double shH = 2.0 * pf.L * dv2 - 4.0;
+        const double Hp = coeff * qdot * shH * H, Bp = coeff * qdot * (shH + c2ck) * Bq;
+        const double v2 = a * a + t * t;
+        const double slh = a * shn + t * sht, slb = a * sbn + t * sbt;
+        const double* as = left ? aL : aR;
+        const double h_a = as[0] * H + as[1] * a * H + as[2] * t * H + 0.5 * as[3] * (v2 * H + Bq);
+        const double h_b = bs[0] * H + bs[1] * a * H + bs[2] * t * H + 0.5 * bs[3] * (v2 * H + Bq);
+        const double h_T = aT[0] * H + aT[1] * a * H + aT[2] * t * H + 0.5 * aT[3] * (v2 * H + Bq);
+        const double b_a = as[0] * Bq + as[1] * a * Bq + as[2] * t * Bq + 0.5 * as[3] * (v2 * Bq + mxi2 * H);
+        const double b_b = bs[0] * Bq + bs[1] * a * Bq + bs[2] * t * Bq + 0.5 * bs[3] * (v2 * Bq + mxi2 * H);
+        const double b_T = aT[0] * Bq + aT[1] * a * Bq + aT[2] * t * Bq + 0.5 * aT[3] * (v2 * Bq + mxi2 * H);
+        const double fh = Mt[0] * a * (H + Hp) + Mt[1] * a * a * h_a + Mt[1] * a * t * h_b + Mt[2] * a * h_T +
+                          Mt[3] * a * hv - Mt[4] * a * slh;
+        const double fb = Mt[0] * a * (Bq + Bp) + Mt[1] * a * a * b_a + Mt[1] * a * t * b_b + Mt[2] * a * b_T +
+                          Mt[3] * a * bv - Mt[4] * a * slb;
+        const double Fhk = flen * fh, Fbk = flen * fb;
+        if (kok) { Fh[k] = Fhk; Fb[k] = Fbk; }
+        moment_add(wk, uk, vk, Fhk, Fbk, acc + 4);   // MomentConserved in the global frame (:470-473)
+    }
+    warp_sum_all<8>(acc);
+    if (lane == 0) {
+        const double rs = fmax(fmax(fmax(fabs(tgt[0]), fabs(tgt[1])), fmax(fabs(tgt[2]), fabs(tgt[3]))), 1.0);
+        double err = 0.0;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) err = fmax(err, fabs(acc[m] - tgt[m]));
+        if (!(err <= 1.0e-10 * rs)) set_status(B.status, ST_FACE_PROJECTION);
+        bool fin = true;
+#pragma unroll
+        for (int m = 0; m < 4; ++m) { Fw[m] = acc[4 + m]; fin = fin && isfinite(acc[4 + m]); }
+        if (!fin) set_status(B.status, ST_NONFINITE_FLUX);
+    }
+}
+
+// -------------------------------------------------------------------------------------------
 // Wall face: W2BMultiscaleFluxBoundary (mod_Evolution.f90:1888-2449) on the horizontal walls.
 // side -1: bottom wall below row 0 (Lside); +1: top wall above row ny-1 (Rside).
 template <int VPT>
@@ -506,6 +700,29 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_faces(LoParams P, LoB
     const size_t o = (size_t)(jf * nx + i);
     lo_face_interior<VPT>(P, B, 1, (jf - 1) * nx + i, jf * nx + i, dt, B.fyh + o * nv, B.fyb + o * nv, B.fyw + o * 4,
                           red, rout, sc);
+}
+
+// one warp per interior face (x faces, then the y faces between rows), NW faces per CTA; nvel <= 1024
+template <int NW>
+__global__ void __launch_bounds__(NW * 32) k_lo_faces_warp(LoParams P, LoBuffers B) {
+    if (eval_cached(B)) return;
+    __shared__ double sH[NW][1024];
+    const double dt = B.dt[0];
+    const int nx = P.nx, ny = P.ny, nv = P.nvel, w = threadIdx.x >> 5;
+    int f = blockIdx.x * NW + w;
+    if (f >= nx * ny + nx * (ny - 1)) return;
+    if (f < nx * ny) {
+        const int j = f / nx, i = f % nx;
+        const size_t o = (size_t)(j * nx + i);
+        lo_face_interior_warp(P, B, 0, j * nx + wrapx(i - 1, nx), j * nx + i, dt, B.fxh + o * nv, B.fxb + o * nv,
+                              B.fxw + o * 4, sH[w]);
+        return;
+    }
+    f -= nx * ny;
+    const int jf = 1 + f / nx, i = f % nx;
+    const size_t o = (size_t)(jf * nx + i);
+    lo_face_interior_warp(P, B, 1, (jf - 1) * nx + i, jf * nx + i, dt, B.fyh + o * nv, B.fyb + o * nv, B.fyw + o * 4,
+                          sH[w]);
 }
 
 template <int VPT, int NTMAX>
@@ -1023,7 +1240,8 @@ cudaError_t launch_lo_slopes(const LoParams& P, const LoBuffers& B, cudaStream_t
 cudaError_t launch_lo_faces(const LoParams& P, const LoBuffers& B, cudaStream_t s) {
     const int nface = P.nx * P.ny + P.nx * (P.ny - 1);
     const int nt = lo_threads(P.nvel);
-    if (lo_vpt(P.nvel) == 4) k_lo_faces<4, 256><<<nface, nt, 0, s>>>(P, B);
+    if (P.nvel <= 1024) k_lo_faces_warp<4><<<(unsigned)((nface + 3) / 4), 128, 0, s>>>(P, B);
+    else if (lo_vpt(P.nvel) == 4) k_lo_faces<4, 256><<<nface, nt, 0, s>>>(P, B);
     else k_lo_faces<5, 512><<<nface, nt, 0, s>>>(P, B);
     return cudaGetLastError();
 }

@@ -1147,7 +1147,7 @@ __global__ void __launch_bounds__(256, 2) k_adj_wall_nodes(LoParams P, LoBuffers
     auto rec = [&](int k, int field) { return S.rec[((size_t)cc * 72 + field * 12 + sidx * 3 + g) * nv + k]; };
     double acc[8];
 #pragma unroll
-    for (int m = 0; m < 6; ++m) acc[m] = 0.0;
+    for (int m = 0; m < 8; ++m) acc[m] = 0.0;
     for (int r = 0; r < nr; ++r) {
         const WVel s = wvel(B, nv, r);
         const double hin = rec(s.k, 0), bin = rec(s.k, 1), ht = rec(s.k, 3), bt = rec(s.k, 5);
@@ -1159,9 +1159,12 @@ __global__ void __launch_bounds__(256, 2) k_adj_wall_nodes(LoParams P, LoBuffers
         const double vt2 = -s.u + ux, w2 = vn * vn + vt2 * vt2;
         acc[4] += 0.5 * s.w * vn * (w2 * hin + bin);
         acc[5] += 0.5 * s.w * vt2 * (w2 * hin + bin);
+        // d/d(wall speed) of the two heat-flux moments (vt2 = -u + u_w)
+        acc[6] += s.w * vn * vt2 * hin;
+        acc[7] += 0.5 * s.w * (w2 * hin + bin) + s.w * vt2 * vt2 * hin;
     }
-    warp_sum_all<6>(acc);
-    const double hlx = acc[4], hly = acc[5];
+    warp_sum_all<8>(acc);
+    const double hlx = acc[4], hly = acc[5], dhlx_dux = acc[6], dhly_dux = acc[7];
     // the scalar chain's values and, one input per lane, its Jacobian
     const double win[kWallIn] = {wcell[0], wcell[1], wcell[2], wcell[3], ux, 1.0 / P.wall_lam[top], P.mu_ref,
                                  acc[0], acc[1], acc[2], acc[3]};
@@ -1328,7 +1331,7 @@ __global__ void __launch_bounds__(256, 2) k_adj_wall_nodes(LoParams P, LoBuffers
     if (lane == 0) {
 #pragma unroll
         for (int m = 0; m < 4; ++m) atomic_add(A.gWi + cc * 4 + m, gI[m]);
-        atomic_add(A.gpar + (top ? GP_UX1 : GP_UX0), gI[4] + a2[22] + gux_direct);
+        atomic_add(A.gpar + (top ? GP_UX1 : GP_UX0), gI[4] + a2[22] + gux_direct + a2[19] * dhlx_dux + a2[20] * dhly_dux);
         atomic_add(A.gpar + (top ? GP_TW1 : GP_TW0), gI[5]);
         atomic_add(A.gpar + GP_MU, gI[6]);
     }

@@ -414,20 +414,6 @@ __device__ __forceinline__ WVel wvel(const LoBuffers& B, int nv, int r) {
     return s;
 }
 
-template <int N>
-__device__ __forceinline__ void warp_sum_all(double* v) {
-    constexpr int sh = 5 - ilog2(pow2_ceil(N));
-    const double r = warp_halving<N, false>(v);
-#pragma unroll
-    for (int i = 0; i < N; ++i) v[i] = __shfl_sync(0xffffffffu, r, i << sh);
-}
-template <int N>
-__device__ __forceinline__ void warp_max_all(double* v) {
-    constexpr int sh = 5 - ilog2(pow2_ceil(N));
-    const double r = warp_halving<N, true>(v);
-#pragma unroll
-    for (int i = 0; i < N; ++i) v[i] = __shfl_sync(0xffffffffu, r, i << sh);
-}
 
 __device__ __forceinline__ double s2_scaled(const double r[4], const double w[4]) {
     double s = 0.0;
