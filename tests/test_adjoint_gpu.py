@@ -18,7 +18,7 @@ from ugks2d_high_order_b200.case import reference_case, velocity_table
 pytestmark = pytest.mark.gpu
 
 PARAMS = ("mu_ref", "wall_ux0", "wall_ux1", "wall_tnative0", "wall_tnative1")
-DOT_TOL = 1e-8      # <J v, u> vs <v, J^T u>, GPU adjoint against the oracle's tangent, relative
+DOT_TOL = 2e-11     # <J v, u> vs <v, J^T u>, GPU adjoint against the oracle's tangent, relative (worst seen 8e-12)
 FD_TOL = 1e-6       # gradient vs central differences (h = 1e-6 relative), relative to the gradient's norm
 EXACT_TOL = 1e-10   # gradient vs the tangent oracle's forward-mode derivative, relative to the gradient's norm
 

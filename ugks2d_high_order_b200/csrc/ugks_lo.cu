@@ -282,15 +282,44 @@ __device__ __forceinline__ void lo_face_interior(const LoParams& P, const LoBuff
 }
 
 // -------------------------------------------------------------------------------------------
-// Interior face, one warp per face (nvel <= 1024): the arithmetic of lo_face_interior, with every
-// velocity sum a per-lane sum over k = lane, lane + 32, ... followed by a warp butterfly whose totals
-// every lane holds.  The face's scalar chain (GetPrimary, MicroSlope x4, CalcMoment, GetTau, Mt) then
-// runs on every lane alike, so the face needs no barrier; H0 of the lane's velocities waits in the
-// warp's slice of shared memory (sH, 1024 doubles) between the passes that use it.
-__device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const LoBuffers& B, int dir, int cL, int cR,
-                                                      double dt, double* __restrict__ Fh, double* __restrict__ Fb,
-                                                      double* Fw, double* sH) {
-    const int nv = P.nvel, lane = threadIdx.x & 31, nr = (nv + 31) >> 5;
+// Interior face on WPF warps (nvel <= 1024): the arithmetic of lo_face_interior, with every velocity
+// sum a per-lane sum over the thread's velocities k = t, t + 32 WPF, ... (t = the thread's index in the
+// face) followed by a warp butterfly and, for WPF > 1, the sum of the WPF warp totals in warp order,
+// which every thread of the face holds.  The face's scalar chain (GetPrimary, MicroSlope x4, CalcMoment,
+// GetTau, Mt) then runs on every thread alike, so no thread waits on another's serial phase; H0 of the
+// thread's velocities waits in shared memory (sH[k]) between the passes that use it.
+
+// totals of v over the face: every thread of the face holds them.  WPF = 1: the warp butterfly; WPF > 1:
+// one face per CTA, the warps' totals exchanged through xch [WPF][32]
+template <int N, int WPF, bool MAX = false>
+__device__ __forceinline__ void face_reduce_all(double* v, double* xch) {
+    if constexpr (WPF == 1) {
+        if constexpr (MAX) warp_max_all<N>(v);
+        else warp_sum_all<N>(v);
+    } else {
+        constexpr int sh = 5 - ilog2(pow2_ceil(N));
+        const double r = warp_halving<N, MAX>(v);
+        const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+        if ((lane & ((1 << sh) - 1)) == 0 && (lane >> sh) < N) xch[w * 32 + (lane >> sh)] = r;
+        __syncthreads();
+#pragma unroll
+        for (int q = 0; q < N; ++q) {
+            double t = xch[q];
+#pragma unroll
+            for (int ww = 1; ww < WPF; ++ww) t = MAX ? fmax(t, xch[ww * 32 + q]) : t + xch[ww * 32 + q];
+            v[q] = t;
+        }
+        __syncthreads();   // xch is rewritten by the next reduction
+    }
+}
+
+template <int WPF>
+__device__ __forceinline__ void lo_face_interior_grp(const LoParams& P, const LoBuffers& B, int dir, int cL, int cR,
+                                                     double dt, double* __restrict__ Fh, double* __restrict__ Fb,
+                                                     double* Fw, double* sH, double* xch) {
+    constexpr int NT = 32 * WPF;
+    const int nv = P.nvel, lane = WPF == 1 ? (threadIdx.x & 31) : (int)threadIdx.x, nr = (nv + NT - 1) / NT;
+    const bool lead = lane == 0;
     const double len = dir == 0 ? P.dx : P.dy, flen = dir == 0 ? P.dy : P.dx, hl = 0.5 * len;
     const double* sN_h = dir == 0 ? B.sxh : B.syh;
     const double* sN_b = dir == 0 ? B.sxb : B.syb;
@@ -302,7 +331,7 @@ __device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const L
     for (int m = 0; m < 8; ++m) acc[m] = 0.0;
 #pragma unroll 4
     for (int r = 0; r < nr; ++r) {
-        const int k = lane + 32 * r;
+        const int k = lane + NT * r;
         const bool kok = k < nv;
         const int kk = kok ? k : nv - 1;
         const double uk = B.u[kk], vk = B.v[kk], wk = kok ? B.w[kk] : 0.0;
@@ -322,8 +351,8 @@ __device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const L
         acc[6] += wk * vt * sht;
         acc[7] += 0.5 * wk * (v2 * sht + sbt);
     }
-    warp_sum_all<8>(acc);
-    // the face's scalar chain, on every lane
+    face_reduce_all<8, WPF>(acc, xch);
+    // the face's scalar chain, on every thread
     Prim pf;
     const double cv[4] = {acc[0], acc[1], acc[2], acc[3]};
     const bool ok = get_primary(P.gm1, cv, pf);
@@ -349,7 +378,7 @@ __device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const L
     const bool tok = get_tau(P.mu_ref, P.omega, pf, tau);
     if (!tok) tau = 1.0;
     time_coeffs(dt, tau, Mt);
-    if (lane == 0) {
+    if (lead) {
         if (!ok) set_status(B.status, ST_GETPRIMARY);
         if (ok && !tok) set_status(B.status, ST_TAU);
     }
@@ -369,7 +398,7 @@ __device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const L
     for (int m = 0; m < 4; ++m) acc[m] = 0.0;
 #pragma unroll 4
     for (int r = 0; r < nr; ++r) {
-        const int k = lane + 32 * r;
+        const int k = lane + NT * r;
         const bool kok = k < nv;
         const int kk = kok ? k : nv - 1;
         const double uk = B.u[kk], vk = B.v[kk], wk = kok ? B.w[kk] : 0.0;
@@ -380,15 +409,15 @@ __device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const L
         const double hv = B.h[q] + sg * sN_h[q], bv = B.b[q] + sg * sN_b[q];
         const double dvn = vn - pf.U, dvt = vt - pf.V, v2 = dvn * dvn + dvt * dvt;
         const double H0 = pref * exp(-pf.L * v2);
-        sH[r * 32 + lane] = H0;
+        sH[k] = H0;
         const double t = 0.5 * wk * (v2 * hv + bv);
         acc[0] += t * dvn;
         acc[1] += t * dvt;
         acc[2] = fmax(acc[2], kok ? fabs(H0) : 0.0);
         acc[3] = fmax(acc[3], kok ? fabs(H0 * bfac) : 0.0);
     }
-    warp_sum_all<2>(acc);
-    warp_max_all<2>(acc + 2);
+    face_reduce_all<2, WPF>(acc, xch);
+    face_reduce_all<2, WPF, true>(acc + 2, xch);
     const double qf0 = acc[0], qf1 = acc[1];
     const double sch = fmax(acc[2], 1.0), scb = fmax(acc[3], 1.0);
     // ProjectToConservedMoments of (H0, B0) onto GetConserved(pf), local frame (mod_ImplicitCommon.f90:42-82)
@@ -396,16 +425,16 @@ __device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const L
     for (int m = 0; m < 14; ++m) acc[m] = 0.0;
 #pragma unroll 4
     for (int r = 0; r < nr; ++r) {
-        const int k = lane + 32 * r;
+        const int k = lane + NT * r;
         const bool kok = k < nv;
         const int kk = kok ? k : nv - 1;
         const double uk = B.u[kk], vk = B.v[kk], wk = kok ? B.w[kk] : 0.0;
         const double vn = dir == 0 ? uk : vk, vt = dir == 0 ? vk : -uk;
-        const double H0 = sH[r * 32 + lane], b0 = H0 * bfac;
+        const double H0 = sH[k], b0 = H0 * bfac;
         moment_add(wk, vn, vt, H0, b0, acc);
         gram_add(wk, fmax(fabs(H0), kEps * sch), fmax(fabs(b0), kEps * scb), vn, vt, acc + 4);
     }
-    warp_sum_all<14>(acc);
+    face_reduce_all<14, WPF>(acc, xch);
     double tgt[4], lam[4];
     get_conserved(P.gm1, pf, tgt);
     {
@@ -415,7 +444,7 @@ __device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const L
         gram_expand(acc + 4, gm);
         if (!solve_dense4(gm, rhs, lam)) {
             lam[0] = lam[1] = lam[2] = lam[3] = 0.0;
-            if (lane == 0) set_status(B.status, ST_FACE_PROJECTION);
+            if (lead) set_status(B.status, ST_FACE_PROJECTION);
         }
     }
     // Shakhov part and the micro flux (mod_Evolution.f90:396-453), times the face length
@@ -425,12 +454,12 @@ __device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const L
     for (int m = 0; m < 8; ++m) acc[m] = 0.0;
 #pragma unroll 2
     for (int r = 0; r < nr; ++r) {
-        const int k = lane + 32 * r;
+        const int k = lane + NT * r;
         const bool kok = k < nv;
         const int kk = kok ? k : nv - 1;
         const double uk = B.u[kk], vk = B.v[kk], wk = kok ? B.w[kk] : 0.0;
         const double a = dir == 0 ? uk : vk, t = dir == 0 ? vk : -uk;
-        const double H0 = sH[r * 32 + lane], b0 = H0 * bfac;
+        const double H0 = sH[k], b0 = H0 * bfac;
         const double e = 0.5 * (a * a + t * t);
         const double H = H0 + fmax(fabs(H0), kEps * sch) * (lam[0] + a * lam[1] + t * lam[2] + e * lam[3]);
         const double Bq = b0 + 0.5 * fmax(fabs(b0), kEps * scb) * lam[3];
@@ -461,8 +490,8 @@ __device__ __forceinline__ void lo_face_interior_warp(const LoParams& P, const L
         if (kok) { Fh[k] = Fhk; Fb[k] = Fbk; }
         moment_add(wk, uk, vk, Fhk, Fbk, acc + 4);   // MomentConserved in the global frame (:470-473)
     }
-    warp_sum_all<8>(acc);
-    if (lane == 0) {
+    face_reduce_all<8, WPF>(acc, xch);
+    if (lead) {
         const double rs = fmax(fmax(fmax(fabs(tgt[0]), fabs(tgt[1])), fmax(fabs(tgt[2]), fabs(tgt[3]))), 1.0);
         double err = 0.0;
 #pragma unroll
@@ -702,27 +731,30 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_lo_faces(LoParams P, LoB
                           red, rout, sc);
 }
 
-// one warp per interior face (x faces, then the y faces between rows), NW faces per CTA; nvel <= 1024
-template <int NW>
-__global__ void __launch_bounds__(NW * 32) k_lo_faces_warp(LoParams P, LoBuffers B) {
+// the interior faces (x faces, then the y faces between rows) on WPF warps each: NF faces per CTA when
+// WPF = 1, one when WPF > 1; nvel <= 1024
+template <int NF, int WPF>
+__global__ void __launch_bounds__(NF * WPF * 32) k_lo_faces_grp(LoParams P, LoBuffers B) {
+    static_assert(NF == 1 || WPF == 1, "several faces per CTA only with one warp each");
     if (eval_cached(B)) return;
-    __shared__ double sH[NW][1024];
+    __shared__ double sH[NF][1024];
+    __shared__ double xch[WPF > 1 ? WPF * 32 : 1];
     const double dt = B.dt[0];
-    const int nx = P.nx, ny = P.ny, nv = P.nvel, w = threadIdx.x >> 5;
-    int f = blockIdx.x * NW + w;
-    if (f >= nx * ny + nx * (ny - 1)) return;
+    const int nx = P.nx, ny = P.ny, nv = P.nvel, w = NF == 1 ? 0 : (int)(threadIdx.x >> 5);
+    int f = blockIdx.x * NF + w;
+    if (f >= nx * ny + nx * (ny - 1)) return;   // only when NF > 1 (no face-wide barrier then)
     if (f < nx * ny) {
         const int j = f / nx, i = f % nx;
         const size_t o = (size_t)(j * nx + i);
-        lo_face_interior_warp(P, B, 0, j * nx + wrapx(i - 1, nx), j * nx + i, dt, B.fxh + o * nv, B.fxb + o * nv,
-                              B.fxw + o * 4, sH[w]);
+        lo_face_interior_grp<WPF>(P, B, 0, j * nx + wrapx(i - 1, nx), j * nx + i, dt, B.fxh + o * nv, B.fxb + o * nv,
+                                  B.fxw + o * 4, sH[w], xch);
         return;
     }
     f -= nx * ny;
     const int jf = 1 + f / nx, i = f % nx;
     const size_t o = (size_t)(jf * nx + i);
-    lo_face_interior_warp(P, B, 1, (jf - 1) * nx + i, jf * nx + i, dt, B.fyh + o * nv, B.fyb + o * nv, B.fyw + o * 4,
-                          sH[w]);
+    lo_face_interior_grp<WPF>(P, B, 1, (jf - 1) * nx + i, jf * nx + i, dt, B.fyh + o * nv, B.fyb + o * nv,
+                              B.fyw + o * 4, sH[w], xch);
 }
 
 template <int VPT, int NTMAX>
@@ -1240,7 +1272,7 @@ cudaError_t launch_lo_slopes(const LoParams& P, const LoBuffers& B, cudaStream_t
 cudaError_t launch_lo_faces(const LoParams& P, const LoBuffers& B, cudaStream_t s) {
     const int nface = P.nx * P.ny + P.nx * (P.ny - 1);
     const int nt = lo_threads(P.nvel);
-    if (P.nvel <= 1024) k_lo_faces_warp<4><<<(unsigned)((nface + 3) / 4), 128, 0, s>>>(P, B);
+    if (P.nvel <= 1024) k_lo_faces_grp<1, 4><<<(unsigned)nface, 128, 0, s>>>(P, B);
     else if (lo_vpt(P.nvel) == 4) k_lo_faces<4, 256><<<nface, nt, 0, s>>>(P, B);
     else k_lo_faces<5, 512><<<nface, nt, 0, s>>>(P, B);
     return cudaGetLastError();
