@@ -89,8 +89,9 @@ struct ugks_ctx {
     // S2CN2 adjoint (ugks_s2cn2_forward_checkpointed / ugks_s2cn2_backward / ugks_s2cn2_step_vjp)
     double* amem = nullptr;        // checkpoints (held from the checkpointed forward to the context's end)
     double* bmem = nullptr;        // segment slots, cotangent sets, adjoint work (reserved by the backward)
+    double* rmem = nullptr;        // per-step records of one segment: the scratch each step's adjoint reads
     unsigned* aflags = nullptr;    // [0..2] halt, counter, accepted of the re-runs, [3] adjoint status
-    int adj_capacity_ckpt = 0, adj_capacity_seg = 0;
+    int adj_capacity_ckpt = 0, adj_capacity_seg = 0, adj_capacity_rec = 0;
     double* ckpt = nullptr;        // [ckpt][h | b | W | ledger]
     double* seg = nullptr;         // [slot][h | b | W | 6 targets | ledger]
     double* cot[2] = {nullptr, nullptr};   // [h | b | W | 6 targets] cotangent sets
@@ -308,6 +309,7 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->cgraph) cudaGraphExecDestroy(c->cgraph);
     if (c->amem) cudaFree(c->amem);
     if (c->bmem) cudaFree(c->bmem);
+    if (c->rmem) cudaFree(c->rmem);
     if (c->aflags) cudaFree(c->aflags);
     if (c->cmem) cudaFree(c->cmem);
     if (c->cflags) cudaFree(c->cflags);
@@ -1097,6 +1099,41 @@ SlotView ckpt_view(const ugks_ctx* c, int q) { return view_of(c, c->ckpt + (size
 SlotView seg_view(const ugks_ctx* c, int m) { return view_of(c, c->seg + (size_t)m * seg_doubles(c), true, true); }
 SlotView cot_view(const ugks_ctx* c, int i) { return view_of(c, c->cot[i], true, false); }
 
+// A step's record: what its adjoint reads of the step's evaluation and update -- the face cache, the
+// first layer, the face-node scalars, the wall-node macro fluxes, the stream state's volume-node states
+// and scalars, the CN right-hand side and the stream state.  The segment recompute writes step m's
+// into record m, so the reverse sweep needs no second run of the step.
+size_t record_doubles(const ugks_ctx* c) {
+    const size_t nx = c->P.nx, ny = c->P.ny, nv = c->P.nvel, nc = nx * ny, S = nc * nv;
+    const size_t nf = nc + nx * (ny - 1), nfw = nf + 2 * nx;
+    return rnd32(nc * 72 * nv) + rnd32(nc * 22 * nv) + rnd32(nf * 3 * kS2FScal) + rnd32(nfw * 3 * 4) +
+           rnd32(nc * 9 * 4) + rnd32(nc * 9 * kS2TScal) + 2 * rnd32(S) + rnd32(nc * 4);
+}
+// T with its evaluation scratch in record m (node and mac, which the adjoint does not read, stay shared)
+S2Buffers with_record(const ugks_ctx* c, S2Buffers T, int m) {
+    const size_t nx = c->P.nx, ny = c->P.ny, nv = c->P.nvel, nc = nx * ny;
+    const size_t nf = nc + nx * (ny - 1), nfw = nf + 2 * nx;
+    double* r = c->rmem + (size_t)m * record_doubles(c);
+    T.rec = r; r += rnd32(nc * 72 * nv);
+    T.l1 = r; r += rnd32(nc * 22 * nv);
+    T.fscal = r; r += rnd32(nf * 3 * kS2FScal);
+    T.nodew = r; r += rnd32(nfw * 3 * 4);
+    T.wq = r; r += rnd32(nc * 9 * 4);
+    T.tscal = r;
+    return T;
+}
+// the step buffers (rerun_cn) with the stream state and the CN right-hand side in record m
+CnBuffers record_cn(const ugks_ctx* c, CnBuffers C, int m) {
+    const size_t nx = c->P.nx, ny = c->P.ny, nv = c->P.nvel, nc = nx * ny, S = nc * nv;
+    const size_t nf = nc + nx * (ny - 1), nfw = nf + 2 * nx;
+    double* r = c->rmem + (size_t)m * record_doubles(c) + rnd32(nc * 72 * nv) + rnd32(nc * 22 * nv) +
+                rnd32(nf * 3 * kS2FScal) + rnd32(nfw * 3 * 4) + rnd32(nc * 9 * 4) + rnd32(nc * 9 * kS2TScal);
+    C.rh = r; r += rnd32(S);
+    C.rb = r; r += rnd32(S);
+    C.ws = r;
+    return C;
+}
+
 // the state set of a slot: the context's set 0 with the slot's arrays and the re-runs' halt flag
 LoBuffers slot_lo(const ugks_ctx* c, const SlotView& v) {
     LoBuffers B = c->Bs[0];
@@ -1157,6 +1194,16 @@ cudaError_t rerun_step(ugks_ctx* c, const LoBuffers& Bin, const S2Buffers& Tin, 
     return e;
 }
 
+// the same with the step buffers C (a record's stream state and right-hand side)
+cudaError_t rerun_step_into(ugks_ctx* c, const LoBuffers& Bin, const S2Buffers& Tin, const LoBuffers& Bout,
+                            const S2Buffers& Tout, const double* ledger, const CnBuffers& C) {
+    cudaError_t e = cudaMemsetAsync(c->aflags, 0, 3 * sizeof(unsigned), c->stream);
+    if (e == cudaSuccess) e = copy_ledger(c, c->adj_ledger, ledger);
+    if (e == cudaSuccess)
+        e = enqueue_s2cn2_step(c->P, Bin, Tin, Bout, Tout, C, c->stream, c->stream2, c->ev_fork, c->ev_join, &c->launches);
+    return e;
+}
+
 // the checkpoints of a trajectory (the checkpointed forward); kept until the next reservation or the
 // context's end
 int adj_reserve_ckpt(ugks_ctx* c, int nckpt) {
@@ -1194,6 +1241,20 @@ int adj_reserve_bwd(ugks_ctx* c, int nseg) {
     c->A.status = c->aflags + 3;
     c->adj_capacity_seg = nseg;
     return UGKS_OK;
+}
+
+// records for a segment of `len` steps, when they fit in 3/4 of the free device memory; otherwise none
+// (the reverse sweep then runs every step a second time for its scratch).  Kept with the context.
+bool adj_reserve_records(ugks_ctx* c, int len) {
+    if (c->rmem && c->adj_capacity_rec >= len) return true;
+    if (c->rmem) { cudaFree(c->rmem); c->rmem = nullptr; c->adj_capacity_rec = 0; }
+    size_t freeb = 0, totb = 0;
+    if (cudaMemGetInfo(&freeb, &totb) != cudaSuccess) { cudaGetLastError(); return false; }
+    const size_t need = (size_t)len * record_doubles(c) * sizeof(double);
+    if (need > freeb / 4 * 3) return false;
+    if (cudaMalloc(&c->rmem, need) != cudaSuccess) { cudaGetLastError(); c->rmem = nullptr; return false; }
+    c->adj_capacity_rec = len;
+    return true;
 }
 
 // cotangent sets, parameter cotangents and the seed for a new reverse sweep
@@ -1280,7 +1341,9 @@ extern "C" int ugks_s2cn2_backward(ugks_ctx* c, const double* seed, double* grad
     UGKS_CK(cudaSetDevice(c->device));
     if (int r = collect_status(c)) return r;
     const int nsteps = c->adj_nsteps, every = c->adj_every, nckpt = (nsteps + every - 1) / every;
-    if (int r = adj_reserve_bwd(c, every < nsteps ? every : nsteps)) return r;
+    const int seglen = every < nsteps ? every : nsteps;
+    if (int r = adj_reserve_bwd(c, seglen + 1)) return r;
+    const bool records = adj_reserve_records(c, seglen);
     if (int r = adj_clear(c, seed)) return r;
     const CnBuffers Cr = rerun_cn(c);
     int cur = 0;
@@ -1291,23 +1354,44 @@ extern "C" int ugks_s2cn2_backward(ugks_ctx* c, const double* seed, double* grad
         UGKS_CK(copy_ledger(c, s0.ledger, ck.ledger));
         UGKS_CK(s2_enqueue(3, c->P, slot_lo(c, s0), slot_targets(c, s0), c->stream, c->stream, nullptr, nullptr));
         c->launches += s2_enqueue_kernels(3);
-        for (int m = 0; m + 1 < len; ++m) {   // the segment's states, recomputed from its checkpoint
-            const SlotView a = seg_view(c, m), b = seg_view(c, m + 1);
-            UGKS_CK(rerun_step(c, slot_lo(c, a), slot_targets(c, a), slot_lo(c, b), slot_targets(c, b), a.ledger));
-            UGKS_CK(copy_ledger(c, b.ledger, c->adj_ledger));
-        }
-        for (int m = len - 1; m >= 0; --m) {   // reverse: re-run the step for its scratch, then its adjoint
-            const SlotView a = seg_view(c, m);
-            const LoBuffers Ba = slot_lo(c, a);
-            const S2Buffers Ta = slot_targets(c, a);
-            LoBuffers Bs1 = c->Bs[1];
-            Bs1.halt = c->aflags;
-            UGKS_CK(rerun_step(c, Ba, Ta, Bs1, c->T[1], a.ledger));
-            const bool last = q == nckpt - 1 && m == len - 1;
-            const AdjBuffers A = adj_bind(c, cur, last ? c->adj_seed : nullptr);
-            UGKS_CK(enqueue_s2cn2_adjoint(c->P, Ba, c->T[0], Ta, c->T[1], Cr, A, c->stream));
-            c->launches += kAdjStepKernels;
-            cur = 1 - cur;
+        if (records) {
+            // the segment recomputed once from its checkpoint, each step leaving its record; then the
+            // adjoints in reverse order from the records
+            for (int m = 0; m < len; ++m) {
+                const SlotView a = seg_view(c, m), b = seg_view(c, m + 1);
+                UGKS_CK(rerun_step_into(c, slot_lo(c, a), with_record(c, slot_targets(c, a), m), slot_lo(c, b),
+                                        with_record(c, slot_targets(c, b), m), a.ledger, record_cn(c, Cr, m)));
+                UGKS_CK(copy_ledger(c, b.ledger, c->adj_ledger));
+            }
+            for (int m = len - 1; m >= 0; --m) {
+                const SlotView a = seg_view(c, m), b = seg_view(c, m + 1);
+                const bool last = q == nckpt - 1 && m == len - 1;
+                const AdjBuffers A = adj_bind(c, cur, last ? c->adj_seed : nullptr);
+                const S2Buffers Sm = with_record(c, slot_targets(c, a), m);
+                UGKS_CK(enqueue_s2cn2_adjoint(c->P, slot_lo(c, a), Sm, Sm, with_record(c, slot_targets(c, b), m),
+                                              record_cn(c, Cr, m), A, c->stream));
+                c->launches += kAdjStepKernels;
+                cur = 1 - cur;
+            }
+        } else {
+            for (int m = 0; m + 1 < len; ++m) {   // the segment's states, recomputed from its checkpoint
+                const SlotView a = seg_view(c, m), b = seg_view(c, m + 1);
+                UGKS_CK(rerun_step(c, slot_lo(c, a), slot_targets(c, a), slot_lo(c, b), slot_targets(c, b), a.ledger));
+                UGKS_CK(copy_ledger(c, b.ledger, c->adj_ledger));
+            }
+            for (int m = len - 1; m >= 0; --m) {   // reverse: re-run the step for its scratch, then its adjoint
+                const SlotView a = seg_view(c, m);
+                const LoBuffers Ba = slot_lo(c, a);
+                const S2Buffers Ta = slot_targets(c, a);
+                LoBuffers Bs1 = c->Bs[1];
+                Bs1.halt = c->aflags;
+                UGKS_CK(rerun_step(c, Ba, Ta, Bs1, c->T[1], a.ledger));
+                const bool last = q == nckpt - 1 && m == len - 1;
+                const AdjBuffers A = adj_bind(c, cur, last ? c->adj_seed : nullptr);
+                UGKS_CK(enqueue_s2cn2_adjoint(c->P, Ba, c->T[0], Ta, c->T[1], Cr, A, c->stream));
+                c->launches += kAdjStepKernels;
+                cur = 1 - cur;
+            }
         }
         if (int r = adj_status(c)) return r;
     }
