@@ -92,6 +92,7 @@ struct ugks_ctx {
     double* rmem = nullptr;        // per-step records of one segment: the scratch each step's adjoint reads
     unsigned* aflags = nullptr;    // [0..2] halt, counter, accepted of the re-runs, [3] adjoint status
     int adj_capacity_ckpt = 0, adj_capacity_seg = 0, adj_capacity_rec = 0;
+    cudaEvent_t adj_ev[4] = {nullptr, nullptr, nullptr, nullptr};   // the adjoint's fork / join points
     double* ckpt = nullptr;        // [ckpt][h | b | W | ledger]
     double* seg = nullptr;         // [slot][h | b | W | 6 targets | ledger]
     double* cot[2] = {nullptr, nullptr};   // [h | b | W | 6 targets] cotangent sets
@@ -310,6 +311,7 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->amem) cudaFree(c->amem);
     if (c->bmem) cudaFree(c->bmem);
     if (c->rmem) cudaFree(c->rmem);
+    for (int q = 0; q < 4; ++q) if (c->adj_ev[q]) cudaEventDestroy(c->adj_ev[q]);
     if (c->aflags) cudaFree(c->aflags);
     if (c->cmem) cudaFree(c->cmem);
     if (c->cflags) cudaFree(c->cflags);
@@ -1217,6 +1219,8 @@ int adj_reserve_ckpt(ugks_ctx* c, int nckpt) {
 
 // the reverse sweep's work: nseg segment slots, the two cotangent sets and the adjoint's arrays
 int adj_reserve_bwd(ugks_ctx* c, int nseg) {
+    for (int q = 0; q < 4; ++q)
+        if (!c->adj_ev[q]) UGKS_CK(cudaEventCreateWithFlags(&c->adj_ev[q], cudaEventDisableTiming));
     if (!c->aflags) {
         UGKS_CK(cudaMalloc(&c->aflags, 4 * sizeof(unsigned)));
         UGKS_CK(cudaMemsetAsync(c->aflags, 0, 4 * sizeof(unsigned), c->stream));
@@ -1369,7 +1373,7 @@ extern "C" int ugks_s2cn2_backward(ugks_ctx* c, const double* seed, double* grad
                 const AdjBuffers A = adj_bind(c, cur, last ? c->adj_seed : nullptr);
                 const S2Buffers Sm = with_record(c, slot_targets(c, a), m);
                 UGKS_CK(enqueue_s2cn2_adjoint(c->P, slot_lo(c, a), Sm, Sm, with_record(c, slot_targets(c, b), m),
-                                              record_cn(c, Cr, m), A, c->stream));
+                                              record_cn(c, Cr, m), A, c->stream, c->stream2, c->adj_ev));
                 c->launches += kAdjStepKernels;
                 cur = 1 - cur;
             }
@@ -1388,7 +1392,7 @@ extern "C" int ugks_s2cn2_backward(ugks_ctx* c, const double* seed, double* grad
                 UGKS_CK(rerun_step(c, Ba, Ta, Bs1, c->T[1], a.ledger));
                 const bool last = q == nckpt - 1 && m == len - 1;
                 const AdjBuffers A = adj_bind(c, cur, last ? c->adj_seed : nullptr);
-                UGKS_CK(enqueue_s2cn2_adjoint(c->P, Ba, c->T[0], Ta, c->T[1], Cr, A, c->stream));
+                UGKS_CK(enqueue_s2cn2_adjoint(c->P, Ba, c->T[0], Ta, c->T[1], Cr, A, c->stream, c->stream2, c->adj_ev));
                 c->launches += kAdjStepKernels;
                 cur = 1 - cur;
             }
@@ -1428,7 +1432,7 @@ extern "C" int ugks_s2cn2_step_vjp(ugks_ctx* c, const double* gh, const double* 
     Bs1.halt = c->aflags;
     UGKS_CK(rerun_step(c, B0, c->T[0], Bs1, c->T[1], c->C.ledger));
     const AdjBuffers A = adj_bind(c, 0, c->adj_seed);
-    UGKS_CK(enqueue_s2cn2_adjoint(c->P, B0, c->T[0], c->T[0], c->T[1], rerun_cn(c), A, c->stream));
+    UGKS_CK(enqueue_s2cn2_adjoint(c->P, B0, c->T[0], c->T[0], c->T[1], rerun_cn(c), A, c->stream, c->stream2, c->adj_ev));
     UGKS_CK(s2_enqueue(3, c->P, B0, c->T[1], c->stream, c->stream, nullptr, nullptr));   // W's targets, for their adjoint
     UGKS_CK(enqueue_targets_adjoint(c->P, B0, c->T[0], in.T, in.W, A, c->stream));
     c->launches += kAdjStepKernels + s2_enqueue_kernels(3) + 2;

@@ -1272,7 +1272,7 @@ cudaError_t launch_lo_slopes(const LoParams& P, const LoBuffers& B, cudaStream_t
 cudaError_t launch_lo_faces(const LoParams& P, const LoBuffers& B, cudaStream_t s) {
     const int nface = P.nx * P.ny + P.nx * (P.ny - 1);
     const int nt = lo_threads(P.nvel);
-    if (P.nvel <= 1024) k_lo_faces_grp<1, 4><<<(unsigned)nface, 128, 0, s>>>(P, B);
+    if (P.nvel <= 1024) k_lo_faces_grp<4, 1><<<(unsigned)((nface + 3) / 4), 128, 0, s>>>(P, B);
     else if (lo_vpt(P.nvel) == 4) k_lo_faces<4, 256><<<nface, nt, 0, s>>>(P, B);
     else k_lo_faces<5, 512><<<nface, nt, 0, s>>>(P, B);
     return cudaGetLastError();

@@ -202,58 +202,46 @@ __device__ __forceinline__ void heat_shift_adj(double w, double cx, double cy, d
 }
 
 // ---------------------------------------------------------------------------------------------
-// WENO-AO(5,3) weights: the transpose of fw(q) (weno_coefficients, mod_S2D1Reconstruction.f90:168-204)
-__device__ void weno_weights_vjp(const double q[5], const double gfw[4], double gq[5]) {
-    const double q1 = q[0], q2 = q[1], q3 = q[2], q4 = q[3], q5 = q[4];
+// WENO-AO(5,3) weights: the transpose of fw(q) (weno_coefficients, mod_S2D1Reconstruction.f90:168-204),
+// from the forward's intermediates x (s2_weno_x): only products, the forward holds the reciprocals.
+//   fw_3 = alpha_3 isa / 0.85, fw_c = alpha_c isa - gam_c fw_3 (c < 3), isa = 1 / sum(alpha),
+//   alpha_c = gam_c (1 + r_c^2), r_c = tau inv_c, inv_c = 1 / (beta_c + 1e-8), tau = mean |beta_3 - beta_c|
+__device__ void weno_weights_vjp(const S2Weno& w, const S2WenoX& x, const double gfw[4], double gq[5]) {
+    const double q1 = w.q[0], q2 = w.q[1], q3 = w.q[2], q4 = w.q[3], q5 = w.q[4];
     const double t0 = q1 - 2 * q2 + q3, u0 = q1 - 4 * q2 + 3 * q3;
     const double t1 = q2 - 2 * q3 + q4, u1 = q2 - q4;
     const double t2 = q3 - 2 * q4 + q5, u2 = 3 * q3 - 4 * q4 + q5;
-    double beta[4];
-    beta[0] = 13.0 / 12.0 * (t0 * t0) + 0.25 * (u0 * u0);
-    beta[1] = 13.0 / 12.0 * (t1 * t1) + 0.25 * (u1 * u1);
-    beta[2] = 13.0 / 12.0 * (t2 * t2) + 0.25 * (u2 * u2);
-    double s = 231153 * (q3 * q3) + 104963 * (q2 * q2) + 6908 * (q1 * q1) - 38947 * q1 * q4 + 104963 * (q4 * q4) +
-               q2 * (-(51001 * q1) + 179098 * q4 - 38947 * q5) - 3 * q3 * (99692 * q2 - 22641 * q1 + 99692 * q4 - 22641 * q5) +
-               8209 * q1 * q5 - 51001 * q4 * q5 + 6908 * (q5 * q5);
-    beta[3] = s / 5040.0;
-    const double tau = (fabs(beta[3] - beta[0]) + fabs(beta[3] - beta[1]) + fabs(beta[3] - beta[2])) / 3.0;
     const double gam[4] = {0.01125, 0.1275, 0.01125, 0.85};
-    double d[4], r[4], alpha[4], sa = 0.0;
+    double alpha[4];
 #pragma unroll
-    for (int c = 0; c < 4; ++c) {
-        d[c] = beta[c] + 1.0e-8;
-        r[c] = tau / d[c];
-        alpha[c] = gam[c] * (1.0 + r[c] * r[c]);
-        sa += alpha[c];
-    }
-    // fw_c = alpha_c / sa - gam_c fw_3 (c < 3), fw_3 = alpha_3 / (0.85 sa)
+    for (int c = 0; c < 4; ++c) alpha[c] = gam[c] * (1.0 + x.r[c] * x.r[c]);
     const double g3 = gfw[3] - (gam[0] * gfw[0] + gam[1] * gfw[1] + gam[2] * gfw[2]);
-    const double common = (gfw[0] * alpha[0] + gfw[1] * alpha[1] + gfw[2] * alpha[2] + g3 * alpha[3] / 0.85) / (sa * sa);
+    const double g3s = g3 * (1.0 / 0.85);
+    const double common = (gfw[0] * alpha[0] + gfw[1] * alpha[1] + gfw[2] * alpha[2] + g3s * alpha[3]) * (x.isa * x.isa);
     double ga[4];
-    ga[0] = gfw[0] / sa - common;
-    ga[1] = gfw[1] / sa - common;
-    ga[2] = gfw[2] / sa - common;
-    ga[3] = g3 / (0.85 * sa) - common;
+    ga[0] = gfw[0] * x.isa - common;
+    ga[1] = gfw[1] * x.isa - common;
+    ga[2] = gfw[2] * x.isa - common;
+    ga[3] = g3s * x.isa - common;
     double gtau = 0.0, gb[4];
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
-        const double gr = ga[c] * gam[c] * 2.0 * r[c];
-        gtau += gr / d[c];
-        gb[c] = -gr * tau / (d[c] * d[c]);
+        const double gr = ga[c] * gam[c] * 2.0 * x.r[c];
+        gtau += gr * x.inv[c];
+        gb[c] = -gr * x.r[c] * x.inv[c];
     }
     // tau = mean |beta_3 - beta_c|
 #pragma unroll
     for (int c = 0; c < 3; ++c) {
-        const double x = beta[3] - beta[c];
-        const double sg = x > 0.0 ? 1.0 : (x < 0.0 ? -1.0 : 0.0);
-        gb[3] += gtau / 3.0 * sg;
-        gb[c] -= gtau / 3.0 * sg;
+        const double gt = gtau * (1.0 / 3.0) * x.sg[c];
+        gb[3] += gt;
+        gb[c] -= gt;
     }
     // beta_c(q)
     const double a0 = 13.0 / 6.0 * t0 * gb[0], b0 = 0.5 * u0 * gb[0];
     const double a1 = 13.0 / 6.0 * t1 * gb[1], b1 = 0.5 * u1 * gb[1];
     const double a2 = 13.0 / 6.0 * t2 * gb[2], b2 = 0.5 * u2 * gb[2];
-    const double g5 = gb[3] / 5040.0;
+    const double g5 = gb[3] * (1.0 / 5040.0);
     gq[0] += a0 + b0 + g5 * (13816.0 * q1 - 38947.0 * q4 - 51001.0 * q2 + 67923.0 * q3 + 8209.0 * q5);
     gq[1] += -2.0 * a0 - 4.0 * b0 + a1 + b1 +
              g5 * (209926.0 * q2 - 51001.0 * q1 + 179098.0 * q4 - 38947.0 * q5 - 299076.0 * q3);
@@ -270,38 +258,58 @@ __device__ __forceinline__ void cand_vjp(const double fw[4], const double v[5], 
 #pragma unroll
     for (int c = 0; c < 4; ++c) {
         double cand = 0.0;
+        const double gf = g * fw[c];
 #pragma unroll
         for (int k = (c < 3 ? c : 0); k <= (c < 3 ? c + 2 : 4); ++k) {
             cand = cand + T[c][k] * v[k];
-            gv[k] += g * fw[c] * T[c][k];
+            gv[k] += gf * T[c][k];
         }
         gfw[c] += g * cand;
     }
 }
 
-// transpose of the values (and derivatives) of the WENO-AO interpolant of q at points pts[i]:
+// transpose of the values (and derivatives) of the WENO-AO interpolant (w, x of s2_weno_x) at points pts[i]:
 // gval[i], gder[i] the cotangents of the value and the xi-derivative at pts[i]; gq accumulates
 template <int NP>
-__device__ __forceinline__ void weno_points_vjp(const double q[5], const int pts[NP], const double gval[NP],
-                                                const double gder[NP], double gq[5]) {
-    S2Weno w;
-    s2_weno(q, w);
+__device__ __forceinline__ void weno_points_vjp(const S2Weno& w, const S2WenoX& x, const int pts[NP],
+                                                const double gval[NP], const double gder[NP], double gq[5]) {
     double gfw[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int i = 0; i < NP; ++i) {
         if (gval[i] != 0.0) cand_vjp(w.fw, w.q, c_s2p.E[pts[i]], gval[i], gq, gfw);
         if (gder[i] != 0.0) cand_vjp(w.fw, w.q, c_s2p.D[pts[i]], gder[i], gq, gfw);
     }
-    weno_weights_vjp(q, gfw, gq);
+    weno_weights_vjp(w, x, gfw, gq);
+}
+// the same from the stencil alone (the weights recomputed)
+template <int NP>
+__device__ __forceinline__ void weno_points_vjp(const double q[5], const int pts[NP], const double gval[NP],
+                                                const double gder[NP], double gq[5]) {
+    S2Weno w;
+    S2WenoX x;
+    s2_weno_x<true>(q, w, &x);
+    weno_points_vjp<NP>(w, x, pts, gval, gder, gq);
+}
+
+// s2_companion3 with the weights' intermediates kept for companion3_vjp (the same values bit for bit)
+__device__ __forceinline__ bool companion3_fwd(const double q[5], const double comp[5], double val[3], double der[3],
+                                               double cval[3], S2Weno& w, S2WenoX& x) {
+    if (!s2_weno_x<true>(q, w, &x)) return false;
+    bool ok = true;
+#pragma unroll
+    for (int s = 0; s < 3; ++s) {
+        s2_at(w, S2_G0 + s, val[s], der[s]);
+        cval[s] = s2_cand_sum(w.fw, comp, c_s2p.E[S2_G0 + s]);
+        ok = ok && isfinite(val[s]) && isfinite(der[s]) && isfinite(cval[s]);
+    }
+    return ok;
 }
 
 // transpose of companion_eval3 (s2_companion3): val[s], der[s] of the interpolant of q and cval[s] of the
 // companion samples with q's weights, at the 3 Gauss nodes
-__device__ __forceinline__ void companion3_vjp(const double q[5], const double comp[5], const double gval[3],
-                                               const double gder[3], const double gcval[3], double gq[5],
-                                               double gcomp[5]) {
-    S2Weno w;
-    s2_weno(q, w);
+__device__ __forceinline__ void companion3_vjp(const S2Weno& w, const S2WenoX& x, const double comp[5],
+                                               const double gval[3], const double gder[3], const double gcval[3],
+                                               double gq[5], double gcomp[5]) {
     double gfw[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
     for (int s = 0; s < 3; ++s) {
@@ -309,7 +317,15 @@ __device__ __forceinline__ void companion3_vjp(const double q[5], const double c
         cand_vjp(w.fw, w.q, c_s2p.D[S2_G0 + s], gder[s], gq, gfw);
         cand_vjp(w.fw, comp, c_s2p.E[S2_G0 + s], gcval[s], gcomp, gfw);
     }
-    weno_weights_vjp(q, gfw, gq);
+    weno_weights_vjp(w, x, gfw, gq);
+}
+__device__ __forceinline__ void companion3_vjp(const double q[5], const double comp[5], const double gval[3],
+                                               const double gder[3], const double gcval[3], double gq[5],
+                                               double gcomp[5]) {
+    S2Weno w;
+    S2WenoX x;
+    s2_weno_x<true>(q, w, &x);
+    companion3_vjp(w, x, comp, gval, gder, gcval, gq, gcomp);
 }
 
 // transpose of s2_wall_eval (the one-sided quartic of the wall rows): cotangents of its value and
@@ -1452,10 +1468,12 @@ __global__ void __launch_bounds__(256, 2) k_adj_recon2(LoParams P, LoBuffers B, 
     const S2Field F{(f == 0 ? B.h : B.b) + k, nv, nx, ny};
     // forward: the unlimited face samples and (parts 0..2) the volume Gauss row
     double face[3], dn[3], dt[3], vol[3] = {0.0, 0.0, 0.0}, a5[5], b5[5], c5[5];
+    S2Weno wf;    // the face template's weights and their intermediates, for its transpose
+    S2WenoX xf;
     if (p < 2) {
 #pragma unroll
         for (int r = 0; r < 5; ++r) { a5[r] = X(r, 2 * p); b5[r] = X(r, 2 * p + 1); }
-        if (!nw) s2_companion3(a5, b5, face, dt, dn);
+        if (!nw) companion3_fwd(a5, b5, face, dt, dn, wf, xf);
         else {
             double dummy;
 #pragma unroll
@@ -1482,7 +1500,7 @@ __global__ void __launch_bounds__(256, 2) k_adj_recon2(LoParams P, LoBuffers B, 
                 s2_wall_eval(q, j, ny, s == 0 ? -0.5 : 0.5, a5[r + 2], b5[r + 2]);
             }
         }
-        s2_companion3(a5, b5, face, dt, dn);
+        companion3_fwd(a5, b5, face, dt, dn, wf, xf);
     }
     if (p < 3) {
 #pragma unroll
@@ -1552,7 +1570,7 @@ __global__ void __launch_bounds__(256, 2) k_adj_recon2(LoParams P, LoBuffers B, 
     atomic_add(gS + (size_t)cc * nv, gmf);
     double ga5[5] = {0.0, 0.0, 0.0, 0.0, 0.0}, gb5[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
     if (p < 2) {
-        if (!nw) companion3_vjp(a5, b5, gface, gdt, gdn, ga5, gb5);
+        if (!nw) companion3_vjp(wf, xf, b5, gface, gdt, gdn, ga5, gb5);
         else
 #pragma unroll
             for (int a = 0; a < 3; ++a) {
@@ -1563,7 +1581,7 @@ __global__ void __launch_bounds__(256, 2) k_adj_recon2(LoParams P, LoBuffers B, 
         for (int r = 0; r < 5; ++r) { atomic_add(gX(r, 2 * p), ga5[r]); atomic_add(gX(r, 2 * p + 1), gb5[r]); }
     } else {
         const int s = p - 2;
-        companion3_vjp(a5, b5, gface, gdt, gdn, ga5, gb5);
+        companion3_vjp(wf, xf, b5, gface, gdt, gdn, ga5, gb5);
         if (!nw) {
 #pragma unroll
             for (int r = 0; r < 5; ++r) {
@@ -1662,26 +1680,53 @@ cudaError_t prepare_s2_adjoint() { return s2_upload_tables(); }
 
 template <int VPT>
 static cudaError_t adj_launch(const LoParams& P, const LoBuffers& B, const S2Buffers& S, const S2Buffers& T,
-                              const S2Buffers& To, const CnBuffers& C, const AdjBuffers& A, cudaStream_t s) {
+                              const S2Buffers& To, const CnBuffers& C, const AdjBuffers& A, cudaStream_t s,
+                              cudaStream_t s2, const cudaEvent_t* ev) {
     const int nx = P.nx, ny = P.ny, nv = P.nvel, nc = nx * ny, nf = nx * ny + nx * (ny - 1);
     auto warps = [](long long n, int nt) { return (unsigned)((n * 32 + nt - 1) / nt); };
+    const bool side = s2 != nullptr && ev != nullptr;
+    const cudaStream_t sw = side ? s2 : s;
+    cudaError_t e = cudaSuccess;
     k_adj_collide<VPT, 256><<<nc, 256, 0, s>>>(P, B, To, C, A);
     k_adj_targets<<<warps((long long)nc * 9, 256), 256, 0, s>>>(P, B, S, A, A.gTo[0], A.gTo[1], A.gTo[2], A.gTo[3],
                                                                 A.gTo[4], A.gTo[5]);
     k_adj_macro_cells<<<(unsigned)((nc * 4 + 255) / 256), 256, 0, s>>>(P, C.ws, A.gwq, A.gws);
     k_adj_stream<VPT, 256><<<nc, 256, 0, s>>>(P, B, T, A);
-    k_adj_face_nodes<<<warps((long long)nf * 3, 128), 128, 0, s>>>(P, B, S, A);
-    k_adj_wall_nodes<<<warps(2LL * nx * 3, 256), 256, 0, s>>>(P, B, S, A);
-    k_adj_macro_faces<<<(unsigned)((nf * 8 + 255) / 256), 256, 0, s>>>(P, B.W, A.gmac, A.gWi);
-    const dim3 grid((unsigned)((nv + 31) / 32), (unsigned)nc);
-    k_adj_recon2<<<grid, 256, 0, s>>>(P, B, S, A);
-    k_adj_recon1<<<grid, 128, 0, s>>>(P, B, A);
+    // the wall nodes (2 nx x 3 warps) beside the interior face nodes: they write disjoint sides of the face
+    // cache and add to gWi and the parameters atomically; the macro slopes' transpose beside recon2
+    if (side) {
+        e = cudaEventRecord(ev[0], s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, ev[0], 0);
+    }
+    if (e == cudaSuccess) {
+        k_adj_wall_nodes<<<warps(2LL * nx * 3, 256), 256, 0, sw>>>(P, B, S, A);
+        if (side) e = cudaEventRecord(ev[1], s2);
+    }
+    if (e == cudaSuccess) {
+        k_adj_face_nodes<<<warps((long long)nf * 3, 128), 128, 0, s>>>(P, B, S, A);
+        if (side) e = cudaEventRecord(ev[2], s);
+    }
+    if (e == cudaSuccess && side) e = cudaStreamWaitEvent(s2, ev[2], 0);
+    if (e == cudaSuccess) {
+        k_adj_macro_faces<<<(unsigned)((nf * 8 + 255) / 256), 256, 0, sw>>>(P, B.W, A.gmac, A.gWi);
+        if (side) e = cudaEventRecord(ev[3], s2);
+    }
+    if (e == cudaSuccess && side) e = cudaStreamWaitEvent(s, ev[1], 0);   // recon2 reads the wall sides
+    if (e == cudaSuccess) {
+        const dim3 grid((unsigned)((nv + 31) / 32), (unsigned)nc);
+        k_adj_recon2<<<grid, 256, 0, s>>>(P, B, S, A);
+        k_adj_recon1<<<grid, 128, 0, s>>>(P, B, A);
+    }
+    if (e == cudaSuccess && side) e = cudaStreamWaitEvent(s, ev[3], 0);   // gWi complete before the next step
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
 cudaError_t enqueue_s2cn2_adjoint(const LoParams& P, const LoBuffers& B, const S2Buffers& S, const S2Buffers& T,
-                                  const S2Buffers& To, const CnBuffers& C, const AdjBuffers& A, cudaStream_t s) {
-    return P.nvel <= 1024 ? adj_launch<4>(P, B, S, T, To, C, A, s) : adj_launch<10>(P, B, S, T, To, C, A, s);
+                                  const S2Buffers& To, const CnBuffers& C, const AdjBuffers& A, cudaStream_t s,
+                                  cudaStream_t s2, const cudaEvent_t* ev) {
+    return P.nvel <= 1024 ? adj_launch<4>(P, B, S, T, To, C, A, s, s2, ev)
+                          : adj_launch<10>(P, B, S, T, To, C, A, s, s2, ev);
 }
 
 cudaError_t enqueue_targets_adjoint(const LoParams& P, const LoBuffers& B, const S2Buffers& S, double* const gT[6],

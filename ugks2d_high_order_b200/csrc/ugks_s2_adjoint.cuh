@@ -49,9 +49,11 @@ cudaError_t prepare_s2_adjoint();
 // The adjoint of one step whose forward re-run has just filled S (evaluation scratch), C (stream state,
 // CN right-hand side) and To (targets of the stream state, with their node scalars in S):
 // x = (B.h, B.b, B.W), T = targets of B.W.  Reads A.gho .. A.gTo, writes A.ghi .. A.gTi and adds to
-// A.gpar.  Launches on s.
+// A.gpar.  Launches on s; with s2 and ev (4 events) the wall nodes and the macro slopes' transpose run on
+// s2 beside the interior face nodes and recon2, and s has waited for s2 when the call returns.
 cudaError_t enqueue_s2cn2_adjoint(const LoParams& P, const LoBuffers& B, const S2Buffers& S, const S2Buffers& T,
-                                  const S2Buffers& To, const CnBuffers& C, const AdjBuffers& A, cudaStream_t s);
+                                  const S2Buffers& To, const CnBuffers& C, const AdjBuffers& A, cudaStream_t s,
+                                  cudaStream_t s2 = nullptr, const cudaEvent_t* ev = nullptr);
 // The targets adjoint alone: the cotangent gT of targets(W) (with W's node scalars in S, just built by
 // s2_enqueue(3)) added to gW.
 cudaError_t enqueue_targets_adjoint(const LoParams& P, const LoBuffers& B, const S2Buffers& S, double* const gT[6],

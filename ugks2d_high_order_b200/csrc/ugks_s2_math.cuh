@@ -35,8 +35,15 @@ struct S2Weno {
     double q[5];    // the stencil
 };
 
-// weno_coefficients (:168-204): the nonlinear weights of stencil q
-__device__ __forceinline__ bool s2_weno(const double q[5], S2Weno& w) {
+// intermediates of the weights that their transpose reads (the adjoint): the reciprocal denominators, the
+// ratios tau / (beta_c + eps), 1 / sum(alpha), tau and the signs of beta_3 - beta_c
+struct S2WenoX {
+    double inv[4], r[4], isa, tau, sg[3];
+};
+
+// weno_coefficients (:168-204): the nonlinear weights of stencil q; X: also their intermediates into *x
+template <bool X>
+__device__ __forceinline__ bool s2_weno_x(const double q[5], S2Weno& w, S2WenoX* x) {
     double* fw = w.fw;
 #pragma unroll
     for (int k = 0; k < 5; ++k) w.q[k] = q[k];
@@ -84,13 +91,24 @@ __device__ __forceinline__ bool s2_weno(const double q[5], S2Weno& w) {
         const double r = tau * inv[c];
         alpha[c] = gam[c] * (1.0 + r * r);
         sa = sa + alpha[c];
+        if constexpr (X) { x->inv[c] = inv[c]; x->r[c] = r; }
     }
     const double isa = 1.0 / sa;
     fw[3] = (alpha[3] * isa) * (1.0 / 0.85);
 #pragma unroll
     for (int c = 0; c < 3; ++c) fw[c] = alpha[c] * isa - fw[3] * gam[c];
+    if constexpr (X) {
+        x->isa = isa;
+        x->tau = tau;
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const double dd = beta[3] - beta[c];
+            x->sg[c] = dd > 0.0 ? 1.0 : (dd < 0.0 ? -1.0 : 0.0);
+        }
+    }
     return isfinite(fw[0]) && isfinite(fw[1]) && isfinite(fw[2]) && isfinite(fw[3]);
 }
+__device__ __forceinline__ bool s2_weno(const double q[5], S2Weno& w) { return s2_weno_x<false>(q, w, nullptr); }
 
 // sum_c fw[c] sum_k T[c][k] v[k] over each candidate's stencil samples (prepared_eval, :247-262)
 __device__ __forceinline__ double s2_cand_sum(const double fw[4], const double v[5], const double (*T)[5]) {
