@@ -63,6 +63,7 @@ BATCH_STEPS = 4               # batched steps timed (each advances all 256 insta
 ADJ_STEPS = 50                # adjoint timing: one checkpoint segment of 50 steps per case
 ADJ_EVERY = 50
 ADJ_CASES = 4                 # cases of the 64 timed (each gradient is an independent instance)
+ADJ_LONG_STEPS = 200          # and four segments of the first case: the per-step cost of a long run
 C5_STEPS = 2                  # steps timed at the adjoint config's shape (64 cases, 8x64x1024); even:
                               # one replay of the two-step graph
 # algorithmic bytes per cell*velocity of the stages (FP64 h and b):
@@ -91,6 +92,8 @@ PR2_BYTES_PER_CELL = 52 * 8
 # implicit pseudo-steps count one evaluation less than the reference runs: the device reuses the
 # accepted-state evaluation as the next pre-update one (reference: 3568 and 58725).
 FLOPS_PER_UPDATE = {"explicit": 1565.9, "implicit_steady": 2211.5, "high_order_implicit": 29736.7, "s2cn2": 29241.7}
+# S2CN2 per velocity set (oracle/count_flops.py: S2CN2_24, S2CN2 (32^2), S2CN2_48 on the 8x64 case)
+S2CN2_FLOPS_BY_TABLE = {24: 29306.5, 32: 29241.7, 48: 27542.5}
 WORKLOAD = ("ImplicitSteady 2nd-order UGKS Couette 8x64 cells, 32x32 velocities (velocity_half32_scale2), "
             "CFL 0.1, nCFL 1000, Kn 0.1, mass rescale on, cold start to the five-state gate (tol 1e-8)")
 
@@ -719,15 +722,17 @@ def main():
     barrier()
     bms = max_over_ranks(b0.elapsed_time(b1))
     bcv = sum(bcosts)                                       # all instances, all ranks
+    b_flops = sum(cv * S2CN2_FLOPS_BY_TABLE[n] for cv, (_, n) in zip(bcosts, bcases_all))
     b_value = bcv * BATCH_STEPS / (bms * 1e-3)
     batched = {"value": b_value, "unit": UNIT, "instances": len(bcases_all), "instances_this_rank": len(bcases),
                "cell_velocities_per_step": int(bcv), "scaling": "strong" if world > 1 else None,
                "steps": BATCH_STEPS, "ms_per_batched_step": bms / BATCH_STEPS, "streams": int(k_tuned),
                "all_accepted": bool((bdone == BATCH_STEPS).all() and not bst.any()),
                "vs_plain_s2cn2": b_value / (world * s2cn2["value"]),
-               "fp64": dict(fp64_fraction(FLOPS_PER_UPDATE["s2cn2"], b_value / world, fpk),
-                            note="flops per update counted on the 8x64x1024 S2CN2 case and applied to every "
-                                 "instance size"),
+               "fp64": dict(fp64_fraction(b_flops / bcv, b_value / world, fpk),
+                            note="flops per update counted per velocity set (24^2: %.0f, 32^2: %.0f, 48^2: %.0f) "
+                                 "and weighted by each instance's cell-velocities" %
+                                 (S2CN2_FLOPS_BY_TABLE[24], S2CN2_FLOPS_BY_TABLE[32], S2CN2_FLOPS_BY_TABLE[48])),
                "gpu_launches": int(bt.launch_count - blaunch0),
                "full_run_estimate_s": 2000 * bms / BATCH_STEPS * 1e-3,
                "config": "256 S2CN2 instances, seed PCG64(20261203), CFL 0.1, omega 0.5, cold start; 2 steps "
@@ -775,13 +780,42 @@ def main():
             grads.append([float(x) for x in g])
         finally:
             sv.close()
+    # a run of several segments (all but the last recomputed from their checkpoints in the backward)
+    long_fwd = long_grad = 0.0
+    if c5:
+        case, nva = c5[0]
+        sv = Solver(case, *tables[nva], device=local)
+        try:
+            st_ = torch.cuda.ExternalStream(sv.stream)
+            sv.init_freestream(tnative=2.0)
+            sv.step_s2cn2(2)
+            ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+            sv.init_freestream(tnative=2.0)
+            with torch.cuda.stream(st_):
+                ev[0].record(st_)
+                sv.step_s2cn2(ADJ_LONG_STEPS)
+                ev[1].record(st_)
+            ev[1].synchronize()
+            sv.init_freestream(tnative=2.0)
+            with torch.cuda.stream(st_):
+                ev[2].record(st_)
+                sv.s2cn2_forward_checkpointed(ADJ_LONG_STEPS, every=ADJ_EVERY)
+                sv.s2cn2_backward(seed)
+                ev[3].record(st_)
+            ev[3].synchronize()
+            long_fwd, long_grad = ev[0].elapsed_time(ev[1]), ev[2].elapsed_time(ev[3])
+        finally:
+            sv.close()
     fwd_ms, fc_ms, bw_ms = sum(fwd_list), sum(fc_list), sum(bw_list)
     barrier()
     fwd_ms, fc_ms, bw_ms = max_over_ranks(fwd_ms), max_over_ranks(fc_ms), max_over_ranks(bw_ms)
+    long_fwd, long_grad = max_over_ranks(long_fwd), max_over_ranks(long_grad)
     n_t = len(fwd_list)
+    long_cost = long_grad / long_fwd if long_fwd > 0 else None
     adjoint = {"gradients": "hand-written discrete adjoint of the S2CN2 step (ugks_s2cn2_forward_checkpointed + "
-                            "ugks_s2cn2_backward: checkpoint every %d steps, each segment recomputed, each step "
-                            "re-run for its scratch and transposed)" % ADJ_EVERY,
+                            "ugks_s2cn2_backward: checkpoint every %d steps; the backward recomputes each segment "
+                            "from its checkpoint once, every step leaving the record its transpose reads, except "
+                            "the last segment, whose states and records the forward leaves)" % ADJ_EVERY,
                "cases": len(c5_all), "cases_timed": n_t, "steps": ADJ_STEPS,
                "forward_ms_per_step": fwd_ms / (n_t * ADJ_STEPS),
                "checkpointed_forward_ms_per_step": fc_ms / (n_t * ADJ_STEPS),
@@ -789,11 +823,15 @@ def main():
                "gradient_ms_per_step": (fc_ms + bw_ms) / (n_t * ADJ_STEPS),
                "cost_vs_forward": (fc_ms + bw_ms) / fwd_ms,
                "backward_vs_forward": bw_ms / fwd_ms,
-               "full_run_estimate_s": 2000 * len(c5_all) * (fc_ms + bw_ms) / (n_t * ADJ_STEPS) * 1e-3,
+               "long_run": {"steps": ADJ_LONG_STEPS, "every": ADJ_EVERY, "forward_ms": long_fwd,
+                            "gradient_ms": long_grad, "cost_vs_forward": long_cost,
+                            "note": "the first case; all segments but the last are recomputed in the backward"},
+               "full_run_estimate_s": (2000 * len(c5_all) * long_grad / ADJ_LONG_STEPS * 1e-3) if long_fwd > 0 else None,
                "grad_first_case": grads[0] if grads else None,
                "config": "%d of the 64 cases of the batched distribution at 8x64 cells, 32x32 velocities, from the "
-                         "cold start; one checkpoint segment of %d steps each; seed = sum of the four wall "
-                         "outputs; every case runs on its own context and stream" % (n_t, ADJ_STEPS)}
+                         "cold start; one checkpoint segment of %d steps each (cost_vs_forward); seed = sum of the "
+                         "four wall outputs; every case runs on its own context and stream; long_run: %d steps of "
+                         "the first case, the config's 2000-step run estimated from it" % (n_t, ADJ_STEPS, ADJ_LONG_STEPS)}
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:

@@ -18,7 +18,9 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(HERE)
 NAMES = ("add", "mul", "div", "sqrt", "exp", "erfc", "pow", "acos")
 PLAN = {"Explicit": (1, 2), "ImplicitSteady": (2, 2), "HighOrderImplicit": (2, 2), "S2CN2": (1, 2),
-        "evaluation_lo": (2, 1), "evaluation_s2": (2, 1)}
+        "evaluation_lo": (2, 1), "evaluation_s2": (2, 1), "S2CN2_24": (1, 2), "S2CN2_48": (1, 2)}
+# S2CN2 on the batched distribution's other velocity sets (the generated 24^2 and 48^2 tables), on the
+# delivered 8 x 64 case otherwise
 # the implicit pseudo-step evaluates twice (before the update and for the accepted state); the device
 # reuses the accepted-state evaluation as the next pre-update one, so it runs one evaluation less
 EVALUATION = {"ImplicitSteady": "evaluation_lo", "HighOrderImplicit": "evaluation_s2"}
@@ -35,9 +37,14 @@ def run_one(method, flops):
         oo.LIB_PATH = os.path.join(HERE, "_build", "libugks_oracle_flops.so")
     from ugks2d_high_order_b200.case import load_velocity_half32, reference_case
     oo.set_threads(1)
-    base = {"evaluation_lo": "ImplicitSteady", "evaluation_s2": "HighOrderImplicit"}.get(method, method)
+    base = {"evaluation_lo": "ImplicitSteady", "evaluation_s2": "HighOrderImplicit", "S2CN2_24": "S2CN2",
+            "S2CN2_48": "S2CN2"}.get(method, method)
     case = reference_case(base)
-    u, v, w = load_velocity_half32()
+    if method in ("S2CN2_24", "S2CN2_48"):
+        from ugks2d_high_order_b200.case import velocity_table
+        u, v, w = velocity_table(24 if method == "S2CN2_24" else 48)
+    else:
+        u, v, w = load_velocity_half32()
     o = oo.Oracle(case, u, v, w)
     o.init_freestream()
     if base in ("ImplicitSteady", "HighOrderImplicit"):
@@ -54,7 +61,8 @@ def run_one(method, flops):
             L.uo_s2_evolution(o.ptr, dt)
             L.uo_s2_compute_residual(o.ptr, dt, 1)
 
-    step = {"Explicit": o.explicit_step, "S2CN2": o.s2cn2_step}.get(method, o.implicit_step)
+    step = {"Explicit": o.explicit_step, "S2CN2": o.s2cn2_step, "S2CN2_24": o.s2cn2_step,
+            "S2CN2_48": o.s2cn2_step}.get(method, o.implicit_step)
     warm, counted = PLAN[method]
     for _ in range(warm):
         o.implicit_step() if method.startswith("evaluation") else step()

@@ -101,6 +101,7 @@ struct ugks_ctx {
     double* adj_report = nullptr;  // [kCnReport]
     AdjBuffers A{};
     int adj_nsteps = 0, adj_every = 0;   // the trajectory the checkpoints hold (0: none)
+    int adj_last_recorded = 0;           // 1: the segment slots and records hold the trajectory's last segment
 };
 
 static int cuda_fail(cudaError_t e) {
@@ -1314,24 +1315,72 @@ int adj_download(ugks_ctx* c, const SlotView& v, double* gh, double* gb, double*
 
 }  // namespace
 
+// The trajectory's last segment, run step by step: step m reads segment slot m and writes slot m + 1
+// (the proposal) and its adjoint record m, on the accepted sequence's ledger, report and flags, with the
+// kernels and the order of ugks_s2cn2_steps (so the states are its states bit for bit).  The last
+// accepted state then goes back to set 0 with its targets.  Returns the accepted count in *done.
+int forward_recorded(ugks_ctx* c, int len, int* done) {
+    const size_t S = (size_t)c->P.nx * c->P.ny * c->P.nvel;
+    *done = 0;
+    c->cn_stage = 0;
+    if (int r = collect_status(c)) return r;
+    UGKS_CK(cudaMemsetAsync(c->cflags, 0, 3 * sizeof(unsigned), c->stream));
+    const double inject = (double)c->cn_reject_at;
+    UGKS_CK(cudaMemcpyAsync(c->C.ledger + 8, &inject, sizeof inject, cudaMemcpyHostToDevice, c->stream));
+    c->cn_reject_at = 0;
+    const SlotView s0 = seg_view(c, 0);
+    UGKS_CK(copy_state(c, s0, c->Bs[0].h, c->Bs[0].b, c->Bs[0].W));
+    const double* kept[6] = {c->T[0].mh, c->T[0].mb, c->T[0].kxh, c->T[0].kxb, c->T[0].kyh, c->T[0].kyb};
+    for (int t = 0; t < 6; ++t)
+        UGKS_CK(cudaMemcpyAsync(s0.T[t], kept[t], S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    for (int m = 0; m < len; ++m) {
+        const SlotView a = seg_view(c, m), b = seg_view(c, m + 1);
+        LoBuffers Ba = slot_lo(c, a), Bb = slot_lo(c, b);
+        Ba.halt = Bb.halt = c->C.halt;
+        UGKS_CK(enqueue_s2cn2_step(c->P, Ba, with_record(c, slot_targets(c, a), m), Bb,
+                                   with_record(c, slot_targets(c, b), m), record_cn(c, c->C, m), c->stream, c->stream2,
+                                   c->ev_fork, c->ev_join, &c->launches));
+    }
+    unsigned acc = 0;
+    UGKS_CK(cudaMemcpyAsync(&acc, c->C.accepted, sizeof acc, cudaMemcpyDeviceToHost, c->stream));
+    const int r = collect_status(c);
+    const SlotView e = seg_view(c, (int)acc);   // the last accepted state
+    UGKS_CK(cudaMemcpyAsync(c->Bs[0].h, e.h, S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    UGKS_CK(cudaMemcpyAsync(c->Bs[0].b, e.b, S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    UGKS_CK(cudaMemcpyAsync(c->Bs[0].W, e.W, (size_t)c->P.nx * c->P.ny * 4 * sizeof(double), cudaMemcpyDeviceToDevice,
+                            c->stream));
+    double* dst[6] = {c->T[0].mh, c->T[0].mb, c->T[0].kxh, c->T[0].kxb, c->T[0].kyh, c->T[0].kyb};
+    for (int t = 0; t < 6; ++t)
+        UGKS_CK(cudaMemcpyAsync(dst[t], e.T[t], S * sizeof(double), cudaMemcpyDeviceToDevice, c->stream));
+    UGKS_CK(cudaStreamSynchronize(c->stream));
+    *done = (int)acc;
+    return r;
+}
+
 extern "C" int ugks_s2cn2_forward_checkpointed(ugks_ctx* c, int nsteps, int every, double* outputs) {
     if (!c || nsteps < 1 || every < 1) return UGKS_EINVAL;
     if (!c->cmem) return UGKS_EUNSUPPORTED;
     if (!c->cn_ready) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
-    const int nckpt = (nsteps + every - 1) / every;
+    const int nckpt = (nsteps + every - 1) / every, seglen = every < nsteps ? every : nsteps;
     if (int r = adj_reserve_ckpt(c, nckpt)) return r;
     c->adj_nsteps = 0;
+    c->adj_last_recorded = 0;
+    // the last segment leaves its states and records for the reverse sweep, which then starts without
+    // recomputing it, when the records fit
+    if (int r = adj_reserve_bwd(c, seglen + 1)) return r;
+    const bool record_last = adj_reserve_records(c, seglen);
     for (int q = 0; q < nckpt; ++q) {
         const SlotView v = ckpt_view(c, q);
         UGKS_CK(copy_state(c, v, c->Bs[0].h, c->Bs[0].b, c->Bs[0].W));
         UGKS_CK(copy_ledger(c, v.ledger, c->C.ledger));
         const int n = (q + 1) * every <= nsteps ? every : nsteps - q * every;
         int done = 0;
-        const int r = ugks_s2cn2_steps(c, n, &done, nullptr);
+        const int r = record_last && q == nckpt - 1 ? forward_recorded(c, n, &done) : ugks_s2cn2_steps(c, n, &done, nullptr);
         if (r) return r;
         if (done != n) return UGKS_ENUMERIC;
     }
+    c->adj_last_recorded = record_last ? 1 : 0;
     c->adj_nsteps = nsteps;
     c->adj_every = every;
     return adj_outputs(c, outputs);
@@ -1354,14 +1403,18 @@ extern "C" int ugks_s2cn2_backward(ugks_ctx* c, const double* seed, double* grad
     for (int q = nckpt - 1; q >= 0; --q) {
         const int n0 = q * every, len = n0 + every <= nsteps ? every : nsteps - n0;
         const SlotView ck = ckpt_view(c, q), s0 = seg_view(c, 0);
-        UGKS_CK(copy_state(c, s0, ck.h, ck.b, ck.W));
-        UGKS_CK(copy_ledger(c, s0.ledger, ck.ledger));
-        UGKS_CK(s2_enqueue(3, c->P, slot_lo(c, s0), slot_targets(c, s0), c->stream, c->stream, nullptr, nullptr));
-        c->launches += s2_enqueue_kernels(3);
+        // the last segment's states and records may still be those of the forward
+        const bool held = records && q == nckpt - 1 && c->adj_last_recorded;
+        if (!held) {
+            UGKS_CK(copy_state(c, s0, ck.h, ck.b, ck.W));
+            UGKS_CK(copy_ledger(c, s0.ledger, ck.ledger));
+            UGKS_CK(s2_enqueue(3, c->P, slot_lo(c, s0), slot_targets(c, s0), c->stream, c->stream, nullptr, nullptr));
+            c->launches += s2_enqueue_kernels(3);
+        }
         if (records) {
             // the segment recomputed once from its checkpoint, each step leaving its record; then the
             // adjoints in reverse order from the records
-            for (int m = 0; m < len; ++m) {
+            for (int m = 0; m < len && !held; ++m) {
                 const SlotView a = seg_view(c, m), b = seg_view(c, m + 1);
                 UGKS_CK(rerun_step_into(c, slot_lo(c, a), with_record(c, slot_targets(c, a), m), slot_lo(c, b),
                                         with_record(c, slot_targets(c, b), m), a.ledger, record_cn(c, Cr, m)));
@@ -1399,6 +1452,7 @@ extern "C" int ugks_s2cn2_backward(ugks_ctx* c, const double* seed, double* grad
         }
         if (int r = adj_status(c)) return r;
     }
+    if (nckpt > 1) c->adj_last_recorded = 0;   // the slots and records now hold the first segment
     const SlotView g = cot_view(c, cur);
     if (gh0 || gb0 || gW0) {   // x_0's targets depend on its W: their cotangent goes to W
         const SlotView s0 = seg_view(c, 0);
