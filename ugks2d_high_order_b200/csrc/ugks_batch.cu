@@ -52,7 +52,7 @@ size_t rnd(size_t n) { return (n + 31) / 32 * 32; }
 // doubles of per-step scratch one instance needs
 size_t scratch_doubles(int nx, int ny, int nv) {
     const size_t nc = (size_t)nx * ny, S = nc * nv, SY = (size_t)(ny + 1) * nx * nv;
-    return rnd(S * 72) + rnd(s2_scratch_doubles(nx, ny, nv)) + 2 * rnd(S) + 2 * rnd(SY) + rnd(nc * 4) +
+    return rnd(s2_rec_doubles(nx, ny, nv)) + rnd(s2_scratch_doubles(nx, ny, nv)) + 2 * rnd(S) + 2 * rnd(SY) + rnd(nc * 4) +
            rnd((size_t)(ny + 1) * nx * 4) + rnd(nc) + rnd(nc * kNDiag) + rnd(kNDiag) + rnd(nc * 4) + 2 * rnd(S) +
            rnd(nc * kCnCell) + rnd((size_t)2 * nx * 4);
 }
@@ -90,7 +90,7 @@ static void bind_scratch(ugks_batch* b, Inst& I) {
     const size_t nc = (size_t)nx * ny, S = I.S, SY = (size_t)(ny + 1) * nx * nv;
     double* m = b->scratch + (size_t)I.slot * b->per_slot;
     auto take = [&](size_t k) { double* p = m; m += rnd(k); return p; };
-    double* rec = take(S * 72);
+    double* rec = take(s2_rec_doubles(nx, ny, nv));
     double* s2s = take(s2_scratch_doubles(nx, ny, nv));
     double *fxh = take(S), *fxb = take(S), *fyh = take(SY), *fyb = take(SY), *fxw = take(nc * 4);
     double* fyw = take((size_t)(ny + 1) * nx * 4);

@@ -230,8 +230,8 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
         const size_t i_eh = itake(S), i_eb = itake(S), i_fh = itake(S), i_fb = itake(S), i_bh = itake(S), i_bb = itake(S);
         const size_t i_hu = itake((size_t)2 * nv), i_bu = itake((size_t)2 * nv), i_dr = itake((size_t)2 * nx);
         const size_t i_cell = itake((size_t)nc * kImCell), i_st = itake(IS_COUNT), i_rep = itake(kReport);
-        // high order: reconstruction cache [nc][72][nv] and the six volume targets
-        const size_t i_rec = Q.high_order ? itake((size_t)nc * 72 * nv) : 0;
+        // high order: the face cache (s2_rec_doubles) and the six volume targets
+        const size_t i_rec = Q.high_order ? itake(s2_rec_doubles(nx, ny, nv)) : 0;
         size_t i_tg[6] = {0, 0, 0, 0, 0, 0};
         if (Q.high_order) for (int t = 0; t < 6; ++t) i_tg[t] = itake(S);
         const size_t i_scr = Q.high_order ? itake(s2_scratch_doubles(nx, ny, nv)) : 0;
@@ -262,7 +262,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
         // CN right-hand side, per-cell diagnostics, ledger, report and raw wall fluxes
         size_t co = 0;
         auto ctake = [&](size_t n) { size_t o = co; co += (n + 31) / 32 * 32; return o; };
-        const size_t c_rec = ctake((size_t)nc * 72 * nv);
+        const size_t c_rec = ctake(s2_rec_doubles(nx, ny, nv));
         size_t c_tg[2][6];
         for (int q = 0; q < 2; ++q) for (int t = 0; t < 6; ++t) c_tg[q][t] = ctake(S);
         const size_t c_h1 = ctake(S), c_b1 = ctake(S), c_W1 = ctake((size_t)nc * 4);
@@ -1109,7 +1109,7 @@ SlotView cot_view(const ugks_ctx* c, int i) { return view_of(c, c->cot[i], true,
 size_t record_doubles(const ugks_ctx* c) {
     const size_t nx = c->P.nx, ny = c->P.ny, nv = c->P.nvel, nc = nx * ny, S = nc * nv;
     const size_t nf = nc + nx * (ny - 1), nfw = nf + 2 * nx;
-    return rnd32(nc * 72 * nv) + rnd32(nc * 22 * nv) + rnd32(nf * 3 * kS2FScal) + rnd32(nfw * 3 * 4) +
+    return rnd32(s2_rec_doubles((int)nx, (int)ny, (int)nv)) + rnd32(nc * 22 * nv) + rnd32(nf * 3 * kS2FScal) + rnd32(nfw * 3 * 4) +
            rnd32(nc * 9 * 4) + rnd32(nc * 9 * kS2TScal) + 2 * rnd32(S) + rnd32(nc * 4);
 }
 // T with its evaluation scratch in record m (node and mac, which the adjoint does not read, stay shared)
@@ -1117,7 +1117,7 @@ S2Buffers with_record(const ugks_ctx* c, S2Buffers T, int m) {
     const size_t nx = c->P.nx, ny = c->P.ny, nv = c->P.nvel, nc = nx * ny;
     const size_t nf = nc + nx * (ny - 1), nfw = nf + 2 * nx;
     double* r = c->rmem + (size_t)m * record_doubles(c);
-    T.rec = r; r += rnd32(nc * 72 * nv);
+    T.rec = r; r += rnd32(s2_rec_doubles((int)nx, (int)ny, (int)nv));
     T.l1 = r; r += rnd32(nc * 22 * nv);
     T.fscal = r; r += rnd32(nf * 3 * kS2FScal);
     T.nodew = r; r += rnd32(nfw * 3 * 4);
@@ -1129,7 +1129,7 @@ S2Buffers with_record(const ugks_ctx* c, S2Buffers T, int m) {
 CnBuffers record_cn(const ugks_ctx* c, CnBuffers C, int m) {
     const size_t nx = c->P.nx, ny = c->P.ny, nv = c->P.nvel, nc = nx * ny, S = nc * nv;
     const size_t nf = nc + nx * (ny - 1), nfw = nf + 2 * nx;
-    double* r = c->rmem + (size_t)m * record_doubles(c) + rnd32(nc * 72 * nv) + rnd32(nc * 22 * nv) +
+    double* r = c->rmem + (size_t)m * record_doubles(c) + rnd32(s2_rec_doubles((int)nx, (int)ny, (int)nv)) + rnd32(nc * 22 * nv) +
                 rnd32(nf * 3 * kS2FScal) + rnd32(nfw * 3 * 4) + rnd32(nc * 9 * 4) + rnd32(nc * 9 * kS2TScal);
     C.rh = r; r += rnd32(S);
     C.rb = r; r += rnd32(S);

@@ -29,8 +29,8 @@
 namespace ugks {
 
 // ------------------------------------------------------------------------------------------
-// reconstruction + limiter in two passes.  Cache layout rec[((cell*72 + field*12 + side*3 + node)*nvel + k],
-// fields: h, b, h_n, h_t, b_n, b_t; sides: x left, x right, y bottom, y top.
+// reconstruction + limiter in two passes into the face cache (rec_cell / rec_wall, ugks_s2.cuh; fields: h,
+// b, h_n, h_t, b_n, b_t; sides: x left, x right, y bottom, y top).
 //
 // k_s2_recon1, the first layer (prepare_first_layer_plane, mod_S2D1Reconstruction.f90:501-578):
 // per (cell, velocity, field) the 1-D WENO along x of the cell's own row -- values and derivatives
@@ -157,15 +157,22 @@ __global__ void __launch_bounds__(256, 3) k_s2_recon2(LoParams P, LoBuffers B, S
     // the derivatives are divided by the cell sizes (limit_cell_outputs): multiplied by the reciprocals
     // here, exact when dx and dy are powers of two (the delivered meshes), within an ulp otherwise
     const double ind = 1.0 / (p < 2 ? P.dx : P.dy), itd = 1.0 / (p < 2 ? P.dy : P.dx);
-    double* r = S.rec + (size_t)cc * 72 * nv + k;
+    // the side this velocity leaves the cell through (the face cache's upwind half), and the wall sides
     const int fv = f == 0 ? 0 : 1, fn = f == 0 ? 2 : 4, ft = f == 0 ? 3 : 5;
+    const bool store = kok && rec_leaves(p, B.u[k], B.v[k]);
+    const bool wall = kok && ((p == 2 && j == 0) || (p == 3 && j == ny - 1));
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
         const double v = mf + theta * (face[a] - mf), n = theta * dn[a] * ind, t = theta * dt[a] * itd;
-        if (kok) {
-            r[(size_t)(fv * 12 + p * 3 + a) * nv] = v;
-            r[(size_t)(fn * 12 + p * 3 + a) * nv] = n;
-            r[(size_t)(ft * 12 + p * 3 + a) * nv] = t;
+        if (store) {
+            S.rec[rec_cell(cc, p >> 1, fv, a, nv) + k] = v;
+            S.rec[rec_cell(cc, p >> 1, fn, a, nv) + k] = n;
+            S.rec[rec_cell(cc, p >> 1, ft, a, nv) + k] = t;
+        }
+        if (wall) {
+            S.rec[rec_wall(nx, ny, p - 2, i, fv, a, nv) + k] = v;
+            S.rec[rec_wall(nx, ny, p - 2, i, fn, a, nv) + k] = n;
+            S.rec[rec_wall(nx, ny, p - 2, i, ft, a, nv) + k] = t;
         }
         ok = ok && isfinite(v) && isfinite(n) && isfinite(t);
     }
@@ -324,13 +331,12 @@ __global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffer
     const int axis = fi < nfx ? 0 : 1, f = axis == 0 ? fi : fi - nfx;
     const int cl = f, i = cl % nx, j = cl / nx;
     const int cr = axis == 0 ? j * nx + (i + 1) % nx : (j + 1) * nx + i;
-    const int sl = axis == 0 ? 1 : 3, sr = axis == 0 ? 0 : 2;
     const double dt = B.dt[0];
     const double* mac = SB.mac + (size_t)wid * 12;   // [nl | nr | t][component] of this node
     auto upwind = [&](const WVel& s, int field) {
         const double vn = axis == 0 ? s.u : s.v;
         const bool left = vn >= 0.0;
-        return SB.rec[((size_t)(left ? cl : cr) * 72 + field * 12 + (left ? sl : sr) * 3 + g) * nv + s.k];
+        return SB.rec[rec_cell(left ? cl : cr, axis, field, g, nv) + s.k];
     };
     // W0: moments of the upwind face values
     double acc[16];
@@ -450,7 +456,6 @@ __global__ void __launch_bounds__(256, 3) k_s2_face_flux(LoParams P, LoBuffers B
     const int axis = fi < nfx ? 0 : 1, f = axis == 0 ? fi : fi - nfx;
     const int cl = f, i = cl % nx, j = cl / nx;
     const int cr = axis == 0 ? j * nx + (i + 1) % nx : (j + 1) * nx + i;
-    const int sl = axis == 0 ? 1 : 3, sr = axis == 0 ? 0 : 2;
     if (threadIdx.x < kS2FScal) sc[threadIdx.x] = SB.fscal[(size_t)wid * kS2FScal + threadIdx.x];
     __syncthreads();
     if (sc[0] == 0.0) return;   // the scalars kernel failed (status set there)
@@ -490,9 +495,9 @@ __global__ void __launch_bounds__(256, 3) k_s2_face_flux(LoParams P, LoBuffers B
         moment_add(wk, uk, vk, mth, mtb, acc);
         const double vn = axis == 0 ? uk : vk, vt = axis == 0 ? vk : uk;
         const bool left = vn >= 0.0;
-        const double* rc = SB.rec + ((size_t)(left ? cl : cr) * 72 + (left ? sl : sr) * 3 + g) * nv + k;
-        const double f0h = rc[0], f0b = rc[(size_t)12 * nv], nh = rc[(size_t)24 * nv], th_ = rc[(size_t)36 * nv];
-        const double nb = rc[(size_t)48 * nv], tb_ = rc[(size_t)60 * nv];
+        const double* rc = SB.rec + rec_cell(left ? cl : cr, axis, 0, g, nv) + k;   // fields 3 nv apart
+        const double f0h = rc[0], f0b = rc[(size_t)3 * nv], nh = rc[(size_t)6 * nv], th_ = rc[(size_t)9 * nv];
+        const double nb = rc[(size_t)12 * nv], tb_ = rc[(size_t)15 * nv];
         const double sh = vn * (left ? dlh : drh) + vt * dth;
         const double sb = vn * (left ? dlb : drb) + vt * dtb;
         const double fhv = vn * (mt[0] * s0h + mt[1] * sh + mt[2] * mth + mt[3] * f0h - mt[4] * (vn * nh + vt * th_));
@@ -527,7 +532,7 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
     if (wid >= 2 * nx * 3) return;
     const int wf = wid / 3, g = wid % 3;
     const int top = wf >= nx ? 1 : 0, i = wf - top * nx;
-    const int cc = top ? (ny - 1) * nx + i : i, sidx = top ? 3 : 2;
+    const int cc = top ? (ny - 1) * nx + i : i;
     const size_t node = (size_t)(nf + wf) * 3 + g;
     const double side = top ? 1.0 : -1.0;
     const double ux = P.wall_ux[top], theta = 0.5 / P.wall_lam[top];
@@ -545,7 +550,7 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
     C.jac = s_jac[threadIdx.x >> 5];
     bool ok = pp > 0.0 && isfinite(pp) && w_closure(P, B, wwall, C);
     auto rec = [&](const WVel& s, int field) {
-        return SB.rec[((size_t)cc * 72 + field * 12 + sidx * 3 + g) * nv + s.k];
+        return SB.rec[rec_wall(nx, ny, top, i, field, g, nv) + s.k];
     };
     double acc[8];
     double an[4], at[4], atime[4], mt[5], mxi2 = 0.0, coeff = 0.0, hlx = 0.0, hly = 0.0;

@@ -13,8 +13,30 @@ struct S2Maps {
     double gnode[3];
 };
 
+// The face cache (S2Buffers::rec): the limited face values and normal / tangential derivatives of h and b
+// (fields 0..5: h, b, h_n, h_t, b_n, b_t) at the 3 Gauss nodes of a cell's sides.  Per velocity a cell
+// keeps, along each axis, only the side that velocity leaves it through (x: the right side when u >= 0,
+// else the left; y: the top when v >= 0, else the bottom) -- the upwind side, the only one an interior face
+// reads: [cell][axis][field][node][nvel].  The wall rows' wall sides follow for every velocity (the wall
+// node reads both halves): [wall: bottom, top][i][field][node][nvel].
+__host__ __device__ __forceinline__ size_t s2_rec_doubles(int nx, int ny, int nv) {
+    return ((size_t)nx * ny * 36 + (size_t)2 * nx * 18) * (size_t)nv;
+}
+__host__ __device__ __forceinline__ size_t rec_cell(int cell, int axis, int field, int node, int nv) {
+    return ((((size_t)cell * 2 + axis) * 6 + field) * 3 + node) * (size_t)nv;
+}
+__host__ __device__ __forceinline__ size_t rec_wall(int nx, int ny, int wall, int i, int field, int node, int nv) {
+    return ((size_t)nx * ny * 36 + (((size_t)wall * nx + i) * 6 + field) * 3 + node) * (size_t)nv;
+}
+// whether velocity (u, v) leaves a cell through side p (0 x left, 1 x right, 2 y bottom, 3 y top): the
+// upwind selector of the faces, vn >= 0 taking the lower cell's upper side
+__host__ __device__ __forceinline__ bool rec_leaves(int p, double u, double v) {
+    const bool hi = (p < 2 ? u : v) >= 0.0;
+    return (p & 1) ? hi : !hi;
+}
+
 struct S2Buffers {
-    double* rec;                        // [cell][72][nvel] limited face values / derivatives
+    double* rec;                        // the face cache (layout above, s2_rec_doubles)
     double *mh, *mb, *kxh, *kxb, *kyh, *kyb;   // [cell][nvel] volume targets
     double* wall_raw;                   // [2][nx][4] wall macro fluxes before the face length (bottom,
                                         // top), for the S2CN2 conservation ledger (nullptr: not kept)

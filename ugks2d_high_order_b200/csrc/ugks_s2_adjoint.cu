@@ -755,7 +755,6 @@ __global__ void __launch_bounds__(128) k_adj_face_nodes(LoParams P, LoBuffers B,
     const int axis = fi < nfx ? 0 : 1, f = axis == 0 ? fi : fi - nfx;
     const int cl = f, i = cl % nx, j = cl / nx;
     const int cr = axis == 0 ? j * nx + (i + 1) % nx : (j + 1) * nx + i;
-    const int sl = axis == 0 ? 1 : 3, sr = axis == 0 ? 0 : 2;
     const double dt = B.dt[0];
     const double* sc = S.fscal + (size_t)wid * kS2FScal;
     if (sc[0] == 0.0) return;   // the forward node failed (its status is set)
@@ -779,9 +778,7 @@ __global__ void __launch_bounds__(128) k_adj_face_nodes(LoParams P, LoBuffers B,
     double gnw[4];   // cotangent of the node's macro flux
 #pragma unroll
     for (int m = 0; m < 4; ++m) gnw[m] = fold * (A.gws[cr * 4 + m] - A.gws[cl * 4 + m]);
-    auto rec_at = [&](int cell, int side, int field, int k) {
-        return S.rec[((size_t)cell * 72 + field * 12 + side * 3 + g) * nv + k];
-    };
+    auto rec_at = [&](int cell, int field, int k) { return S.rec[rec_cell(cell, axis, field, g, nv) + k]; };
     // per-velocity cotangents of the node's micro flux (fhv, fbv) times vn
     auto flux_cot = [&](const WVel& s, double vn, double& ah, double& ab) {
         const double Gh = fold * (A.grh[(size_t)cr * nv + s.k] - A.grh[(size_t)cl * nv + s.k]) + psi_h(s.w, s.u, s.v, gnw);
@@ -798,7 +795,7 @@ __global__ void __launch_bounds__(128) k_adj_face_nodes(LoParams P, LoBuffers B,
         if (!s.ok) continue;
         const double vn = axis == 0 ? s.u : s.v, vt = axis == 0 ? s.v : s.u;
         const bool left = vn >= 0.0;
-        const int cell = left ? cl : cr, side = left ? sl : sr;
+        const int cell = left ? cl : cr;
         double ah, ab;
         flux_cot(s, vn, ah, ab);
         const QV v = qv_at(th, s.u, s.v);
@@ -822,9 +819,9 @@ __global__ void __launch_bounds__(128) k_adj_face_nodes(LoParams P, LoBuffers B,
         const double kyh = M.coeff * cy * shh * v.qh - dy_h, kyb = M.coeff * cy * shb * v.qb - dy_b;
         const double s0h = v.qh + kxh * q0x + kyh * q0y, s0b = v.qb + kxb * q0x + kyb * q0y;
         const double sh = vn * lr_h + vt * t_h, sb = vn * lr_b + vt * t_b;
-        const double f0h = rec_at(cell, side, 0, s.k), f0b = rec_at(cell, side, 1, s.k);
-        const double nh = rec_at(cell, side, 2, s.k), th_ = rec_at(cell, side, 3, s.k);
-        const double nb = rec_at(cell, side, 4, s.k), tb_ = rec_at(cell, side, 5, s.k);
+        const double f0h = rec_at(cell, 0, s.k), f0b = rec_at(cell, 1, s.k);
+        const double nh = rec_at(cell, 2, s.k), th_ = rec_at(cell, 3, s.k);
+        const double nb = rec_at(cell, 4, s.k), tb_ = rec_at(cell, 5, s.k);
         acc[0] += ah * s0h + ab * s0b;
         acc[1] += ah * sh + ab * sb;
         acc[2] += ah * m_h + ab * m_b;
@@ -937,7 +934,7 @@ __global__ void __launch_bounds__(128) k_adj_face_nodes(LoParams P, LoBuffers B,
         const WVel s = wvel(B, nv, r);
         const double vn = axis == 0 ? s.u : s.v;
         const bool left = vn >= 0.0;
-        moment_add(s.w, s.u, s.v, rec_at(left ? cl : cr, left ? sl : sr, 0, s.k), rec_at(left ? cl : cr, left ? sl : sr, 1, s.k), W0);
+        moment_add(s.w, s.u, s.v, rec_at(left ? cl : cr, 0, s.k), rec_at(left ? cl : cr, 1, s.k), W0);
     }
     warp_sum_all<4>(W0);
     const double nrho = W0[0], nu = W0[1] / W0[0], nvv = W0[2] / W0[0];
@@ -951,7 +948,7 @@ __global__ void __launch_bounds__(128) k_adj_face_nodes(LoParams P, LoBuffers B,
         if (!s.ok) continue;
         const double vn = axis == 0 ? s.u : s.v;
         const bool left = vn >= 0.0;
-        const int cell = left ? cl : cr, side = left ? sl : sr;
+        const int cell = left ? cl : cr;
         const QV v = qv_at(th, s.u, s.v);
         const double cx = s.u - M.ux, cy = s.v - M.vy, c2 = cx * cx + cy * cy;
         const double shh = 2.0 * M.lam * c2 - 4.0, shb = shh + shb_add;
@@ -978,7 +975,7 @@ __global__ void __launch_bounds__(128) k_adj_face_nodes(LoParams P, LoBuffers B,
         // q0 = heat(w0, f0 - E(W0)) with (cx, cy) about make_mke's (ux, vy)
         const double du = s.u - nu, dv = s.v - nvv, cn2 = du * du + dv * dv;
         const double eah = nrho * lamn / kPi * exp(-lamn * cn2), eab = 0.5 * (double)ck * temp * eah;
-        const double dh = rec_at(cell, side, 0, s.k) - eah, db = rec_at(cell, side, 1, s.k) - eab;
+        const double dh = rec_at(cell, 0, s.k) - eah, db = rec_at(cell, 1, s.k) - eab;
         heat_shift_adj(s.w, cx, cy, dh, db, gq0x, gq0y, acc4[2], acc4[3]);
         const double geah = -0.5 * s.w * c2 * (cx * gq0x + cy * gq0y), geab = -0.5 * s.w * (cx * gq0x + cy * gq0y);
         const double ge = geah + 0.5 * (double)ck * temp * geab;
@@ -1020,13 +1017,9 @@ __global__ void __launch_bounds__(128) k_adj_face_nodes(LoParams P, LoBuffers B,
         const double gh0 = ah * mt[3] + psi_h(s.w, s.u, s.v, gW0) + 0.5 * s.w * c2 * (cx * gq0x + cy * gq0y);
         const double gb0 = ab * mt[3] + psi_b(s.w, gW0) + 0.5 * s.w * (cx * gq0x + cy * gq0y);
         const double gv[6] = {gh0, gb0, -ah * mt[4] * vn, -ah * mt[4] * vt, -ab * mt[4] * vn, -ab * mt[4] * vt};
-        double* up = A.grec + ((size_t)(left ? cl : cr) * 72 + (left ? sl : sr) * 3 + g) * nv + s.k;
-        double* down = A.grec + ((size_t)(left ? cr : cl) * 72 + (left ? sr : sl) * 3 + g) * nv + s.k;
+        double* up = A.grec + rec_cell(left ? cl : cr, axis, 0, g, nv) + s.k;
 #pragma unroll
-        for (int fld = 0; fld < 6; ++fld) {
-            up[(size_t)fld * 12 * nv] = gv[fld];
-            down[(size_t)fld * 12 * nv] = 0.0;
-        }
+        for (int fld = 0; fld < 6; ++fld) up[(size_t)fld * 3 * nv] = gv[fld];
     }
 }
 
@@ -1146,7 +1139,7 @@ __global__ void __launch_bounds__(256, 2) k_adj_wall_nodes(LoParams P, LoBuffers
     if (wid >= 2 * nx * 3) return;
     const int wf = wid / 3, g = wid % 3;
     const int top = wf >= nx ? 1 : 0, i = wf - top * nx;
-    const int cc = top ? (ny - 1) * nx + i : i, sidx = top ? 3 : 2;
+    const int cc = top ? (ny - 1) * nx + i : i;
     const size_t node = (size_t)(nf + wf) * 3 + g;
     const double side = top ? 1.0 : -1.0;
     const double ux = P.wall_ux[top], theta = 0.5 / P.wall_lam[top];
@@ -1160,7 +1153,7 @@ __global__ void __launch_bounds__(256, 2) k_adj_wall_nodes(LoParams P, LoBuffers
     WClosure C;
     C.jac = s_jac[threadIdx.x >> 5];
     if (!(pp > 0.0 && w_closure(P, B, wwall, C))) return;   // the forward node failed (its status is set)
-    auto rec = [&](int k, int field) { return S.rec[((size_t)cc * 72 + field * 12 + sidx * 3 + g) * nv + k]; };
+    auto rec = [&](int k, int field) { return S.rec[rec_wall(nx, ny, top, i, field, g, nv) + k]; };
     double acc[8];
 #pragma unroll
     for (int m = 0; m < 8; ++m) acc[m] = 0.0;
@@ -1366,9 +1359,9 @@ __global__ void __launch_bounds__(256, 2) k_adj_wall_nodes(LoParams P, LoBuffers
         gv[3] = -mt[4] * s.u * gh - s.w * (gI[7] + vn * gI[8] + vt * gI[9] + 0.5 * v2 * gI[10]);
         gv[4] = -mt[4] * vn * gb;
         gv[5] = -mt[4] * s.u * gb - 0.5 * s.w * gI[10];
-        double* o = A.grec + ((size_t)cc * 72 + sidx * 3 + g) * nv + s.k;
+        double* o = A.grec + rec_wall(nx, ny, top, i, 0, g, nv) + s.k;
 #pragma unroll
-        for (int fld = 0; fld < 6; ++fld) o[(size_t)fld * 12 * nv] = gv[fld];
+        for (int fld = 0; fld < 6; ++fld) o[(size_t)fld * 3 * nv] = gv[fld];
     }
 }
 
@@ -1450,7 +1443,7 @@ __global__ void __launch_bounds__(256) k_adj_macro_faces(LoParams P, const doubl
 
 // ---------------------------------------------------------------------------------------------
 // the second layer and the positivity limiter (k_s2_recon2), transposed: CTA = 8 warps (field, part)
-// over 32 velocities of one cell, as the forward kernel.  grec (this cell's 72 rows) -> gl1 of the rows /
+// over 32 velocities of one cell, as the forward kernel.  grec (this cell's face-cache entries) -> gl1 of the rows /
 // columns the templates read, and the state (the limiter's cell means, the wall rows' direct samples).
 __global__ void __launch_bounds__(256, 2) k_adj_recon2(LoParams P, LoBuffers B, S2Buffers S, AdjBuffers A) {
     __shared__ double s_th[8][32];
@@ -1536,13 +1529,17 @@ __global__ void __launch_bounds__(256, 2) k_adj_recon2(LoParams P, LoBuffers B, 
     const double theta = zero ? 0.0 : fmax(0.0, fmin(1.0, tmin));
     const double ind = 1.0 / (p < 2 ? P.dx : P.dy), itd = 1.0 / (p < 2 ? P.dy : P.dx);
     const int fv = f == 0 ? 0 : 1, fn = f == 0 ? 2 : 4, ft = f == 0 ? 3 : 5;
-    const double* gr = A.grec + (size_t)cc * 72 * nv + k;
+    // this side's cotangents: a wall side's from the wall node (every velocity), another side's from the
+    // face the velocity leaves through (the face cache keeps that half only), zero for the other half
+    const bool wside = (p == 2 && j == 0) || (p == 3 && j == ny - 1);
+    const bool held = kok && (wside || rec_leaves(p, B.u[k], B.v[k]));
+    const double* gr = A.grec + (wside ? rec_wall(nx, ny, p - 2, i, 0, 0, nv) : rec_cell(cc, p >> 1, 0, 0, nv)) + k;
     double gface[3], gdn[3], gdt[3], gvol[3] = {0.0, 0.0, 0.0}, gmf = 0.0, gth = 0.0;
 #pragma unroll
     for (int a = 0; a < 3; ++a) {
-        const double gv = kok ? gr[(size_t)(fv * 12 + p * 3 + a) * nv] : 0.0;
-        const double gn = kok ? gr[(size_t)(fn * 12 + p * 3 + a) * nv] : 0.0;
-        const double gt = kok ? gr[(size_t)(ft * 12 + p * 3 + a) * nv] : 0.0;
+        const double gv = held ? gr[(size_t)(fv * 3 + a) * nv] : 0.0;
+        const double gn = held ? gr[(size_t)(fn * 3 + a) * nv] : 0.0;
+        const double gt = held ? gr[(size_t)(ft * 3 + a) * nv] : 0.0;
         gface[a] = theta * gv;
         gmf += (1.0 - theta) * gv;
         gth += (face[a] - mf) * gv + dn[a] * ind * gn + dt[a] * itd * gt;
@@ -1660,7 +1657,8 @@ __global__ void __launch_bounds__(128) k_adj_recon1(LoParams P, LoBuffers B, Adj
 size_t adj_work_doubles(int nx, int ny, int nv) {
     const size_t nc = (size_t)nx * ny, S = nc * nv, nf = nc + (size_t)nx * (ny - 1);
     auto r = [](size_t n) { return (n + 31) / 32 * 32; };
-    return 2 * r(S) + r(nc * 4) + r(nc * 9 * 4) + r(nc * 72 * nv) + r(nc * 22 * nv) + r(nf * 3 * 12) + r(GP_COUNT);
+    return 2 * r(S) + r(nc * 4) + r(nc * 9 * 4) + r(s2_rec_doubles(nx, ny, nv)) + r(nc * 22 * nv) + r(nf * 3 * 12) +
+           r(GP_COUNT);
 }
 
 void adj_bind_work(AdjBuffers& A, double* base, int nx, int ny, int nv) {
@@ -1670,7 +1668,7 @@ void adj_bind_work(AdjBuffers& A, double* base, int nx, int ny, int nv) {
     A.grb = base; base += r(S);
     A.gws = base; base += r(nc * 4);
     A.gwq = base; base += r(nc * 9 * 4);
-    A.grec = base; base += r(nc * 72 * nv);
+    A.grec = base; base += r(s2_rec_doubles(nx, ny, nv));
     A.gl1 = base; base += r(nc * 22 * nv);
     A.gmac = base; base += r(nf * 3 * 12);
     A.gpar = base;
