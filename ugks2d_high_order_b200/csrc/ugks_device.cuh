@@ -281,6 +281,39 @@ __device__ __forceinline__ void warp_max_all(double* v) {
     for (int i = 0; i < N; ++i) v[i] = __shfl_sync(0xffffffffu, r, i << sh);
 }
 
+// Compensated summation.  two_sum (Knuth, TAOCP vol. 2, 4.2.2): s = fl(a + b) and the exact rounding error
+// e = a + b - s, in either argument order.  A compensated sum carries (s, c): every term enters s through
+// two_sum and its error into c (Neumaier's form of Kahan summation); the sum is s + c.
+__device__ __forceinline__ void two_sum(double a, double b, double& s, double& e) {
+    s = a + b;
+    const double bb = s - a;
+    e = (a - (s - bb)) + (b - bb);
+}
+__device__ __forceinline__ void comp_add(double& s, double& c, double x) {
+    double t, e;
+    two_sum(s, x, t, e);
+    s = t;
+    c = c + e;
+}
+// Warp totals of N compensated per-lane sums (s, c): an xor butterfly that joins pairs by two_sum and adds
+// their compensations, so both lanes of a pair compute the same values; every lane returns the totals
+// s + c in s[0..N).
+template <int N>
+__device__ __forceinline__ void warp_sum_all_comp(double* s, double* c) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1)
+#pragma unroll
+        for (int m = 0; m < N; ++m) {
+            const double os = __shfl_xor_sync(0xffffffffu, s[m], o), oc = __shfl_xor_sync(0xffffffffu, c[m], o);
+            double t, e;
+            two_sum(s[m], os, t, e);
+            s[m] = t;
+            c[m] = (c[m] + oc) + e;
+        }
+#pragma unroll
+    for (int m = 0; m < N; ++m) s[m] = s[m] + c[m];
+}
+
 // Reduce into shared memory only: on return out[0..NS+NM) holds the block totals and is visible
 // to every thread.  The next reduction writes `out` only after its first barrier, which no thread
 // passes before it has read this one, so no trailing barrier is needed.

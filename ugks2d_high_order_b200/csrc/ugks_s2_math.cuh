@@ -489,8 +489,9 @@ __device__ bool w_closure(const LoParams& P, const LoBuffers& B, const double w[
     int iter = 0;
     bool first = true;
     for (int guard = 0; guard < 1024; ++guard) {
-        // 16 Jacobian moments, the 4 moments of (qh, qb), flags: nonfinite, nonpositive
-        double acc[22];
+        // 16 Jacobian moments, the 4 moments of (qh, qb) (compensated: the Newton residual is their
+        // difference from w), flags: nonfinite, nonpositive
+        double acc[22], ms[4] = {0.0, 0.0, 0.0, 0.0}, mc[4] = {0.0, 0.0, 0.0, 0.0};
 #pragma unroll
         for (int m = 0; m < 22; ++m) acc[m] = 0.0;
         const S2Th tt = s2_th(trial, ck);
@@ -506,16 +507,19 @@ __device__ bool w_closure(const LoParams& P, const LoBuffers& B, const double w[
                 acc[2 * 4 + a] += s.w * s.v * hk;
                 acc[3 * 4 + a] += 0.5 * s.w * (e2 * hk + bk);
             }
-            acc[16] += s.w * q.qh;
-            acc[17] += s.w * s.u * q.qh;
-            acc[18] += s.w * s.v * q.qh;
-            acc[19] += 0.5 * s.w * (e2 * q.qh + q.qb);
+            comp_add(ms[0], mc[0], s.w * q.qh);
+            comp_add(ms[1], mc[1], s.w * s.u * q.qh);
+            comp_add(ms[2], mc[2], s.w * s.v * q.qh);
+            comp_add(ms[3], mc[3], 0.5 * s.w * (e2 * q.qh + q.qb));
             if (s.ok) {
                 acc[20] = fmax(acc[20], (isfinite(q.qh) && isfinite(q.qb)) ? 0.0 : 1.0);
                 acc[21] = fmax(acc[21], (q.qh > 0.0 && q.qb > 0.0) ? 0.0 : 1.0);
             }
         }
-        warp_sum_all<20>(acc);
+        warp_sum_all<16>(acc);
+        warp_sum_all_comp<4>(ms, mc);
+#pragma unroll
+        for (int m = 0; m < 4; ++m) acc[16 + m] = ms[m];
         warp_max_all<2>(acc + 20);
         bool fin = acc[20] == 0.0;
 #pragma unroll
