@@ -26,6 +26,8 @@ class UOParams(ctypes.Structure):
         ("macro_sweeps", ctypes.c_int),
         ("residual_tol", ctypes.c_double), ("moment_tol", ctypes.c_double), ("min_alpha", ctypes.c_double),
         ("high_order", ctypes.c_int),
+        ("s2_kinetic_wall", ctypes.c_int), ("s2_time_centered", ctypes.c_int), ("s2_face_time", ctypes.c_int),
+        ("s2_shared_predictor", ctypes.c_int),
     ]
 
 
@@ -101,6 +103,9 @@ class Oracle:
         p.macro_sweeps = case.macro_sweeps
         p.residual_tol, p.moment_tol, p.min_alpha = case.residual_tol, case.moment_tol, case.min_alpha
         p.high_order = int(case.method == "HighOrderImplicit")
+        p.s2_kinetic_wall = int(case.flux_wall == 0)
+        p.s2_time_centered, p.s2_face_time = int(case.s2w1_time_centered), int(case.s2w1d_face_time)
+        p.s2_shared_predictor = int(case.s2w2r_shared_predictor)
         self._params = p
         self.ptr = lib().uo_create(ctypes.byref(p), _p(self.u), _p(self.v), _p(self.w))
 

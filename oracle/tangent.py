@@ -33,6 +33,8 @@ class UOParamsT(ctypes.Structure):
         ("macro_sweeps", ctypes.c_int),
         ("residual_tol", D2), ("moment_tol", D2), ("min_alpha", D2),
         ("high_order", ctypes.c_int),
+        ("s2_kinetic_wall", ctypes.c_int), ("s2_time_centered", ctypes.c_int), ("s2_face_time", ctypes.c_int),
+        ("s2_shared_predictor", ctypes.c_int),
     ]
 
 
@@ -109,6 +111,9 @@ class TangentOracle:
         p.nslab, p.mass_rescale, p.macro_sweeps = case.nslab, int(case.mass_rescale), case.macro_sweeps
         p.residual_tol, p.moment_tol, p.min_alpha = _pair(case.residual_tol), _pair(case.moment_tol), _pair(case.min_alpha)
         p.high_order = int(case.method == "HighOrderImplicit")
+        p.s2_kinetic_wall = int(case.flux_wall == 0)
+        p.s2_time_centered, p.s2_face_time = int(case.s2w1_time_centered), int(case.s2w1d_face_time)
+        p.s2_shared_predictor = int(case.s2w2r_shared_predictor)
         self._params = p
         self.dux = np.array(dux, dtype=np.float64)
         self.wall_ux = np.array(case.wall_ux, dtype=np.float64)

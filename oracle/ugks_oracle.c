@@ -64,6 +64,10 @@ struct uo_ctx {
     double *cn_hn, *cn_bn;        /* proposal after the CN collision */
     double *cn_cell;              /* [nc][UO_CN_CELL] per-cell advance diagnostics */
     double cn_total0[4], cn_balance[4];   /* conservation ledger: initial totals, cumulative wall balance */
+    /* research wall variants (ugks_oracle_s2.c) */
+    double *s2_coef;              /* [nc][3 faces as s2_facc][f0 h, f0 b, k h, k b][nvel] leading / time coefficients */
+    double *s2_facc0;             /* the accepted state's face accumulators while a predictor runs */
+    double *v_inst;               /* [nc][3 faces][h nv, b nv] instantaneous fluxes at the predicted state */
     /* scratch: 24 work vectors per OpenMP thread */
     int nthr;
     double **tt;

@@ -35,6 +35,12 @@ typedef struct {
     int macro_sweeps;         /* Implicit_MacroSweeps */
     double residual_tol, moment_tol, min_alpha;
     int high_order;           /* 1: HighOrderImplicit (S2 evolution, S2 physical collision, HO micro RHS) */
+    /* the research S2CN2 wall variants (mod_ImportPara.f90:88-93, checks :455-471, :516-533); all zero is
+     * the delivered configuration (FluxWall_type = 1, the multiscale wall) */
+    int s2_kinetic_wall;      /* FluxWall_type = 0: the free-streaming diffuse wall s2w1_wall_node */
+    int s2_time_centered;     /* S2W1_time_centered = 1: W1T, walls re-evaluated at a predicted midpoint */
+    int s2_face_time;         /* S2W1D_face_time_consistent = 1: W1D, interior faces corrected there too */
+    int s2_shared_predictor;  /* S2W2R_shared_predictor = 1: W2R, every face corrected at a shared predictor */
 } uo_params;
 
 typedef struct uo_ctx uo_ctx;

@@ -645,9 +645,11 @@ typedef struct {
 static s2_scratch* s2_scr(uo_ctx* c, int tid) { return (s2_scratch*)c->s2_scr + tid; }
 
 /* ugks_node (mod_S2D1.f90:421-521) at one face Gauss node.  axis 0: x face (vn = u, vt = v);
- * axis 1: y face (vn = v, vt = u).  in: 12 arrays hl hr bl br hnl hnr htl htr bnl bnr btl btr */
+ * axis 1: y face (vn = v, vt = u).  in: 12 arrays hl hr bl br hnl hnr htl htr bnl bnr btl btr.
+ * coef (NULL: not wanted): the optional f0_h, f0_b, k_h, k_b outputs (:501-505), the leading and the
+ * time coefficients of the node flux, 4 x nvel. */
 static int s2_ugks_node(uo_ctx* c, int tid, int axis, double dt, const double* const in[12], const double mnl4[4],
-                        const double mnr4[4], const double mt4[4], double* fh, double* fb, double fw[4]) {
+                        const double mnr4[4], const double mt4[4], double* fh, double* fb, double fw[4], double* coef) {
     const uo_params* p = &c->p;
     int n = p->nvel;
     const double *u = c->u, *v = c->v, *wt = c->w;
@@ -706,6 +708,12 @@ static int s2_ugks_node(uo_ctx* c, int tid, int axis, double dt, const double* c
         double nh = vn >= 0.0 ? hnl[k] : hnr[k], nb = vn >= 0.0 ? bnl[k] : bnr[k];
         fh[k] = vn * (mt[0] * s0h[k] + mt[1] * sh + mt[2] * mtmh[k] + mt[3] * f0h[k] - mt[4] * (vn * nh + vt * fth[k]));
         fb[k] = vn * (mt[0] * s0b[k] + mt[1] * sb + mt[2] * mtmb[k] + mt[3] * f0b[k] - mt[4] * (vn * nb + vt * ftb[k]));
+        if (coef) {
+            coef[k] = vn * f0h[k];
+            coef[n + k] = vn * f0b[k];
+            coef[2 * n + k] = vn * ((s0h[k] - f0h[k]) / tau - vn * nh - vt * fth[k]);
+            coef[3 * n + k] = vn * ((s0b[k] - f0b[k]) / tau - vn * nb - vt * ftb[k]);
+        }
         ok &= isfinite(fh[k]) && isfinite(fb[k]);
     }
     if (!s2_moment(n, fh, fb, u, v, wt, fw)) return 0;
@@ -798,7 +806,7 @@ static void s2w_time_coeffs(double dt, double tau, double mt[5]) {
  * values, normal (y) and tangential (x) derivatives at this Gauss node. */
 static int s2_wall_node(uo_ctx* c, int tid, int side, double dt, double dn, const double wcell[4], const double* hin,
                         const double* bin, const double* hn, const double* bn, const double* ht, const double* bt,
-                        double ux, double theta, double* fh, double* fb, double fw[4]) {
+                        double ux, double theta, double* fh, double* fb, double fw[4], double* coef) {
     const uo_params* p = &c->p;
     int n = p->nvel, ck = p->ck;
     const double *u = c->u, *v = c->v, *wt = c->w;
@@ -885,7 +893,94 @@ static int s2_wall_node(uo_ctx* c, int tid, int side, double dt, double dn, cons
         for (int m = 0; m < 4; ++m) fw[m] = fw[m] + wt[k] * e[m];
         ok &= isfinite(fh[k]) && isfinite(fb[k]);
     }
+    if (coef) {   /* the optional f0/k outputs (:155-177): the leading and time coefficients of the wall flux */
+        double a0 = 0.0, a1 = 0.0, den = 0.0;
+        for (int k = 0; k < n; ++k) {
+            const double qh = (mh[k] + corrh[k] - hin[k]) / tau_wall - v[k] * hn[k] - u[k] * ht[k];
+            if ((double)side * v[k] > 0.0) { a0 = a0 + wt[k] * v[k] * hin[k]; a1 = a1 + wt[k] * v[k] * qh; }
+            else den = den + wt[k] * v[k] * wall[k];
+        }
+        const double r0 = -a0 / den, r1 = -a1 / den;
+        if (!(isfinite(r0) && isfinite(r1)) || r0 <= 0.0) return 0;
+        double s0 = 0.0, s1 = 0.0;
+        for (int k = 0; k < n; ++k) {
+            if ((double)side * v[k] > 0.0) {
+                coef[k] = v[k] * hin[k];
+                coef[n + k] = v[k] * bin[k];
+                coef[2 * n + k] = v[k] * ((mh[k] + corrh[k] - hin[k]) / tau_wall - v[k] * hn[k] - u[k] * ht[k]);
+                coef[3 * n + k] = v[k] * ((mb[k] + corrb[k] - bin[k]) / tau_wall - v[k] * bn[k] - u[k] * bt[k]);
+            } else {
+                coef[k] = v[k] * r0 * wall[k];
+                coef[n + k] = v[k] * r0 * wallb[k];
+                coef[2 * n + k] = v[k] * r1 * wall[k];
+                coef[3 * n + k] = v[k] * r1 * wallb[k];
+            }
+            s0 = s0 + wt[k] * coef[k];
+            s1 = s1 + wt[k] * coef[2 * n + k];
+        }
+        if (fabs(s0) > S2_GATE || fabs(s1) > S2_GATE) return 0;
+    }
     return ok && isfinite(fw[0]) && fabs(fw[0]) <= S2_GATE * fmax(1.0, fabs(inc));
+}
+
+/* s2w1_wall_node (mod_S2D1.f90:961-995): the time-integrated free-streaming diffuse wall of
+ * FluxWall_type 0 at one tangential Gauss node -- incident half from the face values, reflected half
+ * the continuous wall Maxwellian scaled to zero mass flux. */
+static int s2w1_wall_node(const uo_ctx* c, int side, double dt, const double* hin, const double* bin, double ux,
+                          double theta, double* fh, double* fb, double fw[4]) {
+    const int n = c->p.nvel;
+    const double *u = c->u, *v = c->v, *wt = c->w;
+    const double lambda = 0.5 / theta;
+    double incidence = 0.0, reflection = 0.0;
+    for (int k = 0; k < n; ++k) {
+        const double mh = lambda / PI_D * exp(-lambda * ((u[k] - ux) * (u[k] - ux) + v[k] * v[k]));
+        if ((double)side * v[k] > 0.0) incidence = incidence + wt[k] * v[k] * hin[k];
+        else reflection = reflection + wt[k] * v[k] * mh;
+    }
+    if (!(isfinite(reflection) && fabs(reflection) > DBL_MIN)) return 0;
+    const double rho_w = -incidence / reflection;
+    if (!(isfinite(rho_w) && rho_w > 0.0)) return 0;
+    for (int k = 0; k < n; ++k) {
+        if ((double)side * v[k] > 0.0) { fh[k] = dt * v[k] * hin[k]; fb[k] = dt * v[k] * bin[k]; }
+        else {
+            const double mh = lambda / PI_D * exp(-lambda * ((u[k] - ux) * (u[k] - ux) + v[k] * v[k]));
+            fh[k] = dt * v[k] * rho_w * mh;
+            fb[k] = (double)c->p.ck * theta * fh[k];
+        }
+    }
+    if (!s2_moment(n, fh, fb, u, v, wt, fw)) return 0;
+    return fabs(fw[0]) <= S2_GATE * fmax(1.0, dt * fabs(incidence));
+}
+
+/* s2w2_instantaneous_node, S2PhysicalGas = 1 (mod_S2MultiscaleWall.f90:187-227): the un-integrated
+ * diffuse wall flux of W2R's shared predictor -- incident half from the face values, reflected half the
+ * discrete closure of the unit-density wall state (wall_equilibrium, :231-238) scaled to zero mass flux. */
+static int s2w2_inst_node(uo_ctx* c, int tid, int side, const double* hin, const double* bin, double ux, double theta,
+                          double* fh, double* fb, double fw[4]) {
+    const int n = c->p.nvel, ck = c->p.ck;
+    const double *u = c->u, *v = c->v, *wt = c->w;
+    s2_scratch* S = s2_scr(c, tid);
+    double* nscr = S->buf + 32 * (size_t)n;
+    double inc = 0.0, den = 0.0;
+    fw[0] = fw[1] = fw[2] = fw[3] = 0.0;
+    const double weq[4] = {1.0, ux, 0.0, (double)(ck + 2) * theta / 2.0 + ux * ux / 2.0};
+    if (!s2_closure_prepare(&S->C, weq, ck, n, u, v, wt, nscr)) return 0;
+    const double *wall = S->C.qh, *wallb = S->C.qb;
+    for (int k = 0; k < n; ++k) {
+        if ((double)side * v[k] > 0.0) inc = inc + wt[k] * v[k] * hin[k];
+        else den = den + wt[k] * v[k] * wall[k];
+    }
+    const double rho = -inc / den;
+    if (!(isfinite(rho) && rho > 0.0)) return 0;
+    int ok = 1;
+    for (int k = 0; k < n; ++k) {
+        if ((double)side * v[k] > 0.0) { fh[k] = v[k] * hin[k]; fb[k] = v[k] * bin[k]; }
+        else { fh[k] = v[k] * rho * wall[k]; fb[k] = v[k] * rho * wallb[k]; }
+        const double e[4] = {fh[k], u[k] * fh[k], v[k] * fh[k], 0.5 * ((u[k] * u[k] + v[k] * v[k]) * fh[k] + fb[k])};
+        for (int m = 0; m < 4; ++m) fw[m] = fw[m] + wt[k] * e[m];
+        ok &= isfinite(fh[k]) && isfinite(fb[k]);
+    }
+    return ok && fabs(fw[0]) <= S2_GATE * fmax(1.0, fabs(inc));
 }
 
 /* ---------------------------------------------------------------- evolution pieces */
@@ -895,7 +990,7 @@ static int s2_wall_node(uo_ctx* c, int tid, int side, double dt, double dn, cons
 #define S2_REC 72
 static inline double* s2_rec(uo_ctx* c, int cc, int k) { return c->s2_rec + ((size_t)cc * c->p.nvel + k) * S2_REC; }
 
-typedef struct { uo_ctx* c; int* err; } s2_arg;
+typedef struct { uo_ctx* c; int* err; int coef; } s2_arg;
 
 /* velocity-by-velocity tensor reconstruction and positivity limiting of every cell (compute_flux,
  * mod_S2D1.f90:713-746 with S2_VELOCITY_TILE; limit_cell_outputs) */
@@ -940,6 +1035,9 @@ static void s2_face_body(void* vp, int cc, int tid) {
     for (int t = 0; t < 12; ++t) arr[t] = base + (size_t)t * nv;
     double *fh = base + 12 * (size_t)nv, *fb = base + 13 * (size_t)nv;
     double* acc = c->s2_facc + (size_t)cc * 3 * (2 * nv + 4);   /* [right x, top y, bottom wall][h nv, b nv, w 4] */
+    /* the leading / time coefficients of the same three faces, when a variant corrects the faces */
+    double* coef = a->coef ? c->s2_coef + (size_t)cc * 3 * 4 * nv : NULL;
+    if (coef) for (size_t k = 0; k < (size_t)3 * 4 * nv; ++k) coef[k] = 0.0;
     for (int axis = 0; axis < 2; ++axis) {
         double* ah = acc + (size_t)axis * (2 * nv + 4);
         double *ab = ah + nv, *aw = ah + 2 * nv;
@@ -979,9 +1077,14 @@ static void s2_face_body(void* vp, int cc, int tid) {
             for (int m = 0; m < 4; ++m) { m4l[m] = mnl[m][g]; m4r[m] = mnr[m][g]; m4t[m] = mtg[m][g]; }
             const double* const in[12] = {arr[0], arr[1], arr[2], arr[3], arr[4], arr[5],
                                           arr[6], arr[7], arr[8], arr[9], arr[10], arr[11]};
-            if (!s2_ugks_node(c, tid, axis, dt, in, m4l, m4r, m4t, fh, fb, fw)) { a->err[cc] = 422; return; }
+            double* cn = coef ? base + 14 * (size_t)nv : NULL;
+            if (!s2_ugks_node(c, tid, axis, dt, in, m4l, m4r, m4t, fh, fb, fw, cn)) { a->err[cc] = 422; return; }
             for (int k = 0; k < nv; ++k) { ah[k] = ah[k] + s2_gw[g] * fh[k]; ab[k] = ab[k] + s2_gw[g] * fb[k]; }
             for (int m = 0; m < 4; ++m) aw[m] = aw[m] + s2_gw[g] * fw[m];
+            if (cn) {   /* leading_x/y and time_x/y (compute_flux :833-836, :879-882) */
+                double* cs = coef + (size_t)axis * 4 * nv;
+                for (int k = 0; k < 4 * nv; ++k) cs[k] = cs[k] + s2_gw[g] * cn[k];
+            }
         }
     }
     /* wall faces: bottom of row 0 (into acc slot 2), top of row ny-1 (into the y slot) */
@@ -1002,13 +1105,19 @@ static void s2_face_body(void* vp, int cc, int tid) {
                 arr[5][k] = L[5 * 12 + side * 3 + g];   /* bt  */
             }
             double fw[4];
-            if (!s2_wall_node(c, tid, t == 0 ? -1 : 1, dt, p->dy, c->W + cc * 4, arr[0], arr[1], arr[2], arr[3], arr[4],
-                              arr[5], p->wall_ux[t], 0.5 * p->wall_tnative[t], fh, fb, fw)) {
-                a->err[cc] = 422;
-                return;
-            }
+            double* cn = coef ? base + 14 * (size_t)nv : NULL;
+            int ok = p->s2_kinetic_wall
+                         ? s2w1_wall_node(c, t == 0 ? -1 : 1, dt, arr[0], arr[1], p->wall_ux[t], 0.5 * p->wall_tnative[t],
+                                          fh, fb, fw)
+                         : s2_wall_node(c, tid, t == 0 ? -1 : 1, dt, p->dy, c->W + cc * 4, arr[0], arr[1], arr[2], arr[3],
+                                        arr[4], arr[5], p->wall_ux[t], 0.5 * p->wall_tnative[t], fh, fb, fw, cn);
+            if (!ok) { a->err[cc] = 422; return; }
             for (int k = 0; k < nv; ++k) { ah[k] = ah[k] + s2_gw[g] * fh[k]; ab[k] = ab[k] + s2_gw[g] * fb[k]; }
             for (int m = 0; m < 4; ++m) aw[m] = aw[m] + s2_gw[g] * fw[m];
+            if (cn && !p->s2_kinetic_wall) {   /* lower0/lowerK, and the top wall into leading_y/time_y (:905-940) */
+                double* cs = coef + (size_t)(t == 0 ? 2 : 1) * 4 * nv;
+                for (int k = 0; k < 4 * nv; ++k) cs[k] = cs[k] + s2_gw[g] * cn[k];
+            }
         }
     }
 }
@@ -1103,6 +1212,7 @@ static void s2_alloc(uo_ctx* c) {
     c->s2_kappa = (double*)calloc((size_t)c->nc * 4, sizeof(double));
     c->lco_h = (double*)calloc(S, sizeof(double)); c->lco_b = (double*)calloc(S, sizeof(double));
     c->s2_facc = (double*)calloc((size_t)c->nc * 3 * (2 * nv + 4), sizeof(double));
+    if (c->p.s2_face_time || c->p.s2_shared_predictor) c->s2_coef = (double*)calloc(S * 3 * 4, sizeof(double));
     s2_scratch* sc = (s2_scratch*)calloc((size_t)c->nthr, sizeof(s2_scratch));
     for (int t = 0; t < c->nthr; ++t) {
         sc[t].buf = (double*)calloc((size_t)S2_NBUF * nv, sizeof(double));
@@ -1118,7 +1228,7 @@ static void s2_alloc(uo_ctx* c) {
 static void s2_free(uo_ctx* c) {
     if (!c->s2_rec) return;
     double* ptrs[] = {c->s2_rec, c->s2_mh, c->s2_mb, c->s2_kxh, c->s2_kxb, c->s2_kyh, c->s2_kyb, c->s2_kappa,
-                      c->lco_h, c->lco_b, c->s2_facc};
+                      c->lco_h, c->lco_b, c->s2_facc, c->s2_coef, c->s2_facc0, c->v_inst};
     for (size_t q = 0; q < sizeof ptrs / sizeof ptrs[0]; ++q) free(ptrs[q]);
     s2_scratch* sc = (s2_scratch*)c->s2_scr;
     for (int t = 0; t < c->nthr; ++t) { free(sc[t].buf); free(sc[t].C.qh); free(sc[t].C.qb); free(sc[t].C.qht); free(sc[t].C.qbt); }
@@ -1130,25 +1240,45 @@ static void s2_free(uo_ctx* c) {
  * invalidates them every call, :479; S2CN2 only when they are not ready, :480-484), reconstruct,
  * evaluate every face, and publish the face fluxes times the face length into the face arrays
  * ComputeResidual reads. */
+static void s2_publish(uo_ctx* c);
+static int s2_evaluate(uo_ctx* c, double dt, int coef);
 static int s2_evolution_core(uo_ctx* c, double dt, int rebuild_targets) {
-    const uo_params* p = &c->p;
-    int nx = p->nx, ny = p->ny, nv = p->nvel;
     int nthr = g_threads < c->nthr ? g_threads : c->nthr;
     s2_alloc(c);
-    c->dt = dt;
     memset(c->cell_err, 0, sizeof(int) * c->nc);
-    s2_arg a = {c, c->cell_err};
     if (rebuild_targets) {
         s2tg_arg t = {c, c->cell_err, c->W, c->s2_mh, c->s2_mb, c->s2_kxh, c->s2_kxb, c->s2_kyh, c->s2_kyb, c->s2_kappa};
         par_for(c->nc, s2_target_body, &t, nthr);
         int e = s2_first_error(c);
         if (e) return e;
     }
+    int e = s2_evaluate(c, dt, 0);
+    if (e) return e;
+    s2_publish(c);
+    return 0;
+}
+
+/* compute_flux (mod_S2D1.f90:632-959) of the current state into the face accumulators: the
+ * reconstruction, every interior face and the walls; with coef, also the leading and time coefficients
+ * of every face (its optional leading_* / time_* / lower0* / lowerK* outputs) */
+static int s2_evaluate(uo_ctx* c, double dt, int coef) {
+    int nthr = g_threads < c->nthr ? g_threads : c->nthr;
+    s2_alloc(c);
+    c->dt = dt;
+    memset(c->cell_err, 0, sizeof(int) * c->nc);
+    s2_arg a = {c, c->cell_err, coef};
     int e;
     par_for(c->nc, s2_recon_body, &a, nthr);
     if ((e = s2_first_error(c))) return e;
     par_for(c->nc, s2_face_body, &a, nthr);
-    if ((e = s2_first_error(c))) return e;
+    return s2_first_error(c);
+}
+
+/* the face accumulators into the face arrays ComputeResidual reads, times the face lengths
+ * (S2NativeEvolution's map, mod_S2NativeAdapter.f90:545-594) */
+static void s2_publish(uo_ctx* c) {
+    const uo_params* p = &c->p;
+    int nx = p->nx, ny = p->ny, nv = p->nvel;
     const size_t st = 2 * (size_t)nv + 4;
     for (int j = 0; j < ny; ++j)
         for (int i = 0; i < nx; ++i) {
@@ -1175,7 +1305,6 @@ static int s2_evolution_core(uo_ctx* c, double dt, int rebuild_targets) {
                 for (int m = 0; m < 4; ++m) c->fyLw[(size_t)i * 4 + m] = c->fyRw[(size_t)i * 4 + m] = lw[2 * nv + m] * p->dx;
             }
         }
-    return 0;
 }
 
 int uo_s2_evolution(uo_ctx* c, double dt) { return s2_evolution_core(c, dt, 1); }
@@ -1387,6 +1516,271 @@ static void s2_cn_body(void* vp, int cc, int tid) {
     d[3] = lo_h; d[4] = hi_h; d[5] = lo_b; d[6] = hi_b;
 }
 
+/* ---------------------------------------------------------------- research wall variants */
+
+static const double s2_tau0 = 0.1;   /* the frozen relaxation time of W2R's predictor, mod_S2D1.f90:32 */
+
+/* the option checks of mod_ImportPara.f90:455-471 and :516-533 for the S2CN2 Couette case; 200 is the
+ * reference's AbortInvalidImplicitOption code */
+static int s2_variant_check(const uo_params* p) {
+    if (p->s2_time_centered && !p->s2_kinetic_wall) return 200;        /* W2 type1 requires centered=0 */
+    if (p->s2_face_time && !p->s2_time_centered) return 200;          /* W1D requires the W1T midpoint wall */
+    if (p->s2_shared_predictor &&
+        (p->s2_kinetic_wall || p->ck != 1 || p->pr != 1.0 || p->s2_time_centered || p->s2_face_time))
+        return 200;                                                    /* W2R: flat type1 BGK only */
+    return 0;
+}
+
+static void s2v_alloc(uo_ctx* c) {
+    const size_t nc = (size_t)c->nc, nv = (size_t)c->p.nvel;
+    if (!c->s2_facc0) c->s2_facc0 = (double*)calloc(nc * 3 * (2 * nv + 4), sizeof(double));
+    if (!c->v_inst) c->v_inst = (double*)calloc(nc * 3 * 2 * nv, sizeof(double));
+}
+
+/* one face's reconstructed value of field f (0 h, 1 b) at Gauss node g on side s of cell cc */
+static inline double s2_face_value(uo_ctx* c, int cc, int k, int f, int s, int g) {
+    return s2_rec(c, cc, k)[f * 12 + s * 3 + g];
+}
+
+/* the unchanged instantaneous upwind transport flux of the current reconstruction at the right x face
+ * and (below the top row) the top y face of every cell (s2w1d_instantaneous_flux, mod_S2D1.f90:1052-1095;
+ * s2w2r_instantaneous, :1098-1150), into v_inst slots 0 and 1 */
+static void s2_inst_faces(uo_ctx* c) {
+    const int nx = c->p.nx, ny = c->p.ny, nv = c->p.nvel;
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const int cc = j * nx + i, ir = j * nx + (i + 1) % nx, up = cc + nx;
+            double* xi = c->v_inst + (size_t)cc * 3 * 2 * nv;
+            double* yi = xi + 2 * (size_t)nv;
+            for (int k = 0; k < 2 * nv; ++k) { xi[k] = 0.0; yi[k] = 0.0; }
+            for (int g = 0; g < 3; ++g)
+                for (int k = 0; k < nv; ++k) {
+                    const int xl = c->u[k] >= 0.0;
+                    const double rh = xl ? s2_face_value(c, cc, k, 0, 1, g) : s2_face_value(c, ir, k, 0, 0, g);
+                    const double rb = xl ? s2_face_value(c, cc, k, 1, 1, g) : s2_face_value(c, ir, k, 1, 0, g);
+                    xi[k] = xi[k] + s2_gw[g] * c->u[k] * rh;
+                    xi[nv + k] = xi[nv + k] + s2_gw[g] * c->u[k] * rb;
+                    if (j < ny - 1) {
+                        const int yl = c->v[k] >= 0.0;
+                        const double sh = yl ? s2_face_value(c, cc, k, 0, 3, g) : s2_face_value(c, up, k, 0, 2, g);
+                        const double sb = yl ? s2_face_value(c, cc, k, 1, 3, g) : s2_face_value(c, up, k, 1, 2, g);
+                        yi[k] = yi[k] + s2_gw[g] * c->v[k] * sh;
+                        yi[nv + k] = yi[nv + k] + s2_gw[g] * c->v[k] * sb;
+                    }
+                }
+        }
+}
+
+/* the reconstruction of the state (h, b) into s2_rec, the accepted state staying in place */
+static int s2_recon_of(uo_ctx* c, double* h, double* b) {
+    int nthr = g_threads < c->nthr ? g_threads : c->nthr;
+    double *h0 = c->h, *b0 = c->b;
+    c->h = h;
+    c->b = b;
+    memset(c->cell_err, 0, sizeof(int) * c->nc);
+    s2_arg a = {c, c->cell_err, 0};
+    par_for(c->nc, s2_recon_body, &a, nthr);
+    c->h = h0;
+    c->b = b0;
+    return s2_first_error(c);
+}
+
+/* the corrected micro flux of one face: f + dt (instantaneous - leading) - dt^2/2 time, in the two
+ * groupings the reference writes (W1D: 0.5*dt**2, W2R: 0.5*dt*dt) */
+static inline double s2_correct(double f, double inst, double lead, double time, double dt) {
+    return f + dt * (inst - lead) - 0.5 * (dt * dt) * time;
+}
+
+/* S2W1PredictMidpointWall (mod_S2NativeAdapter.f90:605-685), with the W1D face correction (:660-680):
+ * an isolated half step of the accepted state (compute_flux at dt/2 with the kinetic walls, the
+ * transport, advance_step's CN collision at dt/2) predicts the state at t + dt/2; the walls are then
+ * re-evaluated there at the full dt (s2w1_compute_wall_flux, mod_S2D1.f90:1000-1048) and replace the
+ * official walls.  W1D also moves every interior face's leading-order flux to the midpoint:
+ * f + dt (f_inst(mid) - f_lead) - dt^2/2 f_time, and re-takes its macro flux.  A failure anywhere is the
+ * reference's abort 449. */
+static int s2w1t_predict(uo_ctx* c, double dt) {
+    const uo_params* p = &c->p;
+    const int nx = p->nx, ny = p->ny, nv = p->nvel, nc = c->nc;
+    const int nthr = g_threads < c->nthr ? g_threads : c->nthr;
+    const size_t st = 2 * (size_t)nv + 4;
+    const double half = 0.5 * dt;
+    s2v_alloc(c);
+    cn_alloc(c);
+    memcpy(c->s2_facc0, c->s2_facc, sizeof(double) * (size_t)nc * 3 * st);
+    if (s2_evaluate(c, half, 0)) return 449;
+    /* the transport of the accepted state with the half-step fluxes (:630-647) */
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const int cc = j * nx + i, im = j * nx + (i + nx - 1) % nx;
+            const double* xr = c->s2_facc + (size_t)cc * 3 * st;
+            const double* xl = c->s2_facc + (size_t)im * 3 * st;
+            const double* yt = xr + st;
+            const double* yb = j == 0 ? xr + 2 * st : c->s2_facc + (size_t)(cc - nx) * 3 * st + st;
+            for (int m = 0; m < 4; ++m) {
+                double w = c->W[cc * 4 + m] - (xr[2 * nv + m] - xl[2 * nv + m]) / p->dx;
+                c->cn_wn[cc * 4 + m] = w - (yt[2 * nv + m] - yb[2 * nv + m]) / p->dy;
+            }
+            for (int k = 0; k < nv; ++k) {
+                const size_t q = (size_t)cc * nv + k;
+                double sh = c->h[q] - (xr[k] - xl[k]) / p->dx, sb = c->b[q] - (xr[nv + k] - xl[nv + k]) / p->dx;
+                c->cn_hs[q] = sh - (yt[k] - yb[k]) / p->dy;
+                c->cn_bs[q] = sb - (yt[nv + k] - yb[nv + k]) / p->dy;
+            }
+        }
+    /* advance_step on the stream state at dt/2 (mod_S2D1.f90:1302-1435): targets, CN collision, gates */
+    memset(c->cell_err, 0, sizeof(int) * nc);
+    s2tg_arg t = {c, c->cell_err, c->cn_wn, c->cn_mh, c->cn_mb, c->cn_kxh, c->cn_kxb, c->cn_kyh, c->cn_kyb, c->cn_kappa};
+    par_for(nc, s2_target_body, &t, nthr);
+    if (s2_first_error(c)) return 449;
+    cn_arg ca = {c, half};
+    par_for(nc, s2_cn_body, &ca, nthr);
+    if (s2_first_error(c)) return 449;
+    double cnres = 0.0, mmerr = 0.0;
+    int fin = 1;
+    for (int cc = 0; cc < nc; ++cc) {
+        cnres = fmax(cnres, c->cn_cell[(size_t)cc * UO_CN_CELL + 1]);
+        mmerr = fmax(mmerr, c->cn_cell[(size_t)cc * UO_CN_CELL + 2]);
+    }
+    for (size_t q = 0; q < (size_t)nc * 4; ++q) fin &= isfinite(c->cn_wn[q]);
+    for (size_t q = 0; q < (size_t)nc * nv; ++q) fin &= isfinite(c->cn_hn[q]) && isfinite(c->cn_bn[q]);
+    if (!fin || cnres > S2_GATE || mmerr > S2_GATE) return 449;
+    /* the predicted state's reconstruction; its kinetic walls at the full dt replace the official ones */
+    if (s2_recon_of(c, c->cn_hn, c->cn_bn)) return 449;
+    memcpy(c->s2_facc, c->s2_facc0, sizeof(double) * (size_t)nc * 3 * st);
+    s2_scratch* S = s2_scr(c, 0);
+    double *hin = S->buf + 42 * (size_t)nv, *bin = hin + nv, *fh = bin + nv, *fb = fh + nv;
+    for (int i = 0; i < nx; ++i)
+        for (int t2 = 0; t2 < 2; ++t2) {
+            const int cc = t2 == 0 ? i : (ny - 1) * nx + i, side = t2 == 0 ? 2 : 3;
+            double* acc = c->s2_facc + (size_t)cc * 3 * st + (size_t)(t2 == 0 ? 2 : 1) * st;
+            for (size_t k = 0; k < st; ++k) acc[k] = 0.0;
+            for (int g = 0; g < 3; ++g) {
+                for (int k = 0; k < nv; ++k) { hin[k] = s2_face_value(c, cc, k, 0, side, g); bin[k] = s2_face_value(c, cc, k, 1, side, g); }
+                double fw[4];
+                if (!s2w1_wall_node(c, t2 == 0 ? -1 : 1, dt, hin, bin, p->wall_ux[t2], 0.5 * p->wall_tnative[t2], fh, fb, fw))
+                    return 449;
+                for (int k = 0; k < nv; ++k) { acc[k] = acc[k] + s2_gw[g] * fh[k]; acc[nv + k] = acc[nv + k] + s2_gw[g] * fb[k]; }
+                for (int m = 0; m < 4; ++m) acc[2 * nv + m] = acc[2 * nv + m] + s2_gw[g] * fw[m];
+            }
+        }
+    if (!p->s2_face_time) return 0;
+    s2_inst_faces(c);
+    for (int j = 0; j < ny; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const int cc = j * nx + i;
+            for (int f = 0; f < (j < ny - 1 ? 2 : 1); ++f) {
+                double* a = c->s2_facc + (size_t)cc * 3 * st + (size_t)f * st;
+                const double* in = c->v_inst + ((size_t)cc * 3 + f) * 2 * nv;
+                const double* cf = c->s2_coef + ((size_t)cc * 3 + f) * 4 * nv;
+                for (int k = 0; k < nv; ++k) {
+                    a[k] = s2_correct(a[k], in[k], cf[k], cf[2 * nv + k], dt);
+                    a[nv + k] = s2_correct(a[nv + k], in[nv + k], cf[nv + k], cf[3 * nv + k], dt);
+                }
+                if (!s2_moment(nv, a, a + nv, c->u, c->v, c->w, a + 2 * nv)) return 449;
+            }
+        }
+    return 0;
+}
+
+/* s2w2r_correct (mod_S2D1.f90:1152-1244): W2R's shared predictor.  From compute_flux's leading
+ * coefficients a half step of transport and BGK relaxation with the frozen tau0 predicts the state at
+ * t + dt/2 (its moment gate 2e-12); the instantaneous upwind faces and the instantaneous multiscale walls
+ * there replace every face's leading-order flux: f + dt (f_inst - f_lead) - dt^2/2 f_time, the walls
+ * included, whose mass flux must then vanish (gate 2e-12); every macro flux is re-taken.  A failure is
+ * the reference's abort 456. */
+static int s2w2r_correct(uo_ctx* c, double dt) {
+    const uo_params* p = &c->p;
+    const int nx = p->nx, ny = p->ny, nv = p->nvel, nc = c->nc, ck = p->ck;
+    const size_t st = 2 * (size_t)nv + 4;
+    s2v_alloc(c);
+    cn_alloc(c);
+    double** T = scratch_t(c, 0);
+    double *dlh = T[0], *dlb = T[1];
+    double diag1 = 0.0;
+    int lok = 1;
+    /* the predictor (:1175-1193): ws, hs, bs into cn_wn, cn_hn, cn_bn */
+    for (int j = 0; j < ny && lok; ++j)
+        for (int i = 0; i < nx; ++i) {
+            const int cc = j * nx + i, im = j * nx + (i + nx - 1) % nx;
+            const double* x0 = c->s2_coef + (size_t)cc * 3 * 4 * nv;
+            const double* x0m = c->s2_coef + (size_t)im * 3 * 4 * nv;
+            const double* y0 = x0 + 4 * (size_t)nv;
+            const double* y0l = j == 0 ? x0 + 8 * (size_t)nv : c->s2_coef + ((size_t)(cc - nx) * 3 + 1) * 4 * nv;
+            for (int k = 0; k < nv; ++k) {
+                dlh[k] = -(x0[k] - x0m[k]) / p->dx;
+                dlb[k] = -(x0[nv + k] - x0m[nv + k]) / p->dx;
+                dlh[k] = dlh[k] - (y0[k] - y0l[k]) / p->dy;
+                dlb[k] = dlb[k] - (y0[nv + k] - y0l[nv + k]) / p->dy;
+            }
+            double mom[4];
+            if (!s2_moment(nv, dlh, dlb, c->u, c->v, c->w, mom)) return 456;
+            double* ws = c->cn_wn + cc * 4;
+            for (int m = 0; m < 4; ++m) ws[m] = c->W[cc * 4 + m] + 0.5 * dt * mom[m];
+            for (int k = 0; k < nv; ++k) {
+                const size_t q = (size_t)cc * nv + k;
+                c->cn_hn[q] = c->h[q] + 0.5 * dt * (dlh[k] + (c->s2_mh[q] - c->h[q]) / s2_tau0);
+                c->cn_bn[q] = c->b[q] + 0.5 * dt * (dlb[k] + (c->s2_mb[q] - c->b[q]) / s2_tau0);
+            }
+            double rho, ux, vy, th, pp;
+            if (!s2_primitive(ws, ck, &rho, &ux, &vy, &th, &pp)) { lok = 0; break; }
+            if (!s2_moment(nv, c->cn_hn + (size_t)cc * nv, c->cn_bn + (size_t)cc * nv, c->u, c->v, c->w, mom)) return 456;
+            double mx = 0.0, sc = 0.0;
+            for (int m = 0; m < 4; ++m) { mx = fmax(mx, fabs(mom[m] - ws[m])); sc = fmax(sc, fabs(ws[m])); }
+            diag1 = fmax(diag1, mx / fmax(1.0, sc));
+        }
+    int fin = 1;
+    for (size_t q = 0; q < (size_t)nc * nv; ++q) fin &= isfinite(c->cn_hn[q]) && isfinite(c->cn_bn[q]);
+    if (!lok || diag1 > S2_GATE || !fin) return 456;
+    /* the instantaneous faces and walls at the predictor (s2w2r_instantaneous) */
+    if (s2_recon_of(c, c->cn_hn, c->cn_bn)) return 456;
+    s2_inst_faces(c);
+    s2_scratch* S = s2_scr(c, 0);
+    double *hin = S->buf + 42 * (size_t)nv, *bin = hin + nv, *fh = bin + nv, *fb = fh + nv;
+    for (int i = 0; i < nx; ++i)
+        for (int t2 = 0; t2 < 2; ++t2) {
+            const int cc = t2 == 0 ? i : (ny - 1) * nx + i, side = t2 == 0 ? 2 : 3;
+            double* in = c->v_inst + ((size_t)cc * 3 + (t2 == 0 ? 2 : 1)) * 2 * nv;
+            for (int k = 0; k < 2 * nv; ++k) in[k] = 0.0;
+            for (int g = 0; g < 3; ++g) {
+                for (int k = 0; k < nv; ++k) { hin[k] = s2_face_value(c, cc, k, 0, side, g); bin[k] = s2_face_value(c, cc, k, 1, side, g); }
+                double fw[4];
+                if (!s2w2_inst_node(c, 0, t2 == 0 ? -1 : 1, hin, bin, p->wall_ux[t2], 0.5 * p->wall_tnative[t2], fh, fb, fw))
+                    return 456;
+                for (int k = 0; k < nv; ++k) { in[k] = in[k] + s2_gw[g] * fh[k]; in[nv + k] = in[nv + k] + s2_gw[g] * fb[k]; }
+            }
+        }
+    /* the corrected faces (:1214-1233): every x face, every y face with the top wall, the bottom wall */
+    double diag6 = 0.0;
+    fin = 1;
+    for (int cc = 0; cc < nc; ++cc) {
+        const int j = cc / nx;
+        for (int f = 0; f < 3; ++f) {
+            if (f == 2 && j != 0) continue;
+            double* a = c->s2_facc + (size_t)cc * 3 * st + (size_t)f * st;
+            const double* in = c->v_inst + ((size_t)cc * 3 + f) * 2 * nv;
+            const double* cf = c->s2_coef + ((size_t)cc * 3 + f) * 4 * nv;
+            for (int k = 0; k < nv; ++k) {
+                a[k] = s2_correct(a[k], in[k], cf[k], cf[2 * nv + k], dt);
+                a[nv + k] = s2_correct(a[nv + k], in[nv + k], cf[nv + k], cf[3 * nv + k], dt);
+                if (f < 2) fin &= isfinite(a[k]) && isfinite(a[nv + k]);
+            }
+            if (f == 2 || (f == 1 && j == ny - 1)) {
+                double mom[4];
+                if (!s2_moment(nv, a, a + nv, c->u, c->v, c->w, mom)) return 456;
+                diag6 = fmax(diag6, fabs(mom[0]));
+            }
+        }
+    }
+    if (diag6 > S2_GATE || !fin) return 456;
+    for (int cc = 0; cc < nc; ++cc)
+        for (int f = 0; f < 3; ++f) {
+            if (f == 2 && cc >= nx) continue;
+            double* a = c->s2_facc + (size_t)cc * 3 * st + (size_t)f * st;
+            if (!s2_moment(nv, a, a + nv, c->u, c->v, c->w, a + 2 * nv)) return 456;
+        }
+    return 0;
+}
+
 /* One S2CN2 step of the explicit high-order method (TimeStep; S2NativeEvolution with the targets
  * kept between steps, mod_S2NativeAdapter.f90:469-490; ComputeResidual; S2NativeApplyUpdate,
  * :867-940, with advance_step on the stream state, mod_S2D1.f90:1302-1435): the proposal
@@ -1415,7 +1809,12 @@ int uo_s2cn2_step(uo_ctx* c, double* out, int nout) {
         if ((e = s2_first_error(c))) return e;
         c->s2_ready = 1;
     }
-    if ((e = s2_evolution_core(c, dt, 0))) return e;
+    if ((e = s2_variant_check(p))) return e;
+    if ((e = s2_evaluate(c, dt, p->s2_face_time || p->s2_shared_predictor))) return e;
+    if (p->s2_shared_predictor && (e = s2w2r_correct(c, dt))) return e;
+    if (p->s2_time_centered && (e = s2w1t_predict(c, dt))) return e;
+    c->dt = dt;
+    s2_publish(c);
     if ((e = uo_s2_compute_residual(c, dt, 0))) return e;
     /* the stream state (S2NativeApplyUpdate :884-890) */
     for (int cc = 0; cc < nc; ++cc) {

@@ -16,7 +16,7 @@ CSRC = os.path.join(HERE, "csrc")
 OBJ = os.path.join(ROOT, "_build", "ugks_b200")
 LIB = os.path.join(HERE, "libugks_b200.so")
 SOURCES = ["ugks_lo.cu", "ugks_implicit.cu", "ugks_s2.cu", "ugks_s2cn2.cu", "ugks_batch.cu", "ugks_capi.cu",
-           "ugks_noalloc.cu", "ugks_s2_adjoint.cu"]
+           "ugks_noalloc.cu", "ugks_s2_adjoint.cu", "ugks_s2_walls.cu"]
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 FLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "--expt-relaxed-constexpr",

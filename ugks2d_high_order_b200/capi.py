@@ -54,6 +54,8 @@ class UgksParams(ctypes.Structure):
         ("ncfl", ctypes.c_double), ("nslab", ctypes.c_int), ("mass_rescale", ctypes.c_int),
         ("macro_sweeps", ctypes.c_int),
         ("residual_tol", ctypes.c_double), ("moment_tol", ctypes.c_double), ("min_alpha", ctypes.c_double),
+        ("s2_kinetic_wall", ctypes.c_int), ("s2_time_centered", ctypes.c_int), ("s2_face_time", ctypes.c_int),
+        ("s2_shared_predictor", ctypes.c_int),
     ]
 
 

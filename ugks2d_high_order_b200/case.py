@@ -36,6 +36,11 @@ class CouetteCase:
     moment_tol: float = 1.0e-12      # Implicit_MomentTol
     min_alpha: float = 1.0e-6        # Implicit_MinAlpha
     max_iter: int = 3000             # MAX_ITER (the loop cap; 200000 in the explicit case)
+    # the research S2CN2 wall variants (mod_ImportPara.f90:88-93), off in every delivered case
+    flux_wall: int = 1               # FluxWall_type: 1 multiscale wall (s2w2), 0 free-streaming wall (s2w1)
+    s2w1_time_centered: int = 0      # S2W1_time_centered: W1T midpoint wall (needs FluxWall_type 0)
+    s2w1d_face_time: int = 0         # S2W1D_face_time_consistent: W1D face correction (needs W1T)
+    s2w2r_shared_predictor: int = 0  # S2W2R_shared_predictor: W2R (FluxWall_type 1, ck 1, Pr 1)
 
     @property
     def gamma(self):

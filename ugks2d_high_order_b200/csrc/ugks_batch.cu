@@ -133,6 +133,9 @@ extern "C" int ugks_batch_create(int n, const ugks_instance_desc* desc, int devi
         if (!desc[i].u || !desc[i].v || !desc[i].w || p->method != UGKS_METHOD_S2CN2 || p->nx < 1 || p->ny < 6 ||
             p->nvel < 1 || p->nvel > kMaxVel || !(p->dx > 0) || !(p->dy > 0) || p->ck < 1)
             return UGKS_EINVAL;
+        // the research wall variants run on single contexts only
+        if (p->s2_kinetic_wall || p->s2_time_centered || p->s2_face_time || p->s2_shared_predictor)
+            return UGKS_EUNSUPPORTED;
     }
     BCK(cudaSetDevice(device));
     ugks_batch* b = new (std::nothrow) ugks_batch();

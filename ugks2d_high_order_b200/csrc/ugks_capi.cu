@@ -86,6 +86,11 @@ struct ugks_ctx {
     int cn_reject_at = 0;          // step of the next sequence forced to fail its conservation gate
     int cn_stage = 0;              // per-operator S2CN2 step: 1 after the evolution, 2 after the residual
     cudaGraphExec_t cgraph = nullptr;
+    // the research wall variants of an S2CN2 context (ugks_s2_walls.cu)
+    bool has_var = false;
+    CnVariant V{};
+    double* vmem = nullptr;
+    unsigned* vflags = nullptr;    // [0] the predictor's last-CTA counter
     // S2CN2 adjoint (ugks_s2cn2_forward_checkpointed / ugks_s2cn2_backward / ugks_s2cn2_step_vjp)
     double* amem = nullptr;        // checkpoints (held from the checkpointed forward to the context's end)
     double* bmem = nullptr;        // segment slots, cotangent sets, adjoint work (reserved by the backward)
@@ -137,6 +142,8 @@ extern "C" int ugks_status_reference_code(unsigned st) {
     if (st & ST_NONFINITE_FLUX) return 13;
     if (st & ST_NONFINITE_STATE) return 4;
     if (st & ST_STEP_REJECTED) return 203;
+    if (st & ST_W1T_PREDICTOR) return 449;
+    if (st & ST_W2R) return 456;
     if (st & ST_MOMENT_GATE) return 451;
     if (st & ST_ALPHA) return 433;
     if (st & ST_TIMEOUT) return 999;
@@ -154,9 +161,24 @@ static int collect_status(ugks_ctx* c) {
     return st ? UGKS_ENUMERIC : UGKS_OK;
 }
 
+// The research S2CN2 wall variants a context accepts: S2CN2 only, and the combinations the reference's
+// option checks admit (mod_ImportPara.f90:455-471, :527-528): W1T on the kinetic wall, W1D with W1T, W2R
+// alone on the multiscale wall with ck = 1 and Pr = 1.
+static int check_wall_variant(const ugks_params* p) {
+    const int k = p->s2_kinetic_wall, t = p->s2_time_centered, d = p->s2_face_time, r = p->s2_shared_predictor;
+    if ((k | t | d | r) & ~1) return UGKS_EINVAL;
+    if (!(k | t | d | r)) return UGKS_OK;
+    if (p->method != UGKS_METHOD_S2CN2) return UGKS_EUNSUPPORTED;
+    if (t && !k) return UGKS_EINVAL;
+    if (d && !t) return UGKS_EINVAL;
+    if (r && (k || t || d || p->ck != 1 || p->pr != 1.0)) return UGKS_EINVAL;
+    return UGKS_OK;
+}
+
 extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const double* v, const double* w, int device,
                                ugks_ctx** out) {
     if (!p || !u || !v || !w || !out) return UGKS_EINVAL;
+    if (int r = check_wall_variant(p)) return r;
     if (p->nx < 1 || p->ny < 3 || p->nvel < 1 || p->nvel > kMaxVel || !(p->dx > 0) || !(p->dy > 0) ||
         p->ck < 1)
         return UGKS_EINVAL;
@@ -293,6 +315,52 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
             c->Bs[1] = c->Bs[0];
             c->Bs[1].h = m + c_h1; c->Bs[1].b = m + c_b1; c->Bs[1].W = m + c_W1;
         }
+        const LoParams& P = c->P;
+        if (e == cudaSuccess && (P.s2_kinetic || P.s2_midpoint || P.s2_shared)) {
+            // the wall variant's buffers: coefficient outputs, the predictor's dt, face arrays, evaluation
+            // set, stream state and the predicted state, the instantaneous wall node fluxes
+            c->has_var = true;
+            const size_t nfw = (size_t)nx * ny + (size_t)nx * (ny - 1) + 2 * (size_t)nx;
+            size_t vo = 0;
+            auto vtake = [&](size_t n) { size_t o = vo; vo += (n + 31) / 32 * 32; return o; };
+            const bool coef = P.s2_face_time || P.s2_shared, pred = P.s2_midpoint || P.s2_shared;
+            const size_t v_coef = coef ? vtake(nfw * 3 * 4 * nv) : 0;
+            const size_t v_half = vtake(2), v_fxh = vtake(S), v_fxb = vtake(S), v_fxw = vtake((size_t)nc * 4);
+            const size_t v_fyh = vtake(SY), v_fyb = vtake(SY), v_fyw = vtake((size_t)(ny + 1) * nx * 4);
+            const size_t v_wa = vtake((size_t)2 * nx * 3);
+            const size_t v_rec = pred ? vtake(s2_rec_doubles(nx, ny, nv)) : 0;
+            size_t v_tg[6] = {0, 0, 0, 0, 0, 0};
+            if (P.s2_midpoint) for (int t = 0; t < 6; ++t) v_tg[t] = vtake(S);
+            const size_t v_scr = pred ? vtake(s2_scratch_doubles(nx, ny, nv)) : 0;
+            const size_t v_ws = vtake((size_t)nc * 4), v_rh = vtake(S), v_rb = vtake(S), v_cell = vtake((size_t)nc * kCnCell);
+            const size_t v_rep = vtake(kCnReport), v_h = vtake(S), v_b = vtake(S), v_W = vtake((size_t)nc * 4);
+            const size_t v_inst = P.s2_shared ? vtake((size_t)2 * nx * 3 * 2 * nv) : 0;
+            e = cudaMalloc(&c->vmem, vo * sizeof(double));
+            if (e == cudaSuccess) e = cudaMalloc(&c->vflags, 4 * sizeof(unsigned));
+            if (e == cudaSuccess) e = cudaMemsetAsync(c->vmem, 0, vo * sizeof(double), c->stream);
+            if (e == cudaSuccess) e = cudaMemsetAsync(c->vflags, 0, 4 * sizeof(unsigned), c->stream);
+            if (e == cudaSuccess) {
+                double* m = c->vmem;
+                CnVariant& V = c->V;
+                if (coef) { c->T[0].coef = m + v_coef; c->T[1].coef = m + v_coef; }
+                V.half = m + v_half;
+                V.fxh = m + v_fxh; V.fxb = m + v_fxb; V.fxw = m + v_fxw;
+                V.fyh = m + v_fyh; V.fyb = m + v_fyb; V.fyw = m + v_fyw; V.wall_aero = m + v_wa;
+                if (pred) {
+                    V.Sp.rec = m + v_rec;
+                    s2_bind_scratch(V.Sp, m + v_scr, nx, ny, nv);
+                }
+                if (P.s2_midpoint) {
+                    V.Sp.mh = m + v_tg[0]; V.Sp.mb = m + v_tg[1]; V.Sp.kxh = m + v_tg[2];
+                    V.Sp.kxb = m + v_tg[3]; V.Sp.kyh = m + v_tg[4]; V.Sp.kyb = m + v_tg[5];
+                }
+                V.Cp.ws = m + v_ws; V.Cp.rh = m + v_rh; V.Cp.rb = m + v_rb; V.Cp.cell = m + v_cell;
+                V.Cp.report = m + v_rep; V.Cp.ledger = nullptr; V.Cp.wall_raw = nullptr;
+                V.Cp.halt = c->C.halt; V.Cp.counter = c->vflags; V.Cp.accepted = c->vflags + 1; V.Cp.predict = 1;
+                V.h = m + v_h; V.b = m + v_b; V.W = m + v_W;
+                V.inst = P.s2_shared ? m + v_inst : nullptr;
+            }
+        }
     }
     if (e == cudaSuccess) e = cudaStreamSynchronize(c->stream);
     if (e != cudaSuccess) { ugks_ctx_destroy(c); return cuda_fail(e); }
@@ -316,6 +384,8 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->aflags) cudaFree(c->aflags);
     if (c->cmem) cudaFree(c->cmem);
     if (c->cflags) cudaFree(c->cflags);
+    if (c->vmem) cudaFree(c->vmem);
+    if (c->vflags) cudaFree(c->vflags);
     if (c->imem) cudaFree(c->imem);
     if (c->iflags) cudaFree(c->iflags);
     if (c->hstate) cudaFreeHost(c->hstate);
@@ -463,6 +533,11 @@ static int s2_evolution(ugks_ctx* c, bool rebuild_targets) {
         const int which = rebuild_targets ? 1 : 2;
         UGKS_CK(s2_enqueue(which, c->P, c->Bs[0], c->T[0], c->stream, c->stream2, c->ev_fork, c->ev_join));
         c->launches += s2_enqueue_kernels(which);
+        if (c->has_var) {   // the wall variant's part of S2NativeEvolution (mod_S2NativeAdapter.f90:491-540)
+            UGKS_CK(enqueue_s2cn2_variant(c->P, c->Bs[0], c->T[0], c->V, c->stream, c->stream2, c->ev_fork,
+                                          c->ev_join));
+            c->launches += s2cn2_variant_kernels(c->P);
+        }
         r = collect_status(c);
         c->cn_ready = c->cn_ready || (rebuild_targets && r == UGKS_OK);
         c->cn_stage = r == UGKS_OK ? 1 : 0;
@@ -998,7 +1073,7 @@ extern "C" int ugks_s2cn2_report(ugks_ctx* c, double* report) {
 
 static cudaError_t enqueue_cn_step(ugks_ctx* c, int from) {
     return enqueue_s2cn2_step(c->P, c->Bs[from], c->T[from], c->Bs[1 - from], c->T[1 - from], c->C, c->stream,
-                              c->stream2, c->ev_fork, c->ev_join, nullptr);
+                              c->stream2, c->ev_fork, c->ev_join, nullptr, c->has_var ? &c->V : nullptr);
 }
 
 // a pair of steps, set 0 -> set 1 -> set 0, captured once and replayed
@@ -1038,7 +1113,7 @@ extern "C" int ugks_s2cn2_steps(ugks_ctx* c, int nsteps, int* steps_done, double
         for (int q = 0; q < pairs; ++q) UGKS_CK(cudaGraphLaunch(c->cgraph, c->stream));
     }
     if (nsteps % 2) UGKS_CK(enqueue_cn_step(c, 0));
-    c->launches += (long long)kCnStepKernels * nsteps;
+    c->launches += (long long)(kCnStepKernels + (c->has_var ? s2cn2_variant_kernels(c->P) : 0)) * nsteps;
     unsigned acc = 0;
     UGKS_CK(cudaMemcpyAsync(&acc, c->C.accepted, sizeof acc, cudaMemcpyDeviceToHost, c->stream));
     if (report) UGKS_CK(cudaMemcpyAsync(report, c->C.report, kCnReport * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
@@ -1359,7 +1434,7 @@ int forward_recorded(ugks_ctx* c, int len, int* done) {
 
 extern "C" int ugks_s2cn2_forward_checkpointed(ugks_ctx* c, int nsteps, int every, double* outputs) {
     if (!c || nsteps < 1 || every < 1) return UGKS_EINVAL;
-    if (!c->cmem) return UGKS_EUNSUPPORTED;
+    if (!c->cmem || c->has_var) return UGKS_EUNSUPPORTED;   // the adjoint transposes the delivered walls only
     if (!c->cn_ready) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
     const int nckpt = (nsteps + every - 1) / every, seglen = every < nsteps ? every : nsteps;
@@ -1389,7 +1464,7 @@ extern "C" int ugks_s2cn2_forward_checkpointed(ugks_ctx* c, int nsteps, int ever
 extern "C" int ugks_s2cn2_backward(ugks_ctx* c, const double* seed, double* grad, double* gh0, double* gb0,
                                    double* gW0) {
     if (!c || !seed) return UGKS_EINVAL;
-    if (!c->cmem) return UGKS_EUNSUPPORTED;
+    if (!c->cmem || c->has_var) return UGKS_EUNSUPPORTED;   // the adjoint transposes the delivered walls only
     if (c->adj_nsteps < 1) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
     if (int r = collect_status(c)) return r;
@@ -1468,7 +1543,7 @@ extern "C" int ugks_s2cn2_backward(ugks_ctx* c, const double* seed, double* grad
 extern "C" int ugks_s2cn2_step_vjp(ugks_ctx* c, const double* gh, const double* gb, const double* gW, const double* seed,
                                    double* gh_in, double* gb_in, double* gW_in, double* grad) {
     if (!c) return UGKS_EINVAL;
-    if (!c->cmem) return UGKS_EUNSUPPORTED;
+    if (!c->cmem || c->has_var) return UGKS_EUNSUPPORTED;   // the adjoint transposes the delivered walls only
     if (!c->cn_ready) return UGKS_EINVAL;
     UGKS_CK(cudaSetDevice(c->device));
     if (int r = adj_reserve_bwd(c, c->adj_capacity_seg > 0 ? c->adj_capacity_seg : 1)) return r;

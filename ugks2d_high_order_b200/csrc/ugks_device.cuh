@@ -28,6 +28,8 @@ enum : unsigned {
     ST_ALPHA = 1u << 7,          // implicit admissible alpha not found
     ST_MOMENT_GATE = 1u << 8,    // implicit moment gate (Implicit_MomentTol)
     ST_STEP_REJECTED = 1u << 9,  // 203: an S2CN2 step failed its cnres / mmerr / conservation gates
+    ST_W1T_PREDICTOR = 1u << 11, // 449: the W1T midpoint predictor (or its W1D faces) failed
+    ST_W2R = 1u << 12,           // 456: the W2R shared predictor or its corrected faces failed
 };
 
 struct Prim { double r, U, V, L; };   // [rho, U, V, lambda = 1/T_native]

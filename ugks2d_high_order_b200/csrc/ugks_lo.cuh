@@ -20,6 +20,8 @@ struct LoParams {
     double fixed_dt;         // > 0: Time_global_fixed
     double inv_dx, inv_dy;   // 1/dx, 1/dy for the slope stencils
     double inv_area;         // 1/area when area is a power of two (then x/area == x*inv_area exactly), else 0
+    // the research S2CN2 wall variants (ugks_params): kinetic walls, W1T midpoint walls, W1D, W2R
+    int s2_kinetic, s2_midpoint, s2_face_time, s2_shared;
 };
 
 // x / area, as a multiplication when that is exact (area a power of two: both operations round the
@@ -114,6 +116,10 @@ inline LoParams make_lo_params(const ugks_params& p, double umax, double vmax) {
     P.fixed_dt = p.fixed_dt;
     P.inv_dx = 1.0 / p.dx;
     P.inv_dy = 1.0 / p.dy;
+    P.s2_kinetic = p.s2_kinetic_wall != 0;
+    P.s2_midpoint = p.s2_time_centered != 0;
+    P.s2_face_time = p.s2_face_time != 0;
+    P.s2_shared = p.s2_shared_predictor != 0;
     return P;
 }
 

@@ -353,7 +353,7 @@ __global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffer
     C.jac = s_jac[threadIdx.x >> 5];
     WMke M;
     bool ok = w_closure(P, B, w0, C) && w_make_mke(P, B, w0, C, M);
-    double q0x = 0.0, q0y = 0.0, tdl[4], tdr[4], tdt[4], tdm[4], wt[4], mt[5];
+    double q0x = 0.0, q0y = 0.0, tdl[4], tdr[4], tdt[4], tdm[4], wt[4], mt[5], tau = 0.0;
     if (ok) {   // q0 = heat(w0, f0 - analytic Maxwellian of w0)
         const double nrho = w0[0], nu = w0[1] / w0[0], nvv = w0[2] / w0[0];
         const double temp = 4.0 * (w0[3] / w0[0] - 0.5 * (nu * nu + nvv * nvv)) / (double)(ck + 2);
@@ -409,7 +409,6 @@ __global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffer
 #pragma unroll
         for (int m = 0; m < 4; ++m) wt[m] = -acc[12 + m];
         ok = ok && s2_solve4(C.jac, wt, tdm);
-        double tau = 0.0;
         ok = ok && s2_tau(P, w0, tau);
         const double ex = exp(-dt / tau);
         mt[3] = tau * (1.0 - ex);
@@ -433,6 +432,7 @@ __global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffer
             for (int m = 0; m < 5; ++m) o[35 + m] = mt[m];
 #pragma unroll
             for (int m = 0; m < 16; ++m) o[44 + m] = C.jac[m];
+            o[60] = tau;
         } else {
             set_status(B.status, ST_NONFINITE_FLUX);
         }
@@ -507,6 +507,14 @@ __global__ void __launch_bounds__(256, 3) k_s2_face_flux(LoParams P, LoBuffers B
             outh[sl_.k] = fhv;
             outb[sl_.k] = fbv;
             if (!(isfinite(fhv) && isfinite(fbv))) bad = 1;
+            if (SB.coef) {   // ugks_node's f0_h, f0_b, k_h, k_b (mod_S2D1.f90:501-505)
+                double* cf = SB.coef + (size_t)wid * 4 * nv + sl_.k;
+                const double tau = sc[60];
+                cf[0] = vn * f0h;
+                cf[(size_t)nv] = vn * f0b;
+                cf[2 * (size_t)nv] = vn * ((s0h - f0h) / tau - vn * nh - vt * th_);
+                cf[3 * (size_t)nv] = vn * ((s0b - f0b) / tau - vn * nb - vt * tb_);
+            }
         }
     }
     block_reduce_smem<8, 0>(acc, red, rout);
@@ -553,7 +561,7 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
         return SB.rec[rec_wall(nx, ny, top, i, field, g, nv) + s.k];
     };
     double acc[8];
-    double an[4], at[4], atime[4], mt[5], mxi2 = 0.0, coeff = 0.0, hlx = 0.0, hly = 0.0;
+    double an[4], at[4], atime[4], mt[5], mxi2 = 0.0, coeff = 0.0, hlx = 0.0, hly = 0.0, tau_wall = 0.0;
     if (ok) {
 #pragma unroll
         for (int m = 0; m < 6; ++m) acc[m] = 0.0;
@@ -579,7 +587,6 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
         s2w_auvxi(at, Mu, Mv, Mxi, 0, 1, m2);
         for (int m = 0; m < 4; ++m) sw[m] = -prim_g[0] * (m1[m] + m2[m]);
         s2w_micro_slope(ck, prim_g, sw, atime);
-        double tau_wall = 0.0;
         const double wgg[4] = {wg[0], -wg[2], wg[1], wg[3]};
         ok = s2_tau(P, wgg, tau_wall);
         s2w_time_coeffs(dt, tau_wall, mt);
@@ -590,12 +597,15 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
     }
     // the incident micro flux g_in and the reflected wall Maxwellian of one velocity
     const S2Th tt = s2_th(C.th, ck);
-    auto gin = [&](const WVel& s, double& ginh, double& ginb, double& wallh, double& wallb) {
+    auto gin = [&](const WVel& s, double& ginh, double& ginb, double& wallh, double& wallb, double& mh, double& mb,
+                   double& corrh, double& corrb) {
         const S2Q q = s2_q(tt, s.u, s.v);
-        const double mh = q.qh, mb = q.qb;
+        mh = q.qh;
+        mb = q.qb;
         wallh = mh / prim_g[0];
         wallb = mb / prim_g[0];
-        double corrh = 0.0, corrb = 0.0;
+        corrh = 0.0;
+        corrb = 0.0;
         if (P.pr != 1.0) {
             const double vn = s.v, vt = -s.u + ux, v2 = vn * vn + vt * vt;
             const double qdot = vn * hlx + vt * hly, shh = 2.0 * lambda * v2 - 4.0;
@@ -621,8 +631,8 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
         acc[0] = acc[1] = 0.0;
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
-            double ginh, ginb, wallh, wallb;
-            gin(s, ginh, ginb, wallh, wallb);
+            double ginh, ginb, wallh, wallb, mh, mb, ch, cb;
+            gin(s, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
             if (side * s.v > 0.0) acc[0] += s.w * s.v * ginh;
             else acc[1] += dt * s.w * s.v * wallh;
         }
@@ -639,8 +649,8 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
         for (int m = 0; m < 4; ++m) acc[m] = 0.0;
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
-            double ginh, ginb, wallh, wallb, fh, fb;
-            gin(s, ginh, ginb, wallh, wallb);
+            double ginh, ginb, wallh, wallb, mh, mb, ch, cb, fh, fb;
+            gin(s, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
             if (side * s.v > 0.0) { fh = s.v * ginh; fb = s.v * ginb; }
             else { fh = dt * s.v * rhow * wallh; fb = dt * s.v * rhow * wallb; }
             acc[0] += s.w * fh; acc[1] += s.w * (s.u * fh); acc[2] += s.w * (s.v * fh);
@@ -656,6 +666,57 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
         if (lane < 4) SB.nodew[node * 4 + lane] = lane == 0 ? acc[0] : (lane == 1 ? acc[1] : (lane == 2 ? acc[2] : acc[3]));
     }
     ok = __all_sync(0xffffffffu, ok);
+    if (ok && SB.coef) {   // the optional f0_h, f0_b, k_h, k_b outputs (mod_S2MultiscaleWall.f90:155-177)
+        auto qk = [&](const WVel& s, double m, double corr, int fv, int fn, int ft) {
+            return (m + corr - rec(s, fv)) / tau_wall - s.v * rec(s, fn) - s.u * rec(s, ft);
+        };
+        acc[0] = acc[1] = acc[2] = 0.0;
+        for (int r = 0; r < nr; ++r) {
+            const WVel s = wvel(B, nv, r);
+            double ginh, ginb, wallh, wallb, mh, mb, ch, cb;
+            gin(s, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
+            if (side * s.v > 0.0) {
+                acc[0] += s.w * s.v * rec(s, 0);
+                acc[1] += s.w * s.v * qk(s, mh, ch, 0, 2, 3);
+            } else {
+                acc[2] += s.w * s.v * wallh;
+            }
+        }
+        warp_sum_all<3>(acc);
+        const double r0 = -acc[0] / acc[2], r1 = -acc[1] / acc[2];
+        ok = isfinite(r0) && isfinite(r1) && r0 > 0.0;
+        double* cf = SB.coef + node * 4 * nv;
+        acc[0] = acc[1] = 0.0;
+        for (int r = 0; r < nr && ok; ++r) {
+            const WVel s = wvel(B, nv, r);
+            double ginh, ginb, wallh, wallb, mh, mb, ch, cb, c0, c1, c2, c3;
+            gin(s, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
+            if (side * s.v > 0.0) {
+                c0 = s.v * rec(s, 0);
+                c1 = s.v * rec(s, 1);
+                c2 = s.v * qk(s, mh, ch, 0, 2, 3);
+                c3 = s.v * qk(s, mb, cb, 1, 4, 5);
+            } else {
+                c0 = s.v * r0 * wallh;
+                c1 = s.v * r0 * wallb;
+                c2 = s.v * r1 * wallh;
+                c3 = s.v * r1 * wallb;
+            }
+            acc[0] += s.w * c0;
+            acc[1] += s.w * c2;
+            if (s.ok) {
+                cf[s.k] = c0;
+                cf[(size_t)nv + s.k] = c1;
+                cf[2 * (size_t)nv + s.k] = c2;
+                cf[3 * (size_t)nv + s.k] = c3;
+            }
+        }
+        if (ok) {
+            warp_sum_all<2>(acc);
+            ok = fabs(acc[0]) <= 2.0e-12 && fabs(acc[1]) <= 2.0e-12;
+        }
+    }
+    ok = __all_sync(0xffffffffu, ok);
     if (!ok && lane == 0) set_status(B.status, ST_NONFINITE_FLUX);
 }
 
@@ -663,10 +724,10 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
 // length, into the face arrays ComputeResidual reads; the walls' macro fluxes also unscaled into
 // SB.wall_raw, and the walls' (pnn, pnt, qn) into B.wall_aero.  One thread per (face, velocity);
 // threads k < 4 also do the macro flux.
-__global__ void __launch_bounds__(256) k_s2_combine(LoParams P, LoBuffers B, S2Buffers SB) {
+__global__ void __launch_bounds__(256) k_s2_combine(LoParams P, LoBuffers B, S2Buffers SB, int f0) {
     if (eval_cached(B)) return;
     const int nv = P.nvel, nx = P.nx, ny = P.ny, nfx = nx * ny, nf = nfx + nx * (ny - 1);
-    const int fi = blockIdx.y;
+    const int fi = f0 + (int)blockIdx.y;
     const int k = (int)(blockIdx.x * blockDim.x + threadIdx.x);
     if (k >= nv) return;
     const double gw[3] = {5.0 / 18.0, 4.0 / 9.0, 5.0 / 18.0};
@@ -734,6 +795,13 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
         k_s2_init<<<warps(nc), 256, 0, s>>>(P, B, S);
         return cudaGetLastError();
     }
+    if (which == 4) {
+        const dim3 grid((unsigned)((nv + 31) / 32), (unsigned)nc);
+        k_s2_recon1<<<grid, 128, 0, s>>>(P, B, S);
+        cudaError_t e = cudaGetLastError();
+        if (e == cudaSuccess) { k_s2_recon2<<<grid, 256, 0, s>>>(P, B, S); e = cudaGetLastError(); }
+        return e;
+    }
     const int faces = which != 3, targets = which != 2;
     const long long nmacw = (faces ? (long long)nf * 2 : 0) + (targets ? (long long)nc : 0);   // warps
     k_s2_macro<<<(unsigned)((nmacw * 32 + 127) / 128), 128, 0, s>>>(P, B, S, faces, targets);
@@ -762,7 +830,10 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     if (e == cudaSuccess) { k_s2_recon2<<<grid, 256, 0, s>>>(P, B, S); e = cudaGetLastError(); }
     if (e == cudaSuccess) e = cudaEventRecord(fork, s);
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
-    if (e == cudaSuccess) { k_s2_wall_nodes<<<warps(2LL * nx * 3), 256, 0, s2>>>(P, B, S); e = cudaGetLastError(); }
+    if (e == cudaSuccess) {
+        if (P.s2_kinetic) e = launch_s2_w1_walls(P, B, S, s2);
+        else { k_s2_wall_nodes<<<warps(2LL * nx * 3), 256, 0, s2>>>(P, B, S); e = cudaGetLastError(); }
+    }
     if (e == cudaSuccess) e = cudaEventRecord(join, s2);
     if (e == cudaSuccess) {
         if (S.concurrent) k_s2_face_nodes<256, 2><<<warps((long long)nf * 3), 256, 0, s>>>(P, B, S);
@@ -775,11 +846,14 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s, join, 0);
-    if (e == cudaSuccess) {
-        k_s2_combine<<<dim3((unsigned)((nv + 255) / 256), (unsigned)(nf + 2 * nx)), 256, 0, s>>>(P, B, S);
-        e = cudaGetLastError();
-    }
+    if (e == cudaSuccess) e = launch_s2_combine(P, B, S, 0, nf + 2 * nx, s);
     return e;
+}
+
+cudaError_t launch_s2_combine(const LoParams& P, const LoBuffers& B, const S2Buffers& S, int f0, int nfaces,
+                              cudaStream_t s) {
+    k_s2_combine<<<dim3((unsigned)((P.nvel + 255) / 256), (unsigned)nfaces), 256, 0, s>>>(P, B, S, f0);
+    return cudaGetLastError();
 }
 
 }  // namespace ugks

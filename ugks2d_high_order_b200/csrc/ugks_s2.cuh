@@ -47,7 +47,10 @@ struct S2Buffers {
     double* wq;      // [cell][9][4] mean-shifted volume node states
     double* tscal;   // [cell][9][16] volume node scalars (closure theta, directions, primitive)
     double* l1;      // [cell][22][nvel] first-layer WENO values of h and b (k_s2_recon1)
-    double* fscal;   // [interior face][3][48] face-node scalars (k_s2_face_nodes -> k_s2_face_flux)
+    double* fscal;   // [interior face][3][kS2FScal] face-node scalars (k_s2_face_nodes -> k_s2_face_flux)
+    double* coef;    // [face node][f0 h, f0 b, k h, k b][nvel] the leading and time coefficients of every node
+                     // flux (ugks_node's and s2w2_wall_node's optional outputs) for the wall variants that
+                     // correct the faces; nodes as `node` (nullptr: not wanted)
     int concurrent;  // 1: one of many instances on concurrent streams (the batch): the closure kernels
                      // take the CTA shape with more resident warps
 };
@@ -56,7 +59,7 @@ struct S2Buffers {
 // closure directions, [12..15] ux vy lam coeff, [16..31] the closure's moment Jacobian (row-major).
 // Interior face nodes (fscal): [0] ok, [1..4] theta, [5..12] K directions, [13..16] ux vy lam coeff,
 // [17..18] q0, [19..34] left/right/tangential/time directions, [35..39] Mt, [40..43] the time-direction
-// moments wt, [44..59] the closure's moment Jacobian.  The Jacobians serve the adjoint (ugks_s2_adjoint.cu).
+// moments wt, [44..59] the closure's moment Jacobian, [60] the face tau.  The Jacobians serve the adjoint (ugks_s2_adjoint.cu).
 constexpr int kS2TScal = 32;
 constexpr int kS2FScal = 64;
 
@@ -101,14 +104,20 @@ __device__ __forceinline__ bool s2_primitive(const double w[4], int ck, double& 
 
 cudaError_t prepare_s2();
 // which 0: S2 cold start (h, b := discrete closure Maxwellian of W); 1: S2 Evolution (targets of B.W,
-// reconstruction, faces, walls); 2: S2 Evolution with the targets in S kept; 3: targets of B.W into S
+// reconstruction, faces, walls); 2: S2 Evolution with the targets in S kept; 3: targets of B.W into S;
+// 4: the reconstruction of B's h, b into S.rec only
 cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S2Buffers& S, cudaStream_t s,
                        cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join);
 // kernels s2_enqueue(which, ...) launches: the cold start 1; the macro pass, then 2 for the targets
 // (volume nodes, sum) and 6 for the evolution (reconstruction x2, wall nodes, face nodes, face flux,
-// combine)
+// combine); the reconstruction alone 2
 constexpr int s2_enqueue_kernels(int which) {
-    return which == 0 ? 1 : 1 + (which != 2 ? 2 : 0) + (which != 3 ? 6 : 0);
+    return which == 0 ? 1 : which == 4 ? 2 : 1 + (which != 2 ? 2 : 0) + (which != 3 ? 6 : 0);
 }
+// the wall nodes of the kinetic (FluxWall_type 0) wall into S.node / S.nodew (ugks_s2_walls.cu)
+cudaError_t launch_s2_w1_walls(const LoParams& P, const LoBuffers& B, const S2Buffers& S, cudaStream_t s);
+// k_s2_combine over faces [f0, f0 + nfaces) of the face numbering (interior x, interior y, walls)
+cudaError_t launch_s2_combine(const LoParams& P, const LoBuffers& B, const S2Buffers& S, int f0, int nfaces,
+                              cudaStream_t s);
 
 }  // namespace ugks

@@ -262,7 +262,10 @@ __global__ void __launch_bounds__(NT) k_cn_collide(LoParams P, LoBuffers B, S2Bu
         acc[13] = fmax(acc[13], fabs(B.v[k]));
     }
     block_reduce_smem<4, 10>(acc, red, rout);
-    if (tid == 0) {
+    if (tid == 0 && C.predict) {   // a predictor's advance_step: its finiteness and cnres / mmerr gates only
+        if (!(rout[11] == 0.0 && rout[5] <= kCnGate && rout[6] <= kCnGate)) cn_stop(C, B, ST_W1T_PREDICTOR);
+        *C.counter = 0u;
+    } else if (tid == 0) {
         double* R = C.report;
         R[0] = dt;
         R[1] = rout[5]; R[2] = rout[6]; R[3] = rout[4];
@@ -349,12 +352,13 @@ cudaError_t enqueue_cn_apply(const LoParams& P, const LoBuffers& B, const LoBuff
 // [18..21] wall balance after the step, [22] accepted, [23] accepted steps so far.
 cudaError_t enqueue_s2cn2_step(const LoParams& P, const LoBuffers& B, const S2Buffers& T, const LoBuffers& Bo,
                                const S2Buffers& To, const CnBuffers& C, cudaStream_t s, cudaStream_t s2,
-                               cudaEvent_t fork, cudaEvent_t join, long long* launches) {
+                               cudaEvent_t fork, cudaEvent_t join, long long* launches, const CnVariant* V) {
     cudaError_t e = launch_lo_timestep(P, B, s);
     if (e == cudaSuccess) e = s2_enqueue(2, P, B, T, s, s2, fork, join);
+    if (e == cudaSuccess && V) e = enqueue_s2cn2_variant(P, B, T, *V, s, s2, fork, join);
     if (e == cudaSuccess) e = enqueue_cn_stream(P, B, T, C, s);
     if (e == cudaSuccess) e = enqueue_cn_apply(P, B, Bo, To, C, s);
-    if (launches) *launches += kCnStepKernels;
+    if (launches) *launches += kCnStepKernels + (V ? s2cn2_variant_kernels(P) : 0);
     return e;
 }
 

@@ -213,6 +213,10 @@ def config_text(case, velocity_file="velocity_table.dat", nu=None, nv=None, extr
     }
     if case.wall_tnative[1] != case.wall_tnative[0]:
         cp["S2WallTNative"] = list(case.wall_tnative)
+    if case.s2w1_time_centered or case.s2w1d_face_time or case.s2w2r_shared_predictor:
+        cp["S2W1_time_centered"] = int(case.s2w1_time_centered)
+        cp["S2W1D_face_time_consistent"] = int(case.s2w1d_face_time)
+        cp["S2W2R_shared_predictor"] = int(case.s2w2r_shared_predictor)
     if nu is not None:
         cp["Nu"], cp["Nv"] = nu, nv
     cp.update(extra or {})
@@ -220,7 +224,7 @@ def config_text(case, velocity_file="velocity_table.dat", nu=None, nv=None, extr
     for k, v in cp.items():
         vals = v if isinstance(v, (list, tuple)) else [v]
         lines.append(f"{k} = " + " ".join(_fortran(x) for x in vals))
-    lines += ["/", "", "&boundary_para", "BC_Type = 10 10 2 2", "BG_geometry = 0", "FluxWall_type = 1",
+    lines += ["/", "", "&boundary_para", "BC_Type = 10 10 2 2", "BG_geometry = 0", f"FluxWall_type = {case.flux_wall}",
               "ACC = 1.0d0", "CouetteUseW2BWall = .true.",
               "WallUx = 0.0d0 0.0d0 " + " ".join(_flt(float(x)) for x in case.wall_ux), "/", "",
               "$DIS_para", "0", "0", "0", "$DIS_para", ""]
@@ -433,10 +437,31 @@ def case_from_config(groups, mesh=None):
         _need(int(c.get("implicit_maxretries", 8)) == 0, "Implicit_MaxRetries > 0 (nCFL backoff retries)")
         _need(not bool(c.get("implicit_closedmassconstraint", False)), "Implicit_ClosedMassConstraint")
         _need(bool(c.get("implicit_zhumovingwall", False)), "Implicit_ZhuMovingWall = .false.")
+    variant = {"flux_wall": int(b.get("fluxwall_type", 1)),
+               "s2w1_time_centered": int(c.get("s2w1_time_centered", 0)),
+               "s2w1d_face_time": int(c.get("s2w1d_face_time_consistent", 0)),
+               "s2w2r_shared_predictor": int(c.get("s2w2r_shared_predictor", 0))}
     if s2:
         _need(int(c.get("s2w1_wall_mode", 0)) == 1, "S2W1_wall_mode other than 1")
-        for key in ("s2w2r_shared_predictor", "s2w1_time_centered", "s2w1d_face_time_consistent"):
-            _need(int(c.get(key, 0)) == 0, f"{key} (research wall variants)")
+        _need(variant["flux_wall"] in (0, 1), "FluxWall_type other than 0 (kinetic) or 1 (multiscale)")
+        fw, tc, fd, sp = (variant[k] for k in ("flux_wall", "s2w1_time_centered", "s2w1d_face_time",
+                                               "s2w2r_shared_predictor"))
+        if fw == 0 or tc or fd or sp:   # the research wall variants (mod_ImportPara.f90:455-471, :527-528)
+            _need(method == "S2CN2", "the research S2 wall variants on a method other than S2CN2")
+            for key, val in (("S2W1_time_centered", tc), ("S2W1D_face_time_consistent", fd),
+                             ("S2W2R_shared_predictor", sp)):
+                if val not in (0, 1):
+                    raise CaseError(f"Config.ini: {key} must be 0 or 1", 200)
+            if tc and fw != 0:
+                raise CaseError("Config.ini: S2W2 type1 requires centered=0 and face_time_consistent=0", 200)
+            if fd and not tc:
+                raise CaseError("Config.ini: S2W1D face correction requires W1T midpoint wall", 200)
+            if sp and (fw != 1 or int(c.get("ck", 1)) != 1 or float(c.get("pr", 2.0 / 3.0)) != 1.0 or tc or fd
+                       or npy != 1):
+                raise CaseError("Config.ini: W2R supports only frozen flat type1 BGK setup", 200)
+    else:
+        variant = {k: 0 for k in variant}
+        variant["flux_wall"] = 1
     ck = int(c.get("ck", 1))
     gamma = float(ck + 4) / float(ck + 2)
     mu = float(c.get("couettemuref", -1.0))
@@ -475,7 +500,7 @@ def case_from_config(groups, mesh=None):
         macro_sweeps=int(c.get("implicit_macrosweeps", 2)),
         residual_tol=float(c.get("implicit_residualtol", 1.0e-8)),
         moment_tol=float(c.get("implicit_momenttol", 1.0e-12)),
-        min_alpha=float(c.get("implicit_minalpha", 1.0e-6)), max_iter=int(c.get("max_iter", 10000)))
+        min_alpha=float(c.get("implicit_minalpha", 1.0e-6)), max_iter=int(c.get("max_iter", 10000)), **variant)
     if case.mass_rescale and not implicit:
         raise CaseError("ClosedCouetteMassRescale is for the closed-Couette implicit methods only")
     if not (case.tinf > 0.0):

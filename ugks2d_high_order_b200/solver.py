@@ -53,6 +53,9 @@ class Solver:
                     "S2CN2": capi.UGKS_METHOD_S2CN2}.get(case.method, capi.UGKS_METHOD_EXPLICIT)
         p.ncfl, p.nslab, p.mass_rescale, p.macro_sweeps = case.ncfl, case.nslab, int(case.mass_rescale), case.macro_sweeps
         p.residual_tol, p.moment_tol, p.min_alpha = case.residual_tol, case.moment_tol, case.min_alpha
+        p.s2_kinetic_wall = int(case.flux_wall == 0)
+        p.s2_time_centered, p.s2_face_time = int(case.s2w1_time_centered), int(case.s2w1d_face_time)
+        p.s2_shared_predictor = int(case.s2w2r_shared_predictor)
         return p
 
     def _check(self, code, what, ctx="self"):
