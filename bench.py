@@ -91,6 +91,7 @@ PR2_BYTES_PER_CELL = 52 * 8
 # op-counting build of the oracle on the 8x64x1024 cases (python oracle/count_flops.py).  The
 # implicit pseudo-steps count one evaluation less than the reference runs: the device reuses the
 # accepted-state evaluation as the next pre-update one (reference: 3568 and 58725).
+VARIANT_STEPS = 40   # timed steps of each research wall variant (8x64x1024, after 4 warm-up steps)
 FLOPS_PER_UPDATE = {"explicit": 1565.9, "implicit_steady": 2211.5, "high_order_implicit": 29736.7, "s2cn2": 29241.7}
 # S2CN2 per velocity set (oracle/count_flops.py: S2CN2_24, S2CN2 (32^2), S2CN2_48 on the 8x64 case)
 S2CN2_FLOPS_BY_TABLE = {24: 29306.5, 32: 29241.7, 48: 27542.5}
@@ -696,6 +697,27 @@ def main():
              "fp64": fp64_fraction(FLOPS_PER_UPDATE["s2cn2"], cn_value, fpk),
              "config": "S2CN2 8x64x1024, CFL 0.1, 8 steps warm-up then 400 steps, two steps per CUDA graph; "
                        "FP64-bound"}
+    # the research wall variants of the same step (FluxWall_type 0; W1T; W1T + W1D; W2R at Pr 1)
+    variants = {}
+    for vname, fields in (("kinetic_wall", dict(flux_wall=0)),
+                          ("w1t_midpoint", dict(flux_wall=0, s2w1_time_centered=1)),
+                          ("w1d_face_time", dict(flux_wall=0, s2w1_time_centered=1, s2w1d_face_time=1)),
+                          ("w2r_shared", dict(pr=1.0, s2w2r_shared_predictor=1))):
+        sv = Solver(reference_case("S2CN2").with_(**fields), *vel, device=local)
+        sv.init_freestream()
+        sv.step_s2cn2(4)
+        vstream = torch.cuda.ExternalStream(sv.stream)
+        v0, v1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(vstream):
+            v0.record(vstream)
+            done_v, rep_v = sv.step_s2cn2(VARIANT_STEPS)
+            v1.record(vstream)
+        v1.synchronize()
+        vms = v0.elapsed_time(v1) / max(done_v, 1)
+        sv.close()
+        variants[vname] = {"ms_per_step": vms, "vs_delivered_step": vms / s2cn2["ms_per_step"], "steps": int(done_v),
+                           "value": nc * nv / (vms * 1e-3), "drift": float(rep_v[9]), "cnres": float(rep_v[1])}
+    s2cn2["wall_variants"] = variants
 
     # ---------------- batched S2CN2: 256 instances of uneven sizes
     from ugks2d_high_order_b200.batch import Batch
