@@ -31,6 +31,7 @@
 namespace ugks {
 namespace {
 
+
 // ---------------------------------------------------------------------------------------------
 // forward mode on one input direction per lane (the double versions of the math functions stay visible
 // beside the Dl overloads)
@@ -1611,22 +1612,19 @@ __global__ void __launch_bounds__(256, 2) k_adj_recon2(LoParams P, LoBuffers B, 
     }
 }
 
-// the first layer (k_s2_recon1), transposed: CTA = 4 warps (field, direction) over 32 velocities of one
-// cell; gl1 -> the state's x row / y column stencils.  Each gl1 entry is read here once and then cleared
-// for the next step's accumulation.
-__global__ void __launch_bounds__(128) k_adj_recon1(LoParams P, LoBuffers B, AdjBuffers A) {
-    const int nv = P.nvel, nx = P.nx, ny = P.ny, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const int f = warp >> 1, dir = warp & 1;
-    const int k0 = blockIdx.x * 32 + lane;
-    if (k0 >= nv) return;
-    const int k = k0, cc = blockIdx.y, i = cc % nx, j = cc / nx;
-    if (dir == 1 && s2_near_wall(j, ny)) return;
+// the first layer (k_s2_recon1), transposed, for one cell, field and direction at velocity k: the cell's
+// gl1 entries of that direction (read once and cleared for the next step's accumulation) through the
+// WENO-AO transposes into gq, the cotangents of its 5-cell stencil (x row or y column)
+__device__ __forceinline__ void adj_first_layer(const LoParams& P, const LoBuffers& B, const AdjBuffers& A, int f,
+                                                int dir, int cc, int k, double gq[5]) {
+    const int nv = P.nvel, nx = P.nx, ny = P.ny, i = cc % nx, j = cc / nx;
     const S2Field F{(f == 0 ? B.h : B.b) + k, nv, nx, ny};
     double q[5];
 #pragma unroll
     for (int s = -2; s <= 2; ++s) q[s + 2] = dir == 0 ? F.at(i + s, j) : F.at(i, j + s);
     double* o = A.gl1 + ((size_t)cc * 22 + f * 11 + (dir == 0 ? 0 : 7)) * nv + k;
-    double gq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+    for (int s = 0; s < 5; ++s) gq[s] = 0.0;
     if (dir == 0) {
         const int pts[5] = {S2_XM, S2_XP, S2_G0, S2_G0 + 1, S2_G0 + 2};
         const double gv[5] = {o[0], o[2 * (size_t)nv], o[4 * (size_t)nv], o[5 * (size_t)nv], o[6 * (size_t)nv]};
@@ -1641,6 +1639,91 @@ __global__ void __launch_bounds__(128) k_adj_recon1(LoParams P, LoBuffers B, Adj
         for (int e = 0; e < 4; ++e) o[(size_t)e * nv] = 0.0;
         weno_points_vjp<2>(q, pts, gv, gd, gq);
     }
+}
+
+// The first layer's transposes as gathers.  k_adj_recon1_xy: CTA = one row, 32 velocities, one field; warp
+// w owns cell (w, row) and runs both of its transposes.  The x stencil cotangents go to shared memory and
+// each warp sums the five that land on its own cell into the state cotangent -- a plain read-modify-write
+// per (cell, velocity), nothing else writing the state cotangents meanwhile; the y stencil cotangents go to
+// yq ([cell][field][5][nvel], the face-cache cotangent's storage, free once k_adj_recon2 has read it).
+__global__ void __launch_bounds__(512) k_adj_recon1_xy(LoParams P, LoBuffers B, AdjBuffers A, double* yq) {
+    extern __shared__ double s_gq[];   // [cell][5][32]
+    const int nv = P.nvel, nx = P.nx, ny = P.ny, lane = threadIdx.x & 31, i = threadIdx.x >> 5;
+    const int k = blockIdx.x * 32 + lane, j = blockIdx.y, f = blockIdx.z, cc = j * nx + i;
+    double gq[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+    if (k < nv) {
+        // every load of both transposes first (the stencils and the cell's gl1 entries), then the clears,
+        // so the two directions' memory latencies overlap
+        const bool ydir = !s2_near_wall(j, ny);
+        const S2Field F{(f == 0 ? B.h : B.b) + k, nv, nx, ny};
+        double qx[5], qy[5], ox[7], oy[4];
+#pragma unroll
+        for (int s = -2; s <= 2; ++s) {
+            qx[s + 2] = F.at(i + s, j);
+            qy[s + 2] = ydir ? F.at(i, j + s) : 0.0;
+        }
+        double* o = A.gl1 + ((size_t)cc * 22 + f * 11) * nv + k;
+#pragma unroll
+        for (int e = 0; e < 7; ++e) ox[e] = o[(size_t)e * nv];
+#pragma unroll
+        for (int e = 0; e < 4; ++e) oy[e] = ydir ? o[(size_t)(7 + e) * nv] : 0.0;
+#pragma unroll
+        for (int e = 0; e < 11; ++e)
+            if (e < 7 || ydir) o[(size_t)e * nv] = 0.0;
+        {
+            const int pts[5] = {S2_XM, S2_XP, S2_G0, S2_G0 + 1, S2_G0 + 2};
+            const double gv[5] = {ox[0], ox[2], ox[4], ox[5], ox[6]}, gd[5] = {ox[1], ox[3], 0.0, 0.0, 0.0};
+            weno_points_vjp<5>(qx, pts, gv, gd, gq);
+        }
+        if (ydir) {
+            const int pts[2] = {S2_XM, S2_XP};
+            const double gv[2] = {oy[0], oy[2]}, gd[2] = {oy[1], oy[3]};
+            double gy[5] = {0.0, 0.0, 0.0, 0.0, 0.0};
+            weno_points_vjp<2>(qy, pts, gv, gd, gy);
+#pragma unroll
+            for (int s = 0; s < 5; ++s) yq[(((size_t)cc * 2 + f) * 5 + s) * nv + k] = gy[s];
+        }
+    }
+#pragma unroll
+    for (int s = 0; s < 5; ++s) s_gq[(i * 5 + s) * 32 + lane] = gq[s];
+    __syncthreads();
+    if (k >= nv) return;
+    double sum = 0.0;
+#pragma unroll
+    for (int s = -2; s <= 2; ++s) sum += s_gq[(wrapx(i - s, nx) * 5 + (s + 2)) * 32 + lane];
+    double* g = (f == 0 ? A.ghi : A.gbi) + (size_t)cc * nv + k;
+    *g = *g + sum;
+}
+
+// ... and the y gather: thread per (cell, velocity, field) sums the y stencil cotangents its column's owners
+// (rows t-2 .. t+2 away from the walls) left in yq.  Runs after k_adj_recon1_xy.
+__global__ void __launch_bounds__(256) k_adj_recon1_yg(LoParams P, AdjBuffers A, const double* yq) {
+    const int nv = P.nvel, nx = P.nx, ny = P.ny;
+    const int k = blockIdx.x * blockDim.x + threadIdx.x, cc = blockIdx.y, f = blockIdx.z;
+    if (k >= nv) return;
+    const int i = cc % nx, t = cc / nx;
+    double sum = 0.0;
+#pragma unroll
+    for (int s = -2; s <= 2; ++s) {
+        const int o = t - s;
+        if (o >= 0 && o < ny && !s2_near_wall(o, ny)) sum += yq[(((size_t)(o * nx + i) * 2 + f) * 5 + (s + 2)) * nv + k];
+    }
+    double* g = (f == 0 ? A.ghi : A.gbi) + (size_t)cc * nv + k;
+    *g = *g + sum;
+}
+
+// the scatter form of the same transposes, for grids whose row or column does not fit one CTA: CTA = 4
+// warps (field, direction) over 32 velocities of one cell, only direction `only` at work; atomic adds into
+// the five stencil cells
+__global__ void __launch_bounds__(128) k_adj_recon1(LoParams P, LoBuffers B, AdjBuffers A, int only) {
+    const int nv = P.nvel, nx = P.nx, ny = P.ny, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int f = warp >> 1, dir = warp & 1;
+    const int k0 = blockIdx.x * 32 + lane;
+    if (k0 >= nv || dir != only) return;
+    const int k = k0, cc = blockIdx.y, i = cc % nx, j = cc / nx;
+    if (dir == 1 && s2_near_wall(j, ny)) return;
+    double gq[5];
+    adj_first_layer(P, B, A, f, dir, cc, k, gq);
     double* gS = (f == 0 ? A.ghi : A.gbi) + k;
 #pragma unroll
     for (int s = -2; s <= 2; ++s) {
@@ -1713,7 +1796,15 @@ static cudaError_t adj_launch(const LoParams& P, const LoBuffers& B, const S2Buf
     if (e == cudaSuccess) {
         const dim3 grid((unsigned)((nv + 31) / 32), (unsigned)nc);
         k_adj_recon2<<<grid, 256, 0, s>>>(P, B, S, A);
-        k_adj_recon1<<<grid, 128, 0, s>>>(P, B, A);
+        const unsigned kb = (unsigned)((nv + 31) / 32);
+        if (nx <= 16) {   // one row per CTA
+            k_adj_recon1_xy<<<dim3(kb, (unsigned)ny, 2), 32 * nx, (size_t)nx * 5 * 32 * sizeof(double), s>>>(P, B, A,
+                                                                                                         A.grec);
+            k_adj_recon1_yg<<<dim3((unsigned)((nv + 255) / 256), (unsigned)nc, 2), 256, 0, s>>>(P, A, A.grec);
+        } else {
+            k_adj_recon1<<<grid, 128, 0, s>>>(P, B, A, 0);
+            k_adj_recon1<<<grid, 128, 0, s>>>(P, B, A, 1);
+        }
     }
     if (e == cudaSuccess && side) e = cudaStreamWaitEvent(s, ev[3], 0);   // gWi complete before the next step
     if (e != cudaSuccess) return e;

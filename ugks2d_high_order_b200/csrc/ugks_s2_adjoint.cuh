@@ -58,6 +58,6 @@ cudaError_t enqueue_s2cn2_adjoint(const LoParams& P, const LoBuffers& B, const S
 // s2_enqueue(3)) added to gW.
 cudaError_t enqueue_targets_adjoint(const LoParams& P, const LoBuffers& B, const S2Buffers& S, double* const gT[6],
                                     double* gW, const AdjBuffers& A, cudaStream_t s);
-constexpr int kAdjStepKernels = 9;
+constexpr int kAdjStepKernels = 10;
 
 }  // namespace ugks
