@@ -945,6 +945,10 @@ extern "C" int ugks_implicit_steps(ugks_ctx* c, int max_steps, int* steps_done, 
     UGKS_CK(cudaStreamSynchronize(c->stream));
     const double start = st[IS_STEPS];
     int left = max_steps;
+    if (left > 0 && st[IS_STOP] == 0.0) {   // the first pseudo-step's TimeStep (each later one's is taken by
+        UGKS_CK(launch_lo_timestep(c->P, c->B, c->stream));   // the pseudo-step before it)
+        c->launches += 1;
+    }
     while (left > 0 && st[IS_STOP] == 0.0) {
         if (c->profile) {   // un-graphed, one step at a time, with an event after every stage
             for (int q = 0; q <= kImStages; ++q)

@@ -161,13 +161,16 @@ __device__ void im_residual_epilogue(const LoParams& P, const LoBuffers& B, cons
     // g[0..18]: sums of the per-cell terms; g[19..30]: boundary-face macro fluxes per unit time
     // (x wrap face, bottom wall, top wall; PhysicalDiagnostic flux, mod_R5Observe.f90:107-113);
     // g[31]: max moment error
-    double g[32];
+    // g[32] (POST): max of -dt_local, the next pseudo-step's TimeStep
+    double g[33];
 #pragma unroll
     for (int m = 0; m < 32; ++m) g[m] = 0.0;
+    g[32] = -INFINITY;
     for (int cc = tid; cc < nc; cc += blockDim.x) {
 #pragma unroll
         for (int m = 0; m < 19; ++m) g[m] += __ldcg(I.cell + (size_t)cc * kImCell + m);
         g[31] = fmax(g[31], __ldcg(I.cell + (size_t)cc * kImCell + 19));
+        if (POST) g[32] = fmax(g[32], -__ldcg(B.dtl + cc));
     }
     if (POST) {
         for (int jj = tid; jj < P.ny; jj += blockDim.x)
@@ -180,7 +183,7 @@ __device__ void im_residual_epilogue(const LoParams& P, const LoBuffers& B, cons
                 g[27 + m] += __ldcg(B.fyw + ((size_t)P.ny * nx + ii) * 4 + m) / dt;
             }
     }
-    block_reduce<31, 1>(g, red, rout);
+    block_reduce<31, 2>(g, red, rout);
     if (tid != 0) return;
     const double SMV = kSMV;
     double sci[22];
@@ -251,6 +254,10 @@ __device__ void im_residual_epilogue(const LoParams& P, const LoBuffers& B, cons
     rep[50] = rh; rep[51] = rb;
     rep[52] = Q.mass_rescale ? I.state[IS_MASS_SCALE] - 1.0 : 0.0;
     rep[53] = I.state[IS_ALPHA]; rep[54] = I.state[IS_MALPHA]; rep[55] = dt; rep[56] = streak;
+    // TimeStep of the next pseudo-step (mod_Solve.f90:373-421) from this accepted state, as k_lo_timestep
+    // would take it at the next step's start
+    B.dt[1] = B.dt[0];
+    B.dt[0] = P.fixed_dt > 0.0 ? P.fixed_dt : -g[32];
     *I.counter = 0u;
 }
 
@@ -450,6 +457,11 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_residual(LoParams P, 
         t[19] = merr;
     }
 
+    if (POST && tid == 0) {   // this cell's dt_local for the next pseudo-step's TimeStep
+        bool okd;
+        B.dtl[c] = cell_dt(P, B.W + c * 4, okd);
+        if (!okd) set_status(B.status, ST_GETPRIMARY);
+    }
     im_residual_epilogue<POST>(P, B, Q, I, red, rout);
 }
 
@@ -565,6 +577,11 @@ __global__ void __launch_bounds__(NTMAX, 512 / NTMAX) k_im_residual_s2(LoParams 
         t[13] = rate[0] * P.area;
         t[18] = P.area * rout[8];
         t[19] = merr;
+    }
+    if (POST && tid == 0) {   // this cell's dt_local for the next pseudo-step's TimeStep
+        bool okd;
+        B.dtl[c] = cell_dt(P, B.W + c * 4, okd);
+        if (!okd) set_status(B.status, ST_GETPRIMARY);
     }
     im_residual_epilogue<POST>(P, B, Q, I, red, rout);
 }
@@ -1421,9 +1438,11 @@ cudaError_t prepare_implicit(const LoParams& P, const ImParams& Q) {
 }
 
 // One ImplicitSteady pseudo-step (mod_Solve.f90:84-293 with TimeIntegration_method =
-// 'ImplicitSteady' and ClosedCouetteMassRescale): 16 + macro_sweeps kernels with the second-order
+// 'ImplicitSteady' and ClosedCouetteMassRescale): 15 + macro_sweeps kernels with the second-order
 // evaluations (3 kernels each), 6 more per evaluation with the S2 one of HighOrderImplicit, no host
-// synchronisation.
+// synchronisation.  The TimeStep of the next pseudo-step is taken in the accepted-state residual's last
+// CTA, so it is no launch of its own; the caller launches k_lo_timestep once before the first pseudo-step
+// of a sequence.
 // Returns the number of kernels launched through *launches.
 // marks (optional, profile runs only): kImStages + 1 events recorded on s at the start and after
 // each stage of kImStageNames.
@@ -1456,7 +1475,9 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     LoBuffers Bpre = Bh;
     Bpre.eval = I.state + IS_EVAL_VALID;
     cudaError_t e = mark(cudaSuccess);
-    if (e == cudaSuccess) e = mark(launch_lo_timestep(P, Bh, s));                // TimeStep
+    // TimeStep: taken by the previous pseudo-step's accepted-state residual (or, for the first pseudo-step
+    // of a call, by the k_lo_timestep the call launches first)
+    if (e == cudaSuccess) e = mark(cudaSuccess);
     if (e == cudaSuccess && cond) {
         cudaStreamCaptureStatus cs;
         cudaGraph_t g = nullptr;
@@ -1523,7 +1544,7 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     // (counted once per sequence by ugks_implicit_init / ugks_implicit_restore); the gate replaces the
     // pre-update residual in the count
     const int evaluation = Q.high_order ? s2_enqueue_kernels(1) : 3;
-    if (launches) *launches += 10 + Q.macro_sweeps + (cond ? evaluation : 2 * evaluation);
+    if (launches) *launches += 9 + Q.macro_sweeps + (cond ? evaluation : 2 * evaluation);
     return e;
 }
 
