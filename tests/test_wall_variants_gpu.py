@@ -163,3 +163,29 @@ def test_variant_contexts_refuse_the_adjoint():
         assert s.L.ugks_s2cn2_forward_checkpointed(s.ctx, 4, 2, out) == capi.UGKS_EUNSUPPORTED
     finally:
         s.close()
+
+
+@pytest.mark.parametrize("name", ["w1d_face_time", "w2r_shared"])
+def test_variants_on_the_48_squared_table(name):
+    """The variants with a table above 1024 velocities (48^2 = 2304: the 10-velocity-per-thread cell
+    kernels, every velocity loop of the variant kernels past one pass), 8 x 16 cells, four steps."""
+    from oracle.oracle import Oracle, set_threads
+    from ugks2d_high_order_b200.solver import Solver
+    set_threads(None)
+    case = _case(name, ny=16, dy=1.0 / 16.0)
+    vel = velocity_table(48)
+    s, o = Solver(case, *vel), Oracle(case, *vel)
+    try:
+        s.init_freestream()
+        o.init_freestream()
+        done, rep = s.step_s2cn2(4)
+        for _ in range(4):
+            out = o.s2cn2_step()
+        assert done == 4
+        _check(rep, out, name)
+        hg, bg, Wg = s.download()
+        ho, bo, Wo = o.get_state()
+        assert _rel(Wg, Wo) <= HO_TOL and _rel(hg, ho) <= HO_TOL and _rel(bg, bo) <= HO_TOL, \
+            (_rel(Wg, Wo), _rel(hg, ho), _rel(bg, bo))
+    finally:
+        s.close()
