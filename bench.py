@@ -91,6 +91,7 @@ PR2_BYTES_PER_CELL = 52 * 8
 # op-counting build of the oracle on the 8x64x1024 cases (python oracle/count_flops.py).  The
 # implicit pseudo-steps count one evaluation less than the reference runs: the device reuses the
 # accepted-state evaluation as the next pre-update one (reference: 3568 and 58725).
+GRAPH_PROFILE_STEPS = 96   # pseudo-steps of the graph-mode stage timing (12 batch graphs of 8)
 VARIANT_STEPS = 40   # timed steps of each research wall variant (8x64x1024, after 4 warm-up steps)
 FLOPS_PER_UPDATE = {"explicit": 1565.9, "implicit_steady": 2211.5, "high_order_implicit": 29736.7, "s2cn2": 29241.7}
 # S2CN2 per velocity set (oracle/count_flops.py: S2CN2_24, S2CN2 (32^2), S2CN2_48 on the 8x64 case)
@@ -548,6 +549,15 @@ def main():
     prof_steps = 100
     s.step_implicit(prof_steps)
     from ugks2d_high_order_b200.capi import IMPLICIT_STAGES
+    ustimes = {name: s.profile_read(name) for name in IMPLICIT_STAGES}
+    s.profile(False)
+    # ... and the same stages as the batch graphs run them: the stage events are captured into the graphs
+    # as event nodes, and each 8-step batch's last pseudo-step is timed (no launch gaps of its own)
+    s.init_freestream()
+    s.implicit_init()
+    s.step_implicit(20)
+    s.profile(True, graph=True)
+    s.step_implicit(GRAPH_PROFILE_STEPS)
     stimes = {name: s.profile_read(name) for name in IMPLICIT_STAGES}
     s.profile(False)
     stot = sum(t for t, _ in stimes.values())
@@ -580,9 +590,12 @@ def main():
                                    "frac": stage_bw / peak},
                 "stage_share": {k: t / stot for k, (t, _) in stimes.items()},
                 "stage_us_per_pseudo_step": {k: 1e3 * t / max(n, 1) for k, (t, n) in stimes.items()},
+                "stage_us_ungraphed": {k: 1e3 * t / max(n, 1) for k, (t, n) in ustimes.items()},
                 "note": "one 8.4 MB instance is L2-resident and the step is latency-bound: pr2_sweep and "
                         "the LU-SGS stages are Gauss-Seidel wavefronts, chains of (rows+nx-1) dependent "
-                        "relaxations per pass; stage times come from an un-graphed event pass"}
+                        "relaxations per pass; stage times come from events captured into the batch graphs "
+                        "(the last pseudo-step of each of %d batches); stage_us_ungraphed: the same stages "
+                        "launched one by one, launch gaps included" % (GRAPH_PROFILE_STEPS // 8)}
     fpk = fp64_peak(f"cuda:{local}")
     roofline["fp64"] = fp64_fraction(FLOPS_PER_UPDATE["implicit_steady"], value / world, fpk)
 

@@ -309,7 +309,11 @@ int ugks_synchronize(ugks_ctx* ctx);
 
 /* Kernel-level timing: when enabled, ugks_step_explicit records CUDA events around each kernel
  * launch (graph replay off) and accumulates per-kernel milliseconds and launch counts.
- * names: "slopes", "faces", "walls", "cells". */
+ * names: "slopes", "faces", "walls", "cells".  ugks_implicit_steps times its pseudo-step stages
+ * (names: the stage names of the implicit report, "timestep" ... "post_residual"): enable = 1 runs the
+ * steps one by one with an event after every stage; enable = 2 runs them in batch graphs of 8 with the
+ * stage events captured into the graph, timing each batch's last pseudo-step as the graphs run it
+ * (the launches counted are then the sampled pseudo-steps). */
 int ugks_profile_enable(ugks_ctx* ctx, int enable);
 int ugks_profile_read(ugks_ctx* ctx, const char* kernel, double* total_ms, long long* launches);
 

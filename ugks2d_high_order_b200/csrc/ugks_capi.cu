@@ -71,7 +71,8 @@ struct ugks_ctx {
     long long iloop_launches = 0;              // kernels per loop iteration
     bool iloop_unavailable = false;            // its build failed: the host pipeline runs the batches
     // profiling
-    bool profile = false;
+    int profile = 0;                           // 1: stage events, un-graphed steps; 2: stage events in the graphs
+    cudaGraphExec_t pgraph = nullptr;          // profile 2: the batch graph with the stage events captured
     cudaEvent_t ev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
     KernelTimer t_slopes, t_faces, t_walls, t_cells;
     cudaEvent_t im_ev[kImStages + 1] = {};
@@ -374,6 +375,7 @@ extern "C" int ugks_ctx_destroy(ugks_ctx* c) {
     if (c->stream) cudaStreamSynchronize(c->stream);
     if (c->graph) cudaGraphExecDestroy(c->graph);
     if (c->igraph) cudaGraphExecDestroy(c->igraph);
+    if (c->pgraph) cudaGraphExecDestroy(c->pgraph);
     if (c->iloop) cudaGraphExecDestroy(c->iloop);
     if (c->iloop_ctr) cudaFree(c->iloop_ctr);
     if (c->cgraph) cudaGraphExecDestroy(c->cgraph);
@@ -776,7 +778,7 @@ extern "C" int ugks_synchronize(ugks_ctx* c) {
 
 extern "C" int ugks_profile_enable(ugks_ctx* c, int enable) {
     if (!c) return UGKS_EINVAL;
-    c->profile = enable != 0;
+    c->profile = enable == 2 ? 2 : (enable != 0 ? 1 : 0);
     c->t_slopes = KernelTimer();
     c->t_faces = KernelTimer();
     c->t_walls = KernelTimer();
@@ -950,6 +952,41 @@ extern "C" int ugks_implicit_steps(ugks_ctx* c, int max_steps, int* steps_done, 
         c->launches += 1;
     }
     while (left > 0 && st[IS_STOP] == 0.0) {
+        if (c->profile == 2 && left >= G) {
+            // a batch graph with an external event node after every stage: the events keep the batch's last
+            // pseudo-step, whose stages are timed as the graphs run them (no launch gaps of their own)
+            for (int q = 0; q <= kImStages; ++q)
+                if (!c->im_ev[q]) UGKS_CK(cudaEventCreate(&c->im_ev[q]));
+            if (!c->pgraph) {
+                cudaGraph_t g;
+                long long n = 0;
+                UGKS_CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+                cudaError_t e = cudaSuccess;
+                for (int q = 0; q < G && e == cudaSuccess; ++q)
+                    e = enqueue_implicit_step(c->P, c->B, c->Q, c->I, c->stream, c->stream2, c->ev_fork, c->ev_join, &n,
+                                              c->im_ev, c->Q.high_order ? &c->icap : nullptr);
+                cudaError_t e2 = cudaStreamEndCapture(c->stream, &g);
+                if (e != cudaSuccess) { if (e2 == cudaSuccess) cudaGraphDestroy(g); return cuda_fail(e); }
+                UGKS_CK(e2);
+                e = cudaGraphInstantiate(&c->pgraph, g, 0);
+                cudaGraphDestroy(g);
+                UGKS_CK(e);
+                c->igraph_launches = n;
+            }
+            UGKS_CK(cudaGraphLaunch(c->pgraph, c->stream));
+            UGKS_CK(cudaMemcpyAsync(st, c->I.state, sizeof st, cudaMemcpyDeviceToHost, c->stream));
+            UGKS_CK(cudaStreamSynchronize(c->stream));
+            for (int q = 0; q < kImStages; ++q) {
+                float ms = 0.f;
+                UGKS_CK(cudaEventElapsedTime(&ms, c->im_ev[q], c->im_ev[q + 1]));
+                c->im_t[q].total_ms += ms;
+                c->im_t[q].launches += 1;
+            }
+            c->launches += c->igraph_launches;
+            left -= G;
+            if (int r = collect_status(c)) return r;
+            continue;
+        }
         if (c->profile) {   // un-graphed, one step at a time, with an event after every stage
             for (int q = 0; q <= kImStages; ++q)
                 if (!c->im_ev[q]) UGKS_CK(cudaEventCreate(&c->im_ev[q]));

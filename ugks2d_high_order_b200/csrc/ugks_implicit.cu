@@ -1464,8 +1464,14 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
                                   cudaStream_t s, cudaStream_t s2, cudaEvent_t fork, cudaEvent_t join,
                                   long long* launches, cudaEvent_t* marks, const ImCapture* cond) {
     int stage = 0;
+    // stage events; under stream capture they are captured as external event nodes, which the graph
+    // records as it runs
+    cudaStreamCaptureStatus capturing = cudaStreamCaptureStatusNone;
+    if (marks) cudaStreamIsCapturing(s, &capturing);
     auto mark = [&](cudaError_t e) -> cudaError_t {
-        if (e == cudaSuccess && marks) e = cudaEventRecord(marks[stage++], s);
+        if (e == cudaSuccess && marks)
+            e = cudaEventRecordWithFlags(marks[stage++], s,
+                                         capturing == cudaStreamCaptureStatusActive ? cudaEventRecordExternal : 0);
         return e;
     };
     // The pre-update evaluation reuses the previous accepted-state evaluation when the state and dt

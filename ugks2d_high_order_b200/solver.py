@@ -277,8 +277,10 @@ class Solver:
     def synchronize(self):
         self._check(self.L.ugks_synchronize(self.ctx), "synchronize")
 
-    def profile(self, enable=True):
-        self._check(self.L.ugks_profile_enable(self.ctx, int(enable)), "profile")
+    def profile(self, enable=True, graph=False):
+        """Per-kernel (explicit) and per-stage (implicit) event timing; graph=True times the implicit
+        stages inside the batch graphs instead of in un-graphed steps."""
+        self._check(self.L.ugks_profile_enable(self.ctx, 2 if (enable and graph) else int(bool(enable))), "profile")
 
     def profile_read(self, kernel):
         ms = ctypes.c_double()
