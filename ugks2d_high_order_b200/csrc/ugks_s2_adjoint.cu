@@ -747,7 +747,9 @@ __global__ void __launch_bounds__(NT) k_adj_stream(LoParams P, LoBuffers B, S2Bu
 // the stream rates of the two cells (grh, grb, gws), folded with the Gauss weight and face length.
 // Cotangents out: the face cache at the upwind side of every velocity (grec, written; the other side's
 // entry is set to zero), the macro slopes of the node (gmac) and mu_ref.
-__global__ void __launch_bounds__(128) k_adj_face_nodes(LoParams P, LoBuffers B, S2Buffers S, AdjBuffers A) {
+// Three CTAs per SM (168 registers with spills instead of 254 without): measured 2.5 % faster over the
+// backward, the extra resident warps hiding the spills' latency.
+__global__ void __launch_bounds__(128, 3) k_adj_face_nodes(LoParams P, LoBuffers B, S2Buffers S, AdjBuffers A) {
     const int nv = P.nvel, nx = P.nx, ny = P.ny, ck = P.ck, nr = (nv + 31) >> 5, lane = threadIdx.x & 31;
     const int nfx = nx * ny, nf = nfx + nx * (ny - 1);
     const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -1446,7 +1448,8 @@ __global__ void __launch_bounds__(256) k_adj_macro_faces(LoParams P, const doubl
 // the second layer and the positivity limiter (k_s2_recon2), transposed: CTA = 8 warps (field, part)
 // over 32 velocities of one cell, as the forward kernel.  grec (this cell's face-cache entries) -> gl1 of the rows /
 // columns the templates read, and the state (the limiter's cell means, the wall rows' direct samples).
-__global__ void __launch_bounds__(256, 2) k_adj_recon2(LoParams P, LoBuffers B, S2Buffers S, AdjBuffers A) {
+// Three CTAs per SM (80 registers with spills): measured 2.3 % faster over the backward than two at 128.
+__global__ void __launch_bounds__(256, 3) k_adj_recon2(LoParams P, LoBuffers B, S2Buffers S, AdjBuffers A) {
     __shared__ double s_th[8][32];
     __shared__ double s_gth[8][32];
     const int nv = P.nvel, nx = P.nx, ny = P.ny, lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
