@@ -63,9 +63,10 @@ typedef struct ugks_params {
     double residual_tol;     /* Implicit_ResidualTol */
     double moment_tol;       /* Implicit_MomentTol */
     double min_alpha;        /* Implicit_MinAlpha */
-    /* The research S2CN2 wall variants (mod_ImportPara.f90:88-93, checked as :455-471 and :516-533 check
-     * them); all zero is the delivered configuration, FluxWall_type = 1 (the multiscale wall).  S2CN2
-     * contexts only; ugks_ctx_create returns UGKS_EINVAL for a combination the reference rejects. */
+    /* The research S2 wall variants (mod_ImportPara.f90:88-93, checked as :455-471 and :516-533 check
+     * them); all zero is the delivered configuration, FluxWall_type = 1 (the multiscale wall).  The
+     * kinetic wall on S2CN2 and HighOrderImplicit contexts, the other three on S2CN2 contexts;
+     * ugks_ctx_create returns UGKS_EINVAL for a combination the reference rejects. */
     int s2_kinetic_wall;     /* FluxWall_type = 0: the free-streaming diffuse wall (s2w1_wall_node) */
     int s2_time_centered;    /* S2W1_time_centered = 1: W1T, the walls re-evaluated at a predicted
                                 midpoint state (needs s2_kinetic_wall) */

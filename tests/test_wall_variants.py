@@ -53,8 +53,10 @@ def test_c_abi_keeps_the_variants_to_s2cn2():
     L = capi.load()
     u, v, w = (np.ascontiguousarray(a) for a in velocity_table(24))
     dp = ctypes.POINTER(ctypes.c_double)
-    for method in ("Explicit", "ImplicitSteady", "HighOrderImplicit"):
-        p = Solver.params_for(_small(method, flux_wall=0), len(u))
+    refused = [("Explicit", dict(flux_wall=0)), ("ImplicitSteady", dict(flux_wall=0)),
+               ("HighOrderImplicit", dict(flux_wall=0, s2w1_time_centered=1))]   # the kinetic wall alone is HO's
+    for method, fields in refused:
+        p = Solver.params_for(_small(method, **fields), len(u))
         ctx = ctypes.c_void_p()
         assert L.ugks_ctx_create(ctypes.byref(p), u.ctypes.data_as(dp), v.ctypes.data_as(dp), w.ctypes.data_as(dp), 0,
                                  ctypes.byref(ctx)) == capi.UGKS_EUNSUPPORTED
@@ -117,9 +119,12 @@ def test_case_reader_takes_the_variant_switches(tmp_path):
         case = reference_case("S2CN2").with_(nslab=1, **fields)
         with pytest.raises(refio.CaseError, match="reference abort 200"):
             refio.case_from_config(refio.parse_namelists(refio.config_text(case)), None)
-    with pytest.raises(refio.CaseError):   # the variants are S2CN2's
+    with pytest.raises(refio.CaseError):   # W1T / W1D / W2R are S2CN2's
         refio.case_from_config(refio.parse_namelists(refio.config_text(
-            reference_case("HighOrderImplicit").with_(flux_wall=0))), None)
+            reference_case("HighOrderImplicit").with_(flux_wall=0, s2w1_time_centered=1))), None)
+    got = refio.case_from_config(refio.parse_namelists(refio.config_text(   # the kinetic wall is HO's too
+        reference_case("HighOrderImplicit").with_(flux_wall=0))), None)
+    assert got.flux_wall == 0 and got.method == "HighOrderImplicit"
 
 
 @pytest.mark.parametrize("fields", [{}, VARIANTS["w1d_face_time"], VARIANTS["w2r_shared"]])
@@ -138,3 +143,20 @@ def test_tangent_build_steps_as_the_oracle(fields):
     h, b, W = o.get_state()
     th, _, tb, _, tW, _ = t.get_state()
     assert np.array_equal(h, th) and np.array_equal(b, tb) and np.array_equal(W, tW)
+
+
+def test_oracle_high_order_implicit_with_the_kinetic_wall():
+    """The kinetic wall on the HighOrderImplicit pseudo-step: it runs, keeps the moment gate, and moves
+    the state away from the multiscale wall's."""
+    from oracle.oracle import Oracle
+    vel = velocity_table(24)
+    out = {}
+    for fw in (1, 0):
+        o = Oracle(_small("HighOrderImplicit", flux_wall=fw), *vel)
+        o.init_freestream()
+        o.implicit_init()
+        for _ in range(2):
+            row = o.implicit_step()
+        out[fw] = o.get_state()[0]
+        assert abs(row[1]) <= 1e-12   # the moment gate of the accepted state
+    assert not np.array_equal(out[0], out[1])

@@ -189,3 +189,27 @@ def test_variants_on_the_48_squared_table(name):
             (_rel(Wg, Wo), _rel(hg, ho), _rel(bg, bo))
     finally:
         s.close()
+
+
+def test_high_order_implicit_with_the_kinetic_wall(velocity):
+    """HighOrderImplicit with FluxWall_type 0 (the reference admits the kinetic wall on both S2 methods;
+    its implicit micro wall treatment does not depend on it): five pseudo-steps of the delivered 8 x 64 x 32^2
+    case against the oracle, at the delivered method's bounds (states 1e-11, c_minus_1 5e-11)."""
+    from oracle.oracle import Oracle, set_threads
+    from ugks2d_high_order_b200.solver import Solver
+    set_threads(None)
+    case = reference_case("HighOrderImplicit").with_(flux_wall=0)
+    s, o = Solver(case, *velocity), Oracle(case, *velocity)
+    try:
+        s.init_freestream(); s.implicit_init()
+        o.init_freestream(); o.implicit_init()
+        done, conv, rep = s.step_implicit(5)
+        for _ in range(5):
+            row = o.implicit_step()
+        assert done == 5
+        hg, bg, Wg = s.download()
+        ho, bo, Wo = o.get_state()
+        assert _rel(Wg, Wo) <= 1e-11 and _rel(hg, ho) <= 1e-11, (_rel(Wg, Wo), _rel(hg, ho))
+        assert abs(rep[52] - row[52]) <= 5e-11 * max(abs(row[52]), 1e-3)
+    finally:
+        s.close()

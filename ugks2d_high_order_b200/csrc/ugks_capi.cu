@@ -162,14 +162,16 @@ static int collect_status(ugks_ctx* c) {
     return st ? UGKS_ENUMERIC : UGKS_OK;
 }
 
-// The research S2CN2 wall variants a context accepts: S2CN2 only, and the combinations the reference's
-// option checks admit (mod_ImportPara.f90:455-471, :527-528): W1T on the kinetic wall, W1D with W1T, W2R
-// alone on the multiscale wall with ck = 1 and Pr = 1.
+// The research S2 wall variants a context accepts: the kinetic wall on both S2 methods (the implicit
+// micro wall treatment does not depend on it, mod_ImplicitMicro.f90:701,777), W1T, W1D and W2R on S2CN2,
+// in the combinations the reference's option checks admit (mod_ImportPara.f90:455-471, :527-528): W1T on
+// the kinetic wall, W1D with W1T, W2R alone on the multiscale wall with ck = 1 and Pr = 1.
 static int check_wall_variant(const ugks_params* p) {
     const int k = p->s2_kinetic_wall, t = p->s2_time_centered, d = p->s2_face_time, r = p->s2_shared_predictor;
     if ((k | t | d | r) & ~1) return UGKS_EINVAL;
     if (!(k | t | d | r)) return UGKS_OK;
-    if (p->method != UGKS_METHOD_S2CN2) return UGKS_EUNSUPPORTED;
+    const bool ho_kinetic = p->method == UGKS_METHOD_HIGH_ORDER_IMPLICIT && !(t | d | r);
+    if (p->method != UGKS_METHOD_S2CN2 && !ho_kinetic) return UGKS_EUNSUPPORTED;
     if (t && !k) return UGKS_EINVAL;
     if (d && !t) return UGKS_EINVAL;
     if (r && (k || t || d || p->ck != 1 || p->pr != 1.0)) return UGKS_EINVAL;

@@ -447,7 +447,8 @@ def case_from_config(groups, mesh=None):
         fw, tc, fd, sp = (variant[k] for k in ("flux_wall", "s2w1_time_centered", "s2w1d_face_time",
                                                "s2w2r_shared_predictor"))
         if fw == 0 or tc or fd or sp:   # the research wall variants (mod_ImportPara.f90:455-471, :527-528)
-            _need(method == "S2CN2", "the research S2 wall variants on a method other than S2CN2")
+            _need(method == "S2CN2" or not (tc or fd or sp),
+                  "the W1T / W1D / W2R wall variants on a method other than S2CN2")
             for key, val in (("S2W1_time_centered", tc), ("S2W1D_face_time_consistent", fd),
                              ("S2W2R_shared_predictor", sp)):
                 if val not in (0, 1):
