@@ -1114,9 +1114,11 @@ extern "C" int ugks_s2cn2_report(ugks_ctx* c, double* report) {
     return UGKS_OK;
 }
 
+// one step of a ugks_s2cn2_steps sequence: its dt is the one the previous step's k_cn_collide took from the
+// state it accepted (the sequence's first from the k_lo_timestep ugks_s2cn2_steps launches first)
 static cudaError_t enqueue_cn_step(ugks_ctx* c, int from) {
     return enqueue_s2cn2_step(c->P, c->Bs[from], c->T[from], c->Bs[1 - from], c->T[1 - from], c->C, c->stream,
-                              c->stream2, c->ev_fork, c->ev_join, nullptr, c->has_var ? &c->V : nullptr);
+                              c->stream2, c->ev_fork, c->ev_join, nullptr, c->has_var ? &c->V : nullptr, false);
 }
 
 // a pair of steps, set 0 -> set 1 -> set 0, captured once and replayed
@@ -1149,6 +1151,10 @@ extern "C" int ugks_s2cn2_steps(ugks_ctx* c, int nsteps, int* steps_done, double
     const double inject = (double)c->cn_reject_at;
     UGKS_CK(cudaMemcpyAsync(c->C.ledger + 8, &inject, sizeof inject, cudaMemcpyHostToDevice, c->stream));
     c->cn_reject_at = 0;
+    if (nsteps > 0) {   // the first step's TimeStep
+        UGKS_CK(launch_lo_timestep(c->P, c->Bs[0], c->stream));
+        c->launches += 1;
+    }
     const int pairs = nsteps / 2;
     if (pairs > 0) {
         r = build_cn_graph(c);
@@ -1156,7 +1162,7 @@ extern "C" int ugks_s2cn2_steps(ugks_ctx* c, int nsteps, int* steps_done, double
         for (int q = 0; q < pairs; ++q) UGKS_CK(cudaGraphLaunch(c->cgraph, c->stream));
     }
     if (nsteps % 2) UGKS_CK(enqueue_cn_step(c, 0));
-    c->launches += (long long)(kCnStepKernels + (c->has_var ? s2cn2_variant_kernels(c->P) : 0)) * nsteps;
+    c->launches += (long long)(kCnStepKernels - 1 + (c->has_var ? s2cn2_variant_kernels(c->P) : 0)) * nsteps;
     unsigned acc = 0;
     UGKS_CK(cudaMemcpyAsync(&acc, c->C.accepted, sizeof acc, cudaMemcpyDeviceToHost, c->stream));
     if (report) UGKS_CK(cudaMemcpyAsync(report, c->C.report, kCnReport * sizeof(double), cudaMemcpyDeviceToHost, c->stream));

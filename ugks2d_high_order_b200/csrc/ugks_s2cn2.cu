@@ -14,8 +14,10 @@
 //   k_cn_collide   : the 2x2 solve for the new heat flux and h_new = (rh + beta eq) / (1 + beta),
 //                    written into the other state set; the cnres / mmerr gates; a last-CTA epilogue
 //                    that takes the global conservation drift against the wall ledger and accepts
-//                    (ledger advanced, accepted counter incremented) or rejects (halt flag set: every
-//                    later kernel of the launch sequence returns at entry and the accepted state
+//                    (ledger advanced, accepted counter incremented, and the next step's dt taken from
+//                    the accepted state's per-cell dt_local, so the steps of a ugks_s2cn2_steps sequence
+//                    after its first launch no k_lo_timestep: 12 launches) or rejects (halt flag set:
+//                    every later kernel of the launch sequence returns at entry and the accepted state
 //                    stays in its set).
 // The state and the targets are double-buffered: a step reads set p and writes set 1-p, so a
 // rejected proposal never touches the accepted state and nothing is copied on acceptance.
@@ -229,6 +231,11 @@ __global__ void __launch_bounds__(NT) k_cn_collide(LoParams P, LoBuffers B, S2Bu
         d[2] = isfinite(mx / ws) ? mx / ws : INFINITY;
         d[3] = -rout[12]; d[4] = rout[13]; d[5] = -rout[14]; d[6] = rout[15];
         d[7] = fin ? 0.0 : 1.0;
+        if (!C.predict) {   // the proposal's dt_local: the next step's TimeStep when the step is accepted
+            bool okd;
+            const double dl = cell_dt(P, wn, okd);
+            Bo.dtl[c] = okd ? dl : NAN;
+        }
     }
     // last CTA: reduce the cells in a fixed order, take the conservation drift, accept or reject
     __threadfence();
@@ -238,12 +245,12 @@ __global__ void __launch_bounds__(NT) k_cn_collide(LoParams P, LoBuffers B, S2Bu
     if (!s_last) return;
     __threadfence();
     const int nc = P.nx * P.ny, nx = P.nx;
-    // sums [0..3] of the proposal's W; maxima [4..13]: 2 beta, cnres, mmerr, -min h, max h, -min b,
-    // max b, nonfinite, max|u|, max|v|
+    // sums [0..3] of the proposal's W; maxima [4..15]: 2 beta, cnres, mmerr, -min h, max h, -min b,
+    // max b, nonfinite, max|u|, max|v|, -min dt_local, a dt_local that failed
 #pragma unroll
     for (int m = 0; m < 4; ++m) acc[m] = 0.0;
 #pragma unroll
-    for (int m = 4; m < 14; ++m) acc[m] = -INFINITY;
+    for (int m = 4; m < 16; ++m) acc[m] = -INFINITY;
     for (int cc = tid; cc < nc; cc += blockDim.x) {
 #pragma unroll
         for (int m = 0; m < 4; ++m) acc[m] += __ldcg(C.ws + cc * 4 + m);
@@ -256,12 +263,17 @@ __global__ void __launch_bounds__(NT) k_cn_collide(LoParams P, LoBuffers B, S2Bu
         acc[9] = fmax(acc[9], -__ldcg(d + 5));
         acc[10] = fmax(acc[10], __ldcg(d + 6));
         acc[11] = fmax(acc[11], __ldcg(d + 7));
+        if (!C.predict) {
+            const double dl = __ldcg(Bo.dtl + cc);
+            acc[14] = fmax(acc[14], -dl);
+            acc[15] = fmax(acc[15], isnan(dl) ? 1.0 : 0.0);
+        }
     }
     for (int k = tid; k < nv; k += blockDim.x) {
         acc[12] = fmax(acc[12], fabs(B.u[k]));
         acc[13] = fmax(acc[13], fabs(B.v[k]));
     }
-    block_reduce_smem<4, 10>(acc, red, rout);
+    block_reduce_smem<4, 12>(acc, red, rout);
     if (tid == 0 && C.predict) {   // a predictor's advance_step: its finiteness and cnres / mmerr gates only
         if (!(rout[11] == 0.0 && rout[5] <= kCnGate && rout[6] <= kCnGate)) cn_stop(C, B, ST_W1T_PREDICTOR);
         *C.counter = 0u;
@@ -295,6 +307,11 @@ __global__ void __launch_bounds__(NT) k_cn_collide(LoParams P, LoBuffers B, S2Bu
 #pragma unroll
             for (int m = 0; m < 4; ++m) C.ledger[4 + m] = bal[m];
             *C.accepted = *C.accepted + 1u;
+            // TimeStep of the next step from the accepted state (mod_Solve.f90:373-421), as k_lo_timestep
+            // would take it at that step's start
+            if (rout[15] != 0.0) set_status(B.status, ST_GETPRIMARY);
+            Bo.dt[1] = Bo.dt[0];
+            Bo.dt[0] = P.fixed_dt > 0.0 ? P.fixed_dt : -rout[14];
         } else {
             cn_stop(C, B, ST_STEP_REJECTED);
         }
@@ -352,13 +369,14 @@ cudaError_t enqueue_cn_apply(const LoParams& P, const LoBuffers& B, const LoBuff
 // [18..21] wall balance after the step, [22] accepted, [23] accepted steps so far.
 cudaError_t enqueue_s2cn2_step(const LoParams& P, const LoBuffers& B, const S2Buffers& T, const LoBuffers& Bo,
                                const S2Buffers& To, const CnBuffers& C, cudaStream_t s, cudaStream_t s2,
-                               cudaEvent_t fork, cudaEvent_t join, long long* launches, const CnVariant* V) {
-    cudaError_t e = launch_lo_timestep(P, B, s);
+                               cudaEvent_t fork, cudaEvent_t join, long long* launches, const CnVariant* V,
+                               bool timestep) {
+    cudaError_t e = timestep ? launch_lo_timestep(P, B, s) : cudaSuccess;
     if (e == cudaSuccess) e = s2_enqueue(2, P, B, T, s, s2, fork, join);
     if (e == cudaSuccess && V) e = enqueue_s2cn2_variant(P, B, T, *V, s, s2, fork, join);
     if (e == cudaSuccess) e = enqueue_cn_stream(P, B, T, C, s);
     if (e == cudaSuccess) e = enqueue_cn_apply(P, B, Bo, To, C, s);
-    if (launches) *launches += kCnStepKernels + (V ? s2cn2_variant_kernels(P) : 0);
+    if (launches) *launches += kCnStepKernels - (timestep ? 0 : 1) + (V ? s2cn2_variant_kernels(P) : 0);
     return e;
 }
 

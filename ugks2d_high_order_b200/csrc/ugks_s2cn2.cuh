@@ -45,11 +45,12 @@ cudaError_t enqueue_s2cn2_variant(const LoParams& P, const LoBuffers& B, const S
 int s2cn2_variant_kernels(const LoParams& P);
 
 // One S2CN2 step from state set (B, T) into state set (Bo, To); see ugks_s2cn2.cu.  V: the wall variant's
-// buffers when P names a variant (nullptr otherwise).
+// buffers when P names a variant (nullptr otherwise).  timestep = false: the step's dt is the one its
+// predecessor's k_cn_collide took from the state it accepted (steps of one sequence after its first).
 cudaError_t enqueue_s2cn2_step(const LoParams& P, const LoBuffers& B, const S2Buffers& T, const LoBuffers& Bo,
                                const S2Buffers& To, const CnBuffers& C, cudaStream_t s, cudaStream_t s2,
                                cudaEvent_t fork, cudaEvent_t join, long long* launches,
-                               const CnVariant* V = nullptr);
+                               const CnVariant* V = nullptr, bool timestep = true);
 // The two halves of the step after the evolution, for the per-operator C ABI (ComputeResidual, then
 // S2NativeApplyUpdate): k_cn_stream of set (B, T); then the targets of the stream state into To and
 // k_cn_collide into Bo with the acceptance.  enqueue_s2cn2_step launches exactly these.
