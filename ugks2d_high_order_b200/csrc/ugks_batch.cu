@@ -23,6 +23,7 @@
 #include "ugks_s2cn2.cuh"
 
 namespace ugks {
+cudaError_t launch_lo_timestep(const LoParams& P, const LoBuffers& B, cudaStream_t s);
 cudaError_t launch_lo_init(const LoParams& P, const LoBuffers& B, double rho, double U, double V, double tn,
                            cudaStream_t s);
 }
@@ -252,7 +253,9 @@ static cudaError_t enqueue_all(ugks_batch* b, int nsteps) {
         for (int i = 0; i < b->n && e == cudaSuccess; ++i) {
             Inst& I = b->inst[i];
             const BSlot& S = b->slot[I.slot];
-            e = enqueue_s2cn2_step(I.P, I.B[p], I.T[p], I.B[1 - p], I.T[1 - p], I.C, S.s, S.s2, S.fork, S.join, nullptr);
+            // dt from the previous step's collide (the run's first step: the k_lo_timestep ugks_batch_run launches)
+            e = enqueue_s2cn2_step(I.P, I.B[p], I.T[p], I.B[1 - p], I.T[1 - p], I.C, S.s, S.s2, S.fork, S.join, nullptr,
+                                   nullptr, false);
         }
     }
     for (int s = 0; s < b->slots && e == cudaSuccess; ++s) {
@@ -314,6 +317,8 @@ extern "C" int ugks_batch_run(ugks_batch* b, int nsteps, int* steps_done, unsign
     BCK(cudaSetDevice(b->device));
     // a new sequence for every instance: clear counters, status, halt and accepted counts
     BCK(cudaMemsetAsync(b->flags, 0, (size_t)b->n * 4 * sizeof(unsigned), b->origin));
+    if (nsteps > 0)   // every instance's first TimeStep; each later step's dt is taken by the step before it
+        for (auto& I : b->inst) BCK(launch_lo_timestep(I.P, I.B[0], b->origin));
     const int pairs = nsteps / 2;
     if (pairs > 0) {
         int r = build_graph(b);
@@ -321,7 +326,7 @@ extern "C" int ugks_batch_run(ugks_batch* b, int nsteps, int* steps_done, unsign
         for (int q = 0; q < pairs; ++q) BCK(cudaGraphLaunch(b->graph, b->origin));
     }
     if (nsteps % 2) BCK(enqueue_all(b, 1));
-    b->launches += (long long)kCnStepKernels * nsteps * b->n;
+    b->launches += ((long long)(kCnStepKernels - 1) * nsteps + (nsteps > 0 ? 1 : 0)) * b->n;
     std::vector<unsigned> f((size_t)b->n * 4);
     BCK(cudaMemcpyAsync(f.data(), b->flags, f.size() * sizeof(unsigned), cudaMemcpyDeviceToHost, b->origin));
     BCK(cudaStreamSynchronize(b->origin));
