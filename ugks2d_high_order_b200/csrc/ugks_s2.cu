@@ -271,8 +271,9 @@ __global__ void __launch_bounds__(128) k_s2_macro(LoParams P, LoBuffers B, S2Buf
 constexpr int kS2NodeThreads = 128;
 
 // build_targets, closure part: one warp per (cell, volume node) -> the node scalars
-__global__ void __launch_bounds__(256, 2) k_s2_target_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
+__global__ void __launch_bounds__(256, 2) k_s2_target_nodes(LoParams P, LoBuffers B, S2Buffers SB, int qrec) {
     if (eval_cached(B)) return;
+    extern __shared__ double s_qrec[];
     const int nc = P.nx * P.ny, lane = threadIdx.x & 31;
     const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
     if (wid >= nc * 9) return;
@@ -283,7 +284,8 @@ __global__ void __launch_bounds__(256, 2) k_s2_target_nodes(LoParams P, LoBuffer
     WClosure C;
     C.jac = s_jac[threadIdx.x >> 5];
     WMke M;
-    const bool ok = w_closure(P, B, w, C) && w_make_mke(P, B, w, C, M);
+    const WQRec qr{qrec ? s_qrec + (threadIdx.x >> 5) * (((P.nvel + 31) >> 5) * 32) : nullptr};
+    const bool ok = w_closure(P, B, w, C, qr) && w_make_mke(P, B, w, C, M, qr);
     if (lane == 0) {
         if (ok) w_store_scalars(SB.tscal + (size_t)wid * kS2TScal, C, M);
         else set_status(B.status, ST_PROJECTION);
@@ -321,8 +323,9 @@ __global__ void __launch_bounds__(256) k_s2_target_sum(LoParams P, LoBuffers B, 
 // computes W0, the closure, make_mke, q0, the slope and time directions and Mt, and stores them as
 // the node's scalars (SB.fscal) for k_s2_face_flux.
 template <int NT, int MINB>
-__global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
+__global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffers B, S2Buffers SB, int qrec) {
     if (eval_cached(B)) return;
+    extern __shared__ double s_qrec[];
     const int nv = P.nvel, nx = P.nx, ny = P.ny, ck = P.ck, lane = threadIdx.x & 31, nr = (nv + 31) >> 5;
     const int nfx = nx * ny, nf = nfx + nx * (ny - 1);
     const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -352,7 +355,8 @@ __global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffer
     WClosure C;
     C.jac = s_jac[threadIdx.x >> 5];
     WMke M;
-    bool ok = w_closure(P, B, w0, C) && w_make_mke(P, B, w0, C, M);
+    const WQRec qr{qrec ? s_qrec + (threadIdx.x >> 5) * (nr * 32) : nullptr};
+    bool ok = w_closure(P, B, w0, C, qr) && w_make_mke(P, B, w0, C, M, qr);
     double q0x = 0.0, q0y = 0.0, tdl[4], tdr[4], tdt[4], tdm[4], wt[4], mt[5], tau = 0.0;
     if (ok) {   // q0 = heat(w0, f0 - analytic Maxwellian of w0)
         const double nrho = w0[0], nu = w0[1] / w0[0], nvv = w0[2] / w0[0];
@@ -380,7 +384,7 @@ __global__ void __launch_bounds__(NT, MINB) k_s2_face_nodes(LoParams P, LoBuffer
                 qacc[0] += 0.5 * s.w * cx * (c2 * dh + db);
                 qacc[1] += 0.5 * s.w * cy * (c2 * dh + db);
             }
-            const S2Q q = s2_q(tt, s.u, s.v);
+            const S2Q q = qr.at(tt, s, r);
             double dlh, dlb, drh, drb, dth, dtb;
             s2_dq(q, tdl, dlh, dlb);
             s2_dq(q, tdr, drh, drb);
@@ -532,8 +536,9 @@ __global__ void __launch_bounds__(256, 3) k_s2_face_flux(LoParams P, LoBuffers B
 // wall face nodes (s2w2_wall_node, mod_S2MultiscaleWall.f90:45-184): one warp per (wall face,
 // Gauss node); bottom faces of row 0, then top faces of row ny-1.  Node fluxes go to the node
 // buffers after the interior faces.
-__global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers B, S2Buffers SB) {
+__global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers B, S2Buffers SB, int qrec) {
     if (eval_cached(B)) return;
+    extern __shared__ double s_qrec[];
     const int nv = P.nvel, nx = P.nx, ny = P.ny, ck = P.ck, lane = threadIdx.x & 31, nr = (nv + 31) >> 5;
     const int nf = nx * ny + nx * (ny - 1);
     const int wid = (int)((blockIdx.x * blockDim.x + threadIdx.x) >> 5);
@@ -556,7 +561,8 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
     __shared__ double s_jac[8][16];
     WClosure C;
     C.jac = s_jac[threadIdx.x >> 5];
-    bool ok = pp > 0.0 && isfinite(pp) && w_closure(P, B, wwall, C);
+    const WQRec qr{qrec ? s_qrec + (threadIdx.x >> 5) * (nr * 32) : nullptr};
+    bool ok = pp > 0.0 && isfinite(pp) && w_closure(P, B, wwall, C, qr);
     auto rec = [&](const WVel& s, int field) {
         return SB.rec[rec_wall(nx, ny, top, i, field, g, nv) + s.k];
     };
@@ -597,9 +603,9 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
     }
     // the incident micro flux g_in and the reflected wall Maxwellian of one velocity
     const S2Th tt = s2_th(C.th, ck);
-    auto gin = [&](const WVel& s, double& ginh, double& ginb, double& wallh, double& wallb, double& mh, double& mb,
-                   double& corrh, double& corrb) {
-        const S2Q q = s2_q(tt, s.u, s.v);
+    auto gin = [&](const WVel& s, int r, double& ginh, double& ginb, double& wallh, double& wallb, double& mh,
+                   double& mb, double& corrh, double& corrb) {
+        const S2Q q = qr.at(tt, s, r);
         mh = q.qh;
         mb = q.qb;
         wallh = mh / prim_g[0];
@@ -632,7 +638,7 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
             double ginh, ginb, wallh, wallb, mh, mb, ch, cb;
-            gin(s, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
+            gin(s, r, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
             if (side * s.v > 0.0) acc[0] += s.w * s.v * ginh;
             else acc[1] += dt * s.w * s.v * wallh;
         }
@@ -650,7 +656,7 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
             double ginh, ginb, wallh, wallb, mh, mb, ch, cb, fh, fb;
-            gin(s, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
+            gin(s, r, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
             if (side * s.v > 0.0) { fh = s.v * ginh; fb = s.v * ginb; }
             else { fh = dt * s.v * rhow * wallh; fb = dt * s.v * rhow * wallb; }
             acc[0] += s.w * fh; acc[1] += s.w * (s.u * fh); acc[2] += s.w * (s.v * fh);
@@ -674,7 +680,7 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
             double ginh, ginb, wallh, wallb, mh, mb, ch, cb;
-            gin(s, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
+            gin(s, r, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
             if (side * s.v > 0.0) {
                 acc[0] += s.w * s.v * rec(s, 0);
                 acc[1] += s.w * s.v * qk(s, mh, ch, 0, 2, 3);
@@ -690,7 +696,7 @@ __global__ void __launch_bounds__(256, 2) k_s2_wall_nodes(LoParams P, LoBuffers 
         for (int r = 0; r < nr && ok; ++r) {
             const WVel s = wvel(B, nv, r);
             double ginh, ginb, wallh, wallb, mh, mb, ch, cb, c0, c1, c2, c3;
-            gin(s, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
+            gin(s, r, ginh, ginb, wallh, wallb, mh, mb, ch, cb);
             if (side * s.v > 0.0) {
                 c0 = s.v * rec(s, 0);
                 c1 = s.v * rec(s, 1);
@@ -781,7 +787,27 @@ __global__ void __launch_bounds__(256) k_s2_combine(LoParams P, LoBuffers B, S2B
 }
 
 
-cudaError_t prepare_s2() { return s2_upload_tables(); }
+// Shared memory for the closure kernels' Maxwellian records (WQRec): one record of the velocity set
+// per warp, used when it fits these caps.  The caps keep the kernels' resident CTAs per SM: three
+// 128-thread face-node CTAs (up to 2304 = 48^2 velocities), two 256-thread target- and face-node CTAs
+// (up to 1760 velocities).  The wall-node kernel has only 6 nx warps: one CTA per SM will do.
+constexpr int kQRecCap128x3 = 72 * 1024, kQRecCap256x2 = 110 * 1024, kQRecCapWall = 200 * 1024;
+
+cudaError_t prepare_s2() {
+    cudaError_t e = s2_upload_tables();
+    const auto dyn = cudaFuncAttributeMaxDynamicSharedMemorySize;
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_s2_face_nodes<kS2NodeThreads, 3>, dyn, kQRecCap128x3);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_s2_face_nodes<256, 2>, dyn, kQRecCap256x2);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_s2_target_nodes, dyn, kQRecCap256x2);
+    if (e == cudaSuccess) e = cudaFuncSetAttribute(k_s2_wall_nodes, dyn, kQRecCapWall);
+    return e;
+}
+
+// bytes of the Maxwellian records of a CTA of `threads` threads, 0 (no records) above `cap`
+static int qrec_bytes(int nv, int threads, int cap) {
+    const long long b = (long long)(threads / 32) * ((nv + 31) / 32) * 32 * (long long)sizeof(double);
+    return b <= cap ? (int)b : 0;
+}
 
 
 // which 0: the S2 cold start; 1: the S2 Evolution of one pseudo-step (targets, reconstruction,
@@ -816,7 +842,8 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     }
     if (e == cudaSuccess && targets) {
         cudaStream_t ts = side_targets ? s2 : s;
-        k_s2_target_nodes<<<warps((long long)nc * 9), 256, 0, ts>>>(P, B, S);
+        const int qb = qrec_bytes(nv, 256, kQRecCap256x2);
+        k_s2_target_nodes<<<warps((long long)nc * 9), 256, qb, ts>>>(P, B, S, qb > 0);
         e = cudaGetLastError();
         if (e == cudaSuccess) {
             k_s2_target_sum<<<dim3((unsigned)((nv + 255) / 256), (unsigned)nc), 256, 0, ts>>>(P, B, S);
@@ -832,12 +859,21 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     if (e == cudaSuccess) e = cudaStreamWaitEvent(s2, fork, 0);
     if (e == cudaSuccess) {
         if (P.s2_kinetic) e = launch_s2_w1_walls(P, B, S, s2);
-        else { k_s2_wall_nodes<<<warps(2LL * nx * 3), 256, 0, s2>>>(P, B, S); e = cudaGetLastError(); }
+        else {
+            const int qb = qrec_bytes(nv, 256, kQRecCapWall);
+            k_s2_wall_nodes<<<warps(2LL * nx * 3), 256, qb, s2>>>(P, B, S, qb > 0);
+            e = cudaGetLastError();
+        }
     }
     if (e == cudaSuccess) e = cudaEventRecord(join, s2);
     if (e == cudaSuccess) {
-        if (S.concurrent) k_s2_face_nodes<256, 2><<<warps((long long)nf * 3), 256, 0, s>>>(P, B, S);
-        else k_s2_face_nodes<kS2NodeThreads, 3><<<node_ctas((long long)nf * 3), kS2NodeThreads, 0, s>>>(P, B, S);
+        if (S.concurrent) {
+            const int qb = qrec_bytes(nv, 256, kQRecCap256x2);
+            k_s2_face_nodes<256, 2><<<warps((long long)nf * 3), 256, qb, s>>>(P, B, S, qb > 0);
+        } else {
+            const int qb = qrec_bytes(nv, kS2NodeThreads, kQRecCap128x3);
+            k_s2_face_nodes<kS2NodeThreads, 3><<<node_ctas((long long)nf * 3), kS2NodeThreads, qb, s>>>(P, B, S, qb > 0);
+        }
         e = cudaGetLastError();
     }
     if (e == cudaSuccess) {

@@ -389,15 +389,23 @@ __device__ __forceinline__ S2Th s2_th(const double th[4], int ck) {
 struct S2Q {
     double qh, qb, ld[4], ldb[4];
 };
-__device__ __forceinline__ S2Q s2_q(const S2Th& t, double u, double v) {
+// the closure Maxwellian's value alone: the one exponential of s2_q
+__device__ __forceinline__ double s2_qh(const S2Th& t, double u, double v) {
+    const double du = u - t.u, dv = v - t.v, c2 = du * du + dv * dv;
+    return t.pref * exp(-c2 * t.itw);
+}
+// s2_q with that value given (the same theta and velocity), e.g. recorded by the closure's last
+// Newton evaluation
+__device__ __forceinline__ S2Q s2_q_at(const S2Th& t, double u, double v, double qh) {
     S2Q q;
     const double du = u - t.u, dv = v - t.v, c2 = du * du + dv * dv;
-    q.qh = t.pref * exp(-c2 * t.itw);
+    q.qh = qh;
     q.ld[0] = t.ir; q.ld[1] = 2.0 * du * t.itw; q.ld[2] = 2.0 * dv * t.itw; q.ld[3] = -t.itw + c2 * (t.itw * t.itw);
     q.qb = t.ckh * q.qh;
     q.ldb[0] = q.ld[0]; q.ldb[1] = q.ld[1]; q.ldb[2] = q.ld[2]; q.ldb[3] = q.ld[3] + t.itw;
     return q;
 }
+__device__ __forceinline__ S2Q s2_q(const S2Th& t, double u, double v) { return s2_q_at(t, u, v, s2_qh(t, u, v)); }
 
 // dq for a moment direction m (closure_first_direction): td = solve(jac, m) by thread `who`,
 // broadcast through S.v[base..base+3]
@@ -431,6 +439,17 @@ __device__ __forceinline__ WVel wvel(const LoBuffers& B, int nv, int r) {
     s.w = s.ok ? __ldg(B.w + s.k) : 0.0;
     return s;
 }
+
+// A warp's record of the closure Maxwellian's values at its converged theta, one per velocity
+// (k = lane + 32 r at [r * 32 + lane]: every lane reads back only what it wrote).  The closure, the
+// make_mke passes and the node kernels' later passes all evaluate the Maxwellian at that theta, so
+// with a record they take its exponentials once.  nullptr: no record (each pass evaluates them).
+struct WQRec {
+    double* q;
+    __device__ __forceinline__ S2Q at(const S2Th& t, const WVel& s, int r) const {
+        return q ? s2_q_at(t, s.u, s.v, q[r * 32 + (threadIdx.x & 31)]) : s2_q(t, s.u, s.v);
+    }
+};
 
 
 __device__ __forceinline__ double s2_scaled(const double r[4], const double w[4]) {
@@ -474,7 +493,9 @@ __device__ __forceinline__ int w_newton_next(bool new_iter, const WClosure& C, c
 }
 
 // solve_q_first (mod_CorrectedWF2DClosure.f90:331-426) for the target moments w by one warp
-__device__ bool w_closure(const LoParams& P, const LoBuffers& B, const double w[4], WClosure& C) {
+// With a record (qr.q != nullptr) every evaluation writes its Maxwellian values there, so on success
+// it holds those of the converged theta C.th (the last evaluation is the accepted, converged one).
+__device__ bool w_closure(const LoParams& P, const LoBuffers& B, const double w[4], WClosure& C, WQRec qr = {nullptr}) {
     const int nv = P.nvel, ck = P.ck, nr = (nv + 31) >> 5;
     double trial[4];
     {   // primitive_from_conserved_2d (mod_CorrectedWF2DEquilibrium.f90:25-41)
@@ -498,6 +519,7 @@ __device__ bool w_closure(const LoParams& P, const LoBuffers& B, const double w[
         for (int r = 0; r < nr; ++r) {
             const WVel s = wvel(B, nv, r);
             const S2Q q = s2_q(tt, s.u, s.v);
+            if (qr.q) qr.q[r * 32 + (threadIdx.x & 31)] = q.qh;
             const double e2 = s.u * s.u + s.v * s.v;
 #pragma unroll
             for (int a = 0; a < 4; ++a) {
@@ -568,10 +590,9 @@ __device__ __forceinline__ void w_mke_raw(const WMke& M, const S2Q& q, int ck, d
     kyh = M.coeff * cy * shh * q.qh; kyb = M.coeff * cy * shb * q.qb;
 }
 
-// M, K_x, K_y of one velocity from the node scalars
-__device__ __forceinline__ void w_mke_at(const S2Th& th, const WMke& M, int ck, double uk, double vk, S2Q& q,
-                                         double& mh, double& mb, double& kxh, double& kxb, double& kyh, double& kyb) {
-    q = s2_q(th, uk, vk);
+// M, K_x, K_y of one velocity from the node scalars and the velocity's s2_q
+__device__ __forceinline__ void w_mke_q(const WMke& M, int ck, double uk, double vk, const S2Q& q, double& mh,
+                                        double& mb, double& kxh, double& kxb, double& kyh, double& kyb) {
     mh = q.qh;
     mb = q.qb;
     w_mke_raw(M, q, ck, uk, vk, kxh, kxb, kyh, kyb);
@@ -581,9 +602,16 @@ __device__ __forceinline__ void w_mke_at(const S2Th& th, const WMke& M, int ck, 
     s2_dq(q, M.tdy, dh, db);
     kyh = kyh - dh; kyb = kyb - db;
 }
+__device__ __forceinline__ void w_mke_at(const S2Th& th, const WMke& M, int ck, double uk, double vk, S2Q& q,
+                                         double& mh, double& mb, double& kxh, double& kxb, double& kyh, double& kyb) {
+    q = s2_q(th, uk, vk);
+    w_mke_q(M, ck, uk, vk, q, mh, mb, kxh, kxb, kyh, kyb);
+}
 
 // Returns the gate (moments of M equal w, K_x, K_y moment-free, all finite, to 2e-12).
-__device__ bool w_make_mke(const LoParams& P, const LoBuffers& B, const double w[4], const WClosure& C, WMke& M) {
+// qr: the closure's record of the Maxwellian at C.th, or none.
+__device__ bool w_make_mke(const LoParams& P, const LoBuffers& B, const double w[4], const WClosure& C, WMke& M,
+                           WQRec qr = {nullptr}) {
     const int nv = P.nvel, ck = P.ck, nr = (nv + 31) >> 5;
     double rho, th;
     const bool pok = s2_primitive(w, ck, rho, M.ux, M.vy, th);
@@ -595,7 +623,7 @@ __device__ bool w_make_mke(const LoParams& P, const LoBuffers& B, const double w
     const S2Th tt = s2_th(C.th, ck);
     for (int r = 0; r < nr; ++r) {
         const WVel s = wvel(B, nv, r);
-        const S2Q q = s2_q(tt, s.u, s.v);
+        const S2Q q = qr.at(tt, s, r);
         double kxh, kxb, kyh, kyb;
         w_mke_raw(M, q, ck, s.u, s.v, kxh, kxb, kyh, kyb);
         const double e2 = s.u * s.u + s.v * s.v;
@@ -616,9 +644,9 @@ __device__ bool w_make_mke(const LoParams& P, const LoBuffers& B, const double w
     for (int m = 0; m < 16; ++m) acc[m] = 0.0;
     for (int r = 0; r < nr; ++r) {
         const WVel s = wvel(B, nv, r);
-        S2Q q;
+        const S2Q q = qr.at(tt, s, r);
         double mh, mb, kxh, kxb, kyh, kyb;
-        w_mke_at(tt, M, ck, s.u, s.v, q, mh, mb, kxh, kxb, kyh, kyb);
+        w_mke_q(M, ck, s.u, s.v, q, mh, mb, kxh, kxb, kyh, kyb);
         const double e2 = s.u * s.u + s.v * s.v, cx = s.u - M.ux, cy = s.v - M.vy, c2 = cx * cx + cy * cy;
         acc[0] += s.w * mh; acc[1] += s.w * s.u * mh; acc[2] += s.w * s.v * mh; acc[3] += 0.5 * s.w * (e2 * mh + mb);
         acc[4] += s.w * kxh; acc[5] += s.w * s.u * kxh; acc[6] += s.w * s.v * kxh; acc[7] += 0.5 * s.w * (e2 * kxh + kxb);
