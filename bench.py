@@ -150,8 +150,15 @@ class ClockSampler:
         self.index, self.kind, self.period = index, kind, period
         self.samples, self.reasons, self.smax = [], set(), None
         self._stop = threading.Event()
+        self._lock = threading.Lock()
         self.proc = None
         self.lines = []
+
+    def begin(self):
+        """Start of the timed window: the samples and reasons taken so far (the sampler runs from before
+        the warm-up, so its start-up is not inside the window) are dropped."""
+        with self._lock:
+            self.samples, self.reasons = [], set()
 
     def start(self):
         if self.kind == "none":
@@ -185,11 +192,13 @@ class ClockSampler:
         nv = self.nv
         while not self._stop.is_set():
             try:
-                self.samples.append(float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)))
+                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
                 mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
-                for name, bit in self.REASONS.items():
-                    if mask & bit:
-                        self.reasons.add(name)
+                with self._lock:
+                    self.samples.append(mhz)
+                    for name, bit in self.REASONS.items():
+                        if mask & bit:
+                            self.reasons.add(name)
             except Exception:
                 pass
             self._stop.wait(self.period)
@@ -201,13 +210,14 @@ class ClockSampler:
             if len(parts) < 9:
                 continue
             try:
-                self.samples.append(float(parts[1]))
-                self.smax = float(parts[2])
+                mhz, self.smax = float(parts[1]), float(parts[2])
             except ValueError:
                 continue
-            for n, v in zip(names, parts[5:9]):
-                if v.lower().startswith("active"):
-                    self.reasons.add(n)
+            with self._lock:
+                self.samples.append(mhz)
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower().startswith("active"):
+                        self.reasons.add(n)
 
     def stop(self):
         if self.kind == "none":
@@ -482,24 +492,28 @@ def main():
         return done
 
     # ---------------- device-resident timing: K cold-start solves to the gate
+    # The clock sampler starts before the warm-up (its library start-up stays out of the timed window)
+    # and keeps only the samples taken inside the window.
+    sampler = ClockSampler(local, args.sampler, args.sampler_period)
+    sampler.start()
     for _ in range(args.warmup):
         solve()
     launches0 = s.launch_count
-    sampler = ClockSampler(local, args.sampler, args.sampler_period)
-    sampler.start()
     barrier()
-    ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    sampler.begin()
+    evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     pseudo = []
     with torch.cuda.stream(stream):
-        ev0.record(stream)
-        for _ in range(args.steps):
+        evs[0].record(stream)
+        for k in range(args.steps):
             flush.zero_()          # L2 flush between bench steps (256 MB > 126 MB L2)
             pseudo.append(solve())
-        ev1.record(stream)
-    ev1.synchronize()
+            evs[k + 1].record(stream)
+    evs[-1].synchronize()
     barrier()
     clocks = sampler.stop()
-    ms = max_over_ranks(ev0.elapsed_time(ev1))
+    ms = max_over_ranks(evs[0].elapsed_time(evs[-1]))
+    solve_ms = [evs[k].elapsed_time(evs[k + 1]) for k in range(args.steps)]
     launches = s.launch_count - launches0
     units = nc * nv * sum(pseudo)
     value = world * units / (ms * 1e-3)
@@ -887,6 +901,7 @@ def main():
                 "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
                 "time_to_steady_s": ms / args.steps * 1e-3,
                 "pseudo_steps_to_gate": pseudo,
+                "solve_ms": solve_ms,
                 "config": {"workload": WORKLOAD, "updates_per_pseudo_step": nc * nv,
                            "parallelism": f"replicas x{world}" if world > 1 else "single instance",
                            "l2": "flushed (256 MB write) between bench steps; the 8.4 MB state is L2-resident within a solve"},

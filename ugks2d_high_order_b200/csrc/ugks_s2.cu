@@ -803,10 +803,14 @@ cudaError_t prepare_s2() {
     return e;
 }
 
-// bytes of the Maxwellian records of a CTA of `threads` threads, 0 (no records) above `cap`
-static int qrec_bytes(int nv, int threads, int cap) {
+// bytes of the Maxwellian records of a CTA of `threads` threads, 0 (no records) above `cap`.  Many
+// instances on concurrent streams (S2Buffers::concurrent) take none: their kernels share SMs with other
+// instances' kernels, and the records' shared-memory carve-out cost the batch more than it saved it
+// (7.47e8 -> 7.44e8 updates/s for the 256-instance distribution, same GPU); the values are the same
+// either way.
+static int qrec_bytes(const S2Buffers& S, int nv, int threads, int cap) {
     const long long b = (long long)(threads / 32) * ((nv + 31) / 32) * 32 * (long long)sizeof(double);
-    return b <= cap ? (int)b : 0;
+    return !S.concurrent && b <= cap ? (int)b : 0;
 }
 
 
@@ -842,7 +846,7 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     }
     if (e == cudaSuccess && targets) {
         cudaStream_t ts = side_targets ? s2 : s;
-        const int qb = qrec_bytes(nv, 256, kQRecCap256x2);
+        const int qb = qrec_bytes(S, nv, 256, kQRecCap256x2);
         k_s2_target_nodes<<<warps((long long)nc * 9), 256, qb, ts>>>(P, B, S, qb > 0);
         e = cudaGetLastError();
         if (e == cudaSuccess) {
@@ -860,7 +864,7 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     if (e == cudaSuccess) {
         if (P.s2_kinetic) e = launch_s2_w1_walls(P, B, S, s2);
         else {
-            const int qb = qrec_bytes(nv, 256, kQRecCapWall);
+            const int qb = qrec_bytes(S, nv, 256, kQRecCapWall);
             k_s2_wall_nodes<<<warps(2LL * nx * 3), 256, qb, s2>>>(P, B, S, qb > 0);
             e = cudaGetLastError();
         }
@@ -868,10 +872,10 @@ cudaError_t s2_enqueue(int which, const LoParams& P, const LoBuffers& B, const S
     if (e == cudaSuccess) e = cudaEventRecord(join, s2);
     if (e == cudaSuccess) {
         if (S.concurrent) {
-            const int qb = qrec_bytes(nv, 256, kQRecCap256x2);
+            const int qb = qrec_bytes(S, nv, 256, kQRecCap256x2);
             k_s2_face_nodes<256, 2><<<warps((long long)nf * 3), 256, qb, s>>>(P, B, S, qb > 0);
         } else {
-            const int qb = qrec_bytes(nv, kS2NodeThreads, kQRecCap128x3);
+            const int qb = qrec_bytes(S, nv, kS2NodeThreads, kQRecCap128x3);
             k_s2_face_nodes<kS2NodeThreads, 3><<<node_ctas((long long)nf * 3), kS2NodeThreads, qb, s>>>(P, B, S, qb > 0);
         }
         e = cudaGetLastError();
