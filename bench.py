@@ -38,6 +38,7 @@ replicas ("scaling": "weak").  --impl reference times the CPU restatement of the
 cores on the same workload.
 """
 import argparse
+import gc
 import json
 import os
 import statistics
@@ -500,6 +501,8 @@ def main():
         solve()
     launches0 = s.launch_count
     barrier()
+    gc.collect()
+    gc.disable()           # no collector pause between the solves' host calls inside the timed window
     sampler.begin()
     evs = [torch.cuda.Event(enable_timing=True) for _ in range(args.steps + 1)]
     pseudo = []
@@ -510,6 +513,7 @@ def main():
             pseudo.append(solve())
             evs[k + 1].record(stream)
     evs[-1].synchronize()
+    gc.enable()
     barrier()
     clocks = sampler.stop()
     ms = max_over_ranks(evs[0].elapsed_time(evs[-1]))
@@ -535,6 +539,8 @@ def main():
     rep = np.zeros(80)
     e_pseudo = 0
     barrier()
+    gc.collect()
+    gc.disable()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     with torch.cuda.stream(stream):
         e0.record(stream)
@@ -550,6 +556,7 @@ def main():
             e_pseudo += done_c.value
         e1.record(stream)
     e1.synchronize()
+    gc.enable()
     barrier()
     ems = max_over_ranks(e0.elapsed_time(e1))
     e2e_value = world * nc * nv * e_pseudo / (ems * 1e-3)
