@@ -894,7 +894,7 @@ def main():
         try:
             cpu = cpu_baseline(case, vel)
             cpu["time_to_steady_estimate_s"] = cpu["seconds_per_pseudo_step"] * (sum(pseudo) / len(pseudo))
-        except Exception as e:   # the checker is optional for the device number
+        except Exception as e:   # the oracle sample is optional for the device number
             cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "port", "sample": f"unavailable: {e}"}
         try:
             high_order["cpu_baseline"] = cpu_sample_high_order(vel)

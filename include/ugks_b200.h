@@ -249,8 +249,8 @@ int ugks_s2cn2_step_vjp(ugks_ctx* ctx, const double* gh, const double* gb, const
                         double* gh_in, double* gb_in, double* gW_in, double* grad);
 
 /* Batched S2CN2: many independent Couette instances of uneven grid and velocity-set sizes advanced
- * together (BASELINE's batched form; no counterpart routine in the reference, whose runs are one case
- * per job).  Each instance is described by ugks_params (method UGKS_METHOD_S2CN2) and its velocity
+ * together (a parameter sweep of the Couette case run as one job; no counterpart routine in the
+ * reference, whose runs are one case per job).  Each instance is described by ugks_params (method UGKS_METHOD_S2CN2) and its velocity
  * table.  Instances own their persistent state (two state sets, two target sets, ledger: about 16
  * doubles per cell-velocity); the per-step scratch lives in up to max_streams slots sized for the
  * largest instance, instances being assigned to slots largest-first.  One CUDA graph launch advances
