@@ -602,8 +602,8 @@ def main():
     roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                 "traffic": TRAFFIC_PER_PSEUDO_STEP_8X64X1024 if (case.nx, case.ny, nv) == (8, 64, 1024) else None,
                 "traffic_source": "ncu launch list, cold-cache sum over one pseudo-step's launches",
-                "kernel": "ImplicitSteady pseudo-step (one CUDA graph node group, %d launches)"
-                % (15 + case.macro_sweeps),
+                "kernel": "ImplicitSteady pseudo-step (one CUDA graph node group, 16 launches: the PR(2) "
+                          "sweeps share one)",
                 "bytes_per_update": BYTES_PER_UPDATE_PSEUDO_STEP, "peak_source": peak_kind,
                 "pseudo_step_us": ms / args.steps / (sum(pseudo) / len(pseudo)) * 1e3,
                 "dominant_stage": {"stage": top, "kernel": kname, "avg_us_per_launch": avg_s * 1e6,

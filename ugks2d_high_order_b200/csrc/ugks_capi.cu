@@ -262,9 +262,9 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
         const size_t i_scr = Q.high_order ? itake(s2_scratch_doubles(nx, ny, nv)) : 0;
         if (e == cudaSuccess && Q.high_order) e = prepare_s2();
         if (e == cudaSuccess) e = cudaMalloc(&c->imem, io * sizeof(double));
-        if (e == cudaSuccess) e = cudaMalloc(&c->iflags, 4 * sizeof(unsigned));
+        if (e == cudaSuccess) e = cudaMalloc(&c->iflags, 6 * sizeof(unsigned));
         if (e == cudaSuccess) e = cudaMemsetAsync(c->imem, 0, io * sizeof(double), c->stream);
-        if (e == cudaSuccess) e = cudaMemsetAsync(c->iflags, 0, 4 * sizeof(unsigned), c->stream);
+        if (e == cudaSuccess) e = cudaMemsetAsync(c->iflags, 0, 6 * sizeof(unsigned), c->stream);
         if (e == cudaSuccess) {
             double* m = c->imem;
             ImBuffers& I = c->I;
@@ -279,7 +279,7 @@ extern "C" int ugks_ctx_create(const ugks_params* p, const double* u, const doub
                 I.s2.kxb = m + i_tg[3]; I.s2.kyh = m + i_tg[4]; I.s2.kyb = m + i_tg[5];
                 s2_bind_scratch(I.s2, m + i_scr, nx, ny, nv);
             }
-            I.mask = c->iflags; I.counter = c->iflags + 2; I.stopw = c->iflags + 3;
+            I.mask = c->iflags; I.counter = c->iflags + 2; I.stopw = c->iflags + 3; I.prbar = c->iflags + 4;
         }
     }
     if (e == cudaSuccess && p->method == UGKS_METHOD_S2CN2) {

@@ -727,13 +727,52 @@ __device__ __forceinline__ void pr_wave_sync(int warps) {
 // when one warp did it alone), the first 4 x min(dcells, 32) relax.
 constexpr int kPrThreads = 256;
 
-// first: the sweep also does the PR(2) set-up of its slab (pr_prep_item, straight into shared memory)
-// and starts from the zero correction (X unused); when it is not also the last sweep, CTA 0 resets
-// the admissible-alpha masks.  last: the sweep also does BuildPredictedMacroState
-// (mod_ImplicitMacro.f90:159-185) for its cells: the admissible alpha levels of W + alpha Y,
-// ANDed into the macro mask.
+// Grid barrier between the sweeps of one launch (gridDim.x = nslab CTAs, all resident: a cooperative
+// launch).  bar[0] counts the arrivals, bar[1] is the generation: every CTA reads the generation
+// before it arrives, the last arrival resets the count and advances the generation, the others poll
+// it.  The CTAs' global writes before the barrier are visible to every CTA after it (bar.sync, then a
+// device-scope fence by the arriving thread; a fence after the wait).  Bounded: a CTA that polls
+// kPrBarrierPolls times without the generation moving returns false.
+constexpr long long kPrBarrierPolls = 1LL << 22;   // with 64 ns pauses: about 0.3-1 s
+__device__ bool pr_grid_barrier(unsigned* bar) {
+    __shared__ int s_ok;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        int ok = 1;
+        volatile unsigned* gen = bar + 1;
+        const unsigned g0 = *gen;
+        __threadfence();
+        if (atomicAdd(bar, 1u) == gridDim.x - 1) {
+            atomicExch(bar, 0u);
+            __threadfence();
+            atomicAdd(bar + 1, 1u);
+        } else {
+            long long n = 0;
+            while (*gen == g0) {
+                if (++n > kPrBarrierPolls) { ok = 0; break; }
+                __nanosleep(64);
+            }
+        }
+        __threadfence();
+        s_ok = ok;
+    }
+    __syncthreads();
+    return s_ok != 0;
+}
+
+// first: the launch also does the PR(2) set-up of its slab (pr_prep_item, straight into shared memory)
+// and starts from the zero correction (X unused as input); when the launch does not also end with the
+// last sweep, or does more than one sweep, CTA 0 resets the admissible-alpha masks.  last: the launch
+// ends with the last sweep and also does BuildPredictedMacroState (mod_ImplicitMacro.f90:159-185) for
+// its cells: the admissible alpha levels of W + alpha Y, ANDed into the macro mask.
+// sweeps: the sweeps this launch does.  Sweep k reads the halo corrections of sweep k-1 from (k odd ? Y
+// : X) and writes its own to the other buffer, so they end in Y when `sweeps` is odd, else in X, as
+// `sweeps` one-sweep launches with the buffers swapped between them would leave them.  Between sweeps
+// the CTAs meet at a grid barrier (sweeps > 1 needs a cooperative launch); each CTA keeps its
+// interior cells' corrections, states and flux pairs in shared memory, which are bitwise those the
+// next launch would rebuild from Y, and reloads only its halo.
 __global__ void __launch_bounds__(kPrThreads, 1) k_im_pr2_sweep(LoParams P, LoBuffers B, ImParams Q, ImBuffers I,
-                                                             const double* X, double* Y, int first, int last) {
+                                                             double* X, double* Y, int first, int last, int sweeps) {
     if (I.state[IS_STOP] != 0.0) return;
     extern __shared__ double sm[];
     const int s = blockIdx.x, rows = P.ny / Q.nslab, nx = P.nx, ny = P.ny;
@@ -761,8 +800,9 @@ __global__ void __launch_bounds__(kPrThreads, 1) k_im_pr2_sweep(LoParams P, LoBu
         sW[q] = B.W[c0 * 4 + q];
         sR[q] = I.rate_w[c0 * 4 + q];
     }
+    bool dead = false;   // the set-up failed in this slab (ST_GETPRIMARY set): the CTA only meets the barriers
     if (first) {
-        if (!last && s == 0 && threadIdx.x == 0) { I.mask[0] = 0xffffffffu; I.mask[1] = 0xffffffffu; }
+        if ((!last || sweeps > 1) && s == 0 && threadIdx.x == 0) { I.mask[0] = 0xffffffffu; I.mask[1] = 0xffffffffu; }
         int prep_bad = 0;
         for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) {
             double gam, foi[4], foj[4];
@@ -771,7 +811,8 @@ __global__ void __launch_bounds__(kPrThreads, 1) k_im_pr2_sweep(LoParams P, LoBu
 #pragma unroll
             for (int k = 0; k < 4; ++k) { sFi[k * ncf + q] = foi[k]; sFj[k * ncf + q] = foj[k]; }
         }
-        if (__syncthreads_or(prep_bad)) return;   // the sequence has stopped (ST_GETPRIMARY)
+        dead = __syncthreads_or(prep_bad) != 0;   // the sequence has stopped (ST_GETPRIMARY)
+        if (dead && sweeps == 1) return;
     } else {
         for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) sG[q] = I.pr_gamma[c0 * 4 + q];
         for (int q = threadIdx.x; q < ncs * 16; q += blockDim.x) {
@@ -779,29 +820,34 @@ __global__ void __launch_bounds__(kPrThreads, 1) k_im_pr2_sweep(LoParams P, LoBu
             sFj[(q & 3) * ncf + (q >> 2)] = I.pr_foj[c0 * 16 + q];
         }
     }
-    // interior and halo cells: correction, state, flux pair (halo rows beyond a wall stay unused)
-    for (int l = threadIdx.x; l < nall; l += blockDim.x) {
-        int g;
-        if (l < ncs) g = c0 + l;
-        else if (l < ncs + rows) g = (s * rows + (l - ncs)) * nx + (nx - 1);
-        else if (l < ncs + 2 * rows) g = (s * rows + (l - ncs - rows)) * nx;
-        else if (l < ncs + 2 * rows + nx) g = s * rows > 0 ? (s * rows - 1) * nx + (l - ncs - 2 * rows) : -1;
-        else g = (s + 1) * rows < ny ? ((s + 1) * rows) * nx + (l - ncs - 2 * rows - nx) : -1;
-        double y[4] = {0.0, 0.0, 0.0, 0.0}, t[4] = {1.0, 0.0, 0.0, 1.0};
-        if (g >= 0) {
+    // interior and halo cells: correction, state, flux pair (halo rows beyond a wall stay unused); Xin
+    // nullptr: the zero correction.  The halo corrections come from other CTAs of this launch after a
+    // grid barrier, so they are read past L1.
+    auto load_cells = [&](int l0, const double* Xin) {
+        for (int l = l0 + (int)threadIdx.x; l < nall; l += blockDim.x) {
+            int g;
+            if (l < ncs) g = c0 + l;
+            else if (l < ncs + rows) g = (s * rows + (l - ncs)) * nx + (nx - 1);
+            else if (l < ncs + 2 * rows) g = (s * rows + (l - ncs - rows)) * nx;
+            else if (l < ncs + 2 * rows + nx) g = s * rows > 0 ? (s * rows - 1) * nx + (l - ncs - 2 * rows) : -1;
+            else g = (s + 1) * rows < ny ? ((s + 1) * rows) * nx + (l - ncs - 2 * rows - nx) : -1;
+            double y[4] = {0.0, 0.0, 0.0, 0.0}, t[4] = {1.0, 0.0, 0.0, 1.0};
+            if (g >= 0) {
 #pragma unroll
-            for (int k = 0; k < 4; ++k) { y[k] = first ? 0.0 : X[g * 4 + k]; t[k] = B.W[g * 4 + k] + y[k]; }
-        }
-        double fx[4], fy[4];
-        euler_flux_pair(t, euler_prim(P.gm1, t), fx, fy);
+                for (int k = 0; k < 4; ++k) { y[k] = Xin ? __ldcg(Xin + g * 4 + k) : 0.0; t[k] = B.W[g * 4 + k] + y[k]; }
+            }
+            double fx[4], fy[4];
+            euler_flux_pair(t, euler_prim(P.gm1, t), fx, fy);
 #pragma unroll
-        for (int k = 0; k < 4; ++k) {
-            sY[l * 4 + k] = y[k];
-            sT[l * 4 + k] = t[k];
-            sF[l * 8 + k] = fx[k];
-            sF[l * 8 + 4 + k] = fy[k];
+            for (int k = 0; k < 4; ++k) {
+                sY[l * 4 + k] = y[k];
+                sT[l * 4 + k] = t[k];
+                sF[l * 8 + k] = fx[k];
+                sF[l * 8 + 4 + k] = fy[k];
+            }
         }
-    }
+    };
+    load_cells(0, first ? nullptr : X);
     // the diagonal 1/dt_ps + 0.5 * sum_faces(L * gamma) / area is fixed through the sweeps; the face
     // products are rounded before they are summed in face order, as the reference loop does
     __syncthreads();
@@ -820,70 +866,87 @@ __global__ void __launch_bounds__(kPrThreads, 1) k_im_pr2_sweep(LoParams P, LoBu
     pr_wall_terms(P, Q, s, rows, sW, sY, sWf, sWd);
     __syncthreads();
     const int ndiag = rows + nx - 1;
-    for (int pass = 0; pass < 2; ++pass) {
-        if (pass == 1) {   // the wall-row cells relaxed in the first pass
+    for (int sw = 0; sw < sweeps; ++sw) {
+        double* out = (sw & 1) ? X : Y;
+        if (sw > 0) {   // the previous sweep's halo corrections, then this sweep's wall terms
+            if (!pr_grid_barrier(I.prbar)) {
+                if (threadIdx.x == 0) stop_with(I, B.status, ST_TIMEOUT);
+                return;
+            }
+            if (__ldcg(I.state + IS_STOP) != 0.0) return;   // a slab of the previous sweep failed
+            load_cells(ncs, (sw & 1) ? Y : X);
             __syncthreads();
             pr_wall_terms(P, Q, s, rows, sW, sY, sWf, sWd);
             __syncthreads();
         }
-        if ((int)threadIdx.x >= wave_warps * 32) continue;
-        for (int dd = 0; dd < ndiag; ++dd) {
-            const int d = pass == 0 ? dd : ndiag - 1 - dd;
-            for (int t0 = 0; t0 < dcells; t0 += D) {
-                int i = 0, jl = 0;
-                const bool act = (int)threadIdx.x < wave && diag_cell(d, tc + t0, rows, nx, i, jl);
-                const int j = s * rows + jl, cl = jl * nx + i;
-                double tm = 0.0;
-                if (act) {   // lane = component m of cell (i, j)
-                    double sdt = 0.0, sgn = 0.0;
-#pragma unroll
-                    for (int f = 0; f < 4; ++f) {
-                        const int dir = (f >> 1) * 4 + m;
-                        const bool neg = (f & 1) == 0;   // left and bottom faces: normals (-1,0), (0,-1)
-                        const double flen = f < 2 ? P.dy : P.dx;
-                        const double fo = sF[cl * 8 + dir];
-                        const double fi = neg ? -fo : fo;
-                        const int nl = pr_neighbour(i, jl, j, f, rows, nx, ny);
-                        double fj, dnb;
-                        if (nl < 0) {
-                            const int w = (f == 3 ? nx : 0) + i;
-                            fj = sWf[w * 4 + m];
-                            dnb = sWd[w * 4 + m];
-                        } else {
-                            const double fn = sF[nl * 8 + dir];
-                            fj = neg ? -fn : fn;
-                            dnb = sY[nl * 4 + m];
-                        }
-                        const double dti = fi - sFi[m * ncf + cl * 4 + f];
-                        const double sm4 = dti + (fj - sFj[m * ncf + cl * 4 + f]);
-                        if (!isfinite(sm4)) bad = 1;
-                        sdt = __dadd_rn(sdt, __dmul_rn(flen, sm4));
-                        sgn = __dadd_rn(sgn, __dmul_rn(__dmul_rn(flen, sG[cl * 4 + f]), dnb));
-                    }
-                    const double rhs = sR[cl * 4 + m] - div_area(0.5 * 1.0 * sdt, P) + div_area(0.5 * 1.0 * sgn, P);
-                    if (!isfinite(rhs)) bad = 1;
-                    const double y = div_by_recip(rhs, sD[cl], sRd[cl]);
-                    tm = sW[cl * 4 + m] + y;
-                    sY[cl * 4 + m] = y;
-                    sT[cl * 4 + m] = tm;
-                }
-                // the relaxed state's flux pair, its components gathered from the cell's 4 lanes (every
-                // lane of the warp takes part in the shuffles)
-                double t[4];
-#pragma unroll
-                for (int k = 0; k < 4; ++k) t[k] = __shfl_sync(0xffffffffu, tm, (threadIdx.x & ~3) + k);
-                if (act) {
-                    double fx[4], fy[4];
-                    euler_flux_pair(t, euler_prim(P.gm1, t), fx, fy);
-                    sF[cl * 8 + m] = m == 0 ? fx[0] : (m == 1 ? fx[1] : (m == 2 ? fx[2] : fx[3]));
-                    sF[cl * 8 + 4 + m] = m == 0 ? fy[0] : (m == 1 ? fy[1] : (m == 2 ? fy[2] : fy[3]));
-                }
+        for (int pass = 0; pass < 2 && !dead; ++pass) {
+            if (pass == 1) {   // the wall-row cells relaxed in the first pass
+                __syncthreads();
+                pr_wall_terms(P, Q, s, rows, sW, sY, sWf, sWd);
+                __syncthreads();
             }
-            pr_wave_sync(wave_warps);
+            if ((int)threadIdx.x >= wave_warps * 32) continue;
+            for (int dd = 0; dd < ndiag; ++dd) {
+                const int d = pass == 0 ? dd : ndiag - 1 - dd;
+                for (int t0 = 0; t0 < dcells; t0 += D) {
+                    int i = 0, jl = 0;
+                    const bool act = (int)threadIdx.x < wave && diag_cell(d, tc + t0, rows, nx, i, jl);
+                    const int j = s * rows + jl, cl = jl * nx + i;
+                    double tm = 0.0;
+                    if (act) {   // lane = component m of cell (i, j)
+                        double sdt = 0.0, sgn = 0.0;
+    #pragma unroll
+                        for (int f = 0; f < 4; ++f) {
+                            const int dir = (f >> 1) * 4 + m;
+                            const bool neg = (f & 1) == 0;   // left and bottom faces: normals (-1,0), (0,-1)
+                            const double flen = f < 2 ? P.dy : P.dx;
+                            const double fo = sF[cl * 8 + dir];
+                            const double fi = neg ? -fo : fo;
+                            const int nl = pr_neighbour(i, jl, j, f, rows, nx, ny);
+                            double fj, dnb;
+                            if (nl < 0) {
+                                const int w = (f == 3 ? nx : 0) + i;
+                                fj = sWf[w * 4 + m];
+                                dnb = sWd[w * 4 + m];
+                            } else {
+                                const double fn = sF[nl * 8 + dir];
+                                fj = neg ? -fn : fn;
+                                dnb = sY[nl * 4 + m];
+                            }
+                            const double dti = fi - sFi[m * ncf + cl * 4 + f];
+                            const double sm4 = dti + (fj - sFj[m * ncf + cl * 4 + f]);
+                            if (!isfinite(sm4)) bad = 1;
+                            sdt = __dadd_rn(sdt, __dmul_rn(flen, sm4));
+                            sgn = __dadd_rn(sgn, __dmul_rn(__dmul_rn(flen, sG[cl * 4 + f]), dnb));
+                        }
+                        const double rhs = sR[cl * 4 + m] - div_area(0.5 * 1.0 * sdt, P) + div_area(0.5 * 1.0 * sgn, P);
+                        if (!isfinite(rhs)) bad = 1;
+                        const double y = div_by_recip(rhs, sD[cl], sRd[cl]);
+                        tm = sW[cl * 4 + m] + y;
+                        sY[cl * 4 + m] = y;
+                        sT[cl * 4 + m] = tm;
+                    }
+                    // the relaxed state's flux pair, its components gathered from the cell's 4 lanes (every
+                    // lane of the warp takes part in the shuffles)
+                    double t[4];
+    #pragma unroll
+                    for (int k = 0; k < 4; ++k) t[k] = __shfl_sync(0xffffffffu, tm, (threadIdx.x & ~3) + k);
+                    if (act) {
+                        double fx[4], fy[4];
+                        euler_flux_pair(t, euler_prim(P.gm1, t), fx, fy);
+                        sF[cl * 8 + m] = m == 0 ? fx[0] : (m == 1 ? fx[1] : (m == 2 ? fx[2] : fx[3]));
+                        sF[cl * 8 + 4 + m] = m == 0 ? fy[0] : (m == 1 ? fy[1] : (m == 2 ? fy[2] : fy[3]));
+                    }
+                }
+                pr_wave_sync(wave_warps);
+            }
         }
+        __syncthreads();
+        if (!dead)
+            for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) out[c0 * 4 + q] = sY[q];
+        if (sw < sweeps - 1 && __syncthreads_or(bad) && threadIdx.x == 0) stop_with(I, B.status, ST_NONFINITE_STATE);
     }
-    __syncthreads();
-    for (int q = threadIdx.x; q < ncs * 4; q += blockDim.x) Y[c0 * 4 + q] = sY[q];
+    if (dead) return;
     if (last) {
         const int lv = alpha_levels(Q.min_alpha);
         for (int cl = threadIdx.x; cl < ncs; cl += blockDim.x) {
@@ -1518,7 +1581,7 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
             e = Q.high_order ? s2_enqueue(1, P, Bpre, I.s2, s, s2, fork, join) : im_fluxes(P, Bpre, s, s2, fork, join);
         if (e == cudaSuccess) e = mark(im_cell(0, P, Bpre, Q, I, nullptr, s));   // ComputeResidual + diagnostics
     }
-    const double* X = I.dwA;
+    double* X = I.dwA;
     double* Y = I.dwB;
     const int rows = P.ny / Q.nslab, ncs = rows * P.nx;
     const int dcells = rows < P.nx ? rows : P.nx;                              // longest anti-diagonal
@@ -1526,11 +1589,19 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     // SolveMacroPR2 with its set-up fused into the first sweep and BuildPredictedMacroState into the
     // last; a single sweep resets the alpha masks beforehand (its CTAs AND into them as they finish)
     if (e == cudaSuccess && Q.macro_sweeps == 1) e = cudaMemsetAsync(I.mask, 0xff, 2 * sizeof(unsigned), s);
-    for (int sw = 0; sw < Q.macro_sweeps && e == cudaSuccess; ++sw) {
-        k_im_pr2_sweep<<<Q.nslab, kPrThreads, (size_t)pr_smem_words(rows, P.nx) * sizeof(double), s>>>(
-            P, B, Q, I, X, Y, sw == 0, sw == Q.macro_sweeps - 1);
-        e = cudaGetLastError();
-        const double* t = Y; Y = const_cast<double*>(X); X = t;
+    if (e == cudaSuccess) {   // all sweeps in one launch, its slabs meeting at a grid barrier between them
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3((unsigned)Q.nslab);
+        cfg.blockDim = dim3(kPrThreads);
+        cfg.dynamicSmemBytes = (size_t)pr_smem_words(rows, P.nx) * sizeof(double);
+        cfg.stream = s;
+        cudaLaunchAttribute coop[1];
+        coop[0].id = cudaLaunchAttributeCooperative;
+        coop[0].val.cooperative = 1;
+        cfg.attrs = coop;
+        cfg.numAttrs = Q.macro_sweeps > 1 ? 1 : 0;
+        e = cudaLaunchKernelEx(&cfg, k_im_pr2_sweep, P, B, Q, I, X, Y, 1, 1, Q.macro_sweeps);
+        if (Q.macro_sweeps % 2 == 1) X = Y;   // the last sweep's corrections (Y when the count is odd)
     }
     e = mark(e);
     if (e == cudaSuccess) e = mark(im_cell(2, P, B, Q, I, X, s));                // BuildPredictedEquilibrium
@@ -1550,7 +1621,7 @@ cudaError_t enqueue_implicit_step(const LoParams& P, const LoBuffers& B, const I
     // (counted once per sequence by ugks_implicit_init / ugks_implicit_restore); the gate replaces the
     // pre-update residual in the count
     const int evaluation = Q.high_order ? s2_enqueue_kernels(1) : 3;
-    if (launches) *launches += 9 + Q.macro_sweeps + (cond ? evaluation : 2 * evaluation);
+    if (launches) *launches += 10 + (cond ? evaluation : 2 * evaluation);
     return e;
 }
 

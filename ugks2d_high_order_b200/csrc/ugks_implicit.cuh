@@ -83,6 +83,7 @@ struct ImBuffers {
     unsigned* counter;      // [1] last-CTA counter of the implicit kernels
     unsigned* stopw;        // [1] nonzero once the stop flag is set: the evaluation kernels of the step
                             // sequence see it through LoBuffers::halt and return at entry
+    unsigned* prbar;        // [2] grid barrier between the PR(2) sweeps of one launch: arrivals, generation
 };
 
 }  // namespace ugks
