@@ -501,8 +501,10 @@ def main():
     sampler.start()
     gc.collect()
     gc.disable()
-    for _ in range(args.warmup):
-        solve()
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):   # as the timed loop, flush included (its first call loads its kernel)
+            flush.zero_()
+            solve()
     launches0 = s.launch_count
     barrier()
     sampler.begin()
