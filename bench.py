@@ -160,6 +160,8 @@ class ClockSampler:
         the warm-up, so its start-up is not inside the window) are dropped."""
         with self._lock:
             self.samples, self.reasons = [], set()
+        if self.kind == "nvml" and getattr(self, "nv", None):
+            self._poll_once()   # a sample at the window's start, whatever the polling phase
 
     def start(self):
         if self.kind == "none":
@@ -189,19 +191,22 @@ class ClockSampler:
         self.t = threading.Thread(target=self._poll_nvml, daemon=True)
         self.t.start()
 
-    def _poll_nvml(self):
+    def _poll_once(self):
         nv = self.nv
+        try:
+            mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
+            mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+            with self._lock:
+                self.samples.append(mhz)
+                for name, bit in self.REASONS.items():
+                    if mask & bit:
+                        self.reasons.add(name)
+        except Exception:
+            pass
+
+    def _poll_nvml(self):
         while not self._stop.is_set():
-            try:
-                mhz = float(nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM))
-                mask = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
-                with self._lock:
-                    self.samples.append(mhz)
-                    for name, bit in self.REASONS.items():
-                        if mask & bit:
-                            self.reasons.add(name)
-            except Exception:
-                pass
+            self._poll_once()
             self._stop.wait(self.period)
 
     def _read_smi(self):
